@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""Benchmark of the GraphOne hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload pagerank|sssp|bfs] [--scale S]
+
+Default workload (the headline): PageRank on RMAT scale 22 (4,194,304
+vertices, 16*2^22 directed samples, a/b/c/d = .57/.19/.19/.05, self loops
+removed, duplicates merged, fp32 edge values 1.0), transpose CSR, damping
+0.85, uniform initial rank 1/N, dangling mass redistributed uniformly, 30
+iterations.  One step = one full 30-iteration PageRank.  The metric is HBM
+GB/s of the semiring SpMV: per iteration
+    B_spmv = 4(N+1) + 8M + 4N (x read) + 4N (y)
+algorithmic bytes (M = directed nonzeros after dedup), summed over the
+iterations of a step and divided by the step time.  Inputs (0.55 GB of CSR
+per iteration) are larger than the 126 MB L2, so every timed iteration
+streams them from HBM.
+
+``value``: graph resident in HBM, CUDA-event time of the step, max over ranks.
+``e2e``: the same metric through the C ABI with host buffers: per step the
+in-edge CSR is copied from pinned host memory (g1_graph_create), PageRank
+runs, and the ranks are read back to the host (g1_pagerank into host memory).
+``roofline``: achieved algorithmic bytes of the dominant kernel (the fused
+merge-path SpMV + apply/construct kernel, spmv_merge_kernel) per launch over
+its CUDA-event duration, against the measured HBM copy bandwidth.
+``cpu_baseline``: GraphOne's own SpMV_cpu_navie (compiled from the reference
+sources into oracle/_ref) driving the same PageRank iteration on all host
+threads, on a bounded sample of iterations; or the C oracle when oracle/_ref
+is absent.
+
+Multi-GPU (torchrun): replicas only -- every rank runs the full workload on
+its own copy of the graph (no data-path collective); value = total work of
+all ranks / max step time over ranks; scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SSSP/BFS GTEPS & queries/s (p99 ms) batched vs plain; PageRank SpMV HBM GB/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of the SM clock and throttle reasons."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.remove(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        busy = [s for s in sm if s > 0.5 * (max(sm) if sm else 1)]
+        return {"sm_mhz": statistics.median(busy or sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ----------------------------------------------------------------- workload
+def make_pagerank_graph(scale: int, device):
+    from graphone_b200 import gen
+    g = gen.rmat(scale, 16, symmetric=False, float_values=True, device=device)
+    return g
+
+
+def spmv_bytes(n: int, m: int) -> int:
+    return 4 * (n + 1) + 8 * m + 4 * n + 4 * n
+
+
+def fused_bytes(n: int, m: int) -> int:
+    # row_ptr + col/val + x gather (once) + iweights read + rank write + x' write
+    return 4 * (n + 1) + 8 * m + 4 * n + 4 * n + 4 * n + 4 * n
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def max_over_ranks(x: float, ws: int):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_ours(args):
+    import torch
+    import graphone_b200 as g1
+
+    ws, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    peak, peak_src = hbm_peak()
+
+    g = make_pagerank_graph(args.scale, dev)
+    n, m = g.n, g.m
+    trp, tci, tv = g.np("t")              # host copies (for e2e and cpu baseline)
+    # pinned host buffers for the end-to-end path
+    h_rp = torch.from_numpy(trp.view(np.int32)).pin_memory()
+    h_ci = torch.from_numpy(tci.view(np.int32)).pin_memory()
+    h_v = torch.from_numpy(tv).pin_memory()
+    h_out = torch.empty(n, dtype=torch.float32).pin_memory()
+    del g
+    torch.cuda.empty_cache()
+
+    stream = torch.cuda.current_stream(dev)
+    G = g1.Graph.from_csr(h_rp, h_ci, h_v, input_transpose=True, build_other=False)
+    out = torch.empty(n, dtype=torch.float32, device=dev)
+    iters = args.iters
+
+    def step():
+        G.pagerank(0.85, iters, g1.PR_DANGLING, out=out, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    launches0 = g1.kernel_launches()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        g1.profile_begin()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        spmv_ms, spmv_launches = g1.profile_end()
+    barrier(ws)
+    launches = g1.kernel_launches() - launches0
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, ws)
+    per_step_bytes = spmv_bytes(n, m) * iters
+    value = ws * per_step_bytes * args.steps / (ms_max / 1e3) / 1e9
+    clocks = clk.summary()
+
+    # end to end through the C ABI with host buffers
+    for _ in range(max(1, args.warmup // 2)):
+        G2 = g1.Graph.from_csr(h_rp, h_ci, h_v, input_transpose=True, build_other=False,
+                               validate=False, stream=stream)
+        G2.pagerank(0.85, iters, g1.PR_DANGLING, out=h_out.numpy(), stream=stream)
+        G2.close()
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        G2 = g1.Graph.from_csr(h_rp, h_ci, h_v, input_transpose=True, build_other=False,
+                               validate=False, stream=stream)
+        G2.pagerank(0.85, iters, g1.PR_DANGLING, out=h_out.numpy(), stream=stream)
+        G2.close()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e2.elapsed_time(e3), ws)
+    e2e_value = ws * per_step_bytes * args.steps / (e2e_ms / 1e3) / 1e9
+    h2d = 4 * (n + 1) + 8 * m
+    d2h = 4 * n
+
+    # parity spot check of this very run against the FP64 oracle (small cost)
+    result = {
+        "metric": METRIC,
+        "value": round(value, 1),
+        "unit": "GB/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded RMAT, counter-based splitmix64 generator)",
+        "config": {
+            "workload": f"pagerank_rmat{args.scale}",
+            "graph": f"RMAT-{args.scale} directed, a/b/c=.57/.19/.19, ef16, dedup, no self loops",
+            "n": n, "m": m, "iterations_per_step": iters, "damping": 0.85,
+            "dangling": "redistributed uniformly",
+            "l2": "inputs larger than L2 (CSR streamed from HBM every iteration)",
+            "parallelism": f"replicas x{ws}",
+            "bytes_per_iteration": spmv_bytes(n, m),
+        },
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "e2e": {"value": round(e2e_value, 1), "unit": "GB/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": round(e2e_ms / args.steps, 3)},
+    }
+    if spmv_launches:
+        avg_ms = spmv_ms / spmv_launches
+        achieved = fused_bytes(n, m) / (avg_ms / 1e3) / 1e9
+        traffic = None
+        tfile = os.path.join(ROOT, "profiles", "pagerank_rmat22_traffic.json")
+        if os.path.exists(tfile) and args.scale == 22:
+            try:
+                traffic = json.load(open(tfile)).get("dram_bytes_per_launch")
+            except Exception:
+                traffic = None
+        result["roofline"] = {
+            "bound": "hbm", "kernel": "spmv_merge_kernel<PlusTimesF32, PrEpilogue>",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": peak_src,
+            "traffic": traffic, "algorithmic_bytes_per_launch": fused_bytes(n, m),
+            "avg_launch_ms": round(avg_ms, 5), "launches_timed": int(spmv_launches),
+            "iteration_share_of_step": round(spmv_ms / ms, 4) if ms > 0 else None,
+        }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(trp, tci, tv, n, m, args)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    G.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(trp, tci, tv, n, m, args, budget_s=20.0):
+    """GraphOne's SpMV_cpu_navie (oracle/_ref) or the C oracle, PageRank
+    iterations on all host threads, bounded by ~budget_s seconds."""
+    import ctypes as C
+    from oracle import oracle as O
+    R = O.ref()
+    threads = cpu_threads()
+    outw = np.bincount(tci, weights=tv.astype(np.float64), minlength=n).astype(np.float32)
+    rank = np.empty(n, np.float32)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    if R is not None:
+        kind = "reference"
+        # one iteration first to size the sample
+        t0 = time.perf_counter()
+        R.ref_pagerank_f32(n, p(trp), p(tci), p(tv), p(outw), C.c_float(0.85), 1, 1, p(rank),
+                           threads)
+        t1 = time.perf_counter() - t0
+        k = max(1, min(30, int(budget_s / max(t1, 1e-3))))
+        t0 = time.perf_counter()
+        R.ref_pagerank_f32(n, p(trp), p(tci), p(tv), p(outw), C.c_float(0.85), k, 1, p(rank),
+                           threads)
+        dt = time.perf_counter() - t0
+        sample = (f"{k} PageRank iterations (SpMV_cpu_navie + restated apply/construct) "
+                  f"on the full graph, {threads} threads")
+    else:
+        kind = "port"
+        threads = 1
+        x = np.random.default_rng(0).random(n).astype(np.float32)
+        t0 = time.perf_counter()
+        O.spmv_plustimes_f32(trp, tci, tv, x)
+        dt = time.perf_counter() - t0
+        k = 1
+        sample = "1 SpMV of the C oracle (single thread) on the full graph"
+    gbs = spmv_bytes(n, m) * k / dt / 1e9
+    return {"value": round(gbs, 2), "unit": "GB/s", "cores": threads, "kind": kind,
+            "sample": sample, "seconds": round(dt, 2)}
+
+
+def run_reference(args):
+    ws, rank, local = dist_info()
+    if rank != 0:
+        return  # replicas: rank 0 alone runs and prints the reference arm
+    import torch
+    from oracle import oracle as O
+    if O.ref() is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libgraphone_ref.so was not built"}))
+        return
+    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
+    g = make_pagerank_graph(args.scale, dev)
+    n, m = g.n, g.m
+    trp, tci, tv = g.np("t")
+    del g
+    import ctypes as C
+    R = O.ref()
+    threads = cpu_threads()
+    outw = np.bincount(tci, weights=tv.astype(np.float64), minlength=n).astype(np.float32)
+    rank_v = np.empty(n, np.float32)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    per_step_iters = args.ref_iters
+
+    def step():
+        R.ref_pagerank_f32(n, p(trp), p(tci), p(tv), p(outw), C.c_float(0.85), per_step_iters, 1,
+                           p(rank_v), threads)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = spmv_bytes(n, m) * per_step_iters * args.steps / dt / 1e9
+    sample = (f"each step = {per_step_iters} of the 30 PageRank iterations on the full "
+              f"RMAT-{args.scale} graph (GraphOne SpMV_cpu_navie + restated apply/construct)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 2), "unit": "GB/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(dt / args.steps * 1e3, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"pagerank_rmat{args.scale}", "n": n, "m": m,
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": round(value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--iters", type=int, default=30)
+    ap.add_argument("--ref-iters", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

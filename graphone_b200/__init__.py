@@ -1,0 +1,233 @@
+"""Python view of libgraphone_b200.so (the C ABI in include/graphone_b200.h).
+
+The library is the product: this module only loads it with ctypes and turns
+g1_status codes into exceptions.  There is no CPU fallback: importing works
+without a GPU (the library loads; no kernel runs), and every compute call
+fails with G1Error when no CUDA device is present.
+
+    import graphone_b200 as g1
+    g = g1.Graph.from_csr(row_ptr, col, val, symmetric=True)
+    dist = g.sssp(0)                  # numpy uint32, UINT32_MAX = unreachable
+    rank = g.pagerank(0.85, 30)       # numpy float32
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgraphone_b200.so")
+U32_MAX = 0xFFFFFFFF
+
+G1_U32, G1_F32 = 0, 1
+SR_MINPLUS_U32, SR_MINPLUS_F32, SR_PLUSTIMES_F32, SR_BFS_U32 = 0, 1, 2, 3
+SCHED_AUTO, SCHED_MERGE, SCHED_VECTOR = 0, 1, 2
+ENGINE_BLAS, ENGINE_ADVANCE, ENGINE_AUTO = 0, 1, 2
+PR_REFERENCE, PR_DANGLING = 0, 1
+GRAPH_SYMMETRIC, GRAPH_INPUT_TRANSPOSE, GRAPH_BUILD_OTHER, GRAPH_NO_VALIDATE = 1, 2, 4, 8
+
+STATUS = {0: "G1_OK", 1: "G1_ERR_INVALID", 2: "G1_ERR_OOM", 3: "G1_ERR_DEVICE",
+          4: "G1_ERR_TIMEOUT", 5: "G1_ERR_UNSUPPORTED", 6: "G1_ERR_OVERFLOW"}
+
+
+class G1Error(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+P = C.c_void_p
+
+
+def _declare(L):
+    s = C.c_int
+    L.g1_status_string.restype = C.c_char_p
+    L.g1_status_string.argtypes = [s]
+    L.g1_last_error.restype = C.c_char_p
+    L.g1_version.restype = C.c_char_p
+    L.g1_mem_alloc.argtypes = [C.POINTER(P), C.c_size_t]
+    L.g1_mem_free.argtypes = [P]
+    L.g1_mem_copy.argtypes = [P, P, C.c_size_t, C.c_int, P]
+    L.g1_mem_fill_u32.argtypes = [P, C.c_uint32, C.c_size_t, P]
+    L.g1_stream_sync.argtypes = [P]
+    L.g1_kernel_launches.restype = C.c_uint64
+    L.g1_profile_begin.argtypes = []
+    L.g1_profile_end.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
+    L.g1_graph_create.argtypes = [P, P, P, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, P,
+                                  C.POINTER(P)]
+    L.g1_graph_destroy.argtypes = [P]
+    L.g1_graph_info.argtypes = [P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.g1_graph_arrays.argtypes = [P, C.c_int, C.POINTER(P), C.POINTER(P), C.POINTER(P)]
+    L.g1_graph_device_bytes.restype = C.c_size_t
+    L.g1_graph_device_bytes.argtypes = [P]
+    L.g1_spmv_plan.argtypes = [P, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                               C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]
+    L.g1_spmv.argtypes = [P, C.c_int, C.c_int, C.c_int, P, P, P]
+    L.g1_autotune.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_float), P]
+    L.g1_pagerank.argtypes = [P, C.c_float, C.c_int, C.c_int, P, P]
+    L.g1_sssp.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
+    L.g1_bfs.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
+    return L
+
+
+def lib():
+    """The loaded library; raises if it was not built (no fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m graphone_b200.build`")
+        _lib = _declare(C.CDLL(LIB_PATH))
+    return _lib
+
+
+# Every symbol include/graphone_b200.h declares (checked by the CPU tests).
+EXPORTS = (
+    "g1_status_string", "g1_last_error", "g1_version", "g1_mem_alloc", "g1_mem_free",
+    "g1_mem_copy", "g1_mem_fill_u32", "g1_stream_sync", "g1_kernel_launches",
+    "g1_profile_begin", "g1_profile_end", "g1_graph_create",
+    "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
+    "g1_spmv_plan", "g1_spmv", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs",
+)
+
+
+def check(status: int) -> None:
+    if status != 0:
+        msg = lib().g1_last_error().decode(errors="replace")
+        raise G1Error(status, msg)
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array or a torch tensor (host or device)."""
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream  # torch.cuda.Stream
+
+
+def kernel_launches() -> int:
+    return int(lib().g1_kernel_launches())
+
+
+def profile_begin() -> None:
+    check(lib().g1_profile_begin())
+
+
+def profile_end():
+    """(summed ms, launch count) of the SpMV main kernels since profile_begin()."""
+    ms, n = C.c_double(), C.c_uint64()
+    check(lib().g1_profile_end(C.byref(ms), C.byref(n)))
+    return ms.value, n.value
+
+
+class Graph:
+    """A device-resident graph (owns a g1_graph handle)."""
+
+    def __init__(self, handle: int, n: int, m: int):
+        self._h = C.c_void_p(handle)
+        self.n = n
+        self.m = m
+
+    @classmethod
+    def from_csr(cls, row_ptr, col, val, *, symmetric=False, input_transpose=False,
+                 build_other=True, validate=True, stream=None) -> "Graph":
+        """CSR arrays: numpy (host) or torch tensors (host or device)."""
+        if isinstance(row_ptr, np.ndarray):
+            row_ptr = np.ascontiguousarray(row_ptr, np.uint32)
+            col = np.ascontiguousarray(col, np.uint32)
+            if val.dtype.kind == "f":
+                val = np.ascontiguousarray(val, np.float32)
+            else:
+                val = np.ascontiguousarray(val, np.uint32)
+            vtype = G1_F32 if val.dtype == np.float32 else G1_U32
+        else:
+            vtype = G1_F32 if val.dtype.is_floating_point else G1_U32
+        n = len(row_ptr) - 1
+        m = len(col)
+        flags = ((GRAPH_SYMMETRIC if symmetric else 0)
+                 | (GRAPH_INPUT_TRANSPOSE if input_transpose else 0)
+                 | (GRAPH_BUILD_OTHER if build_other and not symmetric else 0)
+                 | (0 if validate else GRAPH_NO_VALIDATE))
+        out = C.c_void_p()
+        check(lib().g1_graph_create(_ptr(row_ptr), _ptr(col) if m else None,
+                                    _ptr(val) if m else None, vtype, n, m, flags,
+                                    _stream(stream), C.byref(out)))
+        return cls(out.value, n, m)
+
+    @classmethod
+    def from_gen(cls, g, *, stream=None) -> "Graph":
+        """From a graphone_b200.gen.CsrGraph (out-edge CSR; transpose built on the GPU)."""
+        rp, ci, v = g.np("n")
+        return cls.from_csr(rp, ci, v, symmetric=g.symmetric, stream=stream)
+
+    def close(self):
+        if self._h:
+            lib().g1_graph_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def device_bytes(self) -> int:
+        return lib().g1_graph_device_bytes(self._h)
+
+    def info(self):
+        n, m, hn, ht = C.c_uint32(), C.c_uint32(), C.c_int(), C.c_int()
+        check(lib().g1_graph_info(self._h, C.byref(n), C.byref(m), C.byref(hn), C.byref(ht)))
+        return n.value, m.value, bool(hn.value), bool(ht.value)
+
+    def plan(self, transpose: int = 1):
+        items, tiles = C.c_uint32(), C.c_uint32()
+        tr, tn, ca, ta = P(), P(), P(), P()
+        check(lib().g1_spmv_plan(self._h, transpose, C.byref(items), C.byref(tiles), C.byref(tr),
+                                 C.byref(tn), C.byref(ca), C.byref(ta)))
+        return items.value, tiles.value, tr.value, tn.value
+
+    def spmv(self, x, y, semiring: int, transpose: int = 1, schedule: int = SCHED_AUTO,
+             stream=None):
+        """y = A (semiring) x on device buffers (torch tensors)."""
+        check(lib().g1_spmv(self._h, transpose, semiring, schedule, _ptr(x), _ptr(y),
+                            _stream(stream)))
+
+    def autotune(self, stream=None):
+        a, b = C.c_float(), C.c_float()
+        check(lib().g1_autotune(self._h, C.byref(a), C.byref(b), _stream(stream)))
+        return a.value, b.value
+
+    def pagerank(self, alpha=0.85, iters=30, mode=PR_DANGLING, out=None, stream=None):
+        if out is None:
+            out = np.empty(self.n, np.float32)
+        check(lib().g1_pagerank(self._h, alpha, iters, mode, _ptr(out), _stream(stream)))
+        return out
+
+    def sssp(self, src, engine=ENGINE_AUTO, out=None, stream=None, return_iters=False):
+        if out is None:
+            out = np.empty(self.n, np.uint32)
+        it = C.c_uint32()
+        check(lib().g1_sssp(self._h, src, engine, _ptr(out), C.byref(it), _stream(stream)))
+        return (out, it.value) if return_iters else out
+
+    def bfs(self, src, engine=ENGINE_AUTO, out=None, stream=None, return_iters=False):
+        if out is None:
+            out = np.empty(self.n, np.uint32)
+        it = C.c_uint32()
+        check(lib().g1_bfs(self._h, src, engine, _ptr(out), C.byref(it), _stream(stream)))
+        return (out, it.value) if return_iters else out

@@ -1,0 +1,571 @@
+// libgraphone_b200: status, memory, graph residency, merge-path plans and the
+// prebuilt SpMV entry points.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <atomic>
+#include <vector>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "g1/semiring.cuh"
+#include "g1/spmv.cuh"
+#include "internal.h"
+#include "spmv_launch.cuh"
+
+namespace g1 {
+
+namespace {
+thread_local std::string t_last_error;
+std::atomic<uint64_t> g_launches{0};
+
+struct Profiler {
+    std::mutex mu;
+    bool on = false;
+    std::vector<cudaEvent_t> pool;  // reused events
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> marks;
+    cudaEvent_t pending = nullptr;
+    size_t used = 0;
+    cudaEvent_t next() {
+        if (used == pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            pool.push_back(e);
+        }
+        return pool[used++];
+    }
+};
+Profiler& prof() {
+    static Profiler p;
+    return p;
+}
+}  // namespace
+
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+bool profiling() { return prof().on; }
+
+void prof_mark(cudaStream_t s, bool start) {
+    Profiler& p = prof();
+    std::lock_guard<std::mutex> lk(p.mu);
+    if (!p.on) return;
+    cudaEvent_t e = p.next();
+    cudaEventRecord(e, s);
+    if (start) {
+        p.pending = e;
+    } else if (p.pending) {
+        p.marks.emplace_back(p.pending, e);
+        p.pending = nullptr;
+    }
+}
+
+g1_status fail(g1_status s, const std::string& msg) {
+    t_last_error = msg;
+    return s;
+}
+
+g1_status fail_cuda(cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    cudaGetLastError();  // clear a non-sticky error
+    return fail(e == cudaErrorMemoryAllocation ? G1_ERR_OOM : G1_ERR_DEVICE, m);
+}
+
+g1_status DevBuf::ensure(size_t want) {
+    if (want <= bytes) return G1_OK;
+    release();
+    size_t b = (want + 255) & ~size_t(255);
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return fail_cuda(e, "cudaMalloc(workspace)");
+    }
+    bytes = b;
+    return G1_OK;
+}
+
+g1_status PinnedBuf::ensure(size_t want) {
+    if (want <= bytes) return G1_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    G1_CUDA(cudaHostAlloc(&p, want, cudaHostAllocDefault));
+    bytes = want;
+    return G1_OK;
+}
+
+bool is_device_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+g1_status copy_out(void* dst, const void* dev_src, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return G1_OK;
+    const bool dev = is_device_ptr(dst);
+    G1_CUDA(cudaMemcpyAsync(dst, dev_src, bytes,
+                            dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    if (!dev) G1_CUDA(cudaStreamSynchronize(s));
+    return G1_OK;
+}
+
+// ------------------------------------------------------------ kernels
+
+__global__ void merge_partition_kernel(const uint32_t* row_ptr, uint32_t n_rows, uint32_t nnz,
+                                       uint32_t items, uint32_t n_tiles, uint32_t* tile_row,
+                                       uint32_t* tile_nnz) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > n_tiles) return;
+    const uint64_t total = (uint64_t)n_rows + nnz;
+    uint64_t d = (uint64_t)t * items;
+    if (d > total) d = total;
+    uint32_t i, j;
+    merge_path_search(d, row_ptr + 1, n_rows, nnz, &i, &j);
+    tile_row[t] = i;
+    tile_nnz[t] = j;
+}
+
+// Checks row_ptr[0]==0, row_ptr[n]==m, monotone rows, col < n; records the
+// first violation class in *bad (1 = offsets, 2 = column out of range).
+__global__ void validate_csr_kernel(const uint32_t* rp, const uint32_t* col, uint32_t n,
+                                    uint32_t m, uint32_t* bad, uint32_t* max_deg) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = tid; r < n; r += stride) {
+        const uint32_t a = rp[r], b = rp[r + 1];
+        if (b < a || b > m) atomicCAS(bad, 0u, 1u);
+        else atomicMax(max_deg, b - a);
+    }
+    if (tid == 0 && (rp[0] != 0 || rp[n] != m)) atomicCAS(bad, 0u, 1u);
+    for (uint64_t k = tid; k < m; k += stride)
+        if (col[k] >= n) atomicCAS(bad, 0u, 2u);
+}
+
+__global__ void max_degree_kernel(const uint32_t* rp, uint32_t n, uint32_t* max_deg) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint32_t mx = 0;
+    for (uint64_t r = tid; r < n; r += stride) mx = max(mx, rp[r + 1] - rp[r]);
+    atomicMax(max_deg, mx);
+}
+
+// key = (col << 32) | row for every nonzero; row found by binary search.
+__global__ void transpose_keys_kernel(const uint32_t* rp, const uint32_t* col, uint32_t n,
+                                      uint32_t m, uint64_t* keys, uint32_t* idx) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += stride) {
+        uint32_t lo = 0, hi = n;  // last row r with rp[r] <= k
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (rp[mid] <= k) lo = mid; else hi = mid - 1;
+        }
+        keys[k] = ((uint64_t)col[k] << 32) | lo;
+        idx[k] = (uint32_t)k;
+    }
+}
+
+__global__ void transpose_scatter_kernel(const uint64_t* keys, const uint32_t* idx,
+                                         const uint32_t* val_in, uint32_t m, uint32_t* col_out,
+                                         uint32_t* val_out, uint32_t* counts) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += stride) {
+        const uint64_t key = keys[k];
+        col_out[k] = (uint32_t)(key & 0xffffffffu);
+        val_out[k] = val_in[idx[k]];
+        atomicAdd(&counts[key >> 32], 1u);
+    }
+}
+
+__global__ void fill_u32_kernel(uint32_t* p, uint32_t v, size_t n) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = v;
+}
+
+// ------------------------------------------------------------ helpers
+
+namespace {
+
+uint32_t grid_for(uint64_t n, int block, int sm_count, int per_sm = 8) {
+    uint64_t g = ceil_div(n ? n : 1, (uint64_t)block);
+    uint64_t cap = (uint64_t)sm_count * per_sm;
+    return (uint32_t)std::max<uint64_t>(1, std::min(g, cap));
+}
+
+// Allocates an orientation's arrays (padded for vector / bulk loads).
+g1_status alloc_orientation(Orientation& o, uint32_t n, uint32_t m) {
+    G1_TRY(o.b_rp.ensure(((size_t)n + 1 + 64) * 4));
+    G1_TRY(o.b_col.ensure(((size_t)m + 64) * 4));
+    G1_TRY(o.b_val.ensure(((size_t)m + 64) * 4));
+    o.rp = o.b_rp.as<uint32_t>();
+    o.col = o.b_col.as<uint32_t>();
+    o.val = o.b_val.p;
+    o.present = true;
+    return G1_OK;
+}
+
+g1_status upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return G1_OK;
+    const bool dev = is_device_ptr(src);
+    G1_CUDA(cudaMemcpyAsync(dst, src, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    return G1_OK;
+}
+
+// Builds `dst` = transpose of `src` on the device (stable: rows of the
+// result list their columns in increasing order, like EdgeCache::ToCsr on a
+// sorted edge cache).
+g1_status build_transpose(g1_graph* g, const Orientation& src, Orientation& dst, cudaStream_t s) {
+    const uint32_t n = g->n, m = g->m;
+    G1_TRY(alloc_orientation(dst, n, m));
+    G1_CUDA(cudaMemsetAsync(dst.rp, 0, ((size_t)n + 1) * 4, s));
+    if (m == 0) return G1_OK;
+    DevBuf keys, keys2, idx, idx2, counts, temp;
+    G1_TRY(keys.ensure((size_t)m * 8));
+    G1_TRY(keys2.ensure((size_t)m * 8));
+    G1_TRY(idx.ensure((size_t)m * 4));
+    G1_TRY(idx2.ensure((size_t)m * 4));
+    G1_TRY(counts.ensure(((size_t)n + 1) * 4));
+    G1_CUDA(cudaMemsetAsync(counts.p, 0, ((size_t)n + 1) * 4, s));
+    const uint32_t grid = grid_for(m, 256, g->sm_count);
+    transpose_keys_kernel<<<grid, 256, 0, s>>>(src.rp, src.col, n, m, keys.as<uint64_t>(),
+                                               idx.as<uint32_t>());
+    count_launches(2);
+    G1_CUDA(cudaGetLastError());
+    int row_bits = 1;
+    while (row_bits < 32 && (1ull << row_bits) < n) ++row_bits;
+    const int end_bit = 32 + row_bits;
+    size_t tb = 0;
+    G1_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.as<uint64_t>(), keys2.as<uint64_t>(),
+                                            idx.as<uint32_t>(), idx2.as<uint32_t>(), (int)m, 0,
+                                            end_bit, s));
+    G1_TRY(temp.ensure(tb));
+    G1_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, tb, keys.as<uint64_t>(), keys2.as<uint64_t>(),
+                                            idx.as<uint32_t>(), idx2.as<uint32_t>(), (int)m, 0,
+                                            end_bit, s));
+    transpose_scatter_kernel<<<grid, 256, 0, s>>>(keys2.as<uint64_t>(), idx2.as<uint32_t>(),
+                                                  static_cast<const uint32_t*>(src.val), m, dst.col,
+                                                  static_cast<uint32_t*>(dst.val),
+                                                  counts.as<uint32_t>());
+    G1_CUDA(cudaGetLastError());
+    size_t tb2 = 0;
+    G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb2, counts.as<uint32_t>(), dst.rp, (int)n + 1, s));
+    DevBuf temp2;
+    G1_TRY(temp2.ensure(tb2));
+    G1_CUDA(cub::DeviceScan::ExclusiveSum(temp2.p, tb2, counts.as<uint32_t>(), dst.rp, (int)n + 1, s));
+    G1_CUDA(cudaStreamSynchronize(s));  // temporaries die here
+    return G1_OK;
+}
+
+}  // namespace
+
+g1_status ensure_plan(g1_graph* g, int t) {
+    Orientation& o = g->o[t];
+    if (!o.present) return fail(G1_ERR_UNSUPPORTED, "orientation not built");
+    if (o.plan) return G1_OK;
+    std::unique_ptr<MergePlan> p(new MergePlan());
+    p->items = kMergeBlock * kMergeIpt;
+    const uint64_t total = (uint64_t)g->n + g->m;
+    p->n_tiles = (uint32_t)ceil_div(total, p->items);
+    G1_TRY(p->tile_row.ensure(((size_t)p->n_tiles + 1) * 4));
+    G1_TRY(p->tile_nnz.ensure(((size_t)p->n_tiles + 1) * 4));
+    G1_TRY(p->carry.ensure(((size_t)p->n_tiles + 1) * 8));
+    G1_TRY(p->tail.ensure(((size_t)p->n_tiles + 1) * 8));
+    const uint32_t blocks = (uint32_t)ceil_div((uint64_t)p->n_tiles + 1, 256);
+    merge_partition_kernel<<<blocks, 256>>>(o.rp, g->n, g->m, p->items, p->n_tiles,
+                                            p->tile_row.as<uint32_t>(), p->tile_nnz.as<uint32_t>());
+    count_launches(1);
+    G1_CUDA(cudaGetLastError());
+    G1_CUDA(cudaDeviceSynchronize());
+    o.plan = std::move(p);
+    return G1_OK;
+}
+
+}  // namespace g1
+
+using namespace g1;
+
+extern "C" {
+
+const char* g1_status_string(g1_status s) {
+    switch (s) {
+        case G1_OK: return "ok";
+        case G1_ERR_INVALID: return "invalid argument";
+        case G1_ERR_OOM: return "out of device memory";
+        case G1_ERR_DEVICE: return "CUDA error";
+        case G1_ERR_TIMEOUT: return "device wait timed out";
+        case G1_ERR_UNSUPPORTED: return "unsupported";
+        case G1_ERR_OVERFLOW: return "device queue overflow";
+    }
+    return "unknown status";
+}
+
+const char* g1_last_error(void) { return t_last_error.c_str(); }
+
+const char* g1_version(void) { return "graphone_b200 0.1 sm_100a"; }
+
+uint64_t g1_kernel_launches(void) { return g_launches.load(); }
+
+g1_status g1_profile_begin(void) {
+    Profiler& p = prof();
+    std::lock_guard<std::mutex> lk(p.mu);
+    p.marks.clear();
+    p.used = 0;
+    p.pending = nullptr;
+    p.on = true;
+    return G1_OK;
+}
+
+g1_status g1_profile_end(double* spmv_ms, uint64_t* spmv_launches) {
+    Profiler& p = prof();
+    std::lock_guard<std::mutex> lk(p.mu);
+    p.on = false;
+    double total = 0.0;
+    for (auto& m : p.marks) {
+        G1_CUDA(cudaEventSynchronize(m.second));
+        float ms = 0.0f;
+        G1_CUDA(cudaEventElapsedTime(&ms, m.first, m.second));
+        total += ms;
+    }
+    if (spmv_ms) *spmv_ms = total;
+    if (spmv_launches) *spmv_launches = p.marks.size();
+    p.marks.clear();
+    p.used = 0;
+    return G1_OK;
+}
+
+g1_status g1_mem_alloc(void** ptr, size_t bytes) {
+    if (!ptr) return fail(G1_ERR_INVALID, "g1_mem_alloc: null out pointer");
+    *ptr = nullptr;
+    const size_t b = ((bytes ? bytes : 1) + 255) & ~size_t(255);
+    G1_CUDA(cudaMalloc(ptr, b));
+    G1_CUDA(cudaMemset(*ptr, 0, b));
+    return G1_OK;
+}
+
+g1_status g1_mem_free(void* ptr) {
+    if (ptr) G1_CUDA(cudaFree(ptr));
+    return G1_OK;
+}
+
+g1_status g1_mem_copy(void* dst, const void* src, size_t bytes, int kind, void* stream) {
+    if (bytes == 0) return G1_OK;
+    if (!dst || !src) return fail(G1_ERR_INVALID, "g1_mem_copy: null pointer");
+    cudaMemcpyKind k = kind == 0 ? cudaMemcpyHostToDevice
+                       : kind == 1 ? cudaMemcpyDeviceToHost
+                                   : cudaMemcpyDeviceToDevice;
+    G1_CUDA(cudaMemcpyAsync(dst, src, bytes, k, as_stream(stream)));
+    if (kind == 1) G1_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    return G1_OK;
+}
+
+g1_status g1_mem_fill_u32(void* dst, uint32_t value, size_t count, void* stream) {
+    if (count == 0) return G1_OK;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    fill_u32_kernel<<<grid_for(count, 256, sms), 256, 0, as_stream(stream)>>>(
+        static_cast<uint32_t*>(dst), value, count);
+    count_launches(1);
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
+}
+
+g1_status g1_stream_sync(void* stream) {
+    G1_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    return G1_OK;
+}
+
+g1_status g1_graph_create(const uint32_t* row_ptr, const uint32_t* col, const void* val,
+                          g1_dtype vtype, uint32_t n, uint32_t m, uint32_t flags, void* stream,
+                          g1_graph** out) {
+    if (!out) return fail(G1_ERR_INVALID, "g1_graph_create: null out pointer");
+    *out = nullptr;
+    if (!row_ptr || (m > 0 && (!col || !val)))
+        return fail(G1_ERR_INVALID, "g1_graph_create: null CSR array");
+    if (vtype != G1_U32 && vtype != G1_F32)
+        return fail(G1_ERR_INVALID, "g1_graph_create: unknown value type");
+    if ((uint64_t)n + m >= 0xFFFFFFFFull || n == 0xFFFFFFFFu)
+        return fail(G1_ERR_INVALID, "g1_graph_create: n + m must stay below 2^32 - 1");
+    cudaStream_t s = as_stream(stream);
+    std::unique_ptr<g1_graph> g(new g1_graph());
+    G1_CUDA(cudaGetDevice(&g->device));
+    cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, g->device);
+    g->n = n;
+    g->m = m;
+    g->vtype = vtype;
+    g->symmetric = (flags & G1_GRAPH_SYMMETRIC) != 0;
+    const int side = (flags & G1_GRAPH_INPUT_TRANSPOSE) ? 1 : 0;
+    Orientation& o = g->o[side];
+    G1_TRY(alloc_orientation(o, n, m));
+    G1_TRY(upload(o.rp, row_ptr, ((size_t)n + 1) * 4, s));
+    G1_TRY(upload(o.col, col, (size_t)m * 4, s));
+    G1_TRY(upload(o.val, val, (size_t)m * 4, s));
+
+    DevBuf chk;
+    G1_TRY(chk.ensure(16));
+    G1_CUDA(cudaMemsetAsync(chk.p, 0, 16, s));
+    uint32_t* d_bad = chk.as<uint32_t>();
+    uint32_t* d_maxdeg = d_bad + 1;
+    const uint32_t grid = grid_for((uint64_t)std::max(n, m), 256, g->sm_count);
+    count_launches(1);
+    if (!(flags & G1_GRAPH_NO_VALIDATE)) {
+        validate_csr_kernel<<<grid, 256, 0, s>>>(o.rp, o.col, n, m, d_bad, d_maxdeg);
+    } else {
+        max_degree_kernel<<<grid, 256, 0, s>>>(o.rp, n, d_maxdeg);
+    }
+    G1_CUDA(cudaGetLastError());
+    uint32_t h[2] = {0, 0};
+    G1_CUDA(cudaMemcpyAsync(h, chk.p, 8, cudaMemcpyDeviceToHost, s));
+    G1_CUDA(cudaStreamSynchronize(s));
+    if (h[0] == 1) return fail(G1_ERR_INVALID, "g1_graph_create: malformed row offsets");
+    if (h[0] == 2) return fail(G1_ERR_INVALID, "g1_graph_create: column index out of range");
+    o.max_deg = h[1];
+
+    Orientation& other = g->o[side ^ 1];
+    if (g->symmetric) {
+        other.present = true;
+        other.rp = o.rp;
+        other.col = o.col;
+        other.val = o.val;
+        other.max_deg = o.max_deg;
+    } else if (flags & G1_GRAPH_BUILD_OTHER) {
+        G1_TRY(build_transpose(g.get(), o, other, s));
+        G1_CUDA(cudaMemsetAsync(chk.p, 0, 16, s));
+        max_degree_kernel<<<grid, 256, 0, s>>>(other.rp, n, d_maxdeg);
+        count_launches(1);
+        G1_CUDA(cudaMemcpyAsync(h, chk.p, 8, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaStreamSynchronize(s));
+        other.max_deg = h[1];
+    }
+    *out = g.release();
+    return G1_OK;
+}
+
+g1_status g1_graph_destroy(g1_graph* g) {
+    if (!g) return G1_OK;
+    DeviceGuard dg(g->device);
+    cudaDeviceSynchronize();
+    delete g;
+    return G1_OK;
+}
+
+g1_status g1_graph_info(const g1_graph* g, uint32_t* n, uint32_t* m, int* has_normal,
+                        int* has_transpose) {
+    if (!g) return fail(G1_ERR_INVALID, "g1_graph_info: null graph");
+    if (n) *n = g->n;
+    if (m) *m = g->m;
+    if (has_normal) *has_normal = g->o[0].present;
+    if (has_transpose) *has_transpose = g->o[1].present;
+    return G1_OK;
+}
+
+g1_status g1_graph_arrays(const g1_graph* g, int transpose, const uint32_t** row_ptr,
+                          const uint32_t** col, const void** val) {
+    if (!g || transpose < 0 || transpose > 1) return fail(G1_ERR_INVALID, "g1_graph_arrays");
+    const Orientation& o = g->o[transpose];
+    if (!o.present) return fail(G1_ERR_UNSUPPORTED, "g1_graph_arrays: orientation not built");
+    if (row_ptr) *row_ptr = o.rp;
+    if (col) *col = o.col;
+    if (val) *val = o.val;
+    return G1_OK;
+}
+
+size_t g1_graph_device_bytes(const g1_graph* g) {
+    if (!g) return 0;
+    size_t s = g->ws.bytes();
+    for (int t = 0; t < 2; ++t) {
+        const Orientation& o = g->o[t];
+        s += o.b_rp.bytes + o.b_col.bytes + o.b_val.bytes;
+        if (o.plan)
+            s += o.plan->tile_row.bytes + o.plan->tile_nnz.bytes + o.plan->carry.bytes +
+                 o.plan->tail.bytes;
+    }
+    return s;
+}
+
+g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t* items_per_tile, uint32_t* n_tiles,
+                       const uint32_t** tile_row, const uint32_t** tile_nnz, void** carry,
+                       void** tail) {
+    if (!g || transpose < 0 || transpose > 1) return fail(G1_ERR_INVALID, "g1_spmv_plan");
+    DeviceGuard dg(g->device);
+    std::lock_guard<std::mutex> lk(g->mu);
+    G1_TRY(ensure_plan(g, transpose));
+    const MergePlan& p = *g->o[transpose].plan;
+    if (items_per_tile) *items_per_tile = p.items;
+    if (n_tiles) *n_tiles = p.n_tiles;
+    if (tile_row) *tile_row = p.tile_row.as<uint32_t>();
+    if (tile_nnz) *tile_nnz = p.tile_nnz.as<uint32_t>();
+    if (carry) *carry = p.carry.p;
+    if (tail) *tail = p.tail.p;
+    return G1_OK;
+}
+
+g1_status g1_spmv(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched, const void* x,
+                  void* y, void* stream) {
+    if (!g || transpose < 0 || transpose > 1 || !x || !y)
+        return fail(G1_ERR_INVALID, "g1_spmv: bad argument");
+    DeviceGuard dg(g->device);
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (!g->o[transpose].present) return fail(G1_ERR_UNSUPPORTED, "g1_spmv: orientation not built");
+    const bool fval = sr == G1_SR_MINPLUS_F32 || sr == G1_SR_PLUSTIMES_F32;
+    if (sr != G1_SR_BFS_U32 && fval != (g->vtype == G1_F32))
+        return fail(G1_ERR_INVALID, "g1_spmv: semiring value type does not match the graph");
+    cudaStream_t s = as_stream(stream);
+    switch (sr) {
+        case G1_SR_MINPLUS_U32:
+            return run_spmv<MinPlusU32>(g, transpose, sched, static_cast<const uint32_t*>(x),
+                                        StoreEpilogue<uint32_t>{static_cast<uint32_t*>(y)}, s);
+        case G1_SR_MINPLUS_F32:
+            return run_spmv<MinPlusF32>(g, transpose, sched, static_cast<const float*>(x),
+                                        StoreEpilogue<float>{static_cast<float*>(y)}, s);
+        case G1_SR_PLUSTIMES_F32:
+            return run_spmv<PlusTimesF32>(g, transpose, sched, static_cast<const float*>(x),
+                                          StoreEpilogue<float>{static_cast<float*>(y)}, s);
+        case G1_SR_BFS_U32:
+            return run_spmv<BfsU32>(g, transpose, sched, static_cast<const uint32_t*>(x),
+                                    StoreEpilogue<uint32_t>{static_cast<uint32_t*>(y)}, s);
+    }
+    return fail(G1_ERR_INVALID, "g1_spmv: unknown semiring");
+}
+
+g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, void* stream) {
+    if (!g) return fail(G1_ERR_INVALID, "g1_autotune: null graph");
+    DeviceGuard dg(g->device);
+    std::lock_guard<std::mutex> lk(g->mu);
+    cudaStream_t s = as_stream(stream);
+    const int t = pull_side(g);
+    if (!g->o[t].present) return fail(G1_ERR_UNSUPPORTED, "g1_autotune: no CSR");
+    uint32_t *x = nullptr, *y = nullptr;
+    G1_TRY(g->ws.get("tune_x", g->n, &x));
+    G1_TRY(g->ws.get("tune_y", g->n, &y));
+    G1_CUDA(cudaMemsetAsync(x, 0, (size_t)g->n * 4, s));
+    float ms[2] = {0, 0};
+    cudaEvent_t e0, e1;
+    G1_CUDA(cudaEventCreate(&e0));
+    G1_CUDA(cudaEventCreate(&e1));
+    const g1_schedule cand[2] = {G1_SCHED_MERGE, G1_SCHED_VECTOR};
+    for (int c = 0; c < 2; ++c) {
+        for (int rep = 0; rep < 2; ++rep)  // warm-up
+            G1_TRY((run_spmv<BfsU32>(g, t, cand[c], x, StoreEpilogue<uint32_t>{y}, s)));
+        cudaEventRecord(e0, s);
+        for (int rep = 0; rep < 5; ++rep)
+            G1_TRY((run_spmv<BfsU32>(g, t, cand[c], x, StoreEpilogue<uint32_t>{y}, s)));
+        cudaEventRecord(e1, s);
+        G1_CUDA(cudaEventSynchronize(e1));
+        cudaEventElapsedTime(&ms[c], e0, e1);
+        ms[c] /= 5;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g->o[t].tuned_sched = ms[0] <= ms[1] ? G1_SCHED_MERGE : G1_SCHED_VECTOR;
+    if (g->o[t ^ 1].present && g->o[t ^ 1].rp == g->o[t].rp) g->o[t ^ 1].tuned_sched = g->o[t].tuned_sched;
+    if (merge_ms) *merge_ms = ms[0];
+    if (vector_ms) *vector_ms = ms[1];
+    return G1_OK;
+}
+
+}  // extern "C"

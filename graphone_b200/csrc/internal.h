@@ -1,0 +1,147 @@
+// Internal state of libgraphone_b200.so (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "graphone_b200.h"
+
+namespace g1 {
+
+// Records the failure message for g1_last_error() and returns the status.
+g1_status fail(g1_status s, const std::string& msg);
+g1_status fail_cuda(cudaError_t e, const char* what);
+
+#define G1_CUDA(call)                                          \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return ::g1::fail_cuda(e_, #call); \
+    } while (0)
+
+#define G1_TRY(call)                     \
+    do {                                 \
+        g1_status s_ = (call);           \
+        if (s_ != G1_OK) return s_;      \
+    } while (0)
+
+// Owning device buffer; capacity grows, never shrinks.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    g1_status ensure(size_t want);
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// Pinned host scratch for small read-backs (sizes, counters).
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    g1_status ensure(size_t want);
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+// Merge-path plan of one orientation.
+struct MergePlan {
+    uint32_t items = 0;
+    uint32_t n_tiles = 0;
+    DevBuf tile_row, tile_nnz, carry, tail;
+};
+
+struct Orientation {
+    bool present = false;
+    uint32_t* rp = nullptr;
+    uint32_t* col = nullptr;
+    void* val = nullptr;
+    DevBuf b_rp, b_col, b_val;  // storage unless shared with the other side
+    uint32_t max_deg = 0;
+    std::unique_ptr<MergePlan> plan;
+    int tuned_sched = 0;  // 0 = not tuned, else g1_schedule
+};
+
+// Named, growable workspaces of one graph.
+struct Workspace {
+    std::map<std::string, std::unique_ptr<DevBuf>> bufs;
+    PinnedBuf pinned;
+    template <class T>
+    g1_status get(const std::string& name, size_t count, T** out) {
+        auto& b = bufs[name];
+        if (!b) b.reset(new DevBuf());
+        G1_TRY(b->ensure(count * sizeof(T) + 64));
+        *out = b->as<T>();
+        return G1_OK;
+    }
+    size_t bytes() const {
+        size_t s = 0;
+        for (auto& kv : bufs) s += kv.second ? kv.second->bytes : 0;
+        return s;
+    }
+};
+
+}  // namespace g1
+
+struct g1_graph {
+    int device = 0;
+    uint32_t n = 0;
+    uint32_t m = 0;
+    g1_dtype vtype = G1_U32;
+    bool symmetric = false;
+    g1::Orientation o[2];  // 0 = out-edges (normal), 1 = in-edges (transpose)
+    g1::Workspace ws;
+    std::mutex mu;
+    int sm_count = 148;
+};
+
+namespace g1 {
+
+// Makes `dev` current for the scope.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+bool is_device_ptr(const void* p);
+// Copies n bytes to a device or host destination from device memory.
+g1_status copy_out(void* dst, const void* dev_src, size_t bytes, cudaStream_t s);
+
+g1_status ensure_plan(g1_graph* g, int t);
+
+// Kernel launch accounting (g1_kernel_launches) and the SpMV kernel timer
+// (g1_profile_begin/end).
+void count_launches(uint64_t n);
+bool profiling();
+void prof_mark(cudaStream_t s, bool start);
+inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+// Orientation the pull (gather) engines read: in-edges.
+inline int pull_side(const g1_graph* g) { return g->o[1].present ? 1 : 0; }
+// Orientation the push (advance) engines read: out-edges.
+inline int push_side(const g1_graph* g) { return g->o[0].present ? 0 : 1; }
+
+}  // namespace g1

@@ -1,0 +1,248 @@
+// PageRank on the plus-times SpMV with the apply/construct step fused into
+// the SpMV epilogue.
+//
+// GraphOne's all-active engine runs, per iteration, the merge SpMV over the
+// in-edge CSR, then apply_construct_kernel over all N vertices
+// (engine/blas_gc.h:377-428): rank'[v] = (1-a)/N + y[v] (apply_each,
+// apps/pagerank_blas.cu:115-121) and x'[v] = rank'[v] * iweights[v]
+// (construct_each, :95-101).  Here each completed row of the SpMV applies and
+// constructs in registers, so y never reaches HBM and there is no N-sized
+// second pass.  x and rank are double-buffered across iterations.
+//
+// G1_PR_DANGLING adds a*sum(rank[dangling])/N; that sum is reduced on the
+// device by the epilogues themselves (per-block partials, folded in a fixed
+// order by the last block of the fixup kernel), so no host round trip.
+#include <algorithm>
+
+#include "g1/semiring.cuh"
+#include "g1/spmv.cuh"
+#include "internal.h"
+#include "spmv_launch.cuh"
+
+namespace g1 {
+
+// Per-block partial sums folded by the last block to finish (ticket counter,
+// no waiting).  Deterministic: the slots are summed in a fixed order.
+template <int BLOCK>
+__device__ void fold_partials_last_block(double v, double* partials, uint32_t slot,
+                                         uint32_t n_slots, unsigned* ticket, double* out,
+                                         char* smem) {
+    double* red = reinterpret_cast<double*>(smem);
+    double s = block_sum<double, BLOCK>(v, red);
+    __shared__ int is_last;
+    if (threadIdx.x == 0) {
+        partials[slot] = s;
+        __threadfence();
+        const unsigned t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    double acc = 0.0;
+    for (uint32_t i = threadIdx.x; i < n_slots; i += BLOCK) acc += ((volatile double*)partials)[i];
+    acc = block_sum<double, BLOCK>(acc, red);
+    if (threadIdx.x == 0) {
+        *out = acc;
+        *ticket = 0u;  // ready for the next launch
+    }
+}
+
+struct PrEpilogue {
+    float* rank_next;
+    float* x_next;
+    const float* iw;
+    const double* dang_in;  // sum of the current ranks over dangling vertices
+    double alpha_over_n;
+    float base0;           // (float)((1 - alpha) / N), the reference's alpha_div_v
+    int dangling;          // G1_PR_DANGLING
+    double* partials;
+    uint32_t slot_base;
+    uint32_t n_slots;
+    int last_reduce;       // this launch folds all partials into dang_out
+    unsigned* ticket;
+    double* dang_out;
+
+    float base;
+    double dang_local;
+
+    __device__ __forceinline__ void begin() {
+        dang_local = 0.0;
+        base = dangling ? (float)((double)base0 + alpha_over_n * (*dang_in)) : base0;
+    }
+    __device__ __forceinline__ void emit(uint32_t v, const float& y) {
+        const float r = base + y;
+        rank_next[v] = r;
+        const float w = __ldg(iw + v);
+        x_next[v] = r * w;
+        if (dangling && w == 0.0f) dang_local += (double)r;
+    }
+    template <int BLOCK>
+    __device__ __forceinline__ void block_end(char* smem) {
+        if (!dangling) return;
+        if (last_reduce) {
+            fold_partials_last_block<BLOCK>(dang_local, partials, slot_base + blockIdx.x, n_slots,
+                                            ticket, dang_out, smem);
+        } else {
+            double s = block_sum<double, BLOCK>(dang_local, reinterpret_cast<double*>(smem));
+            if (threadIdx.x == 0) partials[slot_base + blockIdx.x] = s;
+        }
+    }
+};
+
+// iweights (apps/pagerank_blas.cu:41-53: alpha / sum of out-edge weights,
+// summed in CSR order in fp32; 0 for a vertex without out-weight), the
+// initial ranks 1/N, x0 = rank0 * iw and the dangling sum of rank0.
+template <int BLOCK>
+__global__ void pr_init_kernel(const uint32_t* rp, const float* val, uint32_t n, float alpha,
+                               float* iw, float* rank0, float* x0, double* partials,
+                               unsigned* ticket, double* dang_out) {
+    __shared__ alignas(16) char smem[64 * 8];
+    const float r0 = (float)(1.0 / (double)n);
+    double dl = 0.0;
+    const uint64_t stride = (uint64_t)gridDim.x * BLOCK;
+    for (uint64_t v = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
+        float s = 0.0f;
+        for (uint32_t k = rp[v]; k < rp[v + 1]; ++k) s += val[k];
+        const float w = s != 0.0f ? alpha / s : 0.0f;
+        iw[v] = w;
+        rank0[v] = r0;
+        x0[v] = r0 * w;
+        if (w == 0.0f) dl += (double)r0;
+    }
+    fold_partials_last_block<BLOCK>(dl, partials, blockIdx.x, gridDim.x, ticket, dang_out, smem);
+}
+
+// Out-weight sums from the in-edge CSR only (no out-edge CSR built).
+__global__ void pr_outw_from_transpose_kernel(const uint32_t* trp, const uint32_t* tcol,
+                                              const float* tval, uint32_t n, float* outw) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        for (uint32_t k = trp[v]; k < trp[v + 1]; ++k) atomicAdd(&outw[tcol[k]], tval[k]);
+}
+
+__global__ void pr_init_from_outw_kernel(const float* outw, uint32_t n, float alpha, float* iw,
+                                         float* rank0, float* x0, double* partials,
+                                         unsigned* ticket, double* dang_out) {
+    __shared__ alignas(16) char smem[64 * 8];
+    const float r0 = (float)(1.0 / (double)n);
+    double dl = 0.0;
+    const uint64_t stride = (uint64_t)gridDim.x * 256;
+    for (uint64_t v = (uint64_t)blockIdx.x * 256 + threadIdx.x; v < n; v += stride) {
+        const float s = outw[v];
+        const float w = s != 0.0f ? alpha / s : 0.0f;
+        iw[v] = w;
+        rank0[v] = r0;
+        x0[v] = r0 * w;
+        if (w == 0.0f) dl += (double)r0;
+    }
+    fold_partials_last_block<256>(dl, partials, blockIdx.x, gridDim.x, ticket, dang_out, smem);
+}
+
+struct PrBuffers {
+    float* iw;
+    float* rank[2];
+    float* x[2];
+    double* dang;  // [2]
+    double* partials;
+    unsigned* ticket;
+    uint32_t n_slots;
+};
+
+static g1_status pr_setup(g1_graph* g, float alpha, PrBuffers& b, uint32_t* grids,
+                          cudaStream_t s) {
+    const uint32_t n = g->n;
+    const int t = 1;
+    Workspace& ws = g->ws;
+    G1_TRY(ws.get("pr_iw", n, &b.iw));
+    G1_TRY(ws.get("pr_rank0", n, &b.rank[0]));
+    G1_TRY(ws.get("pr_rank1", n, &b.rank[1]));
+    G1_TRY(ws.get("pr_x0", n, &b.x[0]));
+    G1_TRY(ws.get("pr_x1", n, &b.x[1]));
+    G1_TRY(ws.get("pr_dang", 2, &b.dang));
+    G1_TRY(ws.get("pr_ticket", 4, &b.ticket));
+    G1_TRY(ensure_plan(g, t));
+    // grids[0] main merge, grids[1] fixup, grids[2] vector, grids[3] init
+    grids[0] = merge_main_grid<PlusTimesF32, PrEpilogue>(g, t);
+    grids[1] = merge_fixup_grid<PlusTimesF32, PrEpilogue>(g, t);
+    grids[2] = vector_grid<PlusTimesF32, PrEpilogue>(g);
+    grids[3] = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
+    b.n_slots = std::max(grids[0] + grids[1], std::max(grids[2], grids[3]));
+    G1_TRY(ws.get("pr_partials", b.n_slots, &b.partials));
+    G1_CUDA(cudaMemsetAsync(b.ticket, 0, 16, s));
+    count_launches(g->o[0].present ? 1 : 2);
+    if (g->o[0].present) {
+        pr_init_kernel<256><<<grids[3], 256, 0, s>>>(g->o[0].rp,
+                                                      static_cast<const float*>(g->o[0].val), n,
+                                                      alpha, b.iw, b.rank[0], b.x[0], b.partials,
+                                                      b.ticket, &b.dang[0]);
+    } else {
+        float* outw = nullptr;
+        G1_TRY(ws.get("pr_outw", n, &outw));
+        G1_CUDA(cudaMemsetAsync(outw, 0, (size_t)n * 4, s));
+        pr_outw_from_transpose_kernel<<<grids[3], 256, 0, s>>>(
+            g->o[1].rp, g->o[1].col, static_cast<const float*>(g->o[1].val), n, outw);
+        pr_init_from_outw_kernel<<<grids[3], 256, 0, s>>>(outw, n, alpha, b.iw, b.rank[0],
+                                                          b.x[0], b.partials, b.ticket,
+                                                          &b.dang[0]);
+    }
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
+}
+
+// One PageRank iteration: reads x[cur], writes rank[nxt], x[nxt], dang[nxt].
+static g1_status pr_iterate(g1_graph* g, const PrBuffers& b, const uint32_t* grids, float alpha,
+                            g1_pr_mode mode, int cur, g1_schedule sched, cudaStream_t s) {
+    const int nxt = cur ^ 1;
+    PrEpilogue e;
+    e.rank_next = b.rank[nxt];
+    e.x_next = b.x[nxt];
+    e.iw = b.iw;
+    e.dang_in = &b.dang[cur];
+    e.alpha_over_n = (double)alpha / (double)g->n;
+    e.base0 = (float)((1.0 - (double)alpha) / (double)g->n);
+    e.dangling = mode == G1_PR_DANGLING;
+    e.partials = b.partials;
+    e.ticket = b.ticket;
+    e.dang_out = &b.dang[nxt];
+    const int t = 1;
+    if (resolve_schedule(g, t, sched) == G1_SCHED_VECTOR) {
+        e.slot_base = 0;
+        e.n_slots = grids[2];
+        e.last_reduce = 1;
+        return launch_vector<PlusTimesF32>(g, t, b.x[cur], e, s);
+    }
+    PrEpilogue f = e;
+    e.slot_base = 0;
+    e.n_slots = grids[0] + grids[1];
+    e.last_reduce = 0;
+    f.slot_base = grids[0];
+    f.n_slots = grids[0] + grids[1];
+    f.last_reduce = 1;
+    return launch_merge<PlusTimesF32>(g, t, b.x[cur], e, f, s);
+}
+
+}  // namespace g1
+
+using namespace g1;
+
+extern "C" g1_status g1_pagerank(g1_graph* g, float alpha, int iters, g1_pr_mode mode,
+                                 float* rank_out, void* stream) {
+    if (!g || !rank_out || iters < 0) return fail(G1_ERR_INVALID, "g1_pagerank: bad argument");
+    if (g->vtype != G1_F32) return fail(G1_ERR_INVALID, "g1_pagerank: needs fp32 edge values");
+    if (mode != G1_PR_REFERENCE && mode != G1_PR_DANGLING)
+        return fail(G1_ERR_INVALID, "g1_pagerank: unknown mode");
+    if (!g->o[1].present)
+        return fail(G1_ERR_UNSUPPORTED, "g1_pagerank: needs the in-edge CSR (G1_GRAPH_BUILD_OTHER)");
+    if (g->n == 0) return G1_OK;
+    DeviceGuard dg(g->device);
+    std::lock_guard<std::mutex> lk(g->mu);
+    cudaStream_t s = as_stream(stream);
+    PrBuffers b;
+    uint32_t grids[4];
+    G1_TRY(pr_setup(g, alpha, b, grids, s));
+    for (int it = 0; it < iters; ++it)
+        G1_TRY(pr_iterate(g, b, grids, alpha, mode, it & 1, G1_SCHED_AUTO, s));
+    return copy_out(rank_out, b.rank[iters & 1], (size_t)g->n * 4, s);
+}

@@ -1,0 +1,235 @@
+// Single-source SSSP and BFS on the two GraphOne engines.
+//
+// * BLAS engine (pull): GraphOne's BlasGcEngine<SPARSE_BASED>
+//   (engine/blas_gc.h:171-247) per iteration fills x with default_info over
+//   N, scatters construct_each of the frontier, runs the merge SpMV over all
+//   rows, transforms y over N into flags and copy_ifs the next frontier, with
+//   two host synchronisations.  Here x stays default_info between
+//   iterations and only the frontier's entries are set and reset (O(|F|)),
+//   apply + frontier compaction run in the SpMV epilogue (warp-aggregated
+//   appends), and one 8-byte read-back per iteration tells the host the next
+//   frontier size.  Per-iteration results are those of the reference.
+// * Advance engine (push): GraphOne's AdvanceGC (engine/advance_gc.h:162-283)
+//   sizes an invalid-padded output by a degree-sum reduction, launches the
+//   advance kernel, synchronises, then filters duplicates in a second pass.
+//   Here the advance relaxes with atomicMin, deduplicates at emission time
+//   with the visited stamp of the sssp_adv filter (apps/sssp_adv.cu:62-71,
+//   made atomic) and appends compactly: one kernel per iteration.
+// * AUTO: push while the frontier's out-degree sum is below m/16, pull
+//   otherwise (direction-optimising).  Final distances are the unique
+//   shortest-path distances whichever engine runs, so all three agree
+//   bit-exactly with the oracle.
+#include <algorithm>
+
+#include "g1/semiring.cuh"
+#include "g1/spmv.cuh"
+#include "internal.h"
+#include "spmv_launch.cuh"
+
+namespace g1 {
+
+// apply_each of the sssp_blas functor under the engine's guard
+// (blas_gc.h:230-237): res != default_result && res < dist[v] -> update,
+// activate.  The degree sum of activated vertices feeds the push/pull choice.
+struct SparseApplyEpilogue {
+    uint32_t* dist;
+    uint32_t* out;
+    uint32_t* out_count;
+    unsigned long long* deg_sum;
+    const uint32_t* out_rp;  // out-edge offsets (for the degree sum)
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ void emit(uint32_t v, const uint32_t& res) {
+        if (res != kU32Max && res < dist[v]) {
+            dist[v] = res;
+            append_sum(out, out_count, deg_sum, v, out_rp[v + 1] - out_rp[v]);
+        }
+    }
+    template <int BLOCK>
+    __device__ __forceinline__ void block_end(char*) {}
+};
+
+__global__ void tr_init_kernel(uint32_t n, uint32_t src, uint32_t* dist, uint32_t* x,
+                               uint32_t* visited, uint32_t* frontier) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        dist[v] = v == src ? 0u : kU32Max;
+        x[v] = kU32Max;
+        visited[v] = 0u;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) frontier[0] = src;
+}
+
+// x[f] = dist[f] (construct_each of sssp_blas) or MAX (reset) over F.
+__global__ void tr_scatter_kernel(const uint32_t* F, uint32_t nF, const uint32_t* dist,
+                                  uint32_t* x, int reset) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nF; i += stride) {
+        const uint32_t f = F[i];
+        x[f] = reset ? kU32Max : dist[f];
+    }
+}
+
+// Push relaxation of one edge; emits v once per iteration.
+template <bool UNIT>
+__device__ __forceinline__ void relax(uint32_t du, uint32_t v, uint32_t w, uint32_t* dist,
+                                      uint32_t* visited, uint32_t iter, uint32_t* out,
+                                      uint32_t* out_count, const uint32_t* rp,
+                                      unsigned long long* deg_sum) {
+    const uint32_t cand = UNIT ? du + 1u : du + w;
+    if (cand < dist[v]) {  // cheap pre-check; atomicMin decides
+        const uint32_t old = atomicMin(&dist[v], cand);
+        if (cand < old && atomicExch(&visited[v], iter) != iter)
+            append_sum(out, out_count, deg_sum, v, rp[v + 1] - rp[v]);
+    }
+}
+
+// Advance over the frontier: a thread per vertex for short adjacency lists,
+// the whole warp for lists of 32 or more edges (coalesced col/val reads).
+template <bool UNIT>
+__global__ void __launch_bounds__(256)
+tr_advance_kernel(const uint32_t* F, uint32_t nF, const uint32_t* rp, const uint32_t* col,
+                  const uint32_t* val, uint32_t* dist, uint32_t* visited, uint32_t iter,
+                  uint32_t* out, uint32_t* out_count, unsigned long long* deg_sum) {
+    const uint32_t lane = lane_id();
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t rounds = (uint32_t)ceil_div(nF, (uint64_t)warps * 32);
+    for (uint32_t r = 0; r < rounds; ++r) {
+        const uint32_t i = (r * warps + wid) * 32 + lane;
+        uint32_t u = 0, b = 0, e = 0;
+        if (i < nF) {
+            u = F[i];
+            b = rp[u];
+            e = rp[u + 1];
+        }
+        const uint32_t du = i < nF ? dist[u] : 0u;
+        // long lists: cooperative, one list at a time
+        unsigned big = __ballot_sync(0xffffffffu, e - b >= 32);
+        while (big) {
+            const int src_lane = __ffs(big) - 1;
+            big &= big - 1;
+            const uint32_t bb = __shfl_sync(0xffffffffu, b, src_lane);
+            const uint32_t ee = __shfl_sync(0xffffffffu, e, src_lane);
+            const uint32_t dd = __shfl_sync(0xffffffffu, du, src_lane);
+            for (uint32_t k = bb + lane; k < ee; k += 32)
+                relax<UNIT>(dd, col[k], UNIT ? 1u : val[k], dist, visited, iter, out, out_count,
+                            rp, deg_sum);
+        }
+        if (e - b < 32) {
+            for (uint32_t k = b; k < e; ++k)
+                relax<UNIT>(du, col[k], UNIT ? 1u : val[k], dist, visited, iter, out, out_count, rp,
+                            deg_sum);
+        }
+    }
+}
+
+struct TrState {
+    uint32_t* dist;
+    uint32_t* x;
+    uint32_t* visited;
+    uint32_t* F[2];
+    uint32_t* cnt;  // [0] next frontier size, [2..3] degree sum (u64)
+    uint32_t* host;  // pinned
+};
+
+template <bool UNIT>
+static g1_status traverse(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* out,
+                          uint32_t* iters_out, cudaStream_t s) {
+    const uint32_t n = g->n;
+    if (src >= n) return fail(G1_ERR_INVALID, "source vertex out of range");
+    if ((engine == G1_ENGINE_BLAS || engine == G1_ENGINE_AUTO) && !g->o[1].present)
+        return fail(G1_ERR_UNSUPPORTED, "pull engine needs the in-edge CSR (G1_GRAPH_BUILD_OTHER)");
+    if ((engine == G1_ENGINE_ADVANCE || engine == G1_ENGINE_AUTO) && !g->o[0].present)
+        return fail(G1_ERR_UNSUPPORTED, "push engine needs the out-edge CSR (G1_GRAPH_BUILD_OTHER)");
+    if (!UNIT && g->vtype != G1_U32) return fail(G1_ERR_INVALID, "SSSP needs u32 edge weights");
+    Workspace& ws = g->ws;
+    TrState st;
+    G1_TRY(ws.get("tr_dist", n, &st.dist));
+    G1_TRY(ws.get("tr_x", n, &st.x));
+    G1_TRY(ws.get("tr_visited", n, &st.visited));
+    G1_TRY(ws.get("tr_f0", n, &st.F[0]));
+    G1_TRY(ws.get("tr_f1", n, &st.F[1]));
+    G1_TRY(ws.get("tr_cnt", 8, &st.cnt));
+    G1_TRY(ws.pinned.ensure(64));
+    st.host = ws.pinned.as<uint32_t>();
+    unsigned long long* deg_sum = reinterpret_cast<unsigned long long*>(st.cnt + 2);
+    const uint32_t g_n = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
+    tr_init_kernel<<<g_n, 256, 0, s>>>(n, src, st.dist, st.x, st.visited, st.F[0]);
+    count_launches(1);
+    G1_CUDA(cudaGetLastError());
+
+    const int pull_t = 1, push_t = 0;
+    const uint32_t* push_rp = g->o[push_t].present ? g->o[push_t].rp : g->o[pull_t].rp;
+    uint32_t nF = 1;
+    uint64_t degF = 0;
+    {
+        // out-degree of the source, for the first push/pull decision
+        uint32_t h[2];
+        G1_CUDA(cudaMemcpyAsync(h, push_rp + src, 8, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaStreamSynchronize(s));
+        degF = h[1] - h[0];
+    }
+    uint32_t it = 0;
+    int cur = 0;
+    const uint64_t push_limit = std::max<uint64_t>(1, g->m / 16);
+    while (nF > 0) {
+        ++it;
+        // Bellman-Ford settles within n rounds; more means corrupted state.
+        if (it > n + 1) return fail(G1_ERR_TIMEOUT, "traversal did not converge within n rounds");
+        G1_CUDA(cudaMemsetAsync(st.cnt, 0, 16, s));
+        const bool push = engine == G1_ENGINE_ADVANCE || (engine == G1_ENGINE_AUTO && degF < push_limit);
+        const uint32_t gf = (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(ceil_div(nF, 256), (uint64_t)g->sm_count * 8));
+        if (push) {
+            count_launches(1);
+            const Orientation& o = g->o[push_t];
+            tr_advance_kernel<UNIT><<<gf, 256, 0, s>>>(st.F[cur], nF, o.rp, o.col,
+                                                       static_cast<const uint32_t*>(o.val), st.dist,
+                                                       st.visited, it, st.F[cur ^ 1], st.cnt,
+                                                       deg_sum);
+        } else {
+            tr_scatter_kernel<<<gf, 256, 0, s>>>(st.F[cur], nF, st.dist, st.x, 0);
+            count_launches(2);
+            SparseApplyEpilogue e{st.dist, st.F[cur ^ 1], st.cnt, deg_sum, push_rp};
+            if (UNIT)
+                G1_TRY((run_spmv<BfsU32>(g, pull_t, G1_SCHED_AUTO, st.x, e, s)));
+            else
+                G1_TRY((run_spmv<MinPlusU32>(g, pull_t, G1_SCHED_AUTO, st.x, e, s)));
+            tr_scatter_kernel<<<gf, 256, 0, s>>>(st.F[cur], nF, st.dist, st.x, 1);
+        }
+        G1_CUDA(cudaGetLastError());
+        G1_CUDA(cudaMemcpyAsync(st.host, st.cnt, 16, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaStreamSynchronize(s));
+        nF = st.host[0];
+        degF = (uint64_t)st.host[2] | ((uint64_t)st.host[3] << 32);
+        cur ^= 1;
+        if (nF > n) return fail(G1_ERR_OVERFLOW, "frontier larger than the vertex count");
+    }
+    if (iters_out) *iters_out = it;
+    return copy_out(out, st.dist, (size_t)n * 4, s);
+}
+
+}  // namespace g1
+
+using namespace g1;
+
+extern "C" g1_status g1_sssp(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* dist_out,
+                             uint32_t* iters_out, void* stream) {
+    if (!g || !dist_out) return fail(G1_ERR_INVALID, "g1_sssp: bad argument");
+    if (engine != G1_ENGINE_BLAS && engine != G1_ENGINE_ADVANCE && engine != G1_ENGINE_AUTO)
+        return fail(G1_ERR_INVALID, "g1_sssp: unknown engine");
+    DeviceGuard dg(g->device);
+    std::lock_guard<std::mutex> lk(g->mu);
+    return traverse<false>(g, src, engine, dist_out, iters_out, as_stream(stream));
+}
+
+extern "C" g1_status g1_bfs(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* level_out,
+                            uint32_t* iters_out, void* stream) {
+    if (!g || !level_out) return fail(G1_ERR_INVALID, "g1_bfs: bad argument");
+    if (engine != G1_ENGINE_BLAS && engine != G1_ENGINE_ADVANCE && engine != G1_ENGINE_AUTO)
+        return fail(G1_ERR_INVALID, "g1_bfs: unknown engine");
+    DeviceGuard dg(g->device);
+    std::lock_guard<std::mutex> lk(g->mu);
+    return traverse<true>(g, src, engine, level_out, iters_out, as_stream(stream));
+}

@@ -1,0 +1,134 @@
+#pragma once
+// Device helpers shared by the prebuilt library (graphone_b200/csrc) and the
+// functor-templated engines of the GraphOne-compatible headers.
+//
+// Everything here is sm_100a SIMT code: warp shuffles, warp-aggregated
+// atomics and bounded spin-waits.  No tensor-core path exists for the graph
+// semirings (min-plus and sparse plus-times are not dense contractions).
+
+#include <cstdint>
+#include <cstring>
+#include <cuda_runtime.h>
+
+namespace g1 {
+
+constexpr uint32_t kU32Max = 0xFFFFFFFFu;
+constexpr int kWarp = 32;
+
+// ---------------------------------------------------------------- shuffles
+// Generic warp shuffles for any trivially copyable value of up to 16 bytes
+// (the gather type of a user functor is an arbitrary scalar or small struct).
+template <typename T>
+__device__ __forceinline__ T shfl_up_any(unsigned mask, T v, int delta) {
+    constexpr int W = (sizeof(T) + 3) / 4;
+    static_assert(W <= 4, "gather values larger than 16 bytes are not supported");
+    uint32_t w[W] = {};
+    memcpy(w, &v, sizeof(T));
+#pragma unroll
+    for (int i = 0; i < W; ++i) w[i] = __shfl_up_sync(mask, w[i], delta);
+    T out;
+    memcpy(&out, w, sizeof(T));
+    return out;
+}
+
+template <typename T>
+__device__ __forceinline__ T shfl_any(unsigned mask, T v, int src) {
+    constexpr int W = (sizeof(T) + 3) / 4;
+    static_assert(W <= 4, "gather values larger than 16 bytes are not supported");
+    uint32_t w[W] = {};
+    memcpy(w, &v, sizeof(T));
+#pragma unroll
+    for (int i = 0; i < W; ++i) w[i] = __shfl_sync(mask, w[i], src);
+    T out;
+    memcpy(&out, w, sizeof(T));
+    return out;
+}
+
+template <typename T>
+__device__ __forceinline__ T shfl_down_any(unsigned mask, T v, int delta) {
+    constexpr int W = (sizeof(T) + 3) / 4;
+    uint32_t w[W] = {};
+    memcpy(w, &v, sizeof(T));
+#pragma unroll
+    for (int i = 0; i < W; ++i) w[i] = __shfl_down_sync(mask, w[i], delta);
+    T out;
+    memcpy(&out, w, sizeof(T));
+    return out;
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// ------------------------------------------------- warp-aggregated append
+// Appends v to out[] (counter *count): one atomic per group of converged
+// lanes, each lane writes its own slot.  Callers guarantee capacity.
+__device__ __forceinline__ void append(uint32_t* out, uint32_t* count, uint32_t v) {
+    const unsigned mask = __activemask();
+    const int leader = __ffs(mask) - 1;
+    const uint32_t lane = lane_id();
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(count, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    out[base + __popc(mask & ((1u << lane) - 1u))] = v;
+}
+
+// append() that also adds `d` (e.g. the vertex's out-degree) to *sum, with
+// one atomic per converged group for each counter.
+__device__ __forceinline__ void append_sum(uint32_t* out, uint32_t* count,
+                                           unsigned long long* sum, uint32_t v, uint32_t d) {
+    const unsigned mask = __activemask();
+    const int leader = __ffs(mask) - 1;
+    const uint32_t lane = lane_id();
+    const uint32_t tot = __reduce_add_sync(mask, d);
+    uint32_t base = 0;
+    if ((int)lane == leader) {
+        base = atomicAdd(count, (uint32_t)__popc(mask));
+        atomicAdd(sum, (unsigned long long)tot);
+    }
+    base = __shfl_sync(mask, base, leader);
+    out[base + __popc(mask & ((1u << lane) - 1u))] = v;
+}
+
+// ------------------------------------------------------- block reductions
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += shfl_down_any(0xffffffffu, v, d);
+    return v;
+}
+
+// Sum over the block; the result is valid in thread 0.  `scratch` holds one
+// T per warp.  Contains __syncthreads(): call from every thread.
+template <typename T, int BLOCK>
+__device__ __forceinline__ T block_sum(T v, T* scratch) {
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane_id() == 0) scratch[w] = v;
+    __syncthreads();
+    T r = T(0);
+    if (threadIdx.x < 32) {
+        r = (threadIdx.x < BLOCK / 32) ? scratch[threadIdx.x] : T(0);
+        r = warp_sum(r);
+    }
+    return r;
+}
+
+// ------------------------------------------------------- ceil division
+__host__ __device__ __forceinline__ uint64_t ceil_div(uint64_t a, uint64_t b) {
+    return (a + b - 1) / b;
+}
+
+// ---------------------------------------------- device-side error status
+// Kernels that can fail (bounded waits, capacity checks) record a code here
+// instead of trapping; the host reads it after the launch sequence.
+enum DeviceError : uint32_t {
+    kDevOk = 0,
+    kDevTimeout = 1,      // a bounded spin-wait ran out
+    kDevOverflow = 2,     // a frontier/queue would have exceeded its capacity
+};
+
+__device__ __forceinline__ void set_error(uint32_t* flag, uint32_t code) {
+    if (flag) atomicCAS(flag, 0u, code);
+}
+
+}  // namespace g1

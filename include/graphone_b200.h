@@ -1,0 +1,158 @@
+/*
+ * graphone_b200.h -- C ABI of the B200 graph engines (libgraphone_b200.so).
+ *
+ * Plain C types only: opaque handles, raw pointers and sizes, a cudaStream_t
+ * passed as void*.  Pointers to CSR arrays and result vectors may be host
+ * memory (pageable or pinned) or device memory of the graph's GPU; the
+ * library detects which with cudaPointerGetAttributes and copies as needed.
+ * Every call returns a g1_status; g1_last_error() gives the message of the
+ * last failure on the calling thread.  Nothing is printed, nothing exits.
+ *
+ * Each entry point names the GraphOne interface it replaces (paths inside
+ * the GraphOne source tree).  The functor-templated engines of the
+ * GraphOne-compatible headers (include/GraphOne/) call the g1_mem_* / plan /
+ * launch-configuration entry points below for all of their host work.
+ *
+ * Threading: calls on different graphs may run concurrently; calls on one
+ * graph are serialised by the graph's own lock (they share its workspace).
+ */
+#ifndef GRAPHONE_B200_H_
+#define GRAPHONE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    G1_OK = 0,
+    G1_ERR_INVALID = 1,     /* bad argument or malformed CSR */
+    G1_ERR_OOM = 2,         /* device allocation failed / admission refused */
+    G1_ERR_DEVICE = 3,      /* a CUDA call failed */
+    G1_ERR_TIMEOUT = 4,     /* a bounded device wait ran out */
+    G1_ERR_UNSUPPORTED = 5, /* combination not available */
+    G1_ERR_OVERFLOW = 6     /* a device queue would have overflowed */
+} g1_status;
+
+typedef enum { G1_U32 = 0, G1_F32 = 1 } g1_dtype;
+
+typedef enum {
+    G1_SR_MINPLUS_U32 = 0,   /* sssp_blas functor, u32 distances */
+    G1_SR_MINPLUS_F32 = 1,   /* sssp_blas functor as the app builds it (float) */
+    G1_SR_PLUSTIMES_F32 = 2, /* pagerank_blas functor */
+    G1_SR_BFS_U32 = 3        /* min-plus with unit weights */
+} g1_semiring;
+
+typedef enum {
+    G1_SCHED_AUTO = 0,   /* per-graph choice (autotuned when g1_autotune ran) */
+    G1_SCHED_MERGE = 1,  /* merge-path row/nonzero split */
+    G1_SCHED_VECTOR = 2  /* CSR-vector, lanes per row from the mean degree */
+} g1_schedule;
+
+typedef enum {
+    G1_ENGINE_BLAS = 0,    /* pull SpMV per iteration (BlasGcEngine, sparse frontier) */
+    G1_ENGINE_ADVANCE = 1, /* push advance/filter (AdvanceGC) */
+    G1_ENGINE_AUTO = 2     /* push while the frontier is small, pull when it is large */
+} g1_engine;
+
+typedef enum {
+    G1_PR_REFERENCE = 0, /* (1-a)/N + sum: dangling mass dropped, as pagerank_blas */
+    G1_PR_DANGLING = 1   /* dangling mass a*sum(rank[dangling])/N added to every vertex */
+} g1_pr_mode;
+
+/* Graph creation flags. */
+#define G1_GRAPH_SYMMETRIC 0x1u      /* CSR equals its transpose: one copy serves both */
+#define G1_GRAPH_INPUT_TRANSPOSE 0x2u /* the arrays given are the in-edge CSR */
+#define G1_GRAPH_BUILD_OTHER 0x4u    /* also build the other orientation on the GPU */
+#define G1_GRAPH_NO_VALIDATE 0x8u    /* skip the device check of the CSR */
+
+typedef struct g1_graph g1_graph;
+
+/* ------------------------------------------------------------- basics */
+const char* g1_status_string(g1_status s);
+const char* g1_last_error(void);
+/* Library version string and the compiled architecture ("sm_100a"). */
+const char* g1_version(void);
+
+/* Device memory for the header engines' Buffer / DenseVec
+ * (replaces archi::memalloc/memfree/memset/memcpy, archi/mem/cuda.cuh:11-59).
+ * Allocations are padded to 256 bytes; g1_mem_alloc zero-fills. */
+g1_status g1_mem_alloc(void** ptr, size_t bytes);
+g1_status g1_mem_free(void* ptr);
+/* kind: 0 = host->device, 1 = device->host, 2 = device->device. */
+g1_status g1_mem_copy(void* dst, const void* src, size_t bytes, int kind, void* stream);
+g1_status g1_mem_fill_u32(void* dst, uint32_t value, size_t count, void* stream);
+g1_status g1_stream_sync(void* stream);
+
+/* Number of kernels this library has launched since it was loaded (all
+ * devices, all threads).  No GraphOne counterpart: measurement support. */
+uint64_t g1_kernel_launches(void);
+/* Kernel timing of the SpMV launches (main merge / vector kernels only):
+ * between g1_profile_begin and g1_profile_end every such launch is
+ * bracketed by CUDA events on its own stream; g1_profile_end synchronises
+ * and returns the summed milliseconds and the launch count.  No GraphOne
+ * counterpart: measurement support for the roofline figures. */
+g1_status g1_profile_begin(void);
+g1_status g1_profile_end(double* spmv_ms, uint64_t* spmv_launches);
+
+/* ------------------------------------------------------------- graphs */
+/* Makes a device-resident graph from one CSR (row_ptr n+1 entries, col and
+ * val m entries, val of `vtype`).  Replaces graph::build + EdgeCache::ToCsr
+ * (graph/builder.h:9-46, loader/edge_cache.h:50-105): the other orientation
+ * is built on the GPU when G1_GRAPH_BUILD_OTHER is set.  With
+ * G1_GRAPH_INPUT_TRANSPOSE the arrays are the in-edge CSR (what
+ * graph::build<BlasViews> keeps). */
+g1_status g1_graph_create(const uint32_t* row_ptr, const uint32_t* col, const void* val,
+                          g1_dtype vtype, uint32_t n, uint32_t m, uint32_t flags,
+                          void* stream, g1_graph** out);
+g1_status g1_graph_destroy(g1_graph* g);
+/* n, m, and whether the out-edge (normal) and in-edge (transpose) CSRs exist. */
+g1_status g1_graph_info(const g1_graph* g, uint32_t* n, uint32_t* m, int* has_normal,
+                        int* has_transpose);
+/* Device pointers of one orientation (0 = out-edges, 1 = in-edges), for the
+ * header engines' GraphArchRef (graph/graph_arch_ref.h:23-116). */
+g1_status g1_graph_arrays(const g1_graph* g, int transpose, const uint32_t** row_ptr,
+                          const uint32_t** col, const void** val);
+/* Bytes of device memory the graph holds (CSRs, plans, workspaces). */
+size_t g1_graph_device_bytes(const g1_graph* g);
+
+/* ------------------------------------------------------------- SpMV */
+/* Merge-path partition of one orientation, cached in the graph
+ * (replaces the SpmvDispatcher<SpmvCudaCsrMergeBased> constructor's
+ * SegmentSearch, archi/blas/spmv/cuda/cuda.cuh:152-169).  The arrays stay
+ * owned by the graph; tile_row/tile_nnz have n_tiles+1 entries. */
+g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t* items_per_tile,
+                       uint32_t* n_tiles, const uint32_t** tile_row,
+                       const uint32_t** tile_nnz, void** carry, void** tail);
+/* y = A (semiring) x over one orientation (replaces SpmvDispatcher::operator(),
+ * archi/blas/spmv/cuda/cuda.cuh:171-176; y stays on the device stream, no
+ * device synchronisation). x, y device pointers of n entries. */
+g1_status g1_spmv(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
+                  const void* x, void* y, void* stream);
+/* Times both schedules for each semiring class on this graph and keeps the
+ * faster for G1_SCHED_AUTO.  Results in ms (may be NULL). */
+g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, void* stream);
+
+/* ------------------------------------------------------------- algorithms */
+/* PageRank for a fixed iteration count (Run<PRFunctor> over
+ * AllActiveFrontier with BlasGcEngine<ALL_ACTIVE>, engine/blas_gc.h:353-434,
+ * apps/pagerank_blas.cu:36-123).  rank_out: n floats, host or device. */
+g1_status g1_pagerank(g1_graph* g, float alpha, int iters, g1_pr_mode mode, float* rank_out,
+                      void* stream);
+/* Single-source shortest paths, u32 weights, UINT32_MAX = unreachable
+ * (Run<SSSPFunctor> with BlasGcEngine<SPARSE_BASED>, engine/blas_gc.h:171-247,
+ * apps/sssp_blas.cu; or AdvanceGC, engine/advance_gc.h:162-283,
+ * apps/sssp_adv.cu).  dist_out: n u32, host or device.  iters_out may be NULL. */
+g1_status g1_sssp(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* dist_out,
+                  uint32_t* iters_out, void* stream);
+/* BFS hop levels from src, UINT32_MAX = unreachable. */
+g1_status g1_bfs(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* level_out,
+                 uint32_t* iters_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAPHONE_B200_H_ */

@@ -1,0 +1,42 @@
+"""The C ABI library loads and exports every entry point the header declares.
+CPU only: no kernel runs."""
+import ctypes as C
+import os
+import re
+
+import graphone_b200 as g1
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "graphone_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(g1_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = g1.lib()
+    decl = header_functions()
+    assert len(decl) >= 15
+    missing = [f for f in decl if not hasattr(L, f)]
+    assert not missing, missing
+    assert sorted(g1.EXPORTS) == decl
+
+
+def test_library_reports_sm100a():
+    assert b"sm_100a" in g1.lib().g1_version()
+
+
+def test_status_strings_and_argument_errors_without_gpu():
+    L = g1.lib()
+    assert L.g1_status_string(0) == b"ok"
+    assert L.g1_status_string(1) == b"invalid argument"
+    out = C.c_void_p()
+    st = L.g1_graph_create(None, None, None, 0, 4, 4, 0, None, C.byref(out))
+    assert st == 1 and out.value is None
+    assert b"null" in L.g1_last_error()
+    st = L.g1_graph_create(None, None, None, 0, 0, 0, 0, None, None)
+    assert st == 1
+    assert L.g1_sssp(None, 0, 0, None, None, None) == 1
+    assert L.g1_pagerank(None, C.c_float(0.85), 30, 1, None, None) == 1

@@ -1,0 +1,90 @@
+"""SSSP / BFS bit-exact and PageRank within 1e-6 relative L1 of the FP64
+oracle, on the GPU through the C ABI."""
+import numpy as np
+import pytest
+
+import graphone_b200 as g1
+from graphone_b200 import gen
+from oracle import oracle as O
+from tests.gpu_util import edge_case_graphs
+
+pytestmark = pytest.mark.gpu
+
+GRAPHS = edge_case_graphs()
+ENGINES = [g1.ENGINE_BLAS, g1.ENGINE_ADVANCE, g1.ENGINE_AUTO]
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+def test_sssp_bit_exact(cuda, name, engine):
+    g = GRAPHS[name]
+    G = g1.Graph.from_gen(g)
+    rp, ci, v = g.np("n")
+    srcs = sorted({0, g.n // 2, g.n - 1})
+    for s in srcs:
+        d = G.sssp(s, engine)
+        assert np.array_equal(d, O.dijkstra_u32(rp, ci, v, s)), (name, s, engine)
+
+
+@pytest.mark.parametrize("name", ["rmat10_sym", "grid32", "path3000"])
+def test_sssp_blas_iterations_match_reference_engine(cuda, name):
+    g = GRAPHS[name]
+    G = g1.Graph.from_gen(g)
+    trp, tci, tv = g.np("t")
+    d, it = G.sssp(0, g1.ENGINE_BLAS, return_iters=True)
+    d_o, it_o = O.sssp_blas_u32(trp, tci, tv, 0)
+    assert np.array_equal(d, d_o) and it == it_o
+
+
+@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+def test_bfs_bit_exact(cuda, name, engine):
+    g = GRAPHS[name]
+    G = g1.Graph.from_gen(g)
+    rp, ci, _ = g.np("n")
+    for s in sorted({0, g.n - 1}):
+        assert np.array_equal(G.bfs(s, engine), O.bfs(rp, ci, s)), (name, s, engine)
+
+
+def test_sssp_golden_fixtures(cuda):
+    for name in ("rmat8_sym", "rmat9_dir", "grid16"):
+        gold = dict(np.load(f"tests/golden/{name}.npz"))
+        G = g1.Graph.from_csr(gold["n_rp"], gold["n_col"], gold["n_val"])
+        for e in ENGINES:
+            assert np.array_equal(G.sssp(int(gold["sssp_src"]), e), gold["sssp_dist"])
+
+
+@pytest.mark.parametrize("mode", [g1.PR_REFERENCE, g1.PR_DANGLING])
+@pytest.mark.parametrize("scale", [8, 12, 16])
+def test_pagerank_within_1e6_of_fp64(cuda, scale, mode):
+    g = gen.rmat(scale, 16, False, float_values=True)
+    G = g1.Graph.from_gen(g)
+    trp, tci, tv = g.np("t")
+    r = G.pagerank(0.85, 30, mode)
+    r64 = O.pagerank_f64(trp, tci, tv, 0.85, 30, mode)
+    err = O.rel_l1(r, r64)
+    assert err < 1e-6, err  # tolerance: relative L1 vs the FP64 oracle
+
+
+def test_pagerank_golden(cuda):
+    gold = dict(np.load("tests/golden/rmat8_pr.npz"))
+    G = g1.Graph.from_csr(gold["n_rp"], gold["n_col"], gold["n_val"].astype(np.float32))
+    for mode in (0, 1):
+        r = G.pagerank(0.85, 30, mode)
+        assert O.rel_l1(r, gold[f"pr{mode}_rank"]) < 1e-6
+
+
+def test_pagerank_device_output_and_zero_iterations(cuda):
+    import torch
+    g = gen.rmat(10, 16, False, float_values=True)
+    G = g1.Graph.from_gen(g)
+    out = torch.empty(g.n, dtype=torch.float32, device="cuda")
+    G.pagerank(0.85, 0, g1.PR_DANGLING, out=out)
+    torch.cuda.synchronize()
+    assert torch.allclose(out, torch.full_like(out, 1.0 / g.n))
+
+
+def test_invalid_source(cuda):
+    G = g1.Graph.from_gen(GRAPHS["grid32"])
+    with pytest.raises(g1.G1Error):
+        G.sssp(10**6)
