@@ -262,26 +262,44 @@ g1_status build_transpose(g1_graph* g, const Orientation& src, Orientation& dst,
 
 }  // namespace
 
-g1_status ensure_plan(g1_graph* g, int t) {
+g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out) {
     Orientation& o = g->o[t];
     if (!o.present) return fail(G1_ERR_UNSUPPORTED, "orientation not built");
-    if (o.plan) return G1_OK;
+    // symmetric graphs share one CSR: share its plans too
+    Orientation& owner = (t == 1 && g->symmetric && g->o[0].present) ? g->o[0] : o;
+    auto it = owner.plans.find(items);
+    if (it != owner.plans.end()) {
+        *out = it->second.get();
+        return G1_OK;
+    }
     std::unique_ptr<MergePlan> p(new MergePlan());
-    p->items = kMergeBlock * kMergeIpt;
+    p->items = items;
     const uint64_t total = (uint64_t)g->n + g->m;
     p->n_tiles = (uint32_t)ceil_div(total, p->items);
     G1_TRY(p->tile_row.ensure(((size_t)p->n_tiles + 1) * 4));
     G1_TRY(p->tile_nnz.ensure(((size_t)p->n_tiles + 1) * 4));
-    G1_TRY(p->carry.ensure(((size_t)p->n_tiles + 1) * 8));
-    G1_TRY(p->tail.ensure(((size_t)p->n_tiles + 1) * 8));
+    G1_TRY(p->carry.ensure(((size_t)p->n_tiles + 1) * 16));
+    G1_TRY(p->tail.ensure(((size_t)p->n_tiles + 1) * 16));
     const uint32_t blocks = (uint32_t)ceil_div((uint64_t)p->n_tiles + 1, 256);
     merge_partition_kernel<<<blocks, 256>>>(o.rp, g->n, g->m, p->items, p->n_tiles,
                                             p->tile_row.as<uint32_t>(), p->tile_nnz.as<uint32_t>());
     count_launches(1);
     G1_CUDA(cudaGetLastError());
     G1_CUDA(cudaDeviceSynchronize());
-    o.plan = std::move(p);
+    *out = p.get();
+    owner.plans[items] = std::move(p);
     return G1_OK;
+}
+
+g1_status check_device_error(g1_graph* g, cudaStream_t s) {
+    uint32_t h = 0;
+    G1_CUDA(cudaMemcpyAsync(&h, g->err_word, 4, cudaMemcpyDeviceToHost, s));
+    G1_CUDA(cudaStreamSynchronize(s));
+    if (h == 0) return G1_OK;
+    G1_CUDA(cudaMemsetAsync(g->err_word, 0, 4, s));
+    if (h == kDevTimeout) return fail(G1_ERR_TIMEOUT, "a bounded device wait ran out");
+    if (h == kDevOverflow) return fail(G1_ERR_OVERFLOW, "a device queue overflowed");
+    return fail(G1_ERR_DEVICE, "device error word " + std::to_string(h));
 }
 
 }  // namespace g1
@@ -394,6 +412,9 @@ g1_status g1_graph_create(const uint32_t* row_ptr, const uint32_t* col, const vo
     std::unique_ptr<g1_graph> g(new g1_graph());
     G1_CUDA(cudaGetDevice(&g->device));
     cudaDeviceGetAttribute(&g->sm_count, cudaDevAttrMultiProcessorCount, g->device);
+    G1_TRY(g->err_buf.ensure(16));
+    g->err_word = g->err_buf.as<uint32_t>();
+    G1_CUDA(cudaMemsetAsync(g->err_word, 0, 16, s));
     g->n = n;
     g->m = m;
     g->vtype = vtype;
@@ -480,9 +501,9 @@ size_t g1_graph_device_bytes(const g1_graph* g) {
     for (int t = 0; t < 2; ++t) {
         const Orientation& o = g->o[t];
         s += o.b_rp.bytes + o.b_col.bytes + o.b_val.bytes;
-        if (o.plan)
-            s += o.plan->tile_row.bytes + o.plan->tile_nnz.bytes + o.plan->carry.bytes +
-                 o.plan->tail.bytes;
+        for (auto& kv : o.plans)
+            s += kv.second->tile_row.bytes + kv.second->tile_nnz.bytes + kv.second->carry.bytes +
+                 kv.second->tail.bytes;
     }
     return s;
 }
@@ -493,8 +514,9 @@ g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t* items_per_tile, uin
     if (!g || transpose < 0 || transpose > 1) return fail(G1_ERR_INVALID, "g1_spmv_plan");
     DeviceGuard dg(g->device);
     std::lock_guard<std::mutex> lk(g->mu);
-    G1_TRY(ensure_plan(g, transpose));
-    const MergePlan& p = *g->o[transpose].plan;
+    MergePlan* pp = nullptr;
+    G1_TRY(ensure_plan(g, transpose, (uint32_t)(kMergeBlock * merge_ipt(g, transpose)), &pp));
+    const MergePlan& p = *pp;
     if (items_per_tile) *items_per_tile = p.items;
     if (n_tiles) *n_tiles = p.n_tiles;
     if (tile_row) *tile_row = p.tile_row.as<uint32_t>();
@@ -543,29 +565,51 @@ g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, void* stre
     G1_TRY(g->ws.get("tune_x", g->n, &x));
     G1_TRY(g->ws.get("tune_y", g->n, &y));
     G1_CUDA(cudaMemsetAsync(x, 0, (size_t)g->n * 4, s));
-    float ms[2] = {0, 0};
     cudaEvent_t e0, e1;
     G1_CUDA(cudaEventCreate(&e0));
     G1_CUDA(cudaEventCreate(&e1));
-    const g1_schedule cand[2] = {G1_SCHED_MERGE, G1_SCHED_VECTOR};
-    for (int c = 0; c < 2; ++c) {
-        for (int rep = 0; rep < 2; ++rep)  // warm-up
-            G1_TRY((run_spmv<BfsU32>(g, t, cand[c], x, StoreEpilogue<uint32_t>{y}, s)));
+    // candidates: merge with 5/7/11 items per thread, and CSR-vector
+    const int ipts[3] = {5, 7, 11};
+    float best_merge = 1e30f, vec = 1e30f;
+    int best_ipt = kDefaultIpt;
+    Orientation& o = g->o[t];
+    const int saved_sched = o.tuned_sched, saved_ipt = o.tuned_ipt;
+    auto time_it = [&](g1_schedule sc, float* out) -> g1_status {
+        for (int rep = 0; rep < 2; ++rep)
+            G1_TRY((run_spmv<BfsU32>(g, t, sc, x, StoreEpilogue<uint32_t>{y}, s)));
         cudaEventRecord(e0, s);
         for (int rep = 0; rep < 5; ++rep)
-            G1_TRY((run_spmv<BfsU32>(g, t, cand[c], x, StoreEpilogue<uint32_t>{y}, s)));
+            G1_TRY((run_spmv<BfsU32>(g, t, sc, x, StoreEpilogue<uint32_t>{y}, s)));
         cudaEventRecord(e1, s);
         G1_CUDA(cudaEventSynchronize(e1));
-        cudaEventElapsedTime(&ms[c], e0, e1);
-        ms[c] /= 5;
+        cudaEventElapsedTime(out, e0, e1);
+        *out /= 5;
+        return G1_OK;
+    };
+    for (int c = 0; c < 3; ++c) {
+        o.tuned_ipt = ipts[c];
+        float ms = 0;
+        G1_TRY(time_it(G1_SCHED_MERGE, &ms));
+        if (ms < best_merge) {
+            best_merge = ms;
+            best_ipt = ipts[c];
+        }
     }
+    G1_TRY(time_it(G1_SCHED_VECTOR, &vec));
+    (void)saved_sched;
+    (void)saved_ipt;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    g->o[t].tuned_sched = ms[0] <= ms[1] ? G1_SCHED_MERGE : G1_SCHED_VECTOR;
-    if (g->o[t ^ 1].present && g->o[t ^ 1].rp == g->o[t].rp) g->o[t ^ 1].tuned_sched = g->o[t].tuned_sched;
-    if (merge_ms) *merge_ms = ms[0];
-    if (vector_ms) *vector_ms = ms[1];
-    return G1_OK;
+    o.tuned_ipt = best_ipt;
+    o.tuned_sched = best_merge <= vec ? G1_SCHED_MERGE : G1_SCHED_VECTOR;
+    Orientation& other = g->o[t ^ 1];
+    if (other.present && other.rp == o.rp) {
+        other.tuned_sched = o.tuned_sched;
+        other.tuned_ipt = o.tuned_ipt;
+    }
+    if (merge_ms) *merge_ms = best_merge;
+    if (vector_ms) *vector_ms = vec;
+    return check_device_error(g, s);
 }
 
 }  // extern "C"

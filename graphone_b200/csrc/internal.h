@@ -73,8 +73,9 @@ struct Orientation {
     void* val = nullptr;
     DevBuf b_rp, b_col, b_val;  // storage unless shared with the other side
     uint32_t max_deg = 0;
-    std::unique_ptr<MergePlan> plan;
+    std::map<uint32_t, std::unique_ptr<MergePlan>> plans;  // by items per tile
     int tuned_sched = 0;  // 0 = not tuned, else g1_schedule
+    int tuned_ipt = 0;    // merge items per thread chosen by g1_autotune (0 = default)
 };
 
 // Named, growable workspaces of one graph.
@@ -108,6 +109,12 @@ struct g1_graph {
     g1::Workspace ws;
     std::mutex mu;
     int sm_count = 148;
+    // Per-vertex sum of out-edge weights (PageRank's iweights denominator),
+    // derived once per graph like the merge-path plans.
+    bool outw_ready = false;
+    // Device error word written by kernels (bounded waits that ran out).
+    g1::DevBuf err_buf;
+    uint32_t* err_word = nullptr;
 };
 
 namespace g1 {
@@ -130,7 +137,9 @@ bool is_device_ptr(const void* p);
 // Copies n bytes to a device or host destination from device memory.
 g1_status copy_out(void* dst, const void* dev_src, size_t bytes, cudaStream_t s);
 
-g1_status ensure_plan(g1_graph* g, int t);
+g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out);
+// Reads and clears the graph's device error word (synchronises `s`).
+g1_status check_device_error(g1_graph* g, cudaStream_t s);
 
 // Kernel launch accounting (g1_kernel_launches) and the SpMV kernel timer
 // (g1_profile_begin/end).

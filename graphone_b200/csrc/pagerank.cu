@@ -90,37 +90,32 @@ struct PrEpilogue {
     }
 };
 
-// iweights (apps/pagerank_blas.cu:41-53: alpha / sum of out-edge weights,
-// summed in CSR order in fp32; 0 for a vertex without out-weight), the
-// initial ranks 1/N, x0 = rank0 * iw and the dangling sum of rank0.
-template <int BLOCK>
-__global__ void pr_init_kernel(const uint32_t* rp, const float* val, uint32_t n, float alpha,
-                               float* iw, float* rank0, float* x0, double* partials,
-                               unsigned* ticket, double* dang_out) {
-    __shared__ alignas(16) char smem[64 * 8];
-    const float r0 = (float)(1.0 / (double)n);
-    double dl = 0.0;
-    const uint64_t stride = (uint64_t)gridDim.x * BLOCK;
-    for (uint64_t v = (uint64_t)blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
-        float s = 0.0f;
-        for (uint32_t k = rp[v]; k < rp[v + 1]; ++k) s += val[k];
-        const float w = s != 0.0f ? alpha / s : 0.0f;
-        iw[v] = w;
-        rank0[v] = r0;
-        x0[v] = r0 * w;
-        if (w == 0.0f) dl += (double)r0;
+// Out-weight sums from the in-edge CSR only (no out-edge CSR built): a
+// weighted histogram of the column indices.  The lowest PRIV vertex ids get
+// block-private shared-memory bins (RMAT hubs sit at low ids), the rest go
+// straight to global atomics.
+template <int PRIV>
+__global__ void __launch_bounds__(256)
+pr_outw_from_transpose_kernel(const uint32_t* tcol, const float* tval, uint32_t m, uint32_t n,
+                              float* outw) {
+    __shared__ float bins[PRIV];
+    for (int i = threadIdx.x; i < PRIV; i += 256) bins[i] = 0.0f;
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * 256;
+    for (uint64_t k = (uint64_t)blockIdx.x * 256 + threadIdx.x; k < m; k += stride) {
+        const uint32_t u = __ldg(tcol + k);
+        const float w = __ldg(tval + k);
+        if (u < PRIV) atomicAdd(&bins[u], w);
+        else atomicAdd(&outw[u], w);
     }
-    fold_partials_last_block<BLOCK>(dl, partials, blockIdx.x, gridDim.x, ticket, dang_out, smem);
+    __syncthreads();
+    for (int i = threadIdx.x; i < PRIV && i < (int)n; i += 256)
+        if (bins[i] != 0.0f) atomicAdd(&outw[i], bins[i]);
 }
 
-// Out-weight sums from the in-edge CSR only (no out-edge CSR built).
-__global__ void pr_outw_from_transpose_kernel(const uint32_t* trp, const uint32_t* tcol,
-                                              const float* tval, uint32_t n, float* outw) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
-        for (uint32_t k = trp[v]; k < trp[v + 1]; ++k) atomicAdd(&outw[tcol[k]], tval[k]);
-}
-
+// iweights = alpha / out-weight (0 for a vertex without out-weight,
+// apps/pagerank_blas.cu:41-53), the initial ranks 1/N, x0 = rank0 * iw and
+// the dangling sum of rank0.
 __global__ void pr_init_from_outw_kernel(const float* outw, uint32_t n, float alpha, float* iw,
                                          float* rank0, float* x0, double* partials,
                                          unsigned* ticket, double* dang_out) {
@@ -161,32 +156,35 @@ static g1_status pr_setup(g1_graph* g, float alpha, PrBuffers& b, uint32_t* grid
     G1_TRY(ws.get("pr_x1", n, &b.x[1]));
     G1_TRY(ws.get("pr_dang", 2, &b.dang));
     G1_TRY(ws.get("pr_ticket", 4, &b.ticket));
-    G1_TRY(ensure_plan(g, t));
     // grids[0] main merge, grids[1] fixup, grids[2] vector, grids[3] init
-    grids[0] = merge_main_grid<PlusTimesF32, PrEpilogue>(g, t);
-    grids[1] = merge_fixup_grid<PlusTimesF32, PrEpilogue>(g, t);
+    G1_TRY((merge_grids<PlusTimesF32, PrEpilogue>(g, t, &grids[0], &grids[1])));
     grids[2] = vector_grid<PlusTimesF32, PrEpilogue>(g);
     grids[3] = (uint32_t)std::max<uint64_t>(
         1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
     b.n_slots = std::max(grids[0] + grids[1], std::max(grids[2], grids[3]));
     G1_TRY(ws.get("pr_partials", b.n_slots, &b.partials));
     G1_CUDA(cudaMemsetAsync(b.ticket, 0, 16, s));
-    count_launches(g->o[0].present ? 1 : 2);
-    if (g->o[0].present) {
-        pr_init_kernel<256><<<grids[3], 256, 0, s>>>(g->o[0].rp,
-                                                      static_cast<const float*>(g->o[0].val), n,
-                                                      alpha, b.iw, b.rank[0], b.x[0], b.partials,
-                                                      b.ticket, &b.dang[0]);
-    } else {
-        float* outw = nullptr;
-        G1_TRY(ws.get("pr_outw", n, &outw));
-        G1_CUDA(cudaMemsetAsync(outw, 0, (size_t)n * 4, s));
-        pr_outw_from_transpose_kernel<<<grids[3], 256, 0, s>>>(
-            g->o[1].rp, g->o[1].col, static_cast<const float*>(g->o[1].val), n, outw);
-        pr_init_from_outw_kernel<<<grids[3], 256, 0, s>>>(outw, n, alpha, b.iw, b.rank[0],
-                                                          b.x[0], b.partials, b.ticket,
-                                                          &b.dang[0]);
+    float* outw = nullptr;
+    G1_TRY(ws.get("pr_outw", n, &outw));
+    if (!g->outw_ready) {
+        if (g->o[0].present) {
+            // row sums of the out-edge CSR = plus-times SpMV against ones
+            float* ones = nullptr;
+            G1_TRY(ws.get("pr_ones", n, &ones));
+            G1_TRY(g1_mem_fill_u32(ones, 0x3f800000u, n, s));
+            G1_TRY((run_spmv<PlusTimesF32>(g, 0, G1_SCHED_AUTO, ones, StoreEpilogue<float>{outw}, s)));
+        } else {
+            G1_CUDA(cudaMemsetAsync(outw, 0, (size_t)n * 4, s));
+            pr_outw_from_transpose_kernel<8192><<<grids[3], 256, 0, s>>>(
+                g->o[1].col, static_cast<const float*>(g->o[1].val), g->m, n, outw);
+            count_launches(1);
+        }
+        G1_CUDA(cudaGetLastError());
+        g->outw_ready = true;
     }
+    pr_init_from_outw_kernel<<<grids[3], 256, 0, s>>>(outw, n, alpha, b.iw, b.rank[0], b.x[0],
+                                                      b.partials, b.ticket, &b.dang[0]);
+    count_launches(1);
     G1_CUDA(cudaGetLastError());
     return G1_OK;
 }
@@ -244,5 +242,6 @@ extern "C" g1_status g1_pagerank(g1_graph* g, float alpha, int iters, g1_pr_mode
     G1_TRY(pr_setup(g, alpha, b, grids, s));
     for (int it = 0; it < iters; ++it)
         G1_TRY(pr_iterate(g, b, grids, alpha, mode, it & 1, G1_SCHED_AUTO, s));
-    return copy_out(rank_out, b.rank[iters & 1], (size_t)g->n * 4, s);
+    G1_TRY(copy_out(rank_out, b.rank[iters & 1], (size_t)g->n * 4, s));
+    return check_device_error(g, s);
 }

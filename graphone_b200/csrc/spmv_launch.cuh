@@ -9,13 +9,13 @@
 namespace g1 {
 
 constexpr int kMergeBlock = 256;
-constexpr int kMergeIpt = 7;  // odd: consecutive threads' shared-memory reads fall in distinct banks
+constexpr int kDefaultIpt = 7;  // odd: consecutive threads' shared-memory reads fall in distinct banks
 constexpr int kVectorBlock = 256;
 
 template <class K>
-int blocks_per_sm(K kernel, int block) {
+int blocks_per_sm(K kernel, int block, size_t smem) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, 0) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, smem) != cudaSuccess) {
         cudaGetLastError();
         n = 1;
     }
@@ -41,30 +41,39 @@ inline g1_schedule resolve_schedule(const g1_graph* g, int t, g1_schedule sched)
                : G1_SCHED_MERGE;
 }
 
-template <class SR, class Epi>
-uint32_t merge_main_grid(const g1_graph* g, int t) {
-    static int occ = blocks_per_sm(spmv_merge_kernel<SR, Epi, kMergeBlock, kMergeIpt>, kMergeBlock);
-    const uint32_t tiles = g->o[t].plan->n_tiles;
-    return std::max<uint32_t>(1, std::min<uint32_t>(tiles, (uint32_t)g->sm_count * occ));
+inline int merge_ipt(const g1_graph* g, int t) {
+    const int ipt = g->o[t].tuned_ipt;
+    return (ipt == 5 || ipt == 7 || ipt == 11) ? ipt : kDefaultIpt;
 }
 
-template <class SR, class Epi>
-uint32_t merge_fixup_grid(const g1_graph* g, int t) {
-    return (uint32_t)std::max<uint64_t>(1, ceil_div(g->o[t].plan->n_tiles, kMergeBlock));
-}
+// Per-instantiation launch facts of the pipelined merge kernel.
+template <class SR, class Epi, int IPT>
+struct MergeKernel {
+    using L = MergeLayout<SR, kMergeBlock, IPT>;
+    static int occupancy() {
+        static int occ = [] {
+            auto k = spmv_merge_kernel<SR, Epi, kMergeBlock, IPT>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
+            return blocks_per_sm(k, kMergeBlock, L::BYTES);
+        }();
+        return occ;
+    }
+    static uint32_t grid(const g1_graph* g, uint32_t n_tiles) {
+        return std::max<uint32_t>(1, std::min<uint32_t>(n_tiles, (uint32_t)g->sm_count * occupancy()));
+    }
+};
 
 template <class SR, class Epi>
 uint32_t vector_grid(const g1_graph* g) {
-    static int occ = blocks_per_sm(spmv_vector_kernel<SR, Epi, kVectorBlock, 32>, kVectorBlock);
+    static int occ = blocks_per_sm(spmv_vector_kernel<SR, Epi, kVectorBlock, 32>, kVectorBlock, 0);
     const int tpr = vector_tpr(g);
     const uint64_t want = ceil_div((uint64_t)g->n * tpr, kVectorBlock);
     return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)g->sm_count * occ));
 }
 
 template <class SR>
-MergeArgs<SR> merge_args(const g1_graph* g, int t, const typename SR::x_t* x) {
+MergeArgs<SR> merge_args(const g1_graph* g, int t, const MergePlan& p, const typename SR::x_t* x) {
     const Orientation& o = g->o[t];
-    const MergePlan& p = *o.plan;
     MergeArgs<SR> a;
     a.plan.n_rows = g->n;
     a.plan.nnz = g->m;
@@ -78,26 +87,57 @@ MergeArgs<SR> merge_args(const g1_graph* g, int t, const typename SR::x_t* x) {
     a.x = x;
     a.carry = p.carry.as<typename SR::value_t>();
     a.tail = p.tail.as<typename SR::value_t>();
+    a.err = g->err_word;
     return a;
+}
+
+// Grid sizes of the merge schedule (main, fixup) for the orientation's
+// current tile size; builds the plan if needed.
+template <class SR, class Epi>
+g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_grid) {
+    const int ipt = merge_ipt(g, t);
+    MergePlan* p = nullptr;
+    G1_TRY(ensure_plan(g, t, (uint32_t)(kMergeBlock * ipt), &p));
+    switch (ipt) {
+        case 5: *main_grid = MergeKernel<SR, Epi, 5>::grid(g, p->n_tiles); break;
+        case 11: *main_grid = MergeKernel<SR, Epi, 11>::grid(g, p->n_tiles); break;
+        default: *main_grid = MergeKernel<SR, Epi, 7>::grid(g, p->n_tiles); break;
+    }
+    *fix_grid = (uint32_t)std::max<uint64_t>(1, ceil_div(p->n_tiles, kMergeBlock));
+    return G1_OK;
+}
+
+template <class SR, class Epi, int IPT>
+g1_status launch_merge_ipt(g1_graph* g, int t, const MergePlan& p, const typename SR::x_t* x,
+                           const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
+    using K = MergeKernel<SR, Epi, IPT>;
+    const MergeArgs<SR> a = merge_args<SR>(g, t, p, x);
+    const bool prof = profiling();
+    if (prof) prof_mark(s, true);
+    spmv_merge_kernel<SR, Epi, kMergeBlock, IPT>
+        <<<K::grid(g, p.n_tiles), kMergeBlock, K::L::BYTES, s>>>(a, main_epi);
+    if (prof) prof_mark(s, false);
+    count_launches(2);
+    spmv_fixup_kernel<SR, Epi, kMergeBlock>
+        <<<(uint32_t)std::max<uint64_t>(1, ceil_div(p.n_tiles, kMergeBlock)), kMergeBlock, 0, s>>>(
+            a, fix_epi);
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
 }
 
 // Merge schedule: main kernel + fixup, with distinct epilogue instances.
 template <class SR, class Epi>
 g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi& main_epi,
                        const Epi& fix_epi, cudaStream_t s) {
-    G1_TRY(ensure_plan(g, t));
-    if (g->o[t].plan->n_tiles == 0) return G1_OK;
-    const MergeArgs<SR> a = merge_args<SR>(g, t, x);
-    const bool prof = profiling();
-    if (prof) prof_mark(s, true);
-    spmv_merge_kernel<SR, Epi, kMergeBlock, kMergeIpt>
-        <<<merge_main_grid<SR, Epi>(g, t), kMergeBlock, 0, s>>>(a, main_epi);
-    if (prof) prof_mark(s, false);
-    count_launches(2);
-    spmv_fixup_kernel<SR, Epi, kMergeBlock>
-        <<<merge_fixup_grid<SR, Epi>(g, t), kMergeBlock, 0, s>>>(a, fix_epi);
-    G1_CUDA(cudaGetLastError());
-    return G1_OK;
+    const int ipt = merge_ipt(g, t);
+    MergePlan* p = nullptr;
+    G1_TRY(ensure_plan(g, t, (uint32_t)(kMergeBlock * ipt), &p));
+    if (p->n_tiles == 0) return G1_OK;
+    switch (ipt) {
+        case 5: return launch_merge_ipt<SR, Epi, 5>(g, t, *p, x, main_epi, fix_epi, s);
+        case 11: return launch_merge_ipt<SR, Epi, 11>(g, t, *p, x, main_epi, fix_epi, s);
+        default: return launch_merge_ipt<SR, Epi, 7>(g, t, *p, x, main_epi, fix_epi, s);
+    }
 }
 
 template <class SR, class Epi>

@@ -207,7 +207,8 @@ static g1_status traverse(g1_graph* g, uint32_t src, g1_engine engine, uint32_t*
         if (nF > n) return fail(G1_ERR_OVERFLOW, "frontier larger than the vertex count");
     }
     if (iters_out) *iters_out = it;
-    return copy_out(out, st.dist, (size_t)n * 4, s);
+    G1_TRY(copy_out(out, st.dist, (size_t)n * 4, s));
+    return check_device_error(g, s);
 }
 
 }  // namespace g1

@@ -8,6 +8,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 namespace g1 {
@@ -54,6 +55,18 @@ __device__ __forceinline__ T shfl_down_any(unsigned mask, T v, int delta) {
     T out;
     memcpy(&out, w, sizeof(T));
     return out;
+}
+
+// Read-only (non-coherent, L1-cached) load for values the kernel never
+// writes; plain load for types __ldg does not cover.
+template <typename T>
+__device__ __forceinline__ T ldg_any(const T* p) {
+    if constexpr (sizeof(T) == 4 || sizeof(T) == 8 || sizeof(T) == 16) {
+        if constexpr (std::is_arithmetic<T>::value) return __ldg(p);
+        else return *p;
+    } else {
+        return *p;
+    }
 }
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -111,6 +124,55 @@ __device__ __forceinline__ T block_sum(T v, T* scratch) {
         r = warp_sum(r);
     }
     return r;
+}
+
+// ------------------------------------------- TMA bulk copies + mbarriers
+// 1-D bulk copies global -> shared (cp.async.bulk) completing on an
+// mbarrier transaction count.  Source, destination and size must be
+// multiples of 16 bytes; callers pad and align their ranges.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for phase `parity` of the barrier, giving up after `limit` polls
+// (each poll suspends the thread for a bounded hardware interval).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  uint32_t limit = (1u << 22)) {
+    for (uint32_t i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
 }
 
 // ------------------------------------------------------- ceil division

@@ -128,63 +128,138 @@ __device__ __forceinline__ void block_seg_scan(bool head, typename SR::value_t v
 template <class SR>
 struct MergeArgs {
     MergePlanView plan;
-    const uint32_t* col;
-    const typename SR::w_t* val;
+    const uint32_t* col;           // readable (padded) up to round_up(nnz, 4) entries
+    const typename SR::w_t* val;   // readable (padded) up to round_up(nnz, 16 / sizeof(w_t))
     const typename SR::x_t* x;
-    typename SR::value_t* carry;  // n_tiles: partial of the row open at tile end
-    typename SR::value_t* tail;   // n_tiles: in-tile partial of a row begun earlier
+    typename SR::value_t* carry;   // n_tiles: partial of the row open at tile end
+    typename SR::value_t* tail;    // n_tiles: in-tile partial of a row begun earlier
+    uint32_t* err;                 // device error word (kDevTimeout on a stalled copy)
 };
 
-// Shared memory of one merge tile.
+// Dynamic shared memory of the pipelined merge kernel: two staging buffers
+// (row_ptr window, col, val of one tile each), the combined values of the
+// tile being folded, the scan scratch, epilogue scratch and two mbarriers.
 template <class SR, int BLOCK, int IPT>
-struct MergeSmem {
+struct MergeLayout {
+    using V = typename SR::value_t;
+    using W = typename SR::w_t;
+    static_assert(sizeof(W) == 4 || sizeof(W) == 8, "edge values of 4 or 8 bytes");
     static constexpr int ITEMS = BLOCK * IPT;
-    uint32_t row_end[ITEMS + 1];
-    typename SR::value_t v[ITEMS];
-    typename SR::value_t wval[BLOCK / 32];
-    typename SR::value_t wpre[BLOCK / 32];
-    int wflag[BLOCK / 32];
-    alignas(16) char epi[64 * 8];
+    static constexpr int AW = 16 / (int)sizeof(W);  // val elements per 16 bytes
+    static constexpr int SLOTS = ((ITEMS + 8 + 3) / 4) * 4;
+    static constexpr int VSLOTS = ((ITEMS + 2 * AW + AW - 1) / AW) * AW;
+    static constexpr size_t RE_OFF = 0;
+    static constexpr size_t COL_OFF = RE_OFF + (size_t)SLOTS * 4;
+    static constexpr size_t VAL_OFF = COL_OFF + (size_t)SLOTS * 4;
+    static constexpr size_t STAGE_BYTES = VAL_OFF + (size_t)VSLOTS * sizeof(W);
+    static constexpr size_t V_OFF = 2 * STAGE_BYTES;
+    static constexpr size_t V_BYTES = ((ITEMS * sizeof(V) + 15) / 16) * 16;
+    static constexpr size_t WVAL_OFF = V_OFF + V_BYTES;
+    static constexpr size_t WPRE_OFF = WVAL_OFF + ((BLOCK / 32) * sizeof(V) + 15) / 16 * 16;
+    static constexpr size_t WFLAG_OFF = WPRE_OFF + ((BLOCK / 32) * sizeof(V) + 15) / 16 * 16;
+    static constexpr size_t EPI_OFF = WFLAG_OFF + ((BLOCK / 32) * 4 + 15) / 16 * 16;
+    static constexpr size_t BAR_OFF = EPI_OFF + 512;
+    static constexpr size_t BYTES = BAR_OFF + 16;
 };
 
+// Issues the bulk copies of tile `tile` into staging buffer `st` (one thread).
+template <class SR, int BLOCK, int IPT>
+__device__ __forceinline__ void merge_issue_tile(const MergeArgs<SR>& a, uint32_t tile,
+                                                 unsigned char* st, uint64_t* bar) {
+    using L = MergeLayout<SR, BLOCK, IPT>;
+    using W = typename SR::w_t;
+    const uint32_t i0 = a.plan.tile_row[tile], i1 = a.plan.tile_row[tile + 1];
+    const uint32_t j0 = a.plan.tile_nnz[tile], j1 = a.plan.tile_nnz[tile + 1];
+    const uint32_t r_lo = i0 & ~3u, r_hi = (i1 + 1 + 3) & ~3u;
+    const uint32_t c_lo = j0 & ~3u, c_hi = (j1 + 3) & ~3u;
+    const uint32_t v_lo = j0 & ~(uint32_t)(L::AW - 1);
+    const uint32_t v_hi = (j1 + L::AW - 1) & ~(uint32_t)(L::AW - 1);
+    const uint32_t br = (r_hi - r_lo) * 4, bc = (c_hi - c_lo) * 4;
+    const uint32_t bv = (v_hi - v_lo) * (uint32_t)sizeof(W);
+    mbar_arrive_expect_tx(bar, br + bc + bv);
+    bulk_g2s(st + L::RE_OFF, a.plan.row_ptr + r_lo, br, bar);
+    if (bc) bulk_g2s(st + L::COL_OFF, a.col + c_lo, bc, bar);
+    if (bv) bulk_g2s(st + L::VAL_OFF, a.val + v_lo, bv, bar);
+}
+
+// Persistent merge-path SpMV: CTA b folds tiles b, b+grid, ...; while tile t
+// is folded, the bulk copies of tile t+grid land in the other staging buffer.
 template <class SR, class Epi, int BLOCK, int IPT>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, 4)
 spmv_merge_kernel(MergeArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
-    __shared__ MergeSmem<SR, BLOCK, IPT> sm;
+    using W = typename SR::w_t;
+    using L = MergeLayout<SR, BLOCK, IPT>;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    V* sv = reinterpret_cast<V*>(dsm + L::V_OFF);
+    V* s_wval = reinterpret_cast<V*>(dsm + L::WVAL_OFF);
+    V* s_wpre = reinterpret_cast<V*>(dsm + L::WPRE_OFF);
+    int* s_wflag = reinterpret_cast<int*>(dsm + L::WFLAG_OFF);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(dsm + L::BAR_OFF);
     const uint32_t tid = threadIdx.x;
     epi.begin();
 
-    for (uint32_t tile = blockIdx.x; tile < a.plan.n_tiles; tile += gridDim.x) {
-        const uint32_t i0 = a.plan.tile_row[tile];
-        const uint32_t j0 = a.plan.tile_nnz[tile];
-        const uint32_t i1 = a.plan.tile_row[tile + 1];
-        const uint32_t j1 = a.plan.tile_nnz[tile + 1];
-        const uint32_t na = i1 - i0;
-        const uint32_t nb = j1 - j0;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0 && blockIdx.x < a.plan.n_tiles)
+        merge_issue_tile<SR, BLOCK, IPT>(a, blockIdx.x, dsm, &bar[0]);
 
-        // Stage the tile's row ends (relative to j0) and combined values.
-        for (uint32_t k = tid; k < na; k += BLOCK) sm.row_end[k] = a.plan.row_ptr[i0 + 1 + k] - j0;
-        if (tid == 0) sm.row_end[na] = kU32Max;
+    uint32_t it = 0;
+    for (uint32_t tile = blockIdx.x; tile < a.plan.n_tiles; tile += gridDim.x, ++it) {
+        const uint32_t stage = it & 1u;
+        const uint32_t next = tile + gridDim.x;
+        if (tid == 0 && next < a.plan.n_tiles) {
+            fence_proxy_async_smem();
+            merge_issue_tile<SR, BLOCK, IPT>(a, next, dsm + (stage ^ 1u) * L::STAGE_BYTES,
+                                             &bar[stage ^ 1u]);
+        }
+        const uint32_t i0 = a.plan.tile_row[tile], i1 = a.plan.tile_row[tile + 1];
+        const uint32_t j0 = a.plan.tile_nnz[tile], j1 = a.plan.tile_nnz[tile + 1];
+        const uint32_t na = i1 - i0, nb = j1 - j0;
+        unsigned char* st = dsm + stage * L::STAGE_BYTES;
+        const uint32_t* RE = reinterpret_cast<const uint32_t*>(st + L::RE_OFF) + (i0 & 3u);
+        const uint32_t* CO = reinterpret_cast<const uint32_t*>(st + L::COL_OFF) + (j0 & 3u);
+        const W* VA = reinterpret_cast<const W*>(st + L::VAL_OFF) + (j0 & (uint32_t)(L::AW - 1));
+
+        const bool arrived = mbar_wait_bounded(&bar[stage], (it >> 1) & 1u);
+        if (__syncthreads_or(!arrived)) {
+            // A copy never completed: record it, let the copy already issued
+            // for the next tile land (bounded), and stop; the host sees the
+            // error word and discards this launch's results.
+            if (tid == 0) {
+                set_error(a.err, kDevTimeout);
+                if (next < a.plan.n_tiles) mbar_wait_bounded(&bar[stage ^ 1u], ((it + 1) >> 1) & 1u);
+            }
+            break;
+        }
+
+        // Gather x for the tile (IPT independent loads per thread), combine.
+        typename SR::x_t xv[IPT];
 #pragma unroll
         for (int u = 0; u < IPT; ++u) {
             const uint32_t k = (uint32_t)u * BLOCK + tid;
-            if (k < nb) {
-                const uint32_t j = j0 + k;
-                const uint32_t c = __ldg(a.col + j);
-                sm.v[k] = SR::combine(a.val[j], a.x[c]);
-            }
+            if (k < nb) xv[u] = ldg_any(a.x + CO[k]);
+        }
+#pragma unroll
+        for (int u = 0; u < IPT; ++u) {
+            const uint32_t k = (uint32_t)u * BLOCK + tid;
+            if (k < nb) sv[k] = SR::combine(VA[k], xv[u]);
         }
         __syncthreads();
 
-        // Per-thread merge-path start.
+        // Per-thread merge-path start: row-end i precedes nonzero j iff
+        // row_ptr[i0+1+i] - j0 <= j.
         const uint32_t total = na + nb;
         const uint32_t d = min(tid * (uint32_t)IPT, total);
         uint32_t lo = d > nb ? d - nb : 0;
         uint32_t hi = min(d, na);
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (sm.row_end[mid] <= d - 1 - mid)
+            if (RE[1 + mid] - j0 <= d - 1 - mid)
                 lo = mid + 1;
             else
                 hi = mid;
@@ -199,7 +274,7 @@ spmv_merge_kernel(MergeArgs<SR> a, Epi epi) {
 #pragma unroll
         for (int s = 0; s < IPT; ++s) {
             if (d + (uint32_t)s < dend) {
-                if (sm.row_end[i] <= j) {
+                if (i < na && RE[1 + i] - j0 <= j) {
                     if (!has_first) {
                         has_first = true;
                         first_row = i0 + i;
@@ -210,31 +285,28 @@ spmv_merge_kernel(MergeArgs<SR> a, Epi epi) {
                     acc = SR::identity();
                     ++i;
                 } else {
-                    acc = SR::reduce(acc, sm.v[j]);
+                    acc = SR::reduce(acc, sv[j]);
                     ++j;
                 }
             }
         }
 
         V incl, excl;
-        block_seg_scan<SR, BLOCK>(has_first, acc, incl, excl, sm.wval, sm.wflag, sm.wpre);
+        block_seg_scan<SR, BLOCK>(has_first, acc, incl, excl, s_wval, s_wflag, s_wpre);
 
         if (has_first) {
             const V val = SR::reduce(excl, first_val);
-            bool deferred = false;
-            if (first_row == i0) {
-                const uint32_t rs = a.plan.row_ptr[i0];
-                deferred = j0 > rs;  // the row began in an earlier tile
-            }
+            // the tile's first row began in an earlier tile: the fixup owns it
+            const bool deferred = first_row == i0 && j0 > RE[0];
             if (deferred)
                 a.tail[tile] = val;
             else
                 epi.emit(first_row, val);
         }
         if (tid == BLOCK - 1 && tile + 1 < a.plan.n_tiles) a.carry[tile] = incl;
-        __syncthreads();  // smem reuse by the next tile
+        __syncthreads();  // staging buffer and sv are reused next
     }
-    epi.template block_end<BLOCK>(sm.epi);
+    epi.template block_end<BLOCK>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
 }
 
 // Finishes rows that cross tiles: for every tile T whose first row began in
@@ -289,7 +361,7 @@ spmv_vector_kernel(uint32_t n_rows, const uint32_t* row_ptr, const uint32_t* col
         if (row < n_rows) {
             const uint32_t rs = row_ptr[row], re = row_ptr[row + 1];
             for (uint32_t k = rs + lane; k < re; k += TPR)
-                acc = SR::reduce(acc, SR::combine(val[k], x[__ldg(col + k)]));
+                acc = SR::reduce(acc, SR::combine(ldg_any(val + k), ldg_any(x + __ldg(col + k))));
         }
         if constexpr (TPR > 1) {
 #pragma unroll
