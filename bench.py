@@ -162,6 +162,18 @@ def barrier(ws: int):
         dist.barrier()
 
 
+def apply_schedule(G, sched: str, stream):
+    import graphone_b200 as g1
+    if sched == "tune":
+        mm, vm = G.autotune(stream=stream)
+        return f"autotuned (best merge {mm:.3f} ms, vector {vm:.3f} ms)"
+    if sched.startswith("merge"):
+        G.set_schedule(g1.SCHED_MERGE, int(sched[5:] or 0))
+    elif sched == "vector":
+        G.set_schedule(g1.SCHED_VECTOR)
+    return sched
+
+
 def run_ours(args):
     import torch
     import graphone_b200 as g1
@@ -188,6 +200,7 @@ def run_ours(args):
 
     stream = torch.cuda.current_stream(dev)
     G = g1.Graph.from_csr(h_rp, h_ci, h_v, input_transpose=True, build_other=False)
+    sched_note = apply_schedule(G, args.sched, stream)
     out = torch.empty(n, dtype=torch.float32, device=dev)
     iters = args.iters
 
@@ -265,6 +278,7 @@ def run_ours(args):
             "l2": "inputs larger than L2 (CSR streamed from HBM every iteration)",
             "parallelism": f"replicas x{ws}",
             "bytes_per_iteration": spmv_bytes(n, m),
+            "schedule": sched_note,
         },
         "gpu_launches": int(launches),
         "clocks": clocks,
@@ -405,6 +419,8 @@ def main():
     ap.add_argument("--iters", type=int, default=30)
     ap.add_argument("--ref-iters", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sched", default="tune",
+                    help="tune | auto | merge0..merge3 (kernel variant) | vector")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -67,6 +67,7 @@ def _declare(L):
     L.g1_spmv_plan.argtypes = [P, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]
     L.g1_spmv.argtypes = [P, C.c_int, C.c_int, C.c_int, P, P, P]
+    L.g1_graph_set_schedule.argtypes = [P, C.c_int, C.c_int, C.c_int]
     L.g1_autotune.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_float), P]
     L.g1_pagerank.argtypes = [P, C.c_float, C.c_int, C.c_int, P, P]
     L.g1_sssp.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
@@ -91,7 +92,7 @@ EXPORTS = (
     "g1_mem_copy", "g1_mem_fill_u32", "g1_stream_sync", "g1_kernel_launches",
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
-    "g1_spmv_plan", "g1_spmv", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs",
+    "g1_spmv_plan", "g1_spmv", "g1_graph_set_schedule", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs",
 )
 
 
@@ -206,6 +207,9 @@ class Graph:
         """y = A (semiring) x on device buffers (torch tensors)."""
         check(lib().g1_spmv(self._h, transpose, semiring, schedule, _ptr(x), _ptr(y),
                             _stream(stream)))
+
+    def set_schedule(self, schedule: int, variant: int = 0, transpose: int = 1):
+        check(lib().g1_graph_set_schedule(self._h, transpose, schedule, variant))
 
     def autotune(self, stream=None):
         a, b = C.c_float(), C.c_float()

@@ -515,7 +515,7 @@ g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t* items_per_tile, uin
     DeviceGuard dg(g->device);
     std::lock_guard<std::mutex> lk(g->mu);
     MergePlan* pp = nullptr;
-    G1_TRY(ensure_plan(g, transpose, (uint32_t)(kMergeBlock * merge_ipt(g, transpose)), &pp));
+    G1_TRY(ensure_plan(g, transpose, merge_items(merge_variant(g, transpose)), &pp));
     const MergePlan& p = *pp;
     if (items_per_tile) *items_per_tile = p.items;
     if (n_tiles) *n_tiles = p.n_tiles;
@@ -554,6 +554,19 @@ g1_status g1_spmv(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
     return fail(G1_ERR_INVALID, "g1_spmv: unknown semiring");
 }
 
+g1_status g1_graph_set_schedule(g1_graph* g, int transpose, g1_schedule sched, int variant) {
+    if (!g || transpose < 0 || transpose > 1) return fail(G1_ERR_INVALID, "g1_graph_set_schedule");
+    if (sched == G1_SCHED_MERGE && (variant < 0 || variant >= kNumMergeVariants))
+        return fail(G1_ERR_INVALID, "g1_graph_set_schedule: merge variant out of range");
+    std::lock_guard<std::mutex> lk(g->mu);
+    for (int t = 0; t < 2; ++t) {
+        if (t != transpose && !(g->o[t].present && g->o[t].rp == g->o[transpose].rp)) continue;
+        g->o[t].tuned_sched = sched == G1_SCHED_AUTO ? 0 : sched;
+        g->o[t].tuned_variant = sched == G1_SCHED_MERGE ? variant : -1;
+    }
+    return G1_OK;
+}
+
 g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, void* stream) {
     if (!g) return fail(G1_ERR_INVALID, "g1_autotune: null graph");
     DeviceGuard dg(g->device);
@@ -568,12 +581,10 @@ g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, void* stre
     cudaEvent_t e0, e1;
     G1_CUDA(cudaEventCreate(&e0));
     G1_CUDA(cudaEventCreate(&e1));
-    // candidates: merge with 5/7/11 items per thread, and CSR-vector
-    const int ipts[3] = {5, 7, 11};
+    // candidates: every merge variant, and CSR-vector
     float best_merge = 1e30f, vec = 1e30f;
-    int best_ipt = kDefaultIpt;
+    int best_variant = kDefaultVariant;
     Orientation& o = g->o[t];
-    const int saved_sched = o.tuned_sched, saved_ipt = o.tuned_ipt;
     auto time_it = [&](g1_schedule sc, float* out) -> g1_status {
         for (int rep = 0; rep < 2; ++rep)
             G1_TRY((run_spmv<BfsU32>(g, t, sc, x, StoreEpilogue<uint32_t>{y}, s)));
@@ -586,26 +597,24 @@ g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, void* stre
         *out /= 5;
         return G1_OK;
     };
-    for (int c = 0; c < 3; ++c) {
-        o.tuned_ipt = ipts[c];
+    for (int c = 0; c < kNumMergeVariants; ++c) {
+        o.tuned_variant = c;
         float ms = 0;
         G1_TRY(time_it(G1_SCHED_MERGE, &ms));
         if (ms < best_merge) {
             best_merge = ms;
-            best_ipt = ipts[c];
+            best_variant = c;
         }
     }
     G1_TRY(time_it(G1_SCHED_VECTOR, &vec));
-    (void)saved_sched;
-    (void)saved_ipt;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    o.tuned_ipt = best_ipt;
+    o.tuned_variant = best_variant;
     o.tuned_sched = best_merge <= vec ? G1_SCHED_MERGE : G1_SCHED_VECTOR;
     Orientation& other = g->o[t ^ 1];
     if (other.present && other.rp == o.rp) {
         other.tuned_sched = o.tuned_sched;
-        other.tuned_ipt = o.tuned_ipt;
+        other.tuned_variant = o.tuned_variant;
     }
     if (merge_ms) *merge_ms = best_merge;
     if (vector_ms) *vector_ms = vec;

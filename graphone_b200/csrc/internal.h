@@ -75,7 +75,7 @@ struct Orientation {
     uint32_t max_deg = 0;
     std::map<uint32_t, std::unique_ptr<MergePlan>> plans;  // by items per tile
     int tuned_sched = 0;  // 0 = not tuned, else g1_schedule
-    int tuned_ipt = 0;    // merge items per thread chosen by g1_autotune (0 = default)
+    int tuned_variant = -1;  // merge kernel variant chosen by g1_autotune (-1 = default)
 };
 
 // Named, growable workspaces of one graph.

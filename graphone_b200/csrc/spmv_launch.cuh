@@ -9,8 +9,22 @@
 namespace g1 {
 
 constexpr int kMergeBlock = 256;
-constexpr int kDefaultIpt = 7;  // odd: consecutive threads' shared-memory reads fall in distinct banks
 constexpr int kVectorBlock = 256;
+
+// Merge kernel variants the autotuner chooses from.  Warp tiles (one warp
+// per 32*ipt items, no block barrier) or block tiles (256*ipt items staged by
+// TMA bulk copies, `stages` buffers); ipt odd so that consecutive threads'
+// shared-memory reads fall in distinct banks.
+struct MergeVariant {
+    int warp_tiles;
+    int ipt;
+    int stages;  // block tiles: staging buffers; warp tiles: min resident blocks per SM
+};
+constexpr MergeVariant kMergeVariants[] = {{1, 11, 3}, {1, 7, 4}, {1, 7, 6},
+                                           {0, 7, 2}, {0, 7, 1}, {1, 15, 2}};
+constexpr int kNumMergeVariants = 6;
+constexpr int kDefaultVariant = 0;
+constexpr int kWarpsPerBlock = 8;
 
 template <class K>
 int blocks_per_sm(K kernel, int block, size_t smem) {
@@ -41,18 +55,35 @@ inline g1_schedule resolve_schedule(const g1_graph* g, int t, g1_schedule sched)
                : G1_SCHED_MERGE;
 }
 
-inline int merge_ipt(const g1_graph* g, int t) {
-    const int ipt = g->o[t].tuned_ipt;
-    return (ipt == 5 || ipt == 7 || ipt == 11) ? ipt : kDefaultIpt;
+inline int merge_variant(const g1_graph* g, int t) {
+    const int v = g->o[t].tuned_variant;
+    return (v >= 0 && v < kNumMergeVariants) ? v : kDefaultVariant;
+}
+inline uint32_t merge_items(int variant) {
+    return (kMergeVariants[variant].warp_tiles ? 32 : kMergeBlock) * kMergeVariants[variant].ipt;
 }
 
-// Per-instantiation launch facts of the pipelined merge kernel.
-template <class SR, class Epi, int IPT>
+template <class SR, class Epi, int IPT, int MINB>
+struct WarpMergeKernel {
+    static int occupancy() {
+        static int occ = blocks_per_sm(spmv_wmerge_kernel<SR, Epi, kWarpsPerBlock, IPT, MINB>,
+                                       kWarpsPerBlock * 32, 0);
+        return occ;
+    }
+    static uint32_t grid(const g1_graph* g, uint32_t n_tiles) {
+        const uint64_t want = ceil_div(n_tiles, kWarpsPerBlock);
+        return (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(want, (uint64_t)g->sm_count * occupancy()));
+    }
+};
+
+// Per-instantiation launch facts of the merge kernel.
+template <class SR, class Epi, int IPT, int STAGES>
 struct MergeKernel {
-    using L = MergeLayout<SR, kMergeBlock, IPT>;
+    using L = MergeLayout<SR, kMergeBlock, IPT, STAGES>;
     static int occupancy() {
         static int occ = [] {
-            auto k = spmv_merge_kernel<SR, Epi, kMergeBlock, IPT>;
+            auto k = spmv_merge_kernel<SR, Epi, kMergeBlock, IPT, STAGES>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
             return blocks_per_sm(k, kMergeBlock, L::BYTES);
         }();
@@ -95,27 +126,48 @@ MergeArgs<SR> merge_args(const g1_graph* g, int t, const MergePlan& p, const typ
 // current tile size; builds the plan if needed.
 template <class SR, class Epi>
 g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_grid) {
-    const int ipt = merge_ipt(g, t);
+    const int v = merge_variant(g, t);
     MergePlan* p = nullptr;
-    G1_TRY(ensure_plan(g, t, (uint32_t)(kMergeBlock * ipt), &p));
-    switch (ipt) {
-        case 5: *main_grid = MergeKernel<SR, Epi, 5>::grid(g, p->n_tiles); break;
-        case 11: *main_grid = MergeKernel<SR, Epi, 11>::grid(g, p->n_tiles); break;
-        default: *main_grid = MergeKernel<SR, Epi, 7>::grid(g, p->n_tiles); break;
+    G1_TRY(ensure_plan(g, t, merge_items(v), &p));
+    switch (v) {
+        case 1: *main_grid = WarpMergeKernel<SR, Epi, 7, 4>::grid(g, p->n_tiles); break;
+        case 2: *main_grid = WarpMergeKernel<SR, Epi, 7, 6>::grid(g, p->n_tiles); break;
+        case 3: *main_grid = MergeKernel<SR, Epi, 7, 2>::grid(g, p->n_tiles); break;
+        case 4: *main_grid = MergeKernel<SR, Epi, 7, 1>::grid(g, p->n_tiles); break;
+        case 5: *main_grid = WarpMergeKernel<SR, Epi, 15, 2>::grid(g, p->n_tiles); break;
+        default: *main_grid = WarpMergeKernel<SR, Epi, 11, 3>::grid(g, p->n_tiles); break;
     }
     *fix_grid = (uint32_t)std::max<uint64_t>(1, ceil_div(p->n_tiles, kMergeBlock));
     return G1_OK;
 }
 
-template <class SR, class Epi, int IPT>
-g1_status launch_merge_ipt(g1_graph* g, int t, const MergePlan& p, const typename SR::x_t* x,
-                           const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
-    using K = MergeKernel<SR, Epi, IPT>;
+template <class SR, class Epi, int IPT, int STAGES>
+g1_status launch_merge_v(g1_graph* g, int t, const MergePlan& p, const typename SR::x_t* x,
+                         const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
+    using K = MergeKernel<SR, Epi, IPT, STAGES>;
     const MergeArgs<SR> a = merge_args<SR>(g, t, p, x);
     const bool prof = profiling();
     if (prof) prof_mark(s, true);
-    spmv_merge_kernel<SR, Epi, kMergeBlock, IPT>
+    spmv_merge_kernel<SR, Epi, kMergeBlock, IPT, STAGES>
         <<<K::grid(g, p.n_tiles), kMergeBlock, K::L::BYTES, s>>>(a, main_epi);
+    if (prof) prof_mark(s, false);
+    count_launches(2);
+    spmv_fixup_kernel<SR, Epi, kMergeBlock>
+        <<<(uint32_t)std::max<uint64_t>(1, ceil_div(p.n_tiles, kMergeBlock)), kMergeBlock, 0, s>>>(
+            a, fix_epi);
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
+}
+
+template <class SR, class Epi, int IPT, int MINB>
+g1_status launch_wmerge(g1_graph* g, int t, const MergePlan& p, const typename SR::x_t* x,
+                        const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
+    using K = WarpMergeKernel<SR, Epi, IPT, MINB>;
+    const MergeArgs<SR> a = merge_args<SR>(g, t, p, x);
+    const bool prof = profiling();
+    if (prof) prof_mark(s, true);
+    spmv_wmerge_kernel<SR, Epi, kWarpsPerBlock, IPT, MINB>
+        <<<K::grid(g, p.n_tiles), kWarpsPerBlock * 32, 0, s>>>(a, main_epi);
     if (prof) prof_mark(s, false);
     count_launches(2);
     spmv_fixup_kernel<SR, Epi, kMergeBlock>
@@ -129,14 +181,17 @@ g1_status launch_merge_ipt(g1_graph* g, int t, const MergePlan& p, const typenam
 template <class SR, class Epi>
 g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi& main_epi,
                        const Epi& fix_epi, cudaStream_t s) {
-    const int ipt = merge_ipt(g, t);
+    const int v = merge_variant(g, t);
     MergePlan* p = nullptr;
-    G1_TRY(ensure_plan(g, t, (uint32_t)(kMergeBlock * ipt), &p));
+    G1_TRY(ensure_plan(g, t, merge_items(v), &p));
     if (p->n_tiles == 0) return G1_OK;
-    switch (ipt) {
-        case 5: return launch_merge_ipt<SR, Epi, 5>(g, t, *p, x, main_epi, fix_epi, s);
-        case 11: return launch_merge_ipt<SR, Epi, 11>(g, t, *p, x, main_epi, fix_epi, s);
-        default: return launch_merge_ipt<SR, Epi, 7>(g, t, *p, x, main_epi, fix_epi, s);
+    switch (v) {
+        case 1: return launch_wmerge<SR, Epi, 7, 4>(g, t, *p, x, main_epi, fix_epi, s);
+        case 2: return launch_wmerge<SR, Epi, 7, 6>(g, t, *p, x, main_epi, fix_epi, s);
+        case 3: return launch_merge_v<SR, Epi, 7, 2>(g, t, *p, x, main_epi, fix_epi, s);
+        case 4: return launch_merge_v<SR, Epi, 7, 1>(g, t, *p, x, main_epi, fix_epi, s);
+        case 5: return launch_wmerge<SR, Epi, 15, 2>(g, t, *p, x, main_epi, fix_epi, s);
+        default: return launch_wmerge<SR, Epi, 11, 3>(g, t, *p, x, main_epi, fix_epi, s);
     }
 }
 

@@ -72,59 +72,6 @@ __device__ __forceinline__ void merge_path_search(uint64_t d, const uint32_t* ro
     *j_out = (uint32_t)(d - lo);
 }
 
-// Block-wide inclusive/exclusive segmented scan of (head, value) pairs in
-// thread order.  A head starts a new segment with its own value.  `excl` is
-// the inclusive result of the previous thread (identity for thread 0).
-template <class SR, int BLOCK>
-__device__ __forceinline__ void block_seg_scan(bool head, typename SR::value_t val,
-                                               typename SR::value_t& incl,
-                                               typename SR::value_t& excl,
-                                               typename SR::value_t* s_wval, int* s_wflag,
-                                               typename SR::value_t* s_wpre) {
-    using V = typename SR::value_t;
-    constexpr int NW = BLOCK / 32;
-    const unsigned full = 0xffffffffu;
-    const int lane = (int)lane_id();
-    const int w = threadIdx.x >> 5;
-    V s = val;
-    int f = head ? 1 : 0;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        V su = shfl_up_any(full, s, off);
-        int fu = __shfl_up_sync(full, f, off);
-        if (lane >= off) {
-            if (!f) s = SR::reduce(su, s);
-            f |= fu;
-        }
-    }
-    if (lane == 31) {
-        s_wval[w] = s;
-        s_wflag[w] = f;
-    }
-    __syncthreads();
-    if (w == 0) {
-        V ws = lane < NW ? s_wval[lane] : SR::identity();
-        int wf = lane < NW ? s_wflag[lane] : 0;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            V su = shfl_up_any(full, ws, off);
-            int fu = __shfl_up_sync(full, wf, off);
-            if (lane >= off) {
-                if (!wf) ws = SR::reduce(su, ws);
-                wf |= fu;
-            }
-        }
-        V ex = shfl_up_any(full, ws, 1);
-        if (lane == 0) ex = SR::identity();
-        if (lane < NW) s_wpre[lane] = ex;
-    }
-    __syncthreads();
-    const V pre = s_wpre[w];
-    incl = f ? s : SR::reduce(pre, s);
-    V e = shfl_up_any(full, incl, 1);
-    excl = lane == 0 ? pre : e;
-}
-
 template <class SR>
 struct MergeArgs {
     MergePlanView plan;
@@ -136,10 +83,95 @@ struct MergeArgs {
     uint32_t* err;                 // device error word (kDevTimeout on a stalled copy)
 };
 
-// Dynamic shared memory of the pipelined merge kernel: two staging buffers
-// (row_ptr window, col, val of one tile each), the combined values of the
-// tile being folded, the scan scratch, epilogue scratch and two mbarriers.
-template <class SR, int BLOCK, int IPT>
+// (row, partial) pair carried by the tile scan: the row a segment belongs
+// to travels with its partial value.
+template <class V>
+struct RowPartial {
+    uint32_t row;
+    V val;
+};
+
+// Block-wide segmented scan of (head, row, value) in thread order: a head
+// thread starts a new segment with its own (row, value); other threads
+// extend the segment of the nearest head before them.  Rows of segments
+// that began before thread 0 read as kU32Max.
+template <class SR, int BLOCK>
+__device__ __forceinline__ void block_seg_scan_rows(bool head, RowPartial<typename SR::value_t> v,
+                                                    RowPartial<typename SR::value_t>& incl,
+                                                    RowPartial<typename SR::value_t>& excl,
+                                                    RowPartial<typename SR::value_t>* s_w,
+                                                    int* s_wflag,
+                                                    RowPartial<typename SR::value_t>* s_wpre) {
+    using P = RowPartial<typename SR::value_t>;
+    constexpr int NW = BLOCK / 32;
+    const unsigned full = 0xffffffffu;
+    const int lane = (int)lane_id();
+    const int w = threadIdx.x >> 5;
+    P s = v;
+    int f = head ? 1 : 0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        P su = shfl_up_any(full, s, off);
+        int fu = __shfl_up_sync(full, f, off);
+        if (lane >= off) {
+            if (!f) {
+                s.val = SR::reduce(su.val, s.val);
+                s.row = su.row;
+            }
+            f |= fu;
+        }
+    }
+    if (lane == 31) {
+        s_w[w] = s;
+        s_wflag[w] = f;
+    }
+    __syncthreads();
+    if (w == 0) {
+        P ws;
+        ws.row = kU32Max;
+        ws.val = SR::identity();
+        int wf = 0;
+        if (lane < NW) {
+            ws = s_w[lane];
+            wf = s_wflag[lane];
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            P su = shfl_up_any(full, ws, off);
+            int fu = __shfl_up_sync(full, wf, off);
+            if (lane >= off) {
+                if (!wf) {
+                    ws.val = SR::reduce(su.val, ws.val);
+                    ws.row = su.row;
+                }
+                wf |= fu;
+            }
+        }
+        P ex = shfl_up_any(full, ws, 1);
+        if (lane == 0) {
+            ex.row = kU32Max;
+            ex.val = SR::identity();
+        }
+        if (lane < NW) s_wpre[lane] = ex;
+    }
+    __syncthreads();
+    const P pre = s_wpre[w];
+    incl = s;
+    if (!f) {
+        incl.val = SR::reduce(pre.val, s.val);
+        incl.row = pre.row;
+    }
+    P e = shfl_up_any(full, incl, 1);
+    excl = lane == 0 ? pre : e;
+}
+
+// Dynamic shared memory of the merge kernel: STAGES staging buffers (row_ptr
+// window, col, val of one tile each) plus scan/epilogue scratch and the
+// mbarriers.  With 4-byte values the combined values overwrite the staged
+// col slots and the per-item row-start marks overwrite the staged val slots
+// (each thread rewrites only the slots it read), so a stage is all the
+// per-tile memory; other sizes get their own arrays.
+template <class SR, int BLOCK, int IPT, int STAGES>
 struct MergeLayout {
     using V = typename SR::value_t;
     using W = typename SR::w_t;
@@ -148,29 +180,36 @@ struct MergeLayout {
     static constexpr int AW = 16 / (int)sizeof(W);  // val elements per 16 bytes
     static constexpr int SLOTS = ((ITEMS + 8 + 3) / 4) * 4;
     static constexpr int VSLOTS = ((ITEMS + 2 * AW + AW - 1) / AW) * AW;
+    static constexpr bool SV_ALIAS = sizeof(V) == 4;
+    static constexpr bool SROW_ALIAS = sizeof(W) == 4;
     static constexpr size_t RE_OFF = 0;
     static constexpr size_t COL_OFF = RE_OFF + (size_t)SLOTS * 4;
     static constexpr size_t VAL_OFF = COL_OFF + (size_t)SLOTS * 4;
-    static constexpr size_t STAGE_BYTES = VAL_OFF + (size_t)VSLOTS * sizeof(W);
-    static constexpr size_t V_OFF = 2 * STAGE_BYTES;
-    static constexpr size_t V_BYTES = ((ITEMS * sizeof(V) + 15) / 16) * 16;
-    static constexpr size_t WVAL_OFF = V_OFF + V_BYTES;
-    static constexpr size_t WPRE_OFF = WVAL_OFF + ((BLOCK / 32) * sizeof(V) + 15) / 16 * 16;
-    static constexpr size_t WFLAG_OFF = WPRE_OFF + ((BLOCK / 32) * sizeof(V) + 15) / 16 * 16;
+    static constexpr size_t STAGE_BYTES = ((VAL_OFF + (size_t)VSLOTS * sizeof(W)) + 15) / 16 * 16;
+    static constexpr size_t SV_OFF = STAGES * STAGE_BYTES;
+    static constexpr size_t SV_BYTES = SV_ALIAS ? 0 : ((ITEMS * sizeof(V) + 15) / 16) * 16;
+    static constexpr size_t SROW_OFF = SV_OFF + SV_BYTES;
+    static constexpr size_t SROW_BYTES = SROW_ALIAS ? 0 : (size_t)SLOTS * 4;
+    using P = RowPartial<V>;
+    static constexpr size_t W_OFF = SROW_OFF + SROW_BYTES;
+    static constexpr size_t WP_BYTES = ((BLOCK / 32) * sizeof(P) + 15) / 16 * 16;
+    static constexpr size_t WPRE_OFF = W_OFF + WP_BYTES;
+    static constexpr size_t WFLAG_OFF = WPRE_OFF + WP_BYTES;
     static constexpr size_t EPI_OFF = WFLAG_OFF + ((BLOCK / 32) * 4 + 15) / 16 * 16;
     static constexpr size_t BAR_OFF = EPI_OFF + 512;
     static constexpr size_t BYTES = BAR_OFF + 16;
 };
 
-// Issues the bulk copies of tile `tile` into staging buffer `st` (one thread).
-template <class SR, int BLOCK, int IPT>
+// Issues the bulk copies of tile `tile` into staging buffer `st` (one
+// thread): row_ptr[i0 .. i1+1], col and val of nonzeros [j0, j1), each range
+// widened to 16-byte boundaries (the arrays are padded for that).
+template <class L, class SR>
 __device__ __forceinline__ void merge_issue_tile(const MergeArgs<SR>& a, uint32_t tile,
                                                  unsigned char* st, uint64_t* bar) {
-    using L = MergeLayout<SR, BLOCK, IPT>;
     using W = typename SR::w_t;
     const uint32_t i0 = a.plan.tile_row[tile], i1 = a.plan.tile_row[tile + 1];
     const uint32_t j0 = a.plan.tile_nnz[tile], j1 = a.plan.tile_nnz[tile + 1];
-    const uint32_t r_lo = i0 & ~3u, r_hi = (i1 + 1 + 3) & ~3u;
+    const uint32_t r_lo = i0 & ~3u, r_hi = (i1 + 2 + 3) & ~3u;
     const uint32_t c_lo = j0 & ~3u, c_hi = (j1 + 3) & ~3u;
     const uint32_t v_lo = j0 & ~(uint32_t)(L::AW - 1);
     const uint32_t v_hi = (j1 + L::AW - 1) & ~(uint32_t)(L::AW - 1);
@@ -182,18 +221,30 @@ __device__ __forceinline__ void merge_issue_tile(const MergeArgs<SR>& a, uint32_
     if (bv) bulk_g2s(st + L::VAL_OFF, a.val + v_lo, bv, bar);
 }
 
-// Persistent merge-path SpMV: CTA b folds tiles b, b+grid, ...; while tile t
-// is folded, the bulk copies of tile t+grid land in the other staging buffer.
-template <class SR, class Epi, int BLOCK, int IPT>
-__global__ void __launch_bounds__(BLOCK, 4)
+// Persistent merge-path SpMV.  CTA b folds tiles b, b+grid, ... (tile
+// boundaries from the merge-path partition, so rows + nonzeros are balanced
+// across tiles whatever the degree distribution).  Per tile:
+//   1. wait for the tile's bulk copies (with STAGES == 2 the next tile's
+//      copies are already in flight into the other buffer);
+//   2. each thread gathers x for IPT strided nonzeros and combines them;
+//   3. rows are walked: empty rows emit identity at once, every non-empty
+//      row that starts inside the tile marks its first nonzero with its id;
+//   4. each thread folds IPT consecutive nonzeros, closing a segment at
+//      every mark (independent shared-memory reads: no search, no chain);
+//   5. a (row, value) segmented scan carries open segments across threads;
+//      the first segment of each thread and the tile's last segment are
+//      emitted after it.  A row that began in an earlier tile is finished by
+//      spmv_fixup_kernel from the tiles' carries (tail holds its in-tile part).
+template <class SR, class Epi, int BLOCK, int IPT, int STAGES>
+__global__ void __launch_bounds__(BLOCK, STAGES == 1 ? 6 : 4)
 spmv_merge_kernel(MergeArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
     using W = typename SR::w_t;
-    using L = MergeLayout<SR, BLOCK, IPT>;
+    using L = MergeLayout<SR, BLOCK, IPT, STAGES>;
+    using P = RowPartial<V>;
     extern __shared__ __align__(16) unsigned char dsm[];
-    V* sv = reinterpret_cast<V*>(dsm + L::V_OFF);
-    V* s_wval = reinterpret_cast<V*>(dsm + L::WVAL_OFF);
-    V* s_wpre = reinterpret_cast<V*>(dsm + L::WPRE_OFF);
+    P* s_w = reinterpret_cast<P*>(dsm + L::W_OFF);
+    P* s_wpre = reinterpret_cast<P*>(dsm + L::WPRE_OFF);
     int* s_wflag = reinterpret_cast<int*>(dsm + L::WFLAG_OFF);
     uint64_t* bar = reinterpret_cast<uint64_t*>(dsm + L::BAR_OFF);
     const uint32_t tid = threadIdx.x;
@@ -206,38 +257,43 @@ spmv_merge_kernel(MergeArgs<SR> a, Epi epi) {
     }
     __syncthreads();
     if (tid == 0 && blockIdx.x < a.plan.n_tiles)
-        merge_issue_tile<SR, BLOCK, IPT>(a, blockIdx.x, dsm, &bar[0]);
+        merge_issue_tile<L>(a, blockIdx.x, dsm, &bar[0]);
 
     uint32_t it = 0;
     for (uint32_t tile = blockIdx.x; tile < a.plan.n_tiles; tile += gridDim.x, ++it) {
-        const uint32_t stage = it & 1u;
+        const uint32_t stage = STAGES == 2 ? (it & 1u) : 0u;
+        const uint32_t parity = STAGES == 2 ? ((it >> 1) & 1u) : (it & 1u);
         const uint32_t next = tile + gridDim.x;
-        if (tid == 0 && next < a.plan.n_tiles) {
+        if (STAGES == 2 && tid == 0 && next < a.plan.n_tiles) {
             fence_proxy_async_smem();
-            merge_issue_tile<SR, BLOCK, IPT>(a, next, dsm + (stage ^ 1u) * L::STAGE_BYTES,
-                                             &bar[stage ^ 1u]);
+            merge_issue_tile<L>(a, next, dsm + (stage ^ 1u) * L::STAGE_BYTES, &bar[stage ^ 1u]);
         }
         const uint32_t i0 = a.plan.tile_row[tile], i1 = a.plan.tile_row[tile + 1];
         const uint32_t j0 = a.plan.tile_nnz[tile], j1 = a.plan.tile_nnz[tile + 1];
-        const uint32_t na = i1 - i0, nb = j1 - j0;
+        const uint32_t nb = j1 - j0;
         unsigned char* st = dsm + stage * L::STAGE_BYTES;
         const uint32_t* RE = reinterpret_cast<const uint32_t*>(st + L::RE_OFF) + (i0 & 3u);
         const uint32_t* CO = reinterpret_cast<const uint32_t*>(st + L::COL_OFF) + (j0 & 3u);
         const W* VA = reinterpret_cast<const W*>(st + L::VAL_OFF) + (j0 & (uint32_t)(L::AW - 1));
+        V* sv = L::SV_ALIAS ? reinterpret_cast<V*>(const_cast<uint32_t*>(CO))
+                            : reinterpret_cast<V*>(dsm + L::SV_OFF);
+        uint32_t* srow = L::SROW_ALIAS ? reinterpret_cast<uint32_t*>(const_cast<W*>(VA))
+                                       : reinterpret_cast<uint32_t*>(dsm + L::SROW_OFF);
 
-        const bool arrived = mbar_wait_bounded(&bar[stage], (it >> 1) & 1u);
+        const bool arrived = mbar_wait_bounded(&bar[stage], parity);
         if (__syncthreads_or(!arrived)) {
             // A copy never completed: record it, let the copy already issued
             // for the next tile land (bounded), and stop; the host sees the
             // error word and discards this launch's results.
             if (tid == 0) {
                 set_error(a.err, kDevTimeout);
-                if (next < a.plan.n_tiles) mbar_wait_bounded(&bar[stage ^ 1u], ((it + 1) >> 1) & 1u);
+                if (STAGES == 2 && next < a.plan.n_tiles)
+                    mbar_wait_bounded(&bar[stage ^ 1u], ((it + 1) >> 1) & 1u);
             }
             break;
         }
 
-        // Gather x for the tile (IPT independent loads per thread), combine.
+        // 2. gather + combine; clear the row-start marks of the same slots
         typename SR::x_t xv[IPT];
 #pragma unroll
         for (int u = 0; u < IPT; ++u) {
@@ -247,66 +303,289 @@ spmv_merge_kernel(MergeArgs<SR> a, Epi epi) {
 #pragma unroll
         for (int u = 0; u < IPT; ++u) {
             const uint32_t k = (uint32_t)u * BLOCK + tid;
-            if (k < nb) sv[k] = SR::combine(VA[k], xv[u]);
+            if (k < nb) {
+                const V c = SR::combine(VA[k], xv[u]);
+                sv[k] = c;
+                srow[k] = kU32Max;
+            }
         }
         __syncthreads();
 
-        // Per-thread merge-path start: row-end i precedes nonzero j iff
-        // row_ptr[i0+1+i] - j0 <= j.
-        const uint32_t total = na + nb;
-        const uint32_t d = min(tid * (uint32_t)IPT, total);
-        uint32_t lo = d > nb ? d - nb : 0;
-        uint32_t hi = min(d, na);
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (RE[1 + mid] - j0 <= d - 1 - mid)
-                lo = mid + 1;
-            else
-                hi = mid;
+        // 3. rows of the tile: i0 .. i1 (i1 may only start here).  The first
+        // row is "spanning" when some of its nonzeros lie in earlier tiles.
+        const bool spanning = j0 > RE[0];
+        for (uint32_t r = i0 + tid; r <= i1; r += BLOCK) {
+            const uint32_t rs = RE[r - i0], re = RE[r - i0 + 1];
+            if (r == i0 && spanning) {
+                // completes here with no nonzero in this tile: in-tile part is empty
+                if (i1 > i0 && re == j0) a.tail[tile] = SR::identity();
+                continue;
+            }
+            if (r < i1 && re == rs) {
+                epi.emit(r, SR::identity());  // empty row
+            } else if (rs < j1) {
+                srow[rs - j0] = r;  // non-empty row starting in this tile
+            }
         }
-        uint32_t i = lo, j = d - lo;
-        const uint32_t dend = min(d + (uint32_t)IPT, total);
+        __syncthreads();
 
+        // 4. per-thread fold of IPT consecutive nonzeros
+        const uint32_t k0 = tid * (uint32_t)IPT;
         V acc = SR::identity();
-        bool has_first = false;
-        uint32_t first_row = 0;
+        bool head = false;
+        uint32_t open_row = kU32Max;
         V first_val = acc;
+        uint32_t lead = 0;  // nonzeros folded before the first mark
 #pragma unroll
-        for (int s = 0; s < IPT; ++s) {
-            if (d + (uint32_t)s < dend) {
-                if (i < na && RE[1 + i] - j0 <= j) {
-                    if (!has_first) {
-                        has_first = true;
-                        first_row = i0 + i;
+        for (int u = 0; u < IPT; ++u) {
+            const uint32_t k = k0 + (uint32_t)u;
+            if (k < nb) {
+                const uint32_t mark = srow[k];
+                const V val = sv[k];
+                if (mark != kU32Max) {
+                    if (!head) {
+                        head = true;
                         first_val = acc;
+                        lead = (uint32_t)u;
                     } else {
-                        epi.emit(i0 + i, acc);
+                        epi.emit(open_row, acc);
                     }
+                    open_row = mark;
                     acc = SR::identity();
-                    ++i;
-                } else {
-                    acc = SR::reduce(acc, sv[j]);
-                    ++j;
                 }
+                acc = SR::reduce(acc, val);
             }
         }
 
-        V incl, excl;
-        block_seg_scan<SR, BLOCK>(has_first, acc, incl, excl, s_wval, s_wflag, s_wpre);
+        // 5. stitch segments across threads
+        P mine;
+        mine.row = open_row;
+        mine.val = acc;
+        P incl, excl;
+        block_seg_scan_rows<SR, BLOCK>(head, mine, incl, excl, s_w, s_wflag, s_wpre);
 
-        if (has_first) {
-            const V val = SR::reduce(excl, first_val);
-            // the tile's first row began in an earlier tile: the fixup owns it
-            const bool deferred = first_row == i0 && j0 > RE[0];
-            if (deferred)
-                a.tail[tile] = val;
-            else
-                epi.emit(first_row, val);
+        if (head && !(tid == 0 && lead == 0)) {
+            // the segment open at this thread's start ends before its first mark
+            const V val = SR::reduce(excl.val, first_val);
+            if (excl.row == kU32Max) {
+                if (spanning) a.tail[tile] = val;  // first row began in an earlier tile
+            } else {
+                epi.emit(excl.row, val);
+            }
         }
-        if (tid == BLOCK - 1 && tile + 1 < a.plan.n_tiles) a.carry[tile] = incl;
-        __syncthreads();  // staging buffer and sv are reused next
+        if (tid == BLOCK - 1) {
+            // the tile's last segment
+            uint32_t lr = incl.row;
+            if (lr == kU32Max && spanning) lr = i0;
+            V carry = SR::identity();
+            if (lr != kU32Max) {
+                if (lr < i1) {  // completes at the tile's end
+                    if (lr == i0 && spanning)
+                        a.tail[tile] = incl.val;
+                    else
+                        epi.emit(lr, incl.val);
+                } else {
+                    carry = incl.val;  // row i1 continues in the next tile
+                }
+            }
+            if (tile + 1 < a.plan.n_tiles) a.carry[tile] = carry;
+        }
+        __syncthreads();  // staging buffer reuse
+        if (STAGES == 1 && tid == 0 && next < a.plan.n_tiles) {
+            fence_proxy_async_smem();
+            merge_issue_tile<L>(a, next, dsm, &bar[0]);
+        }
     }
     epi.template block_end<BLOCK>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
+}
+
+// Warp-level (row, value) segmented scan, same contract as the block scan.
+template <class SR>
+__device__ __forceinline__ void warp_seg_scan_rows(bool head, RowPartial<typename SR::value_t> v,
+                                                   RowPartial<typename SR::value_t>& incl,
+                                                   RowPartial<typename SR::value_t>& excl) {
+    using P = RowPartial<typename SR::value_t>;
+    const unsigned full = 0xffffffffu;
+    const int lane = (int)lane_id();
+    P s = v;
+    int f = head ? 1 : 0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        P su = shfl_up_any(full, s, off);
+        int fu = __shfl_up_sync(full, f, off);
+        if (lane >= off) {
+            if (!f) {
+                s.val = SR::reduce(su.val, s.val);
+                s.row = su.row;
+            }
+            f |= fu;
+        }
+    }
+    incl = s;
+    P e = shfl_up_any(full, s, 1);
+    if (lane == 0) {
+        e.row = kU32Max;
+        e.val = SR::identity();
+    }
+    excl = e;
+}
+
+// Warp-tile merge-path SpMV: the merge-path partition is cut into tiles of
+// 32*IPT items and every warp folds its own tiles with no block barrier.
+// Lane l loads nonzeros l, l+32, ... of the tile (coalesced), gathers x and
+// combines into the warp's shared-memory slice; rows of the tile are walked
+// the same way (empty rows emit identity, row starts are marked); then lane
+// l folds items [l*IPT, (l+1)*IPT) (odd IPT: bank-conflict free), a warp
+// (row, value) segmented scan carries open segments across lanes, and rows
+// that cross tiles are finished by spmv_fixup_kernel.
+template <class SR, class Epi, int WARPS, int IPT, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
+    using V = typename SR::value_t;
+    using P = RowPartial<V>;
+    constexpr int WITEMS = 32 * IPT;
+    __shared__ V s_v[WARPS][WITEMS];
+    __shared__ uint32_t s_row[WARPS][WITEMS];
+    __shared__ alignas(16) char epi_smem[64 * 8];
+    const uint32_t lane = lane_id();
+    const uint32_t w = threadIdx.x >> 5;
+    V* sv = s_v[w];
+    uint32_t* srow = s_row[w];
+    epi.begin();
+    const uint32_t total_warps = gridDim.x * WARPS;
+    uint32_t tile = blockIdx.x * WARPS + w;
+    // tile coordinates are fetched one tile ahead
+    uint32_t c_i0 = 0, c_i1 = 0, c_j0 = 0, c_j1 = 0;
+    if (tile < a.plan.n_tiles) {
+        c_i0 = a.plan.tile_row[tile];
+        c_i1 = a.plan.tile_row[tile + 1];
+        c_j0 = a.plan.tile_nnz[tile];
+        c_j1 = a.plan.tile_nnz[tile + 1];
+    }
+    for (; tile < a.plan.n_tiles; tile += total_warps) {
+        const uint32_t i0 = c_i0, i1 = c_i1, j0 = c_j0, j1 = c_j1;
+        const uint32_t nxt = tile + total_warps;
+        if (nxt < a.plan.n_tiles) {
+            c_i0 = a.plan.tile_row[nxt];
+            c_i1 = a.plan.tile_row[nxt + 1];
+            c_j0 = a.plan.tile_nnz[nxt];
+            c_j1 = a.plan.tile_nnz[nxt + 1];
+        }
+        const uint32_t nb = j1 - j0;
+        // All independent loads of the tile go out together: col and val of
+        // the nonzeros, and row_ptr of the tile's first 32 rows.
+        uint32_t cv[IPT];
+        typename SR::w_t wv[IPT];
+#pragma unroll
+        for (int u = 0; u < IPT; ++u) {
+            const uint32_t k = (uint32_t)u * 32 + lane;
+            if (k < nb) {
+                cv[u] = __ldg(a.col + j0 + k);
+                wv[u] = ldg_any(a.val + j0 + k);
+            }
+        }
+        const uint32_t r_lane = i0 + lane;
+        uint32_t ra = 0, rb = 0;
+        if (r_lane <= i1) {
+            ra = __ldg(a.plan.row_ptr + r_lane);
+            rb = __ldg(a.plan.row_ptr + r_lane + 1);
+        }
+        typename SR::x_t xv[IPT];
+#pragma unroll
+        for (int u = 0; u < IPT; ++u) {
+            const uint32_t k = (uint32_t)u * 32 + lane;
+            if (k < nb) xv[u] = ldg_any(a.x + cv[u]);
+        }
+        const bool spanning = j0 > __shfl_sync(0xffffffffu, ra, 0);
+#pragma unroll
+        for (int u = 0; u < IPT; ++u) {
+            const uint32_t k = (uint32_t)u * 32 + lane;
+            if (k < nb) {
+                sv[k] = SR::combine(wv[u], xv[u]);
+                srow[k] = kU32Max;
+            }
+        }
+        __syncwarp();
+        // Rows i0..i1 of the tile: empty rows emit identity, starts are marked.
+        for (uint32_t r = r_lane; r <= i1; r += 32) {
+            uint32_t rs = ra, re = rb;
+            if (r != r_lane) {
+                rs = __ldg(a.plan.row_ptr + r);
+                re = __ldg(a.plan.row_ptr + r + 1);
+            }
+            if (r == i0 && spanning) {
+                if (i1 > i0 && re == j0) a.tail[tile] = SR::identity();
+                continue;
+            }
+            if (r < i1) {
+                if (re == rs)
+                    epi.emit(r, SR::identity());  // empty row
+                else
+                    srow[rs - j0] = r;
+            } else if (rs < j1) {
+                srow[rs - j0] = r;  // row i1 starts here and continues
+            }
+        }
+        __syncwarp();
+
+        const uint32_t k0 = lane * (uint32_t)IPT;
+        V acc = SR::identity();
+        bool head = false;
+        uint32_t open_row = kU32Max;
+        V first_val = acc;
+        uint32_t lead = 0;
+#pragma unroll
+        for (int u = 0; u < IPT; ++u) {
+            const uint32_t k = k0 + (uint32_t)u;
+            if (k < nb) {
+                const uint32_t mark = srow[k];
+                const V val = sv[k];
+                if (mark != kU32Max) {
+                    if (!head) {
+                        head = true;
+                        first_val = acc;
+                        lead = (uint32_t)u;
+                    } else {
+                        epi.emit(open_row, acc);
+                    }
+                    open_row = mark;
+                    acc = SR::identity();
+                }
+                acc = SR::reduce(acc, val);
+            }
+        }
+        P mine;
+        mine.row = open_row;
+        mine.val = acc;
+        P incl, excl;
+        warp_seg_scan_rows<SR>(head, mine, incl, excl);
+        if (head && !(lane == 0 && lead == 0)) {
+            const V val = SR::reduce(excl.val, first_val);
+            if (excl.row == kU32Max) {
+                if (spanning) a.tail[tile] = val;
+            } else {
+                epi.emit(excl.row, val);
+            }
+        }
+        if (lane == 31) {
+            uint32_t lr = incl.row;
+            if (lr == kU32Max && spanning) lr = i0;
+            V carry = SR::identity();
+            if (lr != kU32Max) {
+                if (lr < i1) {
+                    if (lr == i0 && spanning)
+                        a.tail[tile] = incl.val;
+                    else
+                        epi.emit(lr, incl.val);
+                } else {
+                    carry = incl.val;
+                }
+            }
+            if (tile + 1 < a.plan.n_tiles) a.carry[tile] = carry;
+        }
+        __syncwarp();
+    }
+    epi.template block_end<WARPS * 32>(epi_smem);
 }
 
 // Finishes rows that cross tiles: for every tile T whose first row began in

@@ -131,8 +131,17 @@ g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t* items_per_tile,
  * device synchronisation). x, y device pointers of n entries. */
 g1_status g1_spmv(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
                   const void* x, void* y, void* stream);
-/* Times both schedules for each semiring class on this graph and keeps the
- * faster for G1_SCHED_AUTO.  Results in ms (may be NULL). */
+/* Fixes the schedule G1_SCHED_AUTO resolves to for one orientation:
+ * G1_SCHED_MERGE with a merge kernel variant (warp tiles of 32 x items:
+ * 0: 11 items/lane, 1: 7 at 4 blocks/SM, 2: 7 at 6 blocks/SM, 5: 15;
+ * block tiles of 256 x 7 items staged by TMA bulk copies: 3: two staging
+ * buffers, 4: one), or G1_SCHED_VECTOR;
+ * G1_SCHED_AUTO restores the heuristic.  No GraphOne counterpart (GraphOne hard-wires the
+ * merge schedule, engine/blas_gc.h:130-132). */
+g1_status g1_graph_set_schedule(g1_graph* g, int transpose, g1_schedule sched, int variant);
+/* Times the merge schedule at each tile size and the CSR-vector schedule on
+ * this graph and keeps the fastest for G1_SCHED_AUTO.  Results in ms (may be
+ * NULL): the best merge time and the vector time. */
 g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, void* stream);
 
 /* ------------------------------------------------------------- algorithms */

@@ -102,3 +102,40 @@ def test_malformed_csr_is_rejected(cuda):
     with pytest.raises(g1.G1Error) as e:
         g1.Graph.from_csr(rp, ci, v)
     assert e.value.status == 1
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("name", ["star20k", "rmat10_sym", "rmat11_dir", "path3000", "empty5"])
+def test_every_merge_variant(cuda, name, variant):
+    g = GRAPHS[name]
+    G = g1.Graph.from_gen(g)
+    G.set_schedule(g1.SCHED_MERGE, variant, transpose=1)
+    rp, ci, v = g.np("t")
+    rng = np.random.default_rng(5)
+    x = np.full(g.n, O.U32_MAX, np.uint32)
+    sel = rng.random(g.n) < 0.3
+    x[sel] = rng.integers(0, 1 << 20, size=int(sel.sum()), dtype=np.uint32)
+    xd = torch.from_numpy(x.view(np.int32)).cuda()
+    yd = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    G.spmv(xd, yd, g1.SR_MINPLUS_U32, transpose=1, schedule=g1.SCHED_MERGE)
+    assert np.array_equal(yd.cpu().numpy().view(np.uint32), O.spmv_minplus_u32(rp, ci, v, x))
+    # plus-times on the same graph, fp32 vs fp64
+    xf = rng.random(g.n).astype(np.float32)
+    vf = v.astype(np.float32)
+    Gf = g1.Graph.from_csr(rp, ci, vf, input_transpose=True, build_other=False)
+    Gf.set_schedule(g1.SCHED_MERGE, variant, transpose=1)
+    yf = torch.empty(g.n, dtype=torch.float32, device="cuda")
+    Gf.spmv(torch.from_numpy(xf).cuda(), yf, g1.SR_PLUSTIMES_F32, transpose=1,
+            schedule=g1.SCHED_MERGE)
+    y64 = O.spmv_plustimes_f64(rp, ci, vf.astype(np.float64), xf.astype(np.float64))
+    assert O.rel_l1(yf.cpu().numpy(), y64) < 1e-6
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5])
+def test_pagerank_every_merge_variant(cuda, variant):
+    g = gen.rmat(13, 16, False, float_values=True)
+    G = g1.Graph.from_gen(g)
+    G.set_schedule(g1.SCHED_MERGE, variant, transpose=1)
+    trp, tci, tv = g.np("t")
+    r = G.pagerank(0.85, 20, g1.PR_DANGLING)
+    assert O.rel_l1(r, O.pagerank_f64(trp, tci, tv, 0.85, 20, 1)) < 1e-6
