@@ -199,7 +199,8 @@ def run_ours(args):
     torch.cuda.empty_cache()
 
     stream = torch.cuda.current_stream(dev)
-    G = g1.Graph.from_csr(h_rp, h_ci, h_v, input_transpose=True, build_other=False)
+    G = g1.Graph.from_csr(h_rp, h_ci, h_v, input_transpose=True, build_other=False,
+                          relabel=not args.no_relabel)
     sched_note = apply_schedule(G, args.sched, stream)
     out = torch.empty(n, dtype=torch.float32, device=dev)
     iters = args.iters
@@ -279,6 +280,8 @@ def run_ours(args):
             "parallelism": f"replicas x{ws}",
             "bytes_per_iteration": spmv_bytes(n, m),
             "schedule": sched_note,
+            "layout": ("resident graph stored in decreasing out-degree order (G1_GRAPH_RELABEL); "
+                       "results in caller order") if not args.no_relabel else "caller order",
         },
         "gpu_launches": int(launches),
         "clocks": clocks,
@@ -419,6 +422,7 @@ def main():
     ap.add_argument("--iters", type=int, default=30)
     ap.add_argument("--ref-iters", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-relabel", action="store_true")
     ap.add_argument("--sched", default="tune",
                     help="tune | auto | merge0..merge3 (kernel variant) | vector")
     args = ap.parse_args()

@@ -27,6 +27,7 @@ SCHED_AUTO, SCHED_MERGE, SCHED_VECTOR = 0, 1, 2
 ENGINE_BLAS, ENGINE_ADVANCE, ENGINE_AUTO = 0, 1, 2
 PR_REFERENCE, PR_DANGLING = 0, 1
 GRAPH_SYMMETRIC, GRAPH_INPUT_TRANSPOSE, GRAPH_BUILD_OTHER, GRAPH_NO_VALIDATE = 1, 2, 4, 8
+GRAPH_RELABEL = 16
 
 STATUS = {0: "G1_OK", 1: "G1_ERR_INVALID", 2: "G1_ERR_OOM", 3: "G1_ERR_DEVICE",
           4: "G1_ERR_TIMEOUT", 5: "G1_ERR_UNSUPPORTED", 6: "G1_ERR_OVERFLOW"}
@@ -142,7 +143,7 @@ class Graph:
 
     @classmethod
     def from_csr(cls, row_ptr, col, val, *, symmetric=False, input_transpose=False,
-                 build_other=True, validate=True, stream=None) -> "Graph":
+                 build_other=True, validate=True, relabel=False, stream=None) -> "Graph":
         """CSR arrays: numpy (host) or torch tensors (host or device)."""
         if isinstance(row_ptr, np.ndarray):
             row_ptr = np.ascontiguousarray(row_ptr, np.uint32)
@@ -159,7 +160,8 @@ class Graph:
         flags = ((GRAPH_SYMMETRIC if symmetric else 0)
                  | (GRAPH_INPUT_TRANSPOSE if input_transpose else 0)
                  | (GRAPH_BUILD_OTHER if build_other and not symmetric else 0)
-                 | (0 if validate else GRAPH_NO_VALIDATE))
+                 | (0 if validate else GRAPH_NO_VALIDATE)
+                 | (GRAPH_RELABEL if relabel else 0))
         out = C.c_void_p()
         check(lib().g1_graph_create(_ptr(row_ptr), _ptr(col) if m else None,
                                     _ptr(val) if m else None, vtype, n, m, flags,
@@ -167,10 +169,10 @@ class Graph:
         return cls(out.value, n, m)
 
     @classmethod
-    def from_gen(cls, g, *, stream=None) -> "Graph":
+    def from_gen(cls, g, *, relabel=False, stream=None) -> "Graph":
         """From a graphone_b200.gen.CsrGraph (out-edge CSR; transpose built on the GPU)."""
         rp, ci, v = g.np("n")
-        return cls.from_csr(rp, ci, v, symmetric=g.symmetric, stream=stream)
+        return cls.from_csr(rp, ci, v, symmetric=g.symmetric, relabel=relabel, stream=stream)
 
     def close(self):
         if self._h:

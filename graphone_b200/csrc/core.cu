@@ -154,9 +154,12 @@ __global__ void max_degree_kernel(const uint32_t* rp, uint32_t n, uint32_t* max_
     atomicMax(max_deg, mx);
 }
 
-// key = (col << 32) | row for every nonzero; row found by binary search.
-__global__ void transpose_keys_kernel(const uint32_t* rp, const uint32_t* col, uint32_t n,
-                                      uint32_t m, uint64_t* keys, uint32_t* idx) {
+// Sort keys of a CSR rebuild: for every nonzero (row, col) the new
+// (row', col') = swap ? (map(col), map(row)) : (map(row), map(col)) packed
+// as (row' << 32) | col'; row found by binary search; map may be null.
+__global__ void rebuild_keys_kernel(const uint32_t* rp, const uint32_t* col, uint32_t n,
+                                    uint32_t m, const uint32_t* map, int swap, uint64_t* keys,
+                                    uint32_t* idx) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += stride) {
         uint32_t lo = 0, hi = n;  // last row r with rp[r] <= k
@@ -164,9 +167,55 @@ __global__ void transpose_keys_kernel(const uint32_t* rp, const uint32_t* col, u
             const uint32_t mid = (lo + hi + 1) >> 1;
             if (rp[mid] <= k) lo = mid; else hi = mid - 1;
         }
-        keys[k] = ((uint64_t)col[k] << 32) | lo;
+        uint32_t r = lo, c = col[k];
+        if (map) {
+            r = map[r];
+            c = map[c];
+        }
+        keys[k] = swap ? (((uint64_t)c << 32) | r) : (((uint64_t)r << 32) | c);
         idx[k] = (uint32_t)k;
     }
+}
+
+__global__ void degree_kernel(const uint32_t* rp, uint32_t n, uint32_t* deg) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        deg[v] = rp[v + 1] - rp[v];
+}
+
+__global__ void histogram_kernel(const uint32_t* col, uint32_t m, uint32_t* deg) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += stride)
+        atomicAdd(&deg[col[k]], 1u);
+}
+
+__global__ void iota_kernel(uint32_t* p, uint32_t n) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        p[v] = (uint32_t)v;
+}
+
+// perm[iperm[k]] = k
+__global__ void invert_perm_kernel(const uint32_t* iperm, uint32_t n, uint32_t* perm) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride)
+        perm[iperm[k]] = (uint32_t)k;
+}
+
+// out[v] = in[perm[v]]: internal (relabelled) order -> caller's order
+__global__ void gather_perm_kernel(uint32_t* out, const uint32_t* in, const uint32_t* perm,
+                                   uint32_t n) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        out[v] = in[perm[v]];
+}
+
+// out[perm[v]] = in[v]: caller's order -> internal order
+__global__ void scatter_perm_kernel(uint32_t* out, const uint32_t* in, const uint32_t* perm,
+                                    uint32_t n) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        out[perm[v]] = in[v];
 }
 
 __global__ void transpose_scatter_kernel(const uint64_t* keys, const uint32_t* idx,
@@ -215,10 +264,12 @@ g1_status upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     return G1_OK;
 }
 
-// Builds `dst` = transpose of `src` on the device (stable: rows of the
-// result list their columns in increasing order, like EdgeCache::ToCsr on a
-// sorted edge cache).
-g1_status build_transpose(g1_graph* g, const Orientation& src, Orientation& dst, cudaStream_t s) {
+// Builds `dst` from `src` on the device: the transpose when `swap`, with
+// vertex ids renamed through `map` when given.  Stable: rows of the result
+// list their columns in increasing order (like EdgeCache::ToCsr on a sorted
+// edge cache).
+g1_status rebuild_csr(g1_graph* g, const Orientation& src, Orientation& dst, bool swap,
+                      const uint32_t* map, cudaStream_t s) {
     const uint32_t n = g->n, m = g->m;
     G1_TRY(alloc_orientation(dst, n, m));
     G1_CUDA(cudaMemsetAsync(dst.rp, 0, ((size_t)n + 1) * 4, s));
@@ -231,8 +282,8 @@ g1_status build_transpose(g1_graph* g, const Orientation& src, Orientation& dst,
     G1_TRY(counts.ensure(((size_t)n + 1) * 4));
     G1_CUDA(cudaMemsetAsync(counts.p, 0, ((size_t)n + 1) * 4, s));
     const uint32_t grid = grid_for(m, 256, g->sm_count);
-    transpose_keys_kernel<<<grid, 256, 0, s>>>(src.rp, src.col, n, m, keys.as<uint64_t>(),
-                                               idx.as<uint32_t>());
+    rebuild_keys_kernel<<<grid, 256, 0, s>>>(src.rp, src.col, n, m, map, swap ? 1 : 0,
+                                             keys.as<uint64_t>(), idx.as<uint32_t>());
     count_launches(2);
     G1_CUDA(cudaGetLastError());
     int row_bits = 1;
@@ -257,6 +308,76 @@ g1_status build_transpose(g1_graph* g, const Orientation& src, Orientation& dst,
     G1_TRY(temp2.ensure(tb2));
     G1_CUDA(cub::DeviceScan::ExclusiveSum(temp2.p, tb2, counts.as<uint32_t>(), dst.rp, (int)n + 1, s));
     G1_CUDA(cudaStreamSynchronize(s));  // temporaries die here
+    return G1_OK;
+}
+
+// Moves the arrays of `fresh` into `o` (old arrays are freed).
+void adopt(Orientation& o, Orientation& fresh) {
+    std::swap(o.b_rp.p, fresh.b_rp.p);
+    std::swap(o.b_rp.bytes, fresh.b_rp.bytes);
+    std::swap(o.b_col.p, fresh.b_col.p);
+    std::swap(o.b_col.bytes, fresh.b_col.bytes);
+    std::swap(o.b_val.p, fresh.b_val.p);
+    std::swap(o.b_val.bytes, fresh.b_val.bytes);
+    o.rp = o.b_rp.as<uint32_t>();
+    o.col = o.b_col.as<uint32_t>();
+    o.val = o.b_val.p;
+    o.present = true;
+    o.plans.clear();
+}
+
+// Degree-ordered relabelling: internal id k is the k-th vertex by
+// decreasing out-degree (ties by id).  The hottest x entries of the pull
+// SpMV become a contiguous prefix that the warp-tile kernel caches in
+// shared memory.
+g1_status relabel_by_degree(g1_graph* g, cudaStream_t s) {
+    const uint32_t n = g->n;
+    DevBuf deg, deg2, ids, temp;
+    G1_TRY(deg.ensure((size_t)n * 4 + 16));
+    G1_TRY(deg2.ensure((size_t)n * 4 + 16));
+    G1_TRY(ids.ensure((size_t)n * 4 + 16));
+    G1_TRY(g->iperm.ensure((size_t)n * 4 + 16));
+    G1_TRY(g->perm.ensure((size_t)n * 4 + 16));
+    const uint32_t grid = grid_for(std::max(n, g->m), 256, g->sm_count);
+    if (g->o[0].present) {
+        degree_kernel<<<grid, 256, 0, s>>>(g->o[0].rp, n, deg.as<uint32_t>());
+    } else {
+        G1_CUDA(cudaMemsetAsync(deg.p, 0, (size_t)n * 4, s));
+        histogram_kernel<<<grid, 256, 0, s>>>(g->o[1].col, g->m, deg.as<uint32_t>());
+    }
+    iota_kernel<<<grid, 256, 0, s>>>(ids.as<uint32_t>(), n);
+    count_launches(2);
+    G1_CUDA(cudaGetLastError());
+    size_t tb = 0;
+    G1_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, deg.as<uint32_t>(),
+                                                      deg2.as<uint32_t>(), ids.as<uint32_t>(),
+                                                      g->iperm.as<uint32_t>(), (int)n, 0, 32, s));
+    G1_TRY(temp.ensure(tb));
+    G1_CUDA(cub::DeviceRadixSort::SortPairsDescending(temp.p, tb, deg.as<uint32_t>(),
+                                                      deg2.as<uint32_t>(), ids.as<uint32_t>(),
+                                                      g->iperm.as<uint32_t>(), (int)n, 0, 32, s));
+    invert_perm_kernel<<<grid, 256, 0, s>>>(g->iperm.as<uint32_t>(), n, g->perm.as<uint32_t>());
+    count_launches(1);
+    G1_CUDA(cudaGetLastError());
+    const uint32_t* map = g->perm.as<uint32_t>();
+    for (int t = 0; t < 2; ++t) {
+        Orientation& o = g->o[t];
+        if (!o.present || !o.b_rp.p) continue;  // shared arrays are renamed once
+        Orientation fresh;
+        G1_TRY(rebuild_csr(g, o, fresh, false, map, s));
+        adopt(o, fresh);
+    }
+    if (g->symmetric) {
+        const int own = g->o[0].b_rp.p ? 0 : 1;
+        Orientation& o = g->o[own];
+        Orientation& other = g->o[own ^ 1];
+        other.rp = o.rp;
+        other.col = o.col;
+        other.val = o.val;
+        other.plans.clear();
+    }
+    g->relabeled = true;
+    G1_CUDA(cudaStreamSynchronize(s));
     return G1_OK;
 }
 
@@ -289,6 +410,42 @@ g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out) {
     *out = p.get();
     owner.plans[items] = std::move(p);
     return G1_OK;
+}
+
+g1_status to_caller_order(g1_graph* g, uint32_t* dev_out, const uint32_t* internal,
+                          cudaStream_t s) {
+    gather_perm_kernel<<<grid_for(g->n, 256, g->sm_count), 256, 0, s>>>(
+        dev_out, internal, g->perm.as<uint32_t>(), g->n);
+    count_launches(1);
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
+}
+
+g1_status to_internal_order(g1_graph* g, uint32_t* dev_out, const uint32_t* caller,
+                            cudaStream_t s) {
+    scatter_perm_kernel<<<grid_for(g->n, 256, g->sm_count), 256, 0, s>>>(
+        dev_out, caller, g->perm.as<uint32_t>(), g->n);
+    count_launches(1);
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
+}
+
+g1_status internal_vertex(g1_graph* g, uint32_t v, uint32_t* out, cudaStream_t s) {
+    if (!g->relabeled) {
+        *out = v;
+        return G1_OK;
+    }
+    G1_CUDA(cudaMemcpyAsync(out, g->perm.as<uint32_t>() + v, 4, cudaMemcpyDeviceToHost, s));
+    G1_CUDA(cudaStreamSynchronize(s));
+    return G1_OK;
+}
+
+g1_status copy_out_vertices(g1_graph* g, void* dst, const void* internal, cudaStream_t s) {
+    if (!g->relabeled) return copy_out(dst, internal, (size_t)g->n * 4, s);
+    uint32_t* tmp = nullptr;
+    G1_TRY(g->ws.get("perm_out", g->n, &tmp));
+    G1_TRY(to_caller_order(g, tmp, static_cast<const uint32_t*>(internal), s));
+    return copy_out(dst, tmp, (size_t)g->n * 4, s);
 }
 
 g1_status check_device_error(g1_graph* g, cudaStream_t s) {
@@ -454,7 +611,7 @@ g1_status g1_graph_create(const uint32_t* row_ptr, const uint32_t* col, const vo
         other.val = o.val;
         other.max_deg = o.max_deg;
     } else if (flags & G1_GRAPH_BUILD_OTHER) {
-        G1_TRY(build_transpose(g.get(), o, other, s));
+        G1_TRY(rebuild_csr(g.get(), o, other, true, nullptr, s));
         G1_CUDA(cudaMemsetAsync(chk.p, 0, 16, s));
         max_degree_kernel<<<grid, 256, 0, s>>>(other.rp, n, d_maxdeg);
         count_launches(1);
@@ -462,6 +619,7 @@ g1_status g1_graph_create(const uint32_t* row_ptr, const uint32_t* col, const vo
         G1_CUDA(cudaStreamSynchronize(s));
         other.max_deg = h[1];
     }
+    if (flags & G1_GRAPH_RELABEL) G1_TRY(relabel_by_degree(g.get(), s));
     *out = g.release();
     return G1_OK;
 }
@@ -537,6 +695,23 @@ g1_status g1_spmv(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
     if (sr != G1_SR_BFS_U32 && fval != (g->vtype == G1_F32))
         return fail(G1_ERR_INVALID, "g1_spmv: semiring value type does not match the graph");
     cudaStream_t s = as_stream(stream);
+    if (g->relabeled) {
+        // x and y are in the caller's vertex order
+        uint32_t *xi = nullptr, *yi = nullptr;
+        G1_TRY(g->ws.get("spmv_xi", g->n, &xi));
+        G1_TRY(g->ws.get("spmv_yi", g->n, &yi));
+        G1_TRY(to_internal_order(g, xi, static_cast<const uint32_t*>(x), s));
+        G1_TRY(spmv_dispatch(g, transpose, sr, sched, xi, yi, s));
+        return to_caller_order(g, static_cast<uint32_t*>(y), yi, s);
+    }
+    return spmv_dispatch(g, transpose, sr, sched, x, y, s);
+}
+
+}  // extern "C"
+
+namespace g1 {
+g1_status spmv_dispatch(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
+                        const void* x, void* y, cudaStream_t s) {
     switch (sr) {
         case G1_SR_MINPLUS_U32:
             return run_spmv<MinPlusU32>(g, transpose, sched, static_cast<const uint32_t*>(x),
@@ -553,6 +728,9 @@ g1_status g1_spmv(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
     }
     return fail(G1_ERR_INVALID, "g1_spmv: unknown semiring");
 }
+}  // namespace g1
+
+extern "C" {
 
 g1_status g1_graph_set_schedule(g1_graph* g, int transpose, g1_schedule sched, int variant) {
     if (!g || transpose < 0 || transpose > 1) return fail(G1_ERR_INVALID, "g1_graph_set_schedule");

@@ -112,6 +112,10 @@ struct g1_graph {
     // Per-vertex sum of out-edge weights (PageRank's iweights denominator),
     // derived once per graph like the merge-path plans.
     bool outw_ready = false;
+    // Degree-ordered relabelling (G1_GRAPH_RELABEL): perm maps a caller's
+    // vertex id to the internal id, iperm the reverse.
+    bool relabeled = false;
+    g1::DevBuf perm, iperm;
     // Device error word written by kernels (bounded waits that ran out).
     g1::DevBuf err_buf;
     uint32_t* err_word = nullptr;
@@ -138,6 +142,14 @@ bool is_device_ptr(const void* p);
 g1_status copy_out(void* dst, const void* dev_src, size_t bytes, cudaStream_t s);
 
 g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out);
+// Vertex-order conversions of a relabelled graph (4-byte values).
+g1_status to_caller_order(g1_graph* g, uint32_t* dev_out, const uint32_t* internal, cudaStream_t s);
+g1_status to_internal_order(g1_graph* g, uint32_t* dev_out, const uint32_t* caller, cudaStream_t s);
+g1_status internal_vertex(g1_graph* g, uint32_t v, uint32_t* out, cudaStream_t s);
+// copy_out of an n-vector of 4-byte values in internal order to the caller.
+g1_status copy_out_vertices(g1_graph* g, void* dst, const void* internal, cudaStream_t s);
+g1_status spmv_dispatch(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
+                        const void* x, void* y, cudaStream_t s);
 // Reads and clears the graph's device error word (synchronises `s`).
 g1_status check_device_error(g1_graph* g, cudaStream_t s);
 

@@ -242,6 +242,6 @@ extern "C" g1_status g1_pagerank(g1_graph* g, float alpha, int iters, g1_pr_mode
     G1_TRY(pr_setup(g, alpha, b, grids, s));
     for (int it = 0; it < iters; ++it)
         G1_TRY(pr_iterate(g, b, grids, alpha, mode, it & 1, G1_SCHED_AUTO, s));
-    G1_TRY(copy_out(rank_out, b.rank[iters & 1], (size_t)g->n * 4, s));
+    G1_TRY(copy_out_vertices(g, rank_out, b.rank[iters & 1], s));
     return check_device_error(g, s);
 }

@@ -19,12 +19,14 @@ struct MergeVariant {
     int warp_tiles;
     int ipt;
     int stages;  // block tiles: staging buffers; warp tiles: min resident blocks per SM
+    int warps;   // warp tiles: warps per block
+    int hot;     // warp tiles: x entries cached in shared memory
 };
-constexpr MergeVariant kMergeVariants[] = {{1, 11, 3}, {1, 7, 4}, {1, 7, 6},
-                                           {0, 7, 2}, {0, 7, 1}, {1, 15, 2}};
+constexpr MergeVariant kMergeVariants[] = {
+    {1, 11, 3, 8, 0},  {1, 7, 4, 8, 0},  {1, 7, 1, 32, 16384}, {0, 7, 2, 8, 0},
+    {0, 7, 1, 8, 0},   {1, 7, 1, 32, 32768}};
 constexpr int kNumMergeVariants = 6;
 constexpr int kDefaultVariant = 0;
-constexpr int kWarpsPerBlock = 8;
 
 template <class K>
 int blocks_per_sm(K kernel, int block, size_t smem) {
@@ -63,15 +65,19 @@ inline uint32_t merge_items(int variant) {
     return (kMergeVariants[variant].warp_tiles ? 32 : kMergeBlock) * kMergeVariants[variant].ipt;
 }
 
-template <class SR, class Epi, int IPT, int MINB>
+template <class SR, class Epi, int WARPS, int IPT, int MINB, int HOT>
 struct WarpMergeKernel {
+    using L = WarpMergeLayout<SR, WARPS, IPT, HOT>;
     static int occupancy() {
-        static int occ = blocks_per_sm(spmv_wmerge_kernel<SR, Epi, kWarpsPerBlock, IPT, MINB>,
-                                       kWarpsPerBlock * 32, 0);
+        static int occ = [] {
+            auto k = spmv_wmerge_kernel<SR, Epi, WARPS, IPT, MINB, HOT>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
+            return blocks_per_sm(k, WARPS * 32, L::BYTES);
+        }();
         return occ;
     }
     static uint32_t grid(const g1_graph* g, uint32_t n_tiles) {
-        const uint64_t want = ceil_div(n_tiles, kWarpsPerBlock);
+        const uint64_t want = ceil_div(n_tiles, WARPS);
         return (uint32_t)std::max<uint64_t>(
             1, std::min<uint64_t>(want, (uint64_t)g->sm_count * occupancy()));
     }
@@ -130,12 +136,12 @@ g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_gri
     MergePlan* p = nullptr;
     G1_TRY(ensure_plan(g, t, merge_items(v), &p));
     switch (v) {
-        case 1: *main_grid = WarpMergeKernel<SR, Epi, 7, 4>::grid(g, p->n_tiles); break;
-        case 2: *main_grid = WarpMergeKernel<SR, Epi, 7, 6>::grid(g, p->n_tiles); break;
+        case 1: *main_grid = WarpMergeKernel<SR, Epi, 8, 7, 4, 0>::grid(g, p->n_tiles); break;
+        case 2: *main_grid = WarpMergeKernel<SR, Epi, 32, 7, 1, 16384>::grid(g, p->n_tiles); break;
         case 3: *main_grid = MergeKernel<SR, Epi, 7, 2>::grid(g, p->n_tiles); break;
         case 4: *main_grid = MergeKernel<SR, Epi, 7, 1>::grid(g, p->n_tiles); break;
-        case 5: *main_grid = WarpMergeKernel<SR, Epi, 15, 2>::grid(g, p->n_tiles); break;
-        default: *main_grid = WarpMergeKernel<SR, Epi, 11, 3>::grid(g, p->n_tiles); break;
+        case 5: *main_grid = WarpMergeKernel<SR, Epi, 32, 7, 1, 32768>::grid(g, p->n_tiles); break;
+        default: *main_grid = WarpMergeKernel<SR, Epi, 8, 11, 3, 0>::grid(g, p->n_tiles); break;
     }
     *fix_grid = (uint32_t)std::max<uint64_t>(1, ceil_div(p->n_tiles, kMergeBlock));
     return G1_OK;
@@ -159,15 +165,15 @@ g1_status launch_merge_v(g1_graph* g, int t, const MergePlan& p, const typename 
     return G1_OK;
 }
 
-template <class SR, class Epi, int IPT, int MINB>
+template <class SR, class Epi, int WARPS, int IPT, int MINB, int HOT>
 g1_status launch_wmerge(g1_graph* g, int t, const MergePlan& p, const typename SR::x_t* x,
                         const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
-    using K = WarpMergeKernel<SR, Epi, IPT, MINB>;
+    using K = WarpMergeKernel<SR, Epi, WARPS, IPT, MINB, HOT>;
     const MergeArgs<SR> a = merge_args<SR>(g, t, p, x);
     const bool prof = profiling();
     if (prof) prof_mark(s, true);
-    spmv_wmerge_kernel<SR, Epi, kWarpsPerBlock, IPT, MINB>
-        <<<K::grid(g, p.n_tiles), kWarpsPerBlock * 32, 0, s>>>(a, main_epi);
+    spmv_wmerge_kernel<SR, Epi, WARPS, IPT, MINB, HOT>
+        <<<K::grid(g, p.n_tiles), WARPS * 32, K::L::BYTES, s>>>(a, main_epi);
     if (prof) prof_mark(s, false);
     count_launches(2);
     spmv_fixup_kernel<SR, Epi, kMergeBlock>
@@ -186,12 +192,12 @@ g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi&
     G1_TRY(ensure_plan(g, t, merge_items(v), &p));
     if (p->n_tiles == 0) return G1_OK;
     switch (v) {
-        case 1: return launch_wmerge<SR, Epi, 7, 4>(g, t, *p, x, main_epi, fix_epi, s);
-        case 2: return launch_wmerge<SR, Epi, 7, 6>(g, t, *p, x, main_epi, fix_epi, s);
+        case 1: return launch_wmerge<SR, Epi, 8, 7, 4, 0>(g, t, *p, x, main_epi, fix_epi, s);
+        case 2: return launch_wmerge<SR, Epi, 32, 7, 1, 16384>(g, t, *p, x, main_epi, fix_epi, s);
         case 3: return launch_merge_v<SR, Epi, 7, 2>(g, t, *p, x, main_epi, fix_epi, s);
         case 4: return launch_merge_v<SR, Epi, 7, 1>(g, t, *p, x, main_epi, fix_epi, s);
-        case 5: return launch_wmerge<SR, Epi, 15, 2>(g, t, *p, x, main_epi, fix_epi, s);
-        default: return launch_wmerge<SR, Epi, 11, 3>(g, t, *p, x, main_epi, fix_epi, s);
+        case 5: return launch_wmerge<SR, Epi, 32, 7, 1, 32768>(g, t, *p, x, main_epi, fix_epi, s);
+        default: return launch_wmerge<SR, Epi, 8, 11, 3, 0>(g, t, *p, x, main_epi, fix_epi, s);
     }
 }
 

@@ -133,10 +133,12 @@ struct TrState {
 };
 
 template <bool UNIT>
-static g1_status traverse(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* out,
+static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, uint32_t* out,
                           uint32_t* iters_out, cudaStream_t s) {
     const uint32_t n = g->n;
-    if (src >= n) return fail(G1_ERR_INVALID, "source vertex out of range");
+    if (src_caller >= n) return fail(G1_ERR_INVALID, "source vertex out of range");
+    uint32_t src = src_caller;
+    G1_TRY(internal_vertex(g, src_caller, &src, s));
     if ((engine == G1_ENGINE_BLAS || engine == G1_ENGINE_AUTO) && !g->o[1].present)
         return fail(G1_ERR_UNSUPPORTED, "pull engine needs the in-edge CSR (G1_GRAPH_BUILD_OTHER)");
     if ((engine == G1_ENGINE_ADVANCE || engine == G1_ENGINE_AUTO) && !g->o[0].present)
@@ -207,7 +209,7 @@ static g1_status traverse(g1_graph* g, uint32_t src, g1_engine engine, uint32_t*
         if (nF > n) return fail(G1_ERR_OVERFLOW, "frontier larger than the vertex count");
     }
     if (iters_out) *iters_out = it;
-    G1_TRY(copy_out(out, st.dist, (size_t)n * 4, s));
+    G1_TRY(copy_out_vertices(g, out, st.dist, s));
     return check_device_error(g, s);
 }
 

@@ -438,20 +438,48 @@ __device__ __forceinline__ void warp_seg_scan_rows(bool head, RowPartial<typenam
 // l folds items [l*IPT, (l+1)*IPT) (odd IPT: bank-conflict free), a warp
 // (row, value) segmented scan carries open segments across lanes, and rows
 // that cross tiles are finished by spmv_fixup_kernel.
-template <class SR, class Epi, int WARPS, int IPT, int MINB>
+// Shared memory of the warp-tile kernel: an optional cache of x[0, HOT)
+// (the hottest vertices when the graph is degree-ordered) and each warp's
+// combined values, row-start marks and completed-row values.
+template <class SR, int WARPS, int IPT, int HOT>
+struct WarpMergeLayout {
+    using V = typename SR::value_t;
+    using X = typename SR::x_t;
+    static constexpr int WITEMS = 32 * IPT;
+    static constexpr size_t XC_OFF = 0;
+    static constexpr size_t XC_BYTES = ((size_t)HOT * sizeof(X) + 15) / 16 * 16;
+    static constexpr size_t V_OFF = XC_OFF + XC_BYTES;
+    static constexpr size_t V_BYTES = ((size_t)WARPS * WITEMS * sizeof(V) + 15) / 16 * 16;
+    static constexpr size_t ROW_OFF = V_OFF + V_BYTES;
+    static constexpr size_t ROW_BYTES = (size_t)WARPS * WITEMS * 4;
+    static constexpr size_t Y_OFF = ROW_OFF + ROW_BYTES;
+    static constexpr size_t Y_BYTES = V_BYTES;
+    static constexpr size_t EPI_OFF = Y_OFF + Y_BYTES;
+    static constexpr size_t BYTES = EPI_OFF + 512;
+};
+
+template <class SR, class Epi, int WARPS, int IPT, int MINB, int HOT>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
 spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
+    using X = typename SR::x_t;
     using P = RowPartial<V>;
-    constexpr int WITEMS = 32 * IPT;
-    __shared__ V s_v[WARPS][WITEMS];
-    __shared__ uint32_t s_row[WARPS][WITEMS];
-    __shared__ alignas(16) char epi_smem[64 * 8];
+    using L = WarpMergeLayout<SR, WARPS, IPT, HOT>;
+    constexpr int WITEMS = L::WITEMS;
+    extern __shared__ __align__(16) unsigned char dsm[];
     const uint32_t lane = lane_id();
     const uint32_t w = threadIdx.x >> 5;
-    V* sv = s_v[w];
-    uint32_t* srow = s_row[w];
+    X* xc = reinterpret_cast<X*>(dsm + L::XC_OFF);
+    V* sv = reinterpret_cast<V*>(dsm + L::V_OFF) + (size_t)w * WITEMS;
+    uint32_t* srow = reinterpret_cast<uint32_t*>(dsm + L::ROW_OFF) + (size_t)w * WITEMS;
+    V* sy = reinterpret_cast<V*>(dsm + L::Y_OFF) + (size_t)w * WITEMS;
     epi.begin();
+    // x[0, HOT) is read once per CTA and served from shared memory.
+    const uint32_t hot = HOT < a.plan.n_rows ? (uint32_t)HOT : a.plan.n_rows;
+    if constexpr (HOT > 0) {
+        for (uint32_t i = threadIdx.x; i < hot; i += WARPS * 32) xc[i] = ldg_any(a.x + i);
+        __syncthreads();
+    }
     const uint32_t total_warps = gridDim.x * WARPS;
     uint32_t tile = blockIdx.x * WARPS + w;
     // tile coordinates are fetched one tile ahead
@@ -490,11 +518,16 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
             ra = __ldg(a.plan.row_ptr + r_lane);
             rb = __ldg(a.plan.row_ptr + r_lane + 1);
         }
-        typename SR::x_t xv[IPT];
+        X xv[IPT];
 #pragma unroll
         for (int u = 0; u < IPT; ++u) {
             const uint32_t k = (uint32_t)u * 32 + lane;
-            if (k < nb) xv[u] = ldg_any(a.x + cv[u]);
+            if (k < nb) {
+                if constexpr (HOT > 0)
+                    xv[u] = cv[u] < hot ? xc[cv[u]] : ldg_any(a.x + cv[u]);
+                else
+                    xv[u] = ldg_any(a.x + cv[u]);
+            }
         }
         const bool spanning = j0 > __shfl_sync(0xffffffffu, ra, 0);
 #pragma unroll
@@ -506,7 +539,7 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
             }
         }
         __syncwarp();
-        // Rows i0..i1 of the tile: empty rows emit identity, starts are marked.
+        // Rows i0..i1 of the tile: empty rows get identity, starts are marked.
         for (uint32_t r = r_lane; r <= i1; r += 32) {
             uint32_t rs = ra, re = rb;
             if (r != r_lane) {
@@ -519,7 +552,7 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
             }
             if (r < i1) {
                 if (re == rs)
-                    epi.emit(r, SR::identity());  // empty row
+                    sy[r - i0] = SR::identity();  // empty row
                 else
                     srow[rs - j0] = r;
             } else if (rs < j1) {
@@ -528,6 +561,7 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
         }
         __syncwarp();
 
+        // Fold IPT consecutive nonzeros; a closed segment is a finished row.
         const uint32_t k0 = lane * (uint32_t)IPT;
         V acc = SR::identity();
         bool head = false;
@@ -546,7 +580,7 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
                         first_val = acc;
                         lead = (uint32_t)u;
                     } else {
-                        epi.emit(open_row, acc);
+                        sy[open_row - i0] = acc;
                     }
                     open_row = mark;
                     acc = SR::identity();
@@ -564,7 +598,7 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
             if (excl.row == kU32Max) {
                 if (spanning) a.tail[tile] = val;
             } else {
-                epi.emit(excl.row, val);
+                sy[excl.row - i0] = val;
             }
         }
         if (lane == 31) {
@@ -576,7 +610,7 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
                     if (lr == i0 && spanning)
                         a.tail[tile] = incl.val;
                     else
-                        epi.emit(lr, incl.val);
+                        sy[lr - i0] = incl.val;
                 } else {
                     carry = incl.val;
                 }
@@ -584,8 +618,11 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
             if (tile + 1 < a.plan.n_tiles) a.carry[tile] = carry;
         }
         __syncwarp();
+        // Coalesced epilogue over the rows completed in this tile.
+        for (uint32_t r = i0 + (spanning ? 1u : 0u) + lane; r < i1; r += 32) epi.emit(r, sy[r - i0]);
+        __syncwarp();
     }
-    epi.template block_end<WARPS * 32>(epi_smem);
+    epi.template block_end<WARPS * 32>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
 }
 
 // Finishes rows that cross tiles: for every tile T whose first row began in

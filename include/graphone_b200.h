@@ -67,6 +67,8 @@ typedef enum {
 #define G1_GRAPH_INPUT_TRANSPOSE 0x2u /* the arrays given are the in-edge CSR */
 #define G1_GRAPH_BUILD_OTHER 0x4u    /* also build the other orientation on the GPU */
 #define G1_GRAPH_NO_VALIDATE 0x8u    /* skip the device check of the CSR */
+#define G1_GRAPH_RELABEL 0x10u       /* store vertices in decreasing out-degree order
+                                        internally (results stay in caller order) */
 
 typedef struct g1_graph g1_graph;
 
@@ -133,9 +135,10 @@ g1_status g1_spmv(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
                   const void* x, void* y, void* stream);
 /* Fixes the schedule G1_SCHED_AUTO resolves to for one orientation:
  * G1_SCHED_MERGE with a merge kernel variant (warp tiles of 32 x items:
- * 0: 11 items/lane, 1: 7 at 4 blocks/SM, 2: 7 at 6 blocks/SM, 5: 15;
- * block tiles of 256 x 7 items staged by TMA bulk copies: 3: two staging
- * buffers, 4: one), or G1_SCHED_VECTOR;
+ * 0: 11 items/lane, 8 warps/block; 1: 7 items, 8 warps; 2: 7 items, one
+ * 32-warp block per SM caching x[0, 16384) in shared memory; 5: the same
+ * caching x[0, 32768); block tiles of 256 x 7 items staged by TMA bulk
+ * copies: 3: two staging buffers, 4: one), or G1_SCHED_VECTOR;
  * G1_SCHED_AUTO restores the heuristic.  No GraphOne counterpart (GraphOne hard-wires the
  * merge schedule, engine/blas_gc.h:130-132). */
 g1_status g1_graph_set_schedule(g1_graph* g, int transpose, g1_schedule sched, int variant);

@@ -88,3 +88,41 @@ def test_invalid_source(cuda):
     G = g1.Graph.from_gen(GRAPHS["grid32"])
     with pytest.raises(g1.G1Error):
         G.sssp(10**6)
+
+
+@pytest.mark.parametrize("name", ["rmat10_sym", "rmat11_dir", "star20k", "grid7x13", "single"])
+def test_relabelled_graph_results_in_caller_order(cuda, name):
+    """G1_GRAPH_RELABEL stores vertices by decreasing out-degree internally;
+    every result must still come back bit-exact in the caller's order."""
+    g = GRAPHS[name]
+    G = g1.Graph.from_gen(g, relabel=True)
+    rp, ci, v = g.np("n")
+    for e in ENGINES:
+        for s in sorted({0, g.n - 1}):
+            assert np.array_equal(G.sssp(s, e), O.dijkstra_u32(rp, ci, v, s)), (name, e, s)
+            assert np.array_equal(G.bfs(s, e), O.bfs(rp, ci, s)), (name, e, s)
+
+
+@pytest.mark.parametrize("variant", [0, 2, 5])
+def test_relabelled_pagerank(cuda, variant):
+    g = gen.rmat(14, 16, False, float_values=True)
+    trp, tci, tv = g.np("t")
+    rp, ci, v = g.np("n")
+    G = g1.Graph.from_csr(rp, ci, v, relabel=True)
+    G.set_schedule(g1.SCHED_MERGE, variant, transpose=1)
+    for mode in (g1.PR_REFERENCE, g1.PR_DANGLING):
+        r = G.pagerank(0.85, 30, mode)
+        assert O.rel_l1(r, O.pagerank_f64(trp, tci, tv, 0.85, 30, mode)) < 1e-6
+
+
+def test_relabelled_spmv_caller_order(cuda):
+    import torch
+    g = gen.rmat(12, 16, True, (1, 64))
+    G = g1.Graph.from_gen(g, relabel=True)
+    rp, ci, v = g.np("t")
+    x = np.full(g.n, O.U32_MAX, np.uint32)
+    x[::7] = np.arange(len(x[::7]), dtype=np.uint32)
+    xd = torch.from_numpy(x.view(np.int32)).cuda()
+    yd = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    G.spmv(xd, yd, g1.SR_MINPLUS_U32, transpose=1)
+    assert np.array_equal(yd.cpu().numpy().view(np.uint32), O.spmv_minplus_u32(rp, ci, v, x))
