@@ -245,11 +245,18 @@ uint32_t grid_for(uint64_t n, int block, int sm_count, int per_sm = 8) {
     return (uint32_t)std::max<uint64_t>(1, std::min(g, cap));
 }
 
-// Allocates an orientation's arrays (padded for vector / bulk loads).
+// Allocates an orientation's arrays.  The padding past row_ptr[n] and past
+// the last nonzero is zero-filled: bulk copies and warp tiles read whole
+// aligned ranges without bounds checks (a padding column 0 is a valid index).
 g1_status alloc_orientation(Orientation& o, uint32_t n, uint32_t m) {
-    G1_TRY(o.b_rp.ensure(((size_t)n + 1 + 64) * 4));
-    G1_TRY(o.b_col.ensure(((size_t)m + 64) * 4));
-    G1_TRY(o.b_val.ensure(((size_t)m + 64) * 4));
+    const size_t rp_bytes = ((size_t)n + 1 + 64) * 4;
+    const size_t nz_bytes = ((size_t)m + kWarpTilePad + 64) * 4;
+    G1_TRY(o.b_rp.ensure(rp_bytes));
+    G1_TRY(o.b_col.ensure(nz_bytes));
+    G1_TRY(o.b_val.ensure(nz_bytes));
+    G1_CUDA(cudaMemset(o.b_rp.p, 0, o.b_rp.bytes));
+    G1_CUDA(cudaMemset(o.b_col.p, 0, o.b_col.bytes));
+    G1_CUDA(cudaMemset(o.b_val.p, 0, o.b_val.bytes));
     o.rp = o.b_rp.as<uint32_t>();
     o.col = o.b_col.as<uint32_t>();
     o.val = o.b_val.p;

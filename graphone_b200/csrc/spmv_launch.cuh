@@ -11,22 +11,30 @@ namespace g1 {
 constexpr int kMergeBlock = 256;
 constexpr int kVectorBlock = 256;
 
-// Merge kernel variants the autotuner chooses from.  Warp tiles (one warp
-// per 32*ipt items, no block barrier) or block tiles (256*ipt items staged by
-// TMA bulk copies, `stages` buffers); ipt odd so that consecutive threads'
-// shared-memory reads fall in distinct banks.
+// Merge kernel variants the autotuner chooses from (all share the
+// merge-path partition; items per lane odd so that consecutive lanes'
+// shared-memory reads fall in distinct banks):
+//   kind 0: warp tiles of 32*ipt items loaded into registers,
+//   kind 1: block tiles of 256*ipt items staged by TMA bulk copies
+//           (`stages` staging buffers),
+//   kind 2: warp tiles staged by per-warp TMA bulk copies.
+// `warps` per block (kind 0/2), `hot` x entries cached in shared memory,
+// `minb` resident blocks per SM the register budget is sized for.
 struct MergeVariant {
-    int warp_tiles;
+    int kind;
     int ipt;
-    int stages;  // block tiles: staging buffers; warp tiles: min resident blocks per SM
-    int warps;   // warp tiles: warps per block
-    int hot;     // warp tiles: x entries cached in shared memory
+    int stages;
+    int warps;
+    int hot;
+    int minb;
 };
 constexpr MergeVariant kMergeVariants[] = {
-    {1, 11, 3, 8, 0},  {1, 7, 4, 8, 0},  {1, 7, 1, 32, 16384}, {0, 7, 2, 8, 0},
-    {0, 7, 1, 8, 0},   {1, 7, 1, 32, 32768}};
-constexpr int kNumMergeVariants = 6;
-constexpr int kDefaultVariant = 0;
+    {0, 11, 0, 8, 0, 3},      {0, 7, 0, 8, 0, 4},       {0, 7, 0, 32, 16384, 1},
+    {1, 7, 2, 8, 0, 4},       {1, 7, 1, 8, 0, 6},       {0, 11, 0, 32, 16384, 1},
+    {2, 15, 0, 24, 16384, 1}, {2, 31, 0, 16, 0, 1},     {2, 15, 0, 32, 0, 1},
+    {2, 23, 0, 16, 16384, 1}};
+constexpr int kNumMergeVariants = 10;
+constexpr int kDefaultVariant = 2;
 
 template <class K>
 int blocks_per_sm(K kernel, int block, size_t smem) {
@@ -62,8 +70,26 @@ inline int merge_variant(const g1_graph* g, int t) {
     return (v >= 0 && v < kNumMergeVariants) ? v : kDefaultVariant;
 }
 inline uint32_t merge_items(int variant) {
-    return (kMergeVariants[variant].warp_tiles ? 32 : kMergeBlock) * kMergeVariants[variant].ipt;
+    return (kMergeVariants[variant].kind == 1 ? kMergeBlock : 32) * kMergeVariants[variant].ipt;
 }
+
+template <class SR, class Epi, int WARPS, int IPT, int HOT>
+struct WarpTmaKernel {
+    using L = WarpTmaLayout<SR, WARPS, IPT, HOT>;
+    static int occupancy() {
+        static int occ = [] {
+            auto k = spmv_wtma_kernel<SR, Epi, WARPS, IPT, HOT>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
+            return blocks_per_sm(k, WARPS * 32, L::BYTES);
+        }();
+        return occ;
+    }
+    static uint32_t grid(const g1_graph* g, uint32_t n_tiles) {
+        const uint64_t want = ceil_div(n_tiles, WARPS);
+        return (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(want, (uint64_t)g->sm_count * occupancy()));
+    }
+};
 
 template <class SR, class Epi, int WARPS, int IPT, int MINB, int HOT>
 struct WarpMergeKernel {
@@ -140,7 +166,11 @@ g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_gri
         case 2: *main_grid = WarpMergeKernel<SR, Epi, 32, 7, 1, 16384>::grid(g, p->n_tiles); break;
         case 3: *main_grid = MergeKernel<SR, Epi, 7, 2>::grid(g, p->n_tiles); break;
         case 4: *main_grid = MergeKernel<SR, Epi, 7, 1>::grid(g, p->n_tiles); break;
-        case 5: *main_grid = WarpMergeKernel<SR, Epi, 32, 7, 1, 32768>::grid(g, p->n_tiles); break;
+        case 5: *main_grid = WarpMergeKernel<SR, Epi, 32, 11, 1, 16384>::grid(g, p->n_tiles); break;
+        case 6: *main_grid = WarpTmaKernel<SR, Epi, 24, 15, 16384>::grid(g, p->n_tiles); break;
+        case 7: *main_grid = WarpTmaKernel<SR, Epi, 16, 31, 0>::grid(g, p->n_tiles); break;
+        case 8: *main_grid = WarpTmaKernel<SR, Epi, 32, 15, 0>::grid(g, p->n_tiles); break;
+        case 9: *main_grid = WarpTmaKernel<SR, Epi, 16, 23, 16384>::grid(g, p->n_tiles); break;
         default: *main_grid = WarpMergeKernel<SR, Epi, 8, 11, 3, 0>::grid(g, p->n_tiles); break;
     }
     *fix_grid = (uint32_t)std::max<uint64_t>(1, ceil_div(p->n_tiles, kMergeBlock));
@@ -183,6 +213,24 @@ g1_status launch_wmerge(g1_graph* g, int t, const MergePlan& p, const typename S
     return G1_OK;
 }
 
+template <class SR, class Epi, int WARPS, int IPT, int HOT>
+g1_status launch_wtma(g1_graph* g, int t, const MergePlan& p, const typename SR::x_t* x,
+                      const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
+    using K = WarpTmaKernel<SR, Epi, WARPS, IPT, HOT>;
+    const MergeArgs<SR> a = merge_args<SR>(g, t, p, x);
+    const bool prof = profiling();
+    if (prof) prof_mark(s, true);
+    spmv_wtma_kernel<SR, Epi, WARPS, IPT, HOT>
+        <<<K::grid(g, p.n_tiles), WARPS * 32, K::L::BYTES, s>>>(a, main_epi);
+    if (prof) prof_mark(s, false);
+    count_launches(2);
+    spmv_fixup_kernel<SR, Epi, kMergeBlock>
+        <<<(uint32_t)std::max<uint64_t>(1, ceil_div(p.n_tiles, kMergeBlock)), kMergeBlock, 0, s>>>(
+            a, fix_epi);
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
+}
+
 // Merge schedule: main kernel + fixup, with distinct epilogue instances.
 template <class SR, class Epi>
 g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi& main_epi,
@@ -196,7 +244,11 @@ g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi&
         case 2: return launch_wmerge<SR, Epi, 32, 7, 1, 16384>(g, t, *p, x, main_epi, fix_epi, s);
         case 3: return launch_merge_v<SR, Epi, 7, 2>(g, t, *p, x, main_epi, fix_epi, s);
         case 4: return launch_merge_v<SR, Epi, 7, 1>(g, t, *p, x, main_epi, fix_epi, s);
-        case 5: return launch_wmerge<SR, Epi, 32, 7, 1, 32768>(g, t, *p, x, main_epi, fix_epi, s);
+        case 5: return launch_wmerge<SR, Epi, 32, 11, 1, 16384>(g, t, *p, x, main_epi, fix_epi, s);
+        case 6: return launch_wtma<SR, Epi, 24, 15, 16384>(g, t, *p, x, main_epi, fix_epi, s);
+        case 7: return launch_wtma<SR, Epi, 16, 31, 0>(g, t, *p, x, main_epi, fix_epi, s);
+        case 8: return launch_wtma<SR, Epi, 32, 15, 0>(g, t, *p, x, main_epi, fix_epi, s);
+        case 9: return launch_wtma<SR, Epi, 16, 23, 16384>(g, t, *p, x, main_epi, fix_epi, s);
         default: return launch_wmerge<SR, Epi, 8, 11, 3, 0>(g, t, *p, x, main_epi, fix_epi, s);
     }
 }

@@ -439,39 +439,51 @@ __device__ __forceinline__ void warp_seg_scan_rows(bool head, RowPartial<typenam
 // (row, value) segmented scan carries open segments across lanes, and rows
 // that cross tiles are finished by spmv_fixup_kernel.
 // Shared memory of the warp-tile kernel: an optional cache of x[0, HOT)
-// (the hottest vertices when the graph is degree-ordered) and each warp's
-// combined values, row-start marks and completed-row values.
+// (the hottest vertices when the graph is degree-ordered) and, per warp, the
+// (combined value, row-start mark) of each item and the value of each row
+// completed in the tile.
+template <class V>
+struct alignas(8) ItemSlot {
+    V val;
+    uint32_t mark;
+};
+
 template <class SR, int WARPS, int IPT, int HOT>
 struct WarpMergeLayout {
     using V = typename SR::value_t;
     using X = typename SR::x_t;
+    using S = ItemSlot<V>;
     static constexpr int WITEMS = 32 * IPT;
     static constexpr size_t XC_OFF = 0;
     static constexpr size_t XC_BYTES = ((size_t)HOT * sizeof(X) + 15) / 16 * 16;
-    static constexpr size_t V_OFF = XC_OFF + XC_BYTES;
-    static constexpr size_t V_BYTES = ((size_t)WARPS * WITEMS * sizeof(V) + 15) / 16 * 16;
-    static constexpr size_t ROW_OFF = V_OFF + V_BYTES;
-    static constexpr size_t ROW_BYTES = (size_t)WARPS * WITEMS * 4;
-    static constexpr size_t Y_OFF = ROW_OFF + ROW_BYTES;
-    static constexpr size_t Y_BYTES = V_BYTES;
+    static constexpr size_t S_OFF = XC_OFF + XC_BYTES;
+    static constexpr size_t S_BYTES = ((size_t)WARPS * WITEMS * sizeof(S) + 15) / 16 * 16;
+    static constexpr size_t Y_OFF = S_OFF + S_BYTES;
+    static constexpr size_t Y_BYTES = ((size_t)WARPS * WITEMS * sizeof(V) + 15) / 16 * 16;
     static constexpr size_t EPI_OFF = Y_OFF + Y_BYTES;
     static constexpr size_t BYTES = EPI_OFF + 512;
 };
+
+// Items each warp tile may read past its last nonzero (the col/val arrays
+// are padded with this many zero entries): loads need no bounds checks.
+constexpr uint32_t kWarpTilePad = 1024;
 
 template <class SR, class Epi, int WARPS, int IPT, int MINB, int HOT>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
 spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
     using X = typename SR::x_t;
+    using W = typename SR::w_t;
     using P = RowPartial<V>;
     using L = WarpMergeLayout<SR, WARPS, IPT, HOT>;
+    using S = ItemSlot<V>;
     constexpr int WITEMS = L::WITEMS;
+    static_assert(WITEMS <= (int)kWarpTilePad, "tile larger than the array padding");
     extern __shared__ __align__(16) unsigned char dsm[];
     const uint32_t lane = lane_id();
     const uint32_t w = threadIdx.x >> 5;
     X* xc = reinterpret_cast<X*>(dsm + L::XC_OFF);
-    V* sv = reinterpret_cast<V*>(dsm + L::V_OFF) + (size_t)w * WITEMS;
-    uint32_t* srow = reinterpret_cast<uint32_t*>(dsm + L::ROW_OFF) + (size_t)w * WITEMS;
+    S* slot = reinterpret_cast<S*>(dsm + L::S_OFF) + (size_t)w * WITEMS;
     V* sy = reinterpret_cast<V*>(dsm + L::Y_OFF) + (size_t)w * WITEMS;
     epi.begin();
     // x[0, HOT) is read once per CTA and served from shared memory.
@@ -500,17 +512,17 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
             c_j1 = a.plan.tile_nnz[nxt + 1];
         }
         const uint32_t nb = j1 - j0;
-        // All independent loads of the tile go out together: col and val of
-        // the nonzeros, and row_ptr of the tile's first 32 rows.
+        // items u*32 + lane exist for u < nv (col/val are loaded regardless:
+        // the arrays are padded, and padding columns are 0)
+        const uint32_t nv = nb > lane ? (nb - lane + 31) >> 5 : 0u;
+        const uint32_t* colp = a.col + j0 + lane;
+        const W* valp = a.val + j0 + lane;
         uint32_t cv[IPT];
-        typename SR::w_t wv[IPT];
+        W wv[IPT];
 #pragma unroll
         for (int u = 0; u < IPT; ++u) {
-            const uint32_t k = (uint32_t)u * 32 + lane;
-            if (k < nb) {
-                cv[u] = __ldg(a.col + j0 + k);
-                wv[u] = ldg_any(a.val + j0 + k);
-            }
+            cv[u] = __ldg(colp + u * 32);
+            wv[u] = ldg_any(valp + u * 32);
         }
         const uint32_t r_lane = i0 + lane;
         uint32_t ra = 0, rb = 0;
@@ -521,8 +533,7 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
         X xv[IPT];
 #pragma unroll
         for (int u = 0; u < IPT; ++u) {
-            const uint32_t k = (uint32_t)u * 32 + lane;
-            if (k < nb) {
+            if ((uint32_t)u < nv) {
                 if constexpr (HOT > 0)
                     xv[u] = cv[u] < hot ? xc[cv[u]] : ldg_any(a.x + cv[u]);
                 else
@@ -530,12 +541,14 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
             }
         }
         const bool spanning = j0 > __shfl_sync(0xffffffffu, ra, 0);
+        S* sl = slot + lane;
 #pragma unroll
         for (int u = 0; u < IPT; ++u) {
-            const uint32_t k = (uint32_t)u * 32 + lane;
-            if (k < nb) {
-                sv[k] = SR::combine(wv[u], xv[u]);
-                srow[k] = kU32Max;
+            if ((uint32_t)u < nv) {
+                S e;
+                e.val = SR::combine(wv[u], xv[u]);
+                e.mark = kU32Max;
+                sl[u * 32] = e;
             }
         }
         __syncwarp();
@@ -554,15 +567,17 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
                 if (re == rs)
                     sy[r - i0] = SR::identity();  // empty row
                 else
-                    srow[rs - j0] = r;
+                    slot[rs - j0].mark = r;
             } else if (rs < j1) {
-                srow[rs - j0] = r;  // row i1 starts here and continues
+                slot[rs - j0].mark = r;  // row i1 starts here and continues
             }
         }
         __syncwarp();
 
-        // Fold IPT consecutive nonzeros; a closed segment is a finished row.
+        // Fold IPT consecutive items; a closed segment is a finished row.
         const uint32_t k0 = lane * (uint32_t)IPT;
+        const uint32_t nk = nb > k0 ? min(nb - k0, (uint32_t)IPT) : 0u;
+        const S* sk = slot + k0;
         V acc = SR::identity();
         bool head = false;
         uint32_t open_row = kU32Max;
@@ -570,11 +585,9 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
         uint32_t lead = 0;
 #pragma unroll
         for (int u = 0; u < IPT; ++u) {
-            const uint32_t k = k0 + (uint32_t)u;
-            if (k < nb) {
-                const uint32_t mark = srow[k];
-                const V val = sv[k];
-                if (mark != kU32Max) {
+            if ((uint32_t)u < nk) {
+                const S e = sk[u];
+                if (e.mark != kU32Max) {
                     if (!head) {
                         head = true;
                         first_val = acc;
@@ -582,10 +595,10 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
                     } else {
                         sy[open_row - i0] = acc;
                     }
-                    open_row = mark;
+                    open_row = e.mark;
                     acc = SR::identity();
                 }
-                acc = SR::reduce(acc, val);
+                acc = SR::reduce(acc, e.val);
             }
         }
         P mine;
@@ -622,6 +635,236 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
         for (uint32_t r = i0 + (spanning ? 1u : 0u) + lane; r < i1; r += 32) epi.emit(r, sy[r - i0]);
         __syncwarp();
     }
+    epi.template block_end<WARPS * 32>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
+}
+
+// Per-warp shared memory of the bulk-staged warp-tile kernel: the tile's
+// col and val (4-byte values) land in `stage` by one bulk copy and the same
+// bytes are then reused as the tile's (value, mark) slots; `y` holds the
+// values of the rows completed in the tile.
+template <class SR, int IPT>
+struct WarpTmaSlice {
+    using V = typename SR::value_t;
+    static constexpr int WITEMS = 32 * IPT;
+    static constexpr size_t COL_OFF = 0;
+    static constexpr size_t VAL_OFF = ((size_t)(WITEMS + 8) * 4 + 15) / 16 * 16;
+    static constexpr size_t STAGE_BYTES = VAL_OFF + ((size_t)(WITEMS + 8) * 4 + 15) / 16 * 16;
+    static constexpr size_t SLOT_BYTES = (size_t)WITEMS * sizeof(ItemSlot<V>);
+    static constexpr size_t BUF_BYTES = STAGE_BYTES > SLOT_BYTES ? STAGE_BYTES : SLOT_BYTES;
+    static constexpr size_t Y_OFF = BUF_BYTES;
+    static constexpr size_t BAR_OFF = Y_OFF + ((size_t)WITEMS * sizeof(V) + 15) / 16 * 16;
+    static constexpr size_t BYTES = BAR_OFF + 16;
+};
+
+template <class SR, int WARPS, int IPT, int HOT>
+struct WarpTmaLayout {
+    using X = typename SR::x_t;
+    using S = WarpTmaSlice<SR, IPT>;
+    static constexpr size_t XC_BYTES = ((size_t)HOT * sizeof(X) + 15) / 16 * 16;
+    static constexpr size_t SLICE_OFF = XC_BYTES;
+    static constexpr size_t EPI_OFF = SLICE_OFF + (size_t)WARPS * S::BYTES;
+    static constexpr size_t BYTES = EPI_OFF + 512;
+};
+
+// One lane issues the bulk copies of a warp tile's col/val ranges widened to
+// 16-byte boundaries (the arrays are padded for that).
+template <class SR, int IPT>
+__device__ __forceinline__ void warp_tile_issue(const MergeArgs<SR>& a, uint32_t j0, uint32_t j1,
+                                                unsigned char* slice, uint64_t* bar) {
+    using S = WarpTmaSlice<SR, IPT>;
+    const uint32_t c_lo = j0 & ~3u, c_hi = (j1 + 3) & ~3u;
+    const uint32_t bytes = (c_hi - c_lo) * 4;
+    if (bytes == 0) {
+        mbar_arrive_expect_tx(bar, 0);
+        return;
+    }
+    mbar_arrive_expect_tx(bar, 2 * bytes);
+    bulk_g2s(slice + S::COL_OFF, a.col + c_lo, bytes, bar);
+    bulk_g2s(slice + S::VAL_OFF, a.val + c_lo, bytes, bar);
+}
+
+// Warp-tile merge SpMV with bulk-staged tiles: as spmv_wmerge_kernel, but the
+// tile's col/val arrive by a bulk copy into the warp's shared memory (no
+// registers tied up by in-flight loads), which allows tiles of 32*IPT items
+// with IPT up to 31 and so amortises the per-tile scan, row walk and
+// epilogue over many more items.  4-byte edge values only.
+template <class SR, class Epi, int WARPS, int IPT, int HOT>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+spmv_wtma_kernel(MergeArgs<SR> a, Epi epi) {
+    using V = typename SR::value_t;
+    using X = typename SR::x_t;
+    using W = typename SR::w_t;
+    using P = RowPartial<V>;
+    using L = WarpTmaLayout<SR, WARPS, IPT, HOT>;
+    using SL = WarpTmaSlice<SR, IPT>;
+    using S = ItemSlot<V>;
+    static_assert(sizeof(W) == 4, "bulk-staged tiles need 4-byte edge values");
+    
+    extern __shared__ __align__(16) unsigned char dsm[];
+    const uint32_t lane = lane_id();
+    const uint32_t w = threadIdx.x >> 5;
+    X* xc = reinterpret_cast<X*>(dsm);
+    unsigned char* slice = dsm + L::SLICE_OFF + (size_t)w * SL::BYTES;
+    S* slot = reinterpret_cast<S*>(slice);
+    V* sy = reinterpret_cast<V*>(slice + SL::Y_OFF);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(slice + SL::BAR_OFF);
+    epi.begin();
+    if (lane == 0) {
+        mbar_init(bar, 1);
+        fence_mbar_init();
+    }
+    const uint32_t hot = HOT < a.plan.n_rows ? (uint32_t)HOT : a.plan.n_rows;
+    if constexpr (HOT > 0)
+        for (uint32_t i = threadIdx.x; i < hot; i += WARPS * 32) xc[i] = ldg_any(a.x + i);
+    __syncthreads();
+
+    const uint32_t total_warps = gridDim.x * WARPS;
+    uint32_t tile = blockIdx.x * WARPS + w;
+    uint32_t c_i0 = 0, c_i1 = 0, c_j0 = 0, c_j1 = 0;
+    if (tile < a.plan.n_tiles) {
+        c_i0 = a.plan.tile_row[tile];
+        c_i1 = a.plan.tile_row[tile + 1];
+        c_j0 = a.plan.tile_nnz[tile];
+        c_j1 = a.plan.tile_nnz[tile + 1];
+        if (lane == 0) warp_tile_issue<SR, IPT>(a, c_j0, c_j1, slice, bar);
+    }
+    uint32_t phase = 0;
+    bool failed = false;
+    for (; tile < a.plan.n_tiles; tile += total_warps, phase ^= 1u) {
+        const uint32_t i0 = c_i0, i1 = c_i1, j0 = c_j0, j1 = c_j1;
+        const uint32_t nxt = tile + total_warps;
+        if (nxt < a.plan.n_tiles) {
+            c_i0 = a.plan.tile_row[nxt];
+            c_i1 = a.plan.tile_row[nxt + 1];
+            c_j0 = a.plan.tile_nnz[nxt];
+            c_j1 = a.plan.tile_nnz[nxt + 1];
+        }
+        const uint32_t nb = j1 - j0;
+        const uint32_t nv = nb > lane ? (nb - lane + 31) >> 5 : 0u;
+        const uint32_t r_lane = i0 + lane;
+        uint32_t ra = 0, rb = 0;
+        if (r_lane <= i1) {
+            ra = __ldg(a.plan.row_ptr + r_lane);
+            rb = __ldg(a.plan.row_ptr + r_lane + 1);
+        }
+        const bool arrived = mbar_wait_bounded(bar, phase);
+        if (!__all_sync(0xffffffffu, arrived)) {
+            if (lane == 0) set_error(a.err, kDevTimeout);
+            failed = true;
+            break;
+        }
+        const uint32_t* CO = reinterpret_cast<const uint32_t*>(slice + SL::COL_OFF) + (j0 & 3u);
+        const W* VA = reinterpret_cast<const W*>(slice + SL::VAL_OFF) + (j0 & 3u);
+        V vv[IPT];
+#pragma unroll
+        for (int u = 0; u < IPT; ++u) {
+            if ((uint32_t)u < nv) {
+                const uint32_t c = CO[u * 32 + lane];
+                X xval;
+                if constexpr (HOT > 0)
+                    xval = c < hot ? xc[c] : ldg_any(a.x + c);
+                else
+                    xval = ldg_any(a.x + c);
+                vv[u] = SR::combine(VA[u * 32 + lane], xval);
+            }
+        }
+        const bool spanning = j0 > __shfl_sync(0xffffffffu, ra, 0);
+        __syncwarp();  // every lane is done with the staged col/val
+#pragma unroll
+        for (int u = 0; u < IPT; ++u) {
+            if ((uint32_t)u < nv) {
+                S e;
+                e.val = vv[u];
+                e.mark = kU32Max;
+                slot[u * 32 + lane] = e;
+            }
+        }
+        __syncwarp();
+        for (uint32_t r = r_lane; r <= i1; r += 32) {
+            uint32_t rs = ra, re = rb;
+            if (r != r_lane) {
+                rs = __ldg(a.plan.row_ptr + r);
+                re = __ldg(a.plan.row_ptr + r + 1);
+            }
+            if (r == i0 && spanning) {
+                if (i1 > i0 && re == j0) a.tail[tile] = SR::identity();
+                continue;
+            }
+            if (r < i1) {
+                if (re == rs)
+                    sy[r - i0] = SR::identity();
+                else
+                    slot[rs - j0].mark = r;
+            } else if (rs < j1) {
+                slot[rs - j0].mark = r;
+            }
+        }
+        __syncwarp();
+
+        const uint32_t k0 = lane * (uint32_t)IPT;
+        const uint32_t nk = nb > k0 ? min(nb - k0, (uint32_t)IPT) : 0u;
+        const S* sk = slot + k0;
+        V acc = SR::identity();
+        bool head = false;
+        uint32_t open_row = kU32Max;
+        V first_val = acc;
+        uint32_t lead = 0;
+#pragma unroll
+        for (int u = 0; u < IPT; ++u) {
+            if ((uint32_t)u < nk) {
+                const S e = sk[u];
+                if (e.mark != kU32Max) {
+                    if (!head) {
+                        head = true;
+                        first_val = acc;
+                        lead = (uint32_t)u;
+                    } else {
+                        sy[open_row - i0] = acc;
+                    }
+                    open_row = e.mark;
+                    acc = SR::identity();
+                }
+                acc = SR::reduce(acc, e.val);
+            }
+        }
+        P mine;
+        mine.row = open_row;
+        mine.val = acc;
+        P incl, excl;
+        warp_seg_scan_rows<SR>(head, mine, incl, excl);
+        if (head && !(lane == 0 && lead == 0)) {
+            const V val = SR::reduce(excl.val, first_val);
+            if (excl.row == kU32Max) {
+                if (spanning) a.tail[tile] = val;
+            } else {
+                sy[excl.row - i0] = val;
+            }
+        }
+        if (lane == 31) {
+            uint32_t lr = incl.row;
+            if (lr == kU32Max && spanning) lr = i0;
+            V carry = SR::identity();
+            if (lr != kU32Max) {
+                if (lr < i1) {
+                    if (lr == i0 && spanning)
+                        a.tail[tile] = incl.val;
+                    else
+                        sy[lr - i0] = incl.val;
+                } else {
+                    carry = incl.val;
+                }
+            }
+            if (tile + 1 < a.plan.n_tiles) a.carry[tile] = carry;
+        }
+        __syncwarp();  // slots are dead: the next tile's bulk copy may land
+        if (lane == 0 && nxt < a.plan.n_tiles) {
+            fence_proxy_async_smem();
+            warp_tile_issue<SR, IPT>(a, c_j0, c_j1, slice, bar);
+        }
+        for (uint32_t r = i0 + (spanning ? 1u : 0u) + lane; r < i1; r += 32) epi.emit(r, sy[r - i0]);
+        __syncwarp();
+    }
+    (void)failed;
     epi.template block_end<WARPS * 32>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
 }
 

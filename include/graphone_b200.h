@@ -134,13 +134,16 @@ g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t* items_per_tile,
 g1_status g1_spmv(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
                   const void* x, void* y, void* stream);
 /* Fixes the schedule G1_SCHED_AUTO resolves to for one orientation:
- * G1_SCHED_MERGE with a merge kernel variant (warp tiles of 32 x items:
- * 0: 11 items/lane, 8 warps/block; 1: 7 items, 8 warps; 2: 7 items, one
- * 32-warp block per SM caching x[0, 16384) in shared memory; 5: the same
- * caching x[0, 32768); block tiles of 256 x 7 items staged by TMA bulk
- * copies: 3: two staging buffers, 4: one), or G1_SCHED_VECTOR;
- * G1_SCHED_AUTO restores the heuristic.  No GraphOne counterpart (GraphOne hard-wires the
- * merge schedule, engine/blas_gc.h:130-132). */
+ * G1_SCHED_MERGE with a merge kernel variant, or G1_SCHED_VECTOR;
+ * G1_SCHED_AUTO restores the default.  Merge variants (all on the
+ * merge-path partition): warp tiles of 32 x k items loaded into registers
+ * (0: k=11, 8 warps/block; 1: k=7, 8 warps; 2: k=7, 32 warps + x[0,16384)
+ * cached in shared memory; 5: k=11, 32 warps + cache), block tiles of
+ * 256 x 7 items staged by TMA bulk copies (3: two staging buffers, 4: one),
+ * warp tiles staged by per-warp TMA bulk copies (6: k=15, 24 warps + cache;
+ * 7: k=31, 16 warps; 8: k=15, 32 warps; 9: k=23, 16 warps + cache).
+ * No GraphOne counterpart (GraphOne hard-wires the merge schedule,
+ * engine/blas_gc.h:130-132). */
 g1_status g1_graph_set_schedule(g1_graph* g, int transpose, g1_schedule sched, int variant);
 /* Times the merge schedule at each tile size and the CSR-vector schedule on
  * this graph and keeps the fastest for G1_SCHED_AUTO.  Results in ms (may be
