@@ -1,0 +1,238 @@
+#pragma once
+// Parallel primitives of the GraphOne API (reference: archi/thrust/
+// functions.h:17-104 over Thrust, archi/only/cuda.cuh:37-99).  The cuda
+// versions are this library's own grid-stride kernels, launched on the
+// default stream; iterators may be raw pointers or any random-access
+// iterator usable in device code (thrust::counting_iterator included), and
+// operators may be __device__ lambdas with or without a declared return
+// type (the accumulator of transform_reduce is the type of `init`).
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <iterator>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "graphone_b200.h"
+#include "GraphOne/macros.h"
+#include "GraphOne/type.hpp"
+
+namespace graph_one::archi {
+
+namespace detail {
+
+constexpr int kBlock = 256;
+
+inline unsigned grid_for(size_t n) {
+    static int sms = [] {
+        int dev = 0, s = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, dev);
+        return s;
+    }();
+    const size_t want = (n + kBlock - 1) / kBlock;
+    return (unsigned)std::max<size_t>(1, std::min<size_t>(want, (size_t)sms * 8));
+}
+
+inline void check_launch(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "[ERROR] %s: %s\n", what, cudaGetErrorString(e));
+        std::exit(1);
+    }
+}
+
+template <typename It, typename T>
+__global__ void fill_kernel(It first, size_t n, T value) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        first[i] = value;
+}
+
+template <typename It, typename Out, typename Op>
+__global__ void transform_kernel(It first, size_t n, Out out, Op op) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        out[i] = op(first[i]);
+}
+
+template <typename It1, typename It2, typename Out, typename Op>
+__global__ void transform2_kernel(It1 a, size_t n, It2 b, Out out, Op op) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        out[i] = op(a[i], b[i]);
+}
+
+template <typename It, typename Op>
+__global__ void for_each_kernel(It first, size_t n, Op op) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        op(first[i]);
+}
+
+// Per-block fold of op(first[i]) with bop; partial[b] holds the block's
+// value and valid[b] whether the block saw any element.
+template <typename It, typename Op, typename T, typename Bop>
+__global__ void reduce_kernel(It first, size_t n, Op op, Bop bop, T* partial, int* valid) {
+    __shared__ T s_val[kBlock];
+    __shared__ int s_ok[kBlock];
+    T acc{};
+    int ok = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const T v = static_cast<T>(op(first[i]));
+        acc = ok ? bop(acc, v) : v;
+        ok = 1;
+    }
+    s_val[threadIdx.x] = acc;
+    s_ok[threadIdx.x] = ok;
+    __syncthreads();
+    for (int w = kBlock / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w && s_ok[threadIdx.x + w]) {
+            s_val[threadIdx.x] = s_ok[threadIdx.x] ? bop(s_val[threadIdx.x], s_val[threadIdx.x + w])
+                                                   : s_val[threadIdx.x + w];
+            s_ok[threadIdx.x] = 1;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = s_val[0];
+        valid[blockIdx.x] = s_ok[0];
+    }
+}
+
+template <typename T>
+struct Identity {
+    __host__ __device__ T operator()(const T& v) const { return v; }
+};
+
+}  // namespace detail
+
+template <arch_t arch, typename It, typename T>
+void fill(It first, It last, const T& value) {
+    const size_t n = (size_t)(last - first);
+    if (n == 0) return;
+    if constexpr (arch == arch_t::cpu) {
+        std::fill(first, last, value);
+    } else {
+        using V = typename std::iterator_traits<It>::value_type;
+        detail::fill_kernel<<<detail::grid_for(n), detail::kBlock>>>(first, n, V(value));
+        detail::check_launch("archi::fill");
+        g1_count_user_launches(1);
+    }
+}
+
+template <arch_t arch, typename It, typename Out, typename Op>
+Out transform(It first, It last, Out result, Op op) {
+    const size_t n = (size_t)(last - first);
+    if (n == 0) return result;
+    if constexpr (arch == arch_t::cpu) {
+        for (size_t i = 0; i < n; ++i) result[i] = op(first[i]);
+    } else {
+        detail::transform_kernel<<<detail::grid_for(n), detail::kBlock>>>(first, n, result, op);
+        detail::check_launch("archi::transform");
+        g1_count_user_launches(1);
+    }
+    return result + n;
+}
+
+template <arch_t arch, typename It1, typename It2, typename Out, typename Op>
+Out transform(It1 first1, It1 last1, It2 first2, Out result, Op op) {
+    const size_t n = (size_t)(last1 - first1);
+    if (n == 0) return result;
+    if constexpr (arch == arch_t::cpu) {
+        for (size_t i = 0; i < n; ++i) result[i] = op(first1[i], first2[i]);
+    } else {
+        detail::transform2_kernel<<<detail::grid_for(n), detail::kBlock>>>(first1, n, first2,
+                                                                           result, op);
+        detail::check_launch("archi::transform");
+        g1_count_user_launches(1);
+    }
+    return result + n;
+}
+
+template <arch_t arch, typename It, typename Op>
+It for_each(It first, It last, Op op) {
+    const size_t n = (size_t)(last - first);
+    if (n == 0) return last;
+    if constexpr (arch == arch_t::cpu) {
+        for (size_t i = 0; i < n; ++i) op(first[i]);
+    } else {
+        detail::for_each_kernel<<<detail::grid_for(n), detail::kBlock>>>(first, n, op);
+        detail::check_launch("archi::for_each");
+        g1_count_user_launches(1);
+    }
+    return last;
+}
+
+template <arch_t arch, typename It, typename Op, typename T, typename Bop>
+T transform_reduce(It first, It last, Op op, T init, Bop bop) {
+    const size_t n = (size_t)(last - first);
+    if (n == 0) return init;
+    if constexpr (arch == arch_t::cpu) {
+        T acc = init;
+        for (size_t i = 0; i < n; ++i) acc = bop(acc, static_cast<T>(op(first[i])));
+        return acc;
+    } else {
+        const unsigned grid = detail::grid_for(n);
+        T* partial = nullptr;
+        int* valid = nullptr;
+        if (g1_mem_alloc(reinterpret_cast<void**>(&partial), sizeof(T) * grid) != G1_OK ||
+            g1_mem_alloc(reinterpret_cast<void**>(&valid), sizeof(int) * grid) != G1_OK) {
+            std::fprintf(stderr, "[ERROR] archi::transform_reduce: %s\n", g1_last_error());
+            std::exit(1);
+        }
+        detail::reduce_kernel<<<grid, detail::kBlock>>>(first, n, op, bop, partial, valid);
+        detail::check_launch("archi::transform_reduce");
+        g1_count_user_launches(1);
+        std::vector<T> hp(grid);
+        std::vector<int> hv(grid);
+        g1_mem_copy(hp.data(), partial, sizeof(T) * grid, 1, nullptr);
+        g1_mem_copy(hv.data(), valid, sizeof(int) * grid, 1, nullptr);
+        g1_mem_free(partial);
+        g1_mem_free(valid);
+        T acc = init;
+        for (unsigned b = 0; b < grid; ++b)
+            if (hv[b]) acc = bop(acc, hp[b]);
+        return acc;
+    }
+}
+
+namespace cuda {
+
+// Atomic minimum returning the previous value (reference:
+// archi/only/cuda.cuh:52-70): native for integers; for floating point a
+// compare-and-swap loop that gives up as soon as the stored value is not
+// larger than `value`.
+template <typename T>
+__device__ __forceinline__ T AtomicMin(T* address, T value) {
+    if constexpr (std::is_same_v<T, float>) {
+        int* p = reinterpret_cast<int*>(address);
+        int cur = *reinterpret_cast<volatile int*>(p);
+        while (__int_as_float(cur) > value) {
+            const int prev = atomicCAS(p, cur, __float_as_int(value));
+            if (prev == cur) break;
+            cur = prev;
+        }
+        return __int_as_float(cur);
+    } else if constexpr (std::is_same_v<T, double>) {
+        unsigned long long* p = reinterpret_cast<unsigned long long*>(address);
+        unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(p);
+        while (__longlong_as_double((long long)cur) > value) {
+            const unsigned long long prev =
+                atomicCAS(p, cur, (unsigned long long)__double_as_longlong(value));
+            if (prev == cur) break;
+            cur = prev;
+        }
+        return __longlong_as_double((long long)cur);
+    } else {
+        return ::atomicMin(address, value);
+    }
+}
+
+}  // namespace cuda
+
+}  // namespace graph_one::archi

@@ -1,0 +1,186 @@
+#pragma once
+// Device-resident graphs of the GraphOne API (reference: graph/graph.h:18-140,
+// graph/graph_arch_ref.h:23-116, graph/graph_view.hpp:10-60,
+// graph/builder.h:9-46).
+//
+// A Graph owns a g1_graph of libgraphone_b200 (CSR arrays padded and
+// validated on the device, merge-path plans cached with it).  `views`
+// selects the orientations: normal (out-edges), transpose (in-edges), or
+// both; the first view listed is the "main" CSR that ToArch() exposes as
+// row_offsets/col_indices/values, exactly as in GraphOne (a transpose-only
+// graph's main CSR is the transpose).
+
+#include <cstdint>
+#include <memory>
+#include <type_traits>
+#include <vector>
+
+#include "graphone_b200.h"
+#include "GraphOne/loader/loader.h"
+#include "GraphOne/macros.h"
+#include "GraphOne/type.hpp"
+#include "GraphOne/utils/log.hpp"
+
+namespace graph_one {
+
+enum class graph_view_t : uint8_t { normal = 1 << 0, transpose = 1 << 1, coo = 1 << 2, csr = 1 << 3 };
+
+constexpr graph_view_t operator|(graph_view_t a, graph_view_t b) {
+    return static_cast<graph_view_t>(static_cast<uint8_t>(a) | static_cast<uint8_t>(b));
+}
+constexpr bool has_view(graph_view_t v, graph_view_t m) {
+    return (static_cast<uint8_t>(v) & static_cast<uint8_t>(m)) == static_cast<uint8_t>(m);
+}
+template <typename... M>
+constexpr bool has_all_views(graph_view_t v, M... m) {
+    return (has_view(v, m) && ...);
+}
+template <typename... M>
+constexpr bool has_some_views(graph_view_t v, M... m) {
+    return (has_view(v, m) || ...);
+}
+
+template <graph_view_t views, arch_t arch, vstart_t v_start, typename vprop_t, typename vertex_t,
+          typename edge_t, typename weight_t>
+struct GraphArchRef {
+    using vprop_type = vprop_t;
+    using vertex_type = vertex_t;
+    using edge_type = edge_t;
+    using weight_type = weight_t;
+    constexpr static arch_t arch_value = arch;
+    constexpr static vstart_t vstart_value = v_start;
+    constexpr static bool both_mat = has_all_views(views, graph_view_t::normal, graph_view_t::transpose);
+
+    template <graph_view_t V = views, std::enable_if_t<has_view(V, graph_view_t::normal), int> = 0>
+    __host__ __device__ vertex_t get_out_degree(vertex_t v) const {
+        return row_offsets[v + 1] - row_offsets[v];
+    }
+    template <graph_view_t V = views, std::enable_if_t<has_view(V, graph_view_t::transpose), int> = 0>
+    __host__ __device__ vertex_t get_in_degree(vertex_t v) const {
+        if constexpr (both_mat)
+            return trans_row_offsets[v + 1] - trans_row_offsets[v];
+        else
+            return row_offsets[v + 1] - row_offsets[v];
+    }
+    template <graph_view_t V = views, std::enable_if_t<has_view(V, graph_view_t::normal), int> = 0>
+    __host__ __device__ edge_t get_starting_out_edge(vertex_t v) const {
+        return row_offsets[v];
+    }
+    template <graph_view_t V = views, std::enable_if_t<has_view(V, graph_view_t::normal), int> = 0>
+    __host__ __device__ vertex_t get_dst_vertex_by_out_edge(edge_t e) const {
+        return col_indices[e];
+    }
+    template <graph_view_t V = views, std::enable_if_t<has_view(V, graph_view_t::normal), int> = 0>
+    __host__ __device__ weight_t get_out_edge_weight(edge_t e) const {
+        return values[e];
+    }
+
+    vertex_t num_vertices{0};
+    edge_t num_edges{0};
+    const edge_t* row_offsets{nullptr};
+    const vertex_t* col_indices{nullptr};
+    const weight_t* values{nullptr};
+    const edge_t* trans_row_offsets{nullptr};
+    const vertex_t* trans_col_indices{nullptr};
+    const weight_t* trans_values{nullptr};
+    vprop_t vprops{};
+};
+
+namespace detail {
+struct GraphHandleDeleter {
+    void operator()(g1_graph* g) const { g1_graph_destroy(g); }
+};
+}  // namespace detail
+
+template <arch_t arch, graph_view_t views, vstart_t v_start, typename vprop_t, typename vertex_t,
+          typename edge_t, typename weight_t>
+class Graph {
+public:
+    static_assert(arch == arch_t::cuda, "graphs live on the GPU");
+    static_assert(has_some_views(views, graph_view_t::normal, graph_view_t::transpose),
+                  "a graph needs the normal or the transpose view");
+    static_assert(sizeof(vertex_t) == 4 && sizeof(edge_t) == 4, "32-bit vertex and edge ids");
+    static_assert(sizeof(weight_t) == 4, "4-byte edge values (u32/i32/f32)");
+
+    using vprop_type = vprop_t;
+    using vertex_type = vertex_t;
+    using edge_type = edge_t;
+    using weight_type = weight_t;
+    using arch_ref_t = GraphArchRef<views, arch, v_start, vprop_t, vertex_t, edge_t, weight_t>;
+    constexpr static arch_t arch_value = arch;
+    constexpr static vstart_t vstart_value = v_start;
+    constexpr static graph_view_t views_value = views;
+    constexpr static bool has_normal = has_view(views, graph_view_t::normal);
+    constexpr static bool has_transpose = has_view(views, graph_view_t::transpose);
+    constexpr static bool both_mat = has_normal && has_transpose;
+
+    Graph(g1_graph* handle, vertex_t n, edge_t m)
+        : h_(handle, detail::GraphHandleDeleter()), n_(n), m_(m) {}
+
+    vertex_t num_vertices() const { return n_; }
+    edge_t num_edges() const { return m_; }
+    g1_graph* handle() const { return h_.get(); }
+
+    arch_ref_t ToArch() const {
+        arch_ref_t r;
+        r.num_vertices = n_;
+        r.num_edges = m_;
+        const int main_side = has_normal ? 0 : 1;
+        fetch_(main_side, &r.row_offsets, &r.col_indices, &r.values);
+        if constexpr (both_mat) fetch_(1, &r.trans_row_offsets, &r.trans_col_indices, &r.trans_values);
+        return r;
+    }
+
+    std::string ToString() const {
+        return "Graph{ num_vertices:" + utils::NumToString(n_) + ", num_edges:" +
+               utils::NumToString(m_) + " }";
+    }
+
+private:
+    void fetch_(int side, const edge_t** rp, const vertex_t** ci, const weight_t** v) const {
+        const uint32_t *a = nullptr, *b = nullptr;
+        const void* c = nullptr;
+        if (g1_graph_arrays(h_.get(), side, &a, &b, &c) != G1_OK)
+            LOG_ERROR("graph arrays: ", g1_last_error());
+        *rp = reinterpret_cast<const edge_t*>(a);
+        *ci = reinterpret_cast<const vertex_t*>(b);
+        *v = static_cast<const weight_t*>(c);
+    }
+
+    std::shared_ptr<g1_graph> h_;
+    vertex_t n_;
+    edge_t m_;
+};
+
+namespace graph {
+
+// graph::build (reference: graph/builder.h:9-46): the host CSR of the first
+// needed orientation is made by EdgeCache's counting sort and handed to
+// libgraphone_b200, which builds the other orientation on the GPU when the
+// views ask for both.
+template <arch_t arch, graph_view_t views, vstart_t v_start, typename vertex_t, typename edge_t,
+          typename weight_t>
+Graph<arch, views, v_start, empty_t, vertex_t, edge_t, weight_t> build(
+    EdgeCache<v_start, weight_t, vertex_t, edge_t>& cache) {
+    using G = Graph<arch, views, v_start, empty_t, vertex_t, edge_t, weight_t>;
+    std::vector<edge_t> rp;
+    std::vector<vertex_t> ci;
+    std::vector<weight_t> val;
+    uint32_t flags = 0;
+    if constexpr (G::has_normal) {
+        cache.template BuildCsr<false>(rp, ci, val);
+        if constexpr (G::has_transpose) flags |= G1_GRAPH_BUILD_OTHER;
+    } else {
+        cache.template BuildCsr<true>(rp, ci, val);
+        flags |= G1_GRAPH_INPUT_TRANSPOSE;
+    }
+    const g1_dtype vt = std::is_floating_point_v<weight_t> ? G1_F32 : G1_U32;
+    g1_graph* h = nullptr;
+    const g1_status s = g1_graph_create(rp.data(), ci.data(), val.data(), vt, cache.num_vertices(),
+                                        (uint32_t)cache.num_edges(), flags, nullptr, &h);
+    if (s != G1_OK) LOG_ERROR("graph::build: ", g1_status_string(s), ": ", g1_last_error());
+    return G(h, cache.num_vertices(), (edge_t)cache.num_edges());
+}
+
+}  // namespace graph
+}  // namespace graph_one

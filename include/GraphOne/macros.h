@@ -1,0 +1,14 @@
+#pragma once
+// Function qualifiers of the GraphOne API (reference: archi/macro/macro.h,
+// archi/macro/cuda.cuh).  User functors and lambdas are written with these.
+
+#define __ONE_CUDA_KERNEL__ __global__
+#define __ONE_CUDA__ __device__
+#define __ONE_CUDA_INL__ __device__ __forceinline__
+#define __ONE_CPU_CUDA__ __host__ __device__
+#define __ONE_CPU_CUDA_INL__ __host__ __device__ __forceinline__
+
+#define __ONE_DEV__ __ONE_CUDA__
+#define __ONE_DEV_INL__ __ONE_CUDA_INL__
+#define __ONE_ARCH__ __ONE_CPU_CUDA__
+#define __ONE_ARCH_INL__ __ONE_CPU_CUDA_INL__

@@ -868,35 +868,63 @@ spmv_wtma_kernel(MergeArgs<SR> a, Epi epi) {
     epi.template block_end<WARPS * 32>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
 }
 
-// Finishes rows that cross tiles: for every tile T whose first row began in
-// an earlier tile and ends inside T, folds carry[first..T-1] and tail[T] in
-// tile order and emits the row.  One thread per tile.
+// Finishes rows that cross tiles.  For every tile T whose first row i0
+// began in an earlier tile and ends inside T, the row's value is
+// carry[first..T-1] (partials of the row in the tiles it spans) folded with
+// tail[T] (its part inside T).  The common case -- the row began in tile
+// T-1 -- is one load per thread; rows spanning more tiles (hubs) are folded
+// by the whole warp: a binary search over tile_row finds the first tile of
+// the row, then the lanes fold the carries strided and combine them with a
+// shuffle tree.  The emit goes through the same epilogue as the main kernel.
 template <class SR, class Epi, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 spmv_fixup_kernel(MergeArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
     __shared__ alignas(16) char epi_smem[64 * 8];
     const uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
+    const uint32_t lane = lane_id();
     epi.begin();
+    bool longc = false;
+    uint32_t i0 = 0, rs = 0;
+    V acc = SR::identity();
     if (t < a.plan.n_tiles) {
-        const uint32_t i0 = a.plan.tile_row[t];
+        i0 = a.plan.tile_row[t];
         const uint32_t j0 = a.plan.tile_nnz[t];
         const uint32_t i1 = a.plan.tile_row[t + 1];
         if (i1 > i0 && i0 < a.plan.n_rows) {
-            const uint32_t rs = a.plan.row_ptr[i0];
+            rs = a.plan.row_ptr[i0];
             if (j0 > rs) {  // spanning row, completed in tile t (t >= 1 here)
-                V acc = a.tail[t];
-                uint32_t k = t - 1;
-                for (;;) {
-                    acc = SR::reduce(a.carry[k], acc);
-                    if (k > 0 && a.plan.tile_row[k] == i0 && a.plan.tile_nnz[k] > rs)
-                        --k;
-                    else
-                        break;
-                }
-                epi.emit(i0, acc);
+                acc = SR::reduce(a.carry[t - 1], a.tail[t]);
+                const uint32_t k = t - 1;
+                if (k > 0 && a.plan.tile_row[k] == i0 && a.plan.tile_nnz[k] > rs)
+                    longc = true;  // the row also spans tile t-2 or earlier
+                else
+                    epi.emit(i0, acc);
             }
         }
+    }
+    unsigned pending = __ballot_sync(0xffffffffu, longc);
+    while (pending) {
+        const int src = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const uint32_t r = __shfl_sync(0xffffffffu, i0, src);
+        const uint32_t rsv = __shfl_sync(0xffffffffu, rs, src);
+        const uint32_t tt = blockIdx.x * BLOCK + (threadIdx.x & ~31u) + (uint32_t)src;
+        // first tile whose start lies in row r
+        uint32_t lo = 0, hi = tt - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (a.plan.tile_row[mid] < r) lo = mid + 1; else hi = mid;
+        }
+        // the row began inside tile lo-1 unless tile lo starts exactly at it
+        const uint32_t first = (lo > 0 && a.plan.tile_nnz[lo] > rsv) ? lo - 1 : lo;
+        V part = SR::identity();
+        for (uint32_t k = first + lane; k + 1 < tt; k += 32)
+            part = SR::reduce(part, a.carry[k]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+            part = SR::reduce(part, shfl_down_any(0xffffffffu, part, off));
+        if ((int)lane == src) epi.emit(i0, SR::reduce(part, acc));
     }
     epi.template block_end<BLOCK>(epi_smem);
 }
