@@ -55,6 +55,7 @@ def _declare(L):
     L.g1_mem_fill_u32.argtypes = [P, C.c_uint32, C.c_size_t, P]
     L.g1_stream_sync.argtypes = [P]
     L.g1_kernel_launches.restype = C.c_uint64
+    L.g1_count_user_launches.argtypes = [C.c_uint64]
     L.g1_profile_begin.argtypes = []
     L.g1_profile_end.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
     L.g1_graph_create.argtypes = [P, P, P, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, P,
@@ -65,7 +66,7 @@ def _declare(L):
     L.g1_graph_arrays.argtypes = [P, C.c_int, C.POINTER(P), C.POINTER(P), C.POINTER(P)]
     L.g1_graph_device_bytes.restype = C.c_size_t
     L.g1_graph_device_bytes.argtypes = [P]
-    L.g1_spmv_plan.argtypes = [P, C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+    L.g1_spmv_plan.argtypes = [P, C.c_int, C.c_uint32, C.POINTER(C.c_uint32),
                                C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]
     L.g1_spmv.argtypes = [P, C.c_int, C.c_int, C.c_int, P, P, P]
     L.g1_graph_set_schedule.argtypes = [P, C.c_int, C.c_int, C.c_int]
@@ -91,6 +92,7 @@ def lib():
 EXPORTS = (
     "g1_status_string", "g1_last_error", "g1_version", "g1_mem_alloc", "g1_mem_free",
     "g1_mem_copy", "g1_mem_fill_u32", "g1_stream_sync", "g1_kernel_launches",
+    "g1_count_user_launches",
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
     "g1_spmv_plan", "g1_spmv", "g1_graph_set_schedule", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs",
@@ -197,12 +199,12 @@ class Graph:
         check(lib().g1_graph_info(self._h, C.byref(n), C.byref(m), C.byref(hn), C.byref(ht)))
         return n.value, m.value, bool(hn.value), bool(ht.value)
 
-    def plan(self, transpose: int = 1):
-        items, tiles = C.c_uint32(), C.c_uint32()
+    def plan(self, transpose: int = 1, items_per_tile: int = 0):
+        tiles = C.c_uint32()
         tr, tn, ca, ta = P(), P(), P(), P()
-        check(lib().g1_spmv_plan(self._h, transpose, C.byref(items), C.byref(tiles), C.byref(tr),
+        check(lib().g1_spmv_plan(self._h, transpose, items_per_tile, C.byref(tiles), C.byref(tr),
                                  C.byref(tn), C.byref(ca), C.byref(ta)))
-        return items.value, tiles.value, tr.value, tn.value
+        return tiles.value, tr.value, tn.value
 
     def spmv(self, x, y, semiring: int, transpose: int = 1, schedule: int = SCHED_AUTO,
              stream=None):

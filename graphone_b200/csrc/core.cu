@@ -491,6 +491,8 @@ const char* g1_version(void) { return "graphone_b200 0.1 sm_100a"; }
 
 uint64_t g1_kernel_launches(void) { return g_launches.load(); }
 
+void g1_count_user_launches(uint64_t n) { count_launches(n); }
+
 g1_status g1_profile_begin(void) {
     Profiler& p = prof();
     std::lock_guard<std::mutex> lk(p.mu);
@@ -673,16 +675,17 @@ size_t g1_graph_device_bytes(const g1_graph* g) {
     return s;
 }
 
-g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t* items_per_tile, uint32_t* n_tiles,
+g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t items_per_tile, uint32_t* n_tiles,
                        const uint32_t** tile_row, const uint32_t** tile_nnz, void** carry,
                        void** tail) {
     if (!g || transpose < 0 || transpose > 1) return fail(G1_ERR_INVALID, "g1_spmv_plan");
     DeviceGuard dg(g->device);
     std::lock_guard<std::mutex> lk(g->mu);
     MergePlan* pp = nullptr;
-    G1_TRY(ensure_plan(g, transpose, merge_items(merge_variant(g, transpose)), &pp));
+    const uint32_t items =
+        items_per_tile ? items_per_tile : merge_items(merge_variant(g, transpose));
+    G1_TRY(ensure_plan(g, transpose, items, &pp));
     const MergePlan& p = *pp;
-    if (items_per_tile) *items_per_tile = p.items;
     if (n_tiles) *n_tiles = p.n_tiles;
     if (tile_row) *tile_row = p.tile_row.as<uint32_t>();
     if (tile_nnz) *tile_nnz = p.tile_nnz.as<uint32_t>();

@@ -165,9 +165,9 @@ public:
         fill_zero_(size_);
     }
 
-    template <arch_t to>
-    Buffer<to, value_t, index_t> to() const {
-        return Buffer<to, value_t, index_t>(*this);
+    template <arch_t dst_arch>
+    Buffer<dst_arch, value_t, index_t> to() const {
+        return Buffer<dst_arch, value_t, index_t>(*this);
     }
 
     std::string ToString() const {
@@ -210,9 +210,9 @@ public:
     DenseVec(const Buffer<arch, value_t, index_t>& b) : Buffer<arch, value_t, index_t>(b) {}
     DenseVec(Buffer<arch, value_t, index_t>&& b) : Buffer<arch, value_t, index_t>(std::move(b)) {}
 
-    template <arch_t to>
-    DenseVec<to, value_t, index_t> to() const {
-        return DenseVec<to, value_t, index_t>(Buffer<to, value_t, index_t>(*this));
+    template <arch_t dst_arch>
+    DenseVec<dst_arch, value_t, index_t> to() const {
+        return DenseVec<dst_arch, value_t, index_t>(Buffer<dst_arch, value_t, index_t>(*this));
     }
 };
 

@@ -1,0 +1,227 @@
+#pragma once
+// The advance/filter engine of the GraphOne API (reference:
+// engine/advance_gc.h:24-303), with the user functor inlined.
+//
+// GraphOne sizes an invalid-padded output by a degree-sum reduction, runs a
+// block-scan load-balanced advance (functor::advance decides per edge
+// whether dst is emitted), synchronises, then filters duplicates in a second
+// pass (functor::filter, when the functor has one).  Here the advance
+// appends emitted vertices compactly (warp-aggregated atomics) while
+// accumulating their out-degrees, so the output's worst-case size for the
+// next iteration is known without a separate reduction; adjacency lists of
+// 32 or more edges are walked by the whole warp (coalesced col/val reads),
+// shorter ones by one lane.  The filter step compacts the same way.  One
+// read-back per step gives the host the new frontier size.
+
+#include <algorithm>
+#include <cstdint>
+#include <type_traits>
+
+#include <cuda_runtime.h>
+
+#include "graphone_b200.h"
+#include "g1/common.cuh"
+#include "GraphOne/engine/base.h"
+#include "GraphOne/frontier/frontier.h"
+#include "GraphOne/graph/graph.h"
+#include "GraphOne/utils/limits.hpp"
+
+namespace graph_one {
+namespace engine {
+namespace adv_detail {
+
+// append with a capacity check; an overflow is recorded, never written
+__device__ __forceinline__ void append_capped(uint32_t* out, uint32_t* ctr, uint32_t cap,
+                                              uint32_t v, uint32_t deg) {
+    const unsigned mask = __activemask();
+    const int leader = __ffs(mask) - 1;
+    const uint32_t lane = g1::lane_id();
+    const uint32_t tot = __reduce_add_sync(mask, deg);
+    uint32_t base = 0;
+    if ((int)lane == leader) {
+        base = atomicAdd(&ctr[0], (uint32_t)__popc(mask));
+        atomicAdd(reinterpret_cast<unsigned long long*>(ctr + 2), (unsigned long long)tot);
+    }
+    base = __shfl_sync(mask, base, leader);
+    const uint32_t slot = base + __popc(mask & ((1u << lane) - 1u));
+    if (slot < cap)
+        out[slot] = v;
+    else
+        atomicExch(&ctr[1], 1u);
+}
+
+template <class F, class V, class E, class W, class D>
+__device__ __forceinline__ void visit(V src, V dst, E e, W w, D& ds, const E* rp, uint32_t* out,
+                                      uint32_t* ctr, uint32_t cap) {
+    if (F::advance(src, dst, e, w, ds)) append_capped(out, ctr, cap, dst, rp[dst + 1] - rp[dst]);
+}
+
+template <class F, class V, class E, class W, class D, vstart_t VS>
+__global__ void __launch_bounds__(256)
+advance_kernel(const E* rp, const V* col, const W* val, D ds, const V* in, uint32_t n_in,
+               uint32_t* out, uint32_t* ctr, uint32_t cap) {
+    const uint32_t lane = g1::lane_id();
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t rounds = (n_in + warps * 32 - 1) / (warps * 32);
+    D local = ds;  // functors may mutate their copy (reference: passed by value)
+    for (uint32_t r = 0; r < rounds; ++r) {
+        const uint32_t i = (r * warps + wid) * 32 + lane;
+        V u = utils::invalid_vertex<VS, V>();
+        E b = 0, e = 0;
+        if (i < n_in) {
+            u = in[i];
+            if (utils::is_vertex_valid<VS>(u)) {
+                b = rp[u];
+                e = rp[u + 1];
+            }
+        }
+        unsigned big = __ballot_sync(0xffffffffu, e - b >= 32);
+        while (big) {
+            const int src = __ffs(big) - 1;
+            big &= big - 1;
+            const V uu = __shfl_sync(0xffffffffu, u, src);
+            const E bb = __shfl_sync(0xffffffffu, b, src);
+            const E ee = __shfl_sync(0xffffffffu, e, src);
+            for (E k = bb + lane; k < ee; k += 32) visit<F>(uu, col[k], k, val[k], local, rp, out, ctr, cap);
+        }
+        if (e - b < 32)
+            for (E k = b; k < e; ++k) visit<F>(u, col[k], k, val[k], local, rp, out, ctr, cap);
+    }
+}
+
+template <class F, class V, class E, class D, vstart_t VS>
+__global__ void filter_kernel(const E* rp, D ds, const V* in, uint32_t n, uint32_t* out,
+                              uint32_t* ctr, uint32_t cap) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V v = in[i];
+        if (utils::is_vertex_valid<VS>(v) && !F::filter(v, ds))
+            append_capped(out, ctr, cap, v, rp[v + 1] - rp[v]);
+    }
+}
+
+template <class V, class E, vstart_t VS>
+__global__ void degree_sum_kernel(const E* rp, const V* in, uint32_t n, unsigned long long* sum) {
+    unsigned long long s = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const V v = in[i];
+        if (utils::is_vertex_valid<VS>(v)) s += rp[v + 1] - rp[v];
+    }
+    if (s) atomicAdd(sum, s);
+}
+
+inline unsigned grid_for(uint64_t n) {
+    const uint64_t want = (n + 255) / 256;
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)detail::sm_count() * 8));
+}
+
+}  // namespace adv_detail
+
+template <typename functor_t, typename comp_t, typename frontier_t>
+class AdvanceGC : public GcEngine<comp_t, frontier_t> {
+public:
+    using base_t = GcEngine<comp_t, frontier_t>;
+    using graph_t = typename comp_t::graph_type;
+    using dstatus_t = typename comp_t::dstatus_type;
+    using vertex_t = typename graph_t::vertex_type;
+    using edge_t = typename graph_t::edge_type;
+    using weight_t = typename graph_t::weight_type;
+    constexpr static vstart_t VS = graph_t::vstart_value;
+    static_assert(frontier_t::kind == SPARSE_BASED, "the advance engine needs a sparse frontier");
+    static_assert(graph_t::has_normal, "the advance engine walks out-edges (normal view)");
+
+    struct HasFilter {
+        template <typename T>
+        static std::true_type test(decltype(&T::filter));
+        template <typename T>
+        static std::false_type test(...);
+        constexpr static bool value = decltype(test<functor_t>(0))::value;
+    };
+
+    AdvanceGC(comp_t& comp, frontier_t& frontier) : base_t(comp, frontier) {
+        detail::check_cuda(cudaStreamCreate(&stream_), "stream");
+        const uint32_t *rp = nullptr, *ci = nullptr;
+        const void* val = nullptr;
+        detail::check_g1(g1_graph_arrays(comp.graph.handle(), 0, &rp, &ci, &val), "graph arrays");
+        rp_ = reinterpret_cast<const edge_t*>(rp);
+        col_ = reinterpret_cast<const vertex_t*>(ci);
+        val_ = static_cast<const weight_t*>(val);
+    }
+
+    ~AdvanceGC() override {
+        cudaStreamSynchronize(stream_);
+        cudaStreamDestroy(stream_);
+    }
+
+    void Forward() override {
+        frontier_t& f = this->frontier_;
+        const dstatus_t ds = this->d_status_;
+        const uint32_t n_in = f.input_size();
+        if (!degree_known_) {  // first step: out-degree sum of the seeds
+            counters_.clear(stream_);
+            adv_detail::degree_sum_kernel<vertex_t, edge_t, VS>
+                <<<adv_detail::grid_for(n_in), 256, 0, stream_>>>(rp_, f.input().data(), n_in,
+                                                                 counters_.degree_sum_dev());
+            g1_count_user_launches(1);
+            counters_.read(stream_);
+            next_degree_ = counters_.degree_sum();
+            degree_known_ = true;
+        }
+        // the advance emits at most one vertex per out-edge of the input
+        const uint32_t cap = (uint32_t)std::min<unsigned long long>(next_degree_ + 1, 0xFFFFFFF0ull);
+        f.reserve_output(cap);
+        counters_.clear(stream_);
+        adv_detail::advance_kernel<functor_t, vertex_t, edge_t, weight_t, dstatus_t, VS>
+            <<<adv_detail::grid_for(n_in), 256, 0, stream_>>>(rp_, col_, val_, ds, f.input().data(),
+                                                              n_in, f.output().data(),
+                                                              counters_.dev, cap);
+        g1_count_user_launches(1);
+        counters_.read(stream_);
+        if (counters_.overflow()) LOG_ERROR("advance: output frontier overflow");
+        f.reset_output(counters_.count());
+        next_degree_ = counters_.degree_sum();
+        if constexpr (HasFilter::value) {
+            f.swap_inout();
+            const uint32_t n = f.input_size();
+            f.reserve_output(std::max<uint32_t>(n, 1));
+            counters_.clear(stream_);
+            adv_detail::filter_kernel<functor_t, vertex_t, edge_t, dstatus_t, VS>
+                <<<adv_detail::grid_for(n), 256, 0, stream_>>>(rp_, ds, f.input().data(), n,
+                                                               f.output().data(), counters_.dev,
+                                                               std::max<uint32_t>(n, 1));
+            g1_count_user_launches(1);
+            counters_.read(stream_);
+            f.reset_output(counters_.count());
+            next_degree_ = counters_.degree_sum();
+        }
+    }
+
+private:
+    cudaStream_t stream_{};
+    const edge_t* rp_ = nullptr;
+    const vertex_t* col_ = nullptr;
+    const weight_t* val_ = nullptr;
+    detail::Counters counters_;
+    bool degree_known_ = false;
+    unsigned long long next_degree_ = 0;
+};
+
+}  // namespace engine
+
+constexpr graph_view_t AdvanceViews = graph_view_t::csr | graph_view_t::normal;
+
+// Base of user advance functors (GraphOne: engine/advance_gc.h:289-303); a
+// functor may add `static bool filter(const vertex_t&, const dstatus_t&)`.
+template <typename vertex_t, typename edge_t, typename weight_t, typename dstatus_t,
+          typename vprop_t = empty_t>
+struct AdvanceFunctor {
+    template <typename functor_t, typename comp_t, typename frontier_t>
+    using engine_type = engine::AdvanceGC<functor_t, comp_t, frontier_t>;
+
+    __device__ __forceinline__ static bool advance(const vertex_t&, const vertex_t&, const edge_t&,
+                                                   const weight_t&, dstatus_t&) {
+        return false;
+    }
+};
+
+}  // namespace graph_one

@@ -91,6 +91,9 @@ g1_status g1_stream_sync(void* stream);
 /* Number of kernels this library has launched since it was loaded (all
  * devices, all threads).  No GraphOne counterpart: measurement support. */
 uint64_t g1_kernel_launches(void);
+/* Adds n to that counter: the functor-templated engines of the GraphOne
+ * headers launch their kernels from the application and report them here. */
+void g1_count_user_launches(uint64_t n);
 /* Kernel timing of the SpMV launches (main merge / vector kernels only):
  * between g1_profile_begin and g1_profile_end every such launch is
  * bracketed by CUDA events on its own stream; g1_profile_end synchronises
@@ -121,11 +124,13 @@ g1_status g1_graph_arrays(const g1_graph* g, int transpose, const uint32_t** row
 size_t g1_graph_device_bytes(const g1_graph* g);
 
 /* ------------------------------------------------------------- SpMV */
-/* Merge-path partition of one orientation, cached in the graph
- * (replaces the SpmvDispatcher<SpmvCudaCsrMergeBased> constructor's
- * SegmentSearch, archi/blas/spmv/cuda/cuda.cuh:152-169).  The arrays stay
- * owned by the graph; tile_row/tile_nnz have n_tiles+1 entries. */
-g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t* items_per_tile,
+/* Merge-path partition of one orientation into tiles of `items_per_tile`
+ * merge items (rows + nonzeros; 0 = the orientation's current default),
+ * cached in the graph (replaces the SpmvDispatcher<SpmvCudaCsrMergeBased>
+ * constructor's SegmentSearch, archi/blas/spmv/cuda/cuda.cuh:152-169).
+ * The arrays stay owned by the graph: tile_row/tile_nnz have n_tiles+1
+ * entries; carry/tail have room for n_tiles+1 values of up to 16 bytes. */
+g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t items_per_tile,
                        uint32_t* n_tiles, const uint32_t** tile_row,
                        const uint32_t** tile_nnz, void** carry, void** tail);
 /* y = A (semiring) x over one orientation (replaces SpmvDispatcher::operator(),

@@ -31,7 +31,14 @@ def _ptr(a: np.ndarray):
 def build(ref: bool = False) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-j4", "-C", HERE, "ref", "refapps", "dropin"], check=True)
+
+
+def app(kind: str, name: str):
+    """Path of a GraphOne app binary (kind 'ref': reference engines, 'g1':
+    this repository's), or None when it was not built."""
+    p = os.path.join(HERE, "_ref", "apps_ref" if kind == "ref" else "apps_g1", name)
+    return p if os.path.exists(p) else None
 
 
 def lib():
