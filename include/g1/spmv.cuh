@@ -924,6 +924,7 @@ spmv_fixup_kernel(MergeArgs<SR> a, Epi epi) {
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1)
             part = SR::reduce(part, shfl_down_any(0xffffffffu, part, off));
+        part = shfl_any(0xffffffffu, part, 0);  // the fold's total sits in lane 0
         if ((int)lane == src) epi.emit(i0, SR::reduce(part, acc));
     }
     epi.template block_end<BLOCK>(epi_smem);
