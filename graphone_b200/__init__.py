@@ -74,6 +74,8 @@ def _declare(L):
     L.g1_pagerank.argtypes = [P, C.c_float, C.c_int, C.c_int, P, P]
     L.g1_sssp.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
     L.g1_bfs.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
+    L.g1_bfs_batch.argtypes = [P, P, C.c_uint32, P, C.POINTER(C.c_uint32), P]
+    L.g1_sssp_batch.argtypes = [P, P, C.c_uint32, P, C.POINTER(C.c_uint32), P]
     return L
 
 
@@ -96,6 +98,7 @@ EXPORTS = (
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
     "g1_spmv_plan", "g1_spmv", "g1_graph_set_schedule", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs",
+    "g1_bfs_batch", "g1_sssp_batch",
 )
 
 
@@ -232,6 +235,24 @@ class Graph:
         it = C.c_uint32()
         check(lib().g1_sssp(self._h, src, engine, _ptr(out), C.byref(it), _stream(stream)))
         return (out, it.value) if return_iters else out
+
+    def _batch(self, fn, srcs, out, stream, return_iters):
+        if isinstance(srcs, np.ndarray) or isinstance(srcs, (list, tuple)):
+            srcs = np.ascontiguousarray(np.asarray(srcs, dtype=np.uint32))
+        k = len(srcs)
+        if out is None:
+            out = np.empty((k, self.n), np.uint32)
+        it = C.c_uint32()
+        check(fn(self._h, _ptr(srcs), k, _ptr(out), C.byref(it), _stream(stream)))
+        return (out, it.value) if return_iters else out
+
+    def bfs_batch(self, srcs, out=None, stream=None, return_iters=False):
+        """Levels of k sources, shape (k, n), one multi-source pass."""
+        return self._batch(lib().g1_bfs_batch, srcs, out, stream, return_iters)
+
+    def sssp_batch(self, srcs, out=None, stream=None, return_iters=False):
+        """Distances of k sources, shape (k, n), one multi-source pass."""
+        return self._batch(lib().g1_sssp_batch, srcs, out, stream, return_iters)
 
     def bfs(self, src, engine=ENGINE_AUTO, out=None, stream=None, return_iters=False):
         if out is None:

@@ -90,9 +90,12 @@ advance_kernel(const E* rp, const V* col, const W* val, D ds, const V* in, uint3
     }
 }
 
+// The filter reads the advance's output size from device memory (*n_dev),
+// so advance and filter run back to back without a host round trip.
 template <class F, class V, class E, class D, vstart_t VS>
-__global__ void filter_kernel(const E* rp, D ds, const V* in, uint32_t n, uint32_t* out,
+__global__ void filter_kernel(const E* rp, D ds, const V* in, const uint32_t* n_dev, uint32_t* out,
                               uint32_t* ctr, uint32_t cap) {
+    const uint32_t n = min(*n_dev, cap);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const V v = in[i];
         if (utils::is_vertex_valid<VS>(v) && !F::filter(v, ds))
@@ -146,6 +149,14 @@ public:
         rp_ = reinterpret_cast<const edge_t*>(rp);
         col_ = reinterpret_cast<const vertex_t*>(ci);
         val_ = static_cast<const weight_t*>(val);
+        // An advance over a duplicate-free frontier emits at most one vertex
+        // per edge: both lists get that room once, up front.
+        const uint32_t room = std::max<uint32_t>(comp.graph.num_edges(), comp.graph.num_vertices()) + 1;
+        frontier.reserve_output(room);
+        frontier.swap_inout();
+        frontier.reserve_output(room);
+        frontier.swap_inout();
+        check_cuda_alloc_ = true;
     }
 
     ~AdvanceGC() override {
@@ -176,21 +187,27 @@ public:
                                                               n_in, f.output().data(),
                                                               counters_.dev, cap);
         g1_count_user_launches(1);
-        counters_.read(stream_);
-        if (counters_.overflow()) LOG_ERROR("advance: output frontier overflow");
-        f.reset_output(counters_.count());
-        next_degree_ = counters_.degree_sum();
         if constexpr (HasFilter::value) {
-            f.swap_inout();
-            const uint32_t n = f.input_size();
-            f.reserve_output(std::max<uint32_t>(n, 1));
-            counters_.clear(stream_);
+            // filter the advance output (size on the device) into the input
+            // list, which the advance no longer needs; counters at +4
+            const uint32_t fcap = (uint32_t)std::min<uint64_t>(f.input().size(), 0xFFFFFFF0ull);
             adv_detail::filter_kernel<functor_t, vertex_t, edge_t, dstatus_t, VS>
-                <<<adv_detail::grid_for(n), 256, 0, stream_>>>(rp_, ds, f.input().data(), n,
-                                                               f.output().data(), counters_.dev,
-                                                               std::max<uint32_t>(n, 1));
+                <<<adv_detail::grid_for(std::min<uint64_t>(cap, (uint64_t)detail::sm_count() * 2048)),
+                   256, 0, stream_>>>(rp_, ds, f.output().data(), counters_.dev, f.input().data(),
+                                      counters_.dev + 4, fcap);
             g1_count_user_launches(1);
             counters_.read(stream_);
+            if (counters_.overflow() || counters_.host[5]) LOG_ERROR("advance: frontier overflow");
+            // GraphOne's Filter swaps in/out and fills the new output; the
+            // Run loop's AfterEngine swaps again (engine/advance_gc.h:224-240)
+            f.reset_output(counters_.count());
+            f.swap_inout();
+            f.reset_output(counters_.host[4]);
+            next_degree_ = (unsigned long long)counters_.host[6] |
+                           ((unsigned long long)counters_.host[7] << 32);
+        } else {
+            counters_.read(stream_);
+            if (counters_.overflow()) LOG_ERROR("advance: output frontier overflow");
             f.reset_output(counters_.count());
             next_degree_ = counters_.degree_sum();
         }
@@ -203,6 +220,7 @@ private:
     const weight_t* val_ = nullptr;
     detail::Counters counters_;
     bool degree_known_ = false;
+    bool check_cuda_alloc_ = false;
     unsigned long long next_degree_ = 0;
 };
 

@@ -63,7 +63,8 @@ inline int sm_count() {
 }
 
 // Device counters and a pinned mirror for the one read-back per iteration:
-// [0] appended vertices, [1] overflow flag, [2..3] out-degree sum (u64).
+// [0] appended vertices, [1] overflow flag, [2..3] out-degree sum (u64);
+// [4..7] the same for a second compaction in the same step.
 struct Counters {
     uint32_t* dev = nullptr;
     uint32_t* host = nullptr;
@@ -78,9 +79,9 @@ struct Counters {
     }
     Counters(const Counters&) = delete;
     Counters& operator=(const Counters&) = delete;
-    void clear(cudaStream_t s) { check_cuda(cudaMemsetAsync(dev, 0, 16, s), "clear counters"); }
+    void clear(cudaStream_t s) { check_cuda(cudaMemsetAsync(dev, 0, 32, s), "clear counters"); }
     void read(cudaStream_t s) {
-        check_cuda(cudaMemcpyAsync(host, dev, 16, cudaMemcpyDeviceToHost, s), "read counters");
+        check_cuda(cudaMemcpyAsync(host, dev, 32, cudaMemcpyDeviceToHost, s), "read counters");
         check_cuda(cudaStreamSynchronize(s), "engine step");
     }
     uint32_t count() const { return host[0]; }

@@ -111,10 +111,12 @@ public:
     bool IsConvergent() override { return in_size_ == 0; }
 
 private:
+    // Grows a list to at least `size` entries, keeping its contents.
     void grow_(int which, index_t size) {
-        // keeps the contents (an output that grows is refilled by the engine)
-        if (size > frontiers_[which].size())
-            frontiers_[which] = Buffer<arch, vertex_t, index_t>(size * 2);
+        if (size <= frontiers_[which].size()) return;
+        Buffer<arch, vertex_t, index_t> bigger(size * 2);
+        bigger.copy_from(frontiers_[which]);
+        frontiers_[which] = std::move(bigger);
     }
 
     int input_selector_{0};

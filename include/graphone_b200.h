@@ -171,6 +171,18 @@ g1_status g1_sssp(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* dist_ou
 g1_status g1_bfs(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* level_out,
                  uint32_t* iters_out, void* stream);
 
+/* ----------------------------------------------------- batched queries */
+/* k sources as one multi-source pass (no GraphOne counterpart: GraphOne
+ * runs one source per Run, apps/sssp_blas.cu:87-136).  srcs: k vertex ids
+ * (host or device); out: k*n u32 in source-major order (out[s*n + v]) --
+ * the layout of k g1_bfs / g1_sssp calls, and bit-identical to them.  More
+ * than 256 sources run as consecutive passes of 256.  Needs the in-edge CSR.
+ * iters_out: iterations of the longest pass (may be NULL). */
+g1_status g1_bfs_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, uint32_t* levels_out,
+                       uint32_t* iters_out, void* stream);
+g1_status g1_sssp_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, uint32_t* dist_out,
+                        uint32_t* iters_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -126,3 +126,23 @@ def test_relabelled_spmv_caller_order(cuda):
     yd = torch.empty(g.n, dtype=torch.int32, device="cuda")
     G.spmv(xd, yd, g1.SR_MINPLUS_U32, transpose=1)
     assert np.array_equal(yd.cpu().numpy().view(np.uint32), O.spmv_minplus_u32(rp, ci, v, x))
+
+
+@pytest.mark.parametrize("k", [1, 37, 256, 300])
+@pytest.mark.parametrize("name", ["rmat10_sym", "rmat11_dir", "grid32", "star20k", "single"])
+def test_batched_bfs_and_sssp_bit_exact(cuda, name, k):
+    """k sources in one multi-source pass == k single-source runs."""
+    g = GRAPHS[name]
+    rp, ci, v = g.np("n")
+    rng = np.random.default_rng(k)
+    srcs = rng.choice(g.n, size=min(k, g.n), replace=False).astype(np.uint32)
+    if len(srcs) < k:
+        srcs = np.resize(srcs, k)  # repeats are allowed
+    for relabel in (False, True):
+        G = g1.Graph.from_gen(g, relabel=relabel)
+        lv = G.bfs_batch(srcs)
+        d = G.sssp_batch(srcs)
+        for i, s in enumerate(srcs[:12].tolist() + srcs[-3:].tolist()):
+            j = i if i < 12 else len(srcs) - 15 + i
+            assert np.array_equal(lv[j], O.bfs(rp, ci, int(srcs[j]))), (name, k, j, relabel)
+            assert np.array_equal(d[j], O.dijkstra_u32(rp, ci, v, int(srcs[j]))), (name, k, j, relabel)

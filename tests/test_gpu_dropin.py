@@ -81,7 +81,9 @@ def test_pagerank_app_on_graphone_b200(cuda, tmp_path):
     gen.write_adj(g, adj, directed=True)
     vals, _ = run_app(path, ["-i", adj, "-d"], tmp_path)
     hist = pagerank_app_expected(g, len(vals))
-    # fp32 vs fp64 may stop one iteration apart; the report is the
-    # second-to-last array of the run
-    errs = [O.rel_l1(vals, h) for h in hist[-3:-1]]
-    assert min(errs) < 1e-5, errs
+    # The app prints "%f" (six decimals, absolute error <= 5e-7); fp32 vs
+    # fp64 may stop one iteration apart (consecutive iterates differ by at
+    # most the 1e-6 convergence threshold).  The report is the second-to-last
+    # array of the run.
+    errs = [float(np.max(np.abs(vals - h))) for h in hist[-3:-1]]
+    assert min(errs) < 2e-6, errs
