@@ -19,6 +19,8 @@
 // (out[s*n + v]), the layout of k single-source calls.  Min-plus is
 // order-independent, so levels and distances are bit-exact with k plain
 // traversals.
+#include <cub/device/device_scan.cuh>
+
 #include <algorithm>
 #include <vector>
 
@@ -30,9 +32,15 @@ namespace g1 {
 constexpr uint32_t kMaxBatch = 256;
 
 // ------------------------------------------------------------------ BFS
+// Row pieces: every vertex's in-edge range cut into pieces of at most
+// kPieceEdges edges, so a hub's row is pulled by many warps (its pieces merge
+// with atomics) while ordinary rows stay one warp each (plain stores).
+constexpr uint32_t kPieceEdges = 1024;
+
 template <int WP>  // words per vertex rounded up to a power of two (1..8)
 __global__ void __launch_bounds__(256)
-msbfs_pull_kernel(const uint32_t* rp, const uint32_t* col, uint32_t n, uint32_t W, uint32_t k,
+msbfs_pull_kernel(const uint32_t* rp, const uint32_t* col, const uint32_t* piece_v,
+                  const uint32_t* piece_e, uint32_t n_pieces, uint32_t W, uint32_t k,
                   const uint32_t* frontier, uint32_t* seen, uint32_t* next, uint32_t* lvm,
                   uint32_t depth, uint32_t* changed) {
     constexpr int SLOTS = 32 / WP;  // neighbours per warp step
@@ -40,29 +48,35 @@ msbfs_pull_kernel(const uint32_t* rp, const uint32_t* col, uint32_t n, uint32_t 
     const uint32_t w = lane % WP, q = lane / WP;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     uint32_t any = 0;
-    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_pieces; p += warps) {
+        const uint32_t v = piece_v[p];
+        const uint32_t rs = rp[v], re = rp[v + 1];
+        const bool multi = re - rs > kPieceEdges;
+        const uint32_t e0 = piece_e[p], e1 = min(e0 + kPieceEdges, re);
         uint32_t sn = 0xffffffffu;
         if (w < W) {
             sn = seen[(size_t)v * W + w];
             const uint32_t live = (w == W - 1 && (k & 31)) ? ((1u << (k & 31)) - 1u) : 0xffffffffu;
             sn |= ~live;  // sources beyond k count as seen
         }
-        if (__all_sync(0xffffffffu, sn == 0xffffffffu)) {
-            if (w < W && q == 0) next[(size_t)v * W + w] = 0u;
-            continue;
-        }
+        if (__all_sync(0xffffffffu, sn == 0xffffffffu)) continue;  // next[v] stays 0
         uint32_t acc = 0;
-        const uint32_t rs = rp[v], re = rp[v + 1];
-        for (uint32_t e = rs + q; e < re; e += SLOTS) {
+        for (uint32_t e = e0 + q; e < e1; e += SLOTS) {
             const uint32_t u = __ldg(col + e);
             if (w < W) acc |= __ldg(frontier + (size_t)u * W + w);
         }
 #pragma unroll
         for (int off = WP; off < 32; off <<= 1) acc |= __shfl_xor_sync(0xffffffffu, acc, off);
-        const uint32_t nw = acc & ~sn;
-        if (w < W && q == 0) {
-            next[(size_t)v * W + w] = nw;
-            if (nw) seen[(size_t)v * W + w] = sn | nw;
+        uint32_t nw = acc & ~sn;
+        if (w < W && q == 0 && nw) {
+            if (multi) {
+                // several pieces of this row: claim the bits first set here
+                nw &= ~atomicOr(&seen[(size_t)v * W + w], nw);
+                if (nw) atomicOr(&next[(size_t)v * W + w], nw);
+            } else {
+                next[(size_t)v * W + w] = nw;
+                seen[(size_t)v * W + w] = sn | nw;
+            }
         }
         // levels of the new bits: row segment j written by all 32 lanes
         for (uint32_t j = 0; j < W; ++j) {
@@ -99,20 +113,24 @@ __global__ void msbfs_seed_kernel(uint32_t W, uint32_t k, const uint32_t* srcs, 
 }
 
 // ------------------------------------------------------------------ SSSP
-// Lane l of the warp for vertex v owns sources 32j + l (j < W).
+// Lane l of the warp owns sources 32j + l (j < W).
 __global__ void __launch_bounds__(256)
-mssssp_pull_kernel(const uint32_t* rp, const uint32_t* col, const uint32_t* val, uint32_t n,
+mssssp_pull_kernel(const uint32_t* rp, const uint32_t* col, const uint32_t* val,
+                   const uint32_t* piece_v, const uint32_t* piece_e, uint32_t n_pieces,
                    uint32_t W, uint32_t k, uint32_t* dist, const uint32_t* chg,
                    uint32_t* chg_next, uint32_t* changed) {
     const uint32_t lane = lane_id();
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     uint32_t any = 0;
-    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+    for (uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < n_pieces; p += warps) {
+        const uint32_t v = piece_v[p];
+        const uint32_t rs = rp[v], re = rp[v + 1];
+        const bool multi = re - rs > kPieceEdges;
+        const uint32_t e0 = piece_e[p], e1 = min(e0 + kPieceEdges, re);
         uint32_t best[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) best[j] = kU32Max;
-        const uint32_t rs = rp[v], re = rp[v + 1];
-        for (uint32_t e = rs; e < re; ++e) {
+        for (uint32_t e = e0; e < e1; ++e) {
             const uint32_t u = __ldg(col + e);
             // the changed row of u (W <= 8 words) is read by every lane
             const uint32_t mine = lane < W ? __ldg(chg + (size_t)u * W + lane) : 0u;
@@ -126,8 +144,7 @@ mssssp_pull_kernel(const uint32_t* rp, const uint32_t* col, const uint32_t* val,
                 const uint32_t bits = __shfl_sync(0xffffffffu, mine, j);
                 if ((bits >> lane) & 1u) {
                     const uint32_t d = du[32 * j + lane];
-                    const uint32_t c = d + w;  // d is finite: it changed
-                    best[j] = min(best[j], c);
+                    best[j] = min(best[j], d + w);  // d is finite: it changed
                 }
             }
         }
@@ -138,18 +155,52 @@ mssssp_pull_kernel(const uint32_t* rp, const uint32_t* col, const uint32_t* val,
             const uint32_t s = 32 * j + lane;
             bool imp = false;
             if (s < k && best[j] != kU32Max) {
-                const uint32_t old = dv[s];
-                if (best[j] < old) {
-                    dv[s] = best[j];
-                    imp = true;
+                if (multi) {
+                    imp = best[j] < atomicMin(&dv[s], best[j]);
+                } else {
+                    const uint32_t old = dv[s];
+                    if (best[j] < old) {
+                        dv[s] = best[j];
+                        imp = true;
+                    }
                 }
             }
             const unsigned bits = __ballot_sync(0xffffffffu, imp);
-            if (lane == 0) chg_next[(size_t)v * W + j] = bits;
+            if (lane == 0 && bits) {
+                if (multi)
+                    atomicOr(&chg_next[(size_t)v * W + j], bits);
+                else
+                    chg_next[(size_t)v * W + j] = bits;
+            }
             any |= bits;
         }
     }
     if (any && lane == 0) atomicOr(changed, 1u);
+}
+
+// Pieces per vertex: max(1, ceil(deg / kPieceEdges)).
+__global__ void piece_count_kernel(const uint32_t* rp, uint32_t n, uint32_t* cnt) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        const uint32_t d = rp[v + 1] - rp[v];
+        cnt[v] = d == 0 ? 1u : (d + kPieceEdges - 1) / kPieceEdges;
+    }
+}
+
+__global__ void piece_fill_kernel(const uint32_t* rp, uint32_t n, const uint32_t* off,
+                                  uint32_t* piece_v, uint32_t* piece_e) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        const uint32_t rs = rp[v], re = rp[v + 1];
+        uint32_t p = off[v];
+        uint32_t e = rs;
+        do {
+            piece_v[p] = (uint32_t)v;
+            piece_e[p] = e;
+            ++p;
+            e += kPieceEdges;
+        } while (e < re);
+    }
 }
 
 __global__ void mssssp_init_kernel(uint32_t n, uint32_t W, uint32_t k, uint32_t* dist,
@@ -208,6 +259,46 @@ __global__ void map_sources_kernel(const uint32_t* in, uint32_t k, const uint32_
 
 namespace {
 
+// The in-edge CSR's row pieces, built once per graph.
+g1_status ensure_pieces(g1_graph* g, cudaStream_t s, const uint32_t** pv, const uint32_t** pe,
+                        uint32_t* np) {
+    Workspace& ws = g->ws;
+    uint32_t *cnt = nullptr, *off = nullptr, *piece_v = nullptr, *piece_e = nullptr, *tot = nullptr;
+    const uint32_t n = g->n;
+    const Orientation& o = g->o[1];
+    if (!g->pieces_ready) {
+        G1_TRY(ws.get("pc_cnt", (size_t)n + 1, &cnt));
+        G1_TRY(ws.get("pc_off", (size_t)n + 1, &off));
+        const uint32_t grid = (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
+        piece_count_kernel<<<grid, 256, 0, s>>>(o.rp, n, cnt);
+        G1_CUDA(cudaMemsetAsync(cnt + n, 0, 4, s));
+        size_t tb = 0;
+        G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, (int)n + 1, s));
+        DevBuf temp;
+        G1_TRY(temp.ensure(tb + 16));
+        G1_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, cnt, off, (int)n + 1, s));
+        uint32_t h = 0;
+        G1_CUDA(cudaMemcpyAsync(&h, off + n, 4, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaStreamSynchronize(s));
+        G1_TRY(ws.get("pc_v", (size_t)h + 1, &piece_v));
+        G1_TRY(ws.get("pc_e", (size_t)h + 1, &piece_e));
+        piece_fill_kernel<<<grid, 256, 0, s>>>(o.rp, n, off, piece_v, piece_e);
+        count_launches(2);
+        G1_CUDA(cudaGetLastError());
+        G1_CUDA(cudaStreamSynchronize(s));
+        g->n_pieces = h;
+        g->pieces_ready = true;
+    }
+    G1_TRY(ws.get("pc_v", (size_t)g->n_pieces + 1, &piece_v));
+    G1_TRY(ws.get("pc_e", (size_t)g->n_pieces + 1, &piece_e));
+    (void)tot;
+    *pv = piece_v;
+    *pe = piece_e;
+    *np = g->n_pieces;
+    return G1_OK;
+}
+
 uint32_t grid_warps(const g1_graph* g, uint64_t n) {
     const uint64_t want = ceil_div(n, 8);  // 8 warps per 256-thread block
     return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)g->sm_count * 8));
@@ -261,24 +352,28 @@ g1_status run_batch(g1_graph* g, const uint32_t* srcs_in, uint32_t k, uint32_t* 
     }
     count_launches(2);
     G1_CUDA(cudaGetLastError());
+    const uint32_t *pv = nullptr, *pe = nullptr;
+    uint32_t np = 0;
+    G1_TRY(ensure_pieces(g, s, &pv, &pe, &np));
     uint32_t it = 0;
     uint32_t* cur = a;
     uint32_t* nxt = b;
-    const uint32_t gw = grid_warps(g, n);
+    const uint32_t gw = grid_warps(g, np);
     for (;;) {
         ++it;
         if (it > n + 2) return fail(G1_ERR_TIMEOUT, "batched traversal did not converge");
         G1_CUDA(cudaMemsetAsync(flag, 0, 4, s));
+        G1_CUDA(cudaMemsetAsync(nxt, 0, (size_t)n * W * 4, s));
         if (BFS) {
             switch (W <= 1 ? 1 : W <= 2 ? 2 : W <= 4 ? 4 : 8) {
-                case 1: msbfs_pull_kernel<1><<<gw, 256, 0, s>>>(o.rp, o.col, n, W, k, cur, c, nxt, rows, it, flag); break;
-                case 2: msbfs_pull_kernel<2><<<gw, 256, 0, s>>>(o.rp, o.col, n, W, k, cur, c, nxt, rows, it, flag); break;
-                case 4: msbfs_pull_kernel<4><<<gw, 256, 0, s>>>(o.rp, o.col, n, W, k, cur, c, nxt, rows, it, flag); break;
-                default: msbfs_pull_kernel<8><<<gw, 256, 0, s>>>(o.rp, o.col, n, W, k, cur, c, nxt, rows, it, flag); break;
+                case 1: msbfs_pull_kernel<1><<<gw, 256, 0, s>>>(o.rp, o.col, pv, pe, np, W, k, cur, c, nxt, rows, it, flag); break;
+                case 2: msbfs_pull_kernel<2><<<gw, 256, 0, s>>>(o.rp, o.col, pv, pe, np, W, k, cur, c, nxt, rows, it, flag); break;
+                case 4: msbfs_pull_kernel<4><<<gw, 256, 0, s>>>(o.rp, o.col, pv, pe, np, W, k, cur, c, nxt, rows, it, flag); break;
+                default: msbfs_pull_kernel<8><<<gw, 256, 0, s>>>(o.rp, o.col, pv, pe, np, W, k, cur, c, nxt, rows, it, flag); break;
             }
         } else {
-            mssssp_pull_kernel<<<gw, 256, 0, s>>>(o.rp, o.col, static_cast<const uint32_t*>(o.val), n,
-                                                  W, k, rows, cur, nxt, flag);
+            mssssp_pull_kernel<<<gw, 256, 0, s>>>(o.rp, o.col, static_cast<const uint32_t*>(o.val), pv,
+                                                  pe, np, W, k, rows, cur, nxt, flag);
         }
         count_launches(1);
         G1_CUDA(cudaGetLastError());

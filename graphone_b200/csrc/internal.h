@@ -112,6 +112,9 @@ struct g1_graph {
     // Per-vertex sum of out-edge weights (PageRank's iweights denominator),
     // derived once per graph like the merge-path plans.
     bool outw_ready = false;
+    // Row pieces of the in-edge CSR for the batched pull kernels.
+    bool pieces_ready = false;
+    uint32_t n_pieces = 0;
     // Degree-ordered relabelling (G1_GRAPH_RELABEL): perm maps a caller's
     // vertex id to the internal id, iperm the reverse.
     bool relabeled = false;

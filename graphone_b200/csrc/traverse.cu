@@ -19,6 +19,8 @@
 //   otherwise (direction-optimising).  Final distances are the unique
 //   shortest-path distances whichever engine runs, so all three agree
 //   bit-exactly with the oracle.
+#include <cub/device/device_scan.cuh>
+
 #include <algorithm>
 
 #include "g1/semiring.cuh"
@@ -123,6 +125,43 @@ tr_advance_kernel(const uint32_t* F, uint32_t nF, const uint32_t* rp, const uint
     }
 }
 
+// Out-degrees of the frontier (deg[nF] = 0) for the edge-balanced advance.
+__global__ void tr_frontier_degrees_kernel(const uint32_t* F, uint32_t nF, const uint32_t* rp,
+                                           uint32_t* deg) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= nF; i += stride)
+        deg[i] = i < nF ? rp[F[i] + 1] - rp[F[i]] : 0u;
+}
+
+// Edge-balanced advance: the frontier's edges are numbered by the
+// exclusive prefix of its degrees; warps take 32 consecutive edge numbers and
+// each lane finds its frontier vertex by binary search, so a hub's edges are
+// spread over as many warps as the rest of the frontier's.
+template <bool UNIT>
+__global__ void __launch_bounds__(256)
+tr_advance_lb_kernel(const uint32_t* F, uint32_t nF, const uint32_t* prefix, const uint32_t* rp,
+                     const uint32_t* col, const uint32_t* val, uint32_t* dist, uint32_t* visited,
+                     uint32_t iter, uint32_t* out, uint32_t* out_count,
+                     unsigned long long* deg_sum) {
+    const uint32_t total = prefix[nF];
+    const uint32_t lane = lane_id();
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; (uint64_t)c * 32 < total;
+         c += warps) {
+        const uint32_t r = c * 32 + lane;
+        if (r >= total) continue;
+        uint32_t lo = 0, hi = nF;  // last i with prefix[i] <= r
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= r) lo = mid; else hi = mid - 1;
+        }
+        const uint32_t u = F[lo];
+        const uint32_t k = rp[u] + (r - prefix[lo]);
+        relax<UNIT>(dist[u], col[k], UNIT ? 1u : val[k], dist, visited, iter, out, out_count, rp,
+                    deg_sum);
+    }
+}
+
 struct TrState {
     uint32_t* dist;
     uint32_t* x;
@@ -130,6 +169,8 @@ struct TrState {
     uint32_t* F[2];
     uint32_t* cnt;  // [0] next frontier size, [2..3] degree sum (u64)
     uint32_t* host;  // pinned
+    uint32_t* deg;     // frontier degrees (n + 1)
+    uint32_t* prefix;  // their exclusive prefix (n + 1)
 };
 
 template <bool UNIT>
@@ -152,6 +193,12 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
     G1_TRY(ws.get("tr_f0", n, &st.F[0]));
     G1_TRY(ws.get("tr_f1", n, &st.F[1]));
     G1_TRY(ws.get("tr_cnt", 8, &st.cnt));
+    G1_TRY(ws.get("tr_deg", (size_t)n + 1, &st.deg));
+    G1_TRY(ws.get("tr_prefix", (size_t)n + 1, &st.prefix));
+    size_t scan_bytes = 0;
+    G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, st.deg, st.prefix, (int)n + 1, s));
+    unsigned char* scan_tmp = nullptr;
+    G1_TRY(ws.get("tr_scan", scan_bytes + 16, &scan_tmp));
     G1_TRY(ws.pinned.ensure(64));
     st.host = ws.pinned.as<uint32_t>();
     unsigned long long* deg_sum = reinterpret_cast<unsigned long long*>(st.cnt + 2);
@@ -184,12 +231,24 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
         const uint32_t gf = (uint32_t)std::max<uint64_t>(
             1, std::min<uint64_t>(ceil_div(nF, 256), (uint64_t)g->sm_count * 8));
         if (push) {
-            count_launches(1);
             const Orientation& o = g->o[push_t];
-            tr_advance_kernel<UNIT><<<gf, 256, 0, s>>>(st.F[cur], nF, o.rp, o.col,
-                                                       static_cast<const uint32_t*>(o.val), st.dist,
-                                                       st.visited, it, st.F[cur ^ 1], st.cnt,
-                                                       deg_sum);
+            if (o.max_deg <= 32) {  // short lists only: a thread per frontier vertex
+                count_launches(1);
+                tr_advance_kernel<UNIT><<<gf, 256, 0, s>>>(st.F[cur], nF, o.rp, o.col,
+                                                           static_cast<const uint32_t*>(o.val),
+                                                           st.dist, st.visited, it, st.F[cur ^ 1],
+                                                           st.cnt, deg_sum);
+            } else {
+                tr_frontier_degrees_kernel<<<gf, 256, 0, s>>>(st.F[cur], nF, o.rp, st.deg);
+                size_t tb = scan_bytes;
+                G1_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, tb, st.deg, st.prefix, (int)nF + 1, s));
+                const uint32_t ga = (uint32_t)std::max<uint64_t>(
+                    1, std::min<uint64_t>(ceil_div(degF, 256), (uint64_t)g->sm_count * 8));
+                tr_advance_lb_kernel<UNIT><<<ga, 256, 0, s>>>(
+                    st.F[cur], nF, st.prefix, o.rp, o.col, static_cast<const uint32_t*>(o.val),
+                    st.dist, st.visited, it, st.F[cur ^ 1], st.cnt, deg_sum);
+                count_launches(3);
+            }
         } else {
             tr_scatter_kernel<<<gf, 256, 0, s>>>(st.F[cur], nF, st.dist, st.x, 0);
             count_launches(2);
