@@ -69,6 +69,7 @@ def _declare(L):
     L.g1_spmv_plan.argtypes = [P, C.c_int, C.c_uint32, C.POINTER(C.c_uint32),
                                C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]
     L.g1_spmv.argtypes = [P, C.c_int, C.c_int, C.c_int, P, P, P]
+    L.g1_spmv_noalloc.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_int, P, P, P]
     L.g1_graph_set_schedule.argtypes = [P, C.c_int, C.c_int, C.c_int]
     L.g1_autotune.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_float), P]
     L.g1_pagerank.argtypes = [P, C.c_float, C.c_int, C.c_int, P, P]
@@ -97,7 +98,7 @@ EXPORTS = (
     "g1_count_user_launches",
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
-    "g1_spmv_plan", "g1_spmv", "g1_graph_set_schedule", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs",
+    "g1_spmv_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs",
     "g1_bfs_batch", "g1_sssp_batch",
 )
 

@@ -468,7 +468,9 @@ struct WarpMergeLayout {
 // are padded with this many zero entries): loads need no bounds checks.
 constexpr uint32_t kWarpTilePad = 1024;
 
-template <class SR, class Epi, int WARPS, int IPT, int MINB, int HOT>
+// BOUNDED: col/val loads stay inside [0, nnz) (for CSR arrays without the
+// tile padding); otherwise loads run past the tile into the padding.
+template <class SR, class Epi, int WARPS, int IPT, int MINB, int HOT, bool BOUNDED = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
 spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
@@ -521,14 +523,17 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
         W wv[IPT];
 #pragma unroll
         for (int u = 0; u < IPT; ++u) {
-            cv[u] = __ldg(colp + u * 32);
-            wv[u] = ldg_any(valp + u * 32);
+            if (!BOUNDED || (uint32_t)u < nv) {
+                cv[u] = __ldg(colp + u * 32);
+                wv[u] = ldg_any(valp + u * 32);
+            }
         }
         const uint32_t r_lane = i0 + lane;
         uint32_t ra = 0, rb = 0;
         if (r_lane <= i1) {
             ra = __ldg(a.plan.row_ptr + r_lane);
-            rb = __ldg(a.plan.row_ptr + r_lane + 1);
+            // row_ptr[n + 1] exists only in padded arrays
+            rb = (!BOUNDED || r_lane < a.plan.n_rows) ? __ldg(a.plan.row_ptr + r_lane + 1) : ra;
         }
         X xv[IPT];
 #pragma unroll
@@ -557,7 +562,7 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
             uint32_t rs = ra, re = rb;
             if (r != r_lane) {
                 rs = __ldg(a.plan.row_ptr + r);
-                re = __ldg(a.plan.row_ptr + r + 1);
+                re = (!BOUNDED || r < a.plan.n_rows) ? __ldg(a.plan.row_ptr + r + 1) : rs;
             }
             if (r == i0 && spanning) {
                 if (i1 > i0 && re == j0) a.tail[tile] = SR::identity();
