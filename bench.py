@@ -165,13 +165,118 @@ def barrier(ws: int):
 def apply_schedule(G, sched: str, stream):
     import graphone_b200 as g1
     if sched == "tune":
-        mm, vm = G.autotune(stream=stream)
-        return f"autotuned (best merge {mm:.3f} ms, vector {vm:.3f} ms)"
+        mm, vm, var = G.autotune(stream=stream)
+        pick = f"merge variant {var}" if mm <= vm else "vector"
+        return (f"autotuned: {pick} (best merge {mm:.3f} ms, vector {vm:.3f} ms)",
+                var if mm <= vm else -1)
     if sched.startswith("merge"):
-        G.set_schedule(g1.SCHED_MERGE, int(sched[5:] or 0))
-    elif sched == "vector":
+        var = int(sched[5:] or 0)
+        G.set_schedule(g1.SCHED_MERGE, var)
+        return sched, var
+    if sched == "vector":
         G.set_schedule(g1.SCHED_VECTOR)
-    return sched
+        return sched, -1
+    return sched, g1.DEFAULT_MERGE_VARIANT
+
+
+def _event_ms(fn, stream):
+    import torch
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    fn()
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b)
+
+
+def _pct(xs, q):
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q))
+
+
+def query_metrics(dev, stream, budget_queries: int = 256):
+    """The query side of the metric, on resident graphs, CUDA-event timed.
+
+    * RMAT-14 (symmetrised, uint32 weights [1,64]) plain SSSP, one source at
+      a time: latency p50/p99 over seeded non-isolated sources and GTEPS
+      (directed CSR edges of reachable vertices / median time), for the BLAS
+      (min-plus SpMV), advance/filter and push/pull engines.
+    * RMAT-20 (same shape) k=256 sources: plain engine queries/s over 64 of
+      the sources vs one batched k=256 pass (bit-exact spot checks).
+    """
+    import torch
+    import graphone_b200 as g1
+    from graphone_b200 import gen
+    out = {}
+
+    g = gen.rmat(14, 16, symmetric=True, weights=(1, 64), device=dev)
+    G = g1.Graph.from_gen(g)
+    rp = g.row_ptr.to(torch.int64)
+    deg = (rp[1:] - rp[:-1])
+    srcs = gen.pick_sources(g, budget_queries)
+    d = torch.empty(g.n, dtype=torch.int32, device=dev)
+    plain = {}
+    for name, eng in (("blas", g1.ENGINE_BLAS), ("advance", g1.ENGINE_ADVANCE),
+                      ("auto", g1.ENGINE_AUTO)):
+        for s in srcs[:8]:
+            G.sssp(int(s), eng, out=d, stream=stream)
+        lat = [_event_ms(lambda s=s: G.sssp(int(s), eng, out=d, stream=stream), stream)
+               for s in srcs]
+        G.sssp(0, eng, out=d, stream=stream)
+        torch.cuda.synchronize()
+        reach_edges = int(deg[d != -1].sum().item())
+        t0 = _event_ms(lambda: G.sssp(0, eng, out=d, stream=stream), stream)
+        plain[name] = {"p50_ms": round(_pct(lat, 50), 4), "p99_ms": round(_pct(lat, 99), 4),
+                       "queries_per_s": round(1e3 / statistics.mean(lat), 1),
+                       "src0_ms": round(t0, 4),
+                       "src0_gteps": round(reach_edges / (t0 / 1e3) / 1e9, 3)}
+    out["sssp_rmat14_plain"] = {"n": g.n, "m": g.m, "queries": len(srcs), **plain}
+    G.close()
+    del g, G, d
+    torch.cuda.empty_cache()
+
+    g = gen.rmat(20, 16, symmetric=True, weights=(1, 64), device=dev)
+    G = g1.Graph.from_gen(g)
+    srcs = gen.pick_sources(g, 256)
+    one = torch.empty(g.n, dtype=torch.int32, device=dev)
+    blk = torch.empty((256, g.n), dtype=torch.int32, device=dev)
+    res = {"n": g.n, "m": g.m, "k": 256}
+    for kind in ("bfs", "sssp"):
+        single = G.bfs if kind == "bfs" else G.sssp
+        batch = G.bfs_batch if kind == "bfs" else G.sssp_batch
+        single(int(srcs[0]), out=one, stream=stream)
+        nq = 64
+        lat = [_event_ms(lambda s=s: single(int(s), out=one, stream=stream), stream)
+               for s in srcs[:nq]]
+        batch(srcs, out=blk, stream=stream)
+        tb = _event_ms(lambda: batch(srcs, out=blk, stream=stream), stream)
+        ok = True
+        for i in (0, 100, 255):
+            single(int(srcs[i]), out=one, stream=stream)
+            torch.cuda.synchronize()
+            ok &= bool(torch.equal(one, blk[i]))
+        qp = 1e3 / statistics.mean(lat)
+        qb = 256 * 1e3 / tb
+        res[kind] = {"plain_queries_per_s": round(qp, 1), "plain_p50_ms": round(_pct(lat, 50), 4),
+                     "plain_p99_ms": round(_pct(lat, 99), 4),
+                     "batched_queries_per_s": round(qb, 1), "batched_ms_per_256": round(tb, 3),
+                     "batched_over_plain": round(qb / qp, 2), "spot_bit_exact": ok}
+    out["batch_rmat20_k256"] = res
+    G.close()
+    del g, G, one, blk
+    torch.cuda.empty_cache()
+    return out
+
+
+def kernel_name(variant: int) -> str:
+    """The SpMV kernel PageRank launches for a merge variant (-1 = vector)."""
+    if variant < 0:
+        return "spmv_vector_kernel<PlusTimesF32, PrEpilogue>"
+    from graphone_b200 import MERGE_VARIANTS
+    kind = MERGE_VARIANTS[variant]
+    base = {"warp": "spmv_wmerge_kernel", "warp_tma": "spmv_wtma_kernel",
+            "cta_tma": "spmv_merge_kernel"}[kind]
+    return f"{base}<PlusTimesF32, PrEpilogue> (merge variant {variant})"
 
 
 def run_ours(args):
@@ -201,7 +306,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     G = g1.Graph.from_csr(h_rp, h_ci, h_v, input_transpose=True, build_other=False,
                           relabel=not args.no_relabel)
-    sched_note = apply_schedule(G, args.sched, stream)
+    sched_note, variant = apply_schedule(G, args.sched, stream)
     out = torch.empty(n, dtype=torch.float32, device=dev)
     iters = args.iters
 
@@ -300,18 +405,20 @@ def run_ours(args):
             except Exception:
                 traffic = None
         result["roofline"] = {
-            "bound": "hbm", "kernel": "spmv_merge_kernel<PlusTimesF32, PrEpilogue>",
+            "bound": "hbm", "kernel": kernel_name(variant),
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_src,
             "traffic": traffic, "algorithmic_bytes_per_launch": fused_bytes(n, m),
             "avg_launch_ms": round(avg_ms, 5), "launches_timed": int(spmv_launches),
             "iteration_share_of_step": round(spmv_ms / ms, 4) if ms > 0 else None,
         }
+    G.close()
+    if not args.no_queries:
+        result["queries"] = query_metrics(dev, stream)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(trp, tci, tv, n, m, args)
     if rank == 0:
         print(json.dumps(result), flush=True)
-    G.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -423,6 +530,8 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-relabel", action="store_true")
+    ap.add_argument("--no-queries", action="store_true",
+                    help="skip the SSSP/BFS plain and batched query measurements")
     ap.add_argument("--sched", default="tune",
                     help="tune | auto | merge0..merge3 (kernel variant) | vector")
     args = ap.parse_args()

@@ -26,6 +26,13 @@ SR_MINPLUS_U32, SR_MINPLUS_F32, SR_PLUSTIMES_F32, SR_BFS_U32 = 0, 1, 2, 3
 SCHED_AUTO, SCHED_MERGE, SCHED_VECTOR = 0, 1, 2
 ENGINE_BLAS, ENGINE_ADVANCE, ENGINE_AUTO = 0, 1, 2
 PR_REFERENCE, PR_DANGLING = 0, 1
+# Kernel family of each merge-schedule variant, indexed like kMergeVariants
+# in csrc/spmv_launch.cuh: "warp" = spmv_wmerge_kernel (warp tiles, plain
+# loads), "cta_tma" = spmv_merge_kernel (CTA tiles staged by bulk copies),
+# "warp_tma" = spmv_wtma_kernel (warp tiles staged by bulk copies).
+MERGE_VARIANTS = ("warp", "warp", "warp", "cta_tma", "cta_tma", "warp",
+                  "warp_tma", "warp_tma", "warp_tma", "warp_tma")
+DEFAULT_MERGE_VARIANT = 2
 GRAPH_SYMMETRIC, GRAPH_INPUT_TRANSPOSE, GRAPH_BUILD_OTHER, GRAPH_NO_VALIDATE = 1, 2, 4, 8
 GRAPH_RELABEL = 16
 
@@ -71,12 +78,21 @@ def _declare(L):
     L.g1_spmv.argtypes = [P, C.c_int, C.c_int, C.c_int, P, P, P]
     L.g1_spmv_noalloc.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_int, P, P, P]
     L.g1_graph_set_schedule.argtypes = [P, C.c_int, C.c_int, C.c_int]
-    L.g1_autotune.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_float), P]
+    L.g1_autotune.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int), P]
     L.g1_pagerank.argtypes = [P, C.c_float, C.c_int, C.c_int, P, P]
     L.g1_sssp.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
     L.g1_bfs.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
     L.g1_bfs_batch.argtypes = [P, P, C.c_uint32, P, C.POINTER(C.c_uint32), P]
     L.g1_sssp_batch.argtypes = [P, P, C.c_uint32, P, C.POINTER(C.c_uint32), P]
+    L.g1_ppr.argtypes = [P, C.c_uint32, C.c_float, C.c_uint32, P, P]
+    L.g1_ppr_batch.argtypes = [P, P, C.c_uint32, C.c_float, C.c_uint32, P, P]
+    L.g1_server_create.argtypes = [C.c_int, C.POINTER(ServerConfig), C.POINTER(P)]
+    L.g1_server_add_graph.argtypes = [P, P, C.POINTER(C.c_uint32)]
+    L.g1_server_submit.argtypes = [P, C.c_uint32, C.c_int, C.c_uint32, P, C.POINTER(C.c_uint64)]
+    L.g1_server_poll.argtypes = [P, C.c_uint64, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.g1_server_wait.argtypes = [P, C.c_uint64, C.c_uint32, C.POINTER(C.c_double)]
+    L.g1_server_stats.argtypes = [P, C.c_int, C.POINTER(ServerStats)]
+    L.g1_server_destroy.argtypes = [P]
     return L
 
 
@@ -99,7 +115,9 @@ EXPORTS = (
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
     "g1_spmv_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs",
-    "g1_bfs_batch", "g1_sssp_batch",
+    "g1_bfs_batch", "g1_sssp_batch", "g1_ppr", "g1_ppr_batch",
+    "g1_server_create", "g1_server_add_graph", "g1_server_submit", "g1_server_poll",
+    "g1_server_wait", "g1_server_stats", "g1_server_destroy",
 )
 
 
@@ -220,9 +238,11 @@ class Graph:
         check(lib().g1_graph_set_schedule(self._h, transpose, schedule, variant))
 
     def autotune(self, stream=None):
-        a, b = C.c_float(), C.c_float()
-        check(lib().g1_autotune(self._h, C.byref(a), C.byref(b), _stream(stream)))
-        return a.value, b.value
+        """(best merge ms, vector ms, winning merge variant); the faster
+        schedule becomes the graph's G1_SCHED_AUTO choice."""
+        a, b, v = C.c_float(), C.c_float(), C.c_int()
+        check(lib().g1_autotune(self._h, C.byref(a), C.byref(b), C.byref(v), _stream(stream)))
+        return a.value, b.value, v.value
 
     def pagerank(self, alpha=0.85, iters=30, mode=PR_DANGLING, out=None, stream=None):
         if out is None:
@@ -255,9 +275,105 @@ class Graph:
         """Distances of k sources, shape (k, n), one multi-source pass."""
         return self._batch(lib().g1_sssp_batch, srcs, out, stream, return_iters)
 
+    def ppr(self, src, alpha=0.85, iters=20, out=None, stream=None):
+        """Personalized PageRank of one source (numpy float32 when out is None)."""
+        if out is None:
+            out = np.empty(self.n, np.float32)
+        check(lib().g1_ppr(self._h, src, alpha, iters, _ptr(out), _stream(stream)))
+        return out
+
+    def ppr_batch(self, srcs, alpha=0.85, iters=20, out=None, stream=None):
+        """Personalized PageRanks of k sources, shape (k, n) float32."""
+        srcs = np.ascontiguousarray(np.asarray(srcs, dtype=np.uint32))
+        k = len(srcs)
+        if out is None:
+            out = np.empty((k, self.n), np.float32)
+        check(lib().g1_ppr_batch(self._h, _ptr(srcs), k, alpha, iters, _ptr(out), _stream(stream)))
+        return out
+
     def bfs(self, src, engine=ENGINE_AUTO, out=None, stream=None, return_iters=False):
         if out is None:
             out = np.empty(self.n, np.uint32)
         it = C.c_uint32()
         check(lib().g1_bfs(self._h, src, engine, _ptr(out), C.byref(it), _stream(stream)))
         return (out, it.value) if return_iters else out
+
+
+QUERY_BFS, QUERY_SSSP, QUERY_PPR = 0, 1, 2
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("max_batch", C.c_uint32), ("reserve_bytes", C.c_uint64),
+                ("memory_limit", C.c_uint64), ("ppr_alpha", C.c_float),
+                ("ppr_iters", C.c_uint32), ("idle_release_ms", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("max_ms", C.c_double), ("queries_per_s", C.c_double), ("steps", C.c_uint64),
+                ("max_occupancy", C.c_uint32), ("engines", C.c_uint32),
+                ("device_bytes", C.c_uint64)]
+
+
+class Server:
+    """The serving loop (g1_server_*): continuous batching over resident graphs.
+
+        srv = g1.Server(max_batch=256)
+        gid = srv.add_graph(G)                      # a Graph with the in-edge CSR
+        t = srv.submit(gid, g1.QUERY_SSSP, src, out)  # out: device tensor / host array
+        srv.wait(t)                                 # latency in ms
+    """
+
+    def __init__(self, device=0, max_batch=0, reserve_bytes=0, memory_limit=0,
+                 ppr_alpha=0.0, ppr_iters=0, idle_release_ms=0):
+        cfg = ServerConfig(max_batch, reserve_bytes, memory_limit, ppr_alpha, ppr_iters,
+                           idle_release_ms)
+        h = C.c_void_p()
+        check(lib().g1_server_create(device, C.byref(cfg), C.byref(h)))
+        self._h = h.value
+        self._graphs = []  # keep the Graph objects alive while registered
+
+    def add_graph(self, graph) -> int:
+        gid = C.c_uint32()
+        check(lib().g1_server_add_graph(self._h, graph.handle, C.byref(gid)))
+        self._graphs.append(graph)
+        return gid.value
+
+    def submit(self, graph_id, kind, src, out) -> int:
+        t = C.c_uint64()
+        check(lib().g1_server_submit(self._h, graph_id, kind, src, _ptr(out), C.byref(t)))
+        return t.value
+
+    def poll(self, ticket):
+        """None while running, else the latency in ms (raises if the query failed)."""
+        done, lat = C.c_int(), C.c_double()
+        check(lib().g1_server_poll(self._h, ticket, C.byref(done), C.byref(lat)))
+        return lat.value if done.value else None
+
+    def wait(self, ticket, timeout_ms=0) -> float:
+        lat = C.c_double()
+        check(lib().g1_server_wait(self._h, ticket, timeout_ms, C.byref(lat)))
+        return lat.value
+
+    def stats(self, reset=False) -> dict:
+        st = ServerStats()
+        check(lib().g1_server_stats(self._h, 1 if reset else 0, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            check(lib().g1_server_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -755,7 +755,8 @@ g1_status g1_graph_set_schedule(g1_graph* g, int transpose, g1_schedule sched, i
     return G1_OK;
 }
 
-g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, void* stream) {
+g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, int* merge_variant,
+                      void* stream) {
     if (!g) return fail(G1_ERR_INVALID, "g1_autotune: null graph");
     DeviceGuard dg(g->device);
     std::lock_guard<std::mutex> lk(g->mu);
@@ -806,6 +807,7 @@ g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, void* stre
     }
     if (merge_ms) *merge_ms = best_merge;
     if (vector_ms) *vector_ms = vec;
+    if (merge_variant) *merge_variant = best_variant;
     return check_device_error(g, s);
 }
 

@@ -13,6 +13,8 @@
 
 namespace g1 {
 
+class SlotEngine;
+
 // Records the failure message for g1_last_error() and returns the status.
 g1_status fail(g1_status s, const std::string& msg);
 g1_status fail_cuda(cudaError_t e, const char* what);
@@ -112,9 +114,16 @@ struct g1_graph {
     // Per-vertex sum of out-edge weights (PageRank's iweights denominator),
     // derived once per graph like the merge-path plans.
     bool outw_ready = false;
-    // Row pieces of the in-edge CSR for the batched pull kernels.
+    // Row pieces of the in-edge CSR for the multi-source pull kernels, the
+    // rows with more than one piece (hubs) and the out-degrees (PPR).
     bool pieces_ready = false;
     uint32_t n_pieces = 0;
+    bool hubs_ready = false;
+    uint32_t n_hubs = 0, n_hub_pieces = 0;
+    bool outdeg_ready = false;
+    // Slot engines of the batched BFS / SSSP / PPR entry points (by kind),
+    // kept between calls.
+    std::shared_ptr<g1::SlotEngine> slot_cache[3];
     // Degree-ordered relabelling (G1_GRAPH_RELABEL): perm maps a caller's
     // vertex id to the internal id, iperm the reverse.
     bool relabeled = false;

@@ -1,0 +1,581 @@
+// Serving loop: continuous batching of BFS / SSSP / personalized-PageRank
+// queries over resident graphs.
+//
+// One host thread runs the loop.  Each (graph, query kind) pair has an
+// executor: a slot engine (slots.cuh) on its own non-blocking stream, a
+// queue of waiting queries and the queries in its slots.  A loop turn, per
+// executor whose previous step has completed (event query, no blocking):
+//   1. the queries whose results were enqueued last turn are complete;
+//   2. slots whose query finished in the last step are extracted into the
+//      queries' outputs and freed;
+//   3. waiting queries take free slots (the engine's state is allocated on
+//      first use, sized by free device memory);
+//   4. the next step (a few iterations, sized so a step takes ~0.3 ms) is
+//      launched and an event recorded behind it.
+// Executors never wait for one another, so work on different graphs and
+// kinds overlaps on the device, and a query joins a running batch at the
+// next step boundary instead of waiting for the batch to drain.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "internal.h"
+#include "slots.cuh"
+
+namespace g1 {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+constexpr double kStepTargetUs = 300.0;
+constexpr uint32_t kMaxGroup = 64;
+
+struct Request {
+    uint64_t id = 0;
+    uint32_t graph = 0;
+    int kind = 0;
+    uint32_t src = 0;
+    void* out = nullptr;
+    void* out_dev = nullptr;  // device-accessible address of out, or null (pageable)
+    Clock::time_point t_sub, t_done;
+    g1_status st = G1_OK;
+    bool done = false;
+};
+
+struct Exec {
+    g1_graph* g = nullptr;
+    int kind = 0;
+    SlotGraph sg;
+    bool usable = false;  // the graph supports this kind
+    SlotEngine eng;
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev = nullptr;
+    bool inflight = false;
+    bool stepped = false;  // the in-flight work includes a step
+    uint32_t step_iters = 0;
+    Clock::time_point t_launch, last_busy;
+    uint32_t group = 1;
+    std::deque<Request*> pending;
+    std::vector<Request*> slot_req;  // query of each slot
+    std::vector<Request*> retiring;  // results enqueued before ev
+    DevBuf staging;                  // pageable outputs
+};
+
+}  // namespace
+}  // namespace g1
+
+using namespace g1;
+
+struct g1_server {
+    int device = 0;
+    uint32_t max_batch = 256;
+    uint64_t reserve = 0, limit = 0;
+    float alpha = 0.85f;
+    uint32_t ppr_iters = 20;
+    uint32_t idle_ms = 1000;
+    std::vector<std::unique_ptr<Exec>> execs;  // graph * 3 + kind
+    std::mutex mu;                             // everything below
+    std::condition_variable cv_in, cv_done;
+    std::deque<Request*> inbox;
+    std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
+    uint64_t next_id = 1;
+    bool stop = false;
+    std::thread th;
+    std::vector<double> lat;
+    uint64_t submitted = 0, completed = 0, failed = 0, steps = 0;
+    uint32_t max_occ = 0;
+    bool have_first = false;
+    Clock::time_point t_first, t_last;
+    std::atomic<uint64_t> dev_bytes{0};
+    std::atomic<uint32_t> engines{0};
+    std::mutex graphs_mu;  // add_graph vs the loop's view of execs
+    std::atomic<size_t> n_execs{0};
+};
+
+namespace g1 {
+namespace {
+
+void complete(g1_server* S, std::vector<Request*>& rs, g1_status st) {
+    if (rs.empty()) return;
+    const auto now = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (Request* r : rs) {
+            r->st = st;
+            r->t_done = now;
+            r->done = true;
+            if (st == G1_OK) {
+                ++S->completed;
+                S->lat.push_back(std::chrono::duration<double, std::milli>(now - r->t_sub).count());
+            } else {
+                ++S->failed;
+            }
+            S->t_last = now;
+        }
+    }
+    rs.clear();
+    S->cv_done.notify_all();
+}
+
+void complete_one(g1_server* S, Request* r, g1_status st) {
+    std::vector<Request*> v{r};
+    complete(S, v, st);
+}
+
+void release_engine(g1_server* S, Exec& E) {
+    if (!E.eng.ready()) return;
+    S->dev_bytes -= E.eng.device_bytes();
+    S->engines -= 1;
+    E.eng.release();
+    E.staging.release();
+}
+
+bool idle(const Exec& E) {
+    return E.eng.ready() && E.eng.occupied() == 0 && !E.inflight && E.pending.empty() &&
+           E.retiring.empty();
+}
+
+// Frees the state of one idle engine other than `self`.
+bool release_one_idle(g1_server* S, const Exec* self) {
+    const size_t ne = S->n_execs.load();
+    for (size_t i = 0; i < ne; ++i) {
+        Exec& E = *S->execs[i];
+        if (&E != self && idle(E)) {
+            release_engine(S, E);
+            return true;
+        }
+    }
+    return false;
+}
+
+bool others_hold_memory(g1_server* S, const Exec* self) {
+    const size_t ne = S->n_execs.load();
+    for (size_t i = 0; i < ne; ++i) {
+        const Exec& E = *S->execs[i];
+        if (&E != self && E.eng.ready()) return true;
+    }
+    return false;
+}
+
+// Allocates the executor's engine: the largest slot count (halving from
+// max_batch down to 32) whose state fits the free device memory minus the
+// reserve and the server's limit.
+bool allocate(g1_server* S, Exec& E) {
+    for (uint32_t K = (S->max_batch + 31) / 32 * 32;;) {
+        const size_t need = SlotEngine::bytes(E.sg, E.kind, K);
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            free_b = 0;
+        }
+        const bool fits = need + S->reserve <= free_b && (!S->limit || S->dev_bytes + need <= S->limit);
+        if (!fits && release_one_idle(S, &E)) continue;
+        if (fits) {
+            if (E.eng.init(E.sg, E.kind, K, S->alpha, S->ppr_iters, E.s) == G1_OK) {
+                S->dev_bytes += E.eng.device_bytes();
+                S->engines += 1;
+                E.slot_req.assign(E.eng.capacity(), nullptr);
+                E.group = 1;
+                return true;
+            }
+            E.eng.release();
+            cudaGetLastError();
+        }
+        if (K <= 32) return false;
+        K = std::max<uint32_t>(32, K / 2);
+    }
+}
+
+void fail_exec(g1_server* S, Exec& E, g1_status st) {
+    std::vector<Request*> rs;
+    for (auto& r : E.slot_req)
+        if (r) {
+            rs.push_back(r);
+            r = nullptr;
+        }
+    rs.insert(rs.end(), E.retiring.begin(), E.retiring.end());
+    E.retiring.clear();
+    complete(S, rs, st);
+    E.inflight = false;
+    release_engine(S, E);
+}
+
+// Extracts the finished slots' results (enqueued on E.s).
+g1_status retire(g1_server* S, Exec& E, const std::vector<uint32_t>& fin) {
+    if (fin.empty()) return G1_OK;
+    const size_t row = (size_t)E.g->n * 4;
+    std::vector<uint32_t> ext_s;
+    std::vector<void*> ext_o;
+    std::vector<std::pair<Request*, size_t>> host;
+    for (uint32_t sl : fin) {
+        Request* r = E.slot_req[sl];
+        if (!r) continue;
+        ext_s.push_back(sl);
+        if (r->out_dev) {
+            ext_o.push_back(r->out_dev);
+        } else {
+            host.emplace_back(r, host.size());
+            ext_o.push_back(nullptr);
+        }
+    }
+    if (!host.empty()) {
+        G1_TRY(E.staging.ensure(host.size() * row + 16));
+        size_t h = 0;
+        for (size_t i = 0; i < ext_o.size(); ++i)
+            if (!ext_o[i]) ext_o[i] = E.staging.as<char>() + (h++) * row;
+    }
+    G1_TRY(E.eng.extract(ext_s.data(), (uint32_t)ext_s.size(), ext_o.data(), E.s));
+    for (auto& hr : host)
+        G1_CUDA(cudaMemcpyAsync(hr.first->out, E.staging.as<char>() + hr.second * row, row,
+                                cudaMemcpyDeviceToHost, E.s));
+    for (uint32_t sl : fin) {
+        if (E.slot_req[sl]) E.retiring.push_back(E.slot_req[sl]);
+        E.slot_req[sl] = nullptr;
+        E.eng.free_slot(sl);
+    }
+    return G1_OK;
+}
+
+// One turn of one executor; true if anything happened.
+bool service(g1_server* S, Exec& E, bool stopping, std::vector<uint32_t>& fin) {
+    bool progress = false;
+    if (E.inflight) {
+        const cudaError_t q = cudaEventQuery(E.ev);
+        if (q == cudaErrorNotReady) return false;
+        progress = true;
+        E.inflight = false;
+        if (q != cudaSuccess) {
+            cudaGetLastError();
+            fail_exec(S, E, G1_ERR_DEVICE);
+            return true;
+        }
+        complete(S, E.retiring, G1_OK);
+        if (E.stepped) {
+            const double us = std::chrono::duration<double, std::micro>(Clock::now() - E.t_launch).count();
+            const double per_it = us / std::max<uint32_t>(1, E.step_iters);
+            E.group = (uint32_t)std::min<double>(kMaxGroup, std::max(1.0, kStepTargetUs / std::max(per_it, 1.0)));
+            E.eng.finished(&fin);
+            if (retire(S, E, fin) != G1_OK) {
+                fail_exec(S, E, G1_ERR_DEVICE);
+                return true;
+            }
+            // a traversal that ran longer than any shortest path can
+            for (uint32_t i = 0; i < E.eng.capacity() && E.kind != kSlotPpr; ++i)
+                if (E.slot_req[i] && E.eng.slot_iterations(i) > E.g->n + 2) {
+                    complete_one(S, E.slot_req[i], G1_ERR_TIMEOUT);
+                    E.slot_req[i] = nullptr;
+                    E.eng.free_slot(i);
+                }
+        }
+    }
+    // admission
+    if (!stopping && !E.pending.empty()) {
+        if (!E.eng.ready() && !allocate(S, E) && !others_hold_memory(S, &E)) {
+            std::vector<Request*> rs(E.pending.begin(), E.pending.end());
+            E.pending.clear();
+            complete(S, rs, G1_ERR_OOM);
+            progress = true;
+        }
+        if (E.eng.ready()) {
+            std::vector<uint32_t> adm_s, adm_v;
+            while (!E.pending.empty()) {
+                const int sl = E.eng.take_slot();
+                if (sl < 0) break;
+                Request* r = E.pending.front();
+                E.pending.pop_front();
+                E.slot_req[sl] = r;
+                adm_s.push_back((uint32_t)sl);
+                adm_v.push_back(r->src);
+            }
+            if (!adm_s.empty()) {
+                progress = true;
+                if (E.eng.admit(adm_s.data(), adm_v.data(), (uint32_t)adm_s.size(), E.s) != G1_OK) {
+                    fail_exec(S, E, G1_ERR_DEVICE);
+                    return true;
+                }
+            }
+        }
+    }
+    E.stepped = false;
+    if (E.eng.ready() && E.eng.occupied() > 0) {
+        E.step_iters = E.eng.max_step(E.group);
+        if (E.eng.step(E.step_iters, E.s) != G1_OK) {
+            fail_exec(S, E, G1_ERR_DEVICE);
+            return true;
+        }
+        E.stepped = true;
+        E.t_launch = Clock::now();
+        std::lock_guard<std::mutex> lk(S->mu);
+        ++S->steps;
+        S->max_occ = std::max(S->max_occ, E.eng.occupied());
+    }
+    if (E.stepped || !E.retiring.empty()) {
+        if (cudaEventRecord(E.ev, E.s) != cudaSuccess) {
+            cudaGetLastError();
+            fail_exec(S, E, G1_ERR_DEVICE);
+            return true;
+        }
+        E.inflight = true;
+        E.last_busy = Clock::now();
+        progress = true;
+    }
+    return progress;
+}
+
+bool busy(const Exec& E) { return E.inflight || E.eng.occupied() > 0 || !E.pending.empty(); }
+
+void loop(g1_server* S) {
+    cudaSetDevice(S->device);
+    std::vector<Request*> fresh;
+    std::vector<uint32_t> fin;
+    for (;;) {
+        bool stopping = false;
+        bool any_busy = false;
+        const size_t ne = S->n_execs.load();
+        for (size_t i = 0; i < ne; ++i) any_busy |= busy(*S->execs[i]);
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            if (S->inbox.empty() && !any_busy && !S->stop)
+                S->cv_in.wait_for(lk, std::chrono::milliseconds(20));
+            fresh.assign(S->inbox.begin(), S->inbox.end());
+            S->inbox.clear();
+            stopping = S->stop;
+        }
+        for (Request* r : fresh) S->execs[(size_t)r->graph * 3 + r->kind]->pending.push_back(r);
+        if (stopping) {
+            std::vector<Request*> rs;
+            for (size_t i = 0; i < ne; ++i) {
+                Exec& E = *S->execs[i];
+                rs.insert(rs.end(), E.pending.begin(), E.pending.end());
+                E.pending.clear();
+            }
+            complete(S, rs, G1_ERR_INVALID);
+        }
+        bool progress = false;
+        for (size_t i = 0; i < ne; ++i) progress |= service(S, *S->execs[i], stopping, fin);
+        const auto now = Clock::now();
+        bool still = false;
+        for (size_t i = 0; i < ne; ++i) {
+            Exec& E = *S->execs[i];
+            still |= busy(E) || !E.retiring.empty();
+            if (idle(E) &&
+                std::chrono::duration<double, std::milli>(now - E.last_busy).count() > S->idle_ms)
+                release_engine(S, E);
+        }
+        if (stopping && !still) break;
+        if (!progress && still) std::this_thread::sleep_for(std::chrono::microseconds(10));
+    }
+    for (size_t i = 0; i < S->n_execs.load(); ++i) release_engine(S, *S->execs[i]);
+}
+
+g1_status server_status_of(const Request& r) { return r.st; }
+
+}  // namespace
+}  // namespace g1
+
+extern "C" g1_status g1_server_create(int device, const g1_server_config* cfg, g1_server** out) {
+    if (!out) return fail(G1_ERR_INVALID, "g1_server_create: null output");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return fail(G1_ERR_INVALID, "g1_server_create: no such device");
+    }
+    std::unique_ptr<g1_server> S(new g1_server());
+    S->device = device;
+    if (cfg) {
+        if (cfg->max_batch > kMaxSlots) return fail(G1_ERR_INVALID, "max_batch above 256");
+        if (cfg->max_batch) S->max_batch = cfg->max_batch;
+        S->reserve = cfg->reserve_bytes;
+        S->limit = cfg->memory_limit;
+        if (cfg->ppr_alpha != 0.0f) {
+            if (!(cfg->ppr_alpha > 0.0f && cfg->ppr_alpha < 1.0f))
+                return fail(G1_ERR_INVALID, "ppr_alpha must be in (0, 1)");
+            S->alpha = cfg->ppr_alpha;
+        }
+        if (cfg->ppr_iters) S->ppr_iters = cfg->ppr_iters;
+        if (cfg->idle_release_ms) S->idle_ms = cfg->idle_release_ms;
+    }
+    // executors for up to 4096 graphs; the vector never reallocates
+    S->execs.reserve(3 * 4096);
+    S->th = std::thread(loop, S.get());
+    *out = S.release();
+    return G1_OK;
+}
+
+extern "C" g1_status g1_server_add_graph(g1_server* S, g1_graph* g, uint32_t* graph_id) {
+    if (!S || !g || !graph_id) return fail(G1_ERR_INVALID, "g1_server_add_graph: null argument");
+    if (g->device != S->device) return fail(G1_ERR_INVALID, "graph lives on another device");
+    if (!g->o[1].present)
+        return fail(G1_ERR_UNSUPPORTED, "serving needs the in-edge CSR (G1_GRAPH_BUILD_OTHER)");
+    std::lock_guard<std::mutex> add_lk(S->graphs_mu);
+    const size_t ne = S->n_execs.load();
+    if (ne + 3 > S->execs.capacity()) return fail(G1_ERR_INVALID, "too many graphs");
+    DeviceGuard dg(g->device);
+    std::unique_ptr<Exec> ex[3];
+    for (int kind = 0; kind < 3; ++kind) {
+        ex[kind].reset(new Exec());
+        Exec& E = *ex[kind];
+        E.g = g;
+        E.kind = kind;
+        G1_CUDA(cudaStreamCreateWithFlags(&E.s, cudaStreamNonBlocking));
+        G1_CUDA(cudaEventCreateWithFlags(&E.ev, cudaEventDisableTiming));
+        E.last_busy = Clock::now();
+        if (kind == kSlotSssp && g->vtype != G1_U32) continue;
+        std::lock_guard<std::mutex> lk(g->mu);
+        G1_TRY(slot_graph(g, kind, E.s, &E.sg));
+        E.usable = true;
+    }
+    // the loop only reads execs[0, n_execs)
+    for (auto& e : ex) S->execs.push_back(std::move(e));
+    *graph_id = (uint32_t)(ne / 3);
+    S->n_execs.store(ne + 3);
+    return G1_OK;
+}
+
+extern "C" g1_status g1_server_submit(g1_server* S, uint32_t graph_id, g1_query_kind kind, uint32_t src,
+                                      void* out, uint64_t* ticket) {
+    if (!S || !out || !ticket) return fail(G1_ERR_INVALID, "g1_server_submit: null argument");
+    if ((size_t)graph_id * 3 + 3 > S->n_execs.load()) return fail(G1_ERR_INVALID, "unknown graph id");
+    if (kind < G1_QUERY_BFS || kind > G1_QUERY_PPR) return fail(G1_ERR_INVALID, "unknown query kind");
+    Exec& E = *S->execs[(size_t)graph_id * 3 + kind];
+    if (!E.usable) return fail(G1_ERR_INVALID, "SSSP needs u32 edge weights");
+    if (src >= E.g->n) return fail(G1_ERR_INVALID, "source vertex out of range");
+    std::unique_ptr<Request> r(new Request());
+    r->graph = graph_id;
+    r->kind = kind;
+    r->src = src;
+    r->out = out;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, out) == cudaSuccess) {
+        if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged)
+            r->out_dev = out;
+        else if (a.type == cudaMemoryTypeHost && a.devicePointer)
+            r->out_dev = a.devicePointer;
+    } else {
+        cudaGetLastError();
+    }
+    r->t_sub = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->stop) return fail(G1_ERR_INVALID, "server is stopping");
+        r->id = S->next_id++;
+        *ticket = r->id;
+        S->inbox.push_back(r.get());
+        if (!S->have_first) {
+            S->have_first = true;
+            S->t_first = r->t_sub;
+        }
+        ++S->submitted;
+        S->reqs.emplace(r->id, std::move(r));
+    }
+    S->cv_in.notify_one();
+    return G1_OK;
+}
+
+static g1_status take_result(g1_server* S, uint64_t ticket, double* latency_ms) {
+    auto it = S->reqs.find(ticket);
+    const Request& r = *it->second;
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r.t_done - r.t_sub).count();
+    const g1_status st = server_status_of(r);
+    S->reqs.erase(it);
+    if (st != G1_OK) return fail(st, "query failed in the serving loop");
+    return G1_OK;
+}
+
+extern "C" g1_status g1_server_poll(g1_server* S, uint64_t ticket, int* done, double* latency_ms) {
+    if (!S || !done) return fail(G1_ERR_INVALID, "g1_server_poll: null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(ticket);
+    if (it == S->reqs.end()) return fail(G1_ERR_INVALID, "unknown ticket");
+    *done = it->second->done ? 1 : 0;
+    if (!*done) return G1_OK;
+    return take_result(S, ticket, latency_ms);
+}
+
+extern "C" g1_status g1_server_wait(g1_server* S, uint64_t ticket, uint32_t timeout_ms, double* latency_ms) {
+    if (!S) return fail(G1_ERR_INVALID, "g1_server_wait: null server");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(ticket);
+    if (it == S->reqs.end()) return fail(G1_ERR_INVALID, "unknown ticket");
+    Request* r = it->second.get();
+    auto ready = [&] { return r->done; };
+    if (timeout_ms) {
+        if (!S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
+            return fail(G1_ERR_TIMEOUT, "query not done within the timeout");
+    } else {
+        S->cv_done.wait(lk, ready);
+    }
+    return take_result(S, ticket, latency_ms);
+}
+
+extern "C" g1_status g1_server_stats(g1_server* S, int reset, g1_server_metrics* out) {
+    if (!S || !out) return fail(G1_ERR_INVALID, "g1_server_stats: null argument");
+    std::memset(out, 0, sizeof(*out));
+    std::vector<double> lat;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        lat = S->lat;
+        out->submitted = S->submitted;
+        out->completed = S->completed;
+        out->failed = S->failed;
+        out->steps = S->steps;
+        out->max_occupancy = S->max_occ;
+        if (S->have_first && S->completed) {
+            const double s = std::chrono::duration<double>(S->t_last - S->t_first).count();
+            out->queries_per_s = s > 0 ? (double)S->completed / s : 0.0;
+        }
+        if (reset) {
+            S->lat.clear();
+            S->submitted = S->completed = S->failed = S->steps = 0;
+            S->max_occ = 0;
+            S->have_first = false;
+        }
+    }
+    out->engines = S->engines.load();
+    out->device_bytes = S->dev_bytes.load();
+    if (!lat.empty()) {
+        std::sort(lat.begin(), lat.end());
+        auto pct = [&](double q) {
+            const double pos = q * (double)(lat.size() - 1);
+            const size_t i = (size_t)pos;
+            const double f = pos - (double)i;
+            return i + 1 < lat.size() ? lat[i] * (1.0 - f) + lat[i + 1] * f : lat[i];
+        };
+        out->p50_ms = pct(0.50);
+        out->p99_ms = pct(0.99);
+        double sum = 0;
+        for (double x : lat) sum += x;
+        out->mean_ms = sum / (double)lat.size();
+        out->max_ms = lat.back();
+    }
+    return G1_OK;
+}
+
+extern "C" g1_status g1_server_destroy(g1_server* S) {
+    if (!S) return G1_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+    }
+    S->cv_in.notify_all();
+    if (S->th.joinable()) S->th.join();
+    {
+        DeviceGuard dg(S->device);
+        for (auto& e : S->execs) {
+            if (e->s) cudaStreamSynchronize(e->s);
+            if (e->ev) cudaEventDestroy(e->ev);
+            if (e->s) cudaStreamDestroy(e->s);
+        }
+    }
+    delete S;
+    return G1_OK;
+}

@@ -166,9 +166,11 @@ g1_status g1_spmv_noalloc(const uint32_t* row_ptr, const uint32_t* col, const vo
                           uint32_t n, uint32_t m, g1_semiring sr, const void* x, void* y,
                           void* stream);
 /* Times the merge schedule at each tile size and the CSR-vector schedule on
- * this graph and keeps the fastest for G1_SCHED_AUTO.  Results in ms (may be
- * NULL): the best merge time and the vector time. */
-g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, void* stream);
+ * this graph and keeps the fastest for G1_SCHED_AUTO.  Results (may be
+ * NULL): the best merge time and the vector time in ms, the winning merge
+ * variant. */
+g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, int* merge_variant,
+                      void* stream);
 
 /* ------------------------------------------------------------- algorithms */
 /* PageRank for a fixed iteration count (Run<PRFunctor> over
@@ -190,13 +192,83 @@ g1_status g1_bfs(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* level_ou
 /* k sources as one multi-source pass (no GraphOne counterpart: GraphOne
  * runs one source per Run, apps/sssp_blas.cu:87-136).  srcs: k vertex ids
  * (host or device); out: k*n u32 in source-major order (out[s*n + v]) --
- * the layout of k g1_bfs / g1_sssp calls, and bit-identical to them.  More
- * than 256 sources run as consecutive passes of 256.  Needs the in-edge CSR.
- * iters_out: iterations of the longest pass (may be NULL). */
+ * the layout of k g1_bfs / g1_sssp calls, and bit-identical to them.  Up to
+ * 256 sources iterate together; when one finishes, the next source takes its
+ * slot while the others keep iterating.  Needs the in-edge CSR.
+ * iters_out: iterations of the longest query (may be NULL). */
 g1_status g1_bfs_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, uint32_t* levels_out,
                        uint32_t* iters_out, void* stream);
 g1_status g1_sssp_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, uint32_t* dist_out,
                         uint32_t* iters_out, void* stream);
+
+/* Personalized PageRank of src (no GraphOne app; the pagerank_blas
+ * iteration, apps/pagerank_blas.cu:86-125, restarted at src): rank starts as
+ * the indicator of src and `iters` times
+ *     rank'[v] = sum_{u->v} rank[u] * alpha / outdeg(u)
+ *                + [v == src] * ((1 - alpha) + alpha * sum_{outdeg(u)=0} rank[u]).
+ * Transition weights are 1/out-degree (edge values are not used).  fp32,
+ * bit-identical whether run alone, batched or served.  rank_out: n f32, host
+ * or device.  Needs the in-edge CSR. */
+g1_status g1_ppr(g1_graph* g, uint32_t src, float alpha, uint32_t iters, float* rank_out,
+                 void* stream);
+/* k personalized PageRanks, rank_out: k*n f32 source-major. */
+g1_status g1_ppr_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, float alpha, uint32_t iters,
+                       float* rank_out, void* stream);
+
+/* --------------------------------------------------------- serving loop */
+/* A request loop (one host thread, one CUDA stream per graph and query
+ * kind) over resident graphs.  Queries on the same graph and of the same
+ * kind share a multi-source engine of up to max_batch slots; a query is
+ * admitted into a free slot between two iterations of the engine and its
+ * result is written as soon as its own traversal completes, while the rest
+ * of the batch keeps running (continuous batching).  Engines of different
+ * graphs / kinds run concurrently on their own streams.  An engine's state
+ * is allocated when its first query arrives, sized by the free device
+ * memory (slots halve until it fits, down to 32; otherwise queries wait
+ * for memory to be released), and released after idle_release_ms without
+ * queries.  No GraphOne counterpart. */
+typedef struct g1_server g1_server;
+typedef enum { G1_QUERY_BFS = 0, G1_QUERY_SSSP = 1, G1_QUERY_PPR = 2 } g1_query_kind;
+typedef struct {
+    uint32_t max_batch;       /* slots per engine, 1..256 (rounded up to 32s); 0 = 256 */
+    uint64_t reserve_bytes;   /* device memory admission leaves free */
+    uint64_t memory_limit;    /* cap on engine state bytes; 0 = none */
+    float ppr_alpha;          /* PPR damping; 0 = 0.85 */
+    uint32_t ppr_iters;       /* PPR iterations; 0 = 20 */
+    uint32_t idle_release_ms; /* release idle engine state after this; 0 = 1000 */
+} g1_server_config;
+typedef struct {
+    uint64_t submitted, completed, failed;
+    double p50_ms, p99_ms, mean_ms, max_ms; /* latency: submit -> result written */
+    double queries_per_s;                   /* completed / (last completion - first submit) */
+    uint64_t steps;                         /* engine steps launched */
+    uint32_t max_occupancy;                 /* most slots busy in one engine step */
+    uint32_t engines;                       /* engines holding device state now */
+    uint64_t device_bytes;                  /* their device bytes */
+} g1_server_metrics;
+
+/* cfg may be NULL (defaults). */
+g1_status g1_server_create(int device, const g1_server_config* cfg, g1_server** out);
+/* Registers a resident graph (not owned; it must outlive the server and must
+ * not be destroyed while registered).  Needs the in-edge CSR. */
+g1_status g1_server_add_graph(g1_server* srv, g1_graph* g, uint32_t* graph_id);
+/* Queues one query; returns at once.  out: n u32 (BFS levels, SSSP
+ * distances) or n f32 (PPR ranks) -- device memory, pinned host memory or
+ * pageable host memory (slowest); it must stay valid until the query is
+ * done. */
+g1_status g1_server_submit(g1_server* srv, uint32_t graph_id, g1_query_kind kind, uint32_t src,
+                           void* out, uint64_t* ticket);
+/* done = 1 once the result is written; then returns the query's status and
+ * forgets the ticket.  latency_ms may be NULL. */
+g1_status g1_server_poll(g1_server* srv, uint64_t ticket, int* done, double* latency_ms);
+/* Blocks until the query is done (G1_ERR_TIMEOUT after timeout_ms; 0 = no
+ * limit), then behaves like g1_server_poll. */
+g1_status g1_server_wait(g1_server* srv, uint64_t ticket, uint32_t timeout_ms, double* latency_ms);
+/* Latency percentiles over the queries completed since creation or the
+ * last reset (reset != 0 clears them after reading). */
+g1_status g1_server_stats(g1_server* srv, int reset, g1_server_metrics* out);
+/* Stops the loop: queued queries fail, running ones finish first. */
+g1_status g1_server_destroy(g1_server* srv);
 
 #ifdef __cplusplus
 }

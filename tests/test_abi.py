@@ -40,3 +40,15 @@ def test_status_strings_and_argument_errors_without_gpu():
     assert st == 1
     assert L.g1_sssp(None, 0, 0, None, None, None) == 1
     assert L.g1_pagerank(None, C.c_float(0.85), 30, 1, None, None) == 1
+
+
+def test_python_variant_table_matches_the_launcher():
+    src = open(os.path.join(ROOT, "graphone_b200", "csrc", "spmv_launch.cuh")).read()
+    n = int(re.search(r"kNumMergeVariants\s*=\s*(\d+)", src).group(1))
+    d = int(re.search(r"kDefaultVariant\s*=\s*(\d+)", src).group(1))
+    table = re.search(r"kMergeVariants\[\]\s*=\s*\{(.*?)\};", src, re.S).group(1)
+    kinds = [int(k) for k in re.findall(r"\{\s*(\d+)\s*,", table)]
+    names = {0: "warp", 1: "cta_tma", 2: "warp_tma"}
+    assert len(g1.MERGE_VARIANTS) == n == len(kinds)
+    assert tuple(names[k] for k in kinds) == g1.MERGE_VARIANTS
+    assert g1.DEFAULT_MERGE_VARIANT == d

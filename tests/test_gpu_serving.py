@@ -1,0 +1,237 @@
+"""Personalized PageRank, continuous multi-source batching and the serving
+loop (g1_ppr*, g1_server_*) against the oracle and against themselves:
+every query's result is the same alone, in a batch and in the served mix.
+
+Tolerances: BFS levels and SSSP distances bit-exact (u32); PPR within 1e-6
+relative L1 of the FP64 oracle, and bit-identical between the alone /
+batched / served runs (the per-slot arithmetic is fixed)."""
+import threading
+import time
+
+import numpy as np
+import pytest
+import torch
+
+import graphone_b200 as g1
+from graphone_b200 import gen
+from oracle import oracle as O
+from tests.gpu_util import edge_case_graphs
+
+pytestmark = pytest.mark.gpu
+
+GRAPHS = edge_case_graphs()
+PPR_TOL = 1e-6
+
+
+def ppr_oracle(g, src, alpha=0.85, iters=20):
+    trp, tci, _ = g.np("t")
+    return O.ppr_f64(trp, tci, np.ones(len(tci), np.float32), src, alpha, iters)
+
+
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+def test_ppr_matches_fp64_oracle(cuda, name):
+    g = GRAPHS[name]
+    G = g1.Graph.from_gen(g)
+    for src in sorted({0, g.n // 2, g.n - 1}):
+        r = G.ppr(src, 0.85, 20)
+        ref = ppr_oracle(g, src)
+        assert O.rel_l1(r, ref) < PPR_TOL, (name, src)
+
+
+def test_ppr_zero_iterations_is_the_indicator(cuda):
+    g = GRAPHS["rmat10_sym"]
+    G = g1.Graph.from_gen(g)
+    r = G.ppr(5, 0.85, 0)
+    e = np.zeros(g.n, np.float32)
+    e[5] = 1.0
+    assert np.array_equal(r, e)
+
+
+@pytest.mark.parametrize("name", ["rmat11_dir", "star20k", "grid32", "path3000"])
+@pytest.mark.parametrize("k", [1, 37, 300])
+def test_ppr_batch_bit_identical_to_single(cuda, name, k):
+    g = GRAPHS[name]
+    G = g1.Graph.from_gen(g)
+    rng = np.random.default_rng(k)
+    srcs = rng.integers(0, g.n, size=k).astype(np.uint32)
+    batch = G.ppr_batch(srcs, 0.85, 20)
+    for i in sorted({0, k // 2, k - 1}):
+        one = G.ppr(int(srcs[i]), 0.85, 20)
+        assert np.array_equal(batch[i], one), (name, k, i)
+    assert O.rel_l1(batch[k - 1], ppr_oracle(g, int(srcs[k - 1]))) < PPR_TOL
+
+
+def test_ppr_batch_device_output_and_relabelled_graph(cuda):
+    g = gen.rmat(12, 16, True, (1, 100))
+    G = g1.Graph.from_gen(g, relabel=True)
+    srcs = gen.pick_sources(g, 40)
+    out = torch.empty((40, g.n), dtype=torch.float32, device="cuda")
+    G.ppr_batch(srcs, 0.85, 20, out=out)
+    torch.cuda.synchronize()
+    host = out.cpu().numpy()
+    for i in (0, 39):
+        assert O.rel_l1(host[i], ppr_oracle(g, int(srcs[i]))) < PPR_TOL
+
+
+def test_ppr_rejects_bad_damping(cuda):
+    G = g1.Graph.from_gen(GRAPHS["rmat10_sym"])
+    with pytest.raises(g1.G1Error):
+        G.ppr(0, 1.5, 20)
+
+
+# ----------------------------------------------------------------- serving
+
+def serving_graphs():
+    """Small stand-ins for the serving mix: RMAT graphs and grids with
+    uint32 weights in [1, 100]."""
+    return [gen.rmat(10, 16, True, (1, 100)), gen.rmat(12, 16, True, (1, 100)),
+            gen.grid2d(24, 24, (1, 100)), gen.grid2d(40, 17, (1, 100))]
+
+
+def request_mix(graphs, count, seed):
+    """(graph index, kind, source): 60% SSSP, 25% BFS, 15% PPR, graph and
+    source uniform."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        gi = int(rng.integers(0, len(graphs)))
+        u = rng.random()
+        kind = g1.QUERY_SSSP if u < 0.60 else (g1.QUERY_BFS if u < 0.85 else g1.QUERY_PPR)
+        out.append((gi, kind, int(rng.integers(0, graphs[gi].n))))
+    return out
+
+
+def alone(G, kind, src):
+    if kind == g1.QUERY_SSSP:
+        return G.sssp(src).view(np.uint32)
+    if kind == g1.QUERY_BFS:
+        return G.bfs(src).view(np.uint32)
+    return G.ppr(src, 0.85, 20)
+
+
+def check_against_oracle(g, kind, src, res):
+    rp, ci, v = g.np("n")
+    if kind == g1.QUERY_SSSP:
+        assert np.array_equal(res.view(np.uint32), O.dijkstra_u32(rp, ci, v, src))
+    elif kind == g1.QUERY_BFS:
+        assert np.array_equal(res.view(np.uint32), O.bfs(rp, ci, src))
+    else:
+        assert O.rel_l1(res.view(np.float32), ppr_oracle(g, src)) < PPR_TOL
+
+
+def host_out(g, kind):
+    return np.empty(g.n, np.float32 if kind == g1.QUERY_PPR else np.uint32)
+
+
+@pytest.mark.parametrize("max_batch", [32, 256])
+def test_served_mix_equals_each_query_alone(cuda, max_batch):
+    graphs = serving_graphs()
+    Gs = [g1.Graph.from_gen(g) for g in graphs]
+    reqs = request_mix(graphs, 400, seed=max_batch)
+    with g1.Server(max_batch=max_batch) as srv:
+        gids = [srv.add_graph(G) for G in Gs]
+        outs = [host_out(graphs[gi], kind) for gi, kind, _ in reqs]
+        # arrivals in waves, so later queries join batches already running
+        tickets = []
+        for i, (gi, kind, src) in enumerate(reqs):
+            tickets.append(srv.submit(gids[gi], kind, src, outs[i]))
+            if i % 50 == 49:
+                time.sleep(0.002)
+        lat = [srv.wait(t, 60000) for t in tickets]
+        st = srv.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
+    assert st["max_occupancy"] > 1  # queries did share engine steps
+    assert all(x > 0 for x in lat)
+    for i, (gi, kind, src) in enumerate(reqs):
+        ref = alone(Gs[gi], kind, src)
+        assert np.array_equal(outs[i].view(np.uint32), ref.view(np.uint32)), (i, gi, kind, src)
+    for i in range(0, len(reqs), 37):
+        gi, kind, src = reqs[i]
+        check_against_oracle(graphs[gi], kind, src, outs[i])
+
+
+def test_served_device_and_pinned_outputs(cuda):
+    g = gen.rmat(11, 16, True, (1, 100))
+    G = g1.Graph.from_gen(g)
+    srcs = gen.pick_sources(g, 64)
+    dev = torch.empty((64, g.n), dtype=torch.int32, device="cuda")
+    pin = torch.empty((64, g.n), dtype=torch.int32).pin_memory()
+    with g1.Server() as srv:
+        gid = srv.add_graph(G)
+        ts = [srv.submit(gid, g1.QUERY_SSSP, int(s), dev[i]) for i, s in enumerate(srcs)]
+        ts += [srv.submit(gid, g1.QUERY_BFS, int(s), pin[i]) for i, s in enumerate(srcs)]
+        for t in ts:
+            srv.wait(t, 60000)
+    torch.cuda.synchronize()
+    d = dev.cpu().numpy().view(np.uint32)
+    p = pin.numpy().view(np.uint32)
+    for i in (0, 31, 63):
+        assert np.array_equal(d[i], G.sssp(int(srcs[i])))
+        assert np.array_equal(p[i], G.bfs(int(srcs[i])))
+
+
+def test_admission_by_memory_limit(cuda):
+    """A memory limit below one 256-slot engine: the engines shrink to fit
+    and queries wait for memory; every result is still exact."""
+    graphs = serving_graphs()[:2]
+    Gs = [g1.Graph.from_gen(g) for g in graphs]
+    n_max = max(g.n for g in graphs)
+    limit = 4 * n_max * 64 * 4  # room for engines of about 32-64 slots
+    reqs = request_mix(graphs, 200, seed=7)
+    with g1.Server(max_batch=256, memory_limit=limit, idle_release_ms=1) as srv:
+        gids = [srv.add_graph(G) for G in Gs]
+        outs = [host_out(graphs[gi], kind) for gi, kind, _ in reqs]
+        ts = [srv.submit(gids[gi], kind, src, outs[i]) for i, (gi, kind, src) in enumerate(reqs)]
+        for t in ts:
+            srv.wait(t, 60000)
+        st = srv.stats()
+    assert st["completed"] == len(reqs)
+    assert st["max_occupancy"] <= 64
+    for i, (gi, kind, src) in enumerate(reqs):
+        assert np.array_equal(outs[i].view(np.uint32), alone(Gs[gi], kind, src).view(np.uint32))
+
+
+def test_server_rejects_bad_requests(cuda):
+    g = GRAPHS["rmat10_sym"]
+    G = g1.Graph.from_gen(g)
+    gf = gen.rmat(9, 8, False, float_values=True)
+    Gf = g1.Graph.from_gen(gf)
+    out = np.empty(g.n, np.uint32)
+    with g1.Server() as srv:
+        gid = srv.add_graph(G)
+        fid = srv.add_graph(Gf)
+        with pytest.raises(g1.G1Error):
+            srv.submit(gid + 5, g1.QUERY_BFS, 0, out)
+        with pytest.raises(g1.G1Error):
+            srv.submit(gid, g1.QUERY_BFS, g.n, out)
+        with pytest.raises(g1.G1Error):
+            srv.submit(fid, g1.QUERY_SSSP, 0, out)  # SSSP needs u32 weights
+        with pytest.raises(g1.G1Error):
+            srv.poll(12345)
+        t = srv.submit(gid, g1.QUERY_BFS, 0, out)
+        srv.wait(t, 60000)
+    assert np.array_equal(out, O.bfs(*g.np("n")[:2], 0))
+
+
+def test_concurrent_submitters(cuda):
+    """Queries from several host threads; results as alone."""
+    g = gen.rmat(11, 16, True, (1, 100))
+    G = g1.Graph.from_gen(g)
+    srcs = gen.pick_sources(g, 96)
+    outs = np.empty((96, g.n), np.uint32)
+    with g1.Server(max_batch=64) as srv:
+        gid = srv.add_graph(G)
+
+        def worker(lo, hi):
+            ts = [srv.submit(gid, g1.QUERY_SSSP, int(srcs[i]), outs[i]) for i in range(lo, hi)]
+            for t in ts:
+                srv.wait(t, 60000)
+
+        th = [threading.Thread(target=worker, args=(i * 24, i * 24 + 24)) for i in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+    for i in (0, 50, 95):
+        assert np.array_equal(outs[i], G.sssp(int(srcs[i])))

@@ -139,3 +139,15 @@ def test_pagerank_every_merge_variant(cuda, variant):
     trp, tci, tv = g.np("t")
     r = G.pagerank(0.85, 20, g1.PR_DANGLING)
     assert O.rel_l1(r, O.pagerank_f64(trp, tci, tv, 0.85, 20, 1)) < 1e-6
+
+
+@pytest.mark.parametrize("relabel", [False, True])
+def test_autotune_picks_a_variant_and_keeps_parity(cuda, relabel):
+    g = gen.rmat(14, 16, False, float_values=True)
+    G = g1.Graph.from_gen(g, relabel=relabel)
+    merge_ms, vector_ms, variant = G.autotune()
+    assert 0 <= variant < len(g1.MERGE_VARIANTS)
+    assert merge_ms > 0 and vector_ms > 0
+    trp, tci, tv = g.np("t")
+    r = G.pagerank(0.85, 20, g1.PR_DANGLING)
+    assert O.rel_l1(r, O.pagerank_f64(trp, tci, tv, 0.85, 20, 1)) < 1e-6
