@@ -268,6 +268,109 @@ def query_metrics(dev, stream, budget_queries: int = 256):
     return out
 
 
+SERVING_GRAPHS = (("rmat", 16), ("rmat", 18), ("rmat", 20), ("rmat", 22),
+                  ("grid", 512), ("grid", 1024), ("grid", 2048), ("grid", 4096))
+
+
+def serving_metrics(dev, n_requests: int, rate: float, seed: int = 20261203):
+    """Serving loop over 8 resident graphs (RMAT 16/18/20/22 symmetrised and
+    4-neighbour grids 512^2 .. 4096^2, uint32 weights in [1, 100]).
+
+    Requests: Poisson arrivals at `rate` per second, graph uniform, 60% SSSP
+    / 25% BFS / 15% personalized PageRank (fp32, damping 0.85, 20
+    iterations), source uniform over the graph's non-isolated vertices,
+    results into device buffers.  The same request stream is then run as
+    plain per-request execution (the single-source entry points, one at a
+    time in arrival order, a request starting when it has arrived and the
+    previous one has finished).  Latency = result written - arrival.
+    """
+    import torch
+    import graphone_b200 as g1
+    from graphone_b200 import gen
+    rng = np.random.default_rng(seed)
+    graphs, cands = [], []
+    for kind, size in SERVING_GRAPHS:
+        g = (gen.rmat(size, 16, symmetric=True, weights=(1, 100), device=dev) if kind == "rmat"
+             else gen.grid2d(size, size, (1, 100), device=dev))
+        cands.append(torch.nonzero(g.out_degree() > 0).flatten().cpu().numpy())
+        graphs.append(g1.Graph.from_gen(g))
+        del g
+    torch.cuda.empty_cache()
+    reqs = []
+    t = 0.0
+    for _ in range(n_requests):
+        t += rng.exponential(1.0 / rate)
+        gi = int(rng.integers(0, len(graphs)))
+        u = rng.random()
+        q = g1.QUERY_SSSP if u < 0.60 else (g1.QUERY_BFS if u < 0.85 else g1.QUERY_PPR)
+        src = int(cands[gi][rng.integers(0, len(cands[gi]))])
+        reqs.append((t, gi, q, src))
+    outs = [torch.empty(graphs[gi].n, dtype=torch.float32 if q == g1.QUERY_PPR else torch.int32,
+                        device=dev) for _, gi, q, _ in reqs]
+    # served
+    with g1.Server(max_batch=256) as srv:
+        gids = [srv.add_graph(G) for G in graphs]
+        # one warm-up query per engine kind and graph (state allocation)
+        for gi, G in enumerate(graphs):
+            for q in (g1.QUERY_SSSP, g1.QUERY_BFS, g1.QUERY_PPR):
+                w = torch.empty(G.n, dtype=torch.int32, device=dev)
+                srv.wait(srv.submit(gids[gi], q, int(cands[gi][0]), w), 600000)
+        srv.stats(reset=True)
+        t0 = time.perf_counter()
+        tickets = []
+        for i, (ta, gi, q, src) in enumerate(reqs):
+            now = time.perf_counter() - t0
+            if ta > now:
+                time.sleep(ta - now)
+            tickets.append(srv.submit(gids[gi], q, src, outs[i]))
+        for tk in tickets:
+            srv.wait(tk, 0)
+        st = srv.stats()
+    served = {"p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+              "mean_ms": round(st["mean_ms"], 3), "queries_per_s": round(st["queries_per_s"], 1),
+              "engine_steps": int(st["steps"]), "max_slots_busy": int(st["max_occupancy"])}
+    # plain per-request execution of the same stream
+    one = {gi: torch.empty(G.n, dtype=torch.int32, device=dev) for gi, G in enumerate(graphs)}
+    onef = {gi: torch.empty(G.n, dtype=torch.float32, device=dev) for gi, G in enumerate(graphs)}
+
+    def run_plain(gi, q, src):
+        G = graphs[gi]
+        if q == g1.QUERY_SSSP:
+            G.sssp(src, out=one[gi])
+            return one[gi]
+        if q == g1.QUERY_BFS:
+            G.bfs(src, out=one[gi])
+            return one[gi]
+        G.ppr(src, 0.85, 20, out=onef[gi])
+        return onef[gi]
+
+    for gi in range(len(graphs)):
+        for q in (g1.QUERY_SSSP, g1.QUERY_BFS, g1.QUERY_PPR):
+            run_plain(gi, q, int(cands[gi][0]))
+    torch.cuda.synchronize()
+    lat, end, same = [], 0.0, True
+    for i, (ta, gi, q, src) in enumerate(reqs):
+        start = max(ta, end)
+        t1 = time.perf_counter()
+        r = run_plain(gi, q, src)
+        torch.cuda.synchronize()
+        end = start + (time.perf_counter() - t1)
+        lat.append((end - ta) * 1e3)
+        if i % 16 == 0:
+            same &= bool(torch.equal(r.view(torch.int32), outs[i].view(torch.int32)))
+    plain = {"p50_ms": round(_pct(lat, 50), 3), "p99_ms": round(_pct(lat, 99), 3),
+             "mean_ms": round(float(np.mean(lat)), 3),
+             "queries_per_s": round(len(reqs) / (end - reqs[0][0]), 1)}
+    for G in graphs:
+        G.close()
+    torch.cuda.empty_cache()
+    return {"graphs": [f"{k}{s}" for k, s in SERVING_GRAPHS], "requests": len(reqs),
+            "offered_rate_per_s": rate, "mix": "60% SSSP / 25% BFS / 15% PPR",
+            "served": served, "plain_per_request": plain,
+            "served_over_plain_qps": round(served["queries_per_s"] / max(plain["queries_per_s"], 1e-9), 2),
+            "spot_bit_identical": same}
+
+
 def kernel_name(variant: int) -> str:
     """The SpMV kernel PageRank launches for a merge variant (-1 = vector)."""
     if variant < 0:
@@ -415,6 +518,8 @@ def run_ours(args):
     G.close()
     if not args.no_queries:
         result["queries"] = query_metrics(dev, stream)
+    if args.serve_requests > 0:
+        result["serving"] = serving_metrics(dev, args.serve_requests, args.serve_rate)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(trp, tci, tv, n, m, args)
     if rank == 0:
@@ -532,6 +637,10 @@ def main():
     ap.add_argument("--no-relabel", action="store_true")
     ap.add_argument("--no-queries", action="store_true",
                     help="skip the SSSP/BFS plain and batched query measurements")
+    ap.add_argument("--serve-requests", type=int, default=256,
+                    help="requests of the serving-loop measurement (0 = skip)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0,
+                    help="offered request rate (Poisson arrivals per second)")
     ap.add_argument("--sched", default="tune",
                     help="tune | auto | merge0..merge3 (kernel variant) | vector")
     args = ap.parse_args()

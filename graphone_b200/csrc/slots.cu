@@ -873,8 +873,14 @@ g1_status SlotEngine::admit(const uint32_t* slots, const uint32_t* srcs, uint32_
     const uint32_t grid = (uint32_t)std::max<uint64_t>(
         1, std::min<uint64_t>(ceil_div(std::max<uint64_t>(work, (uint64_t)sg_.n * W_), 256),
                               (uint64_t)sg_.sm_count * 16));
-    slot_reset_kernel<<<grid, 256, 0, s>>>(sg_.n, K_, W_, cnt, d + kDevAdmSlots, init, rows,
-                                           kind_ == kSlotBfs ? seen_.as<uint32_t>() : nullptr, amask);
+    if (cnt == K_) {
+        // every slot: whole rows (init is a repeated byte)
+        G1_CUDA(cudaMemsetAsync(rows, init ? 0xFF : 0, (size_t)sg_.n * K_ * 4, s));
+        if (kind_ == kSlotBfs) G1_CUDA(cudaMemsetAsync(seen_.p, 0, (size_t)sg_.n * W_ * 4, s));
+    } else {
+        slot_reset_kernel<<<grid, 256, 0, s>>>(sg_.n, K_, W_, cnt, d + kDevAdmSlots, init, rows,
+                                               kind_ == kSlotBfs ? seen_.as<uint32_t>() : nullptr, amask);
+    }
     // seeds count as changed by iteration it_ and feed iteration it_ + 1's list
     Frontier f;
     std::memset(&f, 0, sizeof(f));
