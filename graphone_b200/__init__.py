@@ -29,10 +29,11 @@ PR_REFERENCE, PR_DANGLING = 0, 1
 # Kernel family of each merge-schedule variant, indexed like kMergeVariants
 # in csrc/spmv_launch.cuh: "warp" = spmv_wmerge_kernel (warp tiles, plain
 # loads), "cta_tma" = spmv_merge_kernel (CTA tiles staged by bulk copies),
-# "warp_tma" = spmv_wtma_kernel (warp tiles staged by bulk copies).
+# "warp_tma" = spmv_wtma_kernel (warp tiles staged by bulk copies), "nnz" =
+# spmv_nnz_kernel (nnz-split warp tiles, 16-byte loads, row-start bitmap).
 MERGE_VARIANTS = ("warp", "warp", "warp", "cta_tma", "cta_tma", "warp",
-                  "warp_tma", "warp_tma", "warp_tma", "warp_tma")
-DEFAULT_MERGE_VARIANT = 2
+                  "warp_tma", "warp_tma", "warp_tma", "warp_tma", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz")
+DEFAULT_MERGE_VARIANT = 17
 GRAPH_SYMMETRIC, GRAPH_INPUT_TRANSPOSE, GRAPH_BUILD_OTHER, GRAPH_NO_VALIDATE = 1, 2, 4, 8
 GRAPH_RELABEL = 16
 

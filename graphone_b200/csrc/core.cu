@@ -419,6 +419,94 @@ g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out) {
     return G1_OK;
 }
 
+// ------------------------------------------------------------- nnz plan
+
+__global__ void nnz_flag_kernel(const uint32_t* rp, uint32_t n, uint32_t* flag) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride)
+        flag[r] = rp[r + 1] > rp[r] ? 1u : 0u;
+}
+
+// Non-empty rows to rows[rank], empty rows after them; start bits of the
+// non-empty rows' first nonzeros.
+__global__ void nnz_place_kernel(const uint32_t* rp, uint32_t n, const uint32_t* rank,
+                                 uint32_t n_nonempty, uint32_t* rows, uint32_t* sbits) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+        const uint32_t k = rank[r];
+        if (rp[r + 1] > rp[r]) {
+            rows[k] = (uint32_t)r;
+            atomicOr(&sbits[rp[r] >> 5], 1u << (rp[r] & 31));
+        } else {
+            rows[n_nonempty + ((uint32_t)r - k)] = (uint32_t)r;
+        }
+    }
+}
+
+// tile_seg[t] = rank of the row holding nonzero t*tile (the last row r with
+// rp[r] <= t*tile; it is non-empty); n_nonempty past the last nonzero.
+__global__ void nnz_tile_seg_kernel(const uint32_t* rp, uint32_t n, uint32_t nnz, const uint32_t* rank,
+                                    uint32_t n_nonempty, uint32_t n_tiles, uint32_t tile,
+                                    uint32_t* tile_seg) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > n_tiles) return;
+    const uint64_t k = (uint64_t)t * tile;
+    if (k >= nnz) {
+        tile_seg[t] = n_nonempty;
+        return;
+    }
+    uint32_t lo = 0, hi = n;  // last r in [0, n) with rp[r] <= k
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (rp[mid] <= k) lo = mid; else hi = mid - 1;
+    }
+    tile_seg[t] = rank[lo];
+}
+
+g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
+    Orientation& o = g->o[t];
+    if (!o.present) return fail(G1_ERR_UNSUPPORTED, "orientation not built");
+    Orientation& owner = (t == 1 && g->symmetric && g->o[0].present) ? g->o[0] : o;
+    if (owner.nnz_plan) {
+        *out = owner.nnz_plan.get();
+        return G1_OK;
+    }
+    const uint32_t n = g->n, m = g->m;
+    std::unique_ptr<NnzPlan> p(new NnzPlan());
+    p->n_tiles = (uint32_t)ceil_div(m, kNnzTile);
+    const size_t words = (size_t)p->n_tiles * (kNnzTile / 32) + 1 + 16;
+    G1_TRY(p->tile_seg.ensure(((size_t)p->n_tiles + 1) * 4 + 16));
+    G1_TRY(p->sbits.ensure(words * 4));
+    G1_TRY(p->rows.ensure(((size_t)n + 1) * 4));
+    G1_TRY(p->carry.ensure(((size_t)p->n_tiles + 1) * 16));
+    G1_TRY(p->tail.ensure(((size_t)p->n_tiles + 1) * 16));
+    DevBuf flag, rank, temp;
+    G1_TRY(flag.ensure(((size_t)n + 1) * 4));
+    G1_TRY(rank.ensure(((size_t)n + 1) * 4));
+    const uint32_t grid = grid_for(n, 256, g->sm_count);
+    G1_CUDA(cudaMemset(p->sbits.p, 0, words * 4));
+    G1_CUDA(cudaMemset(flag.p, 0, ((size_t)n + 1) * 4));
+    nnz_flag_kernel<<<grid, 256>>>(o.rp, n, flag.as<uint32_t>());
+    size_t tb = 0;
+    G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag.as<uint32_t>(), rank.as<uint32_t>(), (int)n + 1));
+    G1_TRY(temp.ensure(tb + 16));
+    G1_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, flag.as<uint32_t>(), rank.as<uint32_t>(), (int)n + 1));
+    uint32_t nne = 0;
+    G1_CUDA(cudaMemcpy(&nne, rank.as<uint32_t>() + n, 4, cudaMemcpyDeviceToHost));
+    p->n_nonempty = nne;
+    p->n_empty = n - nne;
+    nnz_place_kernel<<<grid, 256>>>(o.rp, n, rank.as<uint32_t>(), nne, p->rows.as<uint32_t>(),
+                                    p->sbits.as<uint32_t>());
+    nnz_tile_seg_kernel<<<(uint32_t)ceil_div((uint64_t)p->n_tiles + 1, 256), 256>>>(
+        o.rp, n, m, rank.as<uint32_t>(), nne, p->n_tiles, kNnzTile, p->tile_seg.as<uint32_t>());
+    count_launches(3);
+    G1_CUDA(cudaGetLastError());
+    G1_CUDA(cudaDeviceSynchronize());
+    *out = p.get();
+    owner.nnz_plan = std::move(p);
+    return G1_OK;
+}
+
 g1_status to_caller_order(g1_graph* g, uint32_t* dev_out, const uint32_t* internal,
                           cudaStream_t s) {
     gather_perm_kernel<<<grid_for(g->n, 256, g->sm_count), 256, 0, s>>>(

@@ -68,6 +68,14 @@ struct MergePlan {
     DevBuf tile_row, tile_nnz, carry, tail;
 };
 
+// nnz-split plan of one orientation (tiles of 256 nonzeros): rank of the
+// row holding each tile's first nonzero, the row-start bitmap over the
+// nonzeros, the non-empty rows in order followed by the empty rows.
+struct NnzPlan {
+    uint32_t n_tiles = 0, n_nonempty = 0, n_empty = 0;
+    DevBuf tile_seg, sbits, rows, carry, tail;
+};
+
 struct Orientation {
     bool present = false;
     uint32_t* rp = nullptr;
@@ -78,6 +86,7 @@ struct Orientation {
     std::map<uint32_t, std::unique_ptr<MergePlan>> plans;  // by items per tile
     int tuned_sched = 0;  // 0 = not tuned, else g1_schedule
     int tuned_variant = -1;  // merge kernel variant chosen by g1_autotune (-1 = default)
+    std::unique_ptr<NnzPlan> nnz_plan;
 };
 
 // Named, growable workspaces of one graph.
@@ -154,6 +163,7 @@ bool is_device_ptr(const void* p);
 g1_status copy_out(void* dst, const void* dev_src, size_t bytes, cudaStream_t s);
 
 g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out);
+g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out);
 // Vertex-order conversions of a relabelled graph (4-byte values).
 g1_status to_caller_order(g1_graph* g, uint32_t* dev_out, const uint32_t* internal, cudaStream_t s);
 g1_status to_internal_order(g1_graph* g, uint32_t* dev_out, const uint32_t* caller, cudaStream_t s);

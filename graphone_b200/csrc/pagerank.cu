@@ -71,9 +71,13 @@ struct PrEpilogue {
         base = dangling ? (float)((double)base0 + alpha_over_n * (*dang_in)) : base0;
     }
     __device__ __forceinline__ void emit(uint32_t v, const float& y) {
+        emit_prepared(v, y, prepare(v));
+    }
+    // iweights[v] does not depend on the row's value: loaded ahead
+    __device__ __forceinline__ float prepare(uint32_t v) const { return __ldg(iw + v); }
+    __device__ __forceinline__ void emit_prepared(uint32_t v, const float& y, float w) {
         const float r = base + y;
         rank_next[v] = r;
-        const float w = __ldg(iw + v);
         x_next[v] = r * w;
         if (dangling && w == 0.0f) dang_local += (double)r;
     }

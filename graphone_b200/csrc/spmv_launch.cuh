@@ -17,8 +17,12 @@ constexpr int kVectorBlock = 256;
 //   kind 0: warp tiles of 32*ipt items loaded into registers,
 //   kind 1: block tiles of 256*ipt items staged by TMA bulk copies
 //           (`stages` staging buffers),
-//   kind 2: warp tiles staged by per-warp TMA bulk copies.
-// `warps` per block (kind 0/2), `hot` x entries cached in shared memory,
+//   kind 2: warp tiles staged by per-warp TMA bulk copies,
+//   kind 3: nnz-split warp tiles of 256 nonzeros (16-byte loads, row-start
+//           bitmap; its own plan instead of the merge-path partition);
+//           stages: bit 0 = L2 cache policies, bit 1 = three-tile software
+//           pipeline per warp.
+// `warps` per block (kind 0/2/3), `hot` x entries cached in shared memory,
 // `minb` resident blocks per SM the register budget is sized for.
 struct MergeVariant {
     int kind;
@@ -32,9 +36,13 @@ constexpr MergeVariant kMergeVariants[] = {
     {0, 11, 0, 8, 0, 3},      {0, 7, 0, 8, 0, 4},       {0, 7, 0, 32, 16384, 1},
     {1, 7, 2, 8, 0, 4},       {1, 7, 1, 8, 0, 6},       {0, 11, 0, 32, 16384, 1},
     {2, 15, 0, 24, 16384, 1}, {2, 31, 0, 16, 0, 1},     {2, 15, 0, 32, 0, 1},
-    {2, 23, 0, 16, 16384, 1}};
-constexpr int kNumMergeVariants = 10;
-constexpr int kDefaultVariant = 2;
+    {2, 23, 0, 16, 16384, 1}, {3, 8, 0, 32, 16384, 1},  {3, 8, 0, 16, 16384, 2},
+    {3, 8, 0, 32, 0, 1},      {3, 8, 1, 32, 16384, 1},  {3, 8, 1, 16, 16384, 2},
+    {3, 8, 1, 16, 8192, 3},   {3, 8, 0, 16, 8192, 3},   {3, 8, 0, 32, 32768, 1},
+    {3, 8, 0, 32, 49152, 1},  {3, 8, 2, 24, 32768, 1},  {3, 8, 2, 16, 32768, 1},
+    {3, 8, 3, 24, 32768, 1}};
+constexpr int kNumMergeVariants = 22;
+constexpr int kDefaultVariant = 17;
 
 template <class K>
 int blocks_per_sm(K kernel, int block, size_t smem) {
@@ -109,6 +117,28 @@ struct WarpMergeKernel {
     }
 };
 
+template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false>
+struct NnzKernel {
+    using L = NnzLayout<SR, WARPS, HOT>;
+    static int occupancy() {
+        static int occ = [] {
+            auto k = spmv_nnz_kernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
+            return blocks_per_sm(k, WARPS * 32, L::BYTES);
+        }();
+        return occ;
+    }
+    static uint32_t grid(const g1_graph* g, uint32_t n_tiles) {
+        const uint64_t want = ceil_div(n_tiles, WARPS);
+        return (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(want, (uint64_t)g->sm_count * occupancy()));
+    }
+};
+
+inline uint32_t nnz_fix_grid(const NnzPlan& p) {
+    return (uint32_t)std::max<uint64_t>(1, ceil_div(std::max(p.n_tiles, p.n_empty), kMergeBlock));
+}
+
 // Per-instantiation launch facts of the merge kernel.
 template <class SR, class Epi, int IPT, int STAGES>
 struct MergeKernel {
@@ -154,11 +184,70 @@ MergeArgs<SR> merge_args(const g1_graph* g, int t, const MergePlan& p, const typ
     return a;
 }
 
+template <class SR>
+NnzArgs<SR> nnz_args(const g1_graph* g, int t, const NnzPlan& p, const typename SR::x_t* x) {
+    const Orientation& o = g->o[t];
+    NnzArgs<SR> a;
+    a.plan.n_rows = g->n;
+    a.plan.nnz = g->m;
+    a.plan.n_tiles = p.n_tiles;
+    a.plan.n_nonempty = p.n_nonempty;
+    a.plan.n_empty = p.n_empty;
+    a.plan.tile_seg = p.tile_seg.as<uint32_t>();
+    a.plan.sbits = p.sbits.as<uint32_t>();
+    a.plan.nz_rows = p.rows.as<uint32_t>();
+    a.plan.empty_rows = p.rows.as<uint32_t>() + p.n_nonempty;
+    a.col = o.col;
+    a.val = static_cast<const typename SR::w_t*>(o.val);
+    a.x = x;
+    a.carry = p.carry.as<typename SR::value_t>();
+    a.tail = p.tail.as<typename SR::value_t>();
+    return a;
+}
+
+template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false>
+g1_status launch_nnz(g1_graph* g, int t, const NnzPlan& p, const typename SR::x_t* x,
+                     const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
+    using K = NnzKernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE>;
+    const NnzArgs<SR> a = nnz_args<SR>(g, t, p, x);
+    const bool prof = profiling();
+    // launched even without tiles: its blocks' epilogue partials are read
+    if (prof) prof_mark(s, true);
+    spmv_nnz_kernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE>
+        <<<K::grid(g, p.n_tiles), WARPS * 32, K::L::BYTES, s>>>(a, main_epi);
+    if (prof) prof_mark(s, false);
+    count_launches(1);
+    spmv_nnz_fixup_kernel<SR, Epi, kMergeBlock><<<nnz_fix_grid(p), kMergeBlock, 0, s>>>(a, fix_epi);
+    count_launches(1);
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
+}
+
 // Grid sizes of the merge schedule (main, fixup) for the orientation's
 // current tile size; builds the plan if needed.
 template <class SR, class Epi>
 g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_grid) {
     const int v = merge_variant(g, t);
+    if (kMergeVariants[v].kind == 3) {
+        NnzPlan* q = nullptr;
+        G1_TRY(ensure_nnz_plan(g, t, &q));
+        switch (v) {
+            case 11: *main_grid = NnzKernel<SR, Epi, 16, 2, 16384>::grid(g, q->n_tiles); break;
+            case 12: *main_grid = NnzKernel<SR, Epi, 32, 1, 0>::grid(g, q->n_tiles); break;
+            case 13: *main_grid = NnzKernel<SR, Epi, 32, 1, 16384, true>::grid(g, q->n_tiles); break;
+            case 14: *main_grid = NnzKernel<SR, Epi, 16, 2, 16384, true>::grid(g, q->n_tiles); break;
+            case 15: *main_grid = NnzKernel<SR, Epi, 16, 3, 8192, true>::grid(g, q->n_tiles); break;
+            case 16: *main_grid = NnzKernel<SR, Epi, 16, 3, 8192>::grid(g, q->n_tiles); break;
+            case 17: *main_grid = NnzKernel<SR, Epi, 32, 1, 32768>::grid(g, q->n_tiles); break;
+            case 18: *main_grid = NnzKernel<SR, Epi, 32, 1, 49152>::grid(g, q->n_tiles); break;
+            case 19: *main_grid = NnzKernel<SR, Epi, 24, 1, 32768, false, true>::grid(g, q->n_tiles); break;
+            case 20: *main_grid = NnzKernel<SR, Epi, 16, 1, 32768, false, true>::grid(g, q->n_tiles); break;
+            case 21: *main_grid = NnzKernel<SR, Epi, 24, 1, 32768, true, true>::grid(g, q->n_tiles); break;
+            default: *main_grid = NnzKernel<SR, Epi, 32, 1, 16384>::grid(g, q->n_tiles); break;
+        }
+        *fix_grid = nnz_fix_grid(*q);
+        return G1_OK;
+    }
     MergePlan* p = nullptr;
     G1_TRY(ensure_plan(g, t, merge_items(v), &p));
     switch (v) {
@@ -236,6 +325,24 @@ template <class SR, class Epi>
 g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi& main_epi,
                        const Epi& fix_epi, cudaStream_t s) {
     const int v = merge_variant(g, t);
+    if (kMergeVariants[v].kind == 3) {
+        NnzPlan* q = nullptr;
+        G1_TRY(ensure_nnz_plan(g, t, &q));
+        switch (v) {
+            case 11: return launch_nnz<SR, Epi, 16, 2, 16384>(g, t, *q, x, main_epi, fix_epi, s);
+            case 12: return launch_nnz<SR, Epi, 32, 1, 0>(g, t, *q, x, main_epi, fix_epi, s);
+            case 13: return launch_nnz<SR, Epi, 32, 1, 16384, true>(g, t, *q, x, main_epi, fix_epi, s);
+            case 14: return launch_nnz<SR, Epi, 16, 2, 16384, true>(g, t, *q, x, main_epi, fix_epi, s);
+            case 15: return launch_nnz<SR, Epi, 16, 3, 8192, true>(g, t, *q, x, main_epi, fix_epi, s);
+            case 16: return launch_nnz<SR, Epi, 16, 3, 8192>(g, t, *q, x, main_epi, fix_epi, s);
+            case 17: return launch_nnz<SR, Epi, 32, 1, 32768>(g, t, *q, x, main_epi, fix_epi, s);
+            case 18: return launch_nnz<SR, Epi, 32, 1, 49152>(g, t, *q, x, main_epi, fix_epi, s);
+            case 19: return launch_nnz<SR, Epi, 24, 1, 32768, false, true>(g, t, *q, x, main_epi, fix_epi, s);
+            case 20: return launch_nnz<SR, Epi, 16, 1, 32768, false, true>(g, t, *q, x, main_epi, fix_epi, s);
+            case 21: return launch_nnz<SR, Epi, 24, 1, 32768, true, true>(g, t, *q, x, main_epi, fix_epi, s);
+            default: return launch_nnz<SR, Epi, 32, 1, 16384>(g, t, *q, x, main_epi, fix_epi, s);
+        }
+    }
     MergePlan* p = nullptr;
     G1_TRY(ensure_plan(g, t, merge_items(v), &p));
     if (p->n_tiles == 0) return G1_OK;

@@ -176,6 +176,39 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // ------------------------------------------------------- ceil division
+// ------------------------------------------ L2 cache policies and hints
+
+// Access policies for ld ...L2::cache_hint: streamed data is evicted first,
+// gathered data that is reused (x vectors) last.
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// 16-byte read-only load with an L2 policy.
+__device__ __forceinline__ uint4 ldg_v4_policy(const void* ptr, uint64_t pol) {
+    uint4 r;
+    asm("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+        : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+        : "l"(ptr), "l"(pol));
+    return r;
+}
+// 4-byte read-only load with an L2 policy.
+__device__ __forceinline__ uint32_t ldg_u32_policy(const void* ptr, uint64_t pol) {
+    uint32_t r;
+    asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(r) : "l"(ptr), "l"(pol));
+    return r;
+}
+// Brings the line holding `p` into L2 ahead of use.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 __host__ __device__ __forceinline__ uint64_t ceil_div(uint64_t a, uint64_t b) {
     return (a + b - 1) / b;
 }

@@ -37,6 +37,9 @@
 //   __device__ void emit(uint32_t row, const value_t& v);
 //   template <int BLOCK> __device__ void block_end(char* smem);  // all threads, once
 
+#include <type_traits>
+#include <utility>
+
 #include "g1/common.cuh"
 
 namespace g1 {
@@ -932,6 +935,371 @@ spmv_fixup_kernel(MergeArgs<SR> a, Epi epi) {
         part = shfl_any(0xffffffffu, part, 0);  // the fold's total sits in lane 0
         if ((int)lane == src) epi.emit(i0, SR::reduce(part, acc));
     }
+    epi.template block_end<BLOCK>(epi_smem);
+}
+
+// ------------------------------------------------------ nnz-split tiles
+//
+// Tile t covers the nonzeros [t*256, (t+1)*256): lane l of the tile's warp
+// folds the 8 consecutive nonzeros from t*256 + 8l, read with two 16-byte
+// loads of col and two of val.  Row starts come from a bitmap over the
+// nonzeros (bit k: nonzero k is the first of its row), so a lane finds its
+// segment boundaries with one word load and no search; rows are numbered by
+// their rank among the non-empty rows.  Per tile:
+//   1. lane-local fold of the 8 products; every segment that starts and ends
+//      inside the lane is stored (by its number within the tile) in shared
+//      memory; the lane keeps its head (items before its first start) and
+//      its tail (items from its last start);
+//   2. a warp segmented scan of the tails joins segments that cross lanes;
+//   3. the tile's complete rows are emitted in row order, 32 at a time
+//      (coalesced row-id loads and epilogue stores);
+//   4. a row open at the tile end leaves its partial in carry[t]; the part
+//      of a row begun in an earlier tile goes to tail[t]; empty rows and
+//      rows that cross tiles are finished by spmv_nnz_fixup_kernel.
+// Work per tile is exactly 256 nonzeros whatever the degree distribution;
+// empty rows cost nothing here.
+
+constexpr uint32_t kNnzIpt = 8;
+constexpr uint32_t kNnzTile = 32 * kNnzIpt;
+
+struct NnzPlanView {
+    uint32_t n_rows;
+    uint32_t nnz;
+    uint32_t n_tiles;   // ceil(nnz / 256)
+    uint32_t n_nonempty;
+    uint32_t n_empty;
+    const uint32_t* tile_seg;    // n_tiles + 1: rank of the row holding nonzero t*256
+    const uint32_t* sbits;       // row-start bitmap, zero-padded to n_tiles*8 + 1 words
+    const uint32_t* nz_rows;     // non-empty rows in order
+    const uint32_t* empty_rows;  // n_empty
+};
+
+template <class SR>
+struct NnzArgs {
+    NnzPlanView plan;
+    const uint32_t* col;          // padded by at least kNnzTile entries
+    const typename SR::w_t* val;  // padded likewise
+    const typename SR::x_t* x;
+    typename SR::value_t* carry;  // n_tiles: partial of the row open at the tile end
+    typename SR::value_t* tail;   // n_tiles: in-tile partial of a row begun earlier
+};
+
+// Epilogues may split emit into prepare(row) -- the loads that depend only
+// on the row, issued before the row's value is known -- and
+// emit_prepared(row, value, prepared).
+template <class E, class = void>
+struct has_prepare : std::false_type {};
+template <class E>
+struct has_prepare<E, std::void_t<decltype(std::declval<E&>().prepare(0u))>> : std::true_type {};
+
+template <class SR, int WARPS, int HOT>
+struct NnzLayout {
+    using V = typename SR::value_t;
+    using X = typename SR::x_t;
+    static constexpr size_t XC_OFF = 0;
+    static constexpr size_t XC_BYTES = ((size_t)HOT * sizeof(X) + 15) / 16 * 16;
+    static constexpr size_t SY_OFF = XC_OFF + XC_BYTES;
+    static constexpr size_t SY_BYTES = ((size_t)WARPS * kNnzTile * sizeof(V) + 15) / 16 * 16;
+    static constexpr size_t EPI_OFF = SY_OFF + SY_BYTES;
+    static constexpr size_t BYTES = EPI_OFF + 512;
+};
+
+template <class E, bool = has_prepare<E>::value>
+struct prepared_type {
+    using type = int;
+};
+template <class E>
+struct prepared_type<E, true> {
+    using type = decltype(std::declval<E&>().prepare(0u));
+};
+
+// Stage 1 of a tile: its 16-byte col/val loads and bitmap / plan words.
+struct NnzIn {
+    uint4 c0, c1, v0, v1;
+    uint32_t sw, endw, seg0;
+};
+
+// Stage 2: x gathered, rows the tile may emit (and their epilogue loads)
+// requested.
+template <class SR, class Epi>
+struct NnzReady {
+    typename SR::x_t x[kNnzIpt];
+    uint32_t v[kNnzIpt];
+    uint32_t sw, endw, seg_base, row_pre;
+    typename prepared_type<Epi>::type pre;
+};
+
+template <class SR, bool HINTS>
+__device__ __forceinline__ NnzIn nnz_load(const NnzArgs<SR>& a, uint32_t tile, uint64_t pol_stream) {
+    const uint32_t lane = lane_id();
+    const uint32_t j0 = tile * kNnzTile;
+    const uint32_t jl = j0 + lane * kNnzIpt;
+    NnzIn in;
+    if constexpr (HINTS) {
+        in.c0 = ldg_v4_policy(a.col + jl, pol_stream);
+        in.c1 = ldg_v4_policy(a.col + jl + 4, pol_stream);
+        in.v0 = ldg_v4_policy(a.val + jl, pol_stream);
+        in.v1 = ldg_v4_policy(a.val + jl + 4, pol_stream);
+    } else {
+        in.c0 = __ldg(reinterpret_cast<const uint4*>(a.col + jl));
+        in.c1 = __ldg(reinterpret_cast<const uint4*>(a.col + jl + 4));
+        in.v0 = __ldg(reinterpret_cast<const uint4*>(a.val + jl));
+        in.v1 = __ldg(reinterpret_cast<const uint4*>(a.val + jl + 4));
+    }
+    in.sw = __ldg(a.plan.sbits + (j0 >> 5) + (lane >> 2));
+    in.endw = __ldg(a.plan.sbits + ((j0 + kNnzTile) >> 5));
+    in.seg0 = __ldg(a.plan.tile_seg + tile);
+    return in;
+}
+
+template <class SR, class Epi, int HOT, bool HINTS>
+__device__ __forceinline__ NnzReady<SR, Epi> nnz_gather(const NnzArgs<SR>& a, const NnzIn& in,
+                                                        const typename SR::x_t* xc, uint32_t hot,
+                                                        uint64_t pol_keep, Epi& epi) {
+    using X = typename SR::x_t;
+    const uint32_t lane = lane_id();
+    NnzReady<SR, Epi> r;
+    const uint32_t cc[kNnzIpt] = {in.c0.x, in.c0.y, in.c0.z, in.c0.w, in.c1.x, in.c1.y, in.c1.z, in.c1.w};
+    const uint32_t vv[kNnzIpt] = {in.v0.x, in.v0.y, in.v0.z, in.v0.w, in.v1.x, in.v1.y, in.v1.z, in.v1.w};
+#pragma unroll
+    for (int u = 0; u < (int)kNnzIpt; ++u) {
+        r.v[u] = vv[u];
+        if constexpr (HINTS && sizeof(X) == 4) {
+            if (HOT > 0 && cc[u] < hot) {
+                r.x[u] = xc[cc[u]];
+            } else {
+                const uint32_t bits = ldg_u32_policy(a.x + cc[u], pol_keep);
+                memcpy(&r.x[u], &bits, 4);
+            }
+        } else if constexpr (HOT > 0) {
+            r.x[u] = cc[u] < hot ? xc[cc[u]] : ldg_any(a.x + cc[u]);
+        } else {
+            r.x[u] = ldg_any(a.x + cc[u]);
+        }
+    }
+    r.sw = in.sw;
+    r.endw = in.endw;
+    // the first 32 rows the tile may emit (rows past its last are unused)
+    const bool first_start = (__shfl_sync(0xffffffffu, in.sw, 0) & 1u) != 0u;
+    r.seg_base = in.seg0 + (first_start ? 0u : 1u);
+    r.row_pre = r.seg_base + lane < a.plan.n_nonempty ? __ldg(a.plan.nz_rows + r.seg_base + lane) : 0u;
+    if constexpr (has_prepare<Epi>::value) r.pre = epi.prepare(r.row_pre);
+    else r.pre = 0;
+    return r;
+}
+
+template <class SR, class Epi>
+__device__ __forceinline__ void nnz_finish(const NnzArgs<SR>& a, const NnzReady<SR, Epi>& r,
+                                           uint32_t tile, typename SR::value_t* sy, Epi& epi) {
+    using V = typename SR::value_t;
+    using W = typename SR::w_t;
+    constexpr uint32_t IPT = kNnzIpt;
+    const uint32_t lane = lane_id();
+    const uint32_t nnz = a.plan.nnz;
+    const uint32_t j0 = tile * kNnzTile;
+    const uint32_t jl = j0 + lane * IPT;
+    // nonzeros of this lane that exist (the last tile may be short);
+    // padding past nnz has no start bits
+    const uint32_t nv = jl < nnz ? min(nnz - jl, IPT) : 0u;
+    const uint32_t sb = (r.sw >> ((lane & 3u) * 8u)) & 0xFFu;
+    const bool first_start = (__shfl_sync(0xffffffffu, r.sw, 0) & 1u) != 0u;
+    V pv[IPT];
+#pragma unroll
+    for (int u = 0; u < (int)IPT; ++u) {
+        W wv;
+        memcpy(&wv, &r.v[u], 4);
+        pv[u] = (uint32_t)u < nv ? SR::combine(wv, r.x[u]) : SR::identity();
+    }
+    // starts before this lane (exclusive prefix of the per-lane counts)
+    const uint32_t nst = __popc(sb);
+    uint32_t incl = nst;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
+        if ((int)lane >= off) incl += t;
+    }
+    const uint32_t excl = incl - nst;
+    // 1. lane-local fold
+    V head = SR::identity(), acc = SR::identity();
+    uint32_t k = 0;
+#pragma unroll
+    for (int u = 0; u < (int)IPT; ++u) {
+        if ((sb >> u) & 1u) {
+            if (k == 0) head = acc;
+            else sy[excl + k - 1] = acc;
+            acc = SR::identity();
+            ++k;
+        }
+        acc = SR::reduce(acc, pv[u]);
+    }
+    // 2. segmented scan of the lane tails
+    V s = acc;
+    int f = nst ? 1 : 0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const V su = shfl_up_any(0xffffffffu, s, off);
+        const int fu = __shfl_up_sync(0xffffffffu, f, off);
+        if ((int)lane >= off) {
+            if (!f) s = SR::reduce(su, s);
+            f |= fu;
+        }
+    }
+    V prev = shfl_up_any(0xffffffffu, s, 1);
+    if (lane == 0) prev = SR::identity();
+    if (nst) {
+        const V val = SR::reduce(prev, head);
+        if (excl > 0)
+            sy[excl - 1] = val;  // segment begun in an earlier lane ends here
+        else if (!first_start)
+            a.tail[tile] = val;  // the row begun in an earlier tile ends here
+    }
+    const uint32_t nstarts = __shfl_sync(0xffffffffu, incl, 31);
+    const V last = shfl_any(0xffffffffu, s, 31);
+    const bool closed = (j0 + kNnzTile >= nnz) || (r.endw & 1u);
+    if (lane == 0) {
+        if (nstarts == 0) {
+            a.tail[tile] = last;
+            a.carry[tile] = last;
+        } else if (closed) {
+            sy[nstarts - 1] = last;
+        } else {
+            a.carry[tile] = last;
+        }
+    }
+    __syncwarp();
+    // 3. the tile's complete rows, in row order
+    const uint32_t ncomplete = nstarts == 0 ? 0u : (closed ? nstarts : nstarts - 1);
+    if (lane < ncomplete) {
+        if constexpr (has_prepare<Epi>::value) epi.emit_prepared(r.row_pre, sy[lane], r.pre);
+        else epi.emit(r.row_pre, sy[lane]);
+    }
+    for (uint32_t q = lane + 32; q < ncomplete; q += 32)
+        epi.emit(__ldg(a.plan.nz_rows + r.seg_base + q), sy[q]);
+    __syncwarp();
+}
+
+// HINTS: col/val are streamed with an evict-first L2 policy, x gathers use
+// evict-last (x stays in L2 across the iteration).  PIPE: a three-tile
+// software pipeline per warp -- while tile A is folded, the x gathers of
+// tile B and the col/val loads of tile C are in flight.
+template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
+    using V = typename SR::value_t;
+    using X = typename SR::x_t;
+    using W = typename SR::w_t;
+    using L = NnzLayout<SR, WARPS, HOT>;
+    static_assert(sizeof(W) == 4, "16-byte val loads assume 4-byte edge values");
+    extern __shared__ __align__(16) unsigned char dsm[];
+    const uint32_t w = threadIdx.x >> 5;
+    X* xc = reinterpret_cast<X*>(dsm + L::XC_OFF);
+    V* sy = reinterpret_cast<V*>(dsm + L::SY_OFF) + (size_t)w * kNnzTile;
+    epi.begin();
+    const uint32_t hot = HOT < a.plan.n_rows ? (uint32_t)HOT : a.plan.n_rows;
+    if constexpr (HOT > 0) {
+        for (uint32_t i = threadIdx.x; i < hot; i += WARPS * 32) xc[i] = ldg_any(a.x + i);
+        __syncthreads();
+    }
+    const uint32_t total_warps = gridDim.x * WARPS;
+    const uint32_t n_tiles = a.plan.n_tiles;
+    uint64_t pol_stream = 0, pol_keep = 0;
+    if constexpr (HINTS) {
+        pol_stream = l2_policy_evict_first();
+        pol_keep = l2_policy_evict_last();
+    }
+    if constexpr (!PIPE) {
+        for (uint32_t tile = blockIdx.x * WARPS + w; tile < n_tiles; tile += total_warps) {
+            const NnzIn in = nnz_load<SR, HINTS>(a, tile, pol_stream);
+            const NnzReady<SR, Epi> r = nnz_gather<SR, Epi, HOT, HINTS>(a, in, xc, hot, pol_keep, epi);
+            nnz_finish<SR, Epi>(a, r, tile, sy, epi);
+        }
+    } else {
+        uint32_t ta = blockIdx.x * WARPS + w;
+        if (ta < n_tiles) {
+            NnzReady<SR, Epi> ra =
+                nnz_gather<SR, Epi, HOT, HINTS>(a, nnz_load<SR, HINTS>(a, ta, pol_stream), xc, hot, pol_keep, epi);
+            uint32_t tb = ta + total_warps;
+            NnzIn ib{};
+            if (tb < n_tiles) ib = nnz_load<SR, HINTS>(a, tb, pol_stream);
+            for (;;) {
+                const uint32_t tc = tb + total_warps;
+                NnzReady<SR, Epi> rb{};
+                if (tb < n_tiles) rb = nnz_gather<SR, Epi, HOT, HINTS>(a, ib, xc, hot, pol_keep, epi);
+                NnzIn ic{};
+                if (tc < n_tiles) ic = nnz_load<SR, HINTS>(a, tc, pol_stream);
+                nnz_finish<SR, Epi>(a, ra, ta, sy, epi);
+                if (tb >= n_tiles) break;
+                ra = rb;
+                ta = tb;
+                ib = ic;
+                tb = tc;
+            }
+        }
+    }
+    epi.template block_end<WARPS * 32>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
+}
+
+__device__ __forceinline__ bool nnz_start_bit(const uint32_t* sbits, uint32_t k) {
+    return (__ldg(sbits + (k >> 5)) >> (k & 31)) & 1u;
+}
+
+// Rows that cross nnz tiles (deterministic fold of the tiles' partials in
+// tile order, like spmv_fixup_kernel) and the empty rows (identity).
+template <class SR, class Epi, int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+spmv_nnz_fixup_kernel(NnzArgs<SR> a, Epi epi) {
+    using V = typename SR::value_t;
+    __shared__ alignas(16) char epi_smem[64 * 8];
+    const uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
+    const uint32_t lane = lane_id();
+    const NnzPlanView& p = a.plan;
+    epi.begin();
+    bool longc = false;
+    uint32_t row = 0, seg = 0;
+    V acc = SR::identity();
+    if (t > 0 && t < p.n_tiles) {
+        const uint32_t j0 = t * kNnzTile;
+        if (!nnz_start_bit(p.sbits, j0)) {
+            // does the row begun earlier end in this tile?
+            uint32_t any = __ldg(p.sbits + (j0 >> 5)) & ~1u;
+#pragma unroll
+            for (uint32_t q = 1; q < kNnzTile / 32; ++q) any |= __ldg(p.sbits + (j0 >> 5) + q);
+            const bool ends = any != 0u || j0 + kNnzTile >= p.nnz || nnz_start_bit(p.sbits, j0 + kNnzTile);
+            if (ends) {
+                seg = __ldg(p.tile_seg + t);
+                row = __ldg(p.nz_rows + seg);
+                acc = SR::reduce(a.carry[t - 1], a.tail[t]);
+                if (t >= 2 && __ldg(p.tile_seg + t - 1) == seg &&
+                    !nnz_start_bit(p.sbits, (t - 1) * kNnzTile))
+                    longc = true;  // the row also covers tile t-2 or earlier
+                else
+                    epi.emit(row, acc);
+            }
+        }
+    }
+    unsigned pending = __ballot_sync(0xffffffffu, longc);
+    while (pending) {
+        const int src = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const uint32_t sg = __shfl_sync(0xffffffffu, seg, src);
+        const uint32_t tt = blockIdx.x * BLOCK + (threadIdx.x & ~31u) + (uint32_t)src;
+        // first tile whose first nonzero lies in row sg
+        uint32_t lo = 0, hi = tt - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(p.tile_seg + mid) < sg) lo = mid + 1; else hi = mid;
+        }
+        // the row began inside tile lo-1 unless tile lo starts exactly at it
+        const uint32_t first = (lo > 0 && !nnz_start_bit(p.sbits, lo * kNnzTile)) ? lo - 1 : lo;
+        V part = SR::identity();
+        for (uint32_t k = first + lane; k + 1 < tt; k += 32) part = SR::reduce(part, a.carry[k]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+            part = SR::reduce(part, shfl_down_any(0xffffffffu, part, off));
+        part = shfl_any(0xffffffffu, part, 0);
+        if ((int)lane == src) epi.emit(row, SR::reduce(part, acc));
+    }
+    for (uint32_t i = t; i < p.n_empty; i += gridDim.x * BLOCK) epi.emit(__ldg(p.empty_rows + i), SR::identity());
     epi.template block_end<BLOCK>(epi_smem);
 }
 

@@ -104,7 +104,7 @@ def test_malformed_csr_is_rejected(cuda):
     assert e.value.status == 1
 
 
-@pytest.mark.parametrize("variant", list(range(10)))
+@pytest.mark.parametrize("variant", list(range(len(g1.MERGE_VARIANTS))))
 @pytest.mark.parametrize("name", ["star20k", "rmat10_sym", "rmat11_dir", "path3000", "empty5"])
 def test_every_merge_variant(cuda, name, variant):
     g = GRAPHS[name]
@@ -131,7 +131,7 @@ def test_every_merge_variant(cuda, name, variant):
     assert O.rel_l1(yf.cpu().numpy(), y64) < 1e-6
 
 
-@pytest.mark.parametrize("variant", list(range(10)))
+@pytest.mark.parametrize("variant", list(range(len(g1.MERGE_VARIANTS))))
 def test_pagerank_every_merge_variant(cuda, variant):
     g = gen.rmat(13, 16, False, float_values=True)
     G = g1.Graph.from_gen(g)
