@@ -24,7 +24,7 @@ U32_MAX = 0xFFFFFFFF
 G1_U32, G1_F32 = 0, 1
 SR_MINPLUS_U32, SR_MINPLUS_F32, SR_PLUSTIMES_F32, SR_BFS_U32 = 0, 1, 2, 3
 SCHED_AUTO, SCHED_MERGE, SCHED_VECTOR = 0, 1, 2
-ENGINE_BLAS, ENGINE_ADVANCE, ENGINE_AUTO = 0, 1, 2
+ENGINE_BLAS, ENGINE_ADVANCE, ENGINE_AUTO, ENGINE_NEARFAR = 0, 1, 2, 3
 PR_REFERENCE, PR_DANGLING = 0, 1
 # Kernel family of each merge-schedule variant, indexed like kMergeVariants
 # in csrc/spmv_launch.cuh: "warp" = spmv_wmerge_kernel (warp tiles, plain

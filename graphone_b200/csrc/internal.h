@@ -130,6 +130,8 @@ struct g1_graph {
     bool hubs_ready = false;
     uint32_t n_hubs = 0, n_hub_pieces = 0;
     bool outdeg_ready = false;
+    // Mean u32 edge weight (bucket width of the near-far engine), -1 until known.
+    double mean_weight = -1.0;
     // Slot engines of the batched BFS / SSSP / PPR entry points (by kind),
     // kept between calls.
     std::shared_ptr<g1::SlotEngine> slot_cache[3];
@@ -164,6 +166,30 @@ g1_status copy_out(void* dst, const void* dev_src, size_t bytes, cudaStream_t s)
 
 g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out);
 g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out);
+// Near-far SSSP (unit = BFS) from internal vertex src in one persistent
+// launch; *dist_out points to the graph's workspace distances.
+g1_status nearfar_traverse(g1_graph* g, uint32_t src, bool unit, uint32_t** dist_out, uint32_t* rounds,
+                           cudaStream_t s);
+// The same in caller-owned buffers, enqueued only: buffers laid out in one
+// store of nearfar_words(n) words (256-byte aligned), the bucket width (mean weight based; the caller holds
+// g->mu the first time), the launch, and the outcome from a host copy of the
+// control block (nearfar_ctl_bytes() bytes at NfBuffers::ctl).
+struct NfBuffers {
+    uint32_t *dist, *stamp, *fstamp, *near[2], *far[2], *ctl;
+};
+size_t nearfar_words(uint32_t n);  // 4-byte words of one store
+void nearfar_layout(uint32_t n, uint32_t* store, NfBuffers* b);
+g1_status nearfar_delta(g1_graph* g, bool unit, cudaStream_t s, uint32_t* out);
+// src: internal id, or a caller id when perm (the graph's relabelling) is given
+g1_status nearfar_launch(const g1_graph* g, uint32_t src, bool unit, uint32_t delta, const NfBuffers& b,
+                         cudaStream_t s, const uint32_t* perm = nullptr);
+g1_status nearfar_result(const uint32_t* host_ctl, uint32_t* rounds);
+uint32_t nearfar_ctl_bytes();
+// Graphs of small uniform degree (grids, meshes), where the near-far engine
+// beats frontier engines and batches.
+inline bool nearfar_suits(const g1_graph* g) {
+    return g->o[0].present && g->o[0].max_deg <= 16 && (uint64_t)g->m <= 8ull * g->n;
+}
 // Vertex-order conversions of a relabelled graph (4-byte values).
 g1_status to_caller_order(g1_graph* g, uint32_t* dev_out, const uint32_t* internal, cudaStream_t s);
 g1_status to_internal_order(g1_graph* g, uint32_t* dev_out, const uint32_t* caller, cudaStream_t s);

@@ -1,0 +1,356 @@
+// Near-far single-source shortest paths / BFS in one persistent launch.
+//
+// For graphs of small uniform degree and large diameter (grids, meshes,
+// road-like graphs) the frontier engines are bound by per-iteration host
+// round trips (thousands of iterations) and, for SSSP, by Bellman-Ford's
+// repeated relaxations of the same vertices.  This engine keeps the whole
+// traversal on the device and orders the work by distance:
+//   * vertices whose tentative distance is below the threshold T form the
+//     near queue; a relax round pushes every near vertex's out-edges
+//     (atomicMin); improved vertices below T join the next near queue,
+//     the others the far pile (each vertex at most once per queue and per
+//     bucket, by stamps);
+//   * when the near queue runs dry, T moves to (smallest pending distance)
+//     + delta and the far pile is split into the new near queue and the
+//     rest; entries below the old T are stale and dropped.
+// This is the near-far variant of delta-stepping (Davidson, Baxter, Garland
+// and Owens, IPDPS 2014).  Steps are separated by one grid barrier of the
+// cooperative launch (one 1024-thread block per SM); every barrier wait is
+// bounded and reports a timeout through the control block instead of
+// hanging.  Final distances are the
+// unique shortest-path distances, bit-identical to the other engines.
+#include <algorithm>
+#include <cstdlib>
+
+#include "g1/common.cuh"
+#include "internal.h"
+
+namespace g1 {
+
+// Control block.  The traversal is a sequence of steps separated by one
+// grid barrier each; values a step reads are never written during that step:
+// per-step values rotate through three slots (step s reads slot s % 3,
+// fills slot (s+1) % 3 and resets slot (s+2) % 3).
+struct NfCtl {
+    uint32_t qn[3];      // near-queue size
+    uint32_t kind[3];    // 1: the step is a threshold move (after a minimum step)
+    uint32_t thresh[3];  // T
+    uint32_t minfar[3];  // smallest pending far distance
+    uint32_t fn[2];      // far-pile sizes (double-buffered piles)
+    uint32_t bar_count;  // grid barrier
+    uint32_t bar_gen;
+    uint32_t err;        // 1 = a barrier wait ran out
+    uint32_t rounds;     // relax rounds
+};
+
+struct NfArgs {
+    const uint32_t* rp;
+    const uint32_t* col;
+    const uint32_t* val;
+    uint32_t n;
+    uint32_t delta;
+    uint32_t* dist;
+    uint32_t* stamp;   // near-queue generation a vertex was queued in
+    uint32_t* fstamp;  // bucket a vertex was put on the far pile in
+    uint32_t* near[2];
+    uint32_t* far[2];
+    NfCtl* ctl;
+};
+
+// About 2-3 s of waiting before a barrier gives up.
+constexpr uint32_t kNfSpinLimit = 1u << 23;
+
+__device__ __forceinline__ uint32_t ld_vol(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t r;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(r) : "l"(p) : "memory");
+    return r;
+}
+__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t v) {
+    uint32_t r;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(r) : "l"(p), "r"(v) : "memory");
+    return r;
+}
+__device__ __forceinline__ void atom_add_release(uint32_t* p, uint32_t v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Counting grid barrier: the block's writes are released by its thread 0's
+// arrival (after bar.sync), and the other blocks' writes acquired through
+// the generation word.  false if the wait ran out (the kernel then returns:
+// the host reports G1_ERR_TIMEOUT).
+__device__ bool nf_barrier(NfCtl* c, uint32_t nblocks) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t g0 = ld_acquire(&c->bar_gen);
+        if (atom_add_acq_rel(&c->bar_count, 1u) == nblocks - 1) {
+            c->bar_count = 0u;  // seen by the next arrivals through bar_gen
+            atom_add_release(&c->bar_gen, 1u);
+        } else {
+            uint32_t spins = 0;
+            while (ld_acquire(&c->bar_gen) == g0) {
+                if (++spins > kNfSpinLimit) {
+                    atomicOr(&c->err, 1u);
+                    break;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    return (ld_vol(&c->err) & 1u) == 0u;
+}
+
+// src is an internal vertex id, or a caller id mapped through perm.
+__global__ void nf_init_kernel(uint32_t n, uint32_t src, const uint32_t* perm, uint32_t t0, uint32_t* dist,
+                               uint32_t* stamp, uint32_t* fstamp, uint32_t* near0, NfCtl* ctl) {
+    if (perm) src = perm[src];
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        dist[v] = v == src ? 0u : kU32Max;
+        stamp[v] = 0u;
+        fstamp[v] = 0u;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        near0[0] = src;
+        NfCtl c{};
+        c.qn[0] = 1u;
+        c.thresh[0] = t0;
+        c.minfar[0] = c.minfar[1] = c.minfar[2] = kU32Max;
+        *ctl = c;
+    }
+}
+
+template <bool UNIT>
+__global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
+    const uint32_t nb = gridDim.x;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t gs = gridDim.x * blockDim.x;
+    NfCtl* c = a.ctl;
+    uint32_t par = 0, fp = 0;
+    uint32_t gen = 1;     // near-queue generation (stamp)
+    uint32_t bucket = 1;  // far-pile bucket (fstamp)
+    for (uint32_t st = 0;; ++st) {
+        const uint32_t cur = st % 3, nxt = (st + 1) % 3, old = (st + 2) % 3;
+        const uint32_t qn = ld_vol(&c->qn[cur]);
+        const uint32_t T = ld_vol(&c->thresh[cur]);
+        const bool move = ld_vol(&c->kind[cur]) != 0u;
+        const uint32_t fn = ld_vol(&c->fn[fp]);
+        // 0 = relax round, 1 = smallest far distance, 2 = threshold move
+        const int step = move ? 2 : qn > 0 ? 0 : (fn == 0 ? -1 : (UNIT ? 2 : 1));
+        if (step < 0) return;
+        if (gt == 0) {
+            c->qn[old] = 0u;
+            c->kind[old] = 0u;
+            c->minfar[old] = kU32Max;
+            if (step != 2) {
+                c->fn[fp ^ 1] = 0u;  // the other pile is empty until the next move
+                c->thresh[nxt] = T;
+            }
+            if (step == 0) c->rounds += 1u;
+            if (step == 1) c->kind[nxt] = 1u;
+        }
+        if (step == 0) {
+            ++gen;
+            const uint32_t* in = a.near[par];
+            uint32_t* outq = a.near[par ^ 1];
+            uint32_t* farq = a.far[fp];
+            for (uint32_t i = gt; i < qn; i += gs) {
+                const uint32_t u = in[i];
+                const uint32_t du = ld_vol(a.dist + u);
+                const uint32_t e1 = a.rp[u + 1];
+                for (uint32_t e = a.rp[u]; e < e1; ++e) {
+                    const uint32_t v = a.col[e];
+                    const uint32_t nd = du + (UNIT ? 1u : a.val[e]);
+                    // no plain pre-check: one dependent memory access fewer
+                    // on the critical path of a step
+                    if (nd >= atomicMin(a.dist + v, nd)) continue;
+                    if (nd < T) {
+                        // BFS: every improvement in a step sets the same level,
+                        // so only the first one succeeds -- no duplicate to stamp
+                        if (UNIT || atomicExch(a.stamp + v, gen) != gen) outq[atomicAdd(&c->qn[nxt], 1u)] = v;
+                    } else if (atomicExch(a.fstamp + v, bucket) != bucket) {
+                        farq[atomicAdd(&c->fn[fp], 1u)] = v;
+                    }
+                }
+            }
+            par ^= 1;
+        } else if (step == 1) {
+            uint32_t mn = kU32Max;
+            const uint32_t* fin = a.far[fp];
+            for (uint32_t i = gt; i < fn; i += gs) {
+                const uint32_t d = ld_vol(a.dist + fin[i]);
+                if (d >= T) mn = min(mn, d);
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, off));
+            if (lane_id() == 0 && mn != kU32Max) atomicMin(&c->minfar[nxt], mn);
+        } else {
+            // move the threshold: the far pile splits into the next near
+            // queue and the remaining pile; entries below T are stale
+            uint32_t tn;
+            if (UNIT) {
+                tn = T + 1u;
+            } else {
+                const uint32_t mf = ld_vol(&c->minfar[cur]);
+                const uint64_t base = (mf != kU32Max && mf > T) ? mf : T;
+                const uint64_t t64 = base + a.delta;
+                tn = t64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)t64;
+            }
+            if (gt == 0) c->thresh[nxt] = tn;
+            ++gen;
+            ++bucket;
+            const uint32_t* fin = a.far[fp];
+            uint32_t* fout = a.far[fp ^ 1];
+            uint32_t* outq = a.near[par ^ 1];
+            for (uint32_t i = gt; i < fn; i += gs) {
+                const uint32_t v = fin[i];
+                const uint32_t d = ld_vol(a.dist + v);
+                if (d < T) continue;
+                if (d < tn) {
+                    if (atomicExch(a.stamp + v, gen) != gen) outq[atomicAdd(&c->qn[nxt], 1u)] = v;
+                } else if (atomicExch(a.fstamp + v, bucket) != bucket) {
+                    fout[atomicAdd(&c->fn[fp ^ 1], 1u)] = v;
+                }
+            }
+            par ^= 1;
+            fp ^= 1;
+        }
+        if (!nf_barrier(c, nb)) return;
+    }
+}
+
+namespace {
+
+// Reads the control block back through the graph's pinned scratch and
+// reports its outcome.
+g1_status ws_pinned_ctl(g1_graph* g, const uint32_t* ctl, cudaStream_t s, uint32_t* rounds) {
+    G1_TRY(g->ws.pinned.ensure(sizeof(NfCtl) + 64));
+    G1_CUDA(cudaMemcpyAsync(g->ws.pinned.p, ctl, sizeof(NfCtl), cudaMemcpyDeviceToHost, s));
+    G1_CUDA(cudaStreamSynchronize(s));
+    return nearfar_result(g->ws.pinned.as<uint32_t>(), rounds);
+}
+
+__global__ void weight_sum_kernel(const uint32_t* val, uint32_t m, unsigned long long* sum) {
+    unsigned long long s = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += stride) s += val[e];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane_id() == 0 && s) atomicAdd(sum, s);
+}
+
+}  // namespace
+
+// Bucket width: a multiple of the mean edge weight (G1_NEARFAR_DELTA_SCALE,
+// default 32); BFS needs no buckets.
+g1_status nearfar_delta(g1_graph* g, bool unit, cudaStream_t s, uint32_t* out) {
+    if (unit) {
+        *out = 1u;
+        return G1_OK;
+    }
+    if (g->mean_weight < 0.0) {
+        const Orientation& o = g->o[0];
+        unsigned long long* sum = nullptr;
+        G1_TRY(g->ws.get("nf_wsum", 2, &sum));
+        G1_CUDA(cudaMemsetAsync(sum, 0, 8, s));
+        const uint32_t grid = (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(ceil_div(g->m, 256), (uint64_t)g->sm_count * 8));
+        if (g->m) weight_sum_kernel<<<grid, 256, 0, s>>>(static_cast<const uint32_t*>(o.val), g->m, sum);
+        count_launches(1);
+        unsigned long long h = 0;
+        G1_CUDA(cudaMemcpyAsync(&h, sum, 8, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaStreamSynchronize(s));
+        g->mean_weight = g->m ? (double)h / (double)g->m : 1.0;
+    }
+    double scale = 32.0;
+    if (const char* e = std::getenv("G1_NEARFAR_DELTA_SCALE")) scale = std::max(0.01, std::atof(e));
+    *out = (uint32_t)std::max(1.0, std::min(2.0e9, g->mean_weight * scale));
+    return G1_OK;
+}
+
+size_t nearfar_words(uint32_t n) {
+    // dist, stamp, fstamp; two near queues and two far piles (each vertex at
+    // most once in each); the control block (16-byte aligned)
+    return 3 * (size_t)n + 4 * ((size_t)n + 1) + sizeof(NfCtl) / 4 + 8;
+}
+
+void nearfar_layout(uint32_t n, uint32_t* p, NfBuffers* b) {
+    b->dist = p;
+    b->stamp = p + n;
+    b->fstamp = p + 2 * (size_t)n;
+    uint32_t* q = p + 3 * (size_t)n;
+    b->near[0] = q;
+    b->near[1] = q + (n + 1);
+    b->far[0] = q + 2 * (size_t)(n + 1);
+    b->far[1] = q + 3 * (size_t)(n + 1);
+    uintptr_t c = reinterpret_cast<uintptr_t>(q + 4 * (size_t)(n + 1));
+    c = (c + 15) & ~uintptr_t(15);
+    b->ctl = reinterpret_cast<uint32_t*>(c);
+}
+
+g1_status nearfar_launch(const g1_graph* g, uint32_t src, bool unit, uint32_t delta, const NfBuffers& b,
+                         cudaStream_t s, const uint32_t* perm) {
+    if (!g->o[0].present) return fail(G1_ERR_UNSUPPORTED, "near-far engine needs the out-edge CSR");
+    const uint32_t n = g->n;
+    NfArgs a;
+    const Orientation& o = g->o[0];
+    a.rp = o.rp;
+    a.col = o.col;
+    a.val = static_cast<const uint32_t*>(o.val);
+    a.n = n;
+    a.delta = delta;
+    a.dist = b.dist;
+    a.stamp = b.stamp;
+    a.fstamp = b.fstamp;
+    a.near[0] = b.near[0];
+    a.near[1] = b.near[1];
+    a.far[0] = b.far[0];
+    a.far[1] = b.far[1];
+    a.ctl = reinterpret_cast<NfCtl*>(b.ctl);
+    const uint32_t gi = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
+    // BFS: a threshold above every level -- each step is one level and the
+    // far pile stays empty
+    nf_init_kernel<<<gi, 256, 0, s>>>(n, src, perm, unit ? kU32Max : a.delta, a.dist, a.stamp, a.fstamp,
+                                      a.near[0], a.ctl);
+    count_launches(1);
+    G1_CUDA(cudaGetLastError());
+    // every block of a cooperative launch is resident, so the grid barrier
+    // only ever waits for running blocks; one 1024-thread block per SM keeps
+    // the barrier's arrivals few
+    const void* fn = unit ? (const void*)nf_kernel<true> : (const void*)nf_kernel<false>;
+    int per_sm = 0;
+    G1_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 1024, 0));
+    if (per_sm < 1) return fail(G1_ERR_UNSUPPORTED, "near-far engine: kernel does not fit an SM");
+    void* params[] = {&a};
+    G1_CUDA(cudaLaunchCooperativeKernel(fn, dim3((uint32_t)g->sm_count), dim3(1024), params, 0, s));
+    count_launches(1);
+    return G1_OK;
+}
+
+g1_status nearfar_result(const uint32_t* host_ctl, uint32_t* rounds) {
+    NfCtl h;
+    memcpy(&h, host_ctl, sizeof(h));
+    if (h.err & 1u) return fail(G1_ERR_TIMEOUT, "near-far engine: a grid barrier wait ran out");
+    if (rounds) *rounds = h.rounds;
+    return G1_OK;
+}
+
+uint32_t nearfar_ctl_bytes() { return (uint32_t)sizeof(NfCtl); }
+
+g1_status nearfar_traverse(g1_graph* g, uint32_t src, bool unit, uint32_t** dist_out, uint32_t* rounds,
+                           cudaStream_t s) {
+    uint32_t delta = 1;
+    G1_TRY(nearfar_delta(g, unit, s, &delta));
+    uint32_t* store = nullptr;
+    G1_TRY(g->ws.get("nf_store", nearfar_words(g->n), &store));
+    NfBuffers b;
+    nearfar_layout(g->n, store, &b);
+    G1_TRY(nearfar_launch(g, src, unit, delta, b, s));
+    G1_TRY(ws_pinned_ctl(g, b.ctl, s, rounds));
+    *dist_out = b.dist;
+    return G1_OK;
+}
+
+}  // namespace g1

@@ -14,7 +14,10 @@
 //      launched and an event recorded behind it.
 // Executors never wait for one another, so work on different graphs and
 // kinds overlaps on the device, and a query joins a running batch at the
-// next step boundary instead of waiting for the batch to drain.
+// next step boundary instead of waiting for the batch to drain.  SSSP on
+// graphs of small uniform degree (grids) is the exception: there one query
+// at a time runs on the near-far engine (nearfar.cu), which beats batched
+// Bellman-Ford on such graphs by orders of magnitude.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -67,6 +70,15 @@ struct Exec {
     std::vector<Request*> slot_req;  // query of each slot
     std::vector<Request*> retiring;  // results enqueued before ev
     DevBuf staging;                  // pageable outputs
+    // SSSP on graphs of small uniform degree: one query at a time on the
+    // near-far engine instead of slots (batched Bellman-Ford relaxes such
+    // graphs' vertices many times over)
+    bool nearfar = false;
+    uint32_t nf_delta = 1;
+    DevBuf nf_store;
+    NfBuffers nf{};
+    PinnedBuf nf_host;
+    Request* nf_req = nullptr;
 };
 
 }  // namespace
@@ -130,17 +142,20 @@ void complete_one(g1_server* S, Request* r, g1_status st) {
     complete(S, v, st);
 }
 
+bool holds_memory(const Exec& E) { return E.eng.ready() || E.nf_store.p != nullptr; }
+
 void release_engine(g1_server* S, Exec& E) {
-    if (!E.eng.ready()) return;
-    S->dev_bytes -= E.eng.device_bytes();
+    if (!holds_memory(E)) return;
+    S->dev_bytes -= E.eng.device_bytes() + E.nf_store.bytes;
     S->engines -= 1;
     E.eng.release();
+    E.nf_store.release();
     E.staging.release();
 }
 
 bool idle(const Exec& E) {
-    return E.eng.ready() && E.eng.occupied() == 0 && !E.inflight && E.pending.empty() &&
-           E.retiring.empty();
+    return holds_memory(E) && E.eng.occupied() == 0 && !E.inflight && E.pending.empty() &&
+           E.retiring.empty() && !E.nf_req;
 }
 
 // Frees the state of one idle engine other than `self`.
@@ -160,7 +175,7 @@ bool others_hold_memory(g1_server* S, const Exec* self) {
     const size_t ne = S->n_execs.load();
     for (size_t i = 0; i < ne; ++i) {
         const Exec& E = *S->execs[i];
-        if (&E != self && E.eng.ready()) return true;
+        if (&E != self && holds_memory(E)) return true;
     }
     return false;
 }
@@ -244,8 +259,91 @@ g1_status retire(g1_server* S, Exec& E, const std::vector<uint32_t>& fin) {
     return G1_OK;
 }
 
+// Near-far executor: one query in flight.
+bool service_nearfar(g1_server* S, Exec& E, bool stopping) {
+    bool progress = false;
+    if (E.inflight) {
+        const cudaError_t q = cudaEventQuery(E.ev);
+        if (q == cudaErrorNotReady) return false;
+        progress = true;
+        E.inflight = false;
+        g1_status st = G1_OK;
+        if (q != cudaSuccess) {
+            cudaGetLastError();
+            st = G1_ERR_DEVICE;
+        } else {
+            st = nearfar_result(E.nf_host.as<uint32_t>(), nullptr);
+        }
+        complete_one(S, E.nf_req, st);
+        E.nf_req = nullptr;
+        if (st == G1_ERR_DEVICE) release_engine(S, E);
+    }
+    if (stopping || E.pending.empty()) return progress;
+    const size_t need = nearfar_words(E.g->n) * 4;
+    if (!E.nf_store.p) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            free_b = 0;
+        }
+        bool fits = need + S->reserve <= free_b && (!S->limit || S->dev_bytes + need <= S->limit);
+        while (!fits && release_one_idle(S, &E))
+            fits = (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) && need + S->reserve <= free_b &&
+                   (!S->limit || S->dev_bytes + need <= S->limit);
+        if (!fits || E.nf_store.ensure(need) != G1_OK || E.nf_host.ensure(nearfar_ctl_bytes() + 64) != G1_OK) {
+            cudaGetLastError();
+            E.nf_store.release();
+            if (!others_hold_memory(S, &E)) {
+                std::vector<Request*> rs(E.pending.begin(), E.pending.end());
+                E.pending.clear();
+                complete(S, rs, G1_ERR_OOM);
+                return true;
+            }
+            return progress;  // wait for memory
+        }
+        nearfar_layout(E.g->n, E.nf_store.as<uint32_t>(), &E.nf);
+        S->dev_bytes += E.nf_store.bytes;
+        S->engines += 1;
+    }
+    Request* r = E.pending.front();
+    E.pending.pop_front();
+    E.nf_req = r;
+    const g1_graph* g = E.g;
+    const uint32_t* perm = g->relabeled ? g->perm.as<uint32_t>() : nullptr;
+    bool ok = nearfar_launch(g, r->src, false, E.nf_delta, E.nf, E.s, perm) == G1_OK;
+    // distances in caller order into the query's output
+    const size_t row = (size_t)g->n * 4;
+    void* dst = r->out_dev;
+    if (ok && !dst) ok = E.staging.ensure(row + 16) == G1_OK;
+    if (ok) {
+        uint32_t* d = static_cast<uint32_t*>(dst ? dst : E.staging.p);
+        if (perm)
+            ok = to_caller_order(const_cast<g1_graph*>(g), d, E.nf.dist, E.s) == G1_OK;
+        else
+            ok = cudaMemcpyAsync(d, E.nf.dist, row, cudaMemcpyDeviceToDevice, E.s) == cudaSuccess;
+        if (ok && !dst) ok = cudaMemcpyAsync(r->out, E.staging.p, row, cudaMemcpyDeviceToHost, E.s) == cudaSuccess;
+    }
+    if (ok) ok = cudaMemcpyAsync(E.nf_host.p, E.nf.ctl, nearfar_ctl_bytes(), cudaMemcpyDeviceToHost, E.s) == cudaSuccess;
+    if (ok) ok = cudaEventRecord(E.ev, E.s) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        complete_one(S, r, G1_ERR_DEVICE);
+        E.nf_req = nullptr;
+        return true;
+    }
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        ++S->steps;
+        S->max_occ = std::max(S->max_occ, 1u);
+    }
+    E.inflight = true;
+    E.last_busy = Clock::now();
+    return true;
+}
+
 // One turn of one executor; true if anything happened.
 bool service(g1_server* S, Exec& E, bool stopping, std::vector<uint32_t>& fin) {
+    if (E.nearfar) return service_nearfar(S, E, stopping);
     bool progress = false;
     if (E.inflight) {
         const cudaError_t q = cudaEventQuery(E.ev);
@@ -330,7 +428,9 @@ bool service(g1_server* S, Exec& E, bool stopping, std::vector<uint32_t>& fin) {
     return progress;
 }
 
-bool busy(const Exec& E) { return E.inflight || E.eng.occupied() > 0 || !E.pending.empty(); }
+bool busy(const Exec& E) {
+    return E.inflight || E.eng.occupied() > 0 || !E.pending.empty() || E.nf_req != nullptr;
+}
 
 void loop(g1_server* S) {
     cudaSetDevice(S->device);
@@ -432,6 +532,10 @@ extern "C" g1_status g1_server_add_graph(g1_server* S, g1_graph* g, uint32_t* gr
         if (kind == kSlotSssp && g->vtype != G1_U32) continue;
         std::lock_guard<std::mutex> lk(g->mu);
         G1_TRY(slot_graph(g, kind, E.s, &E.sg));
+        if (kind == kSlotSssp && nearfar_suits(g)) {
+            E.nearfar = true;
+            G1_TRY(nearfar_delta(g, false, E.s, &E.nf_delta));
+        }
         E.usable = true;
     }
     // the loop only reads execs[0, n_execs)

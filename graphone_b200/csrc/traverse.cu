@@ -16,8 +16,9 @@
 //   with the visited stamp of the sssp_adv filter (apps/sssp_adv.cu:62-71,
 //   made atomic) and appends compactly: one kernel per iteration.
 // * AUTO: push while the frontier's out-degree sum is below m/16, pull
-//   otherwise (direction-optimising).  Final distances are the unique
-//   shortest-path distances whichever engine runs, so all three agree
+//   otherwise (direction-optimising); on graphs of small uniform degree
+//   (grids) the near-far engine (nearfar.cu) instead.  Final distances are
+//   the unique shortest-path distances whichever engine runs, so all agree
 //   bit-exactly with the oracle.
 #include <cub/device/device_scan.cuh>
 
@@ -180,6 +181,16 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
     if (src_caller >= n) return fail(G1_ERR_INVALID, "source vertex out of range");
     uint32_t src = src_caller;
     G1_TRY(internal_vertex(g, src_caller, &src, s));
+    if (engine == G1_ENGINE_AUTO && nearfar_suits(g)) engine = G1_ENGINE_NEARFAR;
+    if (engine == G1_ENGINE_NEARFAR) {
+        if (!UNIT && g->vtype != G1_U32) return fail(G1_ERR_INVALID, "SSSP needs u32 edge weights");
+        uint32_t* dist = nullptr;
+        uint32_t rounds = 0;
+        G1_TRY(nearfar_traverse(g, src, UNIT, &dist, &rounds, s));
+        if (iters_out) *iters_out = rounds;
+        G1_TRY(copy_out_vertices(g, out, dist, s));
+        return check_device_error(g, s);
+    }
     if ((engine == G1_ENGINE_BLAS || engine == G1_ENGINE_AUTO) && !g->o[1].present)
         return fail(G1_ERR_UNSUPPORTED, "pull engine needs the in-edge CSR (G1_GRAPH_BUILD_OTHER)");
     if ((engine == G1_ENGINE_ADVANCE || engine == G1_ENGINE_AUTO) && !g->o[0].present)
@@ -279,7 +290,7 @@ using namespace g1;
 extern "C" g1_status g1_sssp(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* dist_out,
                              uint32_t* iters_out, void* stream) {
     if (!g || !dist_out) return fail(G1_ERR_INVALID, "g1_sssp: bad argument");
-    if (engine != G1_ENGINE_BLAS && engine != G1_ENGINE_ADVANCE && engine != G1_ENGINE_AUTO)
+    if (engine < G1_ENGINE_BLAS || engine > G1_ENGINE_NEARFAR)
         return fail(G1_ERR_INVALID, "g1_sssp: unknown engine");
     DeviceGuard dg(g->device);
     std::lock_guard<std::mutex> lk(g->mu);
@@ -289,7 +300,7 @@ extern "C" g1_status g1_sssp(g1_graph* g, uint32_t src, g1_engine engine, uint32
 extern "C" g1_status g1_bfs(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* level_out,
                             uint32_t* iters_out, void* stream) {
     if (!g || !level_out) return fail(G1_ERR_INVALID, "g1_bfs: bad argument");
-    if (engine != G1_ENGINE_BLAS && engine != G1_ENGINE_ADVANCE && engine != G1_ENGINE_AUTO)
+    if (engine < G1_ENGINE_BLAS || engine > G1_ENGINE_NEARFAR)
         return fail(G1_ERR_INVALID, "g1_bfs: unknown engine");
     DeviceGuard dg(g->device);
     std::lock_guard<std::mutex> lk(g->mu);

@@ -54,7 +54,10 @@ typedef enum {
 typedef enum {
     G1_ENGINE_BLAS = 0,    /* pull SpMV per iteration (BlasGcEngine, sparse frontier) */
     G1_ENGINE_ADVANCE = 1, /* push advance/filter (AdvanceGC) */
-    G1_ENGINE_AUTO = 2     /* push while the frontier is small, pull when it is large */
+    G1_ENGINE_AUTO = 2,    /* near-far on graphs of small uniform degree, else push while
+                              the frontier is small and pull when it is large */
+    G1_ENGINE_NEARFAR = 3  /* distance-ordered near/far queues in one persistent launch
+                              (no GraphOne counterpart; for high-diameter graphs) */
 } g1_engine;
 
 typedef enum {
@@ -218,7 +221,9 @@ g1_status g1_ppr_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, float alph
 /* --------------------------------------------------------- serving loop */
 /* A request loop (one host thread, one CUDA stream per graph and query
  * kind) over resident graphs.  Queries on the same graph and of the same
- * kind share a multi-source engine of up to max_batch slots; a query is
+ * kind share a multi-source engine of up to max_batch slots (SSSP on graphs
+ * of small uniform degree -- grids -- runs one query at a time on the
+ * near-far engine instead); a query is
  * admitted into a free slot between two iterations of the engine and its
  * result is written as soon as its own traversal completes, while the rest
  * of the batch keeps running (continuous batching).  Engines of different

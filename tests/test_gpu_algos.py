@@ -11,7 +11,7 @@ from tests.gpu_util import edge_case_graphs
 pytestmark = pytest.mark.gpu
 
 GRAPHS = edge_case_graphs()
-ENGINES = [g1.ENGINE_BLAS, g1.ENGINE_ADVANCE, g1.ENGINE_AUTO]
+ENGINES = [g1.ENGINE_BLAS, g1.ENGINE_ADVANCE, g1.ENGINE_AUTO, g1.ENGINE_NEARFAR]
 
 
 @pytest.mark.parametrize("engine", ENGINES)
