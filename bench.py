@@ -21,8 +21,13 @@ streams them from HBM.
 in-edge CSR is copied from pinned host memory (g1_graph_create), PageRank
 runs, and the ranks are read back to the host (g1_pagerank into host memory).
 ``roofline``: achieved algorithmic bytes of the dominant kernel (the fused
-merge-path SpMV + apply/construct kernel, spmv_merge_kernel) per launch over
-its CUDA-event duration, against the measured HBM copy bandwidth.
+SpMV + apply/construct kernel of the schedule in use, by default
+spmv_nnz_kernel) per launch over its CUDA-event duration, against the
+measured HBM copy bandwidth; ``traffic`` is the DRAM bytes per launch ncu
+measured for that kernel (profiles/pagerank_rmat22_traffic.json).
+``queries``: plain and batched SSSP/BFS (RMAT-14, RMAT-20 k=256, 4096^2
+grid); ``serving``: the serving loop over 8 resident graphs vs plain
+per-request execution.
 ``cpu_baseline``: GraphOne's own SpMV_cpu_navie (compiled from the reference
 sources into oracle/_ref) driving the same PageRank iteration on all host
 threads, on a bounded sample of iterations; or the C oracle when oracle/_ref
@@ -203,6 +208,8 @@ def query_metrics(dev, stream, budget_queries: int = 256):
       (min-plus SpMV), advance/filter and push/pull engines.
     * RMAT-20 (same shape) k=256 sources: plain engine queries/s over 64 of
       the sources vs one batched k=256 pass (bit-exact spot checks).
+    * 4096^2 grid (uint32 weights [1,100]) SSSP and BFS from the corner on the
+      near-far and advance engines (GTEPS = directed CSR edges / time).
     """
     import torch
     import graphone_b200 as g1
@@ -236,11 +243,12 @@ def query_metrics(dev, stream, budget_queries: int = 256):
     torch.cuda.empty_cache()
 
     g = gen.rmat(20, 16, symmetric=True, weights=(1, 64), device=dev)
-    G = g1.Graph.from_gen(g)
+    # stored in decreasing-degree order (G1_GRAPH_RELABEL) for both engines
+    G = g1.Graph.from_gen(g, relabel=True)
     srcs = gen.pick_sources(g, 256)
     one = torch.empty(g.n, dtype=torch.int32, device=dev)
     blk = torch.empty((256, g.n), dtype=torch.int32, device=dev)
-    res = {"n": g.n, "m": g.m, "k": 256}
+    res = {"n": g.n, "m": g.m, "k": 256, "layout": "relabelled by degree (both engines)"}
     for kind in ("bfs", "sssp"):
         single = G.bfs if kind == "bfs" else G.sssp
         batch = G.bfs_batch if kind == "bfs" else G.sssp_batch
@@ -264,6 +272,34 @@ def query_metrics(dev, stream, budget_queries: int = 256):
     out["batch_rmat20_k256"] = res
     G.close()
     del g, G, one, blk
+    torch.cuda.empty_cache()
+
+    # 4096 x 4096 grid, uint32 weights [1, 100], source at the corner: the
+    # near-far engine (what ENGINE_AUTO picks here) vs the advance engine
+    g = gen.grid2d(4096, 4096, (1, 100), device=dev)
+    G = g1.Graph.from_gen(g)
+    d = torch.empty(g.n, dtype=torch.int32, device=dev)
+    res = {"n": g.n, "m": g.m, "source": 0}
+    ref = None
+    for kind in ("sssp", "bfs"):
+        fn = G.sssp if kind == "sssp" else G.bfs
+        for name, eng in (("nearfar", g1.ENGINE_NEARFAR), ("advance", g1.ENGINE_ADVANCE)):
+            fn(0, eng, out=d, stream=stream)
+            it = [0]
+
+            def run(fn=fn, eng=eng):
+                it[0] = fn(0, eng, out=d, stream=stream, return_iters=True)[1]
+            ms = _event_ms(run, stream)
+            if kind == "sssp":
+                if ref is None:
+                    ref = d.clone()
+                elif not torch.equal(ref, d):
+                    res["sssp_engines_disagree"] = True
+            res[f"{kind}_{name}"] = {"ms": round(ms, 2), "iterations": int(it[0]),
+                                    "gteps": round(g.m / (ms / 1e3) / 1e9, 3)}
+    out["sssp_grid4096"] = res
+    G.close()
+    del g, G, d, ref
     torch.cuda.empty_cache()
     return out
 
@@ -504,7 +540,10 @@ def run_ours(args):
         tfile = os.path.join(ROOT, "profiles", "pagerank_rmat22_traffic.json")
         if os.path.exists(tfile) and args.scale == 22:
             try:
-                traffic = json.load(open(tfile)).get("dram_bytes_per_launch")
+                tj = json.load(open(tfile))
+                # the capture is of the default variant's kernel
+                if variant == g1.DEFAULT_MERGE_VARIANT or f"variant {variant}," in tj.get("kernel", ""):
+                    traffic = tj.get("dram_bytes_per_launch")
             except Exception:
                 traffic = None
         result["roofline"] = {
@@ -641,8 +680,9 @@ def main():
                     help="requests of the serving-loop measurement (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=2000.0,
                     help="offered request rate (Poisson arrivals per second)")
-    ap.add_argument("--sched", default="tune",
-                    help="tune | auto | merge0..merge3 (kernel variant) | vector")
+    ap.add_argument("--sched", default="auto",
+                    help="auto (the library's default merge variant) | tune (time every "
+                         "variant and keep the fastest) | mergeN (variant N) | vector")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -463,6 +463,32 @@ __global__ void nnz_tile_seg_kernel(const uint32_t* rp, uint32_t n, uint32_t nnz
     tile_seg[t] = rank[lo];
 }
 
+// Tiles t >= 1 whose first nonzero continues a row begun earlier and in
+// which that row ends (another row starts inside, or the next tile starts
+// with a row, or the matrix ends).
+__global__ void nnz_fix_flag_kernel(const uint32_t* sbits, uint32_t n_tiles, uint32_t nnz, uint32_t tile,
+                                    uint32_t* flag) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > n_tiles) return;
+    uint32_t f = 0;
+    if (t > 0 && t < n_tiles) {
+        const uint32_t w0 = t * (tile / 32);
+        if (!(sbits[w0] & 1u)) {
+            uint32_t any = 0;
+            for (uint32_t q = 0; q < tile / 32; ++q) any |= sbits[w0 + q];
+            const bool end_start = (uint64_t)(t + 1) * tile >= nnz || (sbits[w0 + tile / 32] & 1u);
+            f = (any != 0u || end_start) ? 1u : 0u;
+        }
+    }
+    flag[t] = f;
+}
+
+__global__ void nnz_fix_place_kernel(const uint32_t* flag, const uint32_t* pos, uint32_t n_tiles,
+                                     uint32_t* fix_tiles) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n_tiles && flag[t]) fix_tiles[pos[t]] = t;
+}
+
 g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
     Orientation& o = g->o[t];
     if (!o.present) return fail(G1_ERR_UNSUPPORTED, "orientation not built");
@@ -499,7 +525,30 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
                                     p->sbits.as<uint32_t>());
     nnz_tile_seg_kernel<<<(uint32_t)ceil_div((uint64_t)p->n_tiles + 1, 256), 256>>>(
         o.rp, n, m, rank.as<uint32_t>(), nne, p->n_tiles, kNnzTile, p->tile_seg.as<uint32_t>());
-    count_launches(3);
+    // tiles the fixup visits, in tile order (a deterministic compaction)
+    {
+        DevBuf fflag, fpos, ftemp;
+        G1_TRY(fflag.ensure(((size_t)p->n_tiles + 1) * 4));
+        G1_TRY(fpos.ensure(((size_t)p->n_tiles + 1) * 4));
+        const uint32_t tb = (uint32_t)ceil_div((uint64_t)p->n_tiles + 1, 256);
+        nnz_fix_flag_kernel<<<tb, 256>>>(p->sbits.as<uint32_t>(), p->n_tiles, m, kNnzTile,
+                                         fflag.as<uint32_t>());
+        size_t sb = 0;
+        G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, sb, fflag.as<uint32_t>(), fpos.as<uint32_t>(),
+                                              (int)p->n_tiles + 1));
+        G1_TRY(ftemp.ensure(sb + 16));
+        G1_CUDA(cub::DeviceScan::ExclusiveSum(ftemp.p, sb, fflag.as<uint32_t>(), fpos.as<uint32_t>(),
+                                              (int)p->n_tiles + 1));
+        uint32_t nfix = 0;
+        G1_CUDA(cudaMemcpy(&nfix, fpos.as<uint32_t>() + p->n_tiles, 4, cudaMemcpyDeviceToHost));
+        p->n_fix = nfix;
+        G1_TRY(p->fix_tiles.ensure(((size_t)nfix + 1) * 4));
+        nnz_fix_place_kernel<<<tb, 256>>>(fflag.as<uint32_t>(), fpos.as<uint32_t>(), p->n_tiles,
+                                          p->fix_tiles.as<uint32_t>());
+        G1_CUDA(cudaGetLastError());
+        G1_CUDA(cudaDeviceSynchronize());
+    }
+    count_launches(5);
     G1_CUDA(cudaGetLastError());
     G1_CUDA(cudaDeviceSynchronize());
     *out = p.get();

@@ -72,8 +72,9 @@ struct MergePlan {
 // row holding each tile's first nonzero, the row-start bitmap over the
 // nonzeros, the non-empty rows in order followed by the empty rows.
 struct NnzPlan {
-    uint32_t n_tiles = 0, n_nonempty = 0, n_empty = 0;
+    uint32_t n_tiles = 0, n_nonempty = 0, n_empty = 0, n_fix = 0;
     DevBuf tile_seg, sbits, rows, carry, tail;
+    DevBuf fix_tiles;  // tiles in which a row begun in an earlier tile ends
 };
 
 struct Orientation {

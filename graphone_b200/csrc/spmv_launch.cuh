@@ -136,7 +136,7 @@ struct NnzKernel {
 };
 
 inline uint32_t nnz_fix_grid(const NnzPlan& p) {
-    return (uint32_t)std::max<uint64_t>(1, ceil_div(std::max(p.n_tiles, p.n_empty), kMergeBlock));
+    return (uint32_t)std::max<uint64_t>(1, ceil_div(std::max(p.n_fix, p.n_empty), kMergeBlock));
 }
 
 // Per-instantiation launch facts of the merge kernel.
@@ -197,6 +197,9 @@ NnzArgs<SR> nnz_args(const g1_graph* g, int t, const NnzPlan& p, const typename 
     a.plan.sbits = p.sbits.as<uint32_t>();
     a.plan.nz_rows = p.rows.as<uint32_t>();
     a.plan.empty_rows = p.rows.as<uint32_t>() + p.n_nonempty;
+    a.plan.row_ptr = o.rp;
+    a.plan.n_fix = p.n_fix;
+    a.plan.fix_tiles = p.fix_tiles.as<uint32_t>();
     a.col = o.col;
     a.val = static_cast<const typename SR::w_t*>(o.val);
     a.x = x;

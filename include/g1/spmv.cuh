@@ -954,8 +954,8 @@ spmv_fixup_kernel(MergeArgs<SR> a, Epi epi) {
 //   3. the tile's complete rows are emitted in row order, 32 at a time
 //      (coalesced row-id loads and epilogue stores);
 //   4. a row open at the tile end leaves its partial in carry[t]; the part
-//      of a row begun in an earlier tile goes to tail[t]; empty rows and
-//      rows that cross tiles are finished by spmv_nnz_fixup_kernel.
+//      of a row begun in an earlier tile goes to tail[t]; rows that cross
+//      tiles and the empty rows are finished by spmv_nnz_fixup_kernel.
 // Work per tile is exactly 256 nonzeros whatever the degree distribution;
 // empty rows cost nothing here.
 
@@ -972,6 +972,9 @@ struct NnzPlanView {
     const uint32_t* sbits;       // row-start bitmap, zero-padded to n_tiles*8 + 1 words
     const uint32_t* nz_rows;     // non-empty rows in order
     const uint32_t* empty_rows;  // n_empty
+    const uint32_t* row_ptr;     // n_rows + 1
+    uint32_t n_fix;
+    const uint32_t* fix_tiles;   // tiles in which a row begun in an earlier tile ends
 };
 
 template <class SR>
@@ -1243,63 +1246,58 @@ __device__ __forceinline__ bool nnz_start_bit(const uint32_t* sbits, uint32_t k)
     return (__ldg(sbits + (k >> 5)) >> (k & 31)) & 1u;
 }
 
-// Rows that cross nnz tiles (deterministic fold of the tiles' partials in
-// tile order, like spmv_fixup_kernel) and the empty rows (identity).
+// Rows that cross nnz tiles, one thread per tile in which such a row ends
+// (the plan lists them): a deterministic fold of the tiles' partials in
+// tile order, like spmv_fixup_kernel; and the empty rows (identity), one
+// per thread.
 template <class SR, class Epi, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 spmv_nnz_fixup_kernel(NnzArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
     __shared__ alignas(16) char epi_smem[64 * 8];
-    const uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
+    const uint32_t i = blockIdx.x * BLOCK + threadIdx.x;
     const uint32_t lane = lane_id();
     const NnzPlanView& p = a.plan;
     epi.begin();
     bool longc = false;
-    uint32_t row = 0, seg = 0;
+    uint32_t row = 0, first = 0, t = 0;
     V acc = SR::identity();
-    if (t > 0 && t < p.n_tiles) {
-        const uint32_t j0 = t * kNnzTile;
-        if (!nnz_start_bit(p.sbits, j0)) {
-            // does the row begun earlier end in this tile?
-            uint32_t any = __ldg(p.sbits + (j0 >> 5)) & ~1u;
-#pragma unroll
-            for (uint32_t q = 1; q < kNnzTile / 32; ++q) any |= __ldg(p.sbits + (j0 >> 5) + q);
-            const bool ends = any != 0u || j0 + kNnzTile >= p.nnz || nnz_start_bit(p.sbits, j0 + kNnzTile);
-            if (ends) {
-                seg = __ldg(p.tile_seg + t);
-                row = __ldg(p.nz_rows + seg);
-                acc = SR::reduce(a.carry[t - 1], a.tail[t]);
-                if (t >= 2 && __ldg(p.tile_seg + t - 1) == seg &&
-                    !nnz_start_bit(p.sbits, (t - 1) * kNnzTile))
-                    longc = true;  // the row also covers tile t-2 or earlier
-                else
-                    epi.emit(row, acc);
-            }
-        }
+    if (i < p.n_fix) {
+        t = __ldg(p.fix_tiles + i);  // >= 1
+        row = __ldg(p.nz_rows + __ldg(p.tile_seg + t));
+        acc = SR::reduce(a.carry[t - 1], a.tail[t]);
+        // the tile holding the row's first nonzero
+        first = __ldg(p.row_ptr + row) / kNnzTile;
+        if (first + 1 < t)
+            longc = true;  // the row also covers tile t-2 or earlier
+        else
+            epi.emit(row, acc);
     }
     unsigned pending = __ballot_sync(0xffffffffu, longc);
     while (pending) {
         const int src = __ffs(pending) - 1;
         pending &= pending - 1;
-        const uint32_t sg = __shfl_sync(0xffffffffu, seg, src);
-        const uint32_t tt = blockIdx.x * BLOCK + (threadIdx.x & ~31u) + (uint32_t)src;
-        // first tile whose first nonzero lies in row sg
-        uint32_t lo = 0, hi = tt - 1;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (__ldg(p.tile_seg + mid) < sg) lo = mid + 1; else hi = mid;
+        const uint32_t f0 = __shfl_sync(0xffffffffu, first, src);
+        const uint32_t tt = __shfl_sync(0xffffffffu, t, src);
+        // carries of the tiles [f0, tt-1) (tile tt-1's is already in acc);
+        // four independent partial folds keep four loads in flight per lane
+        V part = SR::identity(), p1 = SR::identity(), p2 = SR::identity(), p3 = SR::identity();
+        uint32_t k = f0 + lane;
+        for (; k + 96 + 1 < tt; k += 128) {
+            part = SR::reduce(part, a.carry[k]);
+            p1 = SR::reduce(p1, a.carry[k + 32]);
+            p2 = SR::reduce(p2, a.carry[k + 64]);
+            p3 = SR::reduce(p3, a.carry[k + 96]);
         }
-        // the row began inside tile lo-1 unless tile lo starts exactly at it
-        const uint32_t first = (lo > 0 && !nnz_start_bit(p.sbits, lo * kNnzTile)) ? lo - 1 : lo;
-        V part = SR::identity();
-        for (uint32_t k = first + lane; k + 1 < tt; k += 32) part = SR::reduce(part, a.carry[k]);
+        for (; k + 1 < tt; k += 32) part = SR::reduce(part, a.carry[k]);
+        part = SR::reduce(SR::reduce(part, p1), SR::reduce(p2, p3));
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1)
             part = SR::reduce(part, shfl_down_any(0xffffffffu, part, off));
         part = shfl_any(0xffffffffu, part, 0);
         if ((int)lane == src) epi.emit(row, SR::reduce(part, acc));
     }
-    for (uint32_t i = t; i < p.n_empty; i += gridDim.x * BLOCK) epi.emit(__ldg(p.empty_rows + i), SR::identity());
+    for (uint32_t e = i; e < p.n_empty; e += gridDim.x * BLOCK) epi.emit(__ldg(p.empty_rows + e), SR::identity());
     epi.template block_end<BLOCK>(epi_smem);
 }
 
