@@ -1,0 +1,36 @@
+"""GraphOne's unchanged SSSP apps, built against GraphOne's own headers
+(oracle/_ref/apps_ref) and against this repository's include/
+(oracle/_ref/apps_g1) by `make -C oracle refapps dropin`, run on the same
+generated inputs; prints each app's own "Elapsed" line, wall time and parity
+with the oracle's Dijkstra.  A checker, not part of the library.
+
+    python oracle/compare_apps.py
+"""
+import os, subprocess, sys, time, tempfile
+import numpy as np
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+from graphone_b200 import gen
+from oracle import oracle as O
+tmp = tempfile.mkdtemp()
+cases = {"rmat14": (gen.rmat(14, 16, True, (1, 64)), False),
+         "grid256": (gen.grid2d(256, 256, (1, 100)), False)}
+for name, (g, directed) in cases.items():
+    adj = os.path.join(tmp, name + ".adj")
+    gen.write_adj(g, adj, directed)
+    rp, ci, v = g.np("n")
+    exp = O.dijkstra_u32(rp, ci, v, 0)
+    for app in ["sssp_blas", "sssp_blas2", "sssp_adv"]:
+        for kind in ["ref", "g1"]:
+            path = O.app(kind, app)
+            if not path: continue
+            out = os.path.join(tmp, f"{name}_{app}_{kind}.txt")
+            t0 = time.time()
+            r = subprocess.run([path, "-i", adj, "--src", "0", "-o", out], capture_output=True, text=True, timeout=600)
+            wall = time.time() - t0
+            if r.returncode != 0:
+                print(name, app, kind, "FAILED rc", r.returncode, r.stdout[-300:], r.stderr[-300:]); continue
+            lines = open(out).read().splitlines()
+            vals = np.array([float(l.split("-",1)[1]) for l in lines[1:]], dtype=np.float64)
+            e = exp[:len(vals)].astype(np.float64); e[exp[:len(vals)] == O.U32_MAX] = float(np.float32(3.4028234663852886e38))
+            ok = np.array_equal(vals.astype(np.float32), e.astype(np.float32))
+            print(f"{name:8s} {app:11s} {kind:4s} {lines[0]:28s} wall={wall:.2f}s parity={ok}")
