@@ -8,7 +8,9 @@ with the oracle's Dijkstra.  A checker, not part of the library.
 """
 import os, subprocess, sys, time, tempfile
 import numpy as np
-sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+_HERE = os.path.dirname(os.path.abspath(__file__))
+# the repository root, not this directory (whose oracle.py would shadow the package)
+sys.path[:] = [os.path.dirname(_HERE)] + [q for q in sys.path if os.path.abspath(q or ".") != _HERE]
 from graphone_b200 import gen
 from oracle import oracle as O
 tmp = tempfile.mkdtemp()
