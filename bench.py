@@ -152,13 +152,21 @@ def dist_info():
 
 
 def max_over_ranks(x: float, ws: int):
+    """Max of x over the ranks (the job's time is its slowest rank's)."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(units_per_rank_step: float, steps: int, ms_max: float, ws: int) -> float:
+    """Whole-job throughput of replicas: every rank processes the same
+    units per step, the job takes the slowest rank's time."""
+    return ws * units_per_rank_step * steps / (ms_max / 1e3)
 
 
 def barrier(ws: int):
@@ -474,7 +482,7 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, ws)
     per_step_bytes = spmv_bytes(n, m) * iters
-    value = ws * per_step_bytes * args.steps / (ms_max / 1e3) / 1e9
+    value = job_rate(per_step_bytes, args.steps, ms_max, ws) / 1e9
     clocks = clk.summary()
 
     # end to end through the C ABI with host buffers
@@ -497,7 +505,7 @@ def run_ours(args):
     e3.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e2.elapsed_time(e3), ws)
-    e2e_value = ws * per_step_bytes * args.steps / (e2e_ms / 1e3) / 1e9
+    e2e_value = job_rate(per_step_bytes, args.steps, e2e_ms, ws) / 1e9
     h2d = 4 * (n + 1) + 8 * m
     d2h = 4 * n
 
