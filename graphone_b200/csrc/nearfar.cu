@@ -121,6 +121,18 @@ __global__ void nf_init_kernel(uint32_t n, uint32_t src, const uint32_t* perm, u
     }
 }
 
+// Position for one entry in a queue, one atomic per group of converged
+// lanes (the lanes executing this call together share a single atomicAdd).
+__device__ __forceinline__ uint32_t agg_slot(uint32_t* ctr) {
+    const unsigned mask = __activemask();
+    const uint32_t lane = lane_id();
+    const int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+}
+
 template <bool UNIT>
 __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
     const uint32_t nb = gridDim.x;
@@ -155,24 +167,43 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
             const uint32_t* in = a.near[par];
             uint32_t* outq = a.near[par ^ 1];
             uint32_t* farq = a.far[fp];
-            for (uint32_t i = gt; i < qn; i += gs) {
-                const uint32_t u = in[i];
-                const uint32_t du = ld_vol(a.dist + u);
-                const uint32_t e1 = a.rp[u + 1];
-                for (uint32_t e = a.rp[u]; e < e1; ++e) {
-                    const uint32_t v = a.col[e];
-                    const uint32_t nd = du + (UNIT ? 1u : a.val[e]);
-                    // no plain pre-check: one dependent memory access fewer
-                    // on the critical path of a step
-                    if (nd >= atomicMin(a.dist + v, nd)) continue;
-                    if (nd < T) {
-                        // BFS: every improvement in a step sets the same level,
-                        // so only the first one succeeds -- no duplicate to stamp
-                        if (UNIT || atomicExch(a.stamp + v, gen) != gen) outq[atomicAdd(&c->qn[nxt], 1u)] = v;
-                    } else if (atomicExch(a.fstamp + v, bucket) != bucket) {
-                        farq[atomicAdd(&c->fn[fp], 1u)] = v;
-                    }
+            auto relax = [&](uint32_t du, uint32_t e) {
+                const uint32_t v = a.col[e];
+                const uint32_t nd = du + (UNIT ? 1u : a.val[e]);
+                // no plain pre-check: one dependent memory access fewer on the
+                // critical path of a step
+                if (nd >= atomicMin(a.dist + v, nd)) return;
+                if (nd < T) {
+                    // BFS: every improvement in a step sets the same level, so
+                    // only the first one succeeds -- no duplicate to stamp
+                    if (UNIT || atomicExch(a.stamp + v, gen) != gen) outq[agg_slot(&c->qn[nxt])] = v;
+                } else if (atomicExch(a.fstamp + v, bucket) != bucket) {
+                    farq[agg_slot(&c->fn[fp])] = v;
                 }
+            };
+            const uint32_t lane = lane_id();
+            // warp-uniform rounds: lists of 32 or more edges are pushed by the
+            // whole warp, shorter ones by their own lane
+            for (uint32_t base = gt - lane; base < qn; base += gs) {
+                const uint32_t i = base + lane;
+                uint32_t du = 0, b = 0, e1 = 0;
+                if (i < qn) {
+                    const uint32_t u = in[i];
+                    du = ld_vol(a.dist + u);
+                    b = a.rp[u];
+                    e1 = a.rp[u + 1];
+                }
+                unsigned big = __ballot_sync(0xffffffffu, e1 - b >= 32);
+                while (big) {
+                    const int src = __ffs(big) - 1;
+                    big &= big - 1;
+                    const uint32_t bb = __shfl_sync(0xffffffffu, b, src);
+                    const uint32_t ee = __shfl_sync(0xffffffffu, e1, src);
+                    const uint32_t dd = __shfl_sync(0xffffffffu, du, src);
+                    for (uint32_t e = bb + lane; e < ee; e += 32) relax(dd, e);
+                }
+                if (e1 - b < 32)
+                    for (uint32_t e = b; e < e1; ++e) relax(du, e);
             }
             par ^= 1;
         } else if (step == 1) {
@@ -208,9 +239,9 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
                 const uint32_t d = ld_vol(a.dist + v);
                 if (d < T) continue;
                 if (d < tn) {
-                    if (atomicExch(a.stamp + v, gen) != gen) outq[atomicAdd(&c->qn[nxt], 1u)] = v;
+                    if (atomicExch(a.stamp + v, gen) != gen) outq[agg_slot(&c->qn[nxt])] = v;
                 } else if (atomicExch(a.fstamp + v, bucket) != bucket) {
-                    fout[atomicAdd(&c->fn[fp ^ 1], 1u)] = v;
+                    fout[agg_slot(&c->fn[fp ^ 1])] = v;
                 }
             }
             par ^= 1;

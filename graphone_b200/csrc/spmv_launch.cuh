@@ -21,7 +21,7 @@ constexpr int kVectorBlock = 256;
 //   kind 3: nnz-split warp tiles of 256 nonzeros (16-byte loads, row-start
 //           bitmap; its own plan instead of the merge-path partition);
 //           stages: bit 0 = L2 cache policies, bit 1 = three-tile software
-//           pipeline per warp.
+//           pipeline per warp, bit 2 = next-tile L1 prefetch.
 // `warps` per block (kind 0/2/3), `hot` x entries cached in shared memory,
 // `minb` resident blocks per SM the register budget is sized for.
 struct MergeVariant {
@@ -40,8 +40,8 @@ constexpr MergeVariant kMergeVariants[] = {
     {3, 8, 0, 32, 0, 1},      {3, 8, 1, 32, 16384, 1},  {3, 8, 1, 16, 16384, 2},
     {3, 8, 1, 16, 8192, 3},   {3, 8, 0, 16, 8192, 3},   {3, 8, 0, 32, 32768, 1},
     {3, 8, 0, 32, 49152, 1},  {3, 8, 2, 24, 32768, 1},  {3, 8, 2, 16, 32768, 1},
-    {3, 8, 3, 24, 32768, 1}};
-constexpr int kNumMergeVariants = 22;
+    {3, 8, 3, 24, 32768, 1},  {3, 8, 4, 32, 32768, 1},  {3, 8, 4, 32, 16384, 1}};
+constexpr int kNumMergeVariants = 24;
 constexpr int kDefaultVariant = 17;
 
 template <class K>
@@ -117,12 +117,13 @@ struct WarpMergeKernel {
     }
 };
 
-template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false>
+template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false,
+          bool PFL1 = false>
 struct NnzKernel {
     using L = NnzLayout<SR, WARPS, HOT>;
     static int occupancy() {
         static int occ = [] {
-            auto k = spmv_nnz_kernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE>;
+            auto k = spmv_nnz_kernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
             return blocks_per_sm(k, WARPS * 32, L::BYTES);
         }();
@@ -208,15 +209,16 @@ NnzArgs<SR> nnz_args(const g1_graph* g, int t, const NnzPlan& p, const typename 
     return a;
 }
 
-template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false>
+template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false,
+          bool PFL1 = false>
 g1_status launch_nnz(g1_graph* g, int t, const NnzPlan& p, const typename SR::x_t* x,
                      const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
-    using K = NnzKernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE>;
+    using K = NnzKernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1>;
     const NnzArgs<SR> a = nnz_args<SR>(g, t, p, x);
     const bool prof = profiling();
     // launched even without tiles: its blocks' epilogue partials are read
     if (prof) prof_mark(s, true);
-    spmv_nnz_kernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE>
+    spmv_nnz_kernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1>
         <<<K::grid(g, p.n_tiles), WARPS * 32, K::L::BYTES, s>>>(a, main_epi);
     if (prof) prof_mark(s, false);
     count_launches(1);
@@ -246,6 +248,8 @@ g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_gri
             case 19: *main_grid = NnzKernel<SR, Epi, 24, 1, 32768, false, true>::grid(g, q->n_tiles); break;
             case 20: *main_grid = NnzKernel<SR, Epi, 16, 1, 32768, false, true>::grid(g, q->n_tiles); break;
             case 21: *main_grid = NnzKernel<SR, Epi, 24, 1, 32768, true, true>::grid(g, q->n_tiles); break;
+            case 22: *main_grid = NnzKernel<SR, Epi, 32, 1, 32768, false, false, true>::grid(g, q->n_tiles); break;
+            case 23: *main_grid = NnzKernel<SR, Epi, 32, 1, 16384, false, false, true>::grid(g, q->n_tiles); break;
             default: *main_grid = NnzKernel<SR, Epi, 32, 1, 16384>::grid(g, q->n_tiles); break;
         }
         *fix_grid = nnz_fix_grid(*q);
@@ -343,6 +347,8 @@ g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi&
             case 19: return launch_nnz<SR, Epi, 24, 1, 32768, false, true>(g, t, *q, x, main_epi, fix_epi, s);
             case 20: return launch_nnz<SR, Epi, 16, 1, 32768, false, true>(g, t, *q, x, main_epi, fix_epi, s);
             case 21: return launch_nnz<SR, Epi, 24, 1, 32768, true, true>(g, t, *q, x, main_epi, fix_epi, s);
+            case 22: return launch_nnz<SR, Epi, 32, 1, 32768, false, false, true>(g, t, *q, x, main_epi, fix_epi, s);
+            case 23: return launch_nnz<SR, Epi, 32, 1, 16384, false, false, true>(g, t, *q, x, main_epi, fix_epi, s);
             default: return launch_nnz<SR, Epi, 32, 1, 16384>(g, t, *q, x, main_epi, fix_epi, s);
         }
     }

@@ -208,6 +208,10 @@ __device__ __forceinline__ uint32_t ldg_u32_policy(const void* ptr, uint64_t pol
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
+// Brings the line holding `p` into this SM's L1 ahead of use.
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 
 __host__ __device__ __forceinline__ uint64_t ceil_div(uint64_t a, uint64_t b) {
     return (a + b - 1) / b;

@@ -1182,10 +1182,12 @@ __device__ __forceinline__ void nnz_finish(const NnzArgs<SR>& a, const NnzReady<
 }
 
 // HINTS: col/val are streamed with an evict-first L2 policy, x gathers use
-// evict-last (x stays in L2 across the iteration).  PIPE: a three-tile
+// evict-last (x stays in L2 across the iteration).  PFL1: each warp
+// prefetches its next tile's col/val lines into L1.  PIPE: a three-tile
 // software pipeline per warp -- while tile A is folded, the x gathers of
 // tile B and the col/val loads of tile C are in flight.
-template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false>
+template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false,
+          bool PFL1 = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
 spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
@@ -1212,6 +1214,15 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
     }
     if constexpr (!PIPE) {
         for (uint32_t tile = blockIdx.x * WARPS + w; tile < n_tiles; tile += total_warps) {
+            if constexpr (PFL1) {
+                // the next tile's 8 col and 8 val lines into L1 while this one runs
+                const uint32_t nt = tile + total_warps;
+                const uint32_t lane = lane_id();
+                if (nt < n_tiles && lane < 16) {
+                    const uint32_t jn = nt * kNnzTile + (lane & 7u) * 32u;
+                    prefetch_l1(lane < 8 ? (const void*)(a.col + jn) : (const void*)(a.val + jn));
+                }
+            }
             const NnzIn in = nnz_load<SR, HINTS>(a, tile, pol_stream);
             const NnzReady<SR, Epi> r = nnz_gather<SR, Epi, HOT, HINTS>(a, in, xc, hot, pol_keep, epi);
             nnz_finish<SR, Epi>(a, r, tile, sy, epi);
