@@ -204,30 +204,28 @@ T transform_reduce(It first, It last, Op op, T init, Bop bop) {
 namespace cuda {
 
 // Atomic minimum returning the previous value (reference:
-// archi/only/cuda.cuh:52-70): native for integers; for floating point a
-// compare-and-swap loop that gives up as soon as the stored value is not
-// larger than `value`.
+// archi/only/cuda.cuh:52-70).  Native for integers.  For floating point, one
+// hardware integer atomic instead of a compare-and-swap loop: non-negative
+// IEEE values order like their bit patterns as signed integers, negative ones
+// reversed as unsigned integers, so a non-negative `value` is an integer
+// atomicMin and a negative one an unsigned atomicMax on the same word (a
+// stored negative value is never replaced by a non-negative one, and the
+// reverse holds too).  NaN never replaces the stored value.
 template <typename T>
 __device__ __forceinline__ T AtomicMin(T* address, T value) {
     if constexpr (std::is_same_v<T, float>) {
-        int* p = reinterpret_cast<int*>(address);
-        int cur = *reinterpret_cast<volatile int*>(p);
-        while (__int_as_float(cur) > value) {
-            const int prev = atomicCAS(p, cur, __float_as_int(value));
-            if (prev == cur) break;
-            cur = prev;
-        }
-        return __int_as_float(cur);
+        if (value != value) return *reinterpret_cast<volatile float*>(address);
+        if (!signbit(value))
+            return __int_as_float(::atomicMin(reinterpret_cast<int*>(address), __float_as_int(value)));
+        return __uint_as_float(
+            ::atomicMax(reinterpret_cast<unsigned int*>(address), __float_as_uint(value)));
     } else if constexpr (std::is_same_v<T, double>) {
-        unsigned long long* p = reinterpret_cast<unsigned long long*>(address);
-        unsigned long long cur = *reinterpret_cast<volatile unsigned long long*>(p);
-        while (__longlong_as_double((long long)cur) > value) {
-            const unsigned long long prev =
-                atomicCAS(p, cur, (unsigned long long)__double_as_longlong(value));
-            if (prev == cur) break;
-            cur = prev;
-        }
-        return __longlong_as_double((long long)cur);
+        if (value != value) return *reinterpret_cast<volatile double*>(address);
+        if (!signbit(value))
+            return __longlong_as_double(::atomicMin(reinterpret_cast<long long*>(address),
+                                                    __double_as_longlong(value)));
+        return __longlong_as_double((long long)::atomicMax(
+            reinterpret_cast<unsigned long long*>(address), (unsigned long long)__double_as_longlong(value)));
     } else {
         return ::atomicMin(address, value);
     }

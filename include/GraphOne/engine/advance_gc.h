@@ -30,30 +30,36 @@ namespace graph_one {
 namespace engine {
 namespace adv_detail {
 
-// append with a capacity check; an overflow is recorded, never written
+// append with a capacity check (an overflow is recorded, never written);
+// the appended vertices' out-degrees add to `deg_acc`, flushed once per warp
+// at the end of the kernel (deg_flush) instead of one atomic per append
 __device__ __forceinline__ void append_capped(uint32_t* out, uint32_t* ctr, uint32_t cap,
-                                              uint32_t v, uint32_t deg) {
+                                              uint32_t v, uint32_t deg, unsigned long long& deg_acc) {
     const unsigned mask = __activemask();
     const int leader = __ffs(mask) - 1;
     const uint32_t lane = g1::lane_id();
-    const uint32_t tot = __reduce_add_sync(mask, deg);
     uint32_t base = 0;
-    if ((int)lane == leader) {
-        base = atomicAdd(&ctr[0], (uint32_t)__popc(mask));
-        atomicAdd(reinterpret_cast<unsigned long long*>(ctr + 2), (unsigned long long)tot);
-    }
+    if ((int)lane == leader) base = atomicAdd(&ctr[0], (uint32_t)__popc(mask));
     base = __shfl_sync(mask, base, leader);
     const uint32_t slot = base + __popc(mask & ((1u << lane) - 1u));
     if (slot < cap)
         out[slot] = v;
     else
         atomicExch(&ctr[1], 1u);
+    deg_acc += deg;
+}
+
+// warp-wide sum of the lanes' degree accumulators into ctr[2..3] (u64)
+__device__ __forceinline__ void deg_flush(uint32_t* ctr, unsigned long long deg_acc) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) deg_acc += __shfl_xor_sync(0xffffffffu, deg_acc, off);
+    if (g1::lane_id() == 0 && deg_acc) atomicAdd(reinterpret_cast<unsigned long long*>(ctr + 2), deg_acc);
 }
 
 template <class F, class V, class E, class W, class D>
 __device__ __forceinline__ void visit(V src, V dst, E e, W w, D& ds, const E* rp, uint32_t* out,
-                                      uint32_t* ctr, uint32_t cap) {
-    if (F::advance(src, dst, e, w, ds)) append_capped(out, ctr, cap, dst, rp[dst + 1] - rp[dst]);
+                                      uint32_t* ctr, uint32_t cap, unsigned long long& deg_acc) {
+    if (F::advance(src, dst, e, w, ds)) append_capped(out, ctr, cap, dst, rp[dst + 1] - rp[dst], deg_acc);
 }
 
 template <class F, class V, class E, class W, class D, vstart_t VS>
@@ -65,6 +71,7 @@ advance_kernel(const E* rp, const V* col, const W* val, D ds, const V* in, uint3
     const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t rounds = (n_in + warps * 32 - 1) / (warps * 32);
     D local = ds;  // functors may mutate their copy (reference: passed by value)
+    unsigned long long deg_acc = 0;
     for (uint32_t r = 0; r < rounds; ++r) {
         const uint32_t i = (r * warps + wid) * 32 + lane;
         V u = utils::invalid_vertex<VS, V>();
@@ -83,11 +90,13 @@ advance_kernel(const E* rp, const V* col, const W* val, D ds, const V* in, uint3
             const V uu = __shfl_sync(0xffffffffu, u, src);
             const E bb = __shfl_sync(0xffffffffu, b, src);
             const E ee = __shfl_sync(0xffffffffu, e, src);
-            for (E k = bb + lane; k < ee; k += 32) visit<F>(uu, col[k], k, val[k], local, rp, out, ctr, cap);
+            for (E k = bb + lane; k < ee; k += 32)
+                visit<F>(uu, col[k], k, val[k], local, rp, out, ctr, cap, deg_acc);
         }
         if (e - b < 32)
-            for (E k = b; k < e; ++k) visit<F>(u, col[k], k, val[k], local, rp, out, ctr, cap);
+            for (E k = b; k < e; ++k) visit<F>(u, col[k], k, val[k], local, rp, out, ctr, cap, deg_acc);
     }
+    deg_flush(ctr, deg_acc);
 }
 
 // The filter reads the advance's output size from device memory (*n_dev),
@@ -96,11 +105,17 @@ template <class F, class V, class E, class D, vstart_t VS>
 __global__ void filter_kernel(const E* rp, D ds, const V* in, const uint32_t* n_dev, uint32_t* out,
                               uint32_t* ctr, uint32_t cap) {
     const uint32_t n = min(*n_dev, cap);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned long long deg_acc = 0;
+    // warp-uniform rounds so that every lane reaches the final flush
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint32_t i = base + g1::lane_id();
+        if (i >= n) continue;
         const V v = in[i];
         if (utils::is_vertex_valid<VS>(v) && !F::filter(v, ds))
-            append_capped(out, ctr, cap, v, rp[v + 1] - rp[v]);
+            append_capped(out, ctr, cap, v, rp[v + 1] - rp[v], deg_acc);
     }
+    deg_flush(ctr, deg_acc);
 }
 
 template <class V, class E, vstart_t VS>

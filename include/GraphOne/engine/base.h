@@ -62,21 +62,16 @@ inline int sm_count() {
     return n;
 }
 
-// Device counters and a pinned mirror for the one read-back per iteration:
+// Device counters and a host mirror for the one read-back per iteration:
 // [0] appended vertices, [1] overflow flag, [2..3] out-degree sum (u64);
-// [4..7] the same for a second compaction in the same step.
+// [4..7] the same for a second compaction in the same step.  The mirror is
+// ordinary host memory: a pinned allocation costs milliseconds when an
+// engine is built, more than all the read-backs of a typical run.
 struct Counters {
     uint32_t* dev = nullptr;
-    uint32_t* host = nullptr;
-    Counters() {
-        check_g1(g1_mem_alloc(reinterpret_cast<void**>(&dev), 64), "counters");
-        check_cuda(cudaHostAlloc(reinterpret_cast<void**>(&host), 64, cudaHostAllocDefault),
-                   "pinned counters");
-    }
-    ~Counters() {
-        g1_mem_free(dev);
-        cudaFreeHost(host);
-    }
+    uint32_t host[16] = {};
+    Counters() { check_g1(g1_mem_alloc(reinterpret_cast<void**>(&dev), 64), "counters"); }
+    ~Counters() { g1_mem_free(dev); }
     Counters(const Counters&) = delete;
     Counters& operator=(const Counters&) = delete;
     void clear(cudaStream_t s) { check_cuda(cudaMemsetAsync(dev, 0, 32, s), "clear counters"); }

@@ -15,6 +15,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "graphone_b200.h"
 #include "GraphOne/loader/loader.h"
 #include "GraphOne/macros.h"
@@ -163,6 +165,10 @@ template <arch_t arch, graph_view_t views, vstart_t v_start, typename vertex_t, 
 Graph<arch, views, v_start, empty_t, vertex_t, edge_t, weight_t> build(
     EdgeCache<v_start, weight_t, vertex_t, edge_t>& cache) {
     using G = Graph<arch, views, v_start, empty_t, vertex_t, edge_t, weight_t>;
+    // The application's own CUDA runtime (its kernels live in its binary)
+    // starts here, with the graph, rather than inside the first Run; the
+    // library's runtime starts with g1_graph_create below.
+    if constexpr (arch == arch_t::cuda) cudaFree(nullptr);
     std::vector<edge_t> rp;
     std::vector<vertex_t> ci;
     std::vector<weight_t> val;
