@@ -1,10 +1,11 @@
 // g1_spmv_noalloc: the merge-path SpMV for callers that cannot allocate.
 //
-// Some callers of this library may not call cudaMalloc at all: code that runs
-// inside a CUDA stream capture that must stay free of allocations, a host
-// process that hands out device memory only through its own arena and
-// forbids the driver allocator, or a latency-critical loop where an
-// allocation's implicit synchronisation is unacceptable.  g1_spmv (the
+// Some callers of this library may not call cudaMalloc at all: a host
+// process that hands out device memory only through its own arena or caching
+// pool (a driver allocation outside it would break its accounting and
+// fragment the pool), a plugin loaded into such a host, or a
+// latency-critical loop where cudaMalloc's implicit device-wide
+// synchronisation is unacceptable.  g1_spmv (the
 // regular entry point) keeps its merge-path partition and per-tile carries in
 // memory owned by a g1_graph, created with cudaMalloc.  This entry point
 // instead uses one file-scope device array as its scratch: the caller passes
@@ -13,10 +14,16 @@
 // The scratch array holds the partition of (n + m) merge items into tiles of
 // kNoAllocItems items plus one carry and one tail value per tile, for at most
 // kNoAllocMaxTiles tiles (4 MiB).  Every GPU that loads the library holds
-// this array until the process exits.  All calls on a device share it:
-// calls whose work overlaps on the GPU race on it (serialise them, e.g. on
-// one stream).  Each call rewrites every element it later reads, so stale
-// contents from an earlier call are never used.
+// this array until the process exits.  All calls on a device share it, and it
+// keeps the last call's contents: calls whose work overlaps on the GPU race on
+// it (serialise them, e.g. on one stream).  Nothing in it needs to start at
+// zero: each call writes every element it later reads (the partition kernel
+// writes tile_row/tile_nnz, the tile kernel writes carry/tail of every tile)
+// before reading it, so stale contents from an earlier call are never used.
+//
+// The first call on each device looks up the array's device address with
+// cudaGetSymbolAddress (with that device current) and caches it; make that
+// first call before any stream capture.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -40,10 +47,12 @@ constexpr uint32_t kNoAllocMaxTiles = 1u << 18;       // (n + m) <= 58,720,256
 // tile_row, tile_nnz: max_tiles + 1 each; carry, tail: max_tiles + 1 4-byte values each
 constexpr size_t kNoAllocWords = 4 * ((size_t)kNoAllocMaxTiles + 1);
 
-__device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
 
 // Device address of the scratch array, per device, set up on the first call
-// made on that device (cudaGetSymbolAddress with the device current).
+// made on that device (cudaGetSymbolAddress with the device current).  In host
+// code g_noalloc_scratch names a host-side stand-in, never a device address:
+// only these looked-up pointers are passed to kernels.
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 uint32_t* g_scratch_addr[kMaxDevices] = {};

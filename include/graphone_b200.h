@@ -154,17 +154,21 @@ g1_status g1_spmv(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
  * engine/blas_gc.h:130-132). */
 g1_status g1_graph_set_schedule(g1_graph* g, int transpose, g1_schedule sched, int variant);
 /* y = A (semiring) x like g1_spmv, for callers that cannot allocate device
- * memory (inside a CUDA stream capture that must stay allocation-free, or
- * in a process whose device memory comes only from its own arena).  No
- * GraphOne counterpart: it has no equivalent in the reference.  The CSR
+ * memory: a process whose device memory comes only from its own arena or
+ * caching pool (a cudaMalloc outside it breaks the pool's accounting), a
+ * plugin loaded into such a host, or a latency-critical loop that cannot
+ * afford cudaMalloc's implicit device synchronisation.  No GraphOne
+ * counterpart: it has no equivalent in the reference.  The CSR
  * (row_ptr n+1, col and val m entries, 4-byte values), x and y are the
  * caller's device buffers; nothing is allocated and no g1_graph is needed.
  * Scratch (merge-path partition and per-tile carries) lives in one
  * file-scope device array of 4 MiB per GPU, held until the process exits:
  * n + m may be at most 58,720,256 (G1_ERR_INVALID beyond).  The first call
  * on a device looks up that array's device address; make that first call
- * outside any stream capture.  Calls that overlap on the GPU race on the
- * shared scratch: serialise them (one stream). */
+ * before any stream capture.  Every call shares the array and it keeps the
+ * last call's contents (each call rewrites what it reads, nothing needs
+ * zeroing); calls that overlap on the GPU race on it: serialise them (one
+ * stream). */
 g1_status g1_spmv_noalloc(const uint32_t* row_ptr, const uint32_t* col, const void* val,
                           uint32_t n, uint32_t m, g1_semiring sr, const void* x, void* y,
                           void* stream);

@@ -1,8 +1,9 @@
-"""g1_spmv_noalloc: the SpMV entry point for callers that cannot allocate
-device memory (stream captures that must stay allocation-free, processes
-whose device memory comes only from their own arena).  It keeps its scratch
-in one static device array instead of graph-owned buffers; its results must
-equal those of g1_spmv on the same inputs, call after call.
+"""g1_spmv_noalloc: the SpMV entry point for callers that cannot call
+cudaMalloc (processes whose device memory comes only from their own arena or
+caching pool, plugins inside such hosts, loops that cannot take cudaMalloc's
+implicit synchronisation).  It keeps its scratch in one static device array
+instead of graph-owned buffers; its results must equal those of g1_spmv on the
+same inputs, call after call.
 
 Collected last (file name) so that a failure here cannot hide the others; it
 must pass alone in a fresh process as well as after the other tests."""
