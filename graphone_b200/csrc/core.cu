@@ -489,6 +489,18 @@ __global__ void nnz_fix_place_kernel(const uint32_t* flag, const uint32_t* pos, 
     if (t < n_tiles && flag[t]) fix_tiles[pos[t]] = t;
 }
 
+// The fixup's per-entry facts, resolved once per graph instead of through
+// tile_seg -> rows -> row_ptr on every launch.
+__global__ void nnz_fix_info_kernel(const uint32_t* fix_tiles, uint32_t n_fix, const uint32_t* tile_seg,
+                                    const uint32_t* nz_rows, const uint32_t* rp, uint32_t tile,
+                                    uint4* info) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_fix) return;
+    const uint32_t t = fix_tiles[i];
+    const uint32_t row = nz_rows[tile_seg[t]];
+    info[i] = make_uint4(t, row, rp[row] / tile, 0u);
+}
+
 g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
     Orientation& o = g->o[t];
     if (!o.present) return fail(G1_ERR_UNSUPPORTED, "orientation not built");
@@ -545,10 +557,15 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
         G1_TRY(p->fix_tiles.ensure(((size_t)nfix + 1) * 4));
         nnz_fix_place_kernel<<<tb, 256>>>(fflag.as<uint32_t>(), fpos.as<uint32_t>(), p->n_tiles,
                                           p->fix_tiles.as<uint32_t>());
+        G1_TRY(p->fix_info.ensure(((size_t)nfix + 1) * 16));
+        if (nfix > 0)
+            nnz_fix_info_kernel<<<(uint32_t)ceil_div(nfix, 256), 256>>>(
+                p->fix_tiles.as<uint32_t>(), nfix, p->tile_seg.as<uint32_t>(), p->rows.as<uint32_t>(),
+                o.rp, kNnzTile, p->fix_info.as<uint4>());
         G1_CUDA(cudaGetLastError());
         G1_CUDA(cudaDeviceSynchronize());
     }
-    count_launches(5);
+    count_launches(p->n_fix > 0 ? 6 : 5);
     G1_CUDA(cudaGetLastError());
     G1_CUDA(cudaDeviceSynchronize());
     *out = p.get();

@@ -75,6 +75,7 @@ struct NnzPlan {
     uint32_t n_tiles = 0, n_nonempty = 0, n_empty = 0, n_fix = 0;
     DevBuf tile_seg, sbits, rows, carry, tail;
     DevBuf fix_tiles;  // tiles in which a row begun in an earlier tile ends
+    DevBuf fix_info;   // per such tile: {tile, row, first tile of the row, 0}
 };
 
 struct Orientation {

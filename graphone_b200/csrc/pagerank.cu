@@ -49,6 +49,7 @@ __device__ void fold_partials_last_block(double v, double* partials, uint32_t sl
 }
 
 struct PrEpilogue {
+    static constexpr bool kRowsIndependent = true;
     float* rank_next;
     float* x_next;
     const float* iw;
@@ -68,6 +69,9 @@ struct PrEpilogue {
 
     __device__ __forceinline__ void begin() {
         dang_local = 0.0;
+        // under programmatic dependent launch the fixup runs this before its
+        // dependency wait: dang_in was written by a grid that completed
+        // before this one launched (the previous fixup)
         base = dangling ? (float)((double)base0 + alpha_over_n * (*dang_in)) : base0;
     }
     __device__ __forceinline__ void emit(uint32_t v, const float& y) {

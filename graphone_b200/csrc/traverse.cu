@@ -35,6 +35,7 @@ namespace g1 {
 // (blas_gc.h:230-237): res != default_result && res < dist[v] -> update,
 // activate.  The degree sum of activated vertices feeds the push/pull choice.
 struct SparseApplyEpilogue {
+    static constexpr bool kRowsIndependent = true;
     uint32_t* dist;
     uint32_t* out;
     uint32_t* out_count;

@@ -175,6 +175,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
+// ------------------------------------------ programmatic dependent launch
+// For kernels launched with the programmatic stream serialization
+// attribute: grid_dependency_wait() returns once the preceding grid in the
+// stream has completed and its writes are visible; grid_launch_dependents()
+// lets the next grid start launching once every block of this grid has
+// issued it (or exited).  Both are no-ops for ordinary launches.
+__device__ __forceinline__ void grid_dependency_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void grid_launch_dependents() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ------------------------------------------------------- ceil division
 // ------------------------------------------ L2 cache policies and hints
 

@@ -975,6 +975,7 @@ struct NnzPlanView {
     const uint32_t* row_ptr;     // n_rows + 1
     uint32_t n_fix;
     const uint32_t* fix_tiles;   // tiles in which a row begun in an earlier tile ends
+    const uint4* fix_info;       // per such tile: {tile, row, tile of the row's first nonzero, 0}
 };
 
 template <class SR>
@@ -985,6 +986,7 @@ struct NnzArgs {
     const typename SR::x_t* x;
     typename SR::value_t* carry;  // n_tiles: partial of the row open at the tile end
     typename SR::value_t* tail;   // n_tiles: in-tile partial of a row begun earlier
+    uint32_t* err = nullptr;      // device error word (bounded waits of the bulk variant)
 };
 
 // Epilogues may split emit into prepare(row) -- the loads that depend only
@@ -995,7 +997,11 @@ struct has_prepare : std::false_type {};
 template <class E>
 struct has_prepare<E, std::void_t<decltype(std::declval<E&>().prepare(0u))>> : std::true_type {};
 
-template <class SR, int WARPS, int HOT>
+// Shared memory of one block: the x cache, the per-warp segment values,
+// with BULK the per-warp staging buffer of one tile's col (BULK 2) or col
+// and val (BULK 1), filled by bulk copies, and the warps' mbarriers, then
+// the epilogue's scratch.
+template <class SR, int WARPS, int HOT, int BULK = 0>
 struct NnzLayout {
     using V = typename SR::value_t;
     using X = typename SR::x_t;
@@ -1003,9 +1009,23 @@ struct NnzLayout {
     static constexpr size_t XC_BYTES = ((size_t)HOT * sizeof(X) + 15) / 16 * 16;
     static constexpr size_t SY_OFF = XC_OFF + XC_BYTES;
     static constexpr size_t SY_BYTES = ((size_t)WARPS * kNnzTile * sizeof(V) + 15) / 16 * 16;
-    static constexpr size_t EPI_OFF = SY_OFF + SY_BYTES;
+    static constexpr size_t ST_OFF = SY_OFF + SY_BYTES;
+    static constexpr size_t ST_WARP = (BULK == 2 ? 1 : 2) * kNnzTile * 4;  // col [then val]
+    static constexpr size_t ST_BYTES = BULK ? (size_t)WARPS * ST_WARP : 0;
+    static constexpr size_t BAR_OFF = ST_OFF + ST_BYTES;
+    static constexpr size_t BAR_BYTES = BULK ? (size_t)WARPS * 8 : 0;
+    static constexpr size_t EPI_OFF = BAR_OFF + BAR_BYTES;
     static constexpr size_t BYTES = EPI_OFF + 512;
 };
+
+// Epilogues whose emit(v) touches only row v's outputs (plus block-local
+// partials and atomics) declare `static constexpr bool kRowsIndependent =
+// true`: the fixup then emits the empty rows while the main kernel still
+// runs.
+template <class E, class = void>
+struct rows_independent : std::false_type {};
+template <class E>
+struct rows_independent<E, std::enable_if_t<E::kRowsIndependent>> : std::true_type {};
 
 template <class E, bool = has_prepare<E>::value>
 struct prepared_type {
@@ -1181,32 +1201,110 @@ __device__ __forceinline__ void nnz_finish(const NnzArgs<SR>& a, const NnzReady<
     __syncwarp();
 }
 
+// Lane 0 of a warp: the bulk copies of one tile's col and, unless COL_ONLY,
+// val (1 KB each; the arrays are padded past the last tile) into the warp's
+// staging buffer.
+template <class SR, bool COL_ONLY>
+__device__ __forceinline__ void nnz_issue(const NnzArgs<SR>& a, uint32_t tile, unsigned char* st,
+                                          uint64_t* bar) {
+    constexpr uint32_t kBytes = kNnzTile * 4;
+    const size_t j0 = (size_t)tile * kNnzTile;
+    mbar_arrive_expect_tx(bar, (COL_ONLY ? 1 : 2) * kBytes);
+    bulk_g2s(st, a.col + j0, kBytes, bar);
+    if constexpr (!COL_ONLY) bulk_g2s(st + kBytes, a.val + j0, kBytes, bar);
+}
+
 // HINTS: col/val are streamed with an evict-first L2 policy, x gathers use
 // evict-last (x stays in L2 across the iteration).  PFL1: each warp
 // prefetches its next tile's col/val lines into L1.  PIPE: a three-tile
 // software pipeline per warp -- while tile A is folded, the x gathers of
-// tile B and the col/val loads of tile C are in flight.
+// tile B and the col/val loads of tile C are in flight.  BULK: each warp's
+// next tile of col (BULK 2) or col and val (BULK 1) is brought into its
+// shared-memory staging buffer by bulk copies (the TMA engine, no load
+// registers or LSU work) while the current tile is gathered and folded; with
+// BULK 2 val is loaded at the tile start, its latency overlapping the x
+// gathers.  The wait on the mbarrier is bounded and reports a timeout
+// through the device error word.
 template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false,
-          bool PFL1 = false>
+          bool PFL1 = false, int BULK = 0>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
 spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
     using X = typename SR::x_t;
     using W = typename SR::w_t;
-    using L = NnzLayout<SR, WARPS, HOT>;
+    using L = NnzLayout<SR, WARPS, HOT, BULK>;
     static_assert(sizeof(W) == 4, "16-byte val loads assume 4-byte edge values");
     extern __shared__ __align__(16) unsigned char dsm[];
+    // the fixup (launched with programmatic dependent launch) may start as
+    // soon as every block is past this point
+    grid_launch_dependents();
     const uint32_t w = threadIdx.x >> 5;
     X* xc = reinterpret_cast<X*>(dsm + L::XC_OFF);
     V* sy = reinterpret_cast<V*>(dsm + L::SY_OFF) + (size_t)w * kNnzTile;
     epi.begin();
     const uint32_t hot = HOT < a.plan.n_rows ? (uint32_t)HOT : a.plan.n_rows;
+    const uint32_t total_warps = gridDim.x * WARPS;
+    const uint32_t n_tiles = a.plan.n_tiles;
+    if constexpr (BULK) {
+        // the first tile's copies start before the x cache is filled
+        unsigned char* st = dsm + L::ST_OFF + (size_t)w * L::ST_WARP;
+        uint64_t* bar = reinterpret_cast<uint64_t*>(dsm + L::BAR_OFF) + w;
+        const uint32_t lane = lane_id();
+        uint32_t tile = blockIdx.x * WARPS + w;
+        if (lane == 0) {
+            mbar_init(bar, 1);
+            fence_mbar_init();
+            if (tile < n_tiles) nnz_issue<SR, BULK == 2>(a, tile, st, bar);
+        }
+        if constexpr (HOT > 0)
+            for (uint32_t i = threadIdx.x; i < hot; i += WARPS * 32) xc[i] = ldg_any(a.x + i);
+        __syncthreads();
+        const uint4* sc = reinterpret_cast<const uint4*>(st) + 2 * lane;
+        const uint4* sv = reinterpret_cast<const uint4*>(st + kNnzTile * 4) + 2 * lane;
+        uint32_t phase = 0;
+        for (; tile < n_tiles; tile += total_warps, phase ^= 1u) {
+            NnzIn in;
+            const uint32_t j0 = tile * kNnzTile;
+            in.sw = __ldg(a.plan.sbits + (j0 >> 5) + (lane >> 2));
+            in.endw = __ldg(a.plan.sbits + ((j0 + kNnzTile) >> 5));
+            in.seg0 = __ldg(a.plan.tile_seg + tile);
+            if constexpr (BULK == 2) {
+                in.v0 = __ldg(reinterpret_cast<const uint4*>(a.val + j0) + 2 * lane);
+                in.v1 = __ldg(reinterpret_cast<const uint4*>(a.val + j0) + 2 * lane + 1);
+            }
+            const bool arrived = mbar_wait_bounded(bar, phase);
+            if (!__all_sync(0xffffffffu, arrived)) {
+                // give the copy in flight one more bounded chance to land
+                // before the warp leaves its shared memory
+                if (lane == 0) {
+                    set_error(a.err, kDevTimeout);
+                    mbar_wait_bounded(bar, phase, 1u << 20);
+                }
+                __syncwarp();
+                break;
+            }
+            in.c0 = sc[0];
+            in.c1 = sc[1];
+            if constexpr (BULK == 1) {
+                in.v0 = sv[0];
+                in.v1 = sv[1];
+            }
+            __syncwarp();  // the staging buffer is free: the next tile's copy may land
+            const uint32_t nt = tile + total_warps;
+            if (lane == 0 && nt < n_tiles) {
+                fence_proxy_async_smem();
+                nnz_issue<SR, BULK == 2>(a, nt, st, bar);
+            }
+            const NnzReady<SR, Epi> r = nnz_gather<SR, Epi, HOT, false>(a, in, xc, hot, 0, epi);
+            nnz_finish<SR, Epi>(a, r, tile, sy, epi);
+        }
+        epi.template block_end<WARPS * 32>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
+        return;
+    }
     if constexpr (HOT > 0) {
         for (uint32_t i = threadIdx.x; i < hot; i += WARPS * 32) xc[i] = ldg_any(a.x + i);
         __syncthreads();
     }
-    const uint32_t total_warps = gridDim.x * WARPS;
-    const uint32_t n_tiles = a.plan.n_tiles;
     uint64_t pol_stream = 0, pol_keep = 0;
     if constexpr (HINTS) {
         pol_stream = l2_policy_evict_first();
@@ -1257,58 +1355,88 @@ __device__ __forceinline__ bool nnz_start_bit(const uint32_t* sbits, uint32_t k)
     return (__ldg(sbits + (k >> 5)) >> (k & 31)) & 1u;
 }
 
-// Rows that cross nnz tiles, one thread per tile in which such a row ends
-// (the plan lists them): a deterministic fold of the tiles' partials in
-// tile order, like spmv_fixup_kernel; and the empty rows (identity), one
-// per thread.
+// Rows that cross nnz tiles, one per tile in which such a row ends (the
+// plan lists them with the row and its first tile): a deterministic fold of
+// the tiles' partials in tile order, like spmv_fixup_kernel; and the empty
+// rows (identity).  Grid-stride over both.  The empty rows do not depend on
+// the main kernel: with an epilogue whose rows are independent they are
+// emitted before grid_dependency_wait(), overlapping the main kernel's tail
+// when the two are launched with programmatic dependent launch.
 template <class SR, class Epi, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 spmv_nnz_fixup_kernel(NnzArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
+    constexpr bool kEarly = rows_independent<Epi>::value;
     __shared__ alignas(16) char epi_smem[64 * 8];
-    const uint32_t i = blockIdx.x * BLOCK + threadIdx.x;
+    const uint32_t i0 = blockIdx.x * BLOCK + threadIdx.x;
+    const uint32_t stride = gridDim.x * BLOCK;
     const uint32_t lane = lane_id();
     const NnzPlanView& p = a.plan;
+    if constexpr (!kEarly) grid_dependency_wait();
     epi.begin();
-    bool longc = false;
-    uint32_t row = 0, first = 0, t = 0;
-    V acc = SR::identity();
-    if (i < p.n_fix) {
-        t = __ldg(p.fix_tiles + i);  // >= 1
-        row = __ldg(p.nz_rows + __ldg(p.tile_seg + t));
-        acc = SR::reduce(a.carry[t - 1], a.tail[t]);
-        // the tile holding the row's first nonzero
-        first = __ldg(p.row_ptr + row) / kNnzTile;
-        if (first + 1 < t)
-            longc = true;  // the row also covers tile t-2 or earlier
-        else
-            epi.emit(row, acc);
-    }
-    unsigned pending = __ballot_sync(0xffffffffu, longc);
-    while (pending) {
-        const int src = __ffs(pending) - 1;
-        pending &= pending - 1;
-        const uint32_t f0 = __shfl_sync(0xffffffffu, first, src);
-        const uint32_t tt = __shfl_sync(0xffffffffu, t, src);
-        // carries of the tiles [f0, tt-1) (tile tt-1's is already in acc);
-        // four independent partial folds keep four loads in flight per lane
-        V part = SR::identity(), p1 = SR::identity(), p2 = SR::identity(), p3 = SR::identity();
-        uint32_t k = f0 + lane;
-        for (; k + 96 + 1 < tt; k += 128) {
-            part = SR::reduce(part, a.carry[k]);
-            p1 = SR::reduce(p1, a.carry[k + 32]);
-            p2 = SR::reduce(p2, a.carry[k + 64]);
-            p3 = SR::reduce(p3, a.carry[k + 96]);
-        }
-        for (; k + 1 < tt; k += 32) part = SR::reduce(part, a.carry[k]);
-        part = SR::reduce(SR::reduce(part, p1), SR::reduce(p2, p3));
+    // empty rows four at a time: their row ids and epilogue loads are all in
+    // flight before the first store
+    uint32_t e = i0;
+    for (; e + 3 * stride < p.n_empty; e += 4 * stride) {
+        uint32_t v[4];
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1)
-            part = SR::reduce(part, shfl_down_any(0xffffffffu, part, off));
-        part = shfl_any(0xffffffffu, part, 0);
-        if ((int)lane == src) epi.emit(row, SR::reduce(part, acc));
+        for (int q = 0; q < 4; ++q) v[q] = __ldg(p.empty_rows + e + q * stride);
+        if constexpr (has_prepare<Epi>::value) {
+            typename prepared_type<Epi>::type pre[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) pre[q] = epi.prepare(v[q]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) epi.emit_prepared(v[q], SR::identity(), pre[q]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) epi.emit(v[q], SR::identity());
+        }
     }
-    for (uint32_t e = i; e < p.n_empty; e += gridDim.x * BLOCK) epi.emit(__ldg(p.empty_rows + e), SR::identity());
+    for (; e < p.n_empty; e += stride) epi.emit(__ldg(p.empty_rows + e), SR::identity());
+    if constexpr (kEarly) grid_dependency_wait();
+    grid_launch_dependents();
+    // warp-uniform trip count: the ballot below needs all 32 lanes
+    for (uint32_t wb = i0 - lane; wb < p.n_fix; wb += stride) {
+        const uint32_t i = wb + lane;
+        bool longc = false;
+        uint32_t row = 0, first = 0, t = 0;
+        V acc = SR::identity();
+        if (i < p.n_fix) {
+            const uint4 f = __ldg(p.fix_info + i);
+            t = f.x;  // >= 1
+            row = f.y;
+            first = f.z;  // the tile holding the row's first nonzero
+            acc = SR::reduce(a.carry[t - 1], a.tail[t]);
+            if (first + 1 < t)
+                longc = true;  // the row also covers tile t-2 or earlier
+            else
+                epi.emit(row, acc);
+        }
+        unsigned pending = __ballot_sync(0xffffffffu, longc);
+        while (pending) {
+            const int src = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const uint32_t f0 = __shfl_sync(0xffffffffu, first, src);
+            const uint32_t tt = __shfl_sync(0xffffffffu, t, src);
+            // carries of the tiles [f0, tt-1) (tile tt-1's is already in acc);
+            // four independent partial folds keep four loads in flight per lane
+            V part = SR::identity(), p1 = SR::identity(), p2 = SR::identity(), p3 = SR::identity();
+            uint32_t k = f0 + lane;
+            for (; k + 96 + 1 < tt; k += 128) {
+                part = SR::reduce(part, a.carry[k]);
+                p1 = SR::reduce(p1, a.carry[k + 32]);
+                p2 = SR::reduce(p2, a.carry[k + 64]);
+                p3 = SR::reduce(p3, a.carry[k + 96]);
+            }
+            for (; k + 1 < tt; k += 32) part = SR::reduce(part, a.carry[k]);
+            part = SR::reduce(SR::reduce(part, p1), SR::reduce(p2, p3));
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1)
+                part = SR::reduce(part, shfl_down_any(0xffffffffu, part, off));
+            part = shfl_any(0xffffffffu, part, 0);
+            if ((int)lane == src) epi.emit(row, SR::reduce(part, acc));
+        }
+    }
     epi.template block_end<BLOCK>(epi_smem);
 }
 
@@ -1356,6 +1484,7 @@ spmv_vector_kernel(uint32_t n_rows, const uint32_t* row_ptr, const uint32_t* col
 // Plain SpMV: y[row] = value.
 template <class V>
 struct StoreEpilogue {
+    static constexpr bool kRowsIndependent = true;
     V* y;
     __device__ __forceinline__ void begin() {}
     __device__ __forceinline__ void emit(uint32_t row, const V& v) { y[row] = v; }
