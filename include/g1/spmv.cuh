@@ -494,7 +494,7 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
     // x[0, HOT) is read once per CTA and served from shared memory.
     const uint32_t hot = HOT < a.plan.n_rows ? (uint32_t)HOT : a.plan.n_rows;
     if constexpr (HOT > 0) {
-        for (uint32_t i = threadIdx.x; i < hot; i += WARPS * 32) xc[i] = ldg_any(a.x + i);
+        fill_x_cache<WARPS * 32>(xc, a.x, hot);
         __syncthreads();
     }
     const uint32_t total_warps = gridDim.x * WARPS;
@@ -723,7 +723,7 @@ spmv_wtma_kernel(MergeArgs<SR> a, Epi epi) {
     }
     const uint32_t hot = HOT < a.plan.n_rows ? (uint32_t)HOT : a.plan.n_rows;
     if constexpr (HOT > 0)
-        for (uint32_t i = threadIdx.x; i < hot; i += WARPS * 32) xc[i] = ldg_any(a.x + i);
+        fill_x_cache<WARPS * 32>(xc, a.x, hot);
     __syncthreads();
 
     const uint32_t total_warps = gridDim.x * WARPS;
@@ -1257,7 +1257,7 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
             if (tile < n_tiles) nnz_issue<SR, BULK == 2>(a, tile, st, bar);
         }
         if constexpr (HOT > 0)
-            for (uint32_t i = threadIdx.x; i < hot; i += WARPS * 32) xc[i] = ldg_any(a.x + i);
+            fill_x_cache<WARPS * 32>(xc, a.x, hot);
         __syncthreads();
         const uint4* sc = reinterpret_cast<const uint4*>(st) + 2 * lane;
         const uint4* sv = reinterpret_cast<const uint4*>(st + kNnzTile * 4) + 2 * lane;
@@ -1302,7 +1302,7 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
         return;
     }
     if constexpr (HOT > 0) {
-        for (uint32_t i = threadIdx.x; i < hot; i += WARPS * 32) xc[i] = ldg_any(a.x + i);
+        fill_x_cache<WARPS * 32>(xc, a.x, hot);
         __syncthreads();
     }
     uint64_t pol_stream = 0, pol_keep = 0;
