@@ -490,15 +490,30 @@ __global__ void nnz_fix_place_kernel(const uint32_t* flag, const uint32_t* pos, 
 }
 
 // The fixup's per-entry facts, resolved once per graph instead of through
-// tile_seg -> rows -> row_ptr on every launch.
+// tile_seg -> rows -> row_ptr on every launch; is_long[i]: the row spans
+// more than one tile boundary.
 __global__ void nnz_fix_info_kernel(const uint32_t* fix_tiles, uint32_t n_fix, const uint32_t* tile_seg,
                                     const uint32_t* nz_rows, const uint32_t* rp, uint32_t tile,
-                                    uint4* info) {
+                                    uint4* info, uint32_t* is_long) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_fix) return;
+    if (i > n_fix) return;
+    if (i == n_fix) {
+        is_long[i] = 0;
+        return;
+    }
     const uint32_t t = fix_tiles[i];
     const uint32_t row = nz_rows[tile_seg[t]];
-    info[i] = make_uint4(t, row, rp[row] / tile, 0u);
+    const uint32_t first = rp[row] / tile;
+    info[i] = make_uint4(t, row, first, 0u);
+    is_long[i] = first + 1 < t ? 1u : 0u;
+}
+
+// Stable partition of the fix entries: short ones first, then long ones.
+__global__ void nnz_fix_split_kernel(const uint4* info, const uint32_t* is_long, const uint32_t* lpos,
+                                     uint32_t n_fix, uint32_t n_short, uint4* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_fix) return;
+    out[is_long[i] ? n_short + lpos[i] : i - lpos[i]] = info[i];
 }
 
 g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
@@ -558,14 +573,34 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
         nnz_fix_place_kernel<<<tb, 256>>>(fflag.as<uint32_t>(), fpos.as<uint32_t>(), p->n_tiles,
                                           p->fix_tiles.as<uint32_t>());
         G1_TRY(p->fix_info.ensure(((size_t)nfix + 1) * 16));
-        if (nfix > 0)
-            nnz_fix_info_kernel<<<(uint32_t)ceil_div(nfix, 256), 256>>>(
-                p->fix_tiles.as<uint32_t>(), nfix, p->tile_seg.as<uint32_t>(), p->rows.as<uint32_t>(),
-                o.rp, kNnzTile, p->fix_info.as<uint4>());
+        p->n_fix_short = 0;
+        if (nfix > 0) {
+            DevBuf raw, lflag, lpos, ltemp;
+            G1_TRY(raw.ensure(((size_t)nfix + 1) * 16));
+            G1_TRY(lflag.ensure(((size_t)nfix + 1) * 4));
+            G1_TRY(lpos.ensure(((size_t)nfix + 1) * 4));
+            const uint32_t fb = (uint32_t)ceil_div((uint64_t)nfix + 1, 256);
+            nnz_fix_info_kernel<<<fb, 256>>>(p->fix_tiles.as<uint32_t>(), nfix, p->tile_seg.as<uint32_t>(),
+                                             p->rows.as<uint32_t>(), o.rp, kNnzTile, raw.as<uint4>(),
+                                             lflag.as<uint32_t>());
+            size_t lb = 0;
+            G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, lb, lflag.as<uint32_t>(), lpos.as<uint32_t>(),
+                                                  (int)nfix + 1));
+            G1_TRY(ltemp.ensure(lb + 16));
+            G1_CUDA(cub::DeviceScan::ExclusiveSum(ltemp.p, lb, lflag.as<uint32_t>(), lpos.as<uint32_t>(),
+                                                  (int)nfix + 1));
+            uint32_t nlong = 0;
+            G1_CUDA(cudaMemcpy(&nlong, lpos.as<uint32_t>() + nfix, 4, cudaMemcpyDeviceToHost));
+            p->n_fix_short = nfix - nlong;
+            nnz_fix_split_kernel<<<fb, 256>>>(raw.as<uint4>(), lflag.as<uint32_t>(), lpos.as<uint32_t>(), nfix,
+                                              p->n_fix_short, p->fix_info.as<uint4>());
+            G1_CUDA(cudaGetLastError());
+            G1_CUDA(cudaDeviceSynchronize());
+        }
         G1_CUDA(cudaGetLastError());
         G1_CUDA(cudaDeviceSynchronize());
     }
-    count_launches(p->n_fix > 0 ? 6 : 5);
+    count_launches(p->n_fix > 0 ? 7 : 5);
     G1_CUDA(cudaGetLastError());
     G1_CUDA(cudaDeviceSynchronize());
     *out = p.get();

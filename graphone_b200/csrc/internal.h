@@ -73,9 +73,11 @@ struct MergePlan {
 // nonzeros, the non-empty rows in order followed by the empty rows.
 struct NnzPlan {
     uint32_t n_tiles = 0, n_nonempty = 0, n_empty = 0, n_fix = 0;
+    uint32_t n_fix_short = 0;  // fix entries [0, n_fix_short) end in the tile after their first
     DevBuf tile_seg, sbits, rows, carry, tail;
     DevBuf fix_tiles;  // tiles in which a row begun in an earlier tile ends
-    DevBuf fix_info;   // per such tile: {tile, row, first tile of the row, 0}
+    DevBuf fix_info;   // per such tile: {tile, row, first tile of the row, 0}; rows that
+                       // span one boundary first, then longer chains, each in tile order
 };
 
 struct Orientation {

@@ -10,8 +10,10 @@
 // second pass.  x and rank are double-buffered across iterations.
 //
 // G1_PR_DANGLING adds a*sum(rank[dangling])/N; that sum is reduced on the
-// device by the epilogues themselves (per-block partials, folded in a fixed
-// order by the last block of the fixup kernel), so no host round trip.
+// device by the epilogues themselves, so no host round trip.  It is an exact
+// integer sum of the ranks in 2^-56 fixed point (one 64-bit atomic per
+// block): the result does not depend on which block emits which row, nor on
+// the order of the atomics, so every schedule gives the same bits.
 #include <algorithm>
 
 #include "g1/semiring.cuh"
@@ -21,31 +23,26 @@
 
 namespace g1 {
 
-// Per-block partial sums folded by the last block to finish (ticket counter,
-// no waiting).  Deterministic: the slots are summed in a fixed order.
+// Dangling sums in fixed point: rank r >= 0 (the ranks sum to at most 1)
+// as floor(r * 2^56), from the float's bits with integer shifts only; 64-bit
+// integer sums are exact and order-free.
+constexpr double kDangScale = 72057594037927936.0;  // 2^56
+__device__ __forceinline__ unsigned long long dang_fixed(float r) {
+    const uint32_t b = __float_as_uint(r);
+    const int e = (int)((b >> 23) & 0xFFu);
+    if (e == 0) return 0ull;  // zero or subnormal: below the 2^-56 resolution
+    const unsigned long long m = (unsigned long long)((b & 0x7FFFFFu) | 0x800000u);
+    const int sh = e - 94;  // r * 2^56 = m * 2^(e - 150 + 56); sh <= 33 for r <= 1
+    return sh >= 0 ? (m << min(sh, 39)) : (sh > -24 ? (m >> -sh) : 0ull);
+}
+
+// Adds the block's fixed-point dangling sum to *out.
 template <int BLOCK>
-__device__ void fold_partials_last_block(double v, double* partials, uint32_t slot,
-                                         uint32_t n_slots, unsigned* ticket, double* out,
-                                         char* smem) {
-    double* red = reinterpret_cast<double*>(smem);
-    double s = block_sum<double, BLOCK>(v, red);
-    __shared__ int is_last;
-    if (threadIdx.x == 0) {
-        partials[slot] = s;
-        __threadfence();
-        const unsigned t = atomicAdd(ticket, 1u);
-        is_last = (t == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!is_last) return;
-    __threadfence();
-    double acc = 0.0;
-    for (uint32_t i = threadIdx.x; i < n_slots; i += BLOCK) acc += ((volatile double*)partials)[i];
-    acc = block_sum<double, BLOCK>(acc, red);
-    if (threadIdx.x == 0) {
-        *out = acc;
-        *ticket = 0u;  // ready for the next launch
-    }
+__device__ __forceinline__ void dang_block_add(unsigned long long v, unsigned long long* out,
+                                               char* smem) {
+    const unsigned long long sum =
+        block_sum<unsigned long long, BLOCK>(v, reinterpret_cast<unsigned long long*>(smem));
+    if (threadIdx.x == 0 && sum) atomicAdd(out, sum);
 }
 
 struct PrEpilogue {
@@ -53,26 +50,27 @@ struct PrEpilogue {
     float* rank_next;
     float* x_next;
     const float* iw;
-    const double* dang_in;  // sum of the current ranks over dangling vertices
+    // dangling sums (fixed point) rotate through three words: this
+    // iteration reads dang_in, adds into dang_out (zero on entry) and the
+    // main kernel's first thread zeroes dang_clear (read one iteration ago)
+    const unsigned long long* dang_in;
+    unsigned long long* dang_out;
+    unsigned long long* dang_clear;  // null in the fixup
     double alpha_over_n;
     float base0;           // (float)((1 - alpha) / N), the reference's alpha_div_v
     int dangling;          // G1_PR_DANGLING
-    double* partials;
-    uint32_t slot_base;
-    uint32_t n_slots;
-    int last_reduce;       // this launch folds all partials into dang_out
-    unsigned* ticket;
-    double* dang_out;
 
     float base;
-    double dang_local;
+    unsigned long long dang_local;
 
     __device__ __forceinline__ void begin() {
-        dang_local = 0.0;
+        dang_local = 0ull;
+        if (dang_clear && blockIdx.x == 0 && threadIdx.x == 0) *dang_clear = 0ull;
         // under programmatic dependent launch the fixup runs this before its
         // dependency wait: dang_in was written by a grid that completed
         // before this one launched (the previous fixup)
-        base = dangling ? (float)((double)base0 + alpha_over_n * (*dang_in)) : base0;
+        base = dangling ? (float)((double)base0 + alpha_over_n * ((double)(*dang_in) / kDangScale))
+                        : base0;
     }
     __device__ __forceinline__ void emit(uint32_t v, const float& y) {
         emit_prepared(v, y, prepare(v));
@@ -83,18 +81,11 @@ struct PrEpilogue {
         const float r = base + y;
         rank_next[v] = r;
         x_next[v] = r * w;
-        if (dangling && w == 0.0f) dang_local += (double)r;
+        if (dangling && w == 0.0f) dang_local += dang_fixed(r);
     }
     template <int BLOCK>
     __device__ __forceinline__ void block_end(char* smem) {
-        if (!dangling) return;
-        if (last_reduce) {
-            fold_partials_last_block<BLOCK>(dang_local, partials, slot_base + blockIdx.x, n_slots,
-                                            ticket, dang_out, smem);
-        } else {
-            double s = block_sum<double, BLOCK>(dang_local, reinterpret_cast<double*>(smem));
-            if (threadIdx.x == 0) partials[slot_base + blockIdx.x] = s;
-        }
+        if (dangling) dang_block_add<BLOCK>(dang_local, dang_out, smem);
     }
 };
 
@@ -125,11 +116,10 @@ pr_outw_from_transpose_kernel(const uint32_t* tcol, const float* tval, uint32_t 
 // apps/pagerank_blas.cu:41-53), the initial ranks 1/N, x0 = rank0 * iw and
 // the dangling sum of rank0.
 __global__ void pr_init_from_outw_kernel(const float* outw, uint32_t n, float alpha, float* iw,
-                                         float* rank0, float* x0, double* partials,
-                                         unsigned* ticket, double* dang_out) {
+                                         float* rank0, float* x0, unsigned long long* dang_out) {
     __shared__ alignas(16) char smem[64 * 8];
     const float r0 = (float)(1.0 / (double)n);
-    double dl = 0.0;
+    unsigned long long dl = 0ull;
     const uint64_t stride = (uint64_t)gridDim.x * 256;
     for (uint64_t v = (uint64_t)blockIdx.x * 256 + threadIdx.x; v < n; v += stride) {
         const float s = outw[v];
@@ -137,19 +127,16 @@ __global__ void pr_init_from_outw_kernel(const float* outw, uint32_t n, float al
         iw[v] = w;
         rank0[v] = r0;
         x0[v] = r0 * w;
-        if (w == 0.0f) dl += (double)r0;
+        if (w == 0.0f) dl += dang_fixed(r0);
     }
-    fold_partials_last_block<256>(dl, partials, blockIdx.x, gridDim.x, ticket, dang_out, smem);
+    dang_block_add<256>(dl, dang_out, smem);
 }
 
 struct PrBuffers {
     float* iw;
     float* rank[2];
     float* x[2];
-    double* dang;  // [2]
-    double* partials;
-    unsigned* ticket;
-    uint32_t n_slots;
+    unsigned long long* dang;  // [3], fixed point
 };
 
 static g1_status pr_setup(g1_graph* g, float alpha, PrBuffers& b, uint32_t* grids,
@@ -162,16 +149,13 @@ static g1_status pr_setup(g1_graph* g, float alpha, PrBuffers& b, uint32_t* grid
     G1_TRY(ws.get("pr_rank1", n, &b.rank[1]));
     G1_TRY(ws.get("pr_x0", n, &b.x[0]));
     G1_TRY(ws.get("pr_x1", n, &b.x[1]));
-    G1_TRY(ws.get("pr_dang", 2, &b.dang));
-    G1_TRY(ws.get("pr_ticket", 4, &b.ticket));
+    G1_TRY(ws.get("pr_dang", 4, &b.dang));
     // grids[0] main merge, grids[1] fixup, grids[2] vector, grids[3] init
     G1_TRY((merge_grids<PlusTimesF32, PrEpilogue>(g, t, &grids[0], &grids[1])));
     grids[2] = vector_grid<PlusTimesF32, PrEpilogue>(g);
     grids[3] = (uint32_t)std::max<uint64_t>(
         1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
-    b.n_slots = std::max(grids[0] + grids[1], std::max(grids[2], grids[3]));
-    G1_TRY(ws.get("pr_partials", b.n_slots, &b.partials));
-    G1_CUDA(cudaMemsetAsync(b.ticket, 0, 16, s));
+    G1_CUDA(cudaMemsetAsync(b.dang, 0, 4 * sizeof(unsigned long long), s));
     float* outw = nullptr;
     G1_TRY(ws.get("pr_outw", n, &outw));
     if (!g->outw_ready) {
@@ -191,41 +175,33 @@ static g1_status pr_setup(g1_graph* g, float alpha, PrBuffers& b, uint32_t* grid
         g->outw_ready = true;
     }
     pr_init_from_outw_kernel<<<grids[3], 256, 0, s>>>(outw, n, alpha, b.iw, b.rank[0], b.x[0],
-                                                      b.partials, b.ticket, &b.dang[0]);
+                                                      &b.dang[0]);
     count_launches(1);
     G1_CUDA(cudaGetLastError());
     return G1_OK;
 }
 
-// One PageRank iteration: reads x[cur], writes rank[nxt], x[nxt], dang[nxt].
+// PageRank iteration `it`: reads x[cur], writes rank[nxt], x[nxt] (cur =
+// it & 1); reads dang[it % 3], adds into dang[(it + 1) % 3], zeroes
+// dang[(it + 2) % 3].
 static g1_status pr_iterate(g1_graph* g, const PrBuffers& b, const uint32_t* grids, float alpha,
-                            g1_pr_mode mode, int cur, g1_schedule sched, cudaStream_t s) {
-    const int nxt = cur ^ 1;
+                            g1_pr_mode mode, int it, g1_schedule sched, cudaStream_t s) {
+    const int cur = it & 1, nxt = cur ^ 1;
     PrEpilogue e;
     e.rank_next = b.rank[nxt];
     e.x_next = b.x[nxt];
     e.iw = b.iw;
-    e.dang_in = &b.dang[cur];
+    e.dang_in = &b.dang[it % 3];
+    e.dang_out = &b.dang[(it + 1) % 3];
+    e.dang_clear = &b.dang[(it + 2) % 3];
     e.alpha_over_n = (double)alpha / (double)g->n;
     e.base0 = (float)((1.0 - (double)alpha) / (double)g->n);
     e.dangling = mode == G1_PR_DANGLING;
-    e.partials = b.partials;
-    e.ticket = b.ticket;
-    e.dang_out = &b.dang[nxt];
     const int t = 1;
-    if (resolve_schedule(g, t, sched) == G1_SCHED_VECTOR) {
-        e.slot_base = 0;
-        e.n_slots = grids[2];
-        e.last_reduce = 1;
+    if (resolve_schedule(g, t, sched) == G1_SCHED_VECTOR)
         return launch_vector<PlusTimesF32>(g, t, b.x[cur], e, s);
-    }
     PrEpilogue f = e;
-    e.slot_base = 0;
-    e.n_slots = grids[0] + grids[1];
-    e.last_reduce = 0;
-    f.slot_base = grids[0];
-    f.n_slots = grids[0] + grids[1];
-    f.last_reduce = 1;
+    f.dang_clear = nullptr;
     return launch_merge<PlusTimesF32>(g, t, b.x[cur], e, f, s);
 }
 
@@ -249,7 +225,7 @@ extern "C" g1_status g1_pagerank(g1_graph* g, float alpha, int iters, g1_pr_mode
     uint32_t grids[4];
     G1_TRY(pr_setup(g, alpha, b, grids, s));
     for (int it = 0; it < iters; ++it)
-        G1_TRY(pr_iterate(g, b, grids, alpha, mode, it & 1, G1_SCHED_AUTO, s));
+        G1_TRY(pr_iterate(g, b, grids, alpha, mode, it, G1_SCHED_AUTO, s));
     G1_TRY(copy_out_vertices(g, rank_out, b.rank[iters & 1], s));
     return check_device_error(g, s);
 }

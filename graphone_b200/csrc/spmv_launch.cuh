@@ -140,10 +140,14 @@ struct NnzKernel {
     }
 };
 
-// The nnz fixup runs grid-stride: at most 8 blocks of 256 threads per SM.
-inline uint32_t nnz_fix_grid(const g1_graph* g, const NnzPlan& p) {
+// The nnz fixup runs grid-stride in one wave of resident blocks (blocks of
+// a second wave would start their empty rows only after the main kernel).
+template <class SR, class Epi>
+uint32_t nnz_fix_grid(const g1_graph* g, const NnzPlan& p) {
+    static const int occ =
+        blocks_per_sm(spmv_nnz_fixup_kernel<SR, Epi, kMergeBlock>, kMergeBlock, 0);
     const uint64_t want = ceil_div(std::max(p.n_fix, p.n_empty), kMergeBlock);
-    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)g->sm_count * 8));
+    return (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)g->sm_count * occ));
 }
 
 // Launch with programmatic stream serialization: the kernel may start while
@@ -227,6 +231,7 @@ NnzArgs<SR> nnz_args(const g1_graph* g, int t, const NnzPlan& p, const typename 
     a.plan.n_fix = p.n_fix;
     a.plan.fix_tiles = p.fix_tiles.as<uint32_t>();
     a.plan.fix_info = p.fix_info.as<uint4>();
+    a.plan.n_fix_short = p.n_fix_short;
     a.col = o.col;
     a.val = static_cast<const typename SR::w_t*>(o.val);
     a.x = x;
@@ -253,10 +258,10 @@ g1_status launch_nnz(g1_graph* g, int t, const NnzPlan& p, const typename SR::x_
         prof_mark(s, true);
         mk<<<K::grid(g, p.n_tiles), WARPS * 32, K::L::BYTES, s>>>(a, main_epi);
         prof_mark(s, false);
-        fk<<<nnz_fix_grid(g, p), kMergeBlock, 0, s>>>(a, fix_epi);
+        fk<<<nnz_fix_grid<SR, Epi>(g, p), kMergeBlock, 0, s>>>(a, fix_epi);
     } else {
         mk<<<K::grid(g, p.n_tiles), WARPS * 32, K::L::BYTES, s>>>(a, main_epi);
-        G1_CUDA(launch_pdl(fk, nnz_fix_grid(g, p), kMergeBlock, 0, s, a, fix_epi));
+        G1_CUDA(launch_pdl(fk, nnz_fix_grid<SR, Epi>(g, p), kMergeBlock, 0, s, a, fix_epi));
     }
     count_launches(2);
     G1_CUDA(cudaGetLastError());
@@ -291,7 +296,7 @@ g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_gri
             case 27: *main_grid = NnzKernel<SR, Epi, 32, 1, 24576, false, false, false, 2>::grid(g, q->n_tiles); break;
             default: *main_grid = NnzKernel<SR, Epi, 32, 1, 16384>::grid(g, q->n_tiles); break;
         }
-        *fix_grid = nnz_fix_grid(g, *q);
+        *fix_grid = nnz_fix_grid<SR, Epi>(g, *q);
         return G1_OK;
     }
     MergePlan* p = nullptr;

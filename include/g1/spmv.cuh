@@ -976,6 +976,8 @@ struct NnzPlanView {
     uint32_t n_fix;
     const uint32_t* fix_tiles;   // tiles in which a row begun in an earlier tile ends
     const uint4* fix_info;       // per such tile: {tile, row, tile of the row's first nonzero, 0}
+    uint32_t n_fix_short;        // fix_info[0, n_fix_short): rows begun in the previous tile;
+                                 // the rest: rows that span more tiles
 };
 
 template <class SR>
@@ -1356,12 +1358,17 @@ __device__ __forceinline__ bool nnz_start_bit(const uint32_t* sbits, uint32_t k)
 }
 
 // Rows that cross nnz tiles, one per tile in which such a row ends (the
-// plan lists them with the row and its first tile): a deterministic fold of
-// the tiles' partials in tile order, like spmv_fixup_kernel; and the empty
-// rows (identity).  Grid-stride over both.  The empty rows do not depend on
-// the main kernel: with an epilogue whose rows are independent they are
-// emitted before grid_dependency_wait(), overlapping the main kernel's tail
-// when the two are launched with programmatic dependent launch.
+// plan lists them with the row and its first tile), and the empty rows
+// (identity); grid-stride over all three kinds of work:
+//   - empty rows: independent of the main kernel; with an epilogue whose
+//     rows are independent they are emitted before grid_dependency_wait(),
+//     overlapping the main kernel's tail under programmatic dependent launch;
+//   - rows begun in the previous tile (the plan lists them first): one
+//     thread each, carry[t-1] + tail[t];
+//   - rows that span more tiles (hubs): one warp each, folding the carries
+//     of the tiles they cover in tile order (lanes strided, four partials per
+//     lane, shuffle tree), then + tail[t].  Per row the fold order is fixed,
+//     so results do not depend on the grid.
 template <class SR, class Epi, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 spmv_nnz_fixup_kernel(NnzArgs<SR> a, Epi epi) {
@@ -1395,47 +1402,31 @@ spmv_nnz_fixup_kernel(NnzArgs<SR> a, Epi epi) {
     for (; e < p.n_empty; e += stride) epi.emit(__ldg(p.empty_rows + e), SR::identity());
     if constexpr (kEarly) grid_dependency_wait();
     grid_launch_dependents();
-    // warp-uniform trip count: the ballot below needs all 32 lanes
-    for (uint32_t wb = i0 - lane; wb < p.n_fix; wb += stride) {
-        const uint32_t i = wb + lane;
-        bool longc = false;
-        uint32_t row = 0, first = 0, t = 0;
-        V acc = SR::identity();
-        if (i < p.n_fix) {
-            const uint4 f = __ldg(p.fix_info + i);
-            t = f.x;  // >= 1
-            row = f.y;
-            first = f.z;  // the tile holding the row's first nonzero
-            acc = SR::reduce(a.carry[t - 1], a.tail[t]);
-            if (first + 1 < t)
-                longc = true;  // the row also covers tile t-2 or earlier
-            else
-                epi.emit(row, acc);
+    // rows begun in the previous tile
+    for (uint32_t i = i0; i < p.n_fix_short; i += stride) {
+        const uint4 f = __ldg(p.fix_info + i);
+        epi.emit(f.y, SR::reduce(a.carry[f.x - 1], a.tail[f.x]));
+    }
+    // longer chains, one warp each
+    const uint32_t n_warps = stride >> 5;
+    for (uint32_t j = p.n_fix_short + (i0 >> 5); j < p.n_fix; j += n_warps) {
+        const uint4 f = __ldg(p.fix_info + j);
+        const uint32_t tt = f.x, f0 = f.z;
+        // carries of the tiles [f0, tt-1); tile tt-1's joins tail[tt] below
+        V part = SR::identity(), p1 = SR::identity(), p2 = SR::identity(), p3 = SR::identity();
+        uint32_t k = f0 + lane;
+        for (; k + 96 + 1 < tt; k += 128) {
+            part = SR::reduce(part, a.carry[k]);
+            p1 = SR::reduce(p1, a.carry[k + 32]);
+            p2 = SR::reduce(p2, a.carry[k + 64]);
+            p3 = SR::reduce(p3, a.carry[k + 96]);
         }
-        unsigned pending = __ballot_sync(0xffffffffu, longc);
-        while (pending) {
-            const int src = __ffs(pending) - 1;
-            pending &= pending - 1;
-            const uint32_t f0 = __shfl_sync(0xffffffffu, first, src);
-            const uint32_t tt = __shfl_sync(0xffffffffu, t, src);
-            // carries of the tiles [f0, tt-1) (tile tt-1's is already in acc);
-            // four independent partial folds keep four loads in flight per lane
-            V part = SR::identity(), p1 = SR::identity(), p2 = SR::identity(), p3 = SR::identity();
-            uint32_t k = f0 + lane;
-            for (; k + 96 + 1 < tt; k += 128) {
-                part = SR::reduce(part, a.carry[k]);
-                p1 = SR::reduce(p1, a.carry[k + 32]);
-                p2 = SR::reduce(p2, a.carry[k + 64]);
-                p3 = SR::reduce(p3, a.carry[k + 96]);
-            }
-            for (; k + 1 < tt; k += 32) part = SR::reduce(part, a.carry[k]);
-            part = SR::reduce(SR::reduce(part, p1), SR::reduce(p2, p3));
+        for (; k + 1 < tt; k += 32) part = SR::reduce(part, a.carry[k]);
+        part = SR::reduce(SR::reduce(part, p1), SR::reduce(p2, p3));
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1)
-                part = SR::reduce(part, shfl_down_any(0xffffffffu, part, off));
-            part = shfl_any(0xffffffffu, part, 0);
-            if ((int)lane == src) epi.emit(row, SR::reduce(part, acc));
-        }
+        for (int off = 16; off > 0; off >>= 1)
+            part = SR::reduce(part, shfl_down_any(0xffffffffu, part, off));
+        if (lane == 0) epi.emit(f.y, SR::reduce(part, SR::reduce(a.carry[tt - 1], a.tail[tt])));
     }
     epi.template block_end<BLOCK>(epi_smem);
 }
