@@ -127,6 +127,10 @@ struct g1_graph {
     // Per-vertex sum of out-edge weights (PageRank's iweights denominator),
     // derived once per graph like the merge-path plans.
     bool outw_ready = false;
+    // PageRank: empty in-edge rows with out-weight (workspace "pr_empty_active")
+    // and the count of isolated vertices, for the nnz schedule
+    bool pr_empty_ready = false;
+    uint32_t pr_active_empty = 0, pr_isolated = 0;
     // Row pieces of the in-edge CSR for the multi-source pull kernels, the
     // rows with more than one piece (hubs) and the out-degrees (PPR).
     bool pieces_ready = false;

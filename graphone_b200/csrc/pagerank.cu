@@ -9,12 +9,21 @@
 // constructs in registers, so y never reaches HBM and there is no N-sized
 // second pass.  x and rank are double-buffered across iterations.
 //
+// Writes an iteration does not need are left out: rank only in the last
+// iteration (earlier ones need only x'), x' never for a vertex without
+// out-weight (0 in both x buffers from the start), and under the nnz
+// schedule the fixup skips isolated vertices (no in- or out-edges) until
+// the last iteration, adding their dangling share as a count (exact in the
+// fixed-point sum below).  The final ranks are the same bits.
+//
 // G1_PR_DANGLING adds a*sum(rank[dangling])/N; that sum is reduced on the
 // device by the epilogues themselves, so no host round trip.  It is an exact
 // integer sum of the ranks in 2^-56 fixed point (one 64-bit atomic per
 // block): the result does not depend on which block emits which row, nor on
 // the order of the atomics, so every schedule gives the same bits.
 #include <algorithm>
+
+#include <cub/device/device_select.cuh>
 
 #include "g1/semiring.cuh"
 #include "g1/spmv.cuh"
@@ -59,6 +68,13 @@ struct PrEpilogue {
     double alpha_over_n;
     float base0;           // (float)((1 - alpha) / N), the reference's alpha_div_v
     int dangling;          // G1_PR_DANGLING
+    int write_rank;        // last iteration: rank_next is the result
+    // nnz fixup: the empty rows to emit when set (those with out-weight);
+    // the n_iso isolated vertices left out add n_iso * base to the
+    // dangling sum (block 0, thread 0)
+    const uint32_t* empty_list = nullptr;
+    uint32_t n_empty_list = 0;
+    uint32_t n_iso = 0;
 
     float base;
     unsigned long long dang_local;
@@ -71,6 +87,8 @@ struct PrEpilogue {
         // before this one launched (the previous fixup)
         base = dangling ? (float)((double)base0 + alpha_over_n * ((double)(*dang_in) / kDangScale))
                         : base0;
+        if (n_iso && dangling && blockIdx.x == 0 && threadIdx.x == 0)
+            dang_local = (unsigned long long)n_iso * dang_fixed(base);
     }
     __device__ __forceinline__ void emit(uint32_t v, const float& y) {
         emit_prepared(v, y, prepare(v));
@@ -79,9 +97,9 @@ struct PrEpilogue {
     __device__ __forceinline__ float prepare(uint32_t v) const { return __ldg(iw + v); }
     __device__ __forceinline__ void emit_prepared(uint32_t v, const float& y, float w) {
         const float r = base + y;
-        rank_next[v] = r;
-        x_next[v] = r * w;
-        if (dangling && w == 0.0f) dang_local += dang_fixed(r);
+        if (write_rank) rank_next[v] = r;
+        if (w != 0.0f) x_next[v] = r * w;
+        else if (dangling) dang_local += dang_fixed(r);
     }
     template <int BLOCK>
     __device__ __forceinline__ void block_end(char* smem) {
@@ -113,10 +131,12 @@ pr_outw_from_transpose_kernel(const uint32_t* tcol, const float* tval, uint32_t 
 }
 
 // iweights = alpha / out-weight (0 for a vertex without out-weight,
-// apps/pagerank_blas.cu:41-53), the initial ranks 1/N, x0 = rank0 * iw and
-// the dangling sum of rank0.
+// apps/pagerank_blas.cu:41-53), the initial ranks 1/N, x0 = rank0 * iw,
+// x1 = 0 where there is no out-weight (never written after), and the
+// dangling sum of rank0.
 __global__ void pr_init_from_outw_kernel(const float* outw, uint32_t n, float alpha, float* iw,
-                                         float* rank0, float* x0, unsigned long long* dang_out) {
+                                         float* rank0, float* x0, float* x1,
+                                         unsigned long long* dang_out) {
     __shared__ alignas(16) char smem[64 * 8];
     const float r0 = (float)(1.0 / (double)n);
     unsigned long long dl = 0ull;
@@ -127,9 +147,44 @@ __global__ void pr_init_from_outw_kernel(const float* outw, uint32_t n, float al
         iw[v] = w;
         rank0[v] = r0;
         x0[v] = r0 * w;
-        if (w == 0.0f) dl += dang_fixed(r0);
+        if (w == 0.0f) {
+            x1[v] = 0.0f;
+            dl += dang_fixed(r0);
+        }
     }
     dang_block_add<256>(dl, dang_out, smem);
+}
+
+struct HasOutWeight {
+    const float* outw;
+    __device__ __forceinline__ bool operator()(uint32_t v) const { return outw[v] != 0.0f; }
+};
+
+// The empty in-edge rows with out-weight, in plan order (the nnz fixup
+// emits only these before the last iteration) and the number of isolated
+// vertices; once per graph.
+static g1_status pr_empty_active(g1_graph* g, const NnzPlan& p, const float* outw, cudaStream_t s) {
+    uint32_t* list = nullptr;
+    uint32_t* count = nullptr;
+    G1_TRY(g->ws.get("pr_empty_active", (size_t)p.n_empty + 1, &list));
+    G1_TRY(g->ws.get("pr_empty_count", 4, &count));
+    const uint32_t* empty = p.rows.as<uint32_t>() + p.n_nonempty;
+    uint32_t active = 0;
+    if (p.n_empty > 0) {
+        size_t tb = 0;
+        G1_CUDA(cub::DeviceSelect::If(nullptr, tb, empty, list, count, (int)p.n_empty,
+                                      HasOutWeight{outw}, s));
+        DevBuf temp;
+        G1_TRY(temp.ensure(tb + 16));
+        G1_CUDA(cub::DeviceSelect::If(temp.p, tb, empty, list, count, (int)p.n_empty,
+                                      HasOutWeight{outw}, s));
+        G1_CUDA(cudaMemcpyAsync(&active, count, 4, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaStreamSynchronize(s));
+    }
+    g->pr_active_empty = active;
+    g->pr_isolated = p.n_empty - active;
+    g->pr_empty_ready = true;
+    return G1_OK;
 }
 
 struct PrBuffers {
@@ -175,17 +230,24 @@ static g1_status pr_setup(g1_graph* g, float alpha, PrBuffers& b, uint32_t* grid
         g->outw_ready = true;
     }
     pr_init_from_outw_kernel<<<grids[3], 256, 0, s>>>(outw, n, alpha, b.iw, b.rank[0], b.x[0],
-                                                      &b.dang[0]);
+                                                      b.x[1], &b.dang[0]);
     count_launches(1);
     G1_CUDA(cudaGetLastError());
+    const int v = merge_variant(g, t);
+    if (kMergeVariants[v].kind == 3 && !g->pr_empty_ready) {
+        NnzPlan* p = nullptr;
+        G1_TRY(ensure_nnz_plan(g, t, &p));
+        G1_TRY(pr_empty_active(g, *p, outw, s));
+    }
     return G1_OK;
 }
 
-// PageRank iteration `it`: reads x[cur], writes rank[nxt], x[nxt] (cur =
-// it & 1); reads dang[it % 3], adds into dang[(it + 1) % 3], zeroes
-// dang[(it + 2) % 3].
+// PageRank iteration `it` of `iters`: reads x[cur], writes x[nxt] (cur =
+// it & 1) and, in the last iteration, rank[nxt]; reads dang[it % 3], adds
+// into dang[(it + 1) % 3], zeroes dang[(it + 2) % 3].
 static g1_status pr_iterate(g1_graph* g, const PrBuffers& b, const uint32_t* grids, float alpha,
-                            g1_pr_mode mode, int it, g1_schedule sched, cudaStream_t s) {
+                            g1_pr_mode mode, int it, int iters, g1_schedule sched, cudaStream_t s) {
+    const bool last = it == iters - 1;
     const int cur = it & 1, nxt = cur ^ 1;
     PrEpilogue e;
     e.rank_next = b.rank[nxt];
@@ -197,11 +259,19 @@ static g1_status pr_iterate(g1_graph* g, const PrBuffers& b, const uint32_t* gri
     e.alpha_over_n = (double)alpha / (double)g->n;
     e.base0 = (float)((1.0 - (double)alpha) / (double)g->n);
     e.dangling = mode == G1_PR_DANGLING;
+    e.write_rank = last ? 1 : 0;
     const int t = 1;
     if (resolve_schedule(g, t, sched) == G1_SCHED_VECTOR)
         return launch_vector<PlusTimesF32>(g, t, b.x[cur], e, s);
     PrEpilogue f = e;
     f.dang_clear = nullptr;
+    if (!last && g->pr_empty_ready && kMergeVariants[merge_variant(g, t)].kind == 3) {
+        uint32_t* list = nullptr;  // allocated by pr_empty_active, at least this large
+        G1_TRY(g->ws.get("pr_empty_active", (size_t)g->pr_active_empty + 1, &list));
+        f.empty_list = list;
+        f.n_empty_list = g->pr_active_empty;
+        f.n_iso = g->pr_isolated;
+    }
     return launch_merge<PlusTimesF32>(g, t, b.x[cur], e, f, s);
 }
 
@@ -225,7 +295,7 @@ extern "C" g1_status g1_pagerank(g1_graph* g, float alpha, int iters, g1_pr_mode
     uint32_t grids[4];
     G1_TRY(pr_setup(g, alpha, b, grids, s));
     for (int it = 0; it < iters; ++it)
-        G1_TRY(pr_iterate(g, b, grids, alpha, mode, it, G1_SCHED_AUTO, s));
+        G1_TRY(pr_iterate(g, b, grids, alpha, mode, it, iters, G1_SCHED_AUTO, s));
     G1_TRY(copy_out_vertices(g, rank_out, b.rank[iters & 1], s));
     return check_device_error(g, s);
 }

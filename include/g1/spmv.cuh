@@ -1029,6 +1029,16 @@ struct rows_independent : std::false_type {};
 template <class E>
 struct rows_independent<E, std::enable_if_t<E::kRowsIndependent>> : std::true_type {};
 
+// Epilogues with members `const uint32_t* empty_list; uint32_t
+// n_empty_list;` may narrow the empty rows the nnz fixup emits: when
+// empty_list is set, only those rows are emitted (the epilogue accounts for
+// the others itself).
+template <class E, class = void>
+struct has_empty_list : std::false_type {};
+template <class E>
+struct has_empty_list<E, std::void_t<decltype(std::declval<E&>().empty_list),
+                                     decltype(std::declval<E&>().n_empty_list)>> : std::true_type {};
+
 template <class E, bool = has_prepare<E>::value>
 struct prepared_type {
     using type = int;
@@ -1381,13 +1391,21 @@ spmv_nnz_fixup_kernel(NnzArgs<SR> a, Epi epi) {
     const NnzPlanView& p = a.plan;
     if constexpr (!kEarly) grid_dependency_wait();
     epi.begin();
+    const uint32_t* elist = p.empty_rows;
+    uint32_t n_empty = p.n_empty;
+    if constexpr (has_empty_list<Epi>::value) {
+        if (epi.empty_list) {
+            elist = epi.empty_list;
+            n_empty = epi.n_empty_list;
+        }
+    }
     // empty rows four at a time: their row ids and epilogue loads are all in
     // flight before the first store
     uint32_t e = i0;
-    for (; e + 3 * stride < p.n_empty; e += 4 * stride) {
+    for (; e + 3 * stride < n_empty; e += 4 * stride) {
         uint32_t v[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) v[q] = __ldg(p.empty_rows + e + q * stride);
+        for (int q = 0; q < 4; ++q) v[q] = __ldg(elist + e + q * stride);
         if constexpr (has_prepare<Epi>::value) {
             typename prepared_type<Epi>::type pre[4];
 #pragma unroll
@@ -1399,7 +1417,7 @@ spmv_nnz_fixup_kernel(NnzArgs<SR> a, Epi epi) {
             for (int q = 0; q < 4; ++q) epi.emit(v[q], SR::identity());
         }
     }
-    for (; e < p.n_empty; e += stride) epi.emit(__ldg(p.empty_rows + e), SR::identity());
+    for (; e < n_empty; e += stride) epi.emit(__ldg(elist + e), SR::identity());
     if constexpr (kEarly) grid_dependency_wait();
     grid_launch_dependents();
     // rows begun in the previous tile

@@ -74,6 +74,37 @@ def test_pagerank_golden(cuda):
         assert O.rel_l1(r, gold[f"pr{mode}_rank"]) < 1e-6
 
 
+@pytest.mark.parametrize("iters", [1, 2, 3, 30])
+def test_pagerank_isolated_vertices_every_nnz_variant(cuda, iters):
+    """Isolated vertices (no in- or out-edges) are skipped by the nnz fixup
+    before the last iteration and counted into the dangling mass instead;
+    rank is written only in the last iteration.  Results must match the FP64
+    oracle, and every nnz variant (same fold order) must give the same bits."""
+    import torch
+    g0 = gen.rmat(12, 16, False, float_values=True)
+    rp0, ci0, _ = g0.np("n")
+    n = g0.n + 5000  # 5000 extra isolated vertices at the end
+    src = torch.from_numpy(np.repeat(np.arange(g0.n), np.diff(rp0)).astype(np.int64))
+    dst = torch.from_numpy(ci0.astype(np.int64))
+    g = gen.from_edges(src, dst, n, False, (1, 64), float_values=True)
+    trp, tci, tv = g.np("t")
+    rp, ci, v = g.np("n")
+    G = g1.Graph.from_csr(rp, ci, v, relabel=True)
+    nnz_variants = [i for i, k in enumerate(g1.MERGE_VARIANTS) if k == "nnz"]
+    for mode in (g1.PR_REFERENCE, g1.PR_DANGLING):
+        ref = O.pagerank_f64(trp, tci, tv, 0.85, iters, mode)
+        first = None
+        for var in nnz_variants:
+            G.set_schedule(g1.SCHED_MERGE, var, transpose=1)
+            r = G.pagerank(0.85, iters, mode)
+            assert O.rel_l1(r, ref) < 1e-6, (mode, var)  # tolerance: relative L1 vs FP64
+            if first is None:
+                first = r
+                assert np.array_equal(G.pagerank(0.85, iters, mode), r)  # run to run
+            else:
+                assert np.array_equal(r, first), (mode, var)
+
+
 def test_pagerank_device_output_and_zero_iterations(cuda):
     import torch
     g = gen.rmat(10, 16, False, float_values=True)
