@@ -489,12 +489,11 @@ __global__ void nnz_fix_place_kernel(const uint32_t* flag, const uint32_t* pos, 
     if (t < n_tiles && flag[t]) fix_tiles[pos[t]] = t;
 }
 
-// The fixup's per-entry facts, resolved once per graph instead of through
-// tile_seg -> rows -> row_ptr on every launch; is_long[i]: the row spans
-// more than one tile boundary.
-__global__ void nnz_fix_info_kernel(const uint32_t* fix_tiles, uint32_t n_fix, const uint32_t* tile_seg,
+// is_long[i]: fix entry i's row spans more than one tile boundary (its
+// first nonzero lies before tile t-1).
+__global__ void nnz_fix_long_kernel(const uint32_t* fix_tiles, uint32_t n_fix, const uint32_t* tile_seg,
                                     const uint32_t* nz_rows, const uint32_t* rp, uint32_t tile,
-                                    uint4* info, uint32_t* is_long) {
+                                    uint32_t* is_long) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > n_fix) return;
     if (i == n_fix) {
@@ -503,17 +502,22 @@ __global__ void nnz_fix_info_kernel(const uint32_t* fix_tiles, uint32_t n_fix, c
     }
     const uint32_t t = fix_tiles[i];
     const uint32_t row = nz_rows[tile_seg[t]];
-    const uint32_t first = rp[row] / tile;
-    info[i] = make_uint4(t, row, first, 0u);
-    is_long[i] = first + 1 < t ? 1u : 0u;
+    is_long[i] = rp[row] / tile + 1 < t ? 1u : 0u;
 }
 
-// Stable partition of the fix entries: short ones first, then long ones.
-__global__ void nnz_fix_split_kernel(const uint4* info, const uint32_t* is_long, const uint32_t* lpos,
-                                     uint32_t n_fix, uint32_t n_short, uint4* out) {
+// The fixup's per-entry facts {tile, row, first tile of the row}, resolved
+// once per graph instead of through tile_seg -> rows -> row_ptr on every
+// launch: entries of rows that cross one boundary first, then the longer
+// chains, each in tile order (lpos: exclusive scan of is_long).
+__global__ void nnz_fix_info_kernel(const uint32_t* fix_tiles, uint32_t n_fix, const uint32_t* tile_seg,
+                                    const uint32_t* nz_rows, const uint32_t* rp, uint32_t tile,
+                                    const uint32_t* lpos, uint32_t n_short, uint4* info) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_fix) return;
-    out[is_long[i] ? n_short + lpos[i] : i - lpos[i]] = info[i];
+    const uint32_t t = fix_tiles[i];
+    const uint32_t row = nz_rows[tile_seg[t]];
+    const uint32_t first = rp[row] / tile;
+    info[first + 1 < t ? n_short + lpos[i] : i - lpos[i]] = make_uint4(t, row, first, 0u);
 }
 
 g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
@@ -533,9 +537,11 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
     G1_TRY(p->rows.ensure(((size_t)n + 1) * 4));
     G1_TRY(p->carry.ensure(((size_t)p->n_tiles + 1) * 16));
     G1_TRY(p->tail.ensure(((size_t)p->n_tiles + 1) * 16));
+    // scratch shared by every phase below (vertices, tiles, fix entries)
     DevBuf flag, rank, temp;
-    G1_TRY(flag.ensure(((size_t)n + 1) * 4));
-    G1_TRY(rank.ensure(((size_t)n + 1) * 4));
+    const size_t scratch = ((size_t)std::max(n, p->n_tiles) + 1) * 4;
+    G1_TRY(flag.ensure(scratch));
+    G1_TRY(rank.ensure(scratch));
     const uint32_t grid = grid_for(n, 256, g->sm_count);
     G1_CUDA(cudaMemset(p->sbits.p, 0, words * 4));
     G1_CUDA(cudaMemset(flag.p, 0, ((size_t)n + 1) * 4));
@@ -554,51 +560,39 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
         o.rp, n, m, rank.as<uint32_t>(), nne, p->n_tiles, kNnzTile, p->tile_seg.as<uint32_t>());
     // tiles the fixup visits, in tile order (a deterministic compaction)
     {
-        DevBuf fflag, fpos, ftemp;
-        G1_TRY(fflag.ensure(((size_t)p->n_tiles + 1) * 4));
-        G1_TRY(fpos.ensure(((size_t)p->n_tiles + 1) * 4));
+        uint32_t* fflag = flag.as<uint32_t>();
+        uint32_t* fpos = rank.as<uint32_t>();
         const uint32_t tb = (uint32_t)ceil_div((uint64_t)p->n_tiles + 1, 256);
-        nnz_fix_flag_kernel<<<tb, 256>>>(p->sbits.as<uint32_t>(), p->n_tiles, m, kNnzTile,
-                                         fflag.as<uint32_t>());
+        nnz_fix_flag_kernel<<<tb, 256>>>(p->sbits.as<uint32_t>(), p->n_tiles, m, kNnzTile, fflag);
         size_t sb = 0;
-        G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, sb, fflag.as<uint32_t>(), fpos.as<uint32_t>(),
-                                              (int)p->n_tiles + 1));
-        G1_TRY(ftemp.ensure(sb + 16));
-        G1_CUDA(cub::DeviceScan::ExclusiveSum(ftemp.p, sb, fflag.as<uint32_t>(), fpos.as<uint32_t>(),
-                                              (int)p->n_tiles + 1));
+        G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, sb, fflag, fpos, (int)p->n_tiles + 1));
+        G1_TRY(temp.ensure(sb + 16));
+        G1_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, sb, fflag, fpos, (int)p->n_tiles + 1));
         uint32_t nfix = 0;
-        G1_CUDA(cudaMemcpy(&nfix, fpos.as<uint32_t>() + p->n_tiles, 4, cudaMemcpyDeviceToHost));
+        G1_CUDA(cudaMemcpy(&nfix, fpos + p->n_tiles, 4, cudaMemcpyDeviceToHost));
         p->n_fix = nfix;
         G1_TRY(p->fix_tiles.ensure(((size_t)nfix + 1) * 4));
-        nnz_fix_place_kernel<<<tb, 256>>>(fflag.as<uint32_t>(), fpos.as<uint32_t>(), p->n_tiles,
-                                          p->fix_tiles.as<uint32_t>());
+        nnz_fix_place_kernel<<<tb, 256>>>(fflag, fpos, p->n_tiles, p->fix_tiles.as<uint32_t>());
         G1_TRY(p->fix_info.ensure(((size_t)nfix + 1) * 16));
         p->n_fix_short = 0;
         if (nfix > 0) {
-            DevBuf raw, lflag, lpos, ltemp;
-            G1_TRY(raw.ensure(((size_t)nfix + 1) * 16));
-            G1_TRY(lflag.ensure(((size_t)nfix + 1) * 4));
-            G1_TRY(lpos.ensure(((size_t)nfix + 1) * 4));
+            // fix entries by kind (flag, rank reused: nfix <= n_tiles)
+            uint32_t* lflag = flag.as<uint32_t>();
+            uint32_t* lpos = rank.as<uint32_t>();
             const uint32_t fb = (uint32_t)ceil_div((uint64_t)nfix + 1, 256);
-            nnz_fix_info_kernel<<<fb, 256>>>(p->fix_tiles.as<uint32_t>(), nfix, p->tile_seg.as<uint32_t>(),
-                                             p->rows.as<uint32_t>(), o.rp, kNnzTile, raw.as<uint4>(),
-                                             lflag.as<uint32_t>());
+            nnz_fix_long_kernel<<<fb, 256>>>(p->fix_tiles.as<uint32_t>(), nfix, p->tile_seg.as<uint32_t>(),
+                                             p->rows.as<uint32_t>(), o.rp, kNnzTile, lflag);
             size_t lb = 0;
-            G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, lb, lflag.as<uint32_t>(), lpos.as<uint32_t>(),
-                                                  (int)nfix + 1));
-            G1_TRY(ltemp.ensure(lb + 16));
-            G1_CUDA(cub::DeviceScan::ExclusiveSum(ltemp.p, lb, lflag.as<uint32_t>(), lpos.as<uint32_t>(),
-                                                  (int)nfix + 1));
+            G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, lb, lflag, lpos, (int)nfix + 1));
+            G1_TRY(temp.ensure(lb + 16));
+            G1_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, lb, lflag, lpos, (int)nfix + 1));
             uint32_t nlong = 0;
-            G1_CUDA(cudaMemcpy(&nlong, lpos.as<uint32_t>() + nfix, 4, cudaMemcpyDeviceToHost));
+            G1_CUDA(cudaMemcpy(&nlong, lpos + nfix, 4, cudaMemcpyDeviceToHost));
             p->n_fix_short = nfix - nlong;
-            nnz_fix_split_kernel<<<fb, 256>>>(raw.as<uint4>(), lflag.as<uint32_t>(), lpos.as<uint32_t>(), nfix,
-                                              p->n_fix_short, p->fix_info.as<uint4>());
-            G1_CUDA(cudaGetLastError());
-            G1_CUDA(cudaDeviceSynchronize());
+            nnz_fix_info_kernel<<<fb, 256>>>(p->fix_tiles.as<uint32_t>(), nfix, p->tile_seg.as<uint32_t>(),
+                                             p->rows.as<uint32_t>(), o.rp, kNnzTile, lpos, p->n_fix_short,
+                                             p->fix_info.as<uint4>());
         }
-        G1_CUDA(cudaGetLastError());
-        G1_CUDA(cudaDeviceSynchronize());
     }
     count_launches(p->n_fix > 0 ? 7 : 5);
     G1_CUDA(cudaGetLastError());

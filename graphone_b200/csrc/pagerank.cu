@@ -174,9 +174,9 @@ static g1_status pr_empty_active(g1_graph* g, const NnzPlan& p, const float* out
         size_t tb = 0;
         G1_CUDA(cub::DeviceSelect::If(nullptr, tb, empty, list, count, (int)p.n_empty,
                                       HasOutWeight{outw}, s));
-        DevBuf temp;
-        G1_TRY(temp.ensure(tb + 16));
-        G1_CUDA(cub::DeviceSelect::If(temp.p, tb, empty, list, count, (int)p.n_empty,
+        unsigned char* temp = nullptr;  // kept in the graph's workspace: no free
+        G1_TRY(g->ws.get("pr_select_tmp", tb + 16, &temp));
+        G1_CUDA(cub::DeviceSelect::If(temp, tb, empty, list, count, (int)p.n_empty,
                                       HasOutWeight{outw}, s));
         G1_CUDA(cudaMemcpyAsync(&active, count, 4, cudaMemcpyDeviceToHost, s));
         G1_CUDA(cudaStreamSynchronize(s));
