@@ -247,6 +247,14 @@ __device__ __forceinline__ uint32_t ldg_u32_policy(const void* ptr, uint64_t pol
     asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(r) : "l"(ptr), "l"(pol));
     return r;
 }
+// 4-byte load through a generic address: one instruction whether `p` points
+// into this block's shared memory or into global memory.
+__device__ __forceinline__ uint32_t ld_generic_u32(const void* p) {
+    uint32_t v;
+    asm volatile("ld.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
 // Brings the line holding `p` into L2 ahead of use.
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));

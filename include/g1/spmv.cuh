@@ -1106,6 +1106,13 @@ __device__ __forceinline__ NnzReady<SR, Epi> nnz_gather(const NnzArgs<SR>& a, co
                 const uint32_t bits = ldg_u32_policy(a.x + cc[u], pol_keep);
                 memcpy(&r.x[u], &bits, 4);
             }
+        } else if constexpr (HOT > 0 && sizeof(X) == 4) {
+            // one generic load from the shared-memory copy or from global x
+            // (a shared and a global load per element would both issue for
+            // almost every warp)
+            const X* src = (cc[u] < hot ? xc : a.x) + cc[u];
+            const uint32_t bits = ld_generic_u32(src);
+            memcpy(&r.x[u], &bits, 4);
         } else if constexpr (HOT > 0) {
             r.x[u] = cc[u] < hot ? xc[cc[u]] : ldg_any(a.x + cc[u]);
         } else {
@@ -1123,7 +1130,9 @@ __device__ __forceinline__ NnzReady<SR, Epi> nnz_gather(const NnzArgs<SR>& a, co
     return r;
 }
 
-template <class SR, class Epi>
+// FULL: the tile is not the last one (all 256 nonzeros exist, and the tile
+// does not end the matrix).
+template <class SR, class Epi, bool FULL = false>
 __device__ __forceinline__ void nnz_finish(const NnzArgs<SR>& a, const NnzReady<SR, Epi>& r,
                                            uint32_t tile, typename SR::value_t* sy, Epi& epi) {
     using V = typename SR::value_t;
@@ -1135,7 +1144,7 @@ __device__ __forceinline__ void nnz_finish(const NnzArgs<SR>& a, const NnzReady<
     const uint32_t jl = j0 + lane * IPT;
     // nonzeros of this lane that exist (the last tile may be short);
     // padding past nnz has no start bits
-    const uint32_t nv = jl < nnz ? min(nnz - jl, IPT) : 0u;
+    const uint32_t nv = FULL ? IPT : (jl < nnz ? min(nnz - jl, IPT) : 0u);
     const uint32_t sb = (r.sw >> ((lane & 3u) * 8u)) & 0xFFu;
     const bool first_start = (__shfl_sync(0xffffffffu, r.sw, 0) & 1u) != 0u;
     V pv[IPT];
@@ -1190,7 +1199,7 @@ __device__ __forceinline__ void nnz_finish(const NnzArgs<SR>& a, const NnzReady<
     }
     const uint32_t nstarts = __shfl_sync(0xffffffffu, incl, 31);
     const V last = shfl_any(0xffffffffu, s, 31);
-    const bool closed = (j0 + kNnzTile >= nnz) || (r.endw & 1u);
+    const bool closed = (!FULL && j0 + kNnzTile >= nnz) || (r.endw & 1u);
     if (lane == 0) {
         if (nstarts == 0) {
             a.tail[tile] = last;
@@ -1335,7 +1344,10 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
             }
             const NnzIn in = nnz_load<SR, HINTS>(a, tile, pol_stream);
             const NnzReady<SR, Epi> r = nnz_gather<SR, Epi, HOT, HINTS>(a, in, xc, hot, pol_keep, epi);
-            nnz_finish<SR, Epi>(a, r, tile, sy, epi);
+            if (tile + 1 < n_tiles)
+                nnz_finish<SR, Epi, true>(a, r, tile, sy, epi);
+            else
+                nnz_finish<SR, Epi>(a, r, tile, sy, epi);
         }
     } else {
         uint32_t ta = blockIdx.x * WARPS + w;
