@@ -1121,8 +1121,9 @@ __device__ __forceinline__ NnzReady<SR, Epi> nnz_gather(const NnzArgs<SR>& a, co
     }
     r.sw = in.sw;
     r.endw = in.endw;
-    // the first 32 rows the tile may emit (rows past its last are unused)
-    const bool first_start = (__shfl_sync(0xffffffffu, in.sw, 0) & 1u) != 0u;
+    // the first 32 rows the tile may emit (rows past its last are unused);
+    // bit 0 of the ballot is lane 0's: does the tile begin with a row
+    const bool first_start = (__ballot_sync(0xffffffffu, in.sw & 1u) & 1u) != 0u;
     r.seg_base = in.seg0 + (first_start ? 0u : 1u);
     r.row_pre = r.seg_base + lane < a.plan.n_nonempty ? __ldg(a.plan.nz_rows + r.seg_base + lane) : 0u;
     if constexpr (has_prepare<Epi>::value) r.pre = epi.prepare(r.row_pre);
@@ -1146,7 +1147,7 @@ __device__ __forceinline__ void nnz_finish(const NnzArgs<SR>& a, const NnzReady<
     // padding past nnz has no start bits
     const uint32_t nv = FULL ? IPT : (jl < nnz ? min(nnz - jl, IPT) : 0u);
     const uint32_t sb = (r.sw >> ((lane & 3u) * 8u)) & 0xFFu;
-    const bool first_start = (__shfl_sync(0xffffffffu, r.sw, 0) & 1u) != 0u;
+    const bool first_start = (__ballot_sync(0xffffffffu, r.sw & 1u) & 1u) != 0u;
     V pv[IPT];
 #pragma unroll
     for (int u = 0; u < (int)IPT; ++u) {
@@ -1154,15 +1155,19 @@ __device__ __forceinline__ void nnz_finish(const NnzArgs<SR>& a, const NnzReady<
         memcpy(&wv, &r.v[u], 4);
         pv[u] = (uint32_t)u < nv ? SR::combine(wv, r.x[u]) : SR::identity();
     }
-    // starts before this lane (exclusive prefix of the per-lane counts)
+    // starts before this lane (exclusive prefix of the per-lane counts, 0..8)
+    // and in the whole tile, from four bit-sliced ballots of the counts
     const uint32_t nst = __popc(sb);
-    uint32_t incl = nst;
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t excl = 0, nstarts = 0;
 #pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
-        if ((int)lane >= off) incl += t;
+    for (int b = 0; b < 4; ++b) {
+        const uint32_t bb = __ballot_sync(0xffffffffu, (nst >> b) & 1u);
+        excl += (uint32_t)__popc(bb & below) << b;
+        nstarts += (uint32_t)__popc(bb) << b;
     }
-    const uint32_t excl = incl - nst;
+    // lanes at or below this one that hold a row start
+    const uint32_t has_upto = __ballot_sync(0xffffffffu, nst != 0u) & ((2u << lane) - 1u);
     // 1. lane-local fold
     V head = SR::identity(), acc = SR::identity();
     uint32_t k = 0;
@@ -1176,17 +1181,14 @@ __device__ __forceinline__ void nnz_finish(const NnzArgs<SR>& a, const NnzReady<
         }
         acc = SR::reduce(acc, pv[u]);
     }
-    // 2. segmented scan of the lane tails
+    // 2. segmented scan of the lane tails: at offset `off`, s covers lanes
+    // (lane - off, lane] unless a start lies there (then it is complete)
     V s = acc;
-    int f = nst ? 1 : 0;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
         const V su = shfl_up_any(0xffffffffu, s, off);
-        const int fu = __shfl_up_sync(0xffffffffu, f, off);
-        if ((int)lane >= off) {
-            if (!f) s = SR::reduce(su, s);
-            f |= fu;
-        }
+        const bool open = (int)lane >= off && (has_upto >> ((lane - off + 1) & 31u)) == 0u;
+        if (open) s = SR::reduce(su, s);
     }
     V prev = shfl_up_any(0xffffffffu, s, 1);
     if (lane == 0) prev = SR::identity();
@@ -1197,7 +1199,6 @@ __device__ __forceinline__ void nnz_finish(const NnzArgs<SR>& a, const NnzReady<
         else if (!first_start)
             a.tail[tile] = val;  // the row begun in an earlier tile ends here
     }
-    const uint32_t nstarts = __shfl_sync(0xffffffffu, incl, 31);
     const V last = shfl_any(0xffffffffu, s, 31);
     const bool closed = (!FULL && j0 + kNnzTile >= nnz) || (r.endw & 1u);
     if (lane == 0) {
