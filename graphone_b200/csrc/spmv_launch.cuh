@@ -247,6 +247,9 @@ g1_status launch_nnz(g1_graph* g, int t, const NnzPlan& p, const typename SR::x_
                      const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
     using K = NnzKernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1, BULK>;
     const NnzArgs<SR> a = nnz_args<SR>(g, t, p, x);
+    // the tile kernel reads each lane's col/val with 32-byte loads
+    if (((uintptr_t)a.col | (uintptr_t)a.val) & 31u)
+        return fail(G1_ERR_UNSUPPORTED, "nnz SpMV: col/val not 32-byte aligned");
     const bool prof = profiling();
     // launched even without tiles: its blocks' epilogue partials are read.
     // Both kernels use programmatic dependent launch (the fixup's empty rows

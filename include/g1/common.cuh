@@ -241,6 +241,13 @@ __device__ __forceinline__ uint4 ldg_v4_policy(const void* ptr, uint64_t pol) {
         : "l"(ptr), "l"(pol));
     return r;
 }
+// 32-byte read-only load (sm_100 256-bit vector load); `ptr` must be
+// 32-byte aligned.
+__device__ __forceinline__ void ldg_v8(const void* ptr, uint4& lo, uint4& hi) {
+    asm("ld.global.nc.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(lo.x), "=r"(lo.y), "=r"(lo.z), "=r"(lo.w), "=r"(hi.x), "=r"(hi.y), "=r"(hi.z), "=r"(hi.w)
+        : "l"(ptr));
+}
 // 4-byte read-only load with an L2 policy.
 __device__ __forceinline__ uint32_t ldg_u32_policy(const void* ptr, uint64_t pol) {
     uint32_t r;

@@ -1076,10 +1076,10 @@ __device__ __forceinline__ NnzIn nnz_load(const NnzArgs<SR>& a, uint32_t tile, u
         in.v0 = ldg_v4_policy(a.val + jl, pol_stream);
         in.v1 = ldg_v4_policy(a.val + jl + 4, pol_stream);
     } else {
-        in.c0 = __ldg(reinterpret_cast<const uint4*>(a.col + jl));
-        in.c1 = __ldg(reinterpret_cast<const uint4*>(a.col + jl + 4));
-        in.v0 = __ldg(reinterpret_cast<const uint4*>(a.val + jl));
-        in.v1 = __ldg(reinterpret_cast<const uint4*>(a.val + jl + 4));
+        // a lane's 8 columns and values are 32 aligned bytes each (col and
+        // val are 32-byte aligned; the host checks)
+        ldg_v8(a.col + jl, in.c0, in.c1);
+        ldg_v8(a.val + jl, in.v0, in.v1);
     }
     in.sw = __ldg(a.plan.sbits + (j0 >> 5) + (lane >> 2));
     in.endw = __ldg(a.plan.sbits + ((j0 + kNnzTile) >> 5));
