@@ -445,6 +445,21 @@ __device__ __forceinline__ void warp_seg_scan_rows(bool head, RowPartial<typenam
 // (the hottest vertices when the graph is degree-ordered) and, per warp, the
 // (combined value, row-start mark) of each item and the value of each row
 // completed in the tile.
+// x[c] from the shared-memory copy of x[0, hot) or from global x.  For
+// 4-byte values one generic-address load (a shared and a global load would
+// both issue for almost every warp); otherwise the two-way select.
+template <class X>
+__device__ __forceinline__ X gather_x(const X* xc, const X* x, uint32_t c, uint32_t hot) {
+    if constexpr (sizeof(X) == 4) {
+        const uint32_t bits = ld_generic_u32((c < hot ? xc : x) + c);
+        X v;
+        memcpy(&v, &bits, 4);
+        return v;
+    } else {
+        return c < hot ? xc[c] : ldg_any(x + c);
+    }
+}
+
 template <class V>
 struct alignas(8) ItemSlot {
     V val;
@@ -543,7 +558,7 @@ spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
         for (int u = 0; u < IPT; ++u) {
             if ((uint32_t)u < nv) {
                 if constexpr (HOT > 0)
-                    xv[u] = cv[u] < hot ? xc[cv[u]] : ldg_any(a.x + cv[u]);
+                    xv[u] = gather_x(xc, a.x, cv[u], hot);
                 else
                     xv[u] = ldg_any(a.x + cv[u]);
             }
@@ -770,7 +785,7 @@ spmv_wtma_kernel(MergeArgs<SR> a, Epi epi) {
                 const uint32_t c = CO[u * 32 + lane];
                 X xval;
                 if constexpr (HOT > 0)
-                    xval = c < hot ? xc[c] : ldg_any(a.x + c);
+                    xval = gather_x(xc, a.x, c, hot);
                 else
                     xval = ldg_any(a.x + c);
                 vv[u] = SR::combine(VA[u * 32 + lane], xval);
@@ -1106,15 +1121,8 @@ __device__ __forceinline__ NnzReady<SR, Epi> nnz_gather(const NnzArgs<SR>& a, co
                 const uint32_t bits = ldg_u32_policy(a.x + cc[u], pol_keep);
                 memcpy(&r.x[u], &bits, 4);
             }
-        } else if constexpr (HOT > 0 && sizeof(X) == 4) {
-            // one generic load from the shared-memory copy or from global x
-            // (a shared and a global load per element would both issue for
-            // almost every warp)
-            const X* src = (cc[u] < hot ? xc : a.x) + cc[u];
-            const uint32_t bits = ld_generic_u32(src);
-            memcpy(&r.x[u], &bits, 4);
         } else if constexpr (HOT > 0) {
-            r.x[u] = cc[u] < hot ? xc[cc[u]] : ldg_any(a.x + cc[u]);
+            r.x[u] = gather_x(xc, a.x, cc[u], hot);
         } else {
             r.x[u] = ldg_any(a.x + cc[u]);
         }
