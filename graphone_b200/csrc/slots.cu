@@ -238,6 +238,10 @@ g1_status slot_graph(g1_graph* g, int kind, cudaStream_t s, SlotGraph* out) {
 //   [1] iteration x - 1 built that list and recorded its changed vertices,
 //   [2] how many changed vertices it recorded,
 //   [3] sum of (out-degree + 1) over the vertices it changed.
+//
+// The iteration number is it + *it_base when it_base is set: a step
+// captured in a CUDA graph bakes in offsets and the buffers of its rotation
+// phase, and reads the iterations completed before it from the device.
 struct Frontier {
     uint32_t* mark;             // n: iteration a vertex was listed for
     const uint32_t* plist_in;   // this iteration's row pieces (when valid)
@@ -245,9 +249,23 @@ struct Frontier {
     uint32_t* clist_out;        // vertices this iteration changes
     const uint32_t* clist_old;  // vertices changed two iterations ago
     uint32_t* ctr;
+    const uint32_t* it_base;    // device word added to `it`, or null
     uint32_t it;
     uint32_t thresh;  // the next list is built while the changed degree sum is below
 };
+
+__device__ __forceinline__ uint32_t frontier_iter(const Frontier& f) {
+    return f.it + (f.it_base ? *f.it_base : 0u);
+}
+
+// Bit j: word j of the occupied slots (device words) is not empty.
+__device__ __forceinline__ uint32_t occ_word_mask(const uint32_t* occ, uint32_t W) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        if ((uint32_t)j < W && __ldg(occ + j) != 0u) m |= 1u << j;
+    return m;
+}
 
 struct IterCtl {
     bool dense;      // pull every row piece
@@ -263,12 +281,12 @@ struct IterCtl {
 // previous one listed its pieces and the one before recorded its changed
 // vertices; it builds the next list only while few edges leave the
 // vertices the previous iteration changed.
-__device__ __forceinline__ IterCtl iter_begin(const SlotGraph& sg, const Frontier& f, uint32_t W,
-                                              uint32_t* clear) {
-    const uint32_t* cin = f.ctr + 4 * (f.it & 3u);
-    uint32_t* cout = f.ctr + 4 * ((f.it + 1) & 3u);
-    uint32_t* cz = f.ctr + 4 * ((f.it + 2) & 3u);
-    const uint32_t* cold = f.ctr + 4 * ((f.it + 3) & 3u);
+__device__ __forceinline__ IterCtl iter_begin(const SlotGraph& sg, const Frontier& f, uint32_t it,
+                                              uint32_t W, uint32_t* clear) {
+    const uint32_t* cin = f.ctr + 4 * (it & 3u);
+    uint32_t* cout = f.ctr + 4 * ((it + 1) & 3u);
+    uint32_t* cz = f.ctr + 4 * ((it + 2) & 3u);
+    const uint32_t* cold = f.ctr + 4 * ((it + 3) & 3u);
     IterCtl c;
     c.dense = cin[1] == 0u || cold[1] == 0u;
     c.mark = sg.out_rp != nullptr && cin[3] < f.thresh;
@@ -321,12 +339,12 @@ __device__ void list_out_neighbours(const SlotGraph& sg, uint32_t* mark, uint32_
 // v changed in this iteration (warp-uniform call): its out-degree joins the
 // warp's total; while the next list is built it is recorded for the
 // clearing two iterations on and its out-neighbours are listed.
-__device__ __forceinline__ void note_changed(const SlotGraph& sg, const Frontier& f, const IterCtl& c,
-                                             uint32_t v, uint32_t& deg_acc) {
+__device__ __forceinline__ void note_changed(const SlotGraph& sg, const Frontier& f, uint32_t it,
+                                             const IterCtl& c, uint32_t v, uint32_t& deg_acc) {
     deg_acc += 1u + (sg.out_rp ? sg.out_rp[v + 1] - sg.out_rp[v] : 0u);
     if (!c.mark) return;
     if (lane_id() == 0) f.clist_out[atomicAdd(&c.cout[2], 1u)] = v;
-    list_out_neighbours(sg, f.mark, f.it + 1, f.plist_out, &c.cout[0], v);
+    list_out_neighbours(sg, f.mark, it + 1, f.plist_out, &c.cout[0], v);
 }
 
 __device__ __forceinline__ void iter_end(const IterCtl& c, uint32_t deg_acc) {
@@ -335,18 +353,19 @@ __device__ __forceinline__ void iter_end(const IterCtl& c, uint32_t deg_acc) {
 
 template <int WP>  // words per vertex rounded up to a power of two (1..8)
 __global__ void __launch_bounds__(256)
-slot_bfs_kernel(SlotGraph sg, Frontier f, uint32_t W, uint32_t K, Bits256 live, const uint32_t* front,
+slot_bfs_kernel(SlotGraph sg, Frontier f, uint32_t W, uint32_t K, const uint32_t* occ, const uint32_t* front,
                 uint32_t* seen, uint32_t* next, uint32_t* clear, uint32_t* lv, const uint32_t* start,
                 uint32_t* chw, uint32_t* chw_clear) {
     constexpr int SLOTS = 32 / WP;  // neighbours per warp step
     const uint32_t lane = lane_id();
     const uint32_t w = lane % WP, q = lane / WP;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    const uint32_t depth = f.it;
+    const uint32_t it = frontier_iter(f);
+    const uint32_t depth = it;
     if (blockIdx.x == 0 && threadIdx.x < 8) chw_clear[threadIdx.x] = 0u;
-    const IterCtl c = iter_begin(sg, f, W, clear);
+    const IterCtl c = iter_begin(sg, f, it, W, clear);
     const bool has_word = w < W;
-    const uint32_t lw = has_word ? live.w[w] : 0u;
+    const uint32_t lw = has_word ? __ldg(occ + w) : 0u;
     uint32_t new_acc = 0, deg_acc = 0;
     for (uint32_t idx = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; idx < c.total; idx += warps) {
         const uint32_t p = c.dense ? idx : f.plist_in[idx];
@@ -390,20 +409,22 @@ slot_bfs_kernel(SlotGraph sg, Frontier f, uint32_t W, uint32_t K, Bits256 live, 
             const uint32_t s = 32 * j + lane;
             if ((bits >> lane) & 1u) lv[(size_t)v * K + s] = depth - __ldg(start + s);
         }
-        if (any_new) note_changed(sg, f, c, v, deg_acc);
+        if (any_new) note_changed(sg, f, it, c, v, deg_acc);
     }
     iter_end(c, deg_acc);
     if (q == 0 && has_word && new_acc) atomicOr(&chw[w], new_acc);
 }
 
 __global__ void __launch_bounds__(256)
-slot_sssp_kernel(SlotGraph sg, Frontier f, uint32_t W, uint32_t K, uint32_t wmask, uint32_t* dist,
+slot_sssp_kernel(SlotGraph sg, Frontier f, uint32_t W, uint32_t K, const uint32_t* occ, uint32_t* dist,
                  const uint32_t* chg, uint32_t* chg_next, uint32_t* clear, uint32_t* chw,
                  uint32_t* chw_clear) {
     const uint32_t lane = lane_id();
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    const uint32_t it = frontier_iter(f);
+    const uint32_t wmask = occ_word_mask(occ, W);
     if (blockIdx.x == 0 && threadIdx.x < 8) chw_clear[threadIdx.x] = 0u;
-    const IterCtl c = iter_begin(sg, f, W, clear);
+    const IterCtl c = iter_begin(sg, f, it, W, clear);
     const bool my_word = lane < W && ((wmask >> lane) & 1u);
     uint32_t deg_acc = 0;
     uint32_t changed[8];
@@ -492,7 +513,7 @@ slot_sssp_kernel(SlotGraph sg, Frontier f, uint32_t W, uint32_t K, uint32_t wmas
             changed[j] |= bits;
             vbits |= bits;
         }
-        if (vbits) note_changed(sg, f, c, v, deg_acc);
+        if (vbits) note_changed(sg, f, it, c, v, deg_acc);
     }
     iter_end(c, deg_acc);
 #pragma unroll
@@ -503,8 +524,9 @@ slot_sssp_kernel(SlotGraph sg, Frontier f, uint32_t W, uint32_t K, uint32_t wmas
 // rank' = A^T (rank * iw) over the row's in-edges; hub rows go to
 // per-piece partials; per-warp dangling partial sums of the current rank.
 __global__ void __launch_bounds__(256)
-slot_ppr_pull_kernel(SlotGraph sg, uint32_t W, uint32_t K, uint32_t wmask, const float* iw,
+slot_ppr_pull_kernel(SlotGraph sg, uint32_t W, uint32_t K, const uint32_t* occ, const float* iw,
                      const float* rank, float* rank_next, float* hub_part, float* dang_part) {
+    const uint32_t wmask = occ_word_mask(occ, W);
     const uint32_t lane = lane_id();
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
@@ -551,7 +573,9 @@ slot_ppr_pull_kernel(SlotGraph sg, uint32_t W, uint32_t K, uint32_t wmask, const
 
 // Hub rows: sum of their pieces' partials in piece order.
 __global__ void __launch_bounds__(256)
-slot_ppr_hub_kernel(SlotGraph sg, uint32_t K, uint32_t wmask, const float* hub_part, float* rank_next) {
+slot_ppr_hub_kernel(SlotGraph sg, uint32_t W, uint32_t K, const uint32_t* occ, const float* hub_part,
+                    float* rank_next) {
+    const uint32_t wmask = occ_word_mask(occ, W);
     const uint32_t t = threadIdx.x;
     if (t >= K || !((wmask >> (t >> 5)) & 1u)) return;
     for (uint32_t h = blockIdx.x; h < sg.n_hubs; h += gridDim.x) {
@@ -567,11 +591,11 @@ slot_ppr_hub_kernel(SlotGraph sg, uint32_t K, uint32_t wmask, const float* hub_p
 // One block per slot: the dangling mass (per-warp partials folded in a
 // fixed order) and the teleport go to the slot's source.
 __global__ void __launch_bounds__(256)
-slot_ppr_teleport_kernel(uint32_t K, Bits256 occ, const uint32_t* slot_src, const float* dang_part,
+slot_ppr_teleport_kernel(uint32_t K, const uint32_t* occ, const uint32_t* slot_src, const float* dang_part,
                          uint32_t n_warps, double alpha, float* rank_next) {
     __shared__ double red[8];
     const uint32_t s = blockIdx.x;
-    if (s >= K || !((occ.w[s >> 5] >> (s & 31)) & 1u)) return;
+    if (s >= K || !((__ldg(occ + (s >> 5)) >> (s & 31)) & 1u)) return;
     double d = 0.0;
     for (uint32_t i = threadIdx.x; i < n_warps; i += blockDim.x) d += (double)dang_part[(size_t)i * K + s];
     d = block_sum<double, 256>(d, red);
@@ -579,6 +603,14 @@ slot_ppr_teleport_kernel(uint32_t K, Bits256 occ, const uint32_t* slot_src, cons
         const uint32_t v = slot_src[s];
         rank_next[(size_t)v * K + s] += (float)((1.0 - alpha) + alpha * d);
     }
+}
+
+// The last node of a captured step: the step's iterations are done.
+__global__ void slot_it_advance_kernel(uint32_t* it_base, uint32_t n) { *it_base += n; }
+
+// The occupied slots, by value into the device words the kernels read.
+__global__ void slot_set_occ_kernel(uint32_t* occ, Bits256 b) {
+    if (threadIdx.x < 8) occ[threadIdx.x] = b.w[threadIdx.x];
 }
 
 __global__ void slot_ppr_iw_kernel(const uint32_t* deg, uint32_t n, double alpha, float* iw) {
@@ -633,13 +665,15 @@ __global__ void slot_seed_kernel(int kind, SlotGraph sg, uint32_t W, uint32_t K,
         atomicOr(&front[(size_t)v * W + (s >> 5)], bit);
         if (kind == kSlotBfs) atomicOr(&seen[(size_t)v * W + (s >> 5)], bit);
     }
-    // f.it is the iteration that comes next; its counters are group it % 4
-    uint32_t* cnext = f.ctr + 4 * (f.it & 3u);
+    // the frontier's iteration is the one that comes next; its counters are
+    // group it % 4
+    const uint32_t it = frontier_iter(f);
+    uint32_t* cnext = f.ctr + 4 * (it & 3u);
     if (lane_id() == 0)
         atomicAdd(&cnext[3], 1u + (sg.out_rp ? sg.out_rp[v + 1] - sg.out_rp[v] : 0u));
     if (cnext[1] == 0u) return;  // the next iteration is dense
     if (lane_id() == 0) f.clist_out[atomicAdd(&cnext[2], 1u)] = v;
-    list_out_neighbours(sg, f.mark, f.it, f.plist_out, &cnext[0], v);
+    list_out_neighbours(sg, f.mark, it, f.plist_out, &cnext[0], v);
 }
 
 // out_c[v] = rows[perm(v)][slots[c]]: 32 vertices x 32 slots per block.
@@ -668,8 +702,10 @@ namespace {
 
 // Layout of slot_dev_ (u32 words): admission slots, admission sources,
 // extraction slots, internal sources of the slots, BFS start iterations.
+// Then the iteration counter and the occupied slots (8 words).
 constexpr size_t kDevAdmSlots = 0, kDevAdmSrcs = kMaxSlots, kDevExtSlots = 2 * kMaxSlots,
-                 kDevSlotSrc = 3 * kMaxSlots, kDevStart = 4 * kMaxSlots, kDevWords = 5 * kMaxSlots;
+                 kDevSlotSrc = 3 * kMaxSlots, kDevStart = 4 * kMaxSlots, kDevIt = 5 * kMaxSlots,
+                 kDevOcc = 5 * kMaxSlots + 8, kDevWords = 5 * kMaxSlots + 16;
 // Layout of host_ (pinned, u32 words): chw mirror, admission staging,
 // extraction staging, start staging; then K output pointers.
 constexpr size_t kHostChw = 0, kHostAdm = 16, kHostExt = 16 + 2 * kMaxSlots,
@@ -690,6 +726,7 @@ Frontier SlotEngine::frontier(uint32_t it) {
     f.clist_out = clist_[it % 3].as<uint32_t>();
     f.clist_old = clist_[(it + 1) % 3].as<uint32_t>();  // iteration it - 2's
     f.ctr = ctr_.as<uint32_t>();
+    f.it_base = nullptr;
     f.it = it;
     // the next list is built while fewer than 1/8 of the graph's edges
     // leave the changed vertices: listing costs at most that many marks,
@@ -720,7 +757,21 @@ size_t SlotEngine::device_bytes() const {
     return b;
 }
 
+void SlotEngine::drop_graphs() {
+    for (auto& row : graphs_)
+        for (auto& gx : row) {
+            if (gx) cudaGraphExecDestroy(gx);  // one still running is freed when it completes
+            gx = nullptr;
+        }
+}
+
 void SlotEngine::release() {
+    drop_graphs();
+    if (capture_) {
+        cudaStreamDestroy(capture_);
+        capture_ = nullptr;
+    }
+    occ_dev_valid_ = false;
     rows_.release();
     rows2_.release();
     for (auto& x : bits_) x.release();
@@ -806,6 +857,7 @@ g1_status SlotEngine::set_alpha(float alpha, uint32_t ppr_iters, cudaStream_t s)
     if (kind_ != kSlotPpr || alpha == alpha_) return G1_OK;
     if (n_used_) return fail(G1_ERR_INVALID, "damping changed while queries run");
     alpha_ = alpha;
+    drop_graphs();  // the teleport nodes hold the damping
     slot_ppr_iw_kernel<<<std::max<uint32_t>(1, std::min<uint32_t>(ceil_div(sg_.n, 256), sg_.sm_count * 16)),
                          256, 0, s>>>(sg_.out_deg, sg_.n, (double)alpha, iw_.as<float>());
     count_launches(1);
@@ -836,14 +888,6 @@ Bits256 SlotEngine::occupied_bits() const {
     for (uint32_t i = 0; i < K_; ++i)
         if (used_[i]) b.w[i >> 5] |= 1u << (i & 31);
     return b;
-}
-
-uint32_t SlotEngine::word_mask() const {
-    const Bits256 b = occupied_bits();
-    uint32_t m = 0;
-    for (uint32_t j = 0; j < W_; ++j)
-        if (b.w[j]) m |= 1u << j;
-    return m;
 }
 
 g1_status SlotEngine::admit(const uint32_t* slots, const uint32_t* srcs, uint32_t cnt, cudaStream_t s) {
@@ -905,22 +949,24 @@ uint32_t SlotEngine::max_step(uint32_t want) const {
     return std::max<uint32_t>(1, m);
 }
 
-g1_status SlotEngine::step(uint32_t iters, cudaStream_t s) {
-    if (!ready()) return fail(G1_ERR_INVALID, "slot engine not initialised");
-    const uint32_t wmask = word_mask();
-    const Bits256 occ = occupied_bits();
+g1_status SlotEngine::enqueue_iterations(uint32_t n, uint32_t phase, cudaStream_t s) {
     uint32_t* d = slot_dev_.as<uint32_t>();
     uint32_t* chw = chw_.as<uint32_t>();
+    const uint32_t* occ = d + kDevOcc;
     const uint32_t grid = pull_grid_;
-    for (uint32_t i = 0; i < iters; ++i) {
-        const uint32_t it = it_ + 1;
-        uint32_t* c_now = chw + 8 * (it & 1);
-        uint32_t* c_next = chw + 8 * ((it + 1) & 1);
+    for (uint32_t k = 1; k <= n; ++k) {
+        // buffers of iteration base + k, base = phase (mod 6); its number
+        // comes from the device counter
+        const uint32_t v = phase + k;
+        uint32_t* c_now = chw + 8 * (v & 1);
+        uint32_t* c_next = chw + 8 * ((v + 1) & 1);
         if (kind_ == kSlotBfs) {
-            const uint32_t* front = bits_[it % 3].as<uint32_t>();
-            uint32_t* next = bits_[(it + 1) % 3].as<uint32_t>();
-            uint32_t* clr = bits_[(it + 2) % 3].as<uint32_t>();
-            const Frontier f = frontier(it);
+            Frontier f = frontier(v);
+            f.it_base = d + kDevIt;
+            f.it = k;
+            const uint32_t* front = bits_[v % 3].as<uint32_t>();
+            uint32_t* next = bits_[(v + 1) % 3].as<uint32_t>();
+            uint32_t* clr = bits_[(v + 2) % 3].as<uint32_t>();
 #define G1_SLOT_BFS(WPV)                                                                              \
     slot_bfs_kernel<WPV><<<grid, 256, 0, s>>>(sg_, f, W_, K_, occ, front, seen_.as<uint32_t>(), next, clr, \
                                               rows_.as<uint32_t>(), d + kDevStart, c_now, c_next)
@@ -931,30 +977,82 @@ g1_status SlotEngine::step(uint32_t iters, cudaStream_t s) {
                 default: G1_SLOT_BFS(8); break;
             }
 #undef G1_SLOT_BFS
-            count_launches(1);
         } else if (kind_ == kSlotSssp) {
-            slot_sssp_kernel<<<grid, 256, 0, s>>>(sg_, frontier(it), W_, K_, wmask, rows_.as<uint32_t>(),
-                                                  bits_[it % 3].as<uint32_t>(),
-                                                  bits_[(it + 1) % 3].as<uint32_t>(),
-                                                  bits_[(it + 2) % 3].as<uint32_t>(), c_now, c_next);
-            count_launches(1);
+            Frontier f = frontier(v);
+            f.it_base = d + kDevIt;
+            f.it = k;
+            slot_sssp_kernel<<<grid, 256, 0, s>>>(sg_, f, W_, K_, occ, rows_.as<uint32_t>(),
+                                                  bits_[v % 3].as<uint32_t>(), bits_[(v + 1) % 3].as<uint32_t>(),
+                                                  bits_[(v + 2) % 3].as<uint32_t>(), c_now, c_next);
         } else {
-            const float* cur = (it_ & 1) ? rows2_.as<float>() : rows_.as<float>();
-            float* nxt = (it_ & 1) ? rows_.as<float>() : rows2_.as<float>();
-            slot_ppr_pull_kernel<<<grid, 256, 0, s>>>(sg_, W_, K_, wmask, iw_.as<float>(), cur, nxt,
+            // iteration it reads the rank block of parity (it - 1) and writes the other
+            const float* cur = ((v - 1) & 1) ? rows2_.as<float>() : rows_.as<float>();
+            float* nxt = ((v - 1) & 1) ? rows_.as<float>() : rows2_.as<float>();
+            slot_ppr_pull_kernel<<<grid, 256, 0, s>>>(sg_, W_, K_, occ, iw_.as<float>(), cur, nxt,
                                                       hub_part_.as<float>(), dang_part_.as<float>());
             if (sg_.n_hubs)
                 slot_ppr_hub_kernel<<<std::min<uint32_t>(sg_.n_hubs, sg_.sm_count * 8), 256, 0, s>>>(
-                    sg_, K_, wmask, hub_part_.as<float>(), nxt);
+                    sg_, W_, K_, occ, hub_part_.as<float>(), nxt);
             slot_ppr_teleport_kernel<<<K_, 256, 0, s>>>(K_, occ, d + kDevSlotSrc, dang_part_.as<float>(),
                                                         grid * 8, (double)alpha_, nxt);
-            count_launches(sg_.n_hubs ? 3 : 2);
         }
         G1_CUDA(cudaGetLastError());
-        it_ = it;
+    }
+    slot_it_advance_kernel<<<1, 1, 0, s>>>(d + kDevIt, n);
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
+}
+
+g1_status SlotEngine::step_graph(int i, uint32_t phase, cudaGraphExec_t* out) {
+    cudaGraphExec_t& gx = graphs_[i][phase];
+    if (!gx) {
+        if (!capture_) G1_CUDA(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        G1_CUDA(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal));
+        const g1_status st = enqueue_iterations(1u << i, phase, capture_);
+        const cudaError_t e = cudaStreamEndCapture(capture_, &graph);
+        if (st != G1_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture(slot step)");
+        const cudaError_t ei = cudaGraphInstantiate(&gx, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ei != cudaSuccess) {
+            gx = nullptr;
+            return fail_cuda(ei, "cudaGraphInstantiate(slot step)");
+        }
+    }
+    *out = gx;
+    return G1_OK;
+}
+
+g1_status SlotEngine::step(uint32_t iters, cudaStream_t s) {
+    if (!ready()) return fail(G1_ERR_INVALID, "slot engine not initialised");
+    uint32_t* d = slot_dev_.as<uint32_t>();
+    const Bits256 occ = occupied_bits();
+    if (!occ_dev_valid_ || std::memcmp(&occ, &occ_dev_, sizeof(occ)) != 0) {
+        slot_set_occ_kernel<<<1, 32, 0, s>>>(d + kDevOcc, occ);
+        count_launches(1);
+        G1_CUDA(cudaGetLastError());
+        occ_dev_ = occ;
+        occ_dev_valid_ = true;
+    }
+    // iters as a sum of powers of two, each a captured graph
+    const uint32_t per_iter = kind_ == kSlotPpr ? (sg_.n_hubs ? 3u : 2u) : 1u;
+    for (int i = kStepGraphs - 1; i >= 0; --i) {
+        const uint32_t n = 1u << i;
+        while (iters >= n) {
+            cudaGraphExec_t gx = nullptr;
+            G1_TRY(step_graph(i, it_ % kPhases, &gx));
+            G1_CUDA(cudaGraphLaunch(gx, s));
+            count_launches((uint64_t)n * per_iter + 1);
+            iters -= n;
+            it_ += n;
+        }
     }
     if (kind_ != kSlotPpr)
-        G1_CUDA(cudaMemcpyAsync(host_.as<uint32_t>() + kHostChw, chw + 8 * (it_ & 1), 8 * 4,
+        G1_CUDA(cudaMemcpyAsync(host_.as<uint32_t>() + kHostChw, chw_.as<uint32_t>() + 8 * (it_ & 1), 8 * 4,
                                 cudaMemcpyDeviceToHost, s));
     return G1_OK;
 }

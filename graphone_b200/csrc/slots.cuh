@@ -112,7 +112,15 @@ class SlotEngine {
    private:
     Frontier frontier(uint32_t it);
     Bits256 occupied_bits() const;
-    uint32_t word_mask() const;
+    // Enqueues n iterations on s, then the advance of the device iteration
+    // counter: the body of a captured step.  The buffers rotate with the
+    // iteration (period 6); `phase` is the completed iterations mod 6 when
+    // the step runs, and each iteration reads its number from the counter.
+    g1_status enqueue_iterations(uint32_t n, uint32_t phase, cudaStream_t s);
+    // The executable graph of 2^i iterations starting at rotation `phase`,
+    // captured on first use.
+    g1_status step_graph(int i, uint32_t phase, cudaGraphExec_t* out);
+    void drop_graphs();
 
     SlotGraph sg_;
     int kind_ = 0;
@@ -141,6 +149,15 @@ class SlotEngine {
     DevBuf ctr_;       // 4 x 4 words per iteration: list size, list valid, changed count
     DevBuf ptrs_;      // K output pointers for extract
     PinnedBuf host_;   // pinned mirror of chw and staging of small uploads
+    // Steps run as CUDA graphs of 2^i iterations (i < kStepGraphs) per
+    // rotation phase, captured once on a private stream and replayed on the
+    // caller's.
+    static constexpr int kStepGraphs = 8;
+    static constexpr uint32_t kPhases = 6;
+    cudaGraphExec_t graphs_[kStepGraphs][kPhases] = {};
+    cudaStream_t capture_ = nullptr;
+    Bits256 occ_dev_{};  // occupied slots as last written to the device
+    bool occ_dev_valid_ = false;
 };
 
 }  // namespace g1
