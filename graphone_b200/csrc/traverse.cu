@@ -87,19 +87,23 @@ __device__ __forceinline__ void relax(uint32_t du, uint32_t v, uint32_t w, uint3
     }
 }
 
-// Advance over the frontier: a thread per vertex for short adjacency lists,
-// the whole warp for lists of 32 or more edges (coalesced col/val reads).
-template <bool UNIT>
+// Advance over the frontier: TPV lanes per vertex for short adjacency lists
+// (TPV the power of two at or above the frontier's mean degree, so a small
+// frontier of low-degree vertices still gets about a thread per edge), the
+// whole warp for lists of 32 or more edges (coalesced col/val reads).
+template <bool UNIT, int TPV>
 __global__ void __launch_bounds__(256)
 tr_advance_kernel(const uint32_t* F, uint32_t nF, const uint32_t* rp, const uint32_t* col,
                   const uint32_t* val, uint32_t* dist, uint32_t* visited, uint32_t iter,
                   uint32_t* out, uint32_t* out_count, unsigned long long* deg_sum) {
+    constexpr uint32_t VPW = 32 / TPV;  // vertices per warp and round
     const uint32_t lane = lane_id();
+    const uint32_t sub = lane % TPV, grp = lane / TPV;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t rounds = (uint32_t)ceil_div(nF, (uint64_t)warps * 32);
+    const uint32_t rounds = (uint32_t)ceil_div(nF, (uint64_t)warps * VPW);
     for (uint32_t r = 0; r < rounds; ++r) {
-        const uint32_t i = (r * warps + wid) * 32 + lane;
+        const uint32_t i = (r * warps + wid) * VPW + grp;
         uint32_t u = 0, b = 0, e = 0;
         if (i < nF) {
             u = F[i];
@@ -108,7 +112,7 @@ tr_advance_kernel(const uint32_t* F, uint32_t nF, const uint32_t* rp, const uint
         }
         const uint32_t du = i < nF ? dist[u] : 0u;
         // long lists: cooperative, one list at a time
-        unsigned big = __ballot_sync(0xffffffffu, e - b >= 32);
+        unsigned big = __ballot_sync(0xffffffffu, sub == 0 && e - b >= 32);
         while (big) {
             const int src_lane = __ffs(big) - 1;
             big &= big - 1;
@@ -120,7 +124,7 @@ tr_advance_kernel(const uint32_t* F, uint32_t nF, const uint32_t* rp, const uint
                             rp, deg_sum);
         }
         if (e - b < 32) {
-            for (uint32_t k = b; k < e; ++k)
+            for (uint32_t k = b + sub; k < e; k += TPV)
                 relax<UNIT>(du, col[k], UNIT ? 1u : val[k], dist, visited, iter, out, out_count, rp,
                             deg_sum);
         }
@@ -244,12 +248,25 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
             1, std::min<uint64_t>(ceil_div(nF, 256), (uint64_t)g->sm_count * 8));
         if (push) {
             const Orientation& o = g->o[push_t];
-            if (o.max_deg <= 32) {  // short lists only: a thread per frontier vertex
+            if (o.max_deg <= 32) {  // short lists only: TPV lanes per frontier vertex
+                const uint64_t mean = ceil_div(std::max<uint64_t>(degF, 1), nF);
+                int tpv = 1;
+                while (tpv < 32 && (uint64_t)tpv < mean) tpv <<= 1;
+                const uint32_t gt = (uint32_t)std::max<uint64_t>(
+                    1, std::min<uint64_t>(ceil_div((uint64_t)nF * tpv, 256), (uint64_t)g->sm_count * 8));
                 count_launches(1);
-                tr_advance_kernel<UNIT><<<gf, 256, 0, s>>>(st.F[cur], nF, o.rp, o.col,
-                                                           static_cast<const uint32_t*>(o.val),
-                                                           st.dist, st.visited, it, st.F[cur ^ 1],
-                                                           st.cnt, deg_sum);
+#define G1_TR_ADV(T)                                                                                    \
+    tr_advance_kernel<UNIT, T><<<gt, 256, 0, s>>>(st.F[cur], nF, o.rp, o.col, static_cast<const uint32_t*>(o.val), \
+                                                  st.dist, st.visited, it, st.F[cur ^ 1], st.cnt, deg_sum)
+                switch (tpv) {
+                    case 1: G1_TR_ADV(1); break;
+                    case 2: G1_TR_ADV(2); break;
+                    case 4: G1_TR_ADV(4); break;
+                    case 8: G1_TR_ADV(8); break;
+                    case 16: G1_TR_ADV(16); break;
+                    default: G1_TR_ADV(32); break;
+                }
+#undef G1_TR_ADV
             } else {
                 tr_frontier_degrees_kernel<<<gf, 256, 0, s>>>(st.F[cur], nF, o.rp, st.deg);
                 size_t tb = scan_bytes;

@@ -211,11 +211,9 @@ def write_adj(g: CsrGraph, path: str, directed: bool) -> None:
     if not directed:
         keep = src < ci
         src, ci, v = src[keep], ci[keep], v[keep]
+    import pandas as pd  # vectorised text output (tens of millions of lines)
     with open(path, "w") as f:
         f.write("% generated\n")
-        if v.dtype.kind == "f":
-            for a, b, w in zip(src.tolist(), ci.tolist(), v.tolist()):
-                f.write(f"{a} {b} {w:g}\n")
-        else:
-            for a, b, w in zip(src.tolist(), ci.tolist(), v.tolist()):
-                f.write(f"{a} {b} {w}\n")
+    df = pd.DataFrame({"s": src, "d": ci, "w": v})
+    df.to_csv(path, mode="a", sep=" ", header=False, index=False,
+              float_format="%g" if v.dtype.kind == "f" else None, lineterminator="\n")

@@ -8,10 +8,13 @@
 // pass (functor::filter, when the functor has one).  Here the advance
 // appends emitted vertices compactly (warp-aggregated atomics) while
 // accumulating their out-degrees, so the output's worst-case size for the
-// next iteration is known without a separate reduction; adjacency lists of
-// 32 or more edges are walked by the whole warp (coalesced col/val reads),
-// shorter ones by one lane.  The filter step compacts the same way.  One
-// read-back per step gives the host the new frontier size.
+// next iteration is known without a separate reduction (with a filter step
+// the filter does that accumulation instead).  Adjacency lists of 32 or more
+// edges are walked by the whole warp (coalesced col/val reads); shorter ones
+// by TPV lanes, TPV the power of two at or above the frontier's mean degree,
+// so that a small frontier of low-degree vertices still gets about one
+// thread per edge.  The filter step compacts the same way.  One read-back
+// per step gives the host the new frontier size.
 
 #include <algorithm>
 #include <cstdint>
@@ -56,24 +59,31 @@ __device__ __forceinline__ void deg_flush(uint32_t* ctr, unsigned long long deg_
     if (g1::lane_id() == 0 && deg_acc) atomicAdd(reinterpret_cast<unsigned long long*>(ctr + 2), deg_acc);
 }
 
-template <class F, class V, class E, class W, class D>
+// DEG: accumulate the emitted vertices' out-degrees (not needed when a
+// filter step follows: it accumulates those of its own output).
+template <class F, bool DEG, class V, class E, class W, class D>
 __device__ __forceinline__ void visit(V src, V dst, E e, W w, D& ds, const E* rp, uint32_t* out,
                                       uint32_t* ctr, uint32_t cap, unsigned long long& deg_acc) {
-    if (F::advance(src, dst, e, w, ds)) append_capped(out, ctr, cap, dst, rp[dst + 1] - rp[dst], deg_acc);
+    if (F::advance(src, dst, e, w, ds))
+        append_capped(out, ctr, cap, dst, DEG ? rp[dst + 1] - rp[dst] : 0u, deg_acc);
 }
 
-template <class F, class V, class E, class W, class D, vstart_t VS>
+// TPV lanes per frontier vertex (1..32); vertices of 32 or more edges are
+// walked by the whole warp.
+template <class F, class V, class E, class W, class D, vstart_t VS, int TPV, bool DEG>
 __global__ void __launch_bounds__(256)
 advance_kernel(const E* rp, const V* col, const W* val, D ds, const V* in, uint32_t n_in,
                uint32_t* out, uint32_t* ctr, uint32_t cap) {
+    constexpr uint32_t VPW = 32 / TPV;  // vertices per warp and round
     const uint32_t lane = g1::lane_id();
+    const uint32_t sub = lane % TPV, grp = lane / TPV;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
     const uint32_t wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t rounds = (n_in + warps * 32 - 1) / (warps * 32);
+    const uint32_t rounds = (n_in + warps * VPW - 1) / (warps * VPW);
     D local = ds;  // functors may mutate their copy (reference: passed by value)
     unsigned long long deg_acc = 0;
     for (uint32_t r = 0; r < rounds; ++r) {
-        const uint32_t i = (r * warps + wid) * 32 + lane;
+        const uint32_t i = (r * warps + wid) * VPW + grp;
         V u = utils::invalid_vertex<VS, V>();
         E b = 0, e = 0;
         if (i < n_in) {
@@ -83,7 +93,7 @@ advance_kernel(const E* rp, const V* col, const W* val, D ds, const V* in, uint3
                 e = rp[u + 1];
             }
         }
-        unsigned big = __ballot_sync(0xffffffffu, e - b >= 32);
+        unsigned big = __ballot_sync(0xffffffffu, sub == 0 && e - b >= 32);
         while (big) {
             const int src = __ffs(big) - 1;
             big &= big - 1;
@@ -91,12 +101,21 @@ advance_kernel(const E* rp, const V* col, const W* val, D ds, const V* in, uint3
             const E bb = __shfl_sync(0xffffffffu, b, src);
             const E ee = __shfl_sync(0xffffffffu, e, src);
             for (E k = bb + lane; k < ee; k += 32)
-                visit<F>(uu, col[k], k, val[k], local, rp, out, ctr, cap, deg_acc);
+                visit<F, DEG>(uu, col[k], k, val[k], local, rp, out, ctr, cap, deg_acc);
         }
         if (e - b < 32)
-            for (E k = b; k < e; ++k) visit<F>(u, col[k], k, val[k], local, rp, out, ctr, cap, deg_acc);
+            for (E k = b + sub; k < e; k += TPV) visit<F, DEG>(u, col[k], k, val[k], local, rp, out, ctr, cap, deg_acc);
     }
     deg_flush(ctr, deg_acc);
+}
+
+// Lanes per vertex for a frontier of mean out-degree deg/n: the power of two
+// at or above it (1..32).
+inline int lanes_per_vertex(unsigned long long deg, uint32_t n) {
+    const unsigned long long mean = n ? (deg + n - 1) / n : 1;
+    int t = 1;
+    while (t < 32 && (unsigned long long)t < mean) t <<= 1;
+    return t;
 }
 
 // The filter reads the advance's output size from device memory (*n_dev),
@@ -197,10 +216,22 @@ public:
         const uint32_t cap = (uint32_t)std::min<unsigned long long>(next_degree_ + 1, 0xFFFFFFF0ull);
         f.reserve_output(cap);
         counters_.clear(stream_);
-        adv_detail::advance_kernel<functor_t, vertex_t, edge_t, weight_t, dstatus_t, VS>
-            <<<adv_detail::grid_for(n_in), 256, 0, stream_>>>(rp_, col_, val_, ds, f.input().data(),
-                                                              n_in, f.output().data(),
-                                                              counters_.dev, cap);
+        constexpr bool kDeg = !HasFilter::value;
+        const int tpv = adv_detail::lanes_per_vertex(next_degree_, n_in);
+        const unsigned grid = adv_detail::grid_for((uint64_t)n_in * tpv);
+#define G1_ADVANCE(T)                                                                                  \
+    adv_detail::advance_kernel<functor_t, vertex_t, edge_t, weight_t, dstatus_t, VS, T, kDeg>          \
+        <<<grid, 256, 0, stream_>>>(rp_, col_, val_, ds, f.input().data(), n_in, f.output().data(), \
+                                    counters_.dev, cap)
+        switch (tpv) {
+            case 1: G1_ADVANCE(1); break;
+            case 2: G1_ADVANCE(2); break;
+            case 4: G1_ADVANCE(4); break;
+            case 8: G1_ADVANCE(8); break;
+            case 16: G1_ADVANCE(16); break;
+            default: G1_ADVANCE(32); break;
+        }
+#undef G1_ADVANCE
         g1_count_user_launches(1);
         if constexpr (HasFilter::value) {
             // filter the advance output (size on the device) into the input

@@ -13,6 +13,7 @@
 #include "graphone_b200.h"
 #include "g1/common.cuh"
 #include "GraphOne/utils/log.hpp"
+#include "GraphOne/utils/pinned.h"
 
 namespace graph_one::engine {
 
@@ -65,13 +66,20 @@ inline int sm_count() {
 // Device counters and a host mirror for the one read-back per iteration:
 // [0] appended vertices, [1] overflow flag, [2..3] out-degree sum (u64);
 // [4..7] the same for a second compaction in the same step.  The mirror is
-// ordinary host memory: a pinned allocation costs milliseconds when an
-// engine is built, more than all the read-backs of a typical run.
+// a slot of the process's pinned block (ordinary memory if none is left).
 struct Counters {
     uint32_t* dev = nullptr;
-    uint32_t host[16] = {};
-    Counters() { check_g1(g1_mem_alloc(reinterpret_cast<void**>(&dev), 64), "counters"); }
-    ~Counters() { g1_mem_free(dev); }
+    uint32_t* host = nullptr;
+    uint32_t own_[16] = {};
+    Counters() {
+        check_g1(g1_mem_alloc(reinterpret_cast<void**>(&dev), 64), "counters");
+        host = ::graph_one::detail::PinnedSlots::get().take();
+        if (!host) host = own_;
+    }
+    ~Counters() {
+        g1_mem_free(dev);
+        if (host != own_) ::graph_one::detail::PinnedSlots::get().give(host);
+    }
     Counters(const Counters&) = delete;
     Counters& operator=(const Counters&) = delete;
     void clear(cudaStream_t s) { check_cuda(cudaMemsetAsync(dev, 0, 32, s), "clear counters"); }

@@ -22,6 +22,7 @@
 #include "GraphOne/macros.h"
 #include "GraphOne/type.hpp"
 #include "GraphOne/utils/log.hpp"
+#include "GraphOne/utils/pinned.h"
 
 namespace graph_one {
 
@@ -168,7 +169,11 @@ Graph<arch, views, v_start, empty_t, vertex_t, edge_t, weight_t> build(
     // The application's own CUDA runtime (its kernels live in its binary)
     // starts here, with the graph, rather than inside the first Run; the
     // library's runtime starts with g1_graph_create below.
-    if constexpr (arch == arch_t::cuda) cudaFree(nullptr);
+    // The engines' pinned read-back block is made here too, for the same reason.
+    if constexpr (arch == arch_t::cuda) {
+        cudaFree(nullptr);
+        (void)::graph_one::detail::PinnedSlots::get();
+    }
     std::vector<edge_t> rp;
     std::vector<vertex_t> ci;
     std::vector<weight_t> val;

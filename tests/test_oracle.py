@@ -141,3 +141,21 @@ def test_oracle_ppr_mass_is_conserved():
 def test_golden_fixtures_present():
     names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
     assert set(GRAPHS) <= set(names)
+
+
+@pytest.mark.parametrize("float_values", [False, True])
+def test_write_adj_lists_each_undirected_edge_once(tmp_path, float_values):
+    """The .adj writer (GraphOne's `src dst w` edge list, read by the unchanged
+    apps) lists each undirected edge once, u < v, with its weight."""
+    g = gen.rmat(9, 16, True, (1, 64), float_values=float_values)
+    path = tmp_path / "g.adj"
+    gen.write_adj(g, str(path), False)
+    lines = path.read_text().splitlines()
+    assert lines[0].startswith("%")
+    rows = np.array([l.split() for l in lines[1:]], dtype=np.float64)
+    rp, ci, v = g.np("n")
+    src = np.repeat(np.arange(g.n), np.diff(rp.astype(np.int64)))
+    keep = src < ci
+    assert rows.shape == (int(keep.sum()), 3)
+    assert np.array_equal(rows[:, 0], src[keep]) and np.array_equal(rows[:, 1], ci[keep])
+    assert np.array_equal(rows[:, 2].astype(v.dtype), v[keep])
