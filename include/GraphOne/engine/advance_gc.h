@@ -70,11 +70,14 @@ __device__ __forceinline__ void visit(V src, V dst, E e, W w, D& ds, const E* rp
 
 // TPV lanes per frontier vertex (1..32); vertices of 32 or more edges are
 // walked by the whole warp.
+// zero_next: the other counter set, zeroed for the next step (the host has
+// read it back already).
 template <class F, class V, class E, class W, class D, vstart_t VS, int TPV, bool DEG>
 __global__ void __launch_bounds__(256)
 advance_kernel(const E* rp, const V* col, const W* val, D ds, const V* in, uint32_t n_in,
-               uint32_t* out, uint32_t* ctr, uint32_t cap) {
+               uint32_t* out, uint32_t* ctr, uint32_t cap, uint32_t* zero_next) {
     constexpr uint32_t VPW = 32 / TPV;  // vertices per warp and round
+    if (blockIdx.x == 0 && threadIdx.x < 8) zero_next[threadIdx.x] = 0u;
     const uint32_t lane = g1::lane_id();
     const uint32_t sub = lane % TPV, grp = lane / TPV;
     const uint32_t warps = gridDim.x * (blockDim.x >> 5);
@@ -211,18 +214,23 @@ public:
             counters_.read(stream_);
             next_degree_ = counters_.degree_sum();
             degree_known_ = true;
+            // both counter sets start at zero; from here on each step's
+            // advance zeroes the set of the step after it
+            detail::check_cuda(cudaMemsetAsync(counters_.dev, 0, 64, stream_), "clear counters");
+            set_ = 0;
         }
         // the advance emits at most one vertex per out-edge of the input
         const uint32_t cap = (uint32_t)std::min<unsigned long long>(next_degree_ + 1, 0xFFFFFFF0ull);
         f.reserve_output(cap);
-        counters_.clear(stream_);
+        uint32_t* ctr = counters_.dev + 8 * set_;
+        uint32_t* ctr_next = counters_.dev + 8 * (set_ ^ 1);
         constexpr bool kDeg = !HasFilter::value;
         const int tpv = adv_detail::lanes_per_vertex(next_degree_, n_in);
         const unsigned grid = adv_detail::grid_for((uint64_t)n_in * tpv);
 #define G1_ADVANCE(T)                                                                                  \
     adv_detail::advance_kernel<functor_t, vertex_t, edge_t, weight_t, dstatus_t, VS, T, kDeg>          \
         <<<grid, 256, 0, stream_>>>(rp_, col_, val_, ds, f.input().data(), n_in, f.output().data(), \
-                                    counters_.dev, cap)
+                                    ctr, cap, ctr_next)
         switch (tpv) {
             case 1: G1_ADVANCE(1); break;
             case 2: G1_ADVANCE(2); break;
@@ -239,10 +247,9 @@ public:
             const uint32_t fcap = (uint32_t)std::min<uint64_t>(f.input().size(), 0xFFFFFFF0ull);
             adv_detail::filter_kernel<functor_t, vertex_t, edge_t, dstatus_t, VS>
                 <<<adv_detail::grid_for(std::min<uint64_t>(cap, (uint64_t)detail::sm_count() * 2048)),
-                   256, 0, stream_>>>(rp_, ds, f.output().data(), counters_.dev, f.input().data(),
-                                      counters_.dev + 4, fcap);
+                   256, 0, stream_>>>(rp_, ds, f.output().data(), ctr, f.input().data(), ctr + 4, fcap);
             g1_count_user_launches(1);
-            counters_.read(stream_);
+            counters_.read_set(stream_, set_);
             if (counters_.overflow() || counters_.host[5]) LOG_ERROR("advance: frontier overflow");
             // GraphOne's Filter swaps in/out and fills the new output; the
             // Run loop's AfterEngine swaps again (engine/advance_gc.h:224-240)
@@ -252,11 +259,12 @@ public:
             next_degree_ = (unsigned long long)counters_.host[6] |
                            ((unsigned long long)counters_.host[7] << 32);
         } else {
-            counters_.read(stream_);
+            counters_.read_set(stream_, set_);
             if (counters_.overflow()) LOG_ERROR("advance: output frontier overflow");
             f.reset_output(counters_.count());
             next_degree_ = counters_.degree_sum();
         }
+        set_ ^= 1;
     }
 
 private:
@@ -266,6 +274,7 @@ private:
     const weight_t* val_ = nullptr;
     detail::Counters counters_;
     bool degree_known_ = false;
+    int set_ = 0;  // counter set of this step (dev + 8 * set_)
     bool check_cuda_alloc_ = false;
     unsigned long long next_degree_ = 0;
 };

@@ -83,8 +83,10 @@ struct Counters {
     Counters(const Counters&) = delete;
     Counters& operator=(const Counters&) = delete;
     void clear(cudaStream_t s) { check_cuda(cudaMemsetAsync(dev, 0, 32, s), "clear counters"); }
-    void read(cudaStream_t s) {
-        check_cuda(cudaMemcpyAsync(host, dev, 32, cudaMemcpyDeviceToHost, s), "read counters");
+    void read(cudaStream_t s) { read_set(s, 0); }
+    // The 8 words of set `set` (0 or 1: dev + 8 * set) into host[0..7].
+    void read_set(cudaStream_t s, int set) {
+        check_cuda(cudaMemcpyAsync(host, dev + 8 * set, 32, cudaMemcpyDeviceToHost, s), "read counters");
         check_cuda(cudaStreamSynchronize(s), "engine step");
     }
     uint32_t count() const { return host[0]; }
