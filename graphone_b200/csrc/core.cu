@@ -72,16 +72,118 @@ g1_status fail_cuda(cudaError_t e, const char* what) {
     return fail(e == cudaErrorMemoryAllocation ? G1_ERR_OOM : G1_ERR_DEVICE, m);
 }
 
+namespace {
+
+struct BlockCache {
+    std::mutex mu;
+    std::multimap<size_t, void*> ready;             // idle: reusable now
+    std::vector<std::pair<size_t, void*>> pending;  // released since the last device sync
+    size_t cached = 0;                              // bytes in both
+    size_t cap = 0;                                 // 0 until the device's size is known
+};
+constexpr int kCacheDevices = 64;
+BlockCache g_cache[kCacheDevices];
+
+// Frees every cached block of `dev` (current device); the caller holds c.mu.
+void cache_drain_locked(BlockCache& c) {
+    if (!c.pending.empty()) cudaDeviceSynchronize();
+    for (auto& kv : c.ready) cudaFree(kv.second);
+    for (auto& pr : c.pending) cudaFree(pr.second);
+    c.ready.clear();
+    c.pending.clear();
+    c.cached = 0;
+}
+
+// The smallest ready block of at least `want` bytes and at most about twice
+// that (1 MiB of slack for small requests); the caller holds c.mu.
+bool cache_take_locked(BlockCache& c, size_t want, void** p, size_t* got) {
+    auto it = c.ready.lower_bound(want);
+    if (it == c.ready.end() || it->first > std::max(2 * want, want + (size_t(1) << 20))) return false;
+    *p = it->second;
+    *got = it->first;
+    c.cached -= it->first;
+    c.ready.erase(it);
+    return true;
+}
+
+}  // namespace
+
+void dev_block_release(int dev, void* p, size_t bytes) {
+    if (!p) return;
+    if (dev < 0 || dev >= kCacheDevices) {
+        cudaFree(p);
+        return;
+    }
+    BlockCache& c = g_cache[dev];
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (c.cap == 0 || c.cached + bytes > c.cap) {
+        cudaFree(p);  // over the cap: back to the driver (its implicit sync as before)
+        return;
+    }
+    c.pending.emplace_back(bytes, p);
+    c.cached += bytes;
+}
+
+size_t dev_block_cached(int dev) {
+    if (dev < 0 || dev >= kCacheDevices) return 0;
+    BlockCache& c = g_cache[dev];
+    std::lock_guard<std::mutex> lk(c.mu);
+    return c.cached;
+}
+
+g1_status dev_block_get(size_t want, void** p, size_t* got, int* dev_out) {
+    int dev = 0;
+    G1_CUDA(cudaGetDevice(&dev));
+    *dev_out = dev;
+    const size_t b = (want + 255) & ~size_t(255);
+    if (dev < kCacheDevices) {
+        BlockCache& c = g_cache[dev];
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (c.cap == 0) {
+            size_t fr = 0, total = 0;
+            if (cudaMemGetInfo(&fr, &total) == cudaSuccess) c.cap = total / 4;
+            else cudaGetLastError();
+        }
+        if (cache_take_locked(c, b, p, got)) return G1_OK;
+        if (!c.pending.empty()) {
+            // released blocks become reusable once the device has drained
+            G1_CUDA(cudaDeviceSynchronize());
+            for (auto& pr : c.pending) c.ready.emplace(pr.first, pr.second);
+            c.pending.clear();
+            if (cache_take_locked(c, b, p, got)) return G1_OK;
+        }
+        cudaError_t e = cudaMalloc(p, b);
+        if (e == cudaErrorMemoryAllocation && c.cached > 0) {
+            cudaGetLastError();
+            cache_drain_locked(c);
+            e = cudaMalloc(p, b);
+        }
+        if (e != cudaSuccess) {
+            *p = nullptr;
+            return fail_cuda(e, "cudaMalloc(workspace)");
+        }
+        *got = b;
+        return G1_OK;
+    }
+    cudaError_t e = cudaMalloc(p, b);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail_cuda(e, "cudaMalloc(workspace)");
+    }
+    *got = b;
+    return G1_OK;
+}
+
 g1_status DevBuf::ensure(size_t want) {
     if (want <= bytes) return G1_OK;
     release();
-    size_t b = (want + 255) & ~size_t(255);
-    cudaError_t e = cudaMalloc(&p, b);
-    if (e != cudaSuccess) {
-        p = nullptr;
-        return fail_cuda(e, "cudaMalloc(workspace)");
-    }
-    bytes = b;
+    void* q = nullptr;
+    size_t got = 0;
+    int d = 0;
+    G1_TRY(dev_block_get(want, &q, &got, &d));
+    p = q;
+    bytes = got;
+    dev = d;
     return G1_OK;
 }
 

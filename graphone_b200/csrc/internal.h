@@ -32,15 +32,27 @@ g1_status fail_cuda(cudaError_t e, const char* what);
     } while (0)
 
 // Owning device buffer; capacity grows, never shrinks.
+// Device memory of the library.  Freed blocks go to a per-device cache and
+// are reused by later requests of about their size (a new graph of the same
+// shape allocates and frees nothing); a block is reused only after a device
+// synchronisation that follows its release, so no queued kernel can still
+// touch it.  The cache holds at most a quarter of the device's memory and
+// is emptied when an allocation fails.
+void dev_block_release(int dev, void* p, size_t bytes);
+g1_status dev_block_get(size_t want, void** p, size_t* got, int* dev);
+// Bytes the cache holds on `dev` (reusable without the driver).
+size_t dev_block_cached(int dev);
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    int dev = 0;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_block_release(dev, p, bytes);
         p = nullptr;
         bytes = 0;
     }

@@ -183,14 +183,26 @@ bool others_hold_memory(g1_server* S, const Exec* self) {
 // Allocates the executor's engine: the largest slot count (halving from
 // max_batch down to 32) whose state fits the free device memory minus the
 // reserve and the server's limit.
+// Free device memory on the current device, counting the library's cache of
+// released blocks (reusable, or freed when an allocation needs the room).
+size_t device_free_bytes() {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return free_b;
+    }
+    return free_b + dev_block_cached(dev);
+}
+
 bool allocate(g1_server* S, Exec& E) {
     for (uint32_t K = (S->max_batch + 31) / 32 * 32;;) {
         const size_t need = SlotEngine::bytes(E.sg, E.kind, K);
-        size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
-            cudaGetLastError();
-            free_b = 0;
-        }
+        const size_t free_b = device_free_bytes();
         const bool fits = need + S->reserve <= free_b && (!S->limit || S->dev_bytes + need <= S->limit);
         if (!fits && release_one_idle(S, &E)) continue;
         if (fits) {
@@ -281,15 +293,12 @@ bool service_nearfar(g1_server* S, Exec& E, bool stopping) {
     if (stopping || E.pending.empty()) return progress;
     const size_t need = nearfar_words(E.g->n) * 4;
     if (!E.nf_store.p) {
-        size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
-            cudaGetLastError();
-            free_b = 0;
-        }
+        size_t free_b = device_free_bytes();
         bool fits = need + S->reserve <= free_b && (!S->limit || S->dev_bytes + need <= S->limit);
-        while (!fits && release_one_idle(S, &E))
-            fits = (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) && need + S->reserve <= free_b &&
-                   (!S->limit || S->dev_bytes + need <= S->limit);
+        while (!fits && release_one_idle(S, &E)) {
+            free_b = device_free_bytes();
+            fits = need + S->reserve <= free_b && (!S->limit || S->dev_bytes + need <= S->limit);
+        }
         if (!fits || E.nf_store.ensure(need) != G1_OK || E.nf_host.ensure(nearfar_ctl_bytes() + 64) != G1_OK) {
             cudaGetLastError();
             E.nf_store.release();
