@@ -133,7 +133,12 @@ __device__ __forceinline__ uint32_t agg_slot(uint32_t* ctr) {
     return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
 }
 
-template <bool UNIT>
+// TPV lanes per near-queue item (1..32, the power of two at or above the
+// graph's mean degree): a step's edges then run about one per thread, where
+// one lane per item would chain its items' edges (each an atomicMin, a stamp
+// and an append) one after another.  Lists of 32 or more edges are pushed by
+// the whole warp.
+template <bool UNIT, int TPV>
 __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
     const uint32_t nb = gridDim.x;
     const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -182,10 +187,13 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
                 }
             };
             const uint32_t lane = lane_id();
+            constexpr uint32_t VPW = 32 / TPV;  // items per warp and round
+            const uint32_t sub = lane % TPV, grp = lane / TPV;
+            const uint32_t gw = gt >> 5, nw = gs >> 5;
             // warp-uniform rounds: lists of 32 or more edges are pushed by the
-            // whole warp, shorter ones by their own lane
-            for (uint32_t base = gt - lane; base < qn; base += gs) {
-                const uint32_t i = base + lane;
+            // whole warp, shorter ones by the item's TPV lanes
+            for (uint32_t base = gw * VPW; base < qn; base += nw * VPW) {
+                const uint32_t i = base + grp;
                 uint32_t du = 0, b = 0, e1 = 0;
                 if (i < qn) {
                     const uint32_t u = in[i];
@@ -193,7 +201,7 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
                     b = a.rp[u];
                     e1 = a.rp[u + 1];
                 }
-                unsigned big = __ballot_sync(0xffffffffu, e1 - b >= 32);
+                unsigned big = __ballot_sync(0xffffffffu, sub == 0 && e1 - b >= 32);
                 while (big) {
                     const int src = __ffs(big) - 1;
                     big &= big - 1;
@@ -203,7 +211,7 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
                     for (uint32_t e = bb + lane; e < ee; e += 32) relax(dd, e);
                 }
                 if (e1 - b < 32)
-                    for (uint32_t e = b; e < e1; ++e) relax(du, e);
+                    for (uint32_t e = b + sub; e < e1; e += TPV) relax(du, e);
             }
             par ^= 1;
         } else if (step == 1) {
@@ -350,7 +358,20 @@ g1_status nearfar_launch(const g1_graph* g, uint32_t src, bool unit, uint32_t de
     // every block of a cooperative launch is resident, so the grid barrier
     // only ever waits for running blocks; one 1024-thread block per SM keeps
     // the barrier's arrivals few
-    const void* fn = unit ? (const void*)nf_kernel<true> : (const void*)nf_kernel<false>;
+    int tpv = 1;
+    const uint64_t mean = g->n ? ceil_div(g->m, g->n) : 1;
+    while (tpv < 32 && (uint64_t)tpv < mean) tpv <<= 1;
+    const void* fn = nullptr;
+#define G1_NF_FN(T) fn = unit ? (const void*)nf_kernel<true, T> : (const void*)nf_kernel<false, T>
+    switch (tpv) {
+        case 1: G1_NF_FN(1); break;
+        case 2: G1_NF_FN(2); break;
+        case 4: G1_NF_FN(4); break;
+        case 8: G1_NF_FN(8); break;
+        case 16: G1_NF_FN(16); break;
+        default: G1_NF_FN(32); break;
+    }
+#undef G1_NF_FN
     int per_sm = 0;
     G1_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 1024, 0));
     if (per_sm < 1) return fail(G1_ERR_UNSUPPORTED, "near-far engine: kernel does not fit an SM");
