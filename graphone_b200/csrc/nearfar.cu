@@ -80,7 +80,25 @@ __device__ __forceinline__ void atom_add_release(uint32_t* p, uint32_t v) {
 // arrival (after bar.sync), and the other blocks' writes acquired through
 // the generation word.  false if the wait ran out (the kernel then returns:
 // the host reports G1_ERR_TIMEOUT).
-__device__ bool nf_barrier(NfCtl* c, uint32_t nblocks) {
+// The control words a step reads, copied into shared memory by thread 0 of
+// each block after the barrier (one read per block instead of one per warp
+// of the same few words).
+struct NfStepCtl {
+    uint32_t qn, thresh, kind, fn, minfar, err;
+};
+
+__device__ __forceinline__ void nf_read_ctl(const NfCtl* c, uint32_t st, uint32_t fp, NfStepCtl* sc) {
+    const uint32_t cur = st % 3;
+    sc->qn = ld_vol(&c->qn[cur]);
+    sc->thresh = ld_vol(&c->thresh[cur]);
+    sc->kind = ld_vol(&c->kind[cur]);
+    sc->fn = ld_vol(&c->fn[fp]);
+    sc->minfar = ld_vol(&c->minfar[cur]);
+    sc->err = ld_vol(&c->err);
+}
+
+// Also loads the control words of step `st_next` (far pile `fp`) into sc.
+__device__ bool nf_barrier(NfCtl* c, uint32_t nblocks, uint32_t st_next, uint32_t fp, NfStepCtl* sc) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const uint32_t g0 = ld_acquire(&c->bar_gen);
@@ -96,9 +114,10 @@ __device__ bool nf_barrier(NfCtl* c, uint32_t nblocks) {
                 }
             }
         }
+        nf_read_ctl(c, st_next, fp, sc);
     }
     __syncthreads();
-    return (ld_vol(&c->err) & 1u) == 0u;
+    return (sc->err & 1u) == 0u;
 }
 
 // src is an internal vertex id, or a caller id mapped through perm.
@@ -147,12 +166,15 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
     uint32_t par = 0, fp = 0;
     uint32_t gen = 1;     // near-queue generation (stamp)
     uint32_t bucket = 1;  // far-pile bucket (fstamp)
+    __shared__ NfStepCtl sc;
+    if (threadIdx.x == 0) nf_read_ctl(c, 0, 0, &sc);
+    __syncthreads();
     for (uint32_t st = 0;; ++st) {
         const uint32_t cur = st % 3, nxt = (st + 1) % 3, old = (st + 2) % 3;
-        const uint32_t qn = ld_vol(&c->qn[cur]);
-        const uint32_t T = ld_vol(&c->thresh[cur]);
-        const bool move = ld_vol(&c->kind[cur]) != 0u;
-        const uint32_t fn = ld_vol(&c->fn[fp]);
+        const uint32_t qn = sc.qn;
+        const uint32_t T = sc.thresh;
+        const bool move = sc.kind != 0u;
+        const uint32_t fn = sc.fn;
         // 0 = relax round, 1 = smallest far distance, 2 = threshold move
         const int step = move ? 2 : qn > 0 ? 0 : (fn == 0 ? -1 : (UNIT ? 2 : 1));
         if (step < 0) return;
@@ -231,7 +253,7 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
             if (UNIT) {
                 tn = T + 1u;
             } else {
-                const uint32_t mf = ld_vol(&c->minfar[cur]);
+                const uint32_t mf = sc.minfar;
                 const uint64_t base = (mf != kU32Max && mf > T) ? mf : T;
                 const uint64_t t64 = base + a.delta;
                 tn = t64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)t64;
@@ -255,7 +277,7 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
             par ^= 1;
             fp ^= 1;
         }
-        if (!nf_barrier(c, nb)) return;
+        if (!nf_barrier(c, nb, st + 1, fp, &sc)) return;
     }
 }
 
