@@ -117,7 +117,7 @@ void dev_block_release(int dev, void* p, size_t bytes) {
     BlockCache& c = g_cache[dev];
     std::lock_guard<std::mutex> lk(c.mu);
     if (c.cap == 0 || c.cached + bytes > c.cap) {
-        cudaFree(p);  // over the cap: back to the driver (its implicit sync as before)
+        cudaFree(p);  // over the cap: back to the driver (cudaFree synchronises the device)
         return;
     }
     c.pending.emplace_back(bytes, p);
