@@ -61,6 +61,7 @@ def _declare(L):
     L.g1_mem_alloc.argtypes = [C.POINTER(P), C.c_size_t]
     L.g1_mem_free.argtypes = [P]
     L.g1_mem_copy.argtypes = [P, P, C.c_size_t, C.c_int, P]
+    L.g1_release_cached_memory.argtypes = [C.POINTER(C.c_size_t)]
     L.g1_mem_fill_u32.argtypes = [P, C.c_uint32, C.c_size_t, P]
     L.g1_stream_sync.argtypes = [P]
     L.g1_kernel_launches.restype = C.c_uint64
@@ -112,7 +113,7 @@ def lib():
 # Every symbol include/graphone_b200.h declares (checked by the CPU tests).
 EXPORTS = (
     "g1_status_string", "g1_last_error", "g1_version", "g1_mem_alloc", "g1_mem_free",
-    "g1_mem_copy", "g1_mem_fill_u32", "g1_stream_sync", "g1_kernel_launches",
+    "g1_mem_copy", "g1_release_cached_memory", "g1_mem_fill_u32", "g1_stream_sync", "g1_kernel_launches",
     "g1_count_user_launches",
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
@@ -146,6 +147,15 @@ def _stream(stream) -> int:
 
 def kernel_launches() -> int:
     return int(lib().g1_kernel_launches())
+
+
+def release_cached_memory() -> int:
+    """Returns the device blocks the library keeps for reuse (from closed
+    graphs, plans and engines) on the current device to the driver; the
+    number of bytes released."""
+    b = C.c_size_t()
+    check(lib().g1_release_cached_memory(C.byref(b)))
+    return b.value
 
 
 def profile_begin() -> None:

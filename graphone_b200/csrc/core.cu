@@ -124,6 +124,15 @@ void dev_block_release(int dev, void* p, size_t bytes) {
     c.cached += bytes;
 }
 
+size_t dev_block_drain(int dev) {
+    if (dev < 0 || dev >= kCacheDevices) return 0;
+    BlockCache& c = g_cache[dev];
+    std::lock_guard<std::mutex> lk(c.mu);
+    const size_t b = c.cached;
+    cache_drain_locked(c);
+    return b;
+}
+
 size_t dev_block_cached(int dev) {
     if (dev < 0 || dev >= kCacheDevices) return 0;
     BlockCache& c = g_cache[dev];
@@ -817,6 +826,15 @@ g1_status g1_mem_alloc(void** ptr, size_t bytes) {
 
 g1_status g1_mem_free(void* ptr) {
     if (ptr) G1_CUDA(cudaFree(ptr));
+    return G1_OK;
+}
+
+g1_status g1_release_cached_memory(size_t* released_bytes) {
+    int dev = 0;
+    G1_CUDA(cudaGetDevice(&dev));
+    const size_t b = dev_block_drain(dev);
+    if (released_bytes) *released_bytes = b;
+    G1_CUDA(cudaGetLastError());
     return G1_OK;
 }
 

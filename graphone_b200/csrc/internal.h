@@ -42,6 +42,8 @@ void dev_block_release(int dev, void* p, size_t bytes);
 g1_status dev_block_get(size_t want, void** p, size_t* got, int* dev);
 // Bytes the cache holds on `dev` (reusable without the driver).
 size_t dev_block_cached(int dev);
+// Frees the cached blocks of `dev` (the current device); returns their bytes.
+size_t dev_block_drain(int dev);
 
 struct DevBuf {
     void* p = nullptr;

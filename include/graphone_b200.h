@@ -88,6 +88,12 @@ g1_status g1_mem_alloc(void** ptr, size_t bytes);
 g1_status g1_mem_free(void* ptr);
 /* kind: 0 = host->device, 1 = device->host, 2 = device->device. */
 g1_status g1_mem_copy(void* dst, const void* src, size_t bytes, int kind, void* stream);
+/* The library keeps the device blocks of closed graphs, plans and engines
+ * (up to a quarter of the device's memory) for reuse by later ones of about
+ * the same size.  This returns the current device's kept blocks to the
+ * driver, after waiting for the device; *released_bytes (may be NULL) gets
+ * their total.  No GraphOne counterpart (GraphOne frees at once). */
+g1_status g1_release_cached_memory(size_t* released_bytes);
 g1_status g1_mem_fill_u32(void* dst, uint32_t value, size_t count, void* stream);
 g1_status g1_stream_sync(void* stream);
 

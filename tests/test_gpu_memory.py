@@ -32,3 +32,9 @@ def test_repeated_graphs_reuse_memory_and_stay_exact(cuda):
         free.append(torch.cuda.mem_get_info()[0])
     # after the first cycle the same blocks serve every later one
     assert max(free[1:]) - min(free[1:]) < 64 << 20, free
+    # and the kept blocks go back to the driver on request
+    kept = g1.release_cached_memory()
+    torch.cuda.synchronize()
+    assert kept > 0
+    assert torch.cuda.mem_get_info()[0] >= free[-1] + kept - (64 << 20)
+    assert g1.release_cached_memory() == 0
