@@ -248,6 +248,13 @@ __device__ __forceinline__ void ldg_v8(const void* ptr, uint4& lo, uint4& hi) {
         : "=r"(lo.x), "=r"(lo.y), "=r"(lo.z), "=r"(lo.w), "=r"(hi.x), "=r"(hi.y), "=r"(hi.z), "=r"(hi.w)
         : "l"(ptr));
 }
+// The same for data read once (a stream): the lines are not kept in L1, so
+// L1 stays with the data that is read again.
+__device__ __forceinline__ void ldg_v8_stream(const void* ptr, uint4& lo, uint4& hi) {
+    asm("ld.global.nc.L1::no_allocate.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+        : "=r"(lo.x), "=r"(lo.y), "=r"(lo.z), "=r"(lo.w), "=r"(hi.x), "=r"(hi.y), "=r"(hi.z), "=r"(hi.w)
+        : "l"(ptr));
+}
 // 4-byte read-only load with an L2 policy.
 __device__ __forceinline__ uint32_t ldg_u32_policy(const void* ptr, uint64_t pol) {
     uint32_t r;

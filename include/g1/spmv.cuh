@@ -1092,9 +1092,10 @@ __device__ __forceinline__ NnzIn nnz_load(const NnzArgs<SR>& a, uint32_t tile, u
         in.v1 = ldg_v4_policy(a.val + jl + 4, pol_stream);
     } else {
         // a lane's 8 columns and values are 32 aligned bytes each (col and
-        // val are 32-byte aligned; the host checks)
-        ldg_v8(a.col + jl, in.c0, in.c1);
-        ldg_v8(a.val + jl, in.v0, in.v1);
+        // val are 32-byte aligned; the host checks); read once, so they do
+        // not displace the x lines the gathers reuse from L1
+        ldg_v8_stream(a.col + jl, in.c0, in.c1);
+        ldg_v8_stream(a.val + jl, in.v0, in.v1);
     }
     in.sw = __ldg(a.plan.sbits + (j0 >> 5) + (lane >> 2));
     in.endw = __ldg(a.plan.sbits + ((j0 + kNnzTile) >> 5));
