@@ -431,12 +431,9 @@ g1_status rebuild_csr(g1_graph* g, const Orientation& src, Orientation& dst, boo
 
 // Moves the arrays of `fresh` into `o` (old arrays are freed).
 void adopt(Orientation& o, Orientation& fresh) {
-    std::swap(o.b_rp.p, fresh.b_rp.p);
-    std::swap(o.b_rp.bytes, fresh.b_rp.bytes);
-    std::swap(o.b_col.p, fresh.b_col.p);
-    std::swap(o.b_col.bytes, fresh.b_col.bytes);
-    std::swap(o.b_val.p, fresh.b_val.p);
-    std::swap(o.b_val.bytes, fresh.b_val.bytes);
+    o.b_rp.swap(fresh.b_rp);
+    o.b_col.swap(fresh.b_col);
+    o.b_val.swap(fresh.b_val);
     o.rp = o.b_rp.as<uint32_t>();
     o.col = o.b_col.as<uint32_t>();
     o.val = o.b_val.p;

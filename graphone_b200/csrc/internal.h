@@ -59,6 +59,12 @@ struct DevBuf {
         bytes = 0;
     }
     g1_status ensure(size_t want);
+    // Exchanges the blocks (and their devices) of two buffers.
+    void swap(DevBuf& o) {
+        std::swap(p, o.p);
+        std::swap(bytes, o.bytes);
+        std::swap(dev, o.dev);
+    }
     template <class T>
     T* as() const { return static_cast<T*>(p); }
 };
