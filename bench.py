@@ -531,6 +531,9 @@ def run_ours(args):
             "schedule": sched_note,
             "layout": ("resident graph stored in decreasing out-degree order (G1_GRAPH_RELABEL); "
                        "results in caller order") if not args.no_relabel else "caller order",
+            "e2e_step": ("new graph from the pinned host CSR (caller order; its device blocks come "
+                         "from the library's cache of released blocks), plan, out-weights, PageRank, "
+                         "ranks to pinned host memory, graph closed"),
         },
         "gpu_launches": int(launches),
         "clocks": clocks,
