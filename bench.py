@@ -24,7 +24,7 @@ runs, and the ranks are read back to the host (g1_pagerank into host memory).
 SpMV + apply/construct kernel of the schedule in use, by default
 spmv_nnz_kernel) per launch over its CUDA-event duration, against the
 measured HBM copy bandwidth; ``traffic`` is the DRAM bytes per launch ncu
-measured for that kernel (profiles/pagerank_rmat22_traffic.json).
+measured for that kernel (profiles/spmv_nnz_pagerank_rmat22_traffic.md).
 ``queries``: plain and batched SSSP/BFS (RMAT-14, RMAT-20 k=256, 4096^2
 grid); ``serving``: the serving loop over 8 resident graphs vs plain
 per-request execution.
@@ -423,6 +423,27 @@ def kernel_name(variant: int) -> str:
     return f"{base}<PlusTimesF32, PrEpilogue> (merge variant {variant})"
 
 
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "spmv_nnz_pagerank_rmat22_traffic.md")
+
+
+def measured_traffic(variant: int, path: str = TRAFFIC_FILE):
+    """DRAM bytes per launch that ncu measured for the RMAT-22 PageRank
+    kernel of merge variant `variant`, or None when no capture of that
+    variant is recorded (the summary's `variant:` and
+    `dram_bytes_per_launch:` lines)."""
+    try:
+        with open(path) as f:
+            text = f.read()
+    except OSError:
+        return None
+    import re
+    v = re.search(r"^variant:\s*(-?\d+)\s*$", text, re.M)
+    b = re.search(r"^dram_bytes_per_launch:\s*(\d+)\s*$", text, re.M)
+    if not v or not b or int(v.group(1)) != variant:
+        return None
+    return int(b.group(1))
+
+
 def run_ours(args):
     import torch
     import graphone_b200 as g1
@@ -544,16 +565,7 @@ def run_ours(args):
     if spmv_launches:
         avg_ms = spmv_ms / spmv_launches
         achieved = spmv_bytes(n, m) / (avg_ms / 1e3) / 1e9
-        traffic = None
-        tfile = os.path.join(ROOT, "profiles", "pagerank_rmat22_traffic.json")
-        if os.path.exists(tfile) and args.scale == 22:
-            try:
-                tj = json.load(open(tfile))
-                # the capture is of the default variant's kernel
-                if variant == g1.DEFAULT_MERGE_VARIANT or f"variant {variant}," in tj.get("kernel", ""):
-                    traffic = tj.get("dram_bytes_per_launch")
-            except Exception:
-                traffic = None
+        traffic = measured_traffic(variant) if args.scale == 22 else None
         result["roofline"] = {
             "bound": "hbm", "kernel": kernel_name(variant),
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
