@@ -848,6 +848,7 @@ g1_status g1_mem_copy(void* dst, const void* src, size_t bytes, int kind, void* 
 
 g1_status g1_mem_fill_u32(void* dst, uint32_t value, size_t count, void* stream) {
     if (count == 0) return G1_OK;
+    if (!dst) return fail(G1_ERR_INVALID, "g1_mem_fill_u32: null pointer");
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -42,6 +42,38 @@ def test_status_strings_and_argument_errors_without_gpu():
     assert L.g1_pagerank(None, C.c_float(0.85), 30, 1, None, None) == 1
 
 
+# Entry points for which null arguments are valid (a no-op, optional outputs,
+# the default stream) or that take no pointer at all.
+NULL_OK = {"g1_graph_destroy", "g1_mem_free", "g1_server_destroy", "g1_profile_begin",
+           "g1_profile_end", "g1_release_cached_memory", "g1_stream_sync",
+           "g1_graph_device_bytes", "g1_kernel_launches", "g1_count_user_launches",
+           "g1_status_string", "g1_last_error", "g1_version"}
+
+
+def test_every_entry_point_rejects_null_arguments_before_any_device_work():
+    """Every other entry point, called with null pointers and sizes of 1,
+    returns G1_ERR_INVALID from its argument checks (it reaches no CUDA
+    call, which would answer G1_ERR_DEVICE on a machine without a GPU)."""
+    L = g1.lib()
+    checked = []
+    for name in sorted(g1.EXPORTS):
+        if name in NULL_OK:
+            continue
+        f = getattr(L, name)
+        args = []
+        for t in f.argtypes or []:
+            if t in (C.c_float, C.c_double):
+                args.append(0.5)
+            elif t in (C.c_int, C.c_uint32, C.c_uint64, C.c_size_t, C.c_int64):
+                args.append(1)
+            else:
+                args.append(None)
+        st = f(*args)
+        assert st == 1, (name, st, L.g1_last_error())
+        checked.append(name)
+    assert len(checked) >= 20
+
+
 def test_python_variant_table_matches_the_launcher():
     src = open(os.path.join(ROOT, "graphone_b200", "csrc", "spmv_launch.cuh")).read()
     n = int(re.search(r"kNumMergeVariants\s*=\s*(\d+)", src).group(1))
