@@ -180,9 +180,6 @@ bool others_hold_memory(g1_server* S, const Exec* self) {
     return false;
 }
 
-// Allocates the executor's engine: the largest slot count (halving from
-// max_batch down to 32) whose state fits the free device memory minus the
-// reserve and the server's limit.
 // Free device memory on the current device, counting the library's cache of
 // released blocks (reusable, or freed when an allocation needs the room).
 size_t device_free_bytes() {
@@ -199,6 +196,9 @@ size_t device_free_bytes() {
     return free_b + dev_block_cached(dev);
 }
 
+// Allocates the executor's engine: the largest slot count (halving from
+// max_batch down to 32) whose state fits the free device memory minus the
+// reserve and the server's limit.
 bool allocate(g1_server* S, Exec& E) {
     for (uint32_t K = (S->max_batch + 31) / 32 * 32;;) {
         const size_t need = SlotEngine::bytes(E.sg, E.kind, K);
@@ -520,6 +520,31 @@ extern "C" g1_status g1_server_create(int device, const g1_server_config* cfg, g
     return G1_OK;
 }
 
+namespace g1 {
+namespace {
+
+// The executor of one (graph, query kind): its stream and event, and the
+// slot view of the graph when the graph supports the kind.
+g1_status init_exec(g1_graph* g, int kind, Exec& E) {
+    E.g = g;
+    E.kind = kind;
+    G1_CUDA(cudaStreamCreateWithFlags(&E.s, cudaStreamNonBlocking));
+    G1_CUDA(cudaEventCreateWithFlags(&E.ev, cudaEventDisableTiming));
+    E.last_busy = Clock::now();
+    if (kind == kSlotSssp && g->vtype != G1_U32) return G1_OK;
+    std::lock_guard<std::mutex> lk(g->mu);
+    G1_TRY(slot_graph(g, kind, E.s, &E.sg));
+    if (kind == kSlotSssp && nearfar_suits(g)) {
+        E.nearfar = true;
+        G1_TRY(nearfar_delta(g, false, E.s, &E.nf_delta));
+    }
+    E.usable = true;
+    return G1_OK;
+}
+
+}  // namespace
+}  // namespace g1
+
 extern "C" g1_status g1_server_add_graph(g1_server* S, g1_graph* g, uint32_t* graph_id) {
     if (!S || !g || !graph_id) return fail(G1_ERR_INVALID, "g1_server_add_graph: null argument");
     if (g->device != S->device) return fail(G1_ERR_INVALID, "graph lives on another device");
@@ -532,20 +557,16 @@ extern "C" g1_status g1_server_add_graph(g1_server* S, g1_graph* g, uint32_t* gr
     std::unique_ptr<Exec> ex[3];
     for (int kind = 0; kind < 3; ++kind) {
         ex[kind].reset(new Exec());
-        Exec& E = *ex[kind];
-        E.g = g;
-        E.kind = kind;
-        G1_CUDA(cudaStreamCreateWithFlags(&E.s, cudaStreamNonBlocking));
-        G1_CUDA(cudaEventCreateWithFlags(&E.ev, cudaEventDisableTiming));
-        E.last_busy = Clock::now();
-        if (kind == kSlotSssp && g->vtype != G1_U32) continue;
-        std::lock_guard<std::mutex> lk(g->mu);
-        G1_TRY(slot_graph(g, kind, E.s, &E.sg));
-        if (kind == kSlotSssp && nearfar_suits(g)) {
-            E.nearfar = true;
-            G1_TRY(nearfar_delta(g, false, E.s, &E.nf_delta));
+        const g1_status st = init_exec(g, kind, *ex[kind]);
+        if (st != G1_OK) {
+            // nothing of this graph is visible to the loop yet
+            for (auto& e : ex) {
+                if (!e) continue;
+                if (e->ev) cudaEventDestroy(e->ev);
+                if (e->s) cudaStreamDestroy(e->s);
+            }
+            return st;
         }
-        E.usable = true;
     }
     // the loop only reads execs[0, n_execs)
     for (auto& e : ex) S->execs.push_back(std::move(e));
