@@ -1,0 +1,34 @@
+// Prints the CSR that the drop-in GraphOne loader (include/GraphOne/loader/
+// loader.h) builds from an .adj file: for the out-edge then the in-edge
+// orientation, a line "n m" and the row offsets, columns and values.
+// Usage: loader_driver FILE.adj DIRECTED(0|1)
+#include <cstdio>
+
+#include "GraphOne/loader/loader.h"
+
+using namespace graph_one;
+
+int main(int argc, char** argv) {
+    if (argc != 3) return 2;
+    LoadEdgeOpts opts;
+    opts.is_directed = argv[2][0] == '1';
+    GraphLoader<vstart_t::FROM_0_TO_0> loader;
+    auto cache = loader.LoadEdgesFromTxt<uint32_t>(argv[1], opts);
+    for (int t = 0; t < 2; ++t) {
+        std::vector<eid_t> rp;
+        std::vector<vid_t> ci;
+        std::vector<uint32_t> v;
+        if (t)
+            cache.BuildCsr<true>(rp, ci, v);
+        else
+            cache.BuildCsr<false>(rp, ci, v);
+        std::printf("%u %llu\n", (unsigned)cache.num_vertices(), (unsigned long long)cache.num_edges());
+        for (auto x : rp) std::printf("%llu ", (unsigned long long)x);
+        std::printf("\n");
+        for (auto x : ci) std::printf("%u ", (unsigned)x);
+        std::printf("\n");
+        for (auto x : v) std::printf("%u ", (unsigned)x);
+        std::printf("\n");
+    }
+    return 0;
+}

@@ -1,0 +1,146 @@
+"""The drop-in loader (include/GraphOne/loader/loader.h, host code) against
+GraphOne's own GraphLoader + EdgeCache::ToCsr (oracle/_ref, when built) and
+the oracle's counting sort, on .adj files with comments, blank lines, tabs,
+self loops, missing weights, duplicates and isolated vertices.  CPU only."""
+import ctypes as C
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+pytestmark = pytest.mark.skipif(shutil.which("g++") is None, reason="g++ not available")
+
+TRICKY = """% a comment line
+% another one
+
+0 1 5
+  0\t2 7   
+1 1 9
+2 4
+3 0 4
+0 1 5
+% duplicate above, self loop 1-1 dropped
+6 3 2
+\t
+7\t6\t1
+5
+9 9 3
+"""
+
+
+def random_adj(rng, n, m):
+    """Weighted lines over vertices [0, n), weightless ones over [n, n + 50);
+    duplicates (in either direction) carry the same weight, because the
+    reference keeps an unspecified one of differing duplicates."""
+    a = rng.integers(0, n, m)
+    b = rng.integers(0, n, m)
+    lo, hi = np.minimum(a, b), np.maximum(a, b)
+    w = (lo * 7919 + hi * 104729) % 97 + 1
+    lines = [f"{x} {y} {z}" for x, y, z in zip(a, b, w)]
+    c = rng.integers(n, n + 50, (m // 5, 2))
+    lines += [f"{x}\t{y}" for x, y in c]
+    lines += lines[: m // 10]  # verbatim repeats
+    order = rng.permutation(len(lines))
+    return "\n".join(lines[i] for i in order)  # no newline after the last line
+
+
+def parse(text, directed):
+    """The reference's reading rules restated (loader/graph_loader.h:32-122,
+    edge_cache.h:50-105): edges in file order, self loops dropped, reverse
+    edges for undirected input, duplicates merged after sorting by (src, dst)."""
+    edges = []
+    for line in text.split("\n"):
+        s = line.strip()
+        if not s or s.startswith("%"):
+            continue
+        tok = s.replace("\t", " ").split()
+        if len(tok) < 2:
+            continue
+        u, v = int(tok[0]), int(tok[1])
+        w = int(tok[2]) if len(tok) > 2 else 1
+        if u == v:
+            continue
+        edges.append((u, v, w))
+        if not directed:
+            edges.append((v, u, w))
+    edges = sorted(set(edges), key=lambda e: (e[0], e[1]))
+    n = max([max(u, v) for u, v, _ in edges], default=0) + 1
+    src = np.array([e[0] for e in edges], np.uint32)
+    dst = np.array([e[1] for e in edges], np.uint32)
+    w = np.array([e[2] for e in edges], np.uint32)
+    return n, src, dst, w
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    exe = tmp_path_factory.mktemp("loader") / "loader_driver"
+    r = subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "loader_driver.cpp"), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return str(exe)
+
+
+def ours(driver, path, directed):
+    r = subprocess.run([driver, path, "1" if directed else "0"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    # the loader's warnings ("[WARN] ...", the one-token line) share stdout
+    lines = [ln for ln in r.stdout.split("\n") if not ln.startswith("[")]
+    out = []
+    for t in range(2):
+        n, m = map(int, lines[4 * t].split())
+        arr = [np.array(lines[4 * t + k].split(), dtype=np.int64).astype(np.uint32) for k in (1, 2, 3)]
+        out.append((n, m, *arr))
+    return out
+
+
+def reference(path, directed):
+    R = O.ref()
+    if R is None:
+        return None
+    n, m = C.c_uint32(), C.c_uint64()
+    assert R.ref_load_adj(path.encode(), int(directed), C.byref(n), C.byref(m)) == 0
+    out = []
+    for t in range(2):
+        rp = np.zeros(n.value + 1, np.uint32)
+        ci = np.zeros(max(1, m.value), np.uint32)
+        v = np.zeros(max(1, m.value), np.uint32)
+        assert R.ref_to_csr(t, O._ptr(rp), O._ptr(ci), O._ptr(v)) == 0
+        out.append((n.value, m.value, rp, ci[: m.value], v[: m.value]))
+    return out
+
+
+CASES = {"tricky": lambda: TRICKY,
+         "random": lambda: random_adj(np.random.default_rng(7), 300, 4000),
+         "one_edge": lambda: "4 2 3",
+         "only_comments": lambda: "% nothing\n\n% here\n"}
+
+
+@pytest.mark.parametrize("directed", [True, False])
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_loader_matches_graphone_loader_and_oracle(driver, tmp_path, case, directed):
+    text = CASES[case]()
+    path = str(tmp_path / f"{case}.adj")
+    with open(path, "w") as f:
+        f.write(text)
+    got = ours(driver, path, directed)
+    n, src, dst, w = parse(text, directed)
+    for t, (gn, gm, rp, ci, v) in enumerate(got):
+        assert (gn, gm) == (n, len(src))
+        if t == 0:
+            erp, eci, ev = O.csr_build(n, src, dst, w, transpose=False)
+        else:
+            erp, eci, ev = O.csr_build(n, src, dst, w, transpose=True)
+        assert np.array_equal(rp, erp) and np.array_equal(ci, eci) and np.array_equal(v, ev)
+    ref = reference(path, directed)
+    if ref is not None:
+        for g, r in zip(got, ref):
+            assert g[:2] == r[:2]
+            for a, b in zip(g[2:], r[2:]):
+                assert np.array_equal(a, b)
