@@ -81,6 +81,8 @@ def ref():
             R = C.CDLL(path)
             R.ref_load_adj.restype = C.c_int
             R.ref_load_adj.argtypes = [C.c_char_p, C.c_int, P, P]
+            R.ref_load_adj_opts.restype = C.c_int
+            R.ref_load_adj_opts.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, P, P]
             R.ref_to_csr.restype = C.c_int
             R.ref_to_csr.argtypes = [C.c_int, P, P, P]
             R.ref_spmv_minplus_u32.argtypes = [C.c_uint32, P, P, P, P, P, C.c_int]

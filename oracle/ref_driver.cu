@@ -98,6 +98,21 @@ int ref_load_adj(const char* path, int directed, uint32_t* n_out, uint64_t* m_ou
     return 0;
 }
 
+// The same with the loader's other switches: first-seen vertex renumbering
+// (GraphLoader(reorder_vid)), self loops and duplicate edges kept.
+int ref_load_adj_opts(const char* path, int directed, int reorder, int keep_self, int keep_dup,
+                      uint32_t* n_out, uint64_t* m_out) {
+    LoadEdgeOpts opts;
+    opts.is_directed = directed != 0;
+    opts.keep_self_loop = keep_self != 0;
+    opts.keep_duplicate_edges = keep_dup != 0;
+    GraphLoader<vstart_t::FROM_0_TO_0> loader(reorder != 0);
+    g_loaded.reset(new Loaded{loader.LoadEdgesFromTxt<uint32_t>(path, opts)});
+    *n_out = g_loaded->cache.num_vertices();
+    *m_out = g_loaded->cache.num_edges();
+    return 0;
+}
+
 // EdgeCache::ToCsr<cpu, transpose> of the last loaded graph.
 int ref_to_csr(int transpose, uint32_t* row_ptr, uint32_t* col, uint32_t* val) {
     if (!g_loaded) return 1;

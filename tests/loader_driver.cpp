@@ -1,7 +1,7 @@
 // Prints the CSR that the drop-in GraphOne loader (include/GraphOne/loader/
 // loader.h) builds from an .adj file: for the out-edge then the in-edge
 // orientation, a line "n m" and the row offsets, columns and values.
-// Usage: loader_driver FILE.adj DIRECTED(0|1)
+// Usage: loader_driver FILE.adj DIRECTED REORDER KEEP_SELF KEEP_DUP (each 0|1)
 #include <cstdio>
 
 #include "GraphOne/loader/loader.h"
@@ -9,10 +9,12 @@
 using namespace graph_one;
 
 int main(int argc, char** argv) {
-    if (argc != 3) return 2;
+    if (argc != 6) return 2;
     LoadEdgeOpts opts;
     opts.is_directed = argv[2][0] == '1';
-    GraphLoader<vstart_t::FROM_0_TO_0> loader;
+    opts.keep_self_loop = argv[4][0] == '1';
+    opts.keep_duplicate_edges = argv[5][0] == '1';
+    GraphLoader<vstart_t::FROM_0_TO_0> loader(argv[3][0] == '1');
     auto cache = loader.LoadEdgesFromTxt<uint32_t>(argv[1], opts);
     for (int t = 0; t < 2; ++t) {
         std::vector<eid_t> rp;

@@ -1,7 +1,9 @@
 """The drop-in loader (include/GraphOne/loader/loader.h, host code) against
 GraphOne's own GraphLoader + EdgeCache::ToCsr (oracle/_ref, when built) and
 the oracle's counting sort, on .adj files with comments, blank lines, tabs,
-self loops, missing weights, duplicates and isolated vertices.  CPU only."""
+self loops, missing weights, duplicates and isolated vertices, with each of
+the loader's switches (directed, first-seen renumbering, self loops and
+duplicates kept).  CPU only."""
 import ctypes as C
 import os
 import shutil
@@ -50,11 +52,21 @@ def random_adj(rng, n, m):
     return "\n".join(lines[i] for i in order)  # no newline after the last line
 
 
-def parse(text, directed):
+def parse(text, directed, reorder=False, keep_self=False, keep_dup=False):
     """The reference's reading rules restated (loader/graph_loader.h:32-122,
-    edge_cache.h:50-105): edges in file order, self loops dropped, reverse
-    edges for undirected input, duplicates merged after sorting by (src, dst)."""
-    edges = []
+    255-296, edge_cache.h:50-105): edges in file order, self loops dropped
+    unless kept, ids renumbered in first-seen order when asked (after the
+    self-loop check), reverse edges for undirected input, duplicates merged
+    after sorting by (src, dst) unless kept."""
+    edges, vmap = [], {}
+
+    def rn(x):
+        if not reorder:
+            return x
+        if x not in vmap:
+            vmap[x] = len(vmap)
+        return vmap[x]
+
     for line in text.split("\n"):
         s = line.strip()
         if not s or s.startswith("%"):
@@ -64,12 +76,14 @@ def parse(text, directed):
             continue
         u, v = int(tok[0]), int(tok[1])
         w = int(tok[2]) if len(tok) > 2 else 1
-        if u == v:
+        if u == v and not keep_self:
             continue
+        u, v = rn(u), rn(v)
         edges.append((u, v, w))
-        if not directed:
+        if not directed and u != v:
             edges.append((v, u, w))
-    edges = sorted(set(edges), key=lambda e: (e[0], e[1]))
+    if not keep_dup:
+        edges = sorted(set(edges), key=lambda e: (e[0], e[1]))
     n = max([max(u, v) for u, v, _ in edges], default=0) + 1
     src = np.array([e[0] for e in edges], np.uint32)
     dst = np.array([e[1] for e in edges], np.uint32)
@@ -87,8 +101,8 @@ def driver(tmp_path_factory):
     return str(exe)
 
 
-def ours(driver, path, directed):
-    r = subprocess.run([driver, path, "1" if directed else "0"], capture_output=True, text=True)
+def ours(driver, path, flags):
+    r = subprocess.run([driver, path, *("1" if f else "0" for f in flags)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
     # the loader's warnings ("[WARN] ...", the one-token line) share stdout
     lines = [ln for ln in r.stdout.split("\n") if not ln.startswith("[")]
@@ -100,12 +114,12 @@ def ours(driver, path, directed):
     return out
 
 
-def reference(path, directed):
+def reference(path, flags):
     R = O.ref()
     if R is None:
         return None
     n, m = C.c_uint32(), C.c_uint64()
-    assert R.ref_load_adj(path.encode(), int(directed), C.byref(n), C.byref(m)) == 0
+    assert R.ref_load_adj_opts(path.encode(), *(int(f) for f in flags), C.byref(n), C.byref(m)) == 0
     out = []
     for t in range(2):
         rp = np.zeros(n.value + 1, np.uint32)
@@ -122,23 +136,27 @@ CASES = {"tricky": lambda: TRICKY,
          "only_comments": lambda: "% nothing\n\n% here\n"}
 
 
-@pytest.mark.parametrize("directed", [True, False])
+# (directed, reorder, keep_self, keep_dup); the reference's own loader test
+# (test/loader_test.cpp) reads a directed file with renumbering on
+FLAGS = [(True, False, False, False), (False, False, False, False), (True, True, False, False),
+         (False, True, False, False), (True, False, True, False), (False, False, True, True),
+         (True, True, True, True), (False, True, False, True)]
+
+
+@pytest.mark.parametrize("flags", FLAGS, ids=lambda f: "".join("dRsD"[i] if x else "-" for i, x in enumerate(f)))
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_loader_matches_graphone_loader_and_oracle(driver, tmp_path, case, directed):
+def test_loader_matches_graphone_loader_and_oracle(driver, tmp_path, case, flags):
     text = CASES[case]()
     path = str(tmp_path / f"{case}.adj")
     with open(path, "w") as f:
         f.write(text)
-    got = ours(driver, path, directed)
-    n, src, dst, w = parse(text, directed)
+    got = ours(driver, path, flags)
+    n, src, dst, w = parse(text, *flags)
     for t, (gn, gm, rp, ci, v) in enumerate(got):
         assert (gn, gm) == (n, len(src))
-        if t == 0:
-            erp, eci, ev = O.csr_build(n, src, dst, w, transpose=False)
-        else:
-            erp, eci, ev = O.csr_build(n, src, dst, w, transpose=True)
+        erp, eci, ev = O.csr_build(n, src, dst, w, transpose=bool(t))
         assert np.array_equal(rp, erp) and np.array_equal(ci, eci) and np.array_equal(v, ev)
-    ref = reference(path, directed)
+    ref = reference(path, flags)
     if ref is not None:
         for g, r in zip(got, ref):
             assert g[:2] == r[:2]
