@@ -1,0 +1,4 @@
+#pragma once
+// GraphOne's frontier/sparse_dbl.h: the same names, provided by
+// frontier/frontier.h.
+#include "GraphOne/frontier/frontier.h"

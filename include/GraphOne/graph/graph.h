@@ -42,6 +42,19 @@ template <typename... M>
 constexpr bool has_some_views(graph_view_t v, M... m) {
     return (has_view(v, m) || ...);
 }
+constexpr graph_view_t set_view(graph_view_t v, graph_view_t m) { return v | m; }
+constexpr graph_view_t unset_view(graph_view_t v, graph_view_t m) {
+    return static_cast<graph_view_t>(static_cast<uint8_t>(v) & ~static_cast<uint8_t>(m));
+}
+// Position (1-based) of the highest set bit of N; 0 for N == 0.
+template <uint8_t N>
+struct highest_bit {
+    static constexpr uint8_t value = N == 0 ? 0 : 1 + highest_bit<N / 2>::value;
+};
+template <>
+struct highest_bit<0> {
+    static constexpr uint8_t value = 0;
+};
 
 template <graph_view_t views, arch_t arch, vstart_t v_start, typename vprop_t, typename vertex_t,
           typename edge_t, typename weight_t>

@@ -15,6 +15,7 @@
 #include "GraphOne/utils/cli.hpp"
 #include "GraphOne/base/buffer.h"
 #include "GraphOne/archi/archi.cuh"
+#include "GraphOne/archi/blas/spmv/spmv.h"
 #include "GraphOne/loader/loader.h"
 #include "GraphOne/graph/graph.h"
 #include "GraphOne/base/component.h"

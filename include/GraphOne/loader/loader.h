@@ -42,8 +42,10 @@ struct CsrMat {
           col_indices(std::move(ci)), values(std::move(v)) {}
 
     std::string ToString() const {
-        return "CsrMat{ n_rows:" + utils::NumToString(n_rows) + ", n_cols:" +
-               utils::NumToString(n_cols) + ", nnz:" + utils::NumToString(nnz) + " }";
+        return "CsrMat{ arch_value:" + utils::ToString(arch_value) + ", n_rows:" + utils::NumToString(n_rows) +
+               ", n_cols:" + utils::NumToString(n_cols) + ", nnz:" + utils::NumToString(nnz) +
+               ", row_offsets:" + row_offsets.ToString() + ", col_indices:" + col_indices.ToString() +
+               ", values:" + values.ToString() + " }";
     }
 
     index_t n_rows{0};

@@ -68,14 +68,25 @@ std::string ToString(const std::pair<K, V>& p) {
     return "(" + ToString(p.first) + "," + ToString(p.second) + ")";
 }
 
-template <typename T>
-std::string VecToString(const T* vec, size_t size) {
+// "[a,b,c]"; str_func formats one element (default ToString).
+template <typename T, typename F>
+std::string VecToString(const T* vec, size_t size, F str_func) {
     std::string str = "[";
     for (size_t i = 0; i < size; ++i) {
         if (i) str += ",";
-        str += ToString(vec[i]);
+        str += str_func(vec[i]);
     }
     return str + "]";
+}
+
+template <typename T>
+std::string VecToString(const T* vec, size_t size) {
+    return VecToString(vec, size, [](const T& x) { return ToString(x); });
+}
+
+template <typename T, typename F>
+std::string VecToString(const std::vector<T>& vec, F str_func) {
+    return VecToString(vec.data(), vec.size(), str_func);
 }
 
 template <typename T>
@@ -83,16 +94,21 @@ std::string VecToString(const std::vector<T>& vec) {
     return VecToString(vec.data(), vec.size());
 }
 
-template <typename K, typename V>
-std::string HashmapToString(const std::unordered_map<K, V>& hashmap) {
+template <typename K, typename V, typename F>
+std::string HashmapToString(const std::unordered_map<K, V>& hashmap, F str_func) {
     std::string str = "[";
     bool first = true;
     for (const auto& kv : hashmap) {
         if (!first) str += ",";
         first = false;
-        str += ToString(kv);
+        str += str_func(kv);
     }
     return str + "]";
+}
+
+template <typename K, typename V>
+std::string HashmapToString(const std::unordered_map<K, V>& hashmap) {
+    return HashmapToString(hashmap, [](const std::pair<const K, V>& kv) { return ToString(kv); });
 }
 
 }  // namespace graph_one::utils

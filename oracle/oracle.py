@@ -31,7 +31,7 @@ def _ptr(a: np.ndarray):
 def build(ref: bool = False) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
     if ref:
-        subprocess.run(["make", "-s", "-j4", "-C", HERE, "ref", "refapps", "dropin"], check=True)
+        subprocess.run(["make", "-s", "-j4", "-C", HERE, "ref", "refapps", "dropin", "reftests"], check=True)
 
 
 def app(kind: str, name: str):
