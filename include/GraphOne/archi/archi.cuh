@@ -1,20 +1,34 @@
 #pragma once
 // Parallel primitives of the GraphOne API (reference: archi/thrust/
-// functions.h:17-104 over Thrust, archi/only/cuda.cuh:37-99).  The cuda
-// versions are this library's own grid-stride kernels, launched on the
-// default stream; iterators may be raw pointers or any random-access
-// iterator usable in device code (thrust::counting_iterator included), and
-// operators may be __device__ lambdas with or without a declared return
-// type (the accumulator of transform_reduce is the type of `init`).
+// functions.h:17-104 over Thrust, archi/only/cuda.cuh:37-99, archi/mem/
+// def.hpp:8-42, archi/thrust/def.hpp:9-27).  The element-wise ones (fill,
+// transform, for_each, transform_reduce) are this library's own grid-stride
+// kernels on the default stream; iterators may be raw pointers or any
+// random-access iterator usable in device code (thrust::counting_iterator
+// included), and operators may be __device__ lambdas with or without a
+// declared return type (the accumulator of transform_reduce is the type of
+// `init`).  The multi-pass ones (copy_if, inclusive_scan, sort_by_key) and
+// scatter, scatter_if and the vectorised lower_bound run on Thrust with the
+// arch's execution policy, as in the reference.  Memory: memalloc / memfree
+// / memset / memcpy<arch...> (device memory from libgraphone_b200).
 
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <iterator>
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <thrust/binary_search.h>
+#include <thrust/copy.h>
+#include <thrust/device_vector.h>
+#include <thrust/execution_policy.h>
+#include <thrust/host_vector.h>
+#include <thrust/scan.h>
+#include <thrust/scatter.h>
+#include <thrust/sort.h>
 
 #include "graphone_b200.h"
 #include "GraphOne/macros.h"
@@ -37,13 +51,14 @@ inline unsigned grid_for(size_t n) {
     return (unsigned)std::max<size_t>(1, std::min<size_t>(want, (size_t)sms * 8));
 }
 
-inline void check_launch(const char* what) {
-    const cudaError_t e = cudaGetLastError();
+inline void check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) {
         std::fprintf(stderr, "[ERROR] %s: %s\n", what, cudaGetErrorString(e));
         std::exit(1);
     }
 }
+
+inline void check_launch(const char* what) { check(cudaGetLastError(), what); }
 
 template <typename It, typename T>
 __global__ void fill_kernel(It first, size_t n, T value) {
@@ -200,6 +215,151 @@ T transform_reduce(It first, It last, Op op, T init, Bop bop) {
         return acc;
     }
 }
+
+// ------------------------------------------------ Thrust-backed primitives
+
+template <arch_t arch>
+struct ExecPolicy;
+template <>
+struct ExecPolicy<arch_t::cpu> {
+    static constexpr decltype(thrust::host) value{};
+};
+template <>
+struct ExecPolicy<arch_t::cuda> {
+    static constexpr decltype(thrust::device) value{};
+};
+template <arch_t arch>
+static const auto exec_policy = ExecPolicy<arch>::value;
+
+template <arch_t arch>
+struct ThrustVec;
+template <>
+struct ThrustVec<arch_t::cpu> {
+    template <typename value_t>
+    using type = thrust::host_vector<value_t>;
+};
+template <>
+struct ThrustVec<arch_t::cuda> {
+    template <typename value_t>
+    using type = thrust::device_vector<value_t>;
+};
+template <arch_t arch, typename value_t>
+using thrust_vec = typename ThrustVec<arch>::template type<value_t>;
+
+namespace detail {
+template <arch_t arch>
+inline void check_thrust(const char* what) {
+    if constexpr (arch == arch_t::cuda) check_launch(what);
+}
+}  // namespace detail
+
+// Copies first[i] to the output where pred(stencil[i]); returns the end of the output.
+template <arch_t arch, typename It1, typename It2, typename Out, typename Pred>
+Out copy_if(It1 first, It1 last, It2 stencil, Out result, Pred pred) {
+    Out end = thrust::copy_if(exec_policy<arch>, first, last, stencil, result, pred);
+    detail::check_thrust<arch>("archi::copy_if");
+    return end;
+}
+
+template <arch_t arch, typename It, typename Out, typename Op>
+Out inclusive_scan(It first, It last, Out result, Op op) {
+    Out end = thrust::inclusive_scan(exec_policy<arch>, first, last, result, op);
+    detail::check_thrust<arch>("archi::inclusive_scan");
+    return end;
+}
+
+// For each value, the first position in the sorted [first, last) not less than it.
+template <arch_t arch, typename It, typename ValIt, typename Out>
+Out lower_bound(It first, It last, ValIt values_first, ValIt values_last, Out output) {
+    Out end = thrust::lower_bound(exec_policy<arch>, first, last, values_first, values_last, output);
+    detail::check_thrust<arch>("archi::lower_bound");
+    return end;
+}
+
+// result[map[i]] = first[i]
+template <arch_t arch, typename It, typename MapIt, typename Out>
+void scatter(It first, It last, MapIt map, Out result) {
+    thrust::scatter(exec_policy<arch>, first, last, map, result);
+    detail::check_thrust<arch>("archi::scatter");
+}
+
+// result[map[i]] = first[i] where stencil[i]
+template <arch_t arch, typename It, typename MapIt, typename StIt, typename Out>
+void scatter_if(It first, It last, MapIt map, StIt stencil, Out result) {
+    thrust::scatter_if(exec_policy<arch>, first, last, map, stencil, result);
+    detail::check_thrust<arch>("archi::scatter_if");
+}
+
+template <arch_t arch, typename KeyIt, typename ValIt>
+void sort_by_key(KeyIt keys_first, KeyIt keys_last, ValIt values_first) {
+    thrust::sort_by_key(exec_policy<arch>, keys_first, keys_last, values_first);
+    detail::check_thrust<arch>("archi::sort_by_key");
+}
+
+// ---------------------------------------------------------------- memory
+
+template <arch_t arch>
+struct memalloc_t {
+    template <typename T>
+    static T* call(size_t size) {
+        if constexpr (arch == arch_t::cpu) {
+            return static_cast<T*>(std::calloc(size ? size : 1, sizeof(T)));
+        } else {
+            void* p = nullptr;
+            if (g1_mem_alloc(&p, size * sizeof(T)) != G1_OK) {
+                std::fprintf(stderr, "[ERROR] archi::memalloc: %s\n", g1_last_error());
+                std::exit(1);
+            }
+            return static_cast<T*>(p);
+        }
+    }
+};
+template <arch_t arch>
+struct memfree_t {
+    template <typename T>
+    static void call(T* ptr) {
+        if constexpr (arch == arch_t::cpu)
+            std::free(ptr);
+        else
+            g1_mem_free(ptr);
+    }
+};
+template <arch_t arch>
+struct memset_t {
+    template <typename T>
+    static void call(T* ptr, int value, size_t size) {
+        if constexpr (arch == arch_t::cpu) {
+            std::memset(ptr, value, size * sizeof(T));
+        } else {
+            detail::check(cudaMemset(ptr, value, size * sizeof(T)), "archi::memset");
+        }
+    }
+};
+template <arch_t dst_arch, arch_t src_arch>
+struct memcpy_t {
+    template <typename T>
+    static void call(T* dst, const T* src, size_t size) {
+        if (size == 0) return;
+        if constexpr (dst_arch == arch_t::cpu && src_arch == arch_t::cpu) {
+            std::memcpy(dst, src, size * sizeof(T));
+        } else {
+            const int kind = src_arch == arch_t::cpu ? 0 : (dst_arch == arch_t::cpu ? 1 : 2);
+            if (g1_mem_copy(dst, src, size * sizeof(T), kind, nullptr) != G1_OK) {
+                std::fprintf(stderr, "[ERROR] archi::memcpy: %s\n", g1_last_error());
+                std::exit(1);
+            }
+            g1_stream_sync(nullptr);
+        }
+    }
+};
+template <arch_t arch, typename value_t>
+constexpr auto memalloc = memalloc_t<arch>::template call<value_t>;
+template <arch_t arch, typename value_t>
+constexpr auto memfree = memfree_t<arch>::template call<value_t>;
+template <arch_t arch, typename value_t>
+constexpr auto memset = memset_t<arch>::template call<value_t>;
+template <arch_t to_arch, arch_t from_arch, typename value_t>
+constexpr auto memcpy = memcpy_t<to_arch, from_arch>::template call<value_t>;
 
 namespace cuda {
 
