@@ -11,6 +11,8 @@
 // scatter, scatter_if and the vectorised lower_bound run on Thrust with the
 // arch's execution policy, as in the reference.  Memory: memalloc / memfree
 // / memset / memcpy<arch...> (device memory from libgraphone_b200).
+// Launches: LaunchKernel / LaunchSync (GraphOne/archi/kernel/kernel.h);
+// checks: checkCudaErrors / checkArchErrors (GraphOne/archi/check/check.h).
 
 #include <algorithm>
 #include <cstdint>
@@ -31,6 +33,8 @@
 #include <thrust/sort.h>
 
 #include "graphone_b200.h"
+#include "GraphOne/archi/check/check.h"
+#include "GraphOne/archi/kernel/kernel.h"
 #include "GraphOne/macros.h"
 #include "GraphOne/type.hpp"
 

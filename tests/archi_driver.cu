@@ -7,7 +7,8 @@
 // OUT: u32 count, then n-entry u32 arrays: copy_if (first count valid),
 //      inclusive max-scan, lower_bound, scatter, scatter_if (zeros where not
 //      written), keys sorted, vals by key, fill(7), transform(3v+1),
-//      then u64 transform_reduce(sum of v*v), u64 for_each sum of v
+//      2v+5 (cuda: a kernel launched by archi::LaunchKernel), then u64
+//      transform_reduce(sum of v*v), u64 for_each sum of v
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -15,6 +16,12 @@
 #include "GraphOne/archi/archi.cuh"
 
 using namespace graph_one;
+
+// y[i] = 2 x[i] + 5 over a grid-stride loop, launched by archi::LaunchKernel
+template <typename tparams>
+__global__ void twice_plus5(const uint32_t* x, uint32_t* y, uint32_t n) {
+    for (uint32_t i = tparams::global_tid(); i < n; i += tparams::grid_threads()) y[i] = 2u * x[i] + 5u;
+}
 
 template <arch_t A>
 static int run(const std::vector<std::vector<uint32_t>>& in, FILE* o) {
@@ -69,6 +76,17 @@ static int run(const std::vector<std::vector<uint32_t>>& in, FILE* o) {
     });
     unsigned long long each = 0;
     archi::memcpy<arch_t::cpu, A, unsigned long long>(&each, acc, 1);
+    if constexpr (A == arch_t::cuda) {
+        using tp = archi::LaunchTparams<arch_t::cuda>;
+        auto kernel = twice_plus5<tp>;
+        checkArchErrors(A, (archi::LaunchKernel<A, empty_t>({(int64_t)n}, kernel, vals, out, (uint32_t)n)));
+        checkArchErrors(A, archi::LaunchSync<A>());
+        res.push_back(down(out));
+    } else {
+        std::vector<uint32_t> h(n);
+        for (size_t i = 0; i < n; ++i) h[i] = 2u * in[1][i] + 5u;
+        res.push_back(h);
+    }
     std::fwrite(&count, 4, 1, o);
     for (auto& r : res) std::fwrite(r.data(), 4, n, o);
     std::fwrite(&sq, 8, 1, o);

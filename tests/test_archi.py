@@ -1,7 +1,7 @@
 """GraphOne's archi:: primitives (include/GraphOne/archi/archi.cuh: copy_if,
 inclusive_scan, lower_bound, scatter, scatter_if, sort_by_key, fill,
-transform, transform_reduce, for_each and the memalloc / memcpy / memset /
-memfree functors) with arch_t::cpu against numpy.  The driver
+transform, transform_reduce, for_each, the memalloc / memcpy / memset /
+memfree functors and, on the GPU, LaunchKernel / LaunchSync) with arch_t::cpu against numpy.  The driver
 (tests/archi_driver.cu) is built with nvcc; its cuda mode runs under
 `-m gpu` (tests/test_zzz_spmv_api_gpu.py).  CPU only."""
 import os
@@ -52,8 +52,8 @@ def run_archi(exe, tmp_path, kind, arrs):
     assert r.returncode == 0, r.stderr[-2000:]
     raw = open(out, "rb").read()
     count = int(np.frombuffer(raw[:4], np.uint32)[0])
-    body = np.frombuffer(raw[4:4 + 4 * 9 * n], np.uint32).reshape(9, n)
-    sq, each = np.frombuffer(raw[4 + 4 * 9 * n:], np.uint64)
+    body = np.frombuffer(raw[4:4 + 4 * 10 * n], np.uint32).reshape(10, n)
+    sq, each = np.frombuffer(raw[4 + 4 * 10 * n:], np.uint64)
     return count, body, int(sq), int(each)
 
 
@@ -74,6 +74,7 @@ def check_archi(arrs, count, body, sq, each):
     assert np.array_equal(body[5], keys[order]) and np.array_equal(body[6], vals[order])
     assert np.all(body[7] == 7)
     assert np.array_equal(body[8], (3 * vals.astype(np.uint64) + 1).astype(np.uint32))
+    assert np.array_equal(body[9], (2 * vals.astype(np.uint64) + 5).astype(np.uint32))
     assert sq == int((vals.astype(np.uint64) ** 2).sum())
     assert each == int(vals.astype(np.uint64).sum())
 
