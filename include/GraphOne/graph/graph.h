@@ -133,9 +133,41 @@ public:
     Graph(g1_graph* handle, vertex_t n, edge_t m)
         : h_(handle, detail::GraphHandleDeleter()), n_(n), m_(m) {}
 
+    using graph_mat_t = CsrMat<arch, weight_t, vertex_t, edge_t, v_start>;
+    using graph_tmat_t = std::conditional_t<both_mat, graph_mat_t, empty_t>;
+
     vertex_t num_vertices() const { return n_; }
     edge_t num_edges() const { return m_; }
     g1_graph* handle() const { return h_.get(); }
+    const vprop_t& vprops() const { return vprops_; }
+
+    // Degrees from the device CSR: one 8-byte copy to the host per call, like
+    // an element read of a device Buffer (reference: graph/graph.h:62-84).
+    template <graph_view_t V = views>
+    std::enable_if_t<has_view(V, graph_view_t::normal), vertex_t> get_out_degree(vertex_t vid) const {
+        return degree_(0, vid);
+    }
+    template <graph_view_t V = views>
+    std::enable_if_t<has_view(V, graph_view_t::transpose), vertex_t> get_in_degree(vertex_t vid) const {
+        return degree_(1, vid);
+    }
+
+    // The CSR of the first view (and, with both views, the transpose) as
+    // CsrMat.  The library owns the graph's arrays, so these are device
+    // copies made on the first call and kept with the graph: same contents
+    // as ToArch()'s arrays, other addresses (reference: graph/graph.h:86-92).
+    const graph_mat_t& graph_mat() const {
+        if (!mats_->mat) mats_->mat.reset(new graph_mat_t(copy_mat_(has_normal ? 0 : 1)));
+        return *mats_->mat;
+    }
+    const graph_tmat_t& graph_transpose_mat() const {
+        if constexpr (both_mat) {
+            if (!mats_->tmat) mats_->tmat.reset(new graph_mat_t(copy_mat_(1)));
+            return *mats_->tmat;
+        } else {
+            return mats_->none;
+        }
+    }
 
     arch_ref_t ToArch() const {
         arch_ref_t r;
@@ -153,6 +185,35 @@ public:
     }
 
 private:
+    struct Mats {
+        std::unique_ptr<graph_mat_t> mat, tmat;
+        empty_t none{};
+    };
+
+    vertex_t degree_(int side, vertex_t vid) const {
+        const edge_t *rp = nullptr;
+        const vertex_t* ci = nullptr;
+        const weight_t* v = nullptr;
+        fetch_(side, &rp, &ci, &v);
+        edge_t two[2] = {0, 0};
+        ::graph_one::detail::mem_copy<arch_t::cpu, arch_t::cuda>(two, rp + vid, sizeof(two));
+        return (vertex_t)(two[1] - two[0]);
+    }
+
+    graph_mat_t copy_mat_(int side) const {
+        const edge_t *rp = nullptr;
+        const vertex_t* ci = nullptr;
+        const weight_t* v = nullptr;
+        fetch_(side, &rp, &ci, &v);
+        Buffer<arch, edge_t, vertex_t> b_rp((vertex_t)(n_ + 1));
+        Buffer<arch, vertex_t, edge_t> b_ci(m_);
+        Buffer<arch, weight_t, edge_t> b_v(m_);
+        ::graph_one::detail::mem_copy<arch, arch>(b_rp.data(), rp, sizeof(edge_t) * ((size_t)n_ + 1));
+        ::graph_one::detail::mem_copy<arch, arch>(b_ci.data(), ci, sizeof(vertex_t) * (size_t)m_);
+        ::graph_one::detail::mem_copy<arch, arch>(b_v.data(), v, sizeof(weight_t) * (size_t)m_);
+        return graph_mat_t(n_, n_, m_, std::move(b_rp), std::move(b_ci), std::move(b_v));
+    }
+
     void fetch_(int side, const edge_t** rp, const vertex_t** ci, const weight_t** v) const {
         const uint32_t *a = nullptr, *b = nullptr;
         const void* c = nullptr;
@@ -166,6 +227,8 @@ private:
     std::shared_ptr<g1_graph> h_;
     vertex_t n_;
     edge_t m_;
+    vprop_t vprops_{};
+    std::shared_ptr<Mats> mats_ = std::make_shared<Mats>();
 };
 
 namespace graph {
