@@ -85,6 +85,7 @@ def _declare(L):
     L.g1_pagerank.argtypes = [P, C.c_float, C.c_int, C.c_int, P, P]
     L.g1_sssp.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
     L.g1_bfs.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
+    L.g1_advance_run.argtypes = [P, C.c_int, P, C.c_uint32, P, P, C.c_uint32, P, C.POINTER(C.c_uint32), P]
     L.g1_bfs_batch.argtypes = [P, P, C.c_uint32, P, C.POINTER(C.c_uint32), P]
     L.g1_sssp_batch.argtypes = [P, P, C.c_uint32, P, C.POINTER(C.c_uint32), P]
     L.g1_ppr.argtypes = [P, C.c_uint32, C.c_float, C.c_uint32, P, P]
@@ -117,7 +118,7 @@ EXPORTS = (
     "g1_count_user_launches",
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
-    "g1_spmv_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs",
+    "g1_spmv_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs", "g1_advance_run",
     "g1_bfs_batch", "g1_sssp_batch", "g1_ppr", "g1_ppr_batch",
     "g1_server_create", "g1_server_add_graph", "g1_server_submit", "g1_server_poll",
     "g1_server_wait", "g1_server_stats", "g1_server_destroy",
@@ -268,6 +269,14 @@ class Graph:
         it = C.c_uint32()
         check(lib().g1_sssp(self._h, src, engine, _ptr(out), C.byref(it), _stream(stream)))
         return (out, it.value) if return_iters else out
+
+    def advance_run(self, frontier, n_frontier, dist, visited, it, out_frontier, unit=False, stream=None):
+        """One push relax step (g1_advance_run) over device tensors: returns
+        the length of the new frontier written to out_frontier."""
+        n_out = C.c_uint32()
+        check(lib().g1_advance_run(self._h, int(bool(unit)), _ptr(frontier), n_frontier, _ptr(dist),
+                                   _ptr(visited), it, _ptr(out_frontier), C.byref(n_out), _stream(stream)))
+        return n_out.value
 
     def _batch(self, fn, srcs, out, stream, return_iters):
         if isinstance(srcs, np.ndarray) or isinstance(srcs, (list, tuple)):

@@ -301,9 +301,92 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
     return check_device_error(g, s);
 }
 
+// One push step over caller-owned device arrays (g1_advance_run): the push
+// branch of traverse() on a given frontier.  The TPV choice uses the graph's
+// mean degree (the frontier's is not known without a pass over it); the
+// edge-balanced kernel grid-strides over the frontier's edges, so its grid
+// needs no degree sum either.
+template <bool UNIT>
+static g1_status advance_step(g1_graph* g, const uint32_t* F, uint32_t nF, uint32_t* dist,
+                              uint32_t* visited, uint32_t iter, uint32_t* out, uint32_t* out_size,
+                              cudaStream_t s) {
+    const Orientation& o = g->o[0];
+    Workspace& ws = g->ws;
+    uint32_t* cnt = nullptr;
+    G1_TRY(ws.get("adv_cnt", 8, &cnt));
+    G1_TRY(ws.pinned.ensure(64));
+    uint32_t* host = ws.pinned.as<uint32_t>();
+    unsigned long long* deg_sum = reinterpret_cast<unsigned long long*>(cnt + 2);
+    G1_CUDA(cudaMemsetAsync(cnt, 0, 16, s));
+    const uint64_t cap = (uint64_t)g->sm_count * 8;
+    const auto* val = static_cast<const uint32_t*>(o.val);
+    if (o.max_deg <= 32) {
+        const double mean = g->n ? (double)g->m / g->n : 1.0;
+        int tpv = 1;
+        while (tpv < 32 && tpv < mean) tpv <<= 1;
+        const uint32_t gt =
+            (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div((uint64_t)nF * tpv, 256), cap));
+        count_launches(1);
+#define G1_ADV_STEP(T)                                                                              \
+    tr_advance_kernel<UNIT, T><<<gt, 256, 0, s>>>(F, nF, o.rp, o.col, val, dist, visited, iter, out, \
+                                                  cnt, deg_sum)
+        switch (tpv) {
+            case 1: G1_ADV_STEP(1); break;
+            case 2: G1_ADV_STEP(2); break;
+            case 4: G1_ADV_STEP(4); break;
+            case 8: G1_ADV_STEP(8); break;
+            case 16: G1_ADV_STEP(16); break;
+            default: G1_ADV_STEP(32); break;
+        }
+#undef G1_ADV_STEP
+    } else {
+        uint32_t *deg = nullptr, *prefix = nullptr;
+        G1_TRY(ws.get("adv_deg", (size_t)nF + 1, &deg));
+        G1_TRY(ws.get("adv_prefix", (size_t)nF + 1, &prefix));
+        size_t scan_bytes = 0;
+        G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, deg, prefix, (int)nF + 1, s));
+        unsigned char* scan_tmp = nullptr;
+        G1_TRY(ws.get("adv_scan", scan_bytes + 16, &scan_tmp));
+        const uint32_t gf = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div((uint64_t)nF + 1, 256), cap));
+        tr_frontier_degrees_kernel<<<gf, 256, 0, s>>>(F, nF, o.rp, deg);
+        G1_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, deg, prefix, (int)nF + 1, s));
+        tr_advance_lb_kernel<UNIT><<<(uint32_t)cap, 256, 0, s>>>(F, nF, prefix, o.rp, o.col, val, dist, visited,
+                                                                 iter, out, cnt, deg_sum);
+        count_launches(3);
+    }
+    G1_CUDA(cudaGetLastError());
+    G1_CUDA(cudaMemcpyAsync(host, cnt, 16, cudaMemcpyDeviceToHost, s));
+    G1_CUDA(cudaStreamSynchronize(s));
+    if (host[0] > g->n) return fail(G1_ERR_OVERFLOW, "frontier larger than the vertex count");
+    *out_size = host[0];
+    return check_device_error(g, s);
+}
+
 }  // namespace g1
 
 using namespace g1;
+
+extern "C" g1_status g1_advance_run(g1_graph* g, int unit, const uint32_t* frontier, uint32_t n_frontier,
+                                    uint32_t* dist, uint32_t* visited, uint32_t iter, uint32_t* out_frontier,
+                                    uint32_t* out_size, void* stream) {
+    if (!g || !dist || !visited || !out_frontier || !out_size || (n_frontier && !frontier))
+        return fail(G1_ERR_INVALID, "g1_advance_run: null argument");
+    if (n_frontier > g->n) return fail(G1_ERR_INVALID, "g1_advance_run: frontier larger than the vertex count");
+    if (!g->o[0].present)
+        return fail(G1_ERR_UNSUPPORTED, "g1_advance_run: needs the out-edge CSR (G1_GRAPH_BUILD_OTHER)");
+    if (g->relabeled) return fail(G1_ERR_UNSUPPORTED, "g1_advance_run: graph was created with G1_GRAPH_RELABEL");
+    if (!unit && g->vtype != G1_U32) return fail(G1_ERR_INVALID, "g1_advance_run: SSSP needs u32 edge weights");
+    if (!is_device_ptr(frontier ? (const void*)frontier : (const void*)dist) || !is_device_ptr(dist) ||
+        !is_device_ptr(visited) || !is_device_ptr(out_frontier))
+        return fail(G1_ERR_INVALID, "g1_advance_run: frontier, dist, visited and out_frontier must be device memory");
+    *out_size = 0;
+    if (n_frontier == 0) return G1_OK;
+    DeviceGuard dg(g->device);
+    std::lock_guard<std::mutex> lk(g->mu);
+    cudaStream_t s = as_stream(stream);
+    return unit ? advance_step<true>(g, frontier, n_frontier, dist, visited, iter, out_frontier, out_size, s)
+                : advance_step<false>(g, frontier, n_frontier, dist, visited, iter, out_frontier, out_size, s);
+}
 
 extern "C" g1_status g1_sssp(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* dist_out,
                              uint32_t* iters_out, void* stream) {

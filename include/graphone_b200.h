@@ -201,6 +201,21 @@ g1_status g1_sssp(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* dist_ou
 g1_status g1_bfs(g1_graph* g, uint32_t src, g1_engine engine, uint32_t* level_out,
                  uint32_t* iters_out, void* stream);
 
+/* One push step of the advance/filter engine (replaces AdvanceGC::Forward,
+ * engine/advance_gc.h:162-283, with the relax functor of apps/sssp_adv.cu:
+ * 48-72; unit != 0 relaxes with weight 1, i.e. BFS levels).  For each vertex
+ * u of frontier[0, n_frontier) and out-edge (u, v, w): dist[v] =
+ * min(dist[v], dist[u] + w); a vertex whose distance dropped joins
+ * out_frontier once per step (visited[v] is set to iter).  frontier, dist
+ * (n), visited (n) and out_frontier (room for n) are device arrays; pass a
+ * new iter for each step (visited starting at 0, iter from 1).
+ * *out_size (host) gets the new frontier's length; the call synchronises
+ * `stream`.  Needs the out-edge CSR and a graph created without
+ * G1_GRAPH_RELABEL (ids are the caller's). */
+g1_status g1_advance_run(g1_graph* g, int unit, const uint32_t* frontier, uint32_t n_frontier,
+                         uint32_t* dist, uint32_t* visited, uint32_t iter, uint32_t* out_frontier,
+                         uint32_t* out_size, void* stream);
+
 /* ----------------------------------------------------- batched queries */
 /* k sources as one multi-source pass (no GraphOne counterpart: GraphOne
  * runs one source per Run, apps/sssp_blas.cu:87-136).  srcs: k vertex ids

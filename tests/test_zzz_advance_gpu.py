@@ -1,0 +1,62 @@
+"""g1_advance_run, one push relax step of the advance/filter engine over
+caller-owned device arrays, iterated to convergence from a source: the
+distances (BFS levels with unit=1) bit-exact against the oracle's Dijkstra /
+BFS on every edge-case graph (short adjacency lists take the lanes-per-vertex
+kernel, graphs with hubs the edge-balanced one).
+
+Collected last (file name) so that a failure here cannot hide the others."""
+import numpy as np
+import pytest
+import torch
+
+import graphone_b200 as g1
+from oracle import oracle as O
+from tests.gpu_util import edge_case_graphs
+
+pytestmark = pytest.mark.gpu
+
+GRAPHS = edge_case_graphs()
+
+
+def traverse_by_steps(G, n, src, unit):
+    dev = torch.device("cuda:0")
+    dist = torch.full((n,), -1, dtype=torch.int32, device=dev)  # UINT32_MAX
+    dist[src] = 0
+    visited = torch.zeros(n, dtype=torch.int32, device=dev)
+    fr = torch.zeros(max(n, 1), dtype=torch.int32, device=dev)
+    fr[0] = src
+    out = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+    n_f, it = 1, 0
+    while n_f:
+        it += 1
+        assert it <= n + 1
+        n_f = G.advance_run(fr, n_f, dist, visited, it, out, unit=unit)
+        fr, out = out, fr
+    return dist.cpu().numpy().view(np.uint32), it
+
+
+@pytest.mark.parametrize("unit", [False, True])
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+def test_advance_steps_match_oracle(cuda, name, unit):
+    g = GRAPHS[name]
+    rp, ci, v = g.np("n")
+    G = g1.Graph.from_gen(g)
+    src = 0
+    got, _ = traverse_by_steps(G, g.n, src, unit)
+    ref = O.bfs(rp, ci, src) if unit else O.dijkstra_u32(rp, ci, v, src)
+    assert np.array_equal(got, ref)
+    G.close()
+
+
+def test_advance_run_rejects_host_arrays_and_relabelled_graphs(cuda):
+    g = GRAPHS["grid32"]
+    G = g1.Graph.from_gen(g)
+    host = np.zeros(g.n, np.uint32)
+    with pytest.raises(g1.G1Error):
+        G.advance_run(host, 1, host, host, 1, host)
+    G.close()
+    R = g1.Graph.from_gen(g, relabel=True)
+    d = torch.zeros(g.n, dtype=torch.int32, device="cuda:0")
+    with pytest.raises(g1.G1Error):
+        R.advance_run(d, 1, d, d, 1, d)
+    R.close()
