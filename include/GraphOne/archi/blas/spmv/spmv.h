@@ -143,7 +143,7 @@ __global__ void merge_partition_kernel(const uint32_t* row_ptr, uint32_t n_rows,
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t > n_tiles) return;
     const uint64_t total = (uint64_t)n_rows + nnz;
-    const uint64_t d = std::min<uint64_t>((uint64_t)t * items, total);
+    const uint64_t d = (uint64_t)t * items < total ? (uint64_t)t * items : total;
     uint32_t i = 0, j = 0;
     g1::merge_path_search(d, row_ptr + 1, n_rows, nnz, &i, &j);
     tile_row[t] = i;
