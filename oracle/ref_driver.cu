@@ -1,4 +1,4 @@
-// Reference CPU driver -- TEST AND BASELINE INFRASTRUCTURE ONLY.
+// Reference CPU driver -- test and CPU-baseline infrastructure only.
 //
 // Compiled by oracle/Makefile against GraphOne's own headers (the reference
 // source tree, include path given on the command line) into
