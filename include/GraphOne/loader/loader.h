@@ -174,6 +174,76 @@ public:
         return cache;
     }
 
+    // LoadEdgesFromTxt then ToCsr (reference: loader/graph_loader.h:123-129).
+    template <arch_t arch, typename edata_t>
+    CsrMat<arch, edata_t, index_t, offset_t, v_start> LoadCsrFromTxt(const std::string& path,
+                                                                     const LoadEdgeOpts& opts = LoadEdgeOpts()) {
+        return LoadEdgesFromTxt<edata_t>(path, opts).template ToCsr<arch>();
+    }
+
+    // Per-vertex lines "vid data..." (reference: loader/graph_loader.h:131-201):
+    // lines starting with the comment prefix are skipped, the id is the first
+    // token (renumbered like the edges when reordering is on), and the parser
+    // gets either the rest of the line (parse_t = char*) or its tokens parsed
+    // as parse_t.  A parser returning false logs a warning.
+    template <typename parse_t, typename parse_func>
+    void LoadVertexStatusFromTxt(const std::string& path, parse_func&& parser,
+                                 const LoadVertexOpts& opts = LoadVertexOpts()) {
+        std::ifstream fin(path);
+        if (fin.fail()) LOG_ERROR("cannot open graph vertex file: ", path);
+        std::string line;
+        std::vector<parse_t> splits;
+        while (std::getline(fin, line)) {
+            if (utils::StrStartWith(line, opts.comment_prefix)) continue;
+            char* save = nullptr;
+            char* tok = strtok_r(line.data(), opts.vertex_sep.c_str(), &save);
+            if (!tok) continue;  // blank line
+            index_t vid = index_t(std::strtoul(tok, nullptr, 10));
+            if (reorder_vid_) vid = renumber_(vid);
+            if constexpr (std::is_same_v<parse_t, char*>) {
+                if (!parser(vid, save)) LOG_WARNING("can not decode vertex data of vertex ", vid);
+            } else {
+                static_assert(std::is_integral_v<parse_t> || std::is_floating_point_v<parse_t>);
+                splits.clear();
+                for (tok = strtok_r(nullptr, opts.vdata_sep.c_str(), &save); tok;
+                     tok = strtok_r(nullptr, opts.vdata_sep.c_str(), &save)) {
+                    if constexpr (std::is_integral_v<parse_t>)
+                        splits.push_back(parse_t(std::strtoul(tok, nullptr, 10)));
+                    else
+                        splits.push_back(parse_t(std::strtod(tok, nullptr)));
+                }
+                if (!parser(vid, splits))
+                    LOG_WARNING("can not decode vertex data of vertex ", vid, ": ", utils::VecToString(splits));
+            }
+        }
+    }
+
+    // One value per vertex from "vid value" lines (reference:
+    // loader/graph_loader.h:203-227); vertices without a line keep 0.  An id
+    // at or beyond num_vertices is skipped with a warning (the reference
+    // writes past the end of its vector).
+    template <arch_t arch, typename vdata_t>
+    DenseVec<arch, vdata_t, index_t> LoadVertexVecFromTxt(const std::string& path, index_t num_vertices,
+                                                          const LoadVertexOpts& opts = LoadVertexOpts()) {
+        static_assert(std::is_integral_v<vdata_t> || std::is_floating_point_v<vdata_t>);
+        DenseVec<arch_t::cpu, vdata_t, index_t> h(num_vertices);
+        LoadVertexStatusFromTxt<char*>(
+            path,
+            [&](index_t vid, char* rest) {
+                if (vid >= num_vertices) return false;
+                if constexpr (std::is_integral_v<vdata_t>)
+                    h[vid] = vdata_t(std::strtoul(rest, nullptr, 10));
+                else
+                    h[vid] = vdata_t(std::strtod(rest, nullptr));
+                return true;
+            },
+            opts);
+        if constexpr (arch == arch_t::cpu)
+            return h;
+        else
+            return h.template to<arch>();
+    }
+
     /// maps an id of the file to its renumbered id; false when it never appeared
     bool ReorderedVid(index_t& vid) const {
         if (!reorder_vid_) return true;
