@@ -1,6 +1,7 @@
 // Prints the CSR that the drop-in GraphOne loader (include/GraphOne/loader/
 // loader.h) builds from an .adj file: for the out-edge then the in-edge
-// orientation, a line "n m" and the row offsets, columns and values.
+// orientation, a line "n m" and the row offsets, columns and values, then
+// the same for GraphLoader::LoadCsrFromTxt (out-edge CSR).
 // Usage: loader_driver FILE.adj DIRECTED REORDER KEEP_SELF KEEP_DUP (each 0|1)
 #include <cstdio>
 
@@ -32,5 +33,15 @@ int main(int argc, char** argv) {
         for (auto x : v) std::printf("%u ", (unsigned)x);
         std::printf("\n");
     }
+    // LoadCsrFromTxt: the out-edge CSR straight from the file
+    GraphLoader<vstart_t::FROM_0_TO_0> loader2(argv[3][0] == '1');
+    auto csr = loader2.LoadCsrFromTxt<arch_t::cpu, uint32_t>(argv[1], opts);
+    std::printf("%u %llu\n", (unsigned)csr.n_rows, (unsigned long long)csr.nnz);
+    for (size_t i = 0; i < csr.row_offsets.size(); ++i) std::printf("%llu ", (unsigned long long)csr.row_offsets[i]);
+    std::printf("\n");
+    for (size_t i = 0; i < csr.col_indices.size(); ++i) std::printf("%u ", (unsigned)csr.col_indices[i]);
+    std::printf("\n");
+    for (size_t i = 0; i < csr.values.size(); ++i) std::printf("%u ", (unsigned)csr.values[i]);
+    std::printf("\n");
     return 0;
 }
