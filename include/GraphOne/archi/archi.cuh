@@ -1,7 +1,7 @@
 #pragma once
 // Parallel primitives of the GraphOne API (reference: archi/thrust/
 // functions.h:17-104 over Thrust, archi/only/cuda.cuh:37-99, archi/mem/
-// def.hpp:8-42, archi/thrust/def.hpp:9-27).  The element-wise ones (fill,
+// def.hpp:9-43, archi/thrust/def.hpp:9-27).  The element-wise ones (fill,
 // transform, for_each, transform_reduce) are this library's own grid-stride
 // kernels on the default stream; iterators may be raw pointers or any
 // random-access iterator usable in device code (thrust::counting_iterator

@@ -1,7 +1,7 @@
 #pragma once
 // The semiring SpMV operator of the GraphOne API (reference:
-// archi/blas/spmv/def.hpp:7-91, cpu/cpu.hpp:8-33, cpu/naive.hpp:5-20,
-// cuda/cuda.cuh:10-143):
+// archi/blas/spmv/def.hpp:8-76, cpu/cpu.hpp:8-33, cpu/naive.hpp:5-20,
+// cuda/cuda.cuh:10-104):
 //
 //     y[r] = fold of functor_t::reduce over the nonzeros (r, c) of A of
 //            functor_t::combine(A[r][c], x[c]), from functor_t::initialize()

@@ -1,6 +1,6 @@
 #pragma once
-// Error checks of the GraphOne API (reference: archi/check/check.h:9-23,
-// archi/check/cuda.cuh:8-21).  Here a failed CUDA call is always reported
+// Error checks of the GraphOne API (reference: archi/check/check.h:10-20,
+// archi/check/cuda.cuh:7-19).  Here a failed CUDA call is always reported
 // and ends the program (the reference stays silent unless DEBUG_CUDA is
 // defined).
 

@@ -1,6 +1,6 @@
 #pragma once
 // Kernel launches of the GraphOne API (reference: archi/kernel/def.hpp:7-28,
-// archi/kernel/cuda.cuh:8-106):
+// archi/kernel/cuda.cuh:11-99):
 //
 //   archi::LaunchKernel<arch, tparams>(LaunchParams<arch>(n), kernel, args...);
 //   archi::LaunchSync<arch>();

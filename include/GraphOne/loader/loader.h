@@ -174,14 +174,14 @@ public:
         return cache;
     }
 
-    // LoadEdgesFromTxt then ToCsr (reference: loader/graph_loader.h:123-129).
+    // LoadEdgesFromTxt then ToCsr (reference: loader/graph_loader.h:124-129).
     template <arch_t arch, typename edata_t>
     CsrMat<arch, edata_t, index_t, offset_t, v_start> LoadCsrFromTxt(const std::string& path,
                                                                      const LoadEdgeOpts& opts = LoadEdgeOpts()) {
         return LoadEdgesFromTxt<edata_t>(path, opts).template ToCsr<arch>();
     }
 
-    // Per-vertex lines "vid data..." (reference: loader/graph_loader.h:131-201):
+    // Per-vertex lines "vid data..." (reference: loader/graph_loader.h:131-198):
     // lines starting with the comment prefix are skipped, the id is the first
     // token (renumbered like the edges when reordering is on), and the parser
     // gets either the rest of the line (parse_t = char*) or its tokens parsed
@@ -219,7 +219,7 @@ public:
     }
 
     // One value per vertex from "vid value" lines (reference:
-    // loader/graph_loader.h:203-227); vertices without a line keep 0.  An id
+    // loader/graph_loader.h:199-223); vertices without a line keep 0.  An id
     // at or beyond num_vertices is skipped with a warning (the reference
     // writes past the end of its vector).
     template <arch_t arch, typename vdata_t>

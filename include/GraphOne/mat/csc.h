@@ -1,5 +1,5 @@
 #pragma once
-// Column-compressed matrices of the GraphOne API (reference: mat/csc.h:8-62):
+// Column-compressed matrices of the GraphOne API (reference: mat/csc.h:9-58):
 // col_offsets (n_cols + 1), row_indices and values (nnz each).
 
 #include <cstdint>

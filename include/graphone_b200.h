@@ -136,14 +136,14 @@ size_t g1_graph_device_bytes(const g1_graph* g);
 /* Merge-path partition of one orientation into tiles of `items_per_tile`
  * merge items (rows + nonzeros; 0 = the orientation's current default),
  * cached in the graph (replaces the SpmvDispatcher<SpmvCudaCsrMergeBased>
- * constructor's SegmentSearch, archi/blas/spmv/cuda/cuda.cuh:152-169).
+ * constructor's SegmentSearch, archi/blas/spmv/cuda/cuda.cuh:75-92).
  * The arrays stay owned by the graph: tile_row/tile_nnz have n_tiles+1
  * entries; carry/tail have room for n_tiles+1 values of up to 16 bytes. */
 g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t items_per_tile,
                        uint32_t* n_tiles, const uint32_t** tile_row,
                        const uint32_t** tile_nnz, void** carry, void** tail);
 /* y = A (semiring) x over one orientation (replaces SpmvDispatcher::operator(),
- * archi/blas/spmv/cuda/cuda.cuh:171-176; y stays on the device stream, no
+ * archi/blas/spmv/cuda/cuda.cuh:94-99; y stays on the device stream, no
  * device synchronisation). x, y device pointers of n entries. */
 g1_status g1_spmv(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
                   const void* x, void* y, void* stream);
