@@ -24,7 +24,7 @@ runs, and the ranks are read back to the host (g1_pagerank into host memory).
 SpMV + apply/construct kernel of the schedule in use, by default
 spmv_nnz_kernel) per launch over its CUDA-event duration, against the
 measured HBM copy bandwidth; ``traffic`` is the DRAM bytes per launch ncu
-measured for that kernel (profiles/spmv_nnz_pagerank_rmat22_traffic.md).
+measured for that kernel (a capture summary under profiles/).
 ``queries``: plain and batched SSSP/BFS (RMAT-14, RMAT-20 k=256, 4096^2
 grid); ``serving``: the serving loop over 8 resident graphs vs plain
 per-request execution.
@@ -204,7 +204,41 @@ def _pct(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q))
 
 
-def query_metrics(dev, stream, budget_queries: int = 256):
+class Parity:
+    """Checks of this run's own results against the oracle at the workload
+    sizes.  The oracle is the checker here, never the thing timed: its calls
+    run on host threads (ctypes releases the GIL) while the GPU works, and
+    their results are compared after the timed regions.
+
+    ``expect(key, fn, args, check)`` starts ``fn(*args)`` on the pool;
+    ``finish()`` waits and stores ``check(fn's result)`` under ``key``."""
+
+    def __init__(self, threads: int):
+        from concurrent.futures import ThreadPoolExecutor
+        self.pool = ThreadPoolExecutor(max_workers=max(2, threads))
+        self.pending = []
+        self.results = {}
+
+    def expect(self, key, fn, args, check):
+        self.pending.append((key, self.pool.submit(fn, *args), check))
+
+    def put(self, key, value):
+        self.results[key] = value
+
+    def finish(self):
+        for key, fut, check in self.pending:
+            self.results[key] = check(fut.result())
+        self.pending = []
+        self.pool.shutdown()
+        return self.results
+
+
+def _host_u32(t):
+    """Device int32 tensor -> host numpy uint32 (a copy)."""
+    return t.cpu().numpy().view(np.uint32).copy()
+
+
+def query_metrics(dev, stream, parity, ref_gpu=False, budget_queries: int = 256):
     """The query side of the metric, on resident graphs, CUDA-event timed.
 
     * RMAT-14 (symmetrised, uint32 weights [1,64]) plain SSSP, one source at
@@ -212,13 +246,24 @@ def query_metrics(dev, stream, budget_queries: int = 256):
       (directed CSR edges of reachable vertices / median time), for the BLAS
       (min-plus SpMV), advance/filter and push/pull engines.
     * RMAT-20 (same shape) k=256 sources: plain engine queries/s over 64 of
-      the sources vs one batched k=256 pass (bit-exact spot checks).
+      the sources vs one batched k=256 pass.
     * 4096^2 grid (uint32 weights [1,100]) SSSP and BFS from the corner on the
       near-far and advance engines (GTEPS = directed CSR edges / time).
+
+    Parity (into `parity`): RMAT-14 SSSP from vertex 0 on every engine vs the
+    oracle's Dijkstra; all 256 batched BFS/SSSP results vs 256 plain runs,
+    and 8 of each vs the oracle's BFS / Dijkstra; the grid's SSSP and BFS
+    from the corner on both engines vs the oracle.
+
+    With `ref_gpu`, GraphOne's own GPU engines (oracle/_ref, built from the
+    reference sources) run the same RMAT-14 queries (sparse-frontier BLAS
+    engine) and the grid query (advance/filter engine), CUDA-event timed, and
+    their distances join the parity checks.
     """
     import torch
     import graphone_b200 as g1
     from graphone_b200 import gen
+    from oracle import oracle as O
     out = {}
 
     g = gen.rmat(14, 16, symmetric=True, weights=(1, 64), device=dev)
@@ -228,6 +273,7 @@ def query_metrics(dev, stream, budget_queries: int = 256):
     srcs = gen.pick_sources(g, budget_queries)
     d = torch.empty(g.n, dtype=torch.int32, device=dev)
     plain = {}
+    got14 = {}
     for name, eng in (("blas", g1.ENGINE_BLAS), ("advance", g1.ENGINE_ADVANCE),
                       ("auto", g1.ENGINE_AUTO)):
         for s in srcs[:8]:
@@ -236,6 +282,7 @@ def query_metrics(dev, stream, budget_queries: int = 256):
                for s in srcs]
         G.sssp(0, eng, out=d, stream=stream)
         torch.cuda.synchronize()
+        got14[name] = _host_u32(d)
         reach_edges = int(deg[d != -1].sum().item())
         t0 = _event_ms(lambda: G.sssp(0, eng, out=d, stream=stream), stream)
         plain[name] = {"p50_ms": round(_pct(lat, 50), 4), "p99_ms": round(_pct(lat, 99), 4),
@@ -243,6 +290,23 @@ def query_metrics(dev, stream, budget_queries: int = 256):
                        "src0_ms": round(t0, 4),
                        "src0_gteps": round(reach_edges / (t0 / 1e3) / 1e9, 3)}
     out["sssp_rmat14_plain"] = {"n": g.n, "m": g.m, "queries": len(srcs), **plain}
+    if ref_gpu:
+        # GraphOne's own sparse-frontier BLAS engine on the same graph and sources
+        trp14, tci14, tv14 = g.np("t")
+        O.refgpu_sssp_blas(trp14, tci14, tv14, srcs[:8])          # warm-up
+        d0, ms_r, it_r = O.refgpu_sssp_blas(trp14, tci14, tv14, np.concatenate([[0], srcs[:64]]))
+        lat_r = ms_r[1:]
+        got14["reference_gpu_blas"] = d0
+        r = {"engine": "GraphOne BlasGcEngine<SPARSE> + merge-based SpMV (Run<>, u32 min-plus)",
+             "p50_ms": round(_pct(lat_r, 50), 4), "p99_ms": round(_pct(lat_r, 99), 4),
+             "queries_per_s": round(1e3 / statistics.mean(lat_r), 1),
+             "src0_ms": round(float(ms_r[0]), 4), "src0_iterations": int(it_r[0]),
+             "queries": len(lat_r)}
+        r["ours_auto_over_reference_p50"] = round(r["p50_ms"] / plain["auto"]["p50_ms"], 2)
+        r["ours_blas_over_reference_p50"] = round(r["p50_ms"] / plain["blas"]["p50_ms"], 2)
+        out["sssp_rmat14_plain"]["reference_gpu"] = r
+    parity.expect("sssp_rmat14_src0_bit_exact", O.dijkstra_u32, (*g.np("n"), 0),
+                  lambda ref, got=got14: {k: bool(np.array_equal(v, ref)) for k, v in got.items()})
     G.close()
     del g, G, d
     torch.cuda.empty_cache()
@@ -251,9 +315,11 @@ def query_metrics(dev, stream, budget_queries: int = 256):
     # stored in decreasing-degree order (G1_GRAPH_RELABEL) for both engines
     G = g1.Graph.from_gen(g, relabel=True)
     srcs = gen.pick_sources(g, 256)
+    rp20, ci20, v20 = g.np("n")
     one = torch.empty(g.n, dtype=torch.int32, device=dev)
     blk = torch.empty((256, g.n), dtype=torch.int32, device=dev)
     res = {"n": g.n, "m": g.m, "k": 256, "layout": "relabelled by degree (both engines)"}
+    n_oracle = 8
     for kind in ("bfs", "sssp"):
         single = G.bfs if kind == "bfs" else G.sssp
         batch = G.bfs_batch if kind == "bfs" else G.sssp_batch
@@ -263,17 +329,27 @@ def query_metrics(dev, stream, budget_queries: int = 256):
                for s in srcs[:nq]]
         batch(srcs, out=blk, stream=stream)
         tb = _event_ms(lambda: batch(srcs, out=blk, stream=stream), stream)
-        ok = True
-        for i in (0, 100, 255):
+        # every batched result against its plain single-source run
+        same = 0
+        for i in range(256):
             single(int(srcs[i]), out=one, stream=stream)
             torch.cuda.synchronize()
-            ok &= bool(torch.equal(one, blk[i]))
+            same += int(torch.equal(one, blk[i]))
+        parity.put(f"{kind}_rmat20_k256_batched_eq_plain", f"{same}/256")
+        # and n_oracle of them against the oracle
+        picks = np.linspace(0, 255, n_oracle).astype(int)
+        for i in picks:
+            got = _host_u32(blk[i])
+            fn, args = ((O.bfs, (rp20, ci20, int(srcs[i]))) if kind == "bfs"
+                        else (O.dijkstra_u32, (rp20, ci20, v20, int(srcs[i]))))
+            parity.expect(f"{kind}_rmat20_k256_vs_oracle#{i}", fn, args,
+                          lambda ref, got=got: bool(np.array_equal(got, ref)))
         qp = 1e3 / statistics.mean(lat)
         qb = 256 * 1e3 / tb
         res[kind] = {"plain_queries_per_s": round(qp, 1), "plain_p50_ms": round(_pct(lat, 50), 4),
                      "plain_p99_ms": round(_pct(lat, 99), 4),
                      "batched_queries_per_s": round(qb, 1), "batched_ms_per_256": round(tb, 3),
-                     "batched_over_plain": round(qb / qp, 2), "spot_bit_exact": ok}
+                     "batched_over_plain": round(qb / qp, 2)}
     out["batch_rmat20_k256"] = res
     G.close()
     del g, G, one, blk
@@ -283,9 +359,10 @@ def query_metrics(dev, stream, budget_queries: int = 256):
     # near-far engine (what ENGINE_AUTO picks here) vs the advance engine
     g = gen.grid2d(4096, 4096, (1, 100), device=dev)
     G = g1.Graph.from_gen(g)
+    rpg, cig, vg = g.np("n")
     d = torch.empty(g.n, dtype=torch.int32, device=dev)
     res = {"n": g.n, "m": g.m, "source": 0}
-    ref = None
+    got = {"sssp": {}, "bfs": {}}
     for kind in ("sssp", "bfs"):
         fn = G.sssp if kind == "sssp" else G.bfs
         for name, eng in (("nearfar", g1.ENGINE_NEARFAR), ("advance", g1.ENGINE_ADVANCE)):
@@ -295,16 +372,26 @@ def query_metrics(dev, stream, budget_queries: int = 256):
             def run(fn=fn, eng=eng):
                 it[0] = fn(0, eng, out=d, stream=stream, return_iters=True)[1]
             ms = _event_ms(run, stream)
-            if kind == "sssp":
-                if ref is None:
-                    ref = d.clone()
-                elif not torch.equal(ref, d):
-                    res["sssp_engines_disagree"] = True
+            got[kind][name] = _host_u32(d)
             res[f"{kind}_{name}"] = {"ms": round(ms, 2), "iterations": int(it[0]),
                                     "gteps": round(g.m / (ms / 1e3) / 1e9, 3)}
+    if ref_gpu:
+        # GraphOne's own advance/filter engine (sssp_adv) from the corner
+        dref, ms_r, it_r = O.refgpu_sssp_adv(rpg, cig, vg, [0, 0])
+        got["sssp"]["reference_gpu_advance"] = dref
+        r = {"engine": "GraphOne AdvanceGC (Run<>, u32 atomicMin relax + visited filter)",
+             "ms": [round(float(x), 2) for x in ms_r], "iterations": int(it_r[-1])}
+        best = float(min(ms_r))
+        r["ours_advance_over_reference"] = round(best / res["sssp_advance"]["ms"], 2)
+        r["ours_nearfar_over_reference"] = round(best / res["sssp_nearfar"]["ms"], 2)
+        res["reference_gpu_sssp_advance"] = r
+    parity.expect("sssp_grid4096_src0_bit_exact", O.dijkstra_u32, (rpg, cig, vg, 0),
+                  lambda ref, r=got["sssp"]: {k: bool(np.array_equal(v, ref)) for k, v in r.items()})
+    parity.expect("bfs_grid4096_src0_bit_exact", O.bfs, (rpg, cig, 0),
+                  lambda ref, r=got["bfs"]: {k: bool(np.array_equal(v, ref)) for k, v in r.items()})
     out["sssp_grid4096"] = res
     G.close()
-    del g, G, d, ref
+    del g, G, d
     torch.cuda.empty_cache()
     return out
 
@@ -423,7 +510,7 @@ def kernel_name(variant: int) -> str:
     return f"{base}<PlusTimesF32, PrEpilogue> (merge variant {variant})"
 
 
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "spmv_nnz_pagerank_rmat22_traffic.md")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "spmv_nnz_pagerank_rmat22_traffic.txt")
 
 
 def measured_traffic(variant: int, path: str = TRAFFIC_FILE):
@@ -459,7 +546,22 @@ def run_ours(args):
 
     g = make_pagerank_graph(args.scale, dev)
     n, m = g.n, g.m
-    trp, tci, tv = g.np("t")              # host copies (for e2e and cpu baseline)
+    trp, tci, tv = g.np("t")              # host copies (for e2e, parity and cpu baseline)
+    parity = Parity(min(8, cpu_threads()))
+    iters = args.iters
+    pr_got = {}
+    if rank != 0:
+        args.no_parity = True             # rank 0 checks its own replica's results
+    use_ref_gpu = not args.no_reference_gpu and ws == 1 and _refgpu_available()
+    rpn = cin = vn = None
+    if use_ref_gpu:
+        rpn, cin, vn = g.np("n")          # GraphOne's PageRank reads out-degrees from the CSR
+    if not args.no_parity:
+        from oracle import oracle as O
+        # FP64 PageRank of the same graph, computed on host threads while the GPU runs
+        parity.expect(f"pagerank_rmat{args.scale}_rel_l1_vs_fp64", O.pagerank_f64,
+                      (trp, tci, tv, 0.85, iters, 1),
+                      lambda r64: float(O.rel_l1(pr_got["rank"], r64)))
     # pinned host buffers for the end-to-end path
     h_rp = torch.from_numpy(trp.view(np.int32)).pin_memory()
     h_ci = torch.from_numpy(tci.view(np.int32)).pin_memory()
@@ -473,7 +575,6 @@ def run_ours(args):
                           relabel=not args.no_relabel)
     sched_note, variant = apply_schedule(G, args.sched, stream)
     out = torch.empty(n, dtype=torch.float32, device=dev)
-    iters = args.iters
 
     def step():
         G.pagerank(0.85, iters, g1.PR_DANGLING, out=out, stream=stream)
@@ -498,6 +599,7 @@ def run_ours(args):
     barrier(ws)
     launches = g1.kernel_launches() - launches0
     ms = e0.elapsed_time(e1)
+    pr_got["rank"] = out.cpu().numpy().copy()   # the timed steps' ranks (caller order)
     ms_max = max_over_ranks(ms, ws)
     per_step_bytes = spmv_bytes(n, m) * iters
     value = job_rate(per_step_bytes, args.steps, ms_max, ws) / 1e9
@@ -527,7 +629,6 @@ def run_ours(args):
     h2d = 4 * (n + 1) + 8 * m
     d2h = 4 * n
 
-    # parity spot check of this very run against the FP64 oracle (small cost)
     result = {
         "metric": METRIC,
         "value": round(value, 1),
@@ -574,11 +675,31 @@ def run_ours(args):
             "avg_launch_ms": round(avg_ms, 5), "launches_timed": int(spmv_launches),
             "iteration_share_of_step": round(spmv_ms / ms, 4) if ms > 0 else None,
         }
+    if use_ref_gpu:
+        # our PageRank with GraphOne's own formula (no dangling redistribution),
+        # to compare with GraphOne's GPU engine on the same graph
+        G.pagerank(0.85, iters, g1.PR_REFERENCE, out=out, stream=stream)
+        torch.cuda.synchronize()
+        pr_got["rank_reference_formula"] = out.cpu().numpy().copy()
     G.close()
+    del G, out
+    torch.cuda.empty_cache()
+    if use_ref_gpu:
+        result["reference_gpu"] = reference_gpu_pagerank(args, rpn, cin, vn, trp, tci, tv,
+                                                         result, pr_got, parity)
+        del rpn, cin, vn
     if not args.no_queries:
-        result["queries"] = query_metrics(dev, stream)
+        result["queries"] = query_metrics(dev, stream, parity, ref_gpu=use_ref_gpu)
     if args.serve_requests > 0:
         result["serving"] = serving_metrics(dev, args.serve_requests, args.serve_rate)
+    if not args.no_parity:
+        p = parity.finish()
+        key = f"pagerank_rmat{args.scale}_rel_l1_vs_fp64"
+        p["pagerank_tolerance"] = 1e-6
+        p["pagerank_within_tolerance"] = bool(p[key] < 1e-6)
+        result["parity"] = p
+    else:
+        parity.finish()
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(trp, tci, tv, n, m, args)
     if rank == 0:
@@ -586,6 +707,47 @@ def run_ours(args):
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def _refgpu_available():
+    try:
+        from oracle import oracle as O
+        return O.refgpu() is not None
+    except Exception:
+        return False
+
+
+def reference_gpu_pagerank(args, rpn, cin, vn, trp, tci, tv, result, pr_got, parity):
+    """GraphOne's own GPU engine for PageRank on the same graph (oracle/_ref,
+    built from the reference sources for sm_100a): its all-active BLAS engine
+    (Run<> over the merge-based SpMV dispatcher and apply_construct_kernel),
+    GraphOne's formula, the same iteration count, CUDA-event timed; and its
+    SpMV dispatcher alone per call.  Ours is compared per SpMV launch (the
+    metric's kernel) and per whole PageRank."""
+    from oracle import oracle as O
+    n, m = len(trp) - 1, len(tci)
+    iters = args.iters
+    rank_ref, ms_runs, ms_spmv = O.refgpu_pagerank(rpn, cin, vn, trp, tci, tv, 0.85, iters,
+                                                   reps=3, spmv_reps=10)
+    spmv_ms = float(np.median(ms_spmv))
+    run_ms = float(np.min(ms_runs))
+    ours_spmv_ms = result.get("roofline", {}).get("avg_launch_ms")
+    r = {"engine": ("GraphOne BlasGcEngine<ALL_ACTIVE> (Run<>, SpmvDispatcher<SpmvCudaCsrMergeBased> "
+                    "+ apply_construct_kernel), GraphOne's PageRank formula, fixed iterations"),
+         "iterations": iters, "run_ms": [round(float(x), 3) for x in ms_runs],
+         "spmv_ms_per_call_median": round(spmv_ms, 5),
+         "spmv_gbs": round(spmv_bytes(n, m) / (spmv_ms / 1e3) / 1e9, 1),
+         "pagerank_gbs": round(spmv_bytes(n, m) * iters / (run_ms / 1e3) / 1e9, 1)}
+    if ours_spmv_ms:
+        r["ours_over_reference_spmv_launch"] = round(spmv_ms / ours_spmv_ms, 2)
+    r["ours_over_reference_pagerank"] = round(run_ms / result["ms_per_step"], 2)
+    if not args.no_parity:
+        ours = pr_got["rank_reference_formula"]
+        parity.expect("pagerank_reference_formula_rel_l1_vs_fp64", O.pagerank_f64,
+                      (trp, tci, tv, 0.85, iters, 0),
+                      lambda r64, a=ours, b=rank_ref: {"ours": float(O.rel_l1(a, r64)),
+                                                       "reference_gpu": float(O.rel_l1(b, r64))})
+    return r
 
 
 def cpu_threads():
@@ -694,6 +856,10 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-relabel", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the checks of this run's results against the oracle")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing GraphOne's own GPU engines on the same inputs")
     ap.add_argument("--no-queries", action="store_true",
                     help="skip the SSSP/BFS plain and batched query measurements")
     ap.add_argument("--serve-requests", type=int, default=256,

@@ -20,8 +20,8 @@ def test_traffic_summary_is_read_for_the_captured_variant_only():
 
 
 def test_traffic_summary_missing_or_malformed(tmp_path):
-    assert bench.measured_traffic(17, str(tmp_path / "absent.md")) is None
-    p = tmp_path / "s.md"
+    assert bench.measured_traffic(17, str(tmp_path / "absent.txt")) is None
+    p = tmp_path / "s.txt"
     p.write_text("variant: 17\n")
     assert bench.measured_traffic(17, str(p)) is None
     p.write_text("variant: 17\ndram_bytes_per_launch: 123\n")
