@@ -21,12 +21,17 @@
 // writes tile_row/tile_nnz, the tile kernel writes carry/tail of every tile)
 // before reading it, so stale contents from an earlier call are never used.
 //
-// The first call on each device looks up the array's device address with
-// cudaGetSymbolAddress (with that device current) and caches it; make that
-// first call before any stream capture.
+// Every call looks up the array's device address with cudaGetSymbolAddress,
+// with the calling device current, and passes that address to the kernels.
+// The address is not cached: after cudaDeviceReset (or any other teardown of
+// the primary context) the module is loaded again and the array may move.
+// The library is compiled without relocatable device code and CUDA loads
+// modules lazily by default, so the first call on a device (in a context)
+// loads this file's module: the driver then allocates the 4 MiB array and
+// the module's code on that device.  Make that first call at set-up time,
+// before any stream capture, or set CUDA_MODULE_LOADING=EAGER to load the
+// module when the library's CUDA context starts.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "g1/semiring.cuh"
 #include "g1/spmv.cuh"
@@ -49,26 +54,14 @@ constexpr size_t kNoAllocWords = 4 * ((size_t)kNoAllocMaxTiles + 1);
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
 
-// Device address of the scratch array, per device, set up on the first call
-// made on that device (cudaGetSymbolAddress with the device current).  In host
-// code g_noalloc_scratch names a host-side stand-in, never a device address:
-// only these looked-up pointers are passed to kernels.
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-uint32_t* g_scratch_addr[kMaxDevices] = {};
-
+// Device address of the scratch array on the current device, looked up on
+// every call.  In host code g_noalloc_scratch names a host-side stand-in,
+// never a device address: only the looked-up pointer is passed to kernels.
 g1_status scratch_for_current_device(uint32_t** out) {
-    int dev = 0;
-    G1_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return fail(G1_ERR_UNSUPPORTED, "device index too large");
-    std::lock_guard<std::mutex> lk(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return fail_cuda(e, "cudaGetSymbolAddress(scratch)");
-        g_scratch_addr[dev] = static_cast<uint32_t*>(p);
-    }
-    *out = g_scratch_addr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaGetSymbolAddress(scratch)");
+    *out = static_cast<uint32_t*>(p);
     return G1_OK;
 }
 
@@ -92,11 +85,11 @@ g1_status run_noalloc(const uint32_t* row_ptr, const uint32_t* col, const void* 
     a.carry = reinterpret_cast<typename SR::value_t*>(scratch + 2 * stride);
     a.tail = reinterpret_cast<typename SR::value_t*>(scratch + 3 * stride);
     a.err = nullptr;
+    int sms = 0, dev = 0;
+    G1_CUDA(cudaGetDevice(&dev));
+    G1_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     merge_partition_kernel<<<(unsigned)ceil_div((uint64_t)n_tiles + 1, 256), 256, 0, s>>>(
         row_ptr, n, m, kNoAllocItems, n_tiles, scratch, scratch + stride);
-    int sms = 148, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t grid = (uint32_t)std::max<uint64_t>(
         1, std::min<uint64_t>(ceil_div(n_tiles, kNoAllocWarps), (uint64_t)sms * 8));
     using L = WarpMergeLayout<SR, kNoAllocWarps, kNoAllocIpt, 0>;

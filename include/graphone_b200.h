@@ -169,9 +169,12 @@ g1_status g1_graph_set_schedule(g1_graph* g, int transpose, g1_schedule sched, i
  * caller's device buffers; nothing is allocated and no g1_graph is needed.
  * Scratch (merge-path partition and per-tile carries) lives in one
  * file-scope device array of 4 MiB per GPU, held until the process exits:
- * n + m may be at most 58,720,256 (G1_ERR_INVALID beyond).  The first call
- * on a device looks up that array's device address; make that first call
- * before any stream capture.  Every call shares the array and it keeps the
+ * n + m may be at most 58,720,256 (G1_ERR_INVALID beyond).  Each call
+ * looks up that array's device address on the current device.  The first
+ * call on a device (in a CUDA context) loads the library module holding the
+ * array: the driver then allocates its 4 MiB and the module's code there.
+ * Make that first call at set-up time, before any stream capture, or set
+ * CUDA_MODULE_LOADING=EAGER.  Every call shares the array and it keeps the
  * last call's contents (each call rewrites what it reads, nothing needs
  * zeroing); calls that overlap on the GPU race on it: serialise them (one
  * stream). */
