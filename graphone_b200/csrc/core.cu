@@ -754,6 +754,7 @@ g1_status check_device_error(g1_graph* g, cudaStream_t s) {
     G1_CUDA(cudaMemsetAsync(g->err_word, 0, 4, s));
     if (h == kDevTimeout) return fail(G1_ERR_TIMEOUT, "a bounded device wait ran out");
     if (h == kDevOverflow) return fail(G1_ERR_OVERFLOW, "a device queue overflowed");
+    if (h == kDevInvalid) return fail(G1_ERR_INVALID, "a vertex id in the input was out of range");
     return fail(G1_ERR_DEVICE, "device error word " + std::to_string(h));
 }
 

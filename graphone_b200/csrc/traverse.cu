@@ -87,15 +87,26 @@ __device__ __forceinline__ void relax(uint32_t du, uint32_t v, uint32_t w, uint3
     }
 }
 
+// A frontier entry the advance may expand: an id below n (otherwise the
+// device error word records kDevInvalid and the entry is skipped; frontiers
+// the engines build are always in range, g1_advance_run's come from the
+// caller) whose distance is finite (an unreached vertex has nothing to push:
+// MAX + w would wrap).
+__device__ __forceinline__ bool frontier_vertex_ok(uint32_t u, uint32_t n, uint32_t* err) {
+    if (u < n) return true;
+    set_error(err, kDevInvalid);
+    return false;
+}
+
 // Advance over the frontier: TPV lanes per vertex for short adjacency lists
 // (TPV the power of two at or above the frontier's mean degree, so a small
 // frontier of low-degree vertices still gets about a thread per edge), the
 // whole warp for lists of 32 or more edges (coalesced col/val reads).
 template <bool UNIT, int TPV>
 __global__ void __launch_bounds__(256)
-tr_advance_kernel(const uint32_t* F, uint32_t nF, const uint32_t* rp, const uint32_t* col,
+tr_advance_kernel(const uint32_t* F, uint32_t nF, uint32_t n, const uint32_t* rp, const uint32_t* col,
                   const uint32_t* val, uint32_t* dist, uint32_t* visited, uint32_t iter,
-                  uint32_t* out, uint32_t* out_count, unsigned long long* deg_sum) {
+                  uint32_t* out, uint32_t* out_count, unsigned long long* deg_sum, uint32_t* err) {
     constexpr uint32_t VPW = 32 / TPV;  // vertices per warp and round
     const uint32_t lane = lane_id();
     const uint32_t sub = lane % TPV, grp = lane / TPV;
@@ -104,13 +115,17 @@ tr_advance_kernel(const uint32_t* F, uint32_t nF, const uint32_t* rp, const uint
     const uint32_t rounds = (uint32_t)ceil_div(nF, (uint64_t)warps * VPW);
     for (uint32_t r = 0; r < rounds; ++r) {
         const uint32_t i = (r * warps + wid) * VPW + grp;
-        uint32_t u = 0, b = 0, e = 0;
+        uint32_t u = 0, b = 0, e = 0, du = 0;
         if (i < nF) {
             u = F[i];
-            b = rp[u];
-            e = rp[u + 1];
+            if (frontier_vertex_ok(u, n, err)) {
+                du = dist[u];
+                if (du != kU32Max) {
+                    b = rp[u];
+                    e = rp[u + 1];
+                }
+            }
         }
-        const uint32_t du = i < nF ? dist[u] : 0u;
         // long lists: cooperative, one list at a time
         unsigned big = __ballot_sync(0xffffffffu, sub == 0 && e - b >= 32);
         while (big) {
@@ -131,12 +146,20 @@ tr_advance_kernel(const uint32_t* F, uint32_t nF, const uint32_t* rp, const uint
     }
 }
 
-// Out-degrees of the frontier (deg[nF] = 0) for the edge-balanced advance.
-__global__ void tr_frontier_degrees_kernel(const uint32_t* F, uint32_t nF, const uint32_t* rp,
-                                           uint32_t* deg) {
+// Out-degrees of the frontier (deg[nF] = 0) for the edge-balanced advance;
+// 0 for an entry the advance skips (out of range, or unreached).
+__global__ void tr_frontier_degrees_kernel(const uint32_t* F, uint32_t nF, uint32_t n,
+                                           const uint32_t* rp, const uint32_t* dist, uint32_t* deg,
+                                           uint32_t* err) {
     const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= nF; i += stride)
-        deg[i] = i < nF ? rp[F[i] + 1] - rp[F[i]] : 0u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= nF; i += stride) {
+        uint32_t d = 0;
+        if (i < nF) {
+            const uint32_t u = F[i];
+            if (frontier_vertex_ok(u, n, err) && dist[u] != kU32Max) d = rp[u + 1] - rp[u];
+        }
+        deg[i] = d;
+    }
 }
 
 // Edge-balanced advance: the frontier's edges are numbered by the
@@ -161,6 +184,8 @@ tr_advance_lb_kernel(const uint32_t* F, uint32_t nF, const uint32_t* prefix, con
             const uint32_t mid = (lo + hi + 1) >> 1;
             if (prefix[mid] <= r) lo = mid; else hi = mid - 1;
         }
+        // entries the degree pass skipped have degree 0, so edge number r
+        // never lands on one: F[lo] is in range with a finite distance
         const uint32_t u = F[lo];
         const uint32_t k = rp[u] + (r - prefix[lo]);
         relax<UNIT>(dist[u], col[k], UNIT ? 1u : val[k], dist, visited, iter, out, out_count, rp,
@@ -256,8 +281,8 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
                     1, std::min<uint64_t>(ceil_div((uint64_t)nF * tpv, 256), (uint64_t)g->sm_count * 8));
                 count_launches(1);
 #define G1_TR_ADV(T)                                                                                    \
-    tr_advance_kernel<UNIT, T><<<gt, 256, 0, s>>>(st.F[cur], nF, o.rp, o.col, static_cast<const uint32_t*>(o.val), \
-                                                  st.dist, st.visited, it, st.F[cur ^ 1], st.cnt, deg_sum)
+    tr_advance_kernel<UNIT, T><<<gt, 256, 0, s>>>(st.F[cur], nF, n, o.rp, o.col, static_cast<const uint32_t*>(o.val), \
+                                                  st.dist, st.visited, it, st.F[cur ^ 1], st.cnt, deg_sum, g->err_word)
                 switch (tpv) {
                     case 1: G1_TR_ADV(1); break;
                     case 2: G1_TR_ADV(2); break;
@@ -268,7 +293,8 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
                 }
 #undef G1_TR_ADV
             } else {
-                tr_frontier_degrees_kernel<<<gf, 256, 0, s>>>(st.F[cur], nF, o.rp, st.deg);
+                tr_frontier_degrees_kernel<<<gf, 256, 0, s>>>(st.F[cur], nF, n, o.rp, st.dist, st.deg,
+                                                              g->err_word);
                 size_t tb = scan_bytes;
                 G1_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, tb, st.deg, st.prefix, (int)nF + 1, s));
                 const uint32_t ga = (uint32_t)std::max<uint64_t>(
@@ -328,8 +354,8 @@ static g1_status advance_step(g1_graph* g, const uint32_t* F, uint32_t nF, uint3
             (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div((uint64_t)nF * tpv, 256), cap));
         count_launches(1);
 #define G1_ADV_STEP(T)                                                                              \
-    tr_advance_kernel<UNIT, T><<<gt, 256, 0, s>>>(F, nF, o.rp, o.col, val, dist, visited, iter, out, \
-                                                  cnt, deg_sum)
+    tr_advance_kernel<UNIT, T><<<gt, 256, 0, s>>>(F, nF, g->n, o.rp, o.col, val, dist, visited, iter, out, \
+                                                  cnt, deg_sum, g->err_word)
         switch (tpv) {
             case 1: G1_ADV_STEP(1); break;
             case 2: G1_ADV_STEP(2); break;
@@ -348,7 +374,7 @@ static g1_status advance_step(g1_graph* g, const uint32_t* F, uint32_t nF, uint3
         unsigned char* scan_tmp = nullptr;
         G1_TRY(ws.get("adv_scan", scan_bytes + 16, &scan_tmp));
         const uint32_t gf = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div((uint64_t)nF + 1, 256), cap));
-        tr_frontier_degrees_kernel<<<gf, 256, 0, s>>>(F, nF, o.rp, deg);
+        tr_frontier_degrees_kernel<<<gf, 256, 0, s>>>(F, nF, g->n, o.rp, dist, deg, g->err_word);
         G1_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, deg, prefix, (int)nF + 1, s));
         tr_advance_lb_kernel<UNIT><<<(uint32_t)cap, 256, 0, s>>>(F, nF, prefix, o.rp, o.col, val, dist, visited,
                                                                  iter, out, cnt, deg_sum);

@@ -273,6 +273,13 @@ __device__ __forceinline__ uint32_t ld_generic_u32(const void* p) {
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
+// Brings [p, p + bytes) into L2 ahead of use with one bulk prefetch (the
+// TMA engine: no registers, nothing to wait for).  `p` must be 16-byte
+// aligned and `bytes` a multiple of 16; the range must lie inside one
+// allocation.
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 // Brings the line holding `p` into this SM's L1 ahead of use.
 __device__ __forceinline__ void prefetch_l1(const void* p) {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
@@ -289,6 +296,7 @@ enum DeviceError : uint32_t {
     kDevOk = 0,
     kDevTimeout = 1,      // a bounded spin-wait ran out
     kDevOverflow = 2,     // a frontier/queue would have exceeded its capacity
+    kDevInvalid = 3,      // a caller-supplied vertex id was out of range (skipped)
 };
 
 __device__ __forceinline__ void set_error(uint32_t* flag, uint32_t code) {
