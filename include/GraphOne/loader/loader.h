@@ -175,7 +175,7 @@ public:
     }
 
     // LoadEdgesFromTxt then ToCsr (reference: loader/graph_loader.h:124-129).
-    template <arch_t arch, typename edata_t>
+    template <arch_t arch, typename edata_t = double>
     CsrMat<arch, edata_t, index_t, offset_t, v_start> LoadCsrFromTxt(const std::string& path,
                                                                      const LoadEdgeOpts& opts = LoadEdgeOpts()) {
         return LoadEdgesFromTxt<edata_t>(path, opts).template ToCsr<arch>();

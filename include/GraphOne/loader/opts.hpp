@@ -17,7 +17,7 @@ struct LoadEdgeOpts {
 
     std::string ToString() const {
         return "LoadEdgeOpts{ file_ext: " + file_ext + ", comment_prefix: " + comment_prefix +
-               ", is_directed: " + utils::ToString(is_directed) +
+               ", line_sep: " + line_sep + ", is_directed: " + utils::ToString(is_directed) +
                ", keep_self_loop: " + utils::ToString(keep_self_loop) +
                ", keep_duplicate_edges: " + utils::ToString(keep_duplicate_edges) + " }";
     }

@@ -43,5 +43,11 @@ int main(int argc, char** argv) {
     std::printf("\n");
     for (size_t i = 0; i < csr.values.size(); ++i) std::printf("%u ", (unsigned)csr.values[i]);
     std::printf("\n");
+    // LoadCsrFromTxt with the arch argument alone: edge data defaults to double
+    GraphLoader<vstart_t::FROM_0_TO_0> loader3(argv[3][0] == '1');
+    auto csr_d = loader3.LoadCsrFromTxt<arch_t::cpu>(argv[1], opts);
+    constexpr bool is_double = std::is_same_v<typename decltype(csr_d)::value_type, double>;
+    std::printf("default-edata %u %llu %d\n", (unsigned)csr_d.n_rows, (unsigned long long)csr_d.nnz,
+                (int)is_double);
     return 0;
 }

@@ -113,6 +113,8 @@ def ours(driver, path, flags):
         n, m = map(int, lines[4 * t].split())
         arr = [np.array(lines[4 * t + k].split(), dtype=np.int64).astype(np.uint32) for k in (1, 2, 3)]
         out.append((n, m, *arr))
+    # LoadCsrFromTxt<arch> alone (edge data double by default): same shape
+    assert lines[12].split() == ["default-edata", str(out[2][0]), str(out[2][1]), "1"]
     return out
 
 
