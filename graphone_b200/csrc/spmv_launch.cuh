@@ -23,7 +23,7 @@ constexpr int kVectorBlock = 256;
 //           stages: bit 0 = L2 cache policies, bit 1 = three-tile software
 //           pipeline per warp, bit 2 = next-tile L1 prefetch, bit 3 / bit 4
 //           = next tile's col and val / col only staged in shared memory by
-//           bulk copies.
+//           bulk copies, stages / 32 = L2 prefetch distance in rounds.
 // `warps` per block (kind 0/2/3), `hot` x entries cached in shared memory,
 // `minb` resident blocks per SM the register budget is sized for.
 struct MergeVariant {
@@ -44,8 +44,9 @@ constexpr MergeVariant kMergeVariants[] = {
     {3, 8, 0, 32, 49152, 1},  {3, 8, 2, 24, 32768, 1},  {3, 8, 2, 16, 32768, 1},
     {3, 8, 3, 24, 32768, 1},  {3, 8, 4, 32, 32768, 1},  {3, 8, 4, 32, 16384, 1},
     {3, 8, 8, 32, 32768, 1},  {3, 8, 8, 32, 16384, 1},  {3, 8, 16, 32, 32768, 1},
-    {3, 8, 16, 32, 24576, 1}};
-constexpr int kNumMergeVariants = 28;
+    {3, 8, 16, 32, 24576, 1}, {3, 8, 32, 32, 32768, 1}, {3, 8, 64, 32, 32768, 1},
+    {3, 8, 128, 32, 32768, 1}, {3, 8, 66, 24, 32768, 1}};
+constexpr int kNumMergeVariants = 32;
 constexpr int kDefaultVariant = 17;
 
 template <class K>
@@ -122,12 +123,12 @@ struct WarpMergeKernel {
 };
 
 template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false,
-          bool PFL1 = false, int BULK = 0>
+          bool PFL1 = false, int BULK = 0, int PFL2 = 0>
 struct NnzKernel {
     using L = NnzLayout<SR, WARPS, HOT, BULK>;
     static int occupancy() {
         static int occ = [] {
-            auto k = spmv_nnz_kernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1, BULK>;
+            auto k = spmv_nnz_kernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1, BULK, PFL2>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
             return blocks_per_sm(k, WARPS * 32, L::BYTES);
         }();
@@ -242,10 +243,10 @@ NnzArgs<SR> nnz_args(const g1_graph* g, int t, const NnzPlan& p, const typename 
 }
 
 template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false,
-          bool PFL1 = false, int BULK = 0>
+          bool PFL1 = false, int BULK = 0, int PFL2 = 0>
 g1_status launch_nnz(g1_graph* g, int t, const NnzPlan& p, const typename SR::x_t* x,
                      const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
-    using K = NnzKernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1, BULK>;
+    using K = NnzKernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1, BULK, PFL2>;
     const NnzArgs<SR> a = nnz_args<SR>(g, t, p, x);
     // the tile kernel reads each lane's col/val with 32-byte loads
     if (((uintptr_t)a.col | (uintptr_t)a.val) & 31u)
@@ -255,7 +256,7 @@ g1_status launch_nnz(g1_graph* g, int t, const NnzPlan& p, const typename SR::x_
     // Both kernels use programmatic dependent launch (the fixup's empty rows
     // overlap the main kernel's tail), except while the main kernel is being
     // timed: its bracketing events would sit between the two.
-    auto mk = spmv_nnz_kernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1, BULK>;
+    auto mk = spmv_nnz_kernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1, BULK, PFL2>;
     auto fk = spmv_nnz_fixup_kernel<SR, Epi, kMergeBlock>;
     if (prof) {
         prof_mark(s, true);
@@ -297,6 +298,10 @@ g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_gri
             case 25: *main_grid = NnzKernel<SR, Epi, 32, 1, 16384, false, false, false, 1>::grid(g, q->n_tiles); break;
             case 26: *main_grid = NnzKernel<SR, Epi, 32, 1, 32768, false, false, false, 2>::grid(g, q->n_tiles); break;
             case 27: *main_grid = NnzKernel<SR, Epi, 32, 1, 24576, false, false, false, 2>::grid(g, q->n_tiles); break;
+            case 28: *main_grid = NnzKernel<SR, Epi, 32, 1, 32768, false, false, false, 0, 1>::grid(g, q->n_tiles); break;
+            case 29: *main_grid = NnzKernel<SR, Epi, 32, 1, 32768, false, false, false, 0, 2>::grid(g, q->n_tiles); break;
+            case 30: *main_grid = NnzKernel<SR, Epi, 32, 1, 32768, false, false, false, 0, 4>::grid(g, q->n_tiles); break;
+            case 31: *main_grid = NnzKernel<SR, Epi, 24, 1, 32768, false, true, false, 0, 2>::grid(g, q->n_tiles); break;
             default: *main_grid = NnzKernel<SR, Epi, 32, 1, 16384>::grid(g, q->n_tiles); break;
         }
         *fix_grid = nnz_fix_grid<SR, Epi>(g, *q);
@@ -400,6 +405,10 @@ g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi&
             case 25: return launch_nnz<SR, Epi, 32, 1, 16384, false, false, false, 1>(g, t, *q, x, main_epi, fix_epi, s);
             case 26: return launch_nnz<SR, Epi, 32, 1, 32768, false, false, false, 2>(g, t, *q, x, main_epi, fix_epi, s);
             case 27: return launch_nnz<SR, Epi, 32, 1, 24576, false, false, false, 2>(g, t, *q, x, main_epi, fix_epi, s);
+            case 28: return launch_nnz<SR, Epi, 32, 1, 32768, false, false, false, 0, 1>(g, t, *q, x, main_epi, fix_epi, s);
+            case 29: return launch_nnz<SR, Epi, 32, 1, 32768, false, false, false, 0, 2>(g, t, *q, x, main_epi, fix_epi, s);
+            case 30: return launch_nnz<SR, Epi, 32, 1, 32768, false, false, false, 0, 4>(g, t, *q, x, main_epi, fix_epi, s);
+            case 31: return launch_nnz<SR, Epi, 24, 1, 32768, false, true, false, 0, 2>(g, t, *q, x, main_epi, fix_epi, s);
             default: return launch_nnz<SR, Epi, 32, 1, 16384>(g, t, *q, x, main_epi, fix_epi, s);
         }
     }

@@ -1245,6 +1245,19 @@ __device__ __forceinline__ void nnz_issue(const NnzArgs<SR>& a, uint32_t tile, u
     if constexpr (!COL_ONLY) bulk_g2s(st + kBytes, a.val + j0, kBytes, bar);
 }
 
+// Lanes 0-3 of a warp: L2 prefetch of tile `tile`'s col and val (1 KB each,
+// one bulk prefetch each), its row-start bitmap words and its tile_seg word,
+// so that the tile's loads hit L2 instead of waiting for DRAM.
+template <class SR>
+__device__ __forceinline__ void nnz_prefetch_l2(const NnzArgs<SR>& a, uint32_t tile) {
+    const uint32_t lane = lane_id();
+    const size_t j0 = (size_t)tile * kNnzTile;
+    if (lane == 0) prefetch_l2_bulk(a.col + j0, kNnzTile * 4);
+    else if (lane == 1) prefetch_l2_bulk(a.val + j0, kNnzTile * 4);
+    else if (lane == 2) prefetch_l2(a.plan.sbits + (j0 >> 5));
+    else if (lane == 3) prefetch_l2(a.plan.tile_seg + tile);
+}
+
 // HINTS: col/val are streamed with an evict-first L2 policy, x gathers use
 // evict-last (x stays in L2 across the iteration).  PFL1: each warp
 // prefetches its next tile's col/val lines into L1.  PIPE: a three-tile
@@ -1255,9 +1268,10 @@ __device__ __forceinline__ void nnz_issue(const NnzArgs<SR>& a, uint32_t tile, u
 // registers or LSU work) while the current tile is gathered and folded; with
 // BULK 2 val is loaded at the tile start, its latency overlapping the x
 // gathers.  The wait on the mbarrier is bounded and reports a timeout
-// through the device error word.
+// through the device error word.  PFL2 > 0: each warp prefetches into L2
+// the tile it will fold PFL2 rounds later (nnz_prefetch_l2).
 template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false,
-          bool PFL1 = false, int BULK = 0>
+          bool PFL1 = false, int BULK = 0, int PFL2 = 0>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
 spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
     using V = typename SR::value_t;
@@ -1332,6 +1346,13 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
         epi.template block_end<WARPS * 32>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
         return;
     }
+    if constexpr (PFL2 > 0) {
+        // the first rounds' tiles, before the x cache fill
+        for (int d = 1; d < PFL2; ++d) {
+            const uint64_t pt = blockIdx.x * WARPS + w + (uint64_t)d * total_warps;
+            if (pt < n_tiles) nnz_prefetch_l2(a, (uint32_t)pt);
+        }
+    }
     if constexpr (HOT > 0) {
         fill_x_cache<WARPS * 32>(xc, a.x, hot);
         __syncthreads();
@@ -1343,6 +1364,10 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
     }
     if constexpr (!PIPE) {
         for (uint32_t tile = blockIdx.x * WARPS + w; tile < n_tiles; tile += total_warps) {
+            if constexpr (PFL2 > 0) {
+                const uint64_t pt = tile + (uint64_t)PFL2 * total_warps;
+                if (pt < n_tiles) nnz_prefetch_l2(a, (uint32_t)pt);
+            }
             if constexpr (PFL1) {
                 // the next tile's 8 col and 8 val lines into L1 while this one runs
                 const uint32_t nt = tile + total_warps;
@@ -1369,6 +1394,10 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
             if (tb < n_tiles) ib = nnz_load<SR, HINTS>(a, tb, pol_stream);
             for (;;) {
                 const uint32_t tc = tb + total_warps;
+                if constexpr (PFL2 > 0) {
+                    const uint64_t pt = tc + (uint64_t)PFL2 * total_warps;
+                    if (pt < n_tiles) nnz_prefetch_l2(a, (uint32_t)pt);
+                }
                 NnzReady<SR, Epi> rb{};
                 if (tb < n_tiles) rb = nnz_gather<SR, Epi, HOT, HINTS>(a, ib, xc, hot, pol_keep, epi);
                 NnzIn ic{};
