@@ -9,7 +9,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from graphone_b200 import gen
+from graphone_b200 import gen, results
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -17,16 +17,13 @@ pytestmark = pytest.mark.gpu
 FLT_MAX = np.float32(3.4028234663852886e38)
 
 
-def run_app(path, args, tmp_path):
-    out = os.path.join(str(tmp_path), "out.txt")
+def run_app(path, args, tmp_path, name="out.txt"):
+    out = os.path.join(str(tmp_path), name)
     r = subprocess.run([path, *args, "-o", out], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
-    lines = open(out).read().splitlines()
-    assert lines[0].startswith("Elapsed time:")
-    ids = np.array([int(l.split("-", 1)[0]) for l in lines[1:]])
-    vals = np.array([float(l.split("-", 1)[1]) for l in lines[1:]])
-    assert np.array_equal(ids, np.arange(len(ids)))
-    return vals, int(lines[0].split(":")[1].split()[0])
+    res = results.read_result(out)
+    assert res.elapsed_ms is not None and not np.isnan(res.values).any()
+    return res.values, int(res.elapsed_ms)
 
 
 def sssp_expected(g, src, n_out):
@@ -87,3 +84,24 @@ def test_pagerank_app_on_graphone_b200(cuda, tmp_path):
     # array of the run.
     errs = [float(np.max(np.abs(vals - h))) for h in hist[-3:-1]]
     assert min(errs) < 2e-6, errs
+
+
+@pytest.mark.parametrize("app", ["sssp_blas", "sssp_adv"])
+def test_dropin_and_reference_app_outputs_compare_equal(cuda, app, tmp_path):
+    """The same unchanged app source built on GraphOne's headers (the
+    reference GPU engines) and on this repository's: the comparator CLI
+    (python -m graphone_b200.results compare) finds their result files equal."""
+    ours, ref = O.app("g1", app), O.app("ref", app)
+    if ours is None or ref is None:
+        pytest.skip("apps not built (needs the reference sources at build time)")
+    g = gen.rmat(12, 8, True, (1, 64))
+    adj = os.path.join(str(tmp_path), "g.adj")
+    gen.write_adj(g, adj, directed=False)
+    run_app(ours, ["-i", adj, "--src", "0"], tmp_path, "ours.txt")
+    run_app(ref, ["-i", adj, "--src", "0"], tmp_path, "ref.txt")
+    import sys
+    r = subprocess.run([sys.executable, "-m", "graphone_b200.results", "compare",
+                        os.path.join(str(tmp_path), "ours.txt"), os.path.join(str(tmp_path), "ref.txt")],
+                       capture_output=True, text=True, cwd=os.path.dirname(os.path.dirname(__file__)))
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "same" in r.stdout
