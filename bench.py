@@ -319,6 +319,11 @@ def query_metrics(dev, stream, parity, ref_gpu=False, budget_queries: int = 256)
     one = torch.empty(g.n, dtype=torch.int32, device=dev)
     blk = torch.empty((256, g.n), dtype=torch.int32, device=dev)
     res = {"n": g.n, "m": g.m, "k": 256, "layout": "relabelled by degree (both engines)"}
+    # push/pull thresholds of both engines picked by the autotuner (timing
+    # SSSP from 16 spread sources), before either is measured
+    push_div, slot_div = G.autotune_traversal(16, stream=stream)
+    res["autotuned"] = {"push_while_frontier_out_edges_below": f"m/{push_div}",
+                        "sparse_slot_iterations_while_changed_out_edges_below": f"(m+n)/{slot_div}"}
     n_oracle = 8
     for kind in ("bfs", "sssp"):
         single = G.bfs if kind == "bfs" else G.sssp
@@ -400,22 +405,26 @@ SERVING_GRAPHS = (("rmat", 16), ("rmat", 18), ("rmat", 20), ("rmat", 22),
                   ("grid", 512), ("grid", 1024), ("grid", 2048), ("grid", 4096))
 
 
-def serving_metrics(dev, n_requests: int, rate: float, seed: int = 20261203):
+def serving_metrics(dev, n_requests: int, rate: float, sweep=(0.25, 0.5, 0.9, 1.5),
+                    seed: int = 20261203):
     """Serving loop over 8 resident graphs (RMAT 16/18/20/22 symmetrised and
     4-neighbour grids 512^2 .. 4096^2, uint32 weights in [1, 100]).
 
-    Requests: Poisson arrivals at `rate` per second, graph uniform, 60% SSSP
-    / 25% BFS / 15% personalized PageRank (fp32, damping 0.85, 20
-    iterations), source uniform over the graph's non-isolated vertices,
-    results into device buffers.  The same request stream is then run as
-    plain per-request execution (the single-source entry points, one at a
-    time in arrival order, a request starting when it has arrived and the
-    previous one has finished).  Latency = result written - arrival.
+    Requests: Poisson arrivals, graph uniform, 60% SSSP / 25% BFS / 15%
+    personalized PageRank (fp32, damping 0.85, 20 iterations), source
+    uniform over the graph's non-isolated vertices, results into device
+    buffers.  Each request stream is also run as plain per-request execution
+    (the single-source entry points, one at a time in arrival order, a
+    request starting when it has arrived and the previous one has finished).
+    Latency = result written - arrival.
+
+    First a saturating stream (`rate` per second, far above capacity) gives
+    the loop's capacity (served queries/s); then the offered rate is swept
+    over `sweep` x that capacity, each point with its own seeded stream.
     """
     import torch
     import graphone_b200 as g1
     from graphone_b200 import gen
-    rng = np.random.default_rng(seed)
     graphs, cands = [], []
     for kind, size in SERVING_GRAPHS:
         g = (gen.rmat(size, 16, symmetric=True, weights=(1, 100), device=dev) if kind == "rmat"
@@ -424,40 +433,6 @@ def serving_metrics(dev, n_requests: int, rate: float, seed: int = 20261203):
         graphs.append(g1.Graph.from_gen(g))
         del g
     torch.cuda.empty_cache()
-    reqs = []
-    t = 0.0
-    for _ in range(n_requests):
-        t += rng.exponential(1.0 / rate)
-        gi = int(rng.integers(0, len(graphs)))
-        u = rng.random()
-        q = g1.QUERY_SSSP if u < 0.60 else (g1.QUERY_BFS if u < 0.85 else g1.QUERY_PPR)
-        src = int(cands[gi][rng.integers(0, len(cands[gi]))])
-        reqs.append((t, gi, q, src))
-    outs = [torch.empty(graphs[gi].n, dtype=torch.float32 if q == g1.QUERY_PPR else torch.int32,
-                        device=dev) for _, gi, q, _ in reqs]
-    # served
-    with g1.Server(max_batch=256) as srv:
-        gids = [srv.add_graph(G) for G in graphs]
-        # one warm-up query per engine kind and graph (state allocation)
-        for gi, G in enumerate(graphs):
-            for q in (g1.QUERY_SSSP, g1.QUERY_BFS, g1.QUERY_PPR):
-                w = torch.empty(G.n, dtype=torch.int32, device=dev)
-                srv.wait(srv.submit(gids[gi], q, int(cands[gi][0]), w), 600000)
-        srv.stats(reset=True)
-        t0 = time.perf_counter()
-        tickets = []
-        for i, (ta, gi, q, src) in enumerate(reqs):
-            now = time.perf_counter() - t0
-            if ta > now:
-                time.sleep(ta - now)
-            tickets.append(srv.submit(gids[gi], q, src, outs[i]))
-        for tk in tickets:
-            srv.wait(tk, 0)
-        st = srv.stats()
-    served = {"p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
-              "mean_ms": round(st["mean_ms"], 3), "queries_per_s": round(st["queries_per_s"], 1),
-              "engine_steps": int(st["steps"]), "max_slots_busy": int(st["max_occupancy"])}
-    # plain per-request execution of the same stream
     one = {gi: torch.empty(G.n, dtype=torch.int32, device=dev) for gi, G in enumerate(graphs)}
     onef = {gi: torch.empty(G.n, dtype=torch.float32, device=dev) for gi, G in enumerate(graphs)}
 
@@ -476,27 +451,74 @@ def serving_metrics(dev, n_requests: int, rate: float, seed: int = 20261203):
         for q in (g1.QUERY_SSSP, g1.QUERY_BFS, g1.QUERY_PPR):
             run_plain(gi, q, int(cands[gi][0]))
     torch.cuda.synchronize()
-    lat, end, same = [], 0.0, True
-    for i, (ta, gi, q, src) in enumerate(reqs):
-        start = max(ta, end)
-        t1 = time.perf_counter()
-        r = run_plain(gi, q, src)
-        torch.cuda.synchronize()
-        end = start + (time.perf_counter() - t1)
-        lat.append((end - ta) * 1e3)
-        if i % 16 == 0:
-            same &= bool(torch.equal(r.view(torch.int32), outs[i].view(torch.int32)))
-    plain = {"p50_ms": round(_pct(lat, 50), 3), "p99_ms": round(_pct(lat, 99), 3),
-             "mean_ms": round(float(np.mean(lat)), 3),
-             "queries_per_s": round(len(reqs) / (end - reqs[0][0]), 1)}
+
+    def stream(r, n_req, sd):
+        rng = np.random.default_rng(sd)
+        reqs, t = [], 0.0
+        for _ in range(n_req):
+            t += rng.exponential(1.0 / r)
+            gi = int(rng.integers(0, len(graphs)))
+            u = rng.random()
+            q = g1.QUERY_SSSP if u < 0.60 else (g1.QUERY_BFS if u < 0.85 else g1.QUERY_PPR)
+            reqs.append((t, gi, q, int(cands[gi][rng.integers(0, len(cands[gi]))])))
+        return reqs
+
+    def run_point(srv, gids, r, n_req, sd):
+        reqs = stream(r, n_req, sd)
+        outs = [torch.empty(graphs[gi].n, dtype=torch.float32 if q == g1.QUERY_PPR else torch.int32,
+                            device=dev) for _, gi, q, _ in reqs]
+        srv.stats(reset=True)
+        t0 = time.perf_counter()
+        tickets = []
+        for i, (ta, gi, q, src) in enumerate(reqs):
+            now = time.perf_counter() - t0
+            if ta > now:
+                time.sleep(ta - now)
+            tickets.append(srv.submit(gids[gi], q, src, outs[i]))
+        for tk in tickets:
+            srv.wait(tk, 0)
+        st = srv.stats()
+        served = {"p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+                  "mean_ms": round(st["mean_ms"], 3), "queries_per_s": round(st["queries_per_s"], 1),
+                  "engine_steps": int(st["steps"]), "max_slots_busy": int(st["max_occupancy"])}
+        lat, end, same = [], 0.0, True
+        for i, (ta, gi, q, src) in enumerate(reqs):
+            start = max(ta, end)
+            t1 = time.perf_counter()
+            res = run_plain(gi, q, src)
+            torch.cuda.synchronize()
+            end = start + (time.perf_counter() - t1)
+            lat.append((end - ta) * 1e3)
+            if i % 16 == 0:
+                same &= bool(torch.equal(res.view(torch.int32), outs[i].view(torch.int32)))
+        plain = {"p50_ms": round(_pct(lat, 50), 3), "p99_ms": round(_pct(lat, 99), 3),
+                 "mean_ms": round(float(np.mean(lat)), 3),
+                 "queries_per_s": round(len(reqs) / (end - reqs[0][0]), 1)}
+        return {"offered_rate_per_s": round(r, 2), "requests": len(reqs), "served": served,
+                "plain_per_request": plain,
+                "served_over_plain_qps": round(served["queries_per_s"] / max(plain["queries_per_s"], 1e-9), 2),
+                "served_over_plain_p99": round(plain["p99_ms"] / max(served["p99_ms"], 1e-9), 2),
+                "spot_bit_identical": same}
+
+    with g1.Server(max_batch=256) as srv:
+        gids = [srv.add_graph(G) for G in graphs]
+        # one warm-up query per engine kind and graph (state allocation)
+        for gi, G in enumerate(graphs):
+            for q in (g1.QUERY_SSSP, g1.QUERY_BFS, g1.QUERY_PPR):
+                w = torch.empty(G.n, dtype=torch.int32, device=dev)
+                srv.wait(srv.submit(gids[gi], q, int(cands[gi][0]), w), 600000)
+        sat = run_point(srv, gids, rate, n_requests, seed)
+        cap = sat["served"]["queries_per_s"]
+        points = [run_point(srv, gids, f * cap, max(64, int(n_requests * min(1.0, f))), seed + 1 + k)
+                  for k, f in enumerate(sweep)]
     for G in graphs:
         G.close()
     torch.cuda.empty_cache()
-    return {"graphs": [f"{k}{s}" for k, s in SERVING_GRAPHS], "requests": len(reqs),
-            "offered_rate_per_s": rate, "mix": "60% SSSP / 25% BFS / 15% PPR",
-            "served": served, "plain_per_request": plain,
-            "served_over_plain_qps": round(served["queries_per_s"] / max(plain["queries_per_s"], 1e-9), 2),
-            "spot_bit_identical": same}
+    for f, pt in zip(sweep, points):
+        pt["fraction_of_capacity"] = f
+    return {"graphs": [f"{k}{s}" for k, s in SERVING_GRAPHS],
+            "mix": "60% SSSP / 25% BFS / 15% PPR",
+            "capacity_queries_per_s": cap, "saturated": sat, "sweep": points}
 
 
 def kernel_name(variant: int) -> str:
@@ -506,7 +528,7 @@ def kernel_name(variant: int) -> str:
     from graphone_b200 import MERGE_VARIANTS
     kind = MERGE_VARIANTS[variant]
     base = {"warp": "spmv_wmerge_kernel", "warp_tma": "spmv_wtma_kernel",
-            "cta_tma": "spmv_merge_kernel", "nnz": "spmv_nnz_kernel"}[kind]
+            "cta_tma": "spmv_merge_kernel", "nnz": "spmv_nnz_kernel", "colsort": "spmv_cs_kernel"}[kind]
     return f"{base}<PlusTimesF32, PrEpilogue> (merge variant {variant})"
 
 

@@ -30,10 +30,13 @@ PR_REFERENCE, PR_DANGLING = 0, 1
 # in csrc/spmv_launch.cuh: "warp" = spmv_wmerge_kernel (warp tiles, plain
 # loads), "cta_tma" = spmv_merge_kernel (CTA tiles staged by bulk copies),
 # "warp_tma" = spmv_wtma_kernel (warp tiles staged by bulk copies), "nnz" =
-# spmv_nnz_kernel (nnz-split warp tiles, 16-byte loads, row-start bitmap).
+# spmv_nnz_kernel (nnz-split warp tiles, 16-byte loads, row-start bitmap),
+# "colsort" = spmv_cs_kernel (row partitions folded in column order into
+# shared-memory accumulators).
 MERGE_VARIANTS = ("warp", "warp", "warp", "cta_tma", "cta_tma", "warp",
                   "warp_tma", "warp_tma", "warp_tma", "warp_tma", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz",
-                  "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz")
+                  "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz",
+                  "colsort", "colsort", "colsort")
 DEFAULT_MERGE_VARIANT = 17
 GRAPH_SYMMETRIC, GRAPH_INPUT_TRANSPOSE, GRAPH_BUILD_OTHER, GRAPH_NO_VALIDATE = 1, 2, 4, 8
 GRAPH_RELABEL = 16
@@ -66,6 +69,7 @@ def _declare(L):
     L.g1_stream_sync.argtypes = [P]
     L.g1_kernel_launches.restype = C.c_uint64
     L.g1_count_user_launches.argtypes = [C.c_uint64]
+    L.g1_test_set_wait_polls.argtypes = [C.c_int64]
     L.g1_profile_begin.argtypes = []
     L.g1_profile_end.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
     L.g1_graph_create.argtypes = [P, P, P, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, P,
@@ -79,9 +83,11 @@ def _declare(L):
     L.g1_spmv_plan.argtypes = [P, C.c_int, C.c_uint32, C.POINTER(C.c_uint32),
                                C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]
     L.g1_spmv.argtypes = [P, C.c_int, C.c_int, C.c_int, P, P, P]
+    L.g1_spmv_nnz_plan.argtypes = [P, C.c_int, P]
     L.g1_spmv_noalloc.argtypes = [P, P, P, C.c_uint32, C.c_uint32, C.c_int, P, P, P]
     L.g1_graph_set_schedule.argtypes = [P, C.c_int, C.c_int, C.c_int]
     L.g1_autotune.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int), P]
+    L.g1_autotune_traversal.argtypes = [P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), P]
     L.g1_pagerank.argtypes = [P, C.c_float, C.c_int, C.c_int, P, P]
     L.g1_sssp.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
     L.g1_bfs.argtypes = [P, C.c_uint32, C.c_int, P, C.POINTER(C.c_uint32), P]
@@ -115,10 +121,10 @@ def lib():
 EXPORTS = (
     "g1_status_string", "g1_last_error", "g1_version", "g1_mem_alloc", "g1_mem_free",
     "g1_mem_copy", "g1_release_cached_memory", "g1_mem_fill_u32", "g1_stream_sync", "g1_kernel_launches",
-    "g1_count_user_launches",
+    "g1_count_user_launches", "g1_test_set_wait_polls",
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
-    "g1_spmv_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_pagerank", "g1_sssp", "g1_bfs", "g1_advance_run",
+    "g1_spmv_plan", "g1_spmv_nnz_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_autotune_traversal", "g1_pagerank", "g1_sssp", "g1_bfs", "g1_advance_run",
     "g1_bfs_batch", "g1_sssp_batch", "g1_ppr", "g1_ppr_batch",
     "g1_server_create", "g1_server_add_graph", "g1_server_submit", "g1_server_poll",
     "g1_server_wait", "g1_server_stats", "g1_server_destroy",
@@ -157,6 +163,12 @@ def release_cached_memory() -> int:
     b = C.c_size_t()
     check(lib().g1_release_cached_memory(C.byref(b)))
     return b.value
+
+
+def test_set_wait_polls(polls: int) -> None:
+    """Lowers the poll limit of every bounded device wait (negative: the
+    defaults), so that tests can make the waits run out."""
+    check(lib().g1_test_set_wait_polls(polls))
 
 
 def profile_begin() -> None:
@@ -256,6 +268,13 @@ class Graph:
         a, b, v = C.c_float(), C.c_float(), C.c_int()
         check(lib().g1_autotune(self._h, C.byref(a), C.byref(b), C.byref(v), _stream(stream)))
         return a.value, b.value, v.value
+
+    def autotune_traversal(self, n_sources=16, stream=None):
+        """(push_div, slot_div): the push/pull thresholds g1_autotune_traversal
+        picked for this graph by timing SSSP from n_sources sources."""
+        a, b = C.c_uint32(), C.c_uint32()
+        check(lib().g1_autotune_traversal(self._h, n_sources, C.byref(a), C.byref(b), _stream(stream)))
+        return a.value, b.value
 
     def pagerank(self, alpha=0.85, iters=30, mode=PR_DANGLING, out=None, stream=None):
         if out is None:

@@ -123,10 +123,104 @@ g1_status entry(g1_graph* g, int kind, const uint32_t* srcs, uint32_t k, void* o
     return run_queries(g, kind, srcs, k, out, iters_out, alpha, ppr_iters, cap, as_stream(stream));
 }
 
+// Caller ids of up to k vertices with out-edges, evenly spread over the
+// internal order (the push side's CSR).
+g1_status tune_sources(g1_graph* g, uint32_t k, cudaStream_t s, std::vector<uint32_t>* out) {
+    const int t = push_side(g);
+    std::vector<uint32_t> rp((size_t)g->n + 1);
+    G1_CUDA(cudaMemcpyAsync(rp.data(), g->o[t].rp, rp.size() * 4, cudaMemcpyDeviceToHost, s));
+    std::vector<uint32_t> iperm;
+    if (g->relabeled) {
+        iperm.resize(g->n);
+        G1_CUDA(cudaMemcpyAsync(iperm.data(), g->iperm.p, (size_t)g->n * 4, cudaMemcpyDeviceToHost, s));
+    }
+    G1_CUDA(cudaStreamSynchronize(s));
+    std::vector<uint32_t> cand;
+    for (uint32_t v = 0; v < g->n; ++v)
+        if (rp[v + 1] > rp[v]) cand.push_back(v);
+    out->clear();
+    if (cand.empty()) return G1_OK;
+    for (uint32_t i = 0; i < k && i < cand.size(); ++i) {
+        const uint32_t v = cand[(size_t)i * cand.size() / std::min<size_t>(k, cand.size())];
+        out->push_back(g->relabeled ? iperm[v] : v);
+    }
+    return G1_OK;
+}
+
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
 }  // namespace
 }  // namespace g1
 
 using namespace g1;
+
+// Times SSSP from `n_sources` spread sources under each candidate push/pull
+// threshold and keeps the fastest: the single-source AUTO engine's
+// (m / push_div, push while the frontier's out-degree sum is below it) and
+// the slot engines' ((m + n) / slot_div, sparse iterations while the changed
+// vertices' out-edges are below it).
+extern "C" g1_status g1_autotune_traversal(g1_graph* g, uint32_t n_sources, uint32_t* push_div,
+                                           uint32_t* slot_div, void* stream) {
+    if (!g) return fail(G1_ERR_INVALID, "g1_autotune_traversal: null graph");
+    DeviceGuard dg(g->device);
+    std::lock_guard<std::mutex> lk(g->mu);
+    cudaStream_t s = as_stream(stream);
+    const uint32_t k = std::min<uint32_t>(64, n_sources ? n_sources : 16);
+    std::vector<uint32_t> src;
+    G1_TRY(tune_sources(g, k, s, &src));
+    if (!src.empty() && g->vtype == G1_U32) {
+        uint32_t* out = nullptr;
+        G1_TRY(g->ws.get("tune_dist", g->n, &out));
+        // single-source AUTO: push/pull applies unless the near-far engine runs
+        if (g->o[0].present && g->o[1].present && !nearfar_suits(g)) {
+            const uint32_t cands[] = {4, 8, 16, 32, 64, 128};
+            double best = 1e300;
+            uint32_t best_div = g->push_div;
+            for (uint32_t d : cands) {
+                g->push_div = d;
+                G1_TRY(traverse_locked(g, src[0], G1_ENGINE_AUTO, false, out, nullptr, s));
+                const auto t0 = std::chrono::steady_clock::now();
+                for (uint32_t v : src) G1_TRY(traverse_locked(g, v, G1_ENGINE_AUTO, false, out, nullptr, s));
+                G1_CUDA(cudaStreamSynchronize(s));
+                const double t = seconds_since(t0);
+                if (t < best) {
+                    best = t;
+                    best_div = d;
+                }
+            }
+            g->push_div = best_div;
+        }
+        // slot engines: batched SSSP over the same sources
+        if (g->o[1].present) {
+            const uint32_t kb = std::min<uint32_t>((uint32_t)src.size(), 32);
+            uint32_t* bout = nullptr;
+            G1_TRY(g->ws.get("tune_batch", (size_t)kb * g->n, &bout));
+            const uint32_t cands[] = {2, 4, 8, 16, 32};
+            double best = 1e300;
+            uint32_t best_div = g->slot_div;
+            for (uint32_t d : cands) {
+                g->slot_div = d;
+                g->slot_cache[kSlotSssp].reset();  // its captured steps hold the threshold
+                G1_TRY(run_queries(g, kSlotSssp, src.data(), kb, bout, nullptr, 0.85f, 0, kMaxSlots, s));
+                const auto t0 = std::chrono::steady_clock::now();
+                G1_TRY(run_queries(g, kSlotSssp, src.data(), kb, bout, nullptr, 0.85f, 0, kMaxSlots, s));
+                G1_CUDA(cudaStreamSynchronize(s));
+                const double t = seconds_since(t0);
+                if (t < best) {
+                    best = t;
+                    best_div = d;
+                }
+            }
+            g->slot_div = best_div;
+            for (auto& e : g->slot_cache) e.reset();
+        }
+    }
+    if (push_div) *push_div = g->push_div;
+    if (slot_div) *slot_div = g->slot_div;
+    return G1_OK;
+}
 
 extern "C" g1_status g1_bfs_batch(g1_graph* g, const uint32_t* srcs, uint32_t k,
                                   uint32_t* levels_out, uint32_t* iters_out, void* stream) {

@@ -100,6 +100,15 @@ struct NnzPlan {
                        // span one boundary first, then longer chains, each in tile order
 };
 
+// Column-sorted partitions (spmv_cs_kernel): rows cut into partitions of at
+// most kCsRows rows and about m / (SMs x parts_per_sm) nonzeros; inside a
+// partition the nonzeros in column order with their row offsets.
+struct CsPlan {
+    uint32_t n_parts = 0;
+    DevBuf part_row, part_nnz;  // n_parts + 1 each
+    DevBuf col, lrow, val;      // m entries (+ padding) in partition-column order
+};
+
 struct Orientation {
     bool present = false;
     uint32_t* rp = nullptr;
@@ -111,6 +120,33 @@ struct Orientation {
     int tuned_sched = 0;  // 0 = not tuned, else g1_schedule
     int tuned_variant = -1;  // merge kernel variant chosen by g1_autotune (-1 = default)
     std::unique_ptr<NnzPlan> nnz_plan;
+    std::map<uint32_t, std::unique_ptr<CsPlan>> cs_plans;  // by partitions per SM
+};
+
+// Captured CUDA graphs of the device-driven traversal engines (traverse.cu):
+// per mode (engine x {SSSP, BFS}) a graph of 2^i pairs of steps for each
+// i < kSizes, valid for the state store they were captured on (`key`).
+struct AdvGraphs {
+    static constexpr int kSizes = 8;
+    static constexpr int kModes = 4;  // {advance, BLAS pull} x {SSSP, BFS}
+    cudaGraphExec_t exec[kModes][kSizes] = {};
+    const void* key[kModes] = {};
+    cudaStream_t capture = nullptr;
+    AdvGraphs() = default;
+    AdvGraphs(const AdvGraphs&) = delete;
+    AdvGraphs& operator=(const AdvGraphs&) = delete;
+    void reset(int mode) {
+        for (auto& x : exec[mode])
+            if (x) {
+                cudaGraphExecDestroy(x);
+                x = nullptr;
+            }
+        key[mode] = nullptr;
+    }
+    ~AdvGraphs() {
+        for (int m = 0; m < kModes; ++m) reset(m);
+        if (capture) cudaStreamDestroy(capture);
+    }
 };
 
 // Named, growable workspaces of one graph.
@@ -160,9 +196,17 @@ struct g1_graph {
     bool outdeg_ready = false;
     // Mean u32 edge weight (bucket width of the near-far engine), -1 until known.
     double mean_weight = -1.0;
+    // Push/pull switches (g1_autotune_traversal may change them): the
+    // single-source AUTO engine pushes while the frontier's out-degree sum is
+    // below m / push_div; the slot engines list the next iteration's row
+    // pieces while the changed vertices' out-edges are below (m + n) / slot_div.
+    uint32_t push_div = 16;
+    uint32_t slot_div = 8;
     // Slot engines of the batched BFS / SSSP / PPR entry points (by kind),
     // kept between calls.
     std::shared_ptr<g1::SlotEngine> slot_cache[3];
+    // CUDA graphs of the device-driven advance engine.
+    std::unique_ptr<g1::AdvGraphs> adv_graphs;
     // Degree-ordered relabelling (G1_GRAPH_RELABEL): perm maps a caller's
     // vertex id to the internal id, iperm the reverse.
     bool relabeled = false;
@@ -194,6 +238,7 @@ g1_status copy_out(void* dst, const void* dev_src, size_t bytes, cudaStream_t s)
 
 g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out);
 g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out);
+g1_status ensure_cs_plan(g1_graph* g, int t, uint32_t parts_per_sm, CsPlan** out);
 // Near-far SSSP (unit = BFS) from internal vertex src in one persistent
 // launch; *dist_out points to the graph's workspace distances.
 g1_status nearfar_traverse(g1_graph* g, uint32_t src, bool unit, uint32_t** dist_out, uint32_t* rounds,
@@ -226,8 +271,23 @@ g1_status internal_vertex(g1_graph* g, uint32_t v, uint32_t* out, cudaStream_t s
 g1_status copy_out_vertices(g1_graph* g, void* dst, const void* internal, cudaStream_t s);
 g1_status spmv_dispatch(g1_graph* g, int transpose, g1_semiring sr, g1_schedule sched,
                         const void* x, void* y, cudaStream_t s);
+// Single-source SSSP (unit: BFS) from caller vertex `src` on `engine`;
+// the caller holds g->mu.
+g1_status traverse_locked(g1_graph* g, uint32_t src, g1_engine engine, bool unit, uint32_t* out,
+                          uint32_t* iters_out, cudaStream_t s);
 // Reads and clears the graph's device error word (synchronises `s`).
 g1_status check_device_error(g1_graph* g, cudaStream_t s);
+
+// While alive, the calling thread is capturing a CUDA graph: the SpMV timer
+// (profiling) records nothing.
+struct CaptureScope {
+    CaptureScope();
+    ~CaptureScope();
+};
+
+// Poll limit of the bounded device waits: `dflt` unless a test lowered it
+// with g1_test_set_wait_polls.
+uint32_t wait_polls(uint32_t dflt);
 
 // Kernel launch accounting (g1_kernel_launches) and the SpMV kernel timer
 // (g1_profile_begin/end).

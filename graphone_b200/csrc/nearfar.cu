@@ -55,6 +55,7 @@ struct NfArgs {
     uint32_t* near[2];
     uint32_t* far[2];
     NfCtl* ctl;
+    uint32_t spin_limit;  // polls before a barrier wait gives up
 };
 
 // About 2-3 s of waiting before a barrier gives up.
@@ -98,7 +99,8 @@ __device__ __forceinline__ void nf_read_ctl(const NfCtl* c, uint32_t st, uint32_
 }
 
 // Also loads the control words of step `st_next` (far pile `fp`) into sc.
-__device__ bool nf_barrier(NfCtl* c, uint32_t nblocks, uint32_t st_next, uint32_t fp, NfStepCtl* sc) {
+__device__ bool nf_barrier(NfCtl* c, uint32_t nblocks, uint32_t st_next, uint32_t fp, NfStepCtl* sc,
+                           uint32_t spin_limit) {
     __syncthreads();
     if (threadIdx.x == 0) {
         const uint32_t g0 = ld_acquire(&c->bar_gen);
@@ -108,7 +110,7 @@ __device__ bool nf_barrier(NfCtl* c, uint32_t nblocks, uint32_t st_next, uint32_
         } else {
             uint32_t spins = 0;
             while (ld_acquire(&c->bar_gen) == g0) {
-                if (++spins > kNfSpinLimit) {
+                if (++spins > spin_limit) {
                     atomicOr(&c->err, 1u);
                     break;
                 }
@@ -277,7 +279,7 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
             par ^= 1;
             fp ^= 1;
         }
-        if (!nf_barrier(c, nb, st + 1, fp, &sc)) return;
+        if (!nf_barrier(c, nb, st + 1, fp, &sc, a.spin_limit)) return;
     }
 }
 
@@ -369,6 +371,7 @@ g1_status nearfar_launch(const g1_graph* g, uint32_t src, bool unit, uint32_t de
     a.far[0] = b.far[0];
     a.far[1] = b.far[1];
     a.ctl = reinterpret_cast<NfCtl*>(b.ctl);
+    a.spin_limit = wait_polls(kNfSpinLimit);
     const uint32_t gi = (uint32_t)std::max<uint64_t>(
         1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
     // BFS: a threshold above every level -- each step is one level and the

@@ -175,6 +175,7 @@ g1_status slot_graph(g1_graph* g, int kind, cudaStream_t s, SlotGraph* out) {
     sg.n_pieces = g->n_pieces;
     sg.sm_count = g->sm_count;
     sg.perm = g->relabeled ? g->perm.as<uint32_t>() : nullptr;
+    sg.sparse_div = g->slot_div;
     if (kind == kSlotPpr) {
         uint32_t *flag = nullptr, *hpc = nullptr, *hidx = nullptr, *hp0 = nullptr, *hub_v = nullptr,
                  *hub_hp = nullptr, *piece_hp = nullptr, *deg = nullptr;
@@ -728,10 +729,11 @@ Frontier SlotEngine::frontier(uint32_t it) {
     f.ctr = ctr_.as<uint32_t>();
     f.it_base = nullptr;
     f.it = it;
-    // the next list is built while fewer than 1/8 of the graph's edges
-    // leave the changed vertices: listing costs at most that many marks,
-    // and a sparse pull never reads more rows than a dense one
-    f.thresh = (uint32_t)std::max<uint64_t>(64, std::min<uint64_t>(0xFFFFFFFFull, ((uint64_t)sg_.m + sg_.n) / 8));
+    // the next list is built while fewer than 1/sparse_div (by default 1/8)
+    // of the graph's edges leave the changed vertices: listing costs at most
+    // that many marks, and a sparse pull never reads more rows than a dense one
+    f.thresh = (uint32_t)std::max<uint64_t>(
+        64, std::min<uint64_t>(0xFFFFFFFFull, ((uint64_t)sg_.m + sg_.n) / std::max<uint32_t>(1, sg_.sparse_div)));
     return f;
 }
 

@@ -59,6 +59,9 @@ struct SlotGraph {
     const uint32_t* perm = nullptr;      // caller id -> internal id, or null
     uint32_t n = 0, m = 0, n_pieces = 0, n_hubs = 0, n_hub_pieces = 0;
     int sm_count = 148;
+    // the next iteration's row pieces are listed while the changed vertices'
+    // out-edges are below (m + n) / sparse_div
+    uint32_t sparse_div = 8;
 };
 
 // Builds (once per graph) the arrays `kind` needs and fills `out`.  The

@@ -23,7 +23,9 @@ constexpr int kVectorBlock = 256;
 //           stages: bit 0 = L2 cache policies, bit 1 = three-tile software
 //           pipeline per warp, bit 2 = next-tile L1 prefetch, bit 3 / bit 4
 //           = next tile's col and val / col only staged in shared memory by
-//           bulk copies, stages / 32 = L2 prefetch distance in rounds.
+//           bulk copies, stages / 32 = L2 prefetch distance in rounds;
+//   kind 4: column-sorted partitions (spmv_cs_kernel; its own plan), stages
+//           = partitions per SM.
 // `warps` per block (kind 0/2/3), `hot` x entries cached in shared memory,
 // `minb` resident blocks per SM the register budget is sized for.
 struct MergeVariant {
@@ -45,8 +47,9 @@ constexpr MergeVariant kMergeVariants[] = {
     {3, 8, 3, 24, 32768, 1},  {3, 8, 4, 32, 32768, 1},  {3, 8, 4, 32, 16384, 1},
     {3, 8, 8, 32, 32768, 1},  {3, 8, 8, 32, 16384, 1},  {3, 8, 16, 32, 32768, 1},
     {3, 8, 16, 32, 24576, 1}, {3, 8, 32, 32, 32768, 1}, {3, 8, 64, 32, 32768, 1},
-    {3, 8, 128, 32, 32768, 1}, {3, 8, 66, 24, 32768, 1}};
-constexpr int kNumMergeVariants = 32;
+    {3, 8, 128, 32, 32768, 1}, {3, 8, 66, 24, 32768, 1}, {4, 8, 2, 32, 0, 1},
+    {4, 8, 4, 32, 0, 1},      {4, 8, 1, 32, 0, 1}};
+constexpr int kNumMergeVariants = 35;
 constexpr int kDefaultVariant = 17;
 
 template <class K>
@@ -141,6 +144,24 @@ struct NnzKernel {
     }
 };
 
+template <class SR, class Epi>
+struct CsKernel {
+    using L = CsLayout<SR>;
+    static constexpr int kBlock = 1024;
+    static int occupancy() {
+        static int occ = [] {
+            auto k = spmv_cs_kernel<SR, Epi, kBlock>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
+            return blocks_per_sm(k, kBlock, L::BYTES);
+        }();
+        return occ;
+    }
+    static uint32_t grid(const g1_graph* g, uint32_t n_parts) {
+        return (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(n_parts, (uint64_t)g->sm_count * occupancy()));
+    }
+};
+
 // The nnz fixup runs grid-stride in one wave of resident blocks (blocks of
 // a second wave would start their empty rows only after the main kernel).
 template <class SR, class Epi>
@@ -212,6 +233,7 @@ MergeArgs<SR> merge_args(const g1_graph* g, int t, const MergePlan& p, const typ
     a.carry = p.carry.as<typename SR::value_t>();
     a.tail = p.tail.as<typename SR::value_t>();
     a.err = g->err_word;
+    a.wait_limit = wait_polls(kWaitPolls);
     return a;
 }
 
@@ -239,7 +261,32 @@ NnzArgs<SR> nnz_args(const g1_graph* g, int t, const NnzPlan& p, const typename 
     a.carry = p.carry.as<typename SR::value_t>();
     a.tail = p.tail.as<typename SR::value_t>();
     a.err = g->err_word;
+    a.wait_limit = wait_polls(kWaitPolls);
     return a;
+}
+
+template <class SR, class Epi>
+g1_status launch_cs(g1_graph* g, int t, uint32_t parts_per_sm, const typename SR::x_t* x,
+                    const Epi& epi, cudaStream_t s) {
+    static_assert(sizeof(typename SR::w_t) == 4, "column-sorted partitions hold 4-byte edge values");
+    CsPlan* p = nullptr;
+    G1_TRY(ensure_cs_plan(g, t, parts_per_sm, &p));
+    CsArgs<SR> a;
+    a.n_parts = p->n_parts;
+    a.part_row = p->part_row.as<uint32_t>();
+    a.part_nnz = p->part_nnz.as<uint32_t>();
+    a.col = p->col.as<uint32_t>();
+    a.lrow = p->lrow.as<uint16_t>();
+    a.val = p->val.as<typename SR::w_t>();
+    a.x = x;
+    using K = CsKernel<SR, Epi>;
+    const bool prof = profiling();
+    if (prof) prof_mark(s, true);
+    spmv_cs_kernel<SR, Epi, K::kBlock><<<K::grid(g, p->n_parts), K::kBlock, K::L::BYTES, s>>>(a, epi);
+    if (prof) prof_mark(s, false);
+    count_launches(1);
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
 }
 
 template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false,
@@ -277,6 +324,13 @@ g1_status launch_nnz(g1_graph* g, int t, const NnzPlan& p, const typename SR::x_
 template <class SR, class Epi>
 g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_grid) {
     const int v = merge_variant(g, t);
+    if (kMergeVariants[v].kind == 4) {
+        CsPlan* q = nullptr;
+        G1_TRY(ensure_cs_plan(g, t, (uint32_t)kMergeVariants[v].stages, &q));
+        *main_grid = CsKernel<SR, Epi>::grid(g, q->n_parts);
+        *fix_grid = 0;
+        return G1_OK;
+    }
     if (kMergeVariants[v].kind == 3) {
         NnzPlan* q = nullptr;
         G1_TRY(ensure_nnz_plan(g, t, &q));
@@ -384,6 +438,8 @@ template <class SR, class Epi>
 g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi& main_epi,
                        const Epi& fix_epi, cudaStream_t s) {
     const int v = merge_variant(g, t);
+    if (kMergeVariants[v].kind == 4)
+        return launch_cs<SR, Epi>(g, t, (uint32_t)kMergeVariants[v].stages, x, main_epi, s);
     if (kMergeVariants[v].kind == 3) {
         NnzPlan* q = nullptr;
         G1_TRY(ensure_nnz_plan(g, t, &q));

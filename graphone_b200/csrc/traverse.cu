@@ -193,6 +193,415 @@ tr_advance_lb_kernel(const uint32_t* F, uint32_t nF, const uint32_t* prefix, con
     }
 }
 
+// ------------------------------------------------ device-driven advance
+// The push engine for graphs whose out-degrees are all at most 32 (grids,
+// meshes, road-like graphs: thousands of small-frontier iterations).  One
+// kernel per iteration with everything the host loop decided between
+// iterations moved onto the device -- the frontier size and its degree sum
+// are read from device counters, the lanes per vertex follow from them --
+// so iterations are captured as CUDA graphs of 2^i step pairs and the host
+// reads the frontier size back only between graphs.  Per iteration the
+// result is that of GraphOne's AdvanceGC step (engine/advance_gc.h:162-283
+// with apps/sssp_adv.cu:49-71): relax every out-edge of the frontier with
+// atomicMin, emit each improved vertex once (the visited stamp of the
+// sssp_adv filter).  Appends go to a per-block shared-memory queue flushed
+// with one global atomic per block (a single global counter bumped by
+// every warp serialises at one L2 slice when frontiers hold hundreds of
+// thousands of vertices).
+
+// Frontier size and out-degree sum of one frontier buffer.
+struct AgCounter {
+    uint32_t n;
+    uint32_t pad;
+    unsigned long long deg;
+};
+
+// Store layout (4-byte words): dist[n], visited[n], F0[n], F1[n], then the
+// control words: [0] completed iterations, [1] block ticket, and the two
+// counters at words 4 and 8.
+struct AgState {
+    uint32_t *dist, *visited, *F[2], *ctl;
+    AgCounter* c[2];
+};
+
+inline size_t ag_words(uint32_t n) { return 4 * (size_t)n + 16; }
+
+inline AgState ag_layout(uint32_t* store, uint32_t n) {
+    AgState a;
+    a.dist = store;
+    a.visited = store + n;
+    a.F[0] = store + 2 * (size_t)n;
+    a.F[1] = store + 3 * (size_t)n;
+    a.ctl = store + 4 * (size_t)n;
+    a.c[0] = reinterpret_cast<AgCounter*>(a.ctl + 4);
+    a.c[1] = reinterpret_cast<AgCounter*>(a.ctl + 8);
+    return a;
+}
+
+constexpr int kAgBlock = 256;
+constexpr int kAgQueue = 2048;  // shared-memory queue entries per block
+
+// Shared-memory side of a block's appends: the queue, its fill count, the
+// block's base in the global frontier and the warps' degree sums.
+struct AgBlockQueue {
+    uint32_t q[kAgQueue];
+    uint32_t cnt, base;
+    unsigned long long deg[kAgBlock / 32];
+};
+
+// Push relaxation of edge (u -> v) of weight w from distance du: atomicMin;
+// an improved vertex is emitted once per iteration (the visited stamp) into
+// the block's queue (straight to F_out when the queue is full).
+template <bool UNIT>
+__device__ __forceinline__ void ag_relax(uint32_t du, uint32_t v, uint32_t w, uint32_t* dist,
+                                         uint32_t* visited, uint32_t it, const uint32_t* rp,
+                                         unsigned long long& my_deg, AgBlockQueue& bq, uint32_t* F_out,
+                                         AgCounter* c_out) {
+    const uint32_t cand = UNIT ? du + 1u : du + w;
+    if (cand < dist[v]) {  // cheap pre-check; atomicMin decides
+        const uint32_t old = atomicMin(&dist[v], cand);
+        if (cand < old && atomicExch(&visited[v], it) != it) {
+            my_deg += rp[v + 1] - rp[v];
+            const uint32_t p = atomicAdd(&bq.cnt, 1u);
+            if (p < (uint32_t)kAgQueue) bq.q[p] = v;
+            else F_out[atomicAdd(&c_out->n, 1u)] = v;  // queue full: straight out
+        }
+    }
+}
+
+// Publishes a block's appends: one global atomic for the count, one for the
+// degree sum.  All threads of the block; bq.cnt was zeroed before the block's
+// relaxations.
+__device__ __forceinline__ void ag_flush(AgBlockQueue& bq, unsigned long long my_deg, uint32_t* F_out,
+                                         AgCounter* c_out) {
+    my_deg = warp_sum(my_deg);
+    if (lane_id() == 0) bq.deg[threadIdx.x >> 5] = my_deg;
+    __syncthreads();
+    const uint32_t cnt = min(bq.cnt, (uint32_t)kAgQueue);
+    if (threadIdx.x == 0) {
+        unsigned long long d = 0ull;
+        for (int w = 0; w < kAgBlock / 32; ++w) d += bq.deg[w];
+        if (d) atomicAdd(&c_out->deg, d);
+        bq.base = cnt ? atomicAdd(&c_out->n, cnt) : 0u;
+    }
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < cnt; q += kAgBlock) F_out[bq.base + q] = bq.q[q];
+}
+
+// Lanes per frontier vertex: the power of two at or above the mean degree.
+__device__ __forceinline__ uint32_t ag_tpv(uint32_t nF, unsigned long long degF) {
+    const unsigned long long mean = (degF + nF - 1) / nF;
+    uint32_t tpv = 1;
+    while (tpv < 32 && tpv < mean) tpv <<= 1;
+    return tpv;
+}
+
+__global__ void ag_init_kernel(uint32_t n, uint32_t src, const uint32_t* rp, AgState a) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        a.dist[v] = v == src ? 0u : kU32Max;
+        a.visited[v] = 0u;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.F[0][0] = src;
+        a.ctl[0] = 0u;
+        a.ctl[1] = 0u;
+        a.c[0]->n = 1u;
+        a.c[0]->deg = rp[src + 1] - rp[src];
+        a.c[1]->n = 0u;
+        a.c[1]->deg = 0ull;
+    }
+}
+
+// Last block of a step (every block calls this once, thread 0): zeroes c_in
+// (it is the next step's c_out) and advances the iteration count when the
+// step had a frontier.
+__device__ __forceinline__ void ag_last_block_rotate(AgCounter* c_in, uint32_t* ctl, uint32_t nF) {
+    __threadfence();
+    if (atomicAdd(&ctl[1], 1u) == gridDim.x - 1) {
+        // every block has read c_in and published its appends
+        if (nF) ctl[0] += 1u;
+        c_in->n = 0u;
+        c_in->deg = 0ull;
+        ctl[1] = 0u;
+        __threadfence();
+    }
+}
+
+// One advance step: frontier F_in (size and degree sum in c_in) -> F_out
+// (counted in c_out, zero on entry); out-degrees at most 32.  The last block
+// to finish zeroes c_in and bumps the iteration count.  An empty frontier
+// makes the step a no-op, so graphs may run past convergence.
+template <bool UNIT>
+__global__ void __launch_bounds__(kAgBlock)
+ag_step_kernel(const uint32_t* F_in, uint32_t* F_out, AgCounter* c_in, AgCounter* c_out,
+               uint32_t* ctl, uint32_t n, const uint32_t* rp, const uint32_t* col, const uint32_t* val,
+               uint32_t* dist, uint32_t* visited, uint32_t* err) {
+    __shared__ AgBlockQueue bq;
+    const uint32_t nF = c_in->n;
+    if (nF == 0) return;  // the same for every block
+    const uint32_t it = ctl[0] + 1u;  // visited stamp of this iteration
+    const uint32_t tpv = ag_tpv(nF, c_in->deg);
+    if (threadIdx.x == 0) bq.cnt = 0u;
+    __syncthreads();
+    const uint32_t lane = lane_id();
+    const uint32_t sub = lane & (tpv - 1u), grp = lane / tpv, vpw = 32u / tpv;
+    const uint64_t warps = (uint64_t)gridDim.x * (kAgBlock / 32);
+    const uint64_t wid = ((uint64_t)blockIdx.x * kAgBlock + threadIdx.x) >> 5;
+    unsigned long long my_deg = 0ull;
+    for (uint64_t first = wid * vpw; first < nF; first += warps * vpw) {
+        const uint64_t i = first + grp;
+        uint32_t b = 0, e = 0, du = 0;
+        if (i < nF) {
+            const uint32_t u = F_in[i];
+            if (frontier_vertex_ok(u, n, err)) {
+                du = dist[u];
+                if (du != kU32Max) {
+                    b = rp[u];
+                    e = rp[u + 1];
+                }
+            }
+        }
+        for (uint32_t k = b + sub; k < e; k += tpv)
+            ag_relax<UNIT>(du, col[k], UNIT ? 1u : val[k], dist, visited, it, rp, my_deg, bq, F_out, c_out);
+    }
+    ag_flush(bq, my_deg, F_out, c_out);
+    if (threadIdx.x == 0) ag_last_block_rotate(c_in, ctl, nF);
+}
+
+template <bool UNIT>
+static void ag_enqueue_pairs(const g1_graph* g, const AgState& a, uint32_t pairs, uint32_t grid,
+                             cudaStream_t s) {
+    const Orientation& o = g->o[0];
+    const auto* val = static_cast<const uint32_t*>(o.val);
+    for (uint32_t p = 0; p < pairs; ++p)
+        for (int h = 0; h < 2; ++h)
+            ag_step_kernel<UNIT><<<grid, kAgBlock, 0, s>>>(a.F[h], a.F[h ^ 1], a.c[h], a.c[h ^ 1], a.ctl, g->n,
+                                                           o.rp, o.col, val, a.dist, a.visited, g->err_word);
+}
+
+inline bool advance_graph_suits(const g1_graph* g) {
+    return g->o[0].present && g->o[0].max_deg <= 32 && g->n > 0;
+}
+
+template <bool UNIT>
+static g1_status advance_graph_traverse(g1_graph* g, uint32_t src, uint32_t* out, uint32_t* iters_out,
+                                        cudaStream_t s) {
+    const uint32_t n = g->n;
+    const int mode = UNIT ? 1 : 0;
+    uint32_t* store = nullptr;
+    G1_TRY(g->ws.get("ag_store", ag_words(n), &store));
+    const AgState a = ag_layout(store, n);
+    G1_TRY(g->ws.pinned.ensure(64));
+    uint32_t* host = g->ws.pinned.as<uint32_t>();
+    if (!g->adv_graphs) g->adv_graphs.reset(new AdvGraphs());
+    AdvGraphs& ag = *g->adv_graphs;
+    if (ag.key[mode] != store) ag.reset(mode);  // captured on another store
+    if (!ag.capture) G1_CUDA(cudaStreamCreateWithFlags(&ag.capture, cudaStreamNonBlocking));
+    static int occ = [] {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, ag_step_kernel<UNIT>, kAgBlock, 0) != cudaSuccess) {
+            cudaGetLastError();
+            b = 1;
+        }
+        return std::max(1, b);
+    }();
+    const uint32_t grid = (uint32_t)g->sm_count * (uint32_t)occ;
+    const uint32_t gi = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(n, 256), grid));
+    ag_init_kernel<<<gi, 256, 0, s>>>(n, src, g->o[0].rp, a);
+    count_launches(1);
+    G1_CUDA(cudaGetLastError());
+    // graphs of 2^i pairs, i growing to kSizes - 1: few read-backs on long
+    // traversals, little overshoot on short ones
+    int i = 2;
+    for (;;) {
+        cudaGraphExec_t& gx = ag.exec[mode][i];
+        if (!gx) {
+            cudaGraph_t graph = nullptr;
+            CaptureScope cs;
+            G1_CUDA(cudaStreamBeginCapture(ag.capture, cudaStreamCaptureModeThreadLocal));
+            ag_enqueue_pairs<UNIT>(g, a, 1u << i, grid, ag.capture);
+            const cudaError_t e = cudaStreamEndCapture(ag.capture, &graph);
+            if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture(advance steps)");
+            const cudaError_t ei = cudaGraphInstantiate(&gx, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ei != cudaSuccess) {
+                gx = nullptr;
+                return fail_cuda(ei, "cudaGraphInstantiate(advance steps)");
+            }
+            ag.key[mode] = store;
+        }
+        G1_CUDA(cudaGraphLaunch(gx, s));
+        count_launches(2ull << i);
+        G1_CUDA(cudaMemcpyAsync(host, a.ctl, 16, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaMemcpyAsync(host + 4, a.c[0], 4, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaStreamSynchronize(s));
+        if (host[4] == 0) break;  // frontier empty after the last pair
+        // Bellman-Ford settles within n rounds; more means corrupted state.
+        if (host[0] > n + 1) return fail(G1_ERR_TIMEOUT, "traversal did not converge within n rounds");
+        if (host[4] > n) return fail(G1_ERR_OVERFLOW, "frontier larger than the vertex count");
+        if (i < AdvGraphs::kSizes - 1) ++i;
+    }
+    if (iters_out) *iters_out = host[0];
+    G1_TRY(copy_out_vertices(g, out, a.dist, s));
+    return check_device_error(g, s);
+}
+
+// ------------------------------------------------ device-driven BLAS engine
+// GraphOne's sparse-frontier BLAS engine loop (engine/blas_gc.h:199-245,
+// apps/sssp_blas.cu:48-84) with every per-iteration decision on the device,
+// so that iterations are captured as CUDA graphs like the advance engine's:
+//   1. x[f] = dist[f] over the frontier (construct_each), frontier size read
+//      from its device counter;
+//   2. the min-plus SpMV over all rows with apply_each fused in its epilogue
+//      (res != MAX && res < dist[v] -> update, append v to the next
+//      frontier);
+//   3. x[f] = MAX over the frontier again; the last block zeroes the
+//      frontier's counter and advances the iteration count.
+// A step whose frontier is empty is a no-op in all its kernels (the SpMV's
+// epilogue reports itself inactive), so graphs may run past convergence.
+// Per iteration the results are those of the reference loop, iteration
+// count included.
+
+// Store: the advance engine's (ag_layout), then x[n].
+inline size_t bg_words(uint32_t n) { return ag_words(n) + (size_t)n; }
+
+__global__ void bg_x_init_kernel(uint32_t* x, uint32_t n) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) x[v] = kU32Max;
+}
+
+// x[f] = dist[f] (reset: MAX) over the frontier of c_in; with reset, the
+// last block also rotates the counters (ag_last_block_rotate).
+__global__ void __launch_bounds__(kAgBlock)
+bg_frontier_x_kernel(const uint32_t* F_in, AgCounter* c_in, uint32_t* ctl, const uint32_t* dist,
+                     uint32_t* x, int reset) {
+    const uint32_t nF = c_in->n;
+    if (nF == 0) return;
+    const uint64_t stride = (uint64_t)gridDim.x * kAgBlock;
+    for (uint64_t i = (uint64_t)blockIdx.x * kAgBlock + threadIdx.x; i < nF; i += stride) {
+        const uint32_t f = F_in[i];
+        x[f] = reset ? kU32Max : dist[f];
+    }
+    if (reset && threadIdx.x == 0) ag_last_block_rotate(c_in, ctl, nF);
+}
+
+// apply_each of the sssp_blas functor under the engine's guard, for the
+// device-driven loop: inactive (the SpMV kernels return at once) when the
+// step's frontier is empty.
+struct BgApplyEpilogue {
+    static constexpr bool kRowsIndependent = true;
+    uint32_t* dist;
+    uint32_t* out;
+    AgCounter* c_out;
+    const AgCounter* c_in;
+    const uint32_t* out_rp;  // out-edge offsets (for the degree sum)
+    __device__ __forceinline__ bool active() const { return c_in->n != 0u; }
+    __device__ __forceinline__ void begin() {}
+    __device__ __forceinline__ void emit(uint32_t v, const uint32_t& res) {
+        if (res != kU32Max && res < dist[v]) {
+            dist[v] = res;
+            append_sum(out, &c_out->n, &c_out->deg, v, out_rp[v + 1] - out_rp[v]);
+        }
+    }
+    template <int BLOCK>
+    __device__ __forceinline__ void block_end(char*) {}
+};
+
+// Builds the SpMV's plan and its kernels' launch facts outside of any capture
+// (they may allocate and query the device).
+template <class SR, class Epi>
+static g1_status bg_prepare_spmv(g1_graph* g, int t) {
+    if (resolve_schedule(g, t, G1_SCHED_AUTO) == G1_SCHED_VECTOR) {
+        (void)vector_grid<SR, Epi>(g);
+        return G1_OK;
+    }
+    uint32_t mg = 0, fg = 0;
+    return merge_grids<SR, Epi>(g, t, &mg, &fg);
+}
+
+template <bool UNIT>
+static g1_status bg_enqueue_pairs(g1_graph* g, const AgState& a, uint32_t* x, const uint32_t* out_rp,
+                                  uint32_t pairs, uint32_t grid, cudaStream_t s) {
+    const int pull_t = 1;
+    for (uint32_t p = 0; p < pairs; ++p)
+        for (int h = 0; h < 2; ++h) {
+            bg_frontier_x_kernel<<<grid, kAgBlock, 0, s>>>(a.F[h], a.c[h], a.ctl, a.dist, x, 0);
+            BgApplyEpilogue e{a.dist, a.F[h ^ 1], a.c[h ^ 1], a.c[h], out_rp};
+            if (UNIT)
+                G1_TRY((run_spmv<BfsU32>(g, pull_t, G1_SCHED_AUTO, x, e, s)));
+            else
+                G1_TRY((run_spmv<MinPlusU32>(g, pull_t, G1_SCHED_AUTO, x, e, s)));
+            bg_frontier_x_kernel<<<grid, kAgBlock, 0, s>>>(a.F[h], a.c[h], a.ctl, a.dist, x, 1);
+            count_launches(2);
+        }
+    return G1_OK;
+}
+
+template <bool UNIT>
+static g1_status blas_graph_traverse(g1_graph* g, uint32_t src, uint32_t* out, uint32_t* iters_out,
+                                     cudaStream_t s) {
+    const uint32_t n = g->n;
+    const int mode = 2 + (UNIT ? 1 : 0);
+    const int pull_t = 1;
+    const uint32_t* out_rp = g->o[0].present ? g->o[0].rp : g->o[pull_t].rp;
+    if (UNIT)
+        G1_TRY((bg_prepare_spmv<BfsU32, BgApplyEpilogue>(g, pull_t)));
+    else
+        G1_TRY((bg_prepare_spmv<MinPlusU32, BgApplyEpilogue>(g, pull_t)));
+    uint32_t* store = nullptr;
+    G1_TRY(g->ws.get("bg_store", bg_words(n), &store));
+    const AgState a = ag_layout(store, n);
+    uint32_t* x = store + ag_words(n);
+    G1_TRY(g->ws.pinned.ensure(64));
+    uint32_t* host = g->ws.pinned.as<uint32_t>();
+    if (!g->adv_graphs) g->adv_graphs.reset(new AdvGraphs());
+    AdvGraphs& ag = *g->adv_graphs;
+    if (ag.key[mode] != store) ag.reset(mode);  // captured on another store
+    if (!ag.capture) G1_CUDA(cudaStreamCreateWithFlags(&ag.capture, cudaStreamNonBlocking));
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(ceil_div(n, kAgBlock), (uint64_t)g->sm_count * 4));
+    const uint32_t gi = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(n, 256), grid));
+    ag_init_kernel<<<gi, 256, 0, s>>>(n, src, out_rp, a);
+    bg_x_init_kernel<<<gi, 256, 0, s>>>(x, n);
+    count_launches(2);
+    G1_CUDA(cudaGetLastError());
+    int i = 1;
+    for (;;) {
+        cudaGraphExec_t& gx = ag.exec[mode][i];
+        if (!gx) {
+            cudaGraph_t graph = nullptr;
+            CaptureScope cs;
+            G1_CUDA(cudaStreamBeginCapture(ag.capture, cudaStreamCaptureModeThreadLocal));
+            const g1_status st = bg_enqueue_pairs<UNIT>(g, a, x, out_rp, 1u << i, grid, ag.capture);
+            const cudaError_t e = cudaStreamEndCapture(ag.capture, &graph);
+            if (st != G1_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+            if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture(BLAS steps)");
+            const cudaError_t ei = cudaGraphInstantiate(&gx, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ei != cudaSuccess) {
+                gx = nullptr;
+                return fail_cuda(ei, "cudaGraphInstantiate(BLAS steps)");
+            }
+            ag.key[mode] = store;
+        }
+        G1_CUDA(cudaGraphLaunch(gx, s));
+        G1_CUDA(cudaMemcpyAsync(host, a.ctl, 16, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaMemcpyAsync(host + 4, a.c[0], 4, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaStreamSynchronize(s));
+        if (host[4] == 0) break;  // frontier empty after the last pair
+        if (host[0] > n + 1) return fail(G1_ERR_TIMEOUT, "traversal did not converge within n rounds");
+        if (host[4] > n) return fail(G1_ERR_OVERFLOW, "frontier larger than the vertex count");
+        if (i < AdvGraphs::kSizes - 1) ++i;
+    }
+    if (iters_out) *iters_out = host[0];
+    G1_TRY(copy_out_vertices(g, out, a.dist, s));
+    return check_device_error(g, s);
+}
+
 struct TrState {
     uint32_t* dist;
     uint32_t* x;
@@ -226,6 +635,9 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
     if ((engine == G1_ENGINE_ADVANCE || engine == G1_ENGINE_AUTO) && !g->o[0].present)
         return fail(G1_ERR_UNSUPPORTED, "push engine needs the out-edge CSR (G1_GRAPH_BUILD_OTHER)");
     if (!UNIT && g->vtype != G1_U32) return fail(G1_ERR_INVALID, "SSSP needs u32 edge weights");
+    if (engine == G1_ENGINE_ADVANCE && advance_graph_suits(g))
+        return advance_graph_traverse<UNIT>(g, src, out, iters_out, s);
+    if (engine == G1_ENGINE_BLAS) return blas_graph_traverse<UNIT>(g, src, out, iters_out, s);
     Workspace& ws = g->ws;
     TrState st;
     G1_TRY(ws.get("tr_dist", n, &st.dist));
@@ -262,7 +674,7 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
     }
     uint32_t it = 0;
     int cur = 0;
-    const uint64_t push_limit = std::max<uint64_t>(1, g->m / 16);
+    const uint64_t push_limit = std::max<uint64_t>(1, g->m / std::max<uint32_t>(1, g->push_div));
     while (nF > 0) {
         ++it;
         // Bellman-Ford settles within n rounds; more means corrupted state.
@@ -386,6 +798,12 @@ static g1_status advance_step(g1_graph* g, const uint32_t* F, uint32_t nF, uint3
     if (host[0] > g->n) return fail(G1_ERR_OVERFLOW, "frontier larger than the vertex count");
     *out_size = host[0];
     return check_device_error(g, s);
+}
+
+g1_status traverse_locked(g1_graph* g, uint32_t src, g1_engine engine, bool unit, uint32_t* out,
+                          uint32_t* iters_out, cudaStream_t s) {
+    return unit ? traverse<true>(g, src, engine, out, iters_out, s)
+                : traverse<false>(g, src, engine, out, iters_out, s);
 }
 
 }  // namespace g1

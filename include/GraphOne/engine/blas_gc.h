@@ -137,6 +137,11 @@ public:
     static constexpr int kIpt = 7;
     static constexpr int kHot = sizeof(info_t) <= 4 ? 16384 : 0;
     static constexpr uint32_t kItems = 32 * kIpt;
+    // With 4-byte edge weights the library's default schedule instead: the
+    // nnz-split tiles (256 nonzeros per warp tile, 32-byte col/val loads,
+    // row starts from a bitmap; include/g1/spmv.cuh), x[0, 32768) cached.
+    static constexpr bool kNnzOk = sizeof(weight_t) == 4 && sizeof(gather_t) <= 8;
+    static constexpr int kNnzHot = sizeof(info_t) <= 4 ? 32768 : 0;
 
     BlasGcEngineBase(comp_t& comp, frontier_t& frontier)
         : base_t(comp, frontier), n_(comp.graph.num_vertices()),
@@ -168,6 +173,33 @@ public:
         args_.carry = static_cast<gather_t*>(carry);
         args_.tail = static_cast<gather_t*>(tail);
         args_.err = nullptr;
+        if constexpr (kNnzOk) {
+            g1_nnz_plan p{};
+            // the tile kernel reads each lane's col/val with 32-byte loads
+            if (!(((uintptr_t)ci | (uintptr_t)val) & 31u) &&
+                g1_spmv_nnz_plan(h, side_, &p) == G1_OK) {
+                nnz_ = true;
+                nargs_.plan.n_rows = p.n_rows;
+                nargs_.plan.nnz = p.nnz;
+                nargs_.plan.n_tiles = p.n_tiles;
+                nargs_.plan.n_nonempty = p.n_nonempty;
+                nargs_.plan.n_empty = p.n_empty;
+                nargs_.plan.tile_seg = p.tile_seg;
+                nargs_.plan.sbits = p.sbits;
+                nargs_.plan.nz_rows = p.rows;
+                nargs_.plan.empty_rows = p.rows + p.n_nonempty;
+                nargs_.plan.row_ptr = p.row_ptr;
+                nargs_.plan.n_fix = p.n_fix;
+                nargs_.plan.fix_tiles = p.fix_tiles;
+                nargs_.plan.fix_info = static_cast<const uint4*>(p.fix_info);
+                nargs_.plan.n_fix_short = p.n_fix_short;
+                nargs_.col = ci;
+                nargs_.val = static_cast<const weight_t*>(val);
+                nargs_.carry = static_cast<gather_t*>(p.carry);
+                nargs_.tail = static_cast<gather_t*>(p.tail);
+                nargs_.err = nullptr;
+            }
+        }
     }
 
     ~BlasGcEngineBase() override {
@@ -178,6 +210,12 @@ public:
 protected:
     template <class Epi>
     void spmv(const info_t* x, const Epi& epi) {
+        if constexpr (kNnzOk) {
+            if (nnz_) {
+                spmv_nnz(x, epi);
+                return;
+            }
+        }
         using L = g1::WarpMergeLayout<SR, kWarps, kIpt, kHot>;
         auto kernel = g1::spmv_wmerge_kernel<SR, Epi, kWarps, kIpt, 1, kHot>;
         static const int occ = [&] {
@@ -199,6 +237,38 @@ protected:
         g1_count_user_launches(2);
     }
 
+    // The nnz-split schedule: main kernel (one 1024-thread block per SM)
+    // and the fixup of the rows that cross tiles and of the empty rows.
+    template <class Epi>
+    void spmv_nnz(const info_t* x, const Epi& epi) {
+        using L = g1::NnzLayout<SR, 32, kNnzHot>;
+        auto kernel = g1::spmv_nnz_kernel<SR, Epi, 32, 1, kNnzHot>;
+        auto fixup = g1::spmv_nnz_fixup_kernel<SR, Epi, 256>;
+        static const int occ = [&] {
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
+            int b = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 32 * 32, L::BYTES);
+            return std::max(1, b);
+        }();
+        static const int focc = [&] {
+            int b = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fixup, 256, 0);
+            return std::max(1, b);
+        }();
+        g1::NnzArgs<SR> a = nargs_;
+        a.x = x;
+        const uint32_t sms = (uint32_t)detail::sm_count();
+        // launched even without tiles: its blocks' epilogue partials count
+        const uint32_t grid = std::max<uint32_t>(
+            1, std::min<uint32_t>((a.plan.n_tiles + 31) / 32, sms * occ));
+        const uint32_t work = std::max(a.plan.n_fix, a.plan.n_empty);
+        const uint32_t fgrid = std::max<uint32_t>(1, std::min<uint32_t>((work + 255) / 256, sms * focc));
+        kernel<<<grid, 32 * 32, L::BYTES, stream_>>>(a, epi);
+        fixup<<<fgrid, 256, 0, stream_>>>(a, epi);
+        detail::check_cuda(cudaGetLastError(), "nnz SpMV launch");
+        g1_count_user_launches(2);
+    }
+
     void fill_x(int which, info_t value) {
         blas_detail::fill_kernel<<<blas_detail::grid_for(n_), 256, 0, stream_>>>(
             x_[which].data(), (uint32_t)n_, value);
@@ -210,6 +280,8 @@ protected:
     cudaStream_t stream_{};
     DenseVec<arch_t::cuda, info_t> x_[2];
     g1::MergeArgs<SR> args_{};
+    bool nnz_ = false;
+    g1::NnzArgs<SR> nargs_{};
     detail::Counters counters_;
 };
 

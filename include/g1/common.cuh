@@ -196,10 +196,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// Default poll limit of the waits on bulk copies: a few seconds, far longer
+// than any copy that is not stuck.
+constexpr uint32_t kWaitPolls = 1u << 22;
 // Waits for phase `parity` of the barrier, giving up after `limit` polls
 // (each poll suspends the thread for a bounded hardware interval).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
-                                                  uint32_t limit = (1u << 22)) {
+                                                  uint32_t limit = kWaitPolls) {
     for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;

@@ -44,6 +44,19 @@
 
 namespace g1 {
 
+// Epilogues may declare `bool active() const`: when it returns false every
+// SpMV kernel returns at once (a step of a captured CUDA graph that has
+// nothing to do, decided on the device).
+template <class E, class = void>
+struct has_active : std::false_type {};
+template <class E>
+struct has_active<E, std::void_t<decltype(std::declval<const E&>().active())>> : std::true_type {};
+template <class E>
+__device__ __forceinline__ bool epi_active(const E& e) {
+    if constexpr (has_active<E>::value) return e.active();
+    else return true;
+}
+
 // Merge-path partition of one CSR for tiles of `items` merge items.
 // tile t spans merge diagonals [t*items, min((t+1)*items, n_rows+nnz)); its
 // start coordinate is (tile_row[t], tile_nnz[t]).  n_tiles+1 entries.
@@ -84,6 +97,7 @@ struct MergeArgs {
     typename SR::value_t* carry;   // n_tiles: partial of the row open at tile end
     typename SR::value_t* tail;    // n_tiles: in-tile partial of a row begun earlier
     uint32_t* err;                 // device error word (kDevTimeout on a stalled copy)
+    uint32_t wait_limit = kWaitPolls;  // polls before a wait on a bulk copy gives up
 };
 
 // (row, partial) pair carried by the tile scan: the row a segment belongs
@@ -241,6 +255,7 @@ __device__ __forceinline__ void merge_issue_tile(const MergeArgs<SR>& a, uint32_
 template <class SR, class Epi, int BLOCK, int IPT, int STAGES>
 __global__ void __launch_bounds__(BLOCK, STAGES == 1 ? 6 : 4)
 spmv_merge_kernel(MergeArgs<SR> a, Epi epi) {
+    if (!epi_active(epi)) return;
     using V = typename SR::value_t;
     using W = typename SR::w_t;
     using L = MergeLayout<SR, BLOCK, IPT, STAGES>;
@@ -283,16 +298,19 @@ spmv_merge_kernel(MergeArgs<SR> a, Epi epi) {
         uint32_t* srow = L::SROW_ALIAS ? reinterpret_cast<uint32_t*>(const_cast<W*>(VA))
                                        : reinterpret_cast<uint32_t*>(dsm + L::SROW_OFF);
 
-        const bool arrived = mbar_wait_bounded(&bar[stage], parity);
+        const bool arrived = mbar_wait_bounded(&bar[stage], parity, a.wait_limit);
         if (__syncthreads_or(!arrived)) {
-            // A copy never completed: record it, let the copy already issued
-            // for the next tile land (bounded), and stop; the host sees the
-            // error word and discards this launch's results.
+            // A copy did not complete in time: record it, let this tile's
+            // copy and the one already issued for the next tile land
+            // (bounded) before the block leaves its shared memory, and stop;
+            // the host sees the error word and discards this launch's results.
             if (tid == 0) {
                 set_error(a.err, kDevTimeout);
+                mbar_wait_bounded(&bar[stage], parity);
                 if (STAGES == 2 && next < a.plan.n_tiles)
                     mbar_wait_bounded(&bar[stage ^ 1u], ((it + 1) >> 1) & 1u);
             }
+            __syncthreads();
             break;
         }
 
@@ -491,6 +509,7 @@ constexpr uint32_t kWarpTilePad = 1024;
 template <class SR, class Epi, int WARPS, int IPT, int MINB, int HOT, bool BOUNDED = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
 spmv_wmerge_kernel(MergeArgs<SR> a, Epi epi) {
+    if (!epi_active(epi)) return;
     using V = typename SR::value_t;
     using X = typename SR::x_t;
     using W = typename SR::w_t;
@@ -714,6 +733,7 @@ __device__ __forceinline__ void warp_tile_issue(const MergeArgs<SR>& a, uint32_t
 template <class SR, class Epi, int WARPS, int IPT, int HOT>
 __global__ void __launch_bounds__(WARPS * 32, 1)
 spmv_wtma_kernel(MergeArgs<SR> a, Epi epi) {
+    if (!epi_active(epi)) return;
     using V = typename SR::value_t;
     using X = typename SR::x_t;
     using W = typename SR::w_t;
@@ -770,9 +790,15 @@ spmv_wtma_kernel(MergeArgs<SR> a, Epi epi) {
             ra = __ldg(a.plan.row_ptr + r_lane);
             rb = __ldg(a.plan.row_ptr + r_lane + 1);
         }
-        const bool arrived = mbar_wait_bounded(bar, phase);
+        const bool arrived = mbar_wait_bounded(bar, phase, a.wait_limit);
         if (!__all_sync(0xffffffffu, arrived)) {
-            if (lane == 0) set_error(a.err, kDevTimeout);
+            // let the copy in flight land (bounded) before the warp leaves
+            // its shared memory
+            if (lane == 0) {
+                set_error(a.err, kDevTimeout);
+                mbar_wait_bounded(bar, phase);
+            }
+            __syncwarp();
             failed = true;
             break;
         }
@@ -902,6 +928,7 @@ spmv_wtma_kernel(MergeArgs<SR> a, Epi epi) {
 template <class SR, class Epi, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 spmv_fixup_kernel(MergeArgs<SR> a, Epi epi) {
+    if (!epi_active(epi)) return;
     using V = typename SR::value_t;
     __shared__ alignas(16) char epi_smem[64 * 8];
     const uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
@@ -1004,6 +1031,7 @@ struct NnzArgs {
     typename SR::value_t* carry;  // n_tiles: partial of the row open at the tile end
     typename SR::value_t* tail;   // n_tiles: in-tile partial of a row begun earlier
     uint32_t* err = nullptr;      // device error word (bounded waits of the bulk variant)
+    uint32_t wait_limit = kWaitPolls;  // polls before a wait on a bulk copy gives up
 };
 
 // Epilogues may split emit into prepare(row) -- the loads that depend only
@@ -1283,6 +1311,7 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
     // the fixup (launched with programmatic dependent launch) may start as
     // soon as every block is past this point
     grid_launch_dependents();
+    if (!epi_active(epi)) return;
     const uint32_t w = threadIdx.x >> 5;
     X* xc = reinterpret_cast<X*>(dsm + L::XC_OFF);
     V* sy = reinterpret_cast<V*>(dsm + L::SY_OFF) + (size_t)w * kNnzTile;
@@ -1317,13 +1346,13 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
                 in.v0 = __ldg(reinterpret_cast<const uint4*>(a.val + j0) + 2 * lane);
                 in.v1 = __ldg(reinterpret_cast<const uint4*>(a.val + j0) + 2 * lane + 1);
             }
-            const bool arrived = mbar_wait_bounded(bar, phase);
+            const bool arrived = mbar_wait_bounded(bar, phase, a.wait_limit);
             if (!__all_sync(0xffffffffu, arrived)) {
-                // give the copy in flight one more bounded chance to land
-                // before the warp leaves its shared memory
+                // let the copy in flight land (bounded) before the warp
+                // leaves its shared memory
                 if (lane == 0) {
                     set_error(a.err, kDevTimeout);
-                    mbar_wait_bounded(bar, phase, 1u << 20);
+                    mbar_wait_bounded(bar, phase);
                 }
                 __syncwarp();
                 break;
@@ -1433,6 +1462,7 @@ __device__ __forceinline__ bool nnz_start_bit(const uint32_t* sbits, uint32_t k)
 template <class SR, class Epi, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 spmv_nnz_fixup_kernel(NnzArgs<SR> a, Epi epi) {
+    if (!epi_active(epi)) return;
     using V = typename SR::value_t;
     constexpr bool kEarly = rows_independent<Epi>::value;
     __shared__ alignas(16) char epi_smem[64 * 8];
@@ -1505,6 +1535,7 @@ template <class SR, class Epi, int BLOCK, int TPR>
 __global__ void __launch_bounds__(BLOCK)
 spmv_vector_kernel(uint32_t n_rows, const uint32_t* row_ptr, const uint32_t* col,
                    const typename SR::w_t* val, const typename SR::x_t* x, Epi epi) {
+    if (!epi_active(epi)) return;
     using V = typename SR::value_t;
     __shared__ alignas(16) char epi_smem[64 * 8];
     const uint32_t g = (blockIdx.x * BLOCK + threadIdx.x);
@@ -1537,6 +1568,98 @@ spmv_vector_kernel(uint32_t n_rows, const uint32_t* row_ptr, const uint32_t* col
         if (lane == 0 && row < n_rows) epi.emit(row, acc);
     }
     epi.template block_end<BLOCK>(epi_smem);
+}
+
+// ------------------------------------------- column-sorted partitions
+// The rows are cut into partitions of at most kCsRows consecutive rows and
+// about equal nonzero counts; inside a partition the nonzeros are stored in
+// column order (stable), each with its row's offset in the partition (u16)
+// and its value.  One block folds one partition at a time into a
+// shared-memory accumulator per row with the semiring's shared-memory atomic
+// reduce, then emits every row of the partition in order (empty rows as the
+// identity) -- no carries, no fixup kernel.
+//
+// Why column order: a partition of ~m/(2 SMs) nonzeros gathers x entries
+// that share 32-byte sectors (the hot low-id columns of the degree-ordered
+// layout and clusters among the rest); in column order the gathers of a
+// sector are adjacent in time, so they are served by L1 or merged while in
+// flight, instead of one L2 request per gather.  The price is 2 more bytes
+// per nonzero (the row offset) and, for plus-times, a fold order that
+// depends on the atomics' timing (min-plus is order-free and exact).
+
+constexpr uint32_t kCsRows = 16384;  // rows per partition (the accumulators)
+constexpr uint32_t kCsIpt = 8;       // nonzeros per thread and round
+
+template <class SR>
+struct CsArgs {
+    uint32_t n_parts;
+    const uint32_t* part_row;    // n_parts + 1: first row of each partition
+    const uint32_t* part_nnz;    // n_parts + 1: first nonzero (column-sorted arrays)
+    const uint32_t* col;         // column-sorted per partition, padded by kCsIpt
+    const uint16_t* lrow;        // row - part_row[p]
+    const typename SR::w_t* val;
+    const typename SR::x_t* x;
+};
+
+// Shared-memory accumulators of one partition, then the epilogue's scratch.
+template <class SR>
+struct CsLayout {
+    using V = typename SR::value_t;
+    static constexpr size_t Y_BYTES = ((size_t)kCsRows * sizeof(V) + 15) / 16 * 16;
+    static constexpr size_t EPI_OFF = Y_BYTES;
+    static constexpr size_t BYTES = EPI_OFF + 512;
+};
+
+template <class SR, class Epi, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1)
+spmv_cs_kernel(CsArgs<SR> a, Epi epi) {
+    if (!epi_active(epi)) return;
+    using V = typename SR::value_t;
+    using L = CsLayout<SR>;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    V* ys = reinterpret_cast<V*>(dsm);
+    epi.begin();
+    for (uint32_t p = blockIdx.x; p < a.n_parts; p += gridDim.x) {
+        const uint32_t r0 = a.part_row[p], rows = a.part_row[p + 1] - r0;
+        const uint32_t j0 = a.part_nnz[p], j1 = a.part_nnz[p + 1];
+        for (uint32_t i = threadIdx.x; i < rows; i += BLOCK) ys[i] = SR::identity();
+        __syncthreads();
+        // rounds of BLOCK * 8 nonzeros from j0 rounded down to 8: each thread
+        // loads 8 consecutive nonzeros (32-byte col and val loads, 16-byte
+        // row-offset loads); those outside [j0, j1) are masked
+        const uint32_t jb = j0 & ~(kCsIpt - 1u);
+        for (uint32_t base = jb; base < j1; base += BLOCK * kCsIpt) {
+            const uint32_t j = base + threadIdx.x * kCsIpt;
+            if (j < j1) {
+                uint4 c0, c1, v0, v1;
+                ldg_v8_stream(a.col + j, c0, c1);
+                ldg_v8_stream(a.val + j, v0, v1);
+                const uint4 lr = __ldg(reinterpret_cast<const uint4*>(a.lrow + j));
+                const uint32_t cc[kCsIpt] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+                const uint32_t vv[kCsIpt] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+                const uint32_t rr[kCsIpt] = {lr.x & 0xFFFFu, lr.x >> 16, lr.y & 0xFFFFu, lr.y >> 16,
+                                             lr.z & 0xFFFFu, lr.z >> 16, lr.w & 0xFFFFu, lr.w >> 16};
+                typename SR::x_t xv[kCsIpt];
+#pragma unroll
+                for (int u = 0; u < (int)kCsIpt; ++u) {
+                    const bool in = j + u >= j0 && j + u < j1;
+                    xv[u] = in ? ldg_any(a.x + cc[u]) : typename SR::x_t{};
+                }
+#pragma unroll
+                for (int u = 0; u < (int)kCsIpt; ++u) {
+                    if (j + u >= j0 && j + u < j1) {
+                        typename SR::w_t w;
+                        memcpy(&w, &vv[u], 4);
+                        SR::reduce_shared(&ys[rr[u]], SR::combine(w, xv[u]));
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < rows; i += BLOCK) epi.emit(r0 + i, ys[i]);
+        __syncthreads();
+    }
+    epi.template block_end<BLOCK>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
 }
 
 // ----------------------------------------------------------- epilogues

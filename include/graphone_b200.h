@@ -103,6 +103,14 @@ uint64_t g1_kernel_launches(void);
 /* Adds n to that counter: the functor-templated engines of the GraphOne
  * headers launch their kernels from the application and report them here. */
 void g1_count_user_launches(uint64_t n);
+/* For tests of the timeout paths: every bounded device wait launched after
+ * this call (the near-far engine's grid barrier, the waits on bulk copies of
+ * the TMA-staged SpMV variants) gives up after `polls` polls (0: at the
+ * first poll) and the call reports G1_ERR_TIMEOUT; a negative value
+ * restores the defaults (a few seconds each).  Copies already in flight are
+ * still waited for before a kernel leaves.  Process-wide.  No GraphOne
+ * counterpart (GraphOne's kernels never wait on one another). */
+g1_status g1_test_set_wait_polls(int64_t polls);
 /* Kernel timing of the SpMV launches (main merge / vector kernels only):
  * between g1_profile_begin and g1_profile_end every such launch is
  * bracketed by CUDA events on its own stream; g1_profile_end synchronises
@@ -142,6 +150,29 @@ size_t g1_graph_device_bytes(const g1_graph* g);
 g1_status g1_spmv_plan(g1_graph* g, int transpose, uint32_t items_per_tile,
                        uint32_t* n_tiles, const uint32_t** tile_row,
                        const uint32_t** tile_nnz, void** carry, void** tail);
+/* The nnz-split plan of one orientation (built once per graph): tiles of
+ * 256 nonzeros, the rank of the row holding each tile's first nonzero
+ * (tile_seg, n_tiles+1), the row-start bitmap over the nonzeros (sbits),
+ * the non-empty rows in order followed by the empty rows (rows, n_rows), the
+ * tiles in which a row begun in an earlier tile ends (fix_tiles, n_fix) with
+ * {tile, row, first tile of the row, 0} per such tile (fix_info, 16 bytes
+ * each; the first n_fix_short end in the tile after their first), and
+ * carry/tail (room for n_tiles+1 values of up to 16 bytes).  The arrays stay
+ * owned by the graph.  For GraphOne-API engines that instantiate the nnz
+ * kernels with their own functors (replaces the merge-path plan of
+ * SpmvDispatcher<SpmvCudaCsrMergeBased>, archi/blas/spmv/cuda/cuda.cuh:75-92). */
+typedef struct g1_nnz_plan {
+    uint32_t n_rows, nnz, n_tiles, n_nonempty, n_empty, n_fix, n_fix_short;
+    const uint32_t* tile_seg;
+    const uint32_t* sbits;
+    const uint32_t* rows;
+    const uint32_t* row_ptr;
+    const uint32_t* fix_tiles;
+    const void* fix_info;
+    void* carry;
+    void* tail;
+} g1_nnz_plan;
+g1_status g1_spmv_nnz_plan(g1_graph* g, int transpose, g1_nnz_plan* out);
 /* y = A (semiring) x over one orientation (replaces SpmvDispatcher::operator(),
  * archi/blas/spmv/cuda/cuda.cuh:94-99; y stays on the device stream, no
  * device synchronisation). x, y device pointers of n entries. */
@@ -187,6 +218,17 @@ g1_status g1_spmv_noalloc(const uint32_t* row_ptr, const uint32_t* col, const vo
  * variant. */
 g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, int* merge_variant,
                       void* stream);
+/* Picks this graph's push/pull thresholds by timing SSSP from n_sources
+ * (0: 16, at most 64) sources spread over the vertices with out-edges: the
+ * single-source AUTO engine pushes while the frontier's out-degree sum is
+ * below m / push_div (candidates 4 .. 128, default 16), and the batched
+ * engines list the next iteration's rows while the changed vertices'
+ * out-edges are below (m + n) / slot_div (candidates 2 .. 32, default 8).
+ * The chosen divisors are returned (may be NULL) and kept for the graph.
+ * Results never depend on them.  No GraphOne counterpart (GraphOne has no
+ * direction switch: AdvanceGC always pushes, BlasGcEngine always pulls). */
+g1_status g1_autotune_traversal(g1_graph* g, uint32_t n_sources, uint32_t* push_div,
+                                uint32_t* slot_div, void* stream);
 
 /* ------------------------------------------------------------- algorithms */
 /* PageRank for a fixed iteration count (Run<PRFunctor> over

@@ -47,7 +47,7 @@ def test_status_strings_and_argument_errors_without_gpu():
 NULL_OK = {"g1_graph_destroy", "g1_mem_free", "g1_server_destroy", "g1_profile_begin",
            "g1_profile_end", "g1_release_cached_memory", "g1_stream_sync",
            "g1_graph_device_bytes", "g1_kernel_launches", "g1_count_user_launches",
-           "g1_status_string", "g1_last_error", "g1_version"}
+           "g1_status_string", "g1_last_error", "g1_version", "g1_test_set_wait_polls"}
 
 
 def test_every_entry_point_rejects_null_arguments_before_any_device_work():
@@ -80,7 +80,7 @@ def test_python_variant_table_matches_the_launcher():
     d = int(re.search(r"kDefaultVariant\s*=\s*(\d+)", src).group(1))
     table = re.search(r"kMergeVariants\[\]\s*=\s*\{(.*?)\};", src, re.S).group(1)
     kinds = [int(k) for k in re.findall(r"\{\s*(\d+)\s*,", table)]
-    names = {0: "warp", 1: "cta_tma", 2: "warp_tma", 3: "nnz"}
+    names = {0: "warp", 1: "cta_tma", 2: "warp_tma", 3: "nnz", 4: "colsort"}
     assert len(g1.MERGE_VARIANTS) == n == len(kinds)
     assert tuple(names[k] for k in kinds) == g1.MERGE_VARIANTS
     assert g1.DEFAULT_MERGE_VARIANT == d

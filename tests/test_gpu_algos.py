@@ -189,3 +189,21 @@ def test_pagerank_rmat20_within_1e6_of_fp64(cuda, relabel):
     r = G.pagerank(0.85, 30, g1.PR_DANGLING)
     err = O.rel_l1(r, O.pagerank_f64(trp, tci, tv, 0.85, 30, 1))
     assert err < 1e-6, err  # tolerance: relative L1 vs the FP64 oracle
+
+
+@pytest.mark.parametrize("name", ["rmat10_sym", "rmat11_dir", "star20k", "grid32"])
+def test_autotune_traversal_keeps_results_exact(cuda, name):
+    """g1_autotune_traversal picks the push/pull divisors among its
+    candidates; SSSP and BFS (single-source AUTO and batched) stay bit-exact."""
+    g = GRAPHS[name]
+    G = g1.Graph.from_gen(g, relabel=(name == "rmat10_sym"))
+    rp, ci, v = g.np("n")
+    push_div, slot_div = G.autotune_traversal(8)
+    assert push_div in (4, 8, 16, 32, 64, 128) and slot_div in (2, 4, 8, 16, 32)
+    srcs = sorted({0, g.n // 3, g.n - 1})
+    for s in srcs:
+        assert np.array_equal(G.sssp(s, g1.ENGINE_AUTO), O.dijkstra_u32(rp, ci, v, s)), (name, s)
+        assert np.array_equal(G.bfs(s, g1.ENGINE_AUTO), O.bfs(rp, ci, s)), (name, s)
+    d = G.sssp_batch(np.array(srcs, np.uint32))
+    for j, s in enumerate(srcs):
+        assert np.array_equal(d[j], O.dijkstra_u32(rp, ci, v, s)), (name, s)
