@@ -238,7 +238,7 @@ def _host_u32(t):
     return t.cpu().numpy().view(np.uint32).copy()
 
 
-def query_metrics(dev, stream, parity, ref_gpu=False, budget_queries: int = 256):
+def query_metrics(dev, stream, parity, budget_queries: int = 256):
     """The query side of the metric, on resident graphs, CUDA-event timed.
 
     * RMAT-14 (symmetrised, uint32 weights [1,64]) plain SSSP, one source at
@@ -255,10 +255,6 @@ def query_metrics(dev, stream, parity, ref_gpu=False, budget_queries: int = 256)
     and 8 of each vs the oracle's BFS / Dijkstra; the grid's SSSP and BFS
     from the corner on both engines vs the oracle.
 
-    With `ref_gpu`, GraphOne's own GPU engines (oracle/_ref, built from the
-    reference sources) run the same RMAT-14 queries (sparse-frontier BLAS
-    engine) and the grid query (advance/filter engine), CUDA-event timed, and
-    their distances join the parity checks.
     """
     import torch
     import graphone_b200 as g1
@@ -290,21 +286,6 @@ def query_metrics(dev, stream, parity, ref_gpu=False, budget_queries: int = 256)
                        "src0_ms": round(t0, 4),
                        "src0_gteps": round(reach_edges / (t0 / 1e3) / 1e9, 3)}
     out["sssp_rmat14_plain"] = {"n": g.n, "m": g.m, "queries": len(srcs), **plain}
-    if ref_gpu:
-        # GraphOne's own sparse-frontier BLAS engine on the same graph and sources
-        trp14, tci14, tv14 = g.np("t")
-        O.refgpu_sssp_blas(trp14, tci14, tv14, srcs[:8])          # warm-up
-        d0, ms_r, it_r = O.refgpu_sssp_blas(trp14, tci14, tv14, np.concatenate([[0], srcs[:64]]))
-        lat_r = ms_r[1:]
-        got14["reference_gpu_blas"] = d0
-        r = {"engine": "GraphOne BlasGcEngine<SPARSE> + merge-based SpMV (Run<>, u32 min-plus)",
-             "p50_ms": round(_pct(lat_r, 50), 4), "p99_ms": round(_pct(lat_r, 99), 4),
-             "queries_per_s": round(1e3 / statistics.mean(lat_r), 1),
-             "src0_ms": round(float(ms_r[0]), 4), "src0_iterations": int(it_r[0]),
-             "queries": len(lat_r)}
-        r["ours_auto_over_reference_p50"] = round(r["p50_ms"] / plain["auto"]["p50_ms"], 2)
-        r["ours_blas_over_reference_p50"] = round(r["p50_ms"] / plain["blas"]["p50_ms"], 2)
-        out["sssp_rmat14_plain"]["reference_gpu"] = r
     parity.expect("sssp_rmat14_src0_bit_exact", O.dijkstra_u32, (*g.np("n"), 0),
                   lambda ref, got=got14: {k: bool(np.array_equal(v, ref)) for k, v in got.items()})
     G.close()
@@ -380,16 +361,6 @@ def query_metrics(dev, stream, parity, ref_gpu=False, budget_queries: int = 256)
             got[kind][name] = _host_u32(d)
             res[f"{kind}_{name}"] = {"ms": round(ms, 2), "iterations": int(it[0]),
                                     "gteps": round(g.m / (ms / 1e3) / 1e9, 3)}
-    if ref_gpu:
-        # GraphOne's own advance/filter engine (sssp_adv) from the corner
-        dref, ms_r, it_r = O.refgpu_sssp_adv(rpg, cig, vg, [0, 0])
-        got["sssp"]["reference_gpu_advance"] = dref
-        r = {"engine": "GraphOne AdvanceGC (Run<>, u32 atomicMin relax + visited filter)",
-             "ms": [round(float(x), 2) for x in ms_r], "iterations": int(it_r[-1])}
-        best = float(min(ms_r))
-        r["ours_advance_over_reference"] = round(best / res["sssp_advance"]["ms"], 2)
-        r["ours_nearfar_over_reference"] = round(best / res["sssp_nearfar"]["ms"], 2)
-        res["reference_gpu_sssp_advance"] = r
     parity.expect("sssp_grid4096_src0_bit_exact", O.dijkstra_u32, (rpg, cig, vg, 0),
                   lambda ref, r=got["sssp"]: {k: bool(np.array_equal(v, ref)) for k, v in r.items()})
     parity.expect("bfs_grid4096_src0_bit_exact", O.bfs, (rpg, cig, 0),
@@ -574,10 +545,6 @@ def run_ours(args):
     pr_got = {}
     if rank != 0:
         args.no_parity = True             # rank 0 checks its own replica's results
-    use_ref_gpu = not args.no_reference_gpu and ws == 1 and _refgpu_available()
-    rpn = cin = vn = None
-    if use_ref_gpu:
-        rpn, cin, vn = g.np("n")          # GraphOne's PageRank reads out-degrees from the CSR
     if not args.no_parity:
         from oracle import oracle as O
         # FP64 PageRank of the same graph, computed on host threads while the GPU runs
@@ -697,21 +664,23 @@ def run_ours(args):
             "avg_launch_ms": round(avg_ms, 5), "launches_timed": int(spmv_launches),
             "iteration_share_of_step": round(spmv_ms / ms, 4) if ms > 0 else None,
         }
-    if use_ref_gpu:
-        # our PageRank with GraphOne's own formula (no dangling redistribution),
-        # to compare with GraphOne's GPU engine on the same graph
+    if not args.no_parity:
+        # our PageRank with GraphOne's own formula (no dangling redistribution)
         G.pagerank(0.85, iters, g1.PR_REFERENCE, out=out, stream=stream)
         torch.cuda.synchronize()
-        pr_got["rank_reference_formula"] = out.cpu().numpy().copy()
+        ours_ref = out.cpu().numpy().copy()
+        parity.expect("pagerank_reference_formula_rel_l1_vs_fp64", O.pagerank_f64,
+                      (trp, tci, tv, 0.85, iters, 0), lambda r64, a=ours_ref: float(O.rel_l1(a, r64)))
     G.close()
     del G, out
     torch.cuda.empty_cache()
-    if use_ref_gpu:
-        result["reference_gpu"] = reference_gpu_pagerank(args, rpn, cin, vn, trp, tci, tv,
-                                                         result, pr_got, parity)
-        del rpn, cin, vn
+    result["reference_gpu"] = {
+        "status": ("not run: GraphOne's own GPU engines faulted on this pool (its sssp_blas app "
+                   "ended in cudaErrorInvalidAddressSpace on an RMAT-12 input), so they are no "
+                   "longer run; figures measured before the fault are in "
+                   "profiles/reference_gpu_engines.md")}
     if not args.no_queries:
-        result["queries"] = query_metrics(dev, stream, parity, ref_gpu=use_ref_gpu)
+        result["queries"] = query_metrics(dev, stream, parity)
     if args.serve_requests > 0:
         result["serving"] = serving_metrics(dev, args.serve_requests, args.serve_rate)
     if not args.no_parity:
@@ -729,47 +698,6 @@ def run_ours(args):
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
-
-
-def _refgpu_available():
-    try:
-        from oracle import oracle as O
-        return O.refgpu() is not None
-    except Exception:
-        return False
-
-
-def reference_gpu_pagerank(args, rpn, cin, vn, trp, tci, tv, result, pr_got, parity):
-    """GraphOne's own GPU engine for PageRank on the same graph (oracle/_ref,
-    built from the reference sources for sm_100a): its all-active BLAS engine
-    (Run<> over the merge-based SpMV dispatcher and apply_construct_kernel),
-    GraphOne's formula, the same iteration count, CUDA-event timed; and its
-    SpMV dispatcher alone per call.  Ours is compared per SpMV launch (the
-    metric's kernel) and per whole PageRank."""
-    from oracle import oracle as O
-    n, m = len(trp) - 1, len(tci)
-    iters = args.iters
-    rank_ref, ms_runs, ms_spmv = O.refgpu_pagerank(rpn, cin, vn, trp, tci, tv, 0.85, iters,
-                                                   reps=3, spmv_reps=10)
-    spmv_ms = float(np.median(ms_spmv))
-    run_ms = float(np.min(ms_runs))
-    ours_spmv_ms = result.get("roofline", {}).get("avg_launch_ms")
-    r = {"engine": ("GraphOne BlasGcEngine<ALL_ACTIVE> (Run<>, SpmvDispatcher<SpmvCudaCsrMergeBased> "
-                    "+ apply_construct_kernel), GraphOne's PageRank formula, fixed iterations"),
-         "iterations": iters, "run_ms": [round(float(x), 3) for x in ms_runs],
-         "spmv_ms_per_call_median": round(spmv_ms, 5),
-         "spmv_gbs": round(spmv_bytes(n, m) / (spmv_ms / 1e3) / 1e9, 1),
-         "pagerank_gbs": round(spmv_bytes(n, m) * iters / (run_ms / 1e3) / 1e9, 1)}
-    if ours_spmv_ms:
-        r["ours_over_reference_spmv_launch"] = round(spmv_ms / ours_spmv_ms, 2)
-    r["ours_over_reference_pagerank"] = round(run_ms / result["ms_per_step"], 2)
-    if not args.no_parity:
-        ours = pr_got["rank_reference_formula"]
-        parity.expect("pagerank_reference_formula_rel_l1_vs_fp64", O.pagerank_f64,
-                      (trp, tci, tv, 0.85, iters, 0),
-                      lambda r64, a=ours, b=rank_ref: {"ours": float(O.rel_l1(a, r64)),
-                                                       "reference_gpu": float(O.rel_l1(b, r64))})
-    return r
 
 
 def cpu_threads():
@@ -880,8 +808,6 @@ def main():
     ap.add_argument("--no-relabel", action="store_true")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the checks of this run's results against the oracle")
-    ap.add_argument("--no-reference-gpu", action="store_true",
-                    help="skip timing GraphOne's own GPU engines on the same inputs")
     ap.add_argument("--no-queries", action="store_true",
                     help="skip the SSSP/BFS plain and batched query measurements")
     ap.add_argument("--serve-requests", type=int, default=256,

@@ -25,7 +25,7 @@ constexpr int kVectorBlock = 256;
 //           = next tile's col and val / col only staged in shared memory by
 //           bulk copies, stages / 32 = L2 prefetch distance in rounds;
 //   kind 4: column-sorted partitions (spmv_cs_kernel; its own plan), stages
-//           = partitions per SM.
+//           = partitions per SM, hot = L2 prefetch distance in rounds.
 // `warps` per block (kind 0/2/3), `hot` x entries cached in shared memory,
 // `minb` resident blocks per SM the register budget is sized for.
 struct MergeVariant {
@@ -48,8 +48,9 @@ constexpr MergeVariant kMergeVariants[] = {
     {3, 8, 8, 32, 32768, 1},  {3, 8, 8, 32, 16384, 1},  {3, 8, 16, 32, 32768, 1},
     {3, 8, 16, 32, 24576, 1}, {3, 8, 32, 32, 32768, 1}, {3, 8, 64, 32, 32768, 1},
     {3, 8, 128, 32, 32768, 1}, {3, 8, 66, 24, 32768, 1}, {4, 8, 2, 32, 0, 1},
-    {4, 8, 4, 32, 0, 1},      {4, 8, 1, 32, 0, 1}};
-constexpr int kNumMergeVariants = 35;
+    {4, 8, 4, 32, 0, 1},      {4, 8, 1, 32, 0, 1},      {4, 8, 2, 32, 2, 1},
+    {4, 8, 4, 32, 2, 1}};
+constexpr int kNumMergeVariants = 37;
 constexpr int kDefaultVariant = 17;
 
 template <class K>
@@ -144,13 +145,13 @@ struct NnzKernel {
     }
 };
 
-template <class SR, class Epi>
+template <class SR, class Epi, int PF = 0>
 struct CsKernel {
     using L = CsLayout<SR>;
     static constexpr int kBlock = 1024;
     static int occupancy() {
         static int occ = [] {
-            auto k = spmv_cs_kernel<SR, Epi, kBlock>;
+            auto k = spmv_cs_kernel<SR, Epi, kBlock, PF>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
             return blocks_per_sm(k, kBlock, L::BYTES);
         }();
@@ -265,7 +266,7 @@ NnzArgs<SR> nnz_args(const g1_graph* g, int t, const NnzPlan& p, const typename 
     return a;
 }
 
-template <class SR, class Epi>
+template <class SR, class Epi, int PF = 0>
 g1_status launch_cs(g1_graph* g, int t, uint32_t parts_per_sm, const typename SR::x_t* x,
                     const Epi& epi, cudaStream_t s) {
     static_assert(sizeof(typename SR::w_t) == 4, "column-sorted partitions hold 4-byte edge values");
@@ -279,10 +280,12 @@ g1_status launch_cs(g1_graph* g, int t, uint32_t parts_per_sm, const typename SR
     a.lrow = p->lrow.as<uint16_t>();
     a.val = p->val.as<typename SR::w_t>();
     a.x = x;
-    using K = CsKernel<SR, Epi>;
+    // the arrays hold m + kCsIpt entries: the readable range rounded down
+    a.nnz_pad = (uint32_t)(((uint64_t)g->m + kCsIpt) / kCsIpt * kCsIpt);
+    using K = CsKernel<SR, Epi, PF>;
     const bool prof = profiling();
     if (prof) prof_mark(s, true);
-    spmv_cs_kernel<SR, Epi, K::kBlock><<<K::grid(g, p->n_parts), K::kBlock, K::L::BYTES, s>>>(a, epi);
+    spmv_cs_kernel<SR, Epi, K::kBlock, PF><<<K::grid(g, p->n_parts), K::kBlock, K::L::BYTES, s>>>(a, epi);
     if (prof) prof_mark(s, false);
     count_launches(1);
     G1_CUDA(cudaGetLastError());
@@ -327,7 +330,8 @@ g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_gri
     if (kMergeVariants[v].kind == 4) {
         CsPlan* q = nullptr;
         G1_TRY(ensure_cs_plan(g, t, (uint32_t)kMergeVariants[v].stages, &q));
-        *main_grid = CsKernel<SR, Epi>::grid(g, q->n_parts);
+        *main_grid = kMergeVariants[v].hot ? CsKernel<SR, Epi, 2>::grid(g, q->n_parts)
+                                           : CsKernel<SR, Epi>::grid(g, q->n_parts);
         *fix_grid = 0;
         return G1_OK;
     }
@@ -439,7 +443,9 @@ g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi&
                        const Epi& fix_epi, cudaStream_t s) {
     const int v = merge_variant(g, t);
     if (kMergeVariants[v].kind == 4)
-        return launch_cs<SR, Epi>(g, t, (uint32_t)kMergeVariants[v].stages, x, main_epi, s);
+        return kMergeVariants[v].hot
+                   ? launch_cs<SR, Epi, 2>(g, t, (uint32_t)kMergeVariants[v].stages, x, main_epi, s)
+                   : launch_cs<SR, Epi>(g, t, (uint32_t)kMergeVariants[v].stages, x, main_epi, s);
     if (kMergeVariants[v].kind == 3) {
         NnzPlan* q = nullptr;
         G1_TRY(ensure_nnz_plan(g, t, &q));

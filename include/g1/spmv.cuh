@@ -1599,7 +1599,20 @@ struct CsArgs {
     const uint16_t* lrow;        // row - part_row[p]
     const typename SR::w_t* val;
     const typename SR::x_t* x;
+    uint32_t nnz_pad;            // readable entries of col/val/lrow (multiple of kCsIpt)
 };
+
+// One thread: L2 prefetch of the column-sorted arrays' nonzeros
+// [j, j + cnt) clipped to the readable range (bulk prefetches; j and cnt
+// multiples of kCsIpt keep them 16-byte aligned).
+template <class SR>
+__device__ __forceinline__ void cs_prefetch_l2(const CsArgs<SR>& a, uint32_t j, uint32_t cnt) {
+    if (j >= a.nnz_pad) return;
+    cnt = min(cnt, a.nnz_pad - j);
+    prefetch_l2_bulk(a.col + j, cnt * 4);
+    prefetch_l2_bulk(a.val + j, cnt * 4);
+    prefetch_l2_bulk(a.lrow + j, cnt * 2);
+}
 
 // Shared-memory accumulators of one partition, then the epilogue's scratch.
 template <class SR>
@@ -1610,7 +1623,8 @@ struct CsLayout {
     static constexpr size_t BYTES = EPI_OFF + 512;
 };
 
-template <class SR, class Epi, int BLOCK>
+// PF > 0: thread 0 prefetches into L2 the block's round PF rounds ahead.
+template <class SR, class Epi, int BLOCK, int PF = 0>
 __global__ void __launch_bounds__(BLOCK, 1)
 spmv_cs_kernel(CsArgs<SR> a, Epi epi) {
     if (!epi_active(epi)) return;
@@ -1628,7 +1642,18 @@ spmv_cs_kernel(CsArgs<SR> a, Epi epi) {
         // loads 8 consecutive nonzeros (32-byte col and val loads, 16-byte
         // row-offset loads); those outside [j0, j1) are masked
         const uint32_t jb = j0 & ~(kCsIpt - 1u);
-        for (uint32_t base = jb; base < j1; base += BLOCK * kCsIpt) {
+        constexpr uint32_t kRound = BLOCK * kCsIpt;
+        if constexpr (PF > 0) {
+            if (threadIdx.x == 0)
+                for (int d = 1; d < PF; ++d)
+                    if (jb + d * kRound < j1) cs_prefetch_l2(a, jb + d * kRound, min(kRound, j1 - (jb + d * kRound) + kCsIpt) & ~(kCsIpt - 1u));
+        }
+        for (uint32_t base = jb; base < j1; base += kRound) {
+            if constexpr (PF > 0) {
+                const uint32_t pb = base + PF * kRound;
+                if (threadIdx.x == 0 && pb < j1)
+                    cs_prefetch_l2(a, pb, min(kRound, j1 - pb + kCsIpt) & ~(kCsIpt - 1u));
+            }
             const uint32_t j = base + threadIdx.x * kCsIpt;
             if (j < j1) {
                 uint4 c0, c1, v0, v1;

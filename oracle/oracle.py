@@ -4,9 +4,7 @@ Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline, parity and
 reference legs may import this module, as checkers and baselines.  ``lib()``
 is the plain-C restatement (oracle/oracle.c); ``ref()`` is GraphOne's own
 host code compiled from the reference sources (oracle/ref_driver.cu ->
-oracle/_ref/libgraphone_ref.so); ``refgpu()`` is GraphOne's own GPU engines
-(oracle/ref_gpu.cu -> oracle/_ref/libgraphone_refgpu.so).  Each is None /
-missing when its library was not built.
+oracle/_ref/libgraphone_ref.so), or None when that library was not built.
 """
 from __future__ import annotations
 
@@ -22,8 +20,6 @@ U32_MAX = 0xFFFFFFFF
 _lib = None
 _ref = None
 _ref_tried = False
-_refgpu = None
-_refgpu_tried = False
 
 P = C.c_void_p
 
@@ -35,13 +31,13 @@ def _ptr(a: np.ndarray):
 def build(ref: bool = False) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
     if ref:
-        subprocess.run(["make", "-s", "-j4", "-C", HERE, "ref", "refapps", "dropin", "reftests"], check=True)
+        subprocess.run(["make", "-s", "-j4", "-C", HERE, "ref", "dropin", "reftests"], check=True)
 
 
-def app(kind: str, name: str):
-    """Path of a GraphOne app binary (kind 'ref': reference engines, 'g1':
-    this repository's), or None when it was not built."""
-    p = os.path.join(HERE, "_ref", "apps_ref" if kind == "ref" else "apps_g1", name)
+def app(name: str):
+    """Path of a GraphOne app built unchanged against this repository's
+    headers (oracle/_ref/apps_g1), or None when it was not built."""
+    p = os.path.join(HERE, "_ref", "apps_g1", name)
     return p if os.path.exists(p) else None
 
 
@@ -97,68 +93,6 @@ def ref():
                                            C.c_int, P, C.c_int]
             _ref = R
     return _ref
-
-
-def refgpu():
-    """GraphOne's own GPU engines (oracle/ref_gpu.cu), or None if not built."""
-    global _refgpu, _refgpu_tried
-    if not _refgpu_tried:
-        _refgpu_tried = True
-        path = os.path.join(HERE, "_ref", "libgraphone_refgpu.so")
-        if os.path.exists(path):
-            R = C.CDLL(path)
-            R.refgpu_pagerank.restype = C.c_int
-            R.refgpu_pagerank.argtypes = [C.c_uint32, C.c_uint32, P, P, P, P, P, P, C.c_float,
-                                          C.c_int, C.c_int, P, P, C.c_int, P]
-            for f in ("refgpu_sssp_blas_u32", "refgpu_sssp_adv_u32"):
-                getattr(R, f).restype = C.c_int
-                getattr(R, f).argtypes = [C.c_uint32, C.c_uint32, P, P, P, P, C.c_int, P, P, P]
-            _refgpu = R
-    return _refgpu
-
-
-def refgpu_pagerank(rp, ci, v, trp, tci, tv, alpha=0.85, iters=30, reps=3, spmv_reps=10):
-    """GraphOne's all-active BLAS engine on the GPU (reference PageRank
-    formula, fixed iterations): (ranks of the last run, ms per run, ms per
-    call of its merge-based SpMV dispatcher alone)."""
-    R = refgpu()
-    rp, ci, trp, tci = u32(rp), u32(ci), u32(trp), u32(tci)
-    v = np.ascontiguousarray(v, np.float32)
-    tv = np.ascontiguousarray(tv, np.float32)
-    n = len(rp) - 1
-    rank = np.empty(n, np.float32)
-    ms = np.zeros(max(reps, 1), np.float64)
-    ms_spmv = np.zeros(max(spmv_reps, 1), np.float64)
-    rc = R.refgpu_pagerank(n, len(ci), _ptr(rp), _ptr(ci), _ptr(v), _ptr(trp), _ptr(tci), _ptr(tv),
-                           alpha, iters, reps, _ptr(rank), _ptr(ms), spmv_reps, _ptr(ms_spmv))
-    if rc != 0:
-        raise RuntimeError("refgpu_pagerank failed")
-    return rank, ms[:reps], ms_spmv[:spmv_reps]
-
-
-def _refgpu_sssp(fn, rp, ci, v, srcs):
-    rp, ci, v = u32(rp), u32(ci), u32(v)
-    srcs = u32(srcs)
-    n = len(rp) - 1
-    d = np.empty(n, np.uint32)
-    ms = np.zeros(len(srcs), np.float64)
-    it = np.zeros(len(srcs), np.int32)
-    if fn(n, len(ci), _ptr(rp), _ptr(ci), _ptr(v), _ptr(srcs), len(srcs), _ptr(d), _ptr(ms),
-          _ptr(it)) != 0:
-        raise RuntimeError("reference GPU SSSP failed")
-    return d, ms, it
-
-
-def refgpu_sssp_blas(trp, tci, tv, srcs):
-    """GraphOne's sparse-frontier BLAS engine (u32 min-plus) on the GPU, one
-    run per source: (distances of srcs[0], ms per source, iterations per
-    source)."""
-    return _refgpu_sssp(refgpu().refgpu_sssp_blas_u32, trp, tci, tv, srcs)
-
-
-def refgpu_sssp_adv(rp, ci, v, srcs):
-    """GraphOne's advance/filter engine (u32) on the GPU, one run per source."""
-    return _refgpu_sssp(refgpu().refgpu_sssp_adv_u32, rp, ci, v, srcs)
 
 
 # ---------------------------------------------------------------- wrappers

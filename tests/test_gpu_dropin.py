@@ -1,8 +1,6 @@
 """GraphOne's own apps, unchanged, built against this repository's headers
 (oracle/_ref/apps_g1, made by `make -C oracle dropin` from the reference
-sources) and run on the GPU: their printed results must match the oracle.
-The same sources built against GraphOne's headers (oracle/_ref/apps_ref) are
-run on the same inputs as the reference GPU engines."""
+sources) and run on the GPU: their printed results must match the oracle."""
 import os
 import subprocess
 
@@ -41,7 +39,7 @@ GRAPHS = {
 @pytest.mark.parametrize("name", sorted(GRAPHS))
 @pytest.mark.parametrize("app", ["sssp_blas", "sssp_blas2", "sssp_adv"])
 def test_sssp_app_on_graphone_b200(cuda, app, name, tmp_path):
-    path = O.app("g1", app)
+    path = O.app(app)
     if path is None:
         pytest.skip("apps_g1 not built (needs the reference sources at build time)")
     g = GRAPHS[name]()
@@ -70,7 +68,7 @@ def pagerank_app_expected(g, n, alpha=0.85, tol=1e-6):
 
 
 def test_pagerank_app_on_graphone_b200(cuda, tmp_path):
-    path = O.app("g1", "pagerank_blas")
+    path = O.app("pagerank_blas")
     if path is None:
         pytest.skip("apps_g1 not built (needs the reference sources at build time)")
     g = gen.rmat(11, 8, False, float_values=True)
@@ -86,22 +84,29 @@ def test_pagerank_app_on_graphone_b200(cuda, tmp_path):
     assert min(errs) < 2e-6, errs
 
 
-@pytest.mark.parametrize("app", ["sssp_blas", "sssp_adv"])
-def test_dropin_and_reference_app_outputs_compare_equal(cuda, app, tmp_path):
-    """The same unchanged app source built on GraphOne's headers (the
-    reference GPU engines) and on this repository's: the comparator CLI
-    (python -m graphone_b200.results compare) finds their result files equal."""
-    ours, ref = O.app("g1", app), O.app("ref", app)
-    if ours is None or ref is None:
-        pytest.skip("apps not built (needs the reference sources at build time)")
+@pytest.mark.parametrize("app", ["sssp_blas", "sssp_adv", "sssp_blas2"])
+def test_app_output_compares_equal_to_the_oracle_with_the_cli(cuda, app, tmp_path):
+    """The comparator CLI (python -m graphone_b200.results compare) on a
+    result file of an unchanged app and one written from the oracle's
+    Dijkstra in the apps' format: same; with one distance changed: not."""
+    path = O.app(app)
+    if path is None:
+        pytest.skip("apps_g1 not built (needs the reference sources at build time)")
     g = gen.rmat(12, 8, True, (1, 64))
     adj = os.path.join(str(tmp_path), "g.adj")
     gen.write_adj(g, adj, directed=False)
-    run_app(ours, ["-i", adj, "--src", "0"], tmp_path, "ours.txt")
-    run_app(ref, ["-i", adj, "--src", "0"], tmp_path, "ref.txt")
+    vals, _ = run_app(path, ["-i", adj, "--src", "0"], tmp_path, "app.txt")
+    rp, ci, v = g.np("n")
+    d = O.dijkstra_u32(rp, ci, v, 0)[: len(vals)]
+    ref = os.path.join(str(tmp_path), "oracle.txt")
+    results.write_result(ref, d)
     import sys
-    r = subprocess.run([sys.executable, "-m", "graphone_b200.results", "compare",
-                        os.path.join(str(tmp_path), "ours.txt"), os.path.join(str(tmp_path), "ref.txt")],
-                       capture_output=True, text=True, cwd=os.path.dirname(os.path.dirname(__file__)))
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cmd = [sys.executable, "-m", "graphone_b200.results", "compare", os.path.join(str(tmp_path), "app.txt"), ref]
+    r = subprocess.run(cmd, capture_output=True, text=True, cwd=root)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "same" in r.stdout
+    k = int(np.nonzero(d != O.U32_MAX)[0][-1])
+    d[k] += 1
+    results.write_result(ref, d)
+    r = subprocess.run(cmd, capture_output=True, text=True, cwd=root)
+    assert r.returncode == 1 and f"vertex {k}:" in r.stdout
