@@ -642,18 +642,21 @@ __global__ void nnz_fix_info_kernel(const uint32_t* fix_tiles, uint32_t n_fix, c
     info[first + 1 < t ? n_short + lpos[i] : i - lpos[i]] = make_uint4(t, row, first, 0u);
 }
 
-g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
+g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out, uint32_t tile) {
     Orientation& o = g->o[t];
     if (!o.present) return fail(G1_ERR_UNSUPPORTED, "orientation not built");
+    if (tile == 0 || tile % 32 != 0) return fail(G1_ERR_INVALID, "nnz plan: tile not a multiple of 32");
     Orientation& owner = (t == 1 && g->symmetric && g->o[0].present) ? g->o[0] : o;
-    if (owner.nnz_plan) {
-        *out = owner.nnz_plan.get();
+    auto& slot = owner.nnz_plans[tile];
+    if (slot) {
+        *out = slot.get();
         return G1_OK;
     }
     const uint32_t n = g->n, m = g->m;
     std::unique_ptr<NnzPlan> p(new NnzPlan());
-    p->n_tiles = (uint32_t)ceil_div(m, kNnzTile);
-    const size_t words = (size_t)p->n_tiles * (kNnzTile / 32) + 1 + 16;
+    p->tile = tile;
+    p->n_tiles = (uint32_t)ceil_div(m, tile);
+    const size_t words = (size_t)p->n_tiles * (tile / 32) + 2 + 16;
     G1_TRY(p->tile_seg.ensure(((size_t)p->n_tiles + 1) * 4 + 16));
     G1_TRY(p->sbits.ensure(words * 4));
     G1_TRY(p->rows.ensure(((size_t)n + 1) * 4));
@@ -679,13 +682,13 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
     nnz_place_kernel<<<grid, 256>>>(o.rp, n, rank.as<uint32_t>(), nne, p->rows.as<uint32_t>(),
                                     p->sbits.as<uint32_t>());
     nnz_tile_seg_kernel<<<(uint32_t)ceil_div((uint64_t)p->n_tiles + 1, 256), 256>>>(
-        o.rp, n, m, rank.as<uint32_t>(), nne, p->n_tiles, kNnzTile, p->tile_seg.as<uint32_t>());
+        o.rp, n, m, rank.as<uint32_t>(), nne, p->n_tiles, tile, p->tile_seg.as<uint32_t>());
     // tiles the fixup visits, in tile order (a deterministic compaction)
     {
         uint32_t* fflag = flag.as<uint32_t>();
         uint32_t* fpos = rank.as<uint32_t>();
         const uint32_t tb = (uint32_t)ceil_div((uint64_t)p->n_tiles + 1, 256);
-        nnz_fix_flag_kernel<<<tb, 256>>>(p->sbits.as<uint32_t>(), p->n_tiles, m, kNnzTile, fflag);
+        nnz_fix_flag_kernel<<<tb, 256>>>(p->sbits.as<uint32_t>(), p->n_tiles, m, tile, fflag);
         size_t sb = 0;
         G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, sb, fflag, fpos, (int)p->n_tiles + 1));
         G1_TRY(temp.ensure(sb + 16));
@@ -703,7 +706,7 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
             uint32_t* lpos = rank.as<uint32_t>();
             const uint32_t fb = (uint32_t)ceil_div((uint64_t)nfix + 1, 256);
             nnz_fix_long_kernel<<<fb, 256>>>(p->fix_tiles.as<uint32_t>(), nfix, p->tile_seg.as<uint32_t>(),
-                                             p->rows.as<uint32_t>(), o.rp, kNnzTile, lflag);
+                                             p->rows.as<uint32_t>(), o.rp, tile, lflag);
             size_t lb = 0;
             G1_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, lb, lflag, lpos, (int)nfix + 1));
             G1_TRY(temp.ensure(lb + 16));
@@ -712,7 +715,7 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
             G1_CUDA(cudaMemcpy(&nlong, lpos + nfix, 4, cudaMemcpyDeviceToHost));
             p->n_fix_short = nfix - nlong;
             nnz_fix_info_kernel<<<fb, 256>>>(p->fix_tiles.as<uint32_t>(), nfix, p->tile_seg.as<uint32_t>(),
-                                             p->rows.as<uint32_t>(), o.rp, kNnzTile, lpos, p->n_fix_short,
+                                             p->rows.as<uint32_t>(), o.rp, tile, lpos, p->n_fix_short,
                                              p->fix_info.as<uint4>());
         }
     }
@@ -720,7 +723,7 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out) {
     G1_CUDA(cudaGetLastError());
     G1_CUDA(cudaDeviceSynchronize());
     *out = p.get();
-    owner.nnz_plan = std::move(p);
+    slot = std::move(p);
     return G1_OK;
 }
 

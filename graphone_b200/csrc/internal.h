@@ -92,6 +92,7 @@ struct MergePlan {
 // row holding each tile's first nonzero, the row-start bitmap over the
 // nonzeros, the non-empty rows in order followed by the empty rows.
 struct NnzPlan {
+    uint32_t tile = 0;  // nonzeros per tile
     uint32_t n_tiles = 0, n_nonempty = 0, n_empty = 0, n_fix = 0;
     uint32_t n_fix_short = 0;  // fix entries [0, n_fix_short) end in the tile after their first
     DevBuf tile_seg, sbits, rows, carry, tail;
@@ -119,8 +120,8 @@ struct Orientation {
     std::map<uint32_t, std::unique_ptr<MergePlan>> plans;  // by items per tile
     int tuned_sched = 0;  // 0 = not tuned, else g1_schedule
     int tuned_variant = -1;  // merge kernel variant chosen by g1_autotune (-1 = default)
-    std::unique_ptr<NnzPlan> nnz_plan;
-    std::map<uint32_t, std::unique_ptr<CsPlan>> cs_plans;  // by partitions per SM
+    std::map<uint32_t, std::unique_ptr<NnzPlan>> nnz_plans;  // by nonzeros per tile
+    std::map<uint32_t, std::unique_ptr<CsPlan>> cs_plans;    // by partitions per SM
 };
 
 // Captured CUDA graphs of the device-driven traversal engines (traverse.cu):
@@ -237,7 +238,9 @@ bool is_device_ptr(const void* p);
 g1_status copy_out(void* dst, const void* dev_src, size_t bytes, cudaStream_t s);
 
 g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out);
-g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out);
+// The nnz-split plan for tiles of `tile` nonzeros (a multiple of 32; 256 is
+// the default schedule's).
+g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out, uint32_t tile = 256);
 g1_status ensure_cs_plan(g1_graph* g, int t, uint32_t parts_per_sm, CsPlan** out);
 // Near-far SSSP (unit = BFS) from internal vertex src in one persistent
 // launch; *dist_out points to the graph's workspace distances.

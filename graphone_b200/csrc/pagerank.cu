@@ -234,7 +234,7 @@ static g1_status pr_setup(g1_graph* g, float alpha, PrBuffers& b, uint32_t* grid
     count_launches(1);
     G1_CUDA(cudaGetLastError());
     const int v = merge_variant(g, t);
-    if (kMergeVariants[v].kind == 3 && !g->pr_empty_ready) {
+    if ((kMergeVariants[v].kind == 3 || kMergeVariants[v].kind == 5) && !g->pr_empty_ready) {
         NnzPlan* p = nullptr;
         G1_TRY(ensure_nnz_plan(g, t, &p));
         G1_TRY(pr_empty_active(g, *p, outw, s));
@@ -265,7 +265,8 @@ static g1_status pr_iterate(g1_graph* g, const PrBuffers& b, const uint32_t* gri
         return launch_vector<PlusTimesF32>(g, t, b.x[cur], e, s);
     PrEpilogue f = e;
     f.dang_clear = nullptr;
-    if (!last && g->pr_empty_ready && kMergeVariants[merge_variant(g, t)].kind == 3) {
+    const int kind = kMergeVariants[merge_variant(g, t)].kind;
+    if (!last && g->pr_empty_ready && (kind == 3 || kind == 5)) {
         uint32_t* list = nullptr;  // allocated by pr_empty_active, at least this large
         G1_TRY(g->ws.get("pr_empty_active", (size_t)g->pr_active_empty + 1, &list));
         f.empty_list = list;

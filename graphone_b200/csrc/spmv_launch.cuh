@@ -25,7 +25,9 @@ constexpr int kVectorBlock = 256;
 //           = next tile's col and val / col only staged in shared memory by
 //           bulk copies, stages / 32 = L2 prefetch distance in rounds;
 //   kind 4: column-sorted partitions (spmv_cs_kernel; its own plan), stages
-//           = partitions per SM, hot = L2 prefetch distance in rounds.
+//           = partitions per SM, hot = L2 prefetch distance in rounds;
+//   kind 5: nnz-split warp tiles of 32 * ipt nonzeros (spmv_nnz2_kernel, the
+//           nnz plan for that tile size).
 // `warps` per block (kind 0/2/3), `hot` x entries cached in shared memory,
 // `minb` resident blocks per SM the register budget is sized for.
 struct MergeVariant {
@@ -49,8 +51,9 @@ constexpr MergeVariant kMergeVariants[] = {
     {3, 8, 16, 32, 24576, 1}, {3, 8, 32, 32, 32768, 1}, {3, 8, 64, 32, 32768, 1},
     {3, 8, 128, 32, 32768, 1}, {3, 8, 66, 24, 32768, 1}, {4, 8, 2, 32, 0, 1},
     {4, 8, 4, 32, 0, 1},      {4, 8, 1, 32, 0, 1},      {4, 8, 2, 32, 2, 1},
-    {4, 8, 4, 32, 2, 1}};
-constexpr int kNumMergeVariants = 37;
+    {4, 8, 4, 32, 2, 1},      {5, 8, 0, 32, 32768, 1},  {5, 16, 0, 32, 32768, 1},
+    {5, 24, 0, 32, 32768, 1}, {5, 16, 0, 32, 16384, 1}};
+constexpr int kNumMergeVariants = 41;
 constexpr int kDefaultVariant = 17;
 
 template <class K>
@@ -160,6 +163,24 @@ struct CsKernel {
     static uint32_t grid(const g1_graph* g, uint32_t n_parts) {
         return (uint32_t)std::max<uint64_t>(
             1, std::min<uint64_t>(n_parts, (uint64_t)g->sm_count * occupancy()));
+    }
+};
+
+template <class SR, class Epi, int WARPS, int HOT, int IPT>
+struct Nnz2Kernel {
+    using L = Nnz2Layout<SR, WARPS, HOT, IPT>;
+    static int occupancy() {
+        static int occ = [] {
+            auto k = spmv_nnz2_kernel<SR, Epi, WARPS, HOT, IPT>;
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
+            return blocks_per_sm(k, WARPS * 32, L::BYTES);
+        }();
+        return occ;
+    }
+    static uint32_t grid(const g1_graph* g, uint32_t n_tiles) {
+        const uint64_t want = ceil_div(n_tiles, WARPS);
+        return (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(want, (uint64_t)g->sm_count * occupancy()));
     }
 };
 
@@ -292,6 +313,31 @@ g1_status launch_cs(g1_graph* g, int t, uint32_t parts_per_sm, const typename SR
     return G1_OK;
 }
 
+template <class SR, class Epi, int WARPS, int HOT, int IPT>
+g1_status launch_nnz2(g1_graph* g, int t, const typename SR::x_t* x, const Epi& main_epi,
+                      const Epi& fix_epi, cudaStream_t s) {
+    NnzPlan* p = nullptr;
+    G1_TRY(ensure_nnz_plan(g, t, &p, 32u * IPT));
+    using K = Nnz2Kernel<SR, Epi, WARPS, HOT, IPT>;
+    const NnzArgs<SR> a = nnz_args<SR>(g, t, *p, x);
+    if (((uintptr_t)a.col | (uintptr_t)a.val) & 31u)
+        return fail(G1_ERR_UNSUPPORTED, "nnz SpMV: col/val not 32-byte aligned");
+    auto mk = spmv_nnz2_kernel<SR, Epi, WARPS, HOT, IPT>;
+    auto fk = spmv_nnz_fixup_kernel<SR, Epi, kMergeBlock>;
+    if (profiling()) {
+        prof_mark(s, true);
+        mk<<<K::grid(g, p->n_tiles), WARPS * 32, K::L::BYTES, s>>>(a, main_epi);
+        prof_mark(s, false);
+        fk<<<nnz_fix_grid<SR, Epi>(g, *p), kMergeBlock, 0, s>>>(a, fix_epi);
+    } else {
+        mk<<<K::grid(g, p->n_tiles), WARPS * 32, K::L::BYTES, s>>>(a, main_epi);
+        G1_CUDA(launch_pdl(fk, nnz_fix_grid<SR, Epi>(g, *p), kMergeBlock, 0, s, a, fix_epi));
+    }
+    count_launches(2);
+    G1_CUDA(cudaGetLastError());
+    return G1_OK;
+}
+
 template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false,
           bool PFL1 = false, int BULK = 0, int PFL2 = 0>
 g1_status launch_nnz(g1_graph* g, int t, const NnzPlan& p, const typename SR::x_t* x,
@@ -327,6 +373,18 @@ g1_status launch_nnz(g1_graph* g, int t, const NnzPlan& p, const typename SR::x_
 template <class SR, class Epi>
 g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_grid) {
     const int v = merge_variant(g, t);
+    if (kMergeVariants[v].kind == 5) {
+        NnzPlan* q = nullptr;
+        G1_TRY(ensure_nnz_plan(g, t, &q, 32u * (uint32_t)kMergeVariants[v].ipt));
+        switch (v) {
+            case 37: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 8>::grid(g, q->n_tiles); break;
+            case 38: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 16>::grid(g, q->n_tiles); break;
+            case 39: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 24>::grid(g, q->n_tiles); break;
+            default: *main_grid = Nnz2Kernel<SR, Epi, 32, 16384, 16>::grid(g, q->n_tiles); break;
+        }
+        *fix_grid = nnz_fix_grid<SR, Epi>(g, *q);
+        return G1_OK;
+    }
     if (kMergeVariants[v].kind == 4) {
         CsPlan* q = nullptr;
         G1_TRY(ensure_cs_plan(g, t, (uint32_t)kMergeVariants[v].stages, &q));
@@ -442,6 +500,14 @@ template <class SR, class Epi>
 g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi& main_epi,
                        const Epi& fix_epi, cudaStream_t s) {
     const int v = merge_variant(g, t);
+    if (kMergeVariants[v].kind == 5) {
+        switch (v) {
+            case 37: return launch_nnz2<SR, Epi, 32, 32768, 8>(g, t, x, main_epi, fix_epi, s);
+            case 38: return launch_nnz2<SR, Epi, 32, 32768, 16>(g, t, x, main_epi, fix_epi, s);
+            case 39: return launch_nnz2<SR, Epi, 32, 32768, 24>(g, t, x, main_epi, fix_epi, s);
+            default: return launch_nnz2<SR, Epi, 32, 16384, 16>(g, t, x, main_epi, fix_epi, s);
+        }
+    }
     if (kMergeVariants[v].kind == 4)
         return kMergeVariants[v].hot
                    ? launch_cs<SR, Epi, 2>(g, t, (uint32_t)kMergeVariants[v].stages, x, main_epi, s)

@@ -1443,6 +1443,202 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
     epi.template block_end<WARPS * 32>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
 }
 
+// ------------------------------------------ nnz-split tiles, IPT per lane
+// The same tiles as spmv_nnz_kernel with IPT consecutive nonzeros per lane
+// (tiles of 32 * IPT nonzeros; the plan is built for that tile size).  A
+// tile's fixed costs -- the plan-word loads, the start-count ballots, the
+// warp segmented scan, the in-order emission and the loop -- are paid once
+// per 32 * IPT nonzeros, so larger IPT cuts the instructions per nonzero; the
+// per-nonzero work (gather, combine, lane-local fold) is unchanged.
+template <int IPT>
+constexpr int nnz_count_bits() {
+    return IPT < 2 ? 1 : IPT < 4 ? 2 : IPT < 8 ? 3 : IPT < 16 ? 4 : IPT < 32 ? 5 : 6;
+}
+
+template <class SR, class Epi, int IPT>
+struct Nnz2Ready {
+    typename SR::x_t x[IPT];
+    uint32_t v[IPT];
+    uint32_t sb;    // this lane's start bits (bit u: nonzero jl + u starts a row)
+    uint32_t endw;  // bitmap word whose bit 0 is the first nonzero after the tile
+    uint32_t seg_base, row_pre;
+    typename prepared_type<Epi>::type pre;
+};
+
+// Shared memory: the x cache, then per warp the values of the rows completed
+// in its tile, then the epilogue's scratch.
+template <class SR, int WARPS, int HOT, int IPT>
+struct Nnz2Layout {
+    using V = typename SR::value_t;
+    using X = typename SR::x_t;
+    static constexpr uint32_t TILE = 32 * IPT;
+    static constexpr size_t XC_OFF = 0;
+    static constexpr size_t XC_BYTES = ((size_t)HOT * sizeof(X) + 15) / 16 * 16;
+    static constexpr size_t SY_OFF = XC_OFF + XC_BYTES;
+    static constexpr size_t SY_BYTES = ((size_t)WARPS * TILE * sizeof(V) + 15) / 16 * 16;
+    static constexpr size_t EPI_OFF = SY_OFF + SY_BYTES;
+    static constexpr size_t BYTES = EPI_OFF + 512;
+};
+
+template <class SR, class Epi, int HOT, int IPT>
+__device__ __forceinline__ Nnz2Ready<SR, Epi, IPT> nnz2_fetch(const NnzArgs<SR>& a, uint32_t tile,
+                                                              const typename SR::x_t* xc, uint32_t hot,
+                                                              Epi& epi) {
+    static_assert(IPT % 8 == 0 && IPT <= 24, "IPT: 8, 16 or 24 nonzeros per lane");
+    constexpr uint32_t TILE = 32 * IPT;
+    const uint32_t lane = lane_id();
+    const uint32_t j0 = tile * TILE;
+    const uint32_t jl = j0 + lane * IPT;
+    Nnz2Ready<SR, Epi, IPT> r;
+    // a lane's start bits lie inside one 32-bit word when IPT divides 32;
+    // for IPT = 24 they may straddle two
+    const uint32_t w0 = __ldg(a.plan.sbits + (jl >> 5));
+    if constexpr (32 % IPT == 0) {
+        r.sb = (w0 >> (jl & 31u)) & ((1u << IPT) - 1u);
+    } else {
+        const uint32_t w1 = __ldg(a.plan.sbits + (jl >> 5) + 1);
+        const uint64_t w = ((uint64_t)w1 << 32) | w0;
+        r.sb = (uint32_t)(w >> (jl & 31u)) & ((1u << IPT) - 1u);
+    }
+    r.endw = __ldg(a.plan.sbits + ((j0 + TILE) >> 5));
+    const uint32_t seg0 = __ldg(a.plan.tile_seg + tile);
+    // all of the lane's col/val first (32-byte loads kept out of L1), then the gathers
+    uint32_t cc[IPT];
+#pragma unroll
+    for (int c = 0; c < IPT / 8; ++c) {
+        uint4 c0, c1, v0, v1;
+        ldg_v8_stream(a.col + jl + 8 * c, c0, c1);
+        ldg_v8_stream(a.val + jl + 8 * c, v0, v1);
+        const uint32_t ci[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+        const uint32_t vi[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            cc[8 * c + u] = ci[u];
+            r.v[8 * c + u] = vi[u];
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < IPT; ++u) {
+        if constexpr (HOT > 0) r.x[u] = gather_x(xc, a.x, cc[u], hot);
+        else r.x[u] = ldg_any(a.x + cc[u]);
+    }
+    const bool first_start = (__ballot_sync(0xffffffffu, r.sb & 1u) & 1u) != 0u;
+    r.seg_base = seg0 + (first_start ? 0u : 1u);
+    r.row_pre = r.seg_base + lane < a.plan.n_nonempty ? __ldg(a.plan.nz_rows + r.seg_base + lane) : 0u;
+    if constexpr (has_prepare<Epi>::value) r.pre = epi.prepare(r.row_pre);
+    else r.pre = 0;
+    return r;
+}
+
+// FULL: the tile is not the last one.
+template <class SR, class Epi, int IPT, bool FULL>
+__device__ __forceinline__ void nnz2_finish(const NnzArgs<SR>& a, const Nnz2Ready<SR, Epi, IPT>& r,
+                                            uint32_t tile, typename SR::value_t* sy, Epi& epi) {
+    using V = typename SR::value_t;
+    using W = typename SR::w_t;
+    constexpr uint32_t TILE = 32 * IPT;
+    const uint32_t lane = lane_id();
+    const uint32_t nnz = a.plan.nnz;
+    const uint32_t j0 = tile * TILE;
+    const uint32_t jl = j0 + lane * IPT;
+    const uint32_t nv = FULL ? (uint32_t)IPT : (jl < nnz ? min(nnz - jl, (uint32_t)IPT) : 0u);
+    const uint32_t sb = r.sb;
+    const bool first_start = (__ballot_sync(0xffffffffu, sb & 1u) & 1u) != 0u;
+    // starts before this lane and in the whole tile, from bit-sliced ballots
+    const uint32_t nst = __popc(sb);
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t excl = 0, nstarts = 0;
+#pragma unroll
+    for (int b = 0; b < nnz_count_bits<IPT>(); ++b) {
+        const uint32_t bb = __ballot_sync(0xffffffffu, (nst >> b) & 1u);
+        excl += (uint32_t)__popc(bb & below) << b;
+        nstarts += (uint32_t)__popc(bb) << b;
+    }
+    const uint32_t has_upto = __ballot_sync(0xffffffffu, nst != 0u) & ((2u << lane) - 1u);
+    // lane-local fold: segments that start and end in the lane go to sy
+    V head = SR::identity(), acc = SR::identity();
+    uint32_t k = 0;
+#pragma unroll
+    for (int u = 0; u < IPT; ++u) {
+        if ((sb >> u) & 1u) {
+            if (k == 0) head = acc;
+            else sy[excl + k - 1] = acc;
+            acc = SR::identity();
+            ++k;
+        }
+        W wv;
+        memcpy(&wv, &r.v[u], 4);
+        acc = SR::reduce(acc, (uint32_t)u < nv ? SR::combine(wv, r.x[u]) : SR::identity());
+    }
+    // warp segmented scan of the lane tails
+    V s = acc;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const V su = shfl_up_any(0xffffffffu, s, off);
+        const bool open = (int)lane >= off && (has_upto >> ((lane - off + 1) & 31u)) == 0u;
+        if (open) s = SR::reduce(su, s);
+    }
+    V prev = shfl_up_any(0xffffffffu, s, 1);
+    if (lane == 0) prev = SR::identity();
+    if (nst) {
+        const V val = SR::reduce(prev, head);
+        if (excl > 0)
+            sy[excl - 1] = val;
+        else if (!first_start)
+            a.tail[tile] = val;
+    }
+    const V last = shfl_any(0xffffffffu, s, 31);
+    const bool closed = (!FULL && j0 + TILE >= nnz) || (r.endw & 1u);
+    if (lane == 0) {
+        if (nstarts == 0) {
+            a.tail[tile] = last;
+            a.carry[tile] = last;
+        } else if (closed) {
+            sy[nstarts - 1] = last;
+        } else {
+            a.carry[tile] = last;
+        }
+    }
+    __syncwarp();
+    const uint32_t ncomplete = nstarts == 0 ? 0u : (closed ? nstarts : nstarts - 1);
+    if (lane < ncomplete) {
+        if constexpr (has_prepare<Epi>::value) epi.emit_prepared(r.row_pre, sy[lane], r.pre);
+        else epi.emit(r.row_pre, sy[lane]);
+    }
+    for (uint32_t q = lane + 32; q < ncomplete; q += 32)
+        epi.emit(__ldg(a.plan.nz_rows + r.seg_base + q), sy[q]);
+    __syncwarp();
+}
+
+template <class SR, class Epi, int WARPS, int HOT, int IPT>
+__global__ void __launch_bounds__(WARPS * 32, 1)
+spmv_nnz2_kernel(NnzArgs<SR> a, Epi epi) {
+    using X = typename SR::x_t;
+    using V = typename SR::value_t;
+    using L = Nnz2Layout<SR, WARPS, HOT, IPT>;
+    static_assert(sizeof(typename SR::w_t) == 4, "32-byte val loads assume 4-byte edge values");
+    extern __shared__ __align__(16) unsigned char dsm[];
+    grid_launch_dependents();
+    if (!epi_active(epi)) return;
+    const uint32_t w = threadIdx.x >> 5;
+    X* xc = reinterpret_cast<X*>(dsm + L::XC_OFF);
+    V* sy = reinterpret_cast<V*>(dsm + L::SY_OFF) + (size_t)w * L::TILE;
+    epi.begin();
+    const uint32_t hot = HOT < a.plan.n_rows ? (uint32_t)HOT : a.plan.n_rows;
+    if constexpr (HOT > 0) {
+        fill_x_cache<WARPS * 32>(xc, a.x, hot);
+        __syncthreads();
+    }
+    const uint32_t total_warps = gridDim.x * WARPS;
+    const uint32_t n_tiles = a.plan.n_tiles;
+    for (uint32_t tile = blockIdx.x * WARPS + w; tile < n_tiles; tile += total_warps) {
+        const Nnz2Ready<SR, Epi, IPT> r = nnz2_fetch<SR, Epi, HOT, IPT>(a, tile, xc, hot, epi);
+        if (tile + 1 < n_tiles) nnz2_finish<SR, Epi, IPT, true>(a, r, tile, sy, epi);
+        else nnz2_finish<SR, Epi, IPT, false>(a, r, tile, sy, epi);
+    }
+    epi.template block_end<WARPS * 32>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
+}
+
 __device__ __forceinline__ bool nnz_start_bit(const uint32_t* sbits, uint32_t k) {
     return (__ldg(sbits + (k >> 5)) >> (k & 31)) & 1u;
 }

@@ -91,6 +91,8 @@ def test_pagerank_isolated_vertices_every_nnz_variant(cuda, iters):
     rp, ci, v = g.np("n")
     G = g1.Graph.from_csr(rp, ci, v, relabel=True)
     nnz_variants = [i for i, k in enumerate(g1.MERGE_VARIANTS) if k == "nnz"]
+    # tiles of 32 x 8, 16, 24 nonzeros: another fold grouping, same plan logic
+    nnz2_variants = [i for i, k in enumerate(g1.MERGE_VARIANTS) if k == "nnz2"]
     for mode in (g1.PR_REFERENCE, g1.PR_DANGLING):
         ref = O.pagerank_f64(trp, tci, tv, 0.85, iters, mode)
         first = None
@@ -103,6 +105,11 @@ def test_pagerank_isolated_vertices_every_nnz_variant(cuda, iters):
                 assert np.array_equal(G.pagerank(0.85, iters, mode), r)  # run to run
             else:
                 assert np.array_equal(r, first), (mode, var)
+        for var in nnz2_variants:
+            G.set_schedule(g1.SCHED_MERGE, var, transpose=1)
+            r = G.pagerank(0.85, iters, mode)
+            assert O.rel_l1(r, ref) < 1e-6, (mode, var)  # tolerance: relative L1 vs FP64
+            assert np.array_equal(G.pagerank(0.85, iters, mode), r), (mode, var)  # run to run
 
 
 def test_pagerank_device_output_and_zero_iterations(cuda):
