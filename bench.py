@@ -499,8 +499,7 @@ def kernel_name(variant: int) -> str:
     from graphone_b200 import MERGE_VARIANTS
     kind = MERGE_VARIANTS[variant]
     base = {"warp": "spmv_wmerge_kernel", "warp_tma": "spmv_wtma_kernel",
-            "cta_tma": "spmv_merge_kernel", "nnz": "spmv_nnz_kernel", "colsort": "spmv_cs_kernel",
-            "nnz2": "spmv_nnz2_kernel"}[kind]
+            "cta_tma": "spmv_merge_kernel", "nnz": "spmv_nnz_kernel", "nnz2": "spmv_nnz2_kernel"}[kind]
     return f"{base}<PlusTimesF32, PrEpilogue> (merge variant {variant})"
 
 

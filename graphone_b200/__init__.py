@@ -31,13 +31,10 @@ PR_REFERENCE, PR_DANGLING = 0, 1
 # loads), "cta_tma" = spmv_merge_kernel (CTA tiles staged by bulk copies),
 # "warp_tma" = spmv_wtma_kernel (warp tiles staged by bulk copies), "nnz" =
 # spmv_nnz_kernel (nnz-split warp tiles, 16-byte loads, row-start bitmap),
-# "colsort" = spmv_cs_kernel (row partitions folded in column order into
-# shared-memory accumulators), "nnz2" = spmv_nnz2_kernel (nnz-split tiles of
-# 32 x 8, 16 or 24 nonzeros).
+# "nnz2" = spmv_nnz2_kernel (nnz-split tiles of 32 x 8, 16 or 24 nonzeros).
 MERGE_VARIANTS = ("warp", "warp", "warp", "cta_tma", "cta_tma", "warp",
                   "warp_tma", "warp_tma", "warp_tma", "warp_tma", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz",
                   "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz",
-                  "colsort", "colsort", "colsort", "colsort", "colsort",
                   "nnz2", "nnz2", "nnz2", "nnz2")
 DEFAULT_MERGE_VARIANT = 17
 GRAPH_SYMMETRIC, GRAPH_INPUT_TRANSPOSE, GRAPH_BUILD_OTHER, GRAPH_NO_VALIDATE = 1, 2, 4, 8

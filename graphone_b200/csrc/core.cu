@@ -727,121 +727,6 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out, uint32_t tile) {
     return G1_OK;
 }
 
-// Row of every nonzero: the last row whose first nonzero is at or before it.
-__global__ void cs_rowid_kernel(const uint32_t* rp, uint32_t n, uint32_t m, uint32_t* rowid) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += stride) {
-        uint32_t lo = 0, hi = n - 1;  // rp[lo] <= k < rp[n]
-        while (lo < hi) {
-            const uint32_t mid = lo + ((hi - lo + 1) >> 1);
-            if (rp[mid] <= k) lo = mid; else hi = mid - 1;
-        }
-        rowid[k] = lo;
-    }
-}
-
-// Sort keys: (partition of the nonzero's row, column); values: the nonzero.
-__global__ void cs_keys_kernel(const uint32_t* rowid, const uint32_t* col, const uint32_t* part_row,
-                               uint32_t n_parts, uint32_t m, unsigned long long* keys, uint32_t* idx) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += stride) {
-        const uint32_t r = rowid[k];
-        uint32_t lo = 0, hi = n_parts - 1;  // last partition starting at or before r
-        while (lo < hi) {
-            const uint32_t mid = lo + ((hi - lo + 1) >> 1);
-            if (part_row[mid] <= r) lo = mid; else hi = mid - 1;
-        }
-        keys[k] = ((unsigned long long)lo << 32) | col[k];
-        idx[k] = (uint32_t)k;
-    }
-}
-
-__global__ void cs_gather_kernel(const unsigned long long* keys, const uint32_t* idx, const uint32_t* rowid,
-                                 const uint32_t* col, const uint32_t* val, const uint32_t* part_row,
-                                 uint32_t m, uint32_t* cs_col, uint16_t* cs_lrow, uint32_t* cs_val) {
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
-        const uint32_t k = idx[i];
-        const uint32_t p = (uint32_t)(keys[i] >> 32);
-        cs_col[i] = col[k];
-        cs_val[i] = val[k];
-        cs_lrow[i] = (uint16_t)(rowid[k] - part_row[p]);
-    }
-}
-
-g1_status ensure_cs_plan(g1_graph* g, int t, uint32_t parts_per_sm, CsPlan** out) {
-    Orientation& o = g->o[t];
-    if (!o.present) return fail(G1_ERR_UNSUPPORTED, "orientation not built");
-    Orientation& owner = (t == 1 && g->symmetric && g->o[0].present) ? g->o[0] : o;
-    auto& slot = owner.cs_plans[parts_per_sm];
-    if (slot) {
-        *out = slot.get();
-        return G1_OK;
-    }
-    const uint32_t n = g->n, m = g->m;
-    std::unique_ptr<CsPlan> p(new CsPlan());
-    // partitions on the host from the row offsets: about T nonzeros, at most
-    // kCsRows rows, at least one row each
-    std::vector<uint32_t> rp((size_t)n + 1);
-    G1_CUDA(cudaMemcpy(rp.data(), o.rp, rp.size() * 4, cudaMemcpyDeviceToHost));
-    const uint64_t T = std::max<uint64_t>(1, ceil_div(m, (uint64_t)g->sm_count * std::max(1u, parts_per_sm)));
-    std::vector<uint32_t> pr{0}, pn{0};
-    for (uint32_t r = 0; r < n;) {
-        const uint64_t target = (uint64_t)rp[r] + T;
-        uint32_t b = (uint32_t)(std::upper_bound(rp.begin() + r + 1, rp.end(),
-                                                 (uint32_t)std::min<uint64_t>(target, 0xFFFFFFFFull)) -
-                                rp.begin()) - 1;
-        b = std::max(b, r + 1);
-        b = std::min<uint32_t>(std::min<uint64_t>(b, (uint64_t)r + kCsRows), n);
-        pr.push_back(b);
-        pn.push_back(rp[b]);
-        r = b;
-    }
-    p->n_parts = (uint32_t)pr.size() - 1;
-    G1_TRY(p->part_row.ensure(pr.size() * 4));
-    G1_TRY(p->part_nnz.ensure(pn.size() * 4));
-    G1_CUDA(cudaMemcpy(p->part_row.p, pr.data(), pr.size() * 4, cudaMemcpyHostToDevice));
-    G1_CUDA(cudaMemcpy(p->part_nnz.p, pn.data(), pn.size() * 4, cudaMemcpyHostToDevice));
-    const size_t pad = kCsIpt;
-    G1_TRY(p->col.ensure(((size_t)m + pad) * 4));
-    G1_TRY(p->val.ensure(((size_t)m + pad) * 4));
-    G1_TRY(p->lrow.ensure(((size_t)m + pad) * 2));
-    G1_CUDA(cudaMemset(p->col.p, 0, ((size_t)m + pad) * 4));
-    G1_CUDA(cudaMemset(p->val.p, 0, ((size_t)m + pad) * 4));
-    G1_CUDA(cudaMemset(p->lrow.p, 0, ((size_t)m + pad) * 2));
-    if (m > 0) {
-        DevBuf rowid, keys, keys2, idx, idx2, temp;
-        G1_TRY(rowid.ensure((size_t)m * 4));
-        G1_TRY(keys.ensure((size_t)m * 8));
-        G1_TRY(keys2.ensure((size_t)m * 8));
-        G1_TRY(idx.ensure((size_t)m * 4));
-        G1_TRY(idx2.ensure((size_t)m * 4));
-        const uint32_t grid = grid_for(m, 256, g->sm_count);
-        cs_rowid_kernel<<<grid, 256>>>(o.rp, n, m, rowid.as<uint32_t>());
-        cs_keys_kernel<<<grid, 256>>>(rowid.as<uint32_t>(), o.col, p->part_row.as<uint32_t>(), p->n_parts, m,
-                                      keys.as<unsigned long long>(), idx.as<uint32_t>());
-        int end_bit = 32;
-        while (end_bit < 64 && (1ull << (end_bit - 32)) < p->n_parts) ++end_bit;
-        size_t tb = 0;
-        G1_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.as<unsigned long long>(),
-                                                keys2.as<unsigned long long>(), idx.as<uint32_t>(),
-                                                idx2.as<uint32_t>(), (int)m, 0, end_bit));
-        G1_TRY(temp.ensure(tb + 16));
-        G1_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, tb, keys.as<unsigned long long>(),
-                                                keys2.as<unsigned long long>(), idx.as<uint32_t>(),
-                                                idx2.as<uint32_t>(), (int)m, 0, end_bit));
-        cs_gather_kernel<<<grid, 256>>>(keys2.as<unsigned long long>(), idx2.as<uint32_t>(), rowid.as<uint32_t>(),
-                                        o.col, static_cast<const uint32_t*>(o.val), p->part_row.as<uint32_t>(),
-                                        m, p->col.as<uint32_t>(), p->lrow.as<uint16_t>(), p->val.as<uint32_t>());
-        count_launches(5);
-        G1_CUDA(cudaGetLastError());
-        G1_CUDA(cudaDeviceSynchronize());
-    }
-    *out = p.get();
-    slot = std::move(p);
-    return G1_OK;
-}
-
 g1_status to_caller_order(g1_graph* g, uint32_t* dev_out, const uint32_t* internal,
                           cudaStream_t s) {
     gather_perm_kernel<<<grid_for(g->n, 256, g->sm_count), 256, 0, s>>>(

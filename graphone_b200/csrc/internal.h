@@ -101,15 +101,6 @@ struct NnzPlan {
                        // span one boundary first, then longer chains, each in tile order
 };
 
-// Column-sorted partitions (spmv_cs_kernel): rows cut into partitions of at
-// most kCsRows rows and about m / (SMs x parts_per_sm) nonzeros; inside a
-// partition the nonzeros in column order with their row offsets.
-struct CsPlan {
-    uint32_t n_parts = 0;
-    DevBuf part_row, part_nnz;  // n_parts + 1 each
-    DevBuf col, lrow, val;      // m entries (+ padding) in partition-column order
-};
-
 struct Orientation {
     bool present = false;
     uint32_t* rp = nullptr;
@@ -121,7 +112,6 @@ struct Orientation {
     int tuned_sched = 0;  // 0 = not tuned, else g1_schedule
     int tuned_variant = -1;  // merge kernel variant chosen by g1_autotune (-1 = default)
     std::map<uint32_t, std::unique_ptr<NnzPlan>> nnz_plans;  // by nonzeros per tile
-    std::map<uint32_t, std::unique_ptr<CsPlan>> cs_plans;    // by partitions per SM
 };
 
 // Captured CUDA graphs of the device-driven traversal engines (traverse.cu):
@@ -241,7 +231,6 @@ g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out);
 // The nnz-split plan for tiles of `tile` nonzeros (a multiple of 32; 256 is
 // the default schedule's).
 g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out, uint32_t tile = 256);
-g1_status ensure_cs_plan(g1_graph* g, int t, uint32_t parts_per_sm, CsPlan** out);
 // Near-far SSSP (unit = BFS) from internal vertex src in one persistent
 // launch; *dist_out points to the graph's workspace distances.
 g1_status nearfar_traverse(g1_graph* g, uint32_t src, bool unit, uint32_t** dist_out, uint32_t* rounds,

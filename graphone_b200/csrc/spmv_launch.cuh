@@ -24,8 +24,6 @@ constexpr int kVectorBlock = 256;
 //           pipeline per warp, bit 2 = next-tile L1 prefetch, bit 3 / bit 4
 //           = next tile's col and val / col only staged in shared memory by
 //           bulk copies, stages / 32 = L2 prefetch distance in rounds;
-//   kind 4: column-sorted partitions (spmv_cs_kernel; its own plan), stages
-//           = partitions per SM, hot = L2 prefetch distance in rounds;
 //   kind 5: nnz-split warp tiles of 32 * ipt nonzeros (spmv_nnz2_kernel, the
 //           nnz plan for that tile size).
 // `warps` per block (kind 0/2/3), `hot` x entries cached in shared memory,
@@ -49,11 +47,9 @@ constexpr MergeVariant kMergeVariants[] = {
     {3, 8, 3, 24, 32768, 1},  {3, 8, 4, 32, 32768, 1},  {3, 8, 4, 32, 16384, 1},
     {3, 8, 8, 32, 32768, 1},  {3, 8, 8, 32, 16384, 1},  {3, 8, 16, 32, 32768, 1},
     {3, 8, 16, 32, 24576, 1}, {3, 8, 32, 32, 32768, 1}, {3, 8, 64, 32, 32768, 1},
-    {3, 8, 128, 32, 32768, 1}, {3, 8, 66, 24, 32768, 1}, {4, 8, 2, 32, 0, 1},
-    {4, 8, 4, 32, 0, 1},      {4, 8, 1, 32, 0, 1},      {4, 8, 2, 32, 2, 1},
-    {4, 8, 4, 32, 2, 1},      {5, 8, 0, 32, 32768, 1},  {5, 16, 0, 32, 32768, 1},
-    {5, 24, 0, 32, 32768, 1}, {5, 16, 0, 32, 16384, 1}};
-constexpr int kNumMergeVariants = 41;
+    {3, 8, 128, 32, 32768, 1}, {3, 8, 66, 24, 32768, 1}, {5, 8, 0, 32, 32768, 1},
+    {5, 16, 0, 32, 32768, 1}, {5, 24, 0, 32, 32768, 1}, {5, 16, 0, 32, 16384, 1}};
+constexpr int kNumMergeVariants = 36;
 constexpr int kDefaultVariant = 17;
 
 template <class K>
@@ -145,24 +141,6 @@ struct NnzKernel {
         const uint64_t want = ceil_div(n_tiles, WARPS);
         return (uint32_t)std::max<uint64_t>(
             1, std::min<uint64_t>(want, (uint64_t)g->sm_count * occupancy()));
-    }
-};
-
-template <class SR, class Epi, int PF = 0>
-struct CsKernel {
-    using L = CsLayout<SR>;
-    static constexpr int kBlock = 1024;
-    static int occupancy() {
-        static int occ = [] {
-            auto k = spmv_cs_kernel<SR, Epi, kBlock, PF>;
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
-            return blocks_per_sm(k, kBlock, L::BYTES);
-        }();
-        return occ;
-    }
-    static uint32_t grid(const g1_graph* g, uint32_t n_parts) {
-        return (uint32_t)std::max<uint64_t>(
-            1, std::min<uint64_t>(n_parts, (uint64_t)g->sm_count * occupancy()));
     }
 };
 
@@ -287,32 +265,6 @@ NnzArgs<SR> nnz_args(const g1_graph* g, int t, const NnzPlan& p, const typename 
     return a;
 }
 
-template <class SR, class Epi, int PF = 0>
-g1_status launch_cs(g1_graph* g, int t, uint32_t parts_per_sm, const typename SR::x_t* x,
-                    const Epi& epi, cudaStream_t s) {
-    static_assert(sizeof(typename SR::w_t) == 4, "column-sorted partitions hold 4-byte edge values");
-    CsPlan* p = nullptr;
-    G1_TRY(ensure_cs_plan(g, t, parts_per_sm, &p));
-    CsArgs<SR> a;
-    a.n_parts = p->n_parts;
-    a.part_row = p->part_row.as<uint32_t>();
-    a.part_nnz = p->part_nnz.as<uint32_t>();
-    a.col = p->col.as<uint32_t>();
-    a.lrow = p->lrow.as<uint16_t>();
-    a.val = p->val.as<typename SR::w_t>();
-    a.x = x;
-    // the arrays hold m + kCsIpt entries: the readable range rounded down
-    a.nnz_pad = (uint32_t)(((uint64_t)g->m + kCsIpt) / kCsIpt * kCsIpt);
-    using K = CsKernel<SR, Epi, PF>;
-    const bool prof = profiling();
-    if (prof) prof_mark(s, true);
-    spmv_cs_kernel<SR, Epi, K::kBlock, PF><<<K::grid(g, p->n_parts), K::kBlock, K::L::BYTES, s>>>(a, epi);
-    if (prof) prof_mark(s, false);
-    count_launches(1);
-    G1_CUDA(cudaGetLastError());
-    return G1_OK;
-}
-
 template <class SR, class Epi, int WARPS, int HOT, int IPT>
 g1_status launch_nnz2(g1_graph* g, int t, const typename SR::x_t* x, const Epi& main_epi,
                       const Epi& fix_epi, cudaStream_t s) {
@@ -377,20 +329,12 @@ g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_gri
         NnzPlan* q = nullptr;
         G1_TRY(ensure_nnz_plan(g, t, &q, 32u * (uint32_t)kMergeVariants[v].ipt));
         switch (v) {
-            case 37: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 8>::grid(g, q->n_tiles); break;
-            case 38: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 16>::grid(g, q->n_tiles); break;
-            case 39: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 24>::grid(g, q->n_tiles); break;
+            case 32: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 8>::grid(g, q->n_tiles); break;
+            case 33: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 16>::grid(g, q->n_tiles); break;
+            case 34: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 24>::grid(g, q->n_tiles); break;
             default: *main_grid = Nnz2Kernel<SR, Epi, 32, 16384, 16>::grid(g, q->n_tiles); break;
         }
         *fix_grid = nnz_fix_grid<SR, Epi>(g, *q);
-        return G1_OK;
-    }
-    if (kMergeVariants[v].kind == 4) {
-        CsPlan* q = nullptr;
-        G1_TRY(ensure_cs_plan(g, t, (uint32_t)kMergeVariants[v].stages, &q));
-        *main_grid = kMergeVariants[v].hot ? CsKernel<SR, Epi, 2>::grid(g, q->n_parts)
-                                           : CsKernel<SR, Epi>::grid(g, q->n_parts);
-        *fix_grid = 0;
         return G1_OK;
     }
     if (kMergeVariants[v].kind == 3) {
@@ -502,16 +446,12 @@ g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi&
     const int v = merge_variant(g, t);
     if (kMergeVariants[v].kind == 5) {
         switch (v) {
-            case 37: return launch_nnz2<SR, Epi, 32, 32768, 8>(g, t, x, main_epi, fix_epi, s);
-            case 38: return launch_nnz2<SR, Epi, 32, 32768, 16>(g, t, x, main_epi, fix_epi, s);
-            case 39: return launch_nnz2<SR, Epi, 32, 32768, 24>(g, t, x, main_epi, fix_epi, s);
+            case 32: return launch_nnz2<SR, Epi, 32, 32768, 8>(g, t, x, main_epi, fix_epi, s);
+            case 33: return launch_nnz2<SR, Epi, 32, 32768, 16>(g, t, x, main_epi, fix_epi, s);
+            case 34: return launch_nnz2<SR, Epi, 32, 32768, 24>(g, t, x, main_epi, fix_epi, s);
             default: return launch_nnz2<SR, Epi, 32, 16384, 16>(g, t, x, main_epi, fix_epi, s);
         }
     }
-    if (kMergeVariants[v].kind == 4)
-        return kMergeVariants[v].hot
-                   ? launch_cs<SR, Epi, 2>(g, t, (uint32_t)kMergeVariants[v].stages, x, main_epi, s)
-                   : launch_cs<SR, Epi>(g, t, (uint32_t)kMergeVariants[v].stages, x, main_epi, s);
     if (kMergeVariants[v].kind == 3) {
         NnzPlan* q = nullptr;
         G1_TRY(ensure_nnz_plan(g, t, &q));

@@ -22,8 +22,6 @@ struct MinPlusU32 {
     __device__ static __forceinline__ uint32_t reduce(const uint32_t& a, const uint32_t& b) {
         return min(a, b);
     }
-    // *p = reduce(*p, v) on shared memory, atomically
-    __device__ static __forceinline__ void reduce_shared(uint32_t* p, uint32_t v) { atomicMin(p, v); }
 };
 
 // Same over float distances, as the unchanged apps compute them
@@ -38,16 +36,6 @@ struct MinPlusF32 {
     }
     __device__ static __forceinline__ float reduce(const float& a, const float& b) {
         return (b < a) ? b : a;
-    }
-    __device__ static __forceinline__ void reduce_shared(float* p, float v) {
-        // compare-and-swap until *p <= v (any value order gives the same min)
-        int* q = reinterpret_cast<int*>(p);
-        int old = *q;
-        while (v < __int_as_float(old)) {
-            const int seen = atomicCAS(q, old, __float_as_int(v));
-            if (seen == old) break;
-            old = seen;
-        }
     }
 };
 
@@ -64,7 +52,6 @@ struct BfsU32 {
     __device__ static __forceinline__ uint32_t reduce(const uint32_t& a, const uint32_t& b) {
         return min(a, b);
     }
-    __device__ static __forceinline__ void reduce_shared(uint32_t* p, uint32_t v) { atomicMin(p, v); }
 };
 
 // plus-times over fp32 with fp32 accumulation (apps/pagerank_blas.cu:103-113).
@@ -79,7 +66,6 @@ struct PlusTimesF32 {
     __device__ static __forceinline__ float reduce(const float& a, const float& b) {
         return a + b;
     }
-    __device__ static __forceinline__ void reduce_shared(float* p, float v) { atomicAdd(p, v); }
 };
 
 // GraphOne user functor -> semiring, exactly as the reference's SpmvFunctor

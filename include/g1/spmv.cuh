@@ -1766,123 +1766,6 @@ spmv_vector_kernel(uint32_t n_rows, const uint32_t* row_ptr, const uint32_t* col
     epi.template block_end<BLOCK>(epi_smem);
 }
 
-// ------------------------------------------- column-sorted partitions
-// The rows are cut into partitions of at most kCsRows consecutive rows and
-// about equal nonzero counts; inside a partition the nonzeros are stored in
-// column order (stable), each with its row's offset in the partition (u16)
-// and its value.  One block folds one partition at a time into a
-// shared-memory accumulator per row with the semiring's shared-memory atomic
-// reduce, then emits every row of the partition in order (empty rows as the
-// identity) -- no carries, no fixup kernel.
-//
-// Why column order: a partition of ~m/(2 SMs) nonzeros gathers x entries
-// that share 32-byte sectors (the hot low-id columns of the degree-ordered
-// layout and clusters among the rest); in column order the gathers of a
-// sector are adjacent in time, so they are served by L1 or merged while in
-// flight, instead of one L2 request per gather.  The price is 2 more bytes
-// per nonzero (the row offset) and, for plus-times, a fold order that
-// depends on the atomics' timing (min-plus is order-free and exact).
-
-constexpr uint32_t kCsRows = 16384;  // rows per partition (the accumulators)
-constexpr uint32_t kCsIpt = 8;       // nonzeros per thread and round
-
-template <class SR>
-struct CsArgs {
-    uint32_t n_parts;
-    const uint32_t* part_row;    // n_parts + 1: first row of each partition
-    const uint32_t* part_nnz;    // n_parts + 1: first nonzero (column-sorted arrays)
-    const uint32_t* col;         // column-sorted per partition, padded by kCsIpt
-    const uint16_t* lrow;        // row - part_row[p]
-    const typename SR::w_t* val;
-    const typename SR::x_t* x;
-    uint32_t nnz_pad;            // readable entries of col/val/lrow (multiple of kCsIpt)
-};
-
-// One thread: L2 prefetch of the column-sorted arrays' nonzeros
-// [j, j + cnt) clipped to the readable range (bulk prefetches; j and cnt
-// multiples of kCsIpt keep them 16-byte aligned).
-template <class SR>
-__device__ __forceinline__ void cs_prefetch_l2(const CsArgs<SR>& a, uint32_t j, uint32_t cnt) {
-    if (j >= a.nnz_pad) return;
-    cnt = min(cnt, a.nnz_pad - j);
-    prefetch_l2_bulk(a.col + j, cnt * 4);
-    prefetch_l2_bulk(a.val + j, cnt * 4);
-    prefetch_l2_bulk(a.lrow + j, cnt * 2);
-}
-
-// Shared-memory accumulators of one partition, then the epilogue's scratch.
-template <class SR>
-struct CsLayout {
-    using V = typename SR::value_t;
-    static constexpr size_t Y_BYTES = ((size_t)kCsRows * sizeof(V) + 15) / 16 * 16;
-    static constexpr size_t EPI_OFF = Y_BYTES;
-    static constexpr size_t BYTES = EPI_OFF + 512;
-};
-
-// PF > 0: thread 0 prefetches into L2 the block's round PF rounds ahead.
-template <class SR, class Epi, int BLOCK, int PF = 0>
-__global__ void __launch_bounds__(BLOCK, 1)
-spmv_cs_kernel(CsArgs<SR> a, Epi epi) {
-    if (!epi_active(epi)) return;
-    using V = typename SR::value_t;
-    using L = CsLayout<SR>;
-    extern __shared__ __align__(16) unsigned char dsm[];
-    V* ys = reinterpret_cast<V*>(dsm);
-    epi.begin();
-    for (uint32_t p = blockIdx.x; p < a.n_parts; p += gridDim.x) {
-        const uint32_t r0 = a.part_row[p], rows = a.part_row[p + 1] - r0;
-        const uint32_t j0 = a.part_nnz[p], j1 = a.part_nnz[p + 1];
-        for (uint32_t i = threadIdx.x; i < rows; i += BLOCK) ys[i] = SR::identity();
-        __syncthreads();
-        // rounds of BLOCK * 8 nonzeros from j0 rounded down to 8: each thread
-        // loads 8 consecutive nonzeros (32-byte col and val loads, 16-byte
-        // row-offset loads); those outside [j0, j1) are masked
-        const uint32_t jb = j0 & ~(kCsIpt - 1u);
-        constexpr uint32_t kRound = BLOCK * kCsIpt;
-        if constexpr (PF > 0) {
-            if (threadIdx.x == 0)
-                for (int d = 1; d < PF; ++d)
-                    if (jb + d * kRound < j1) cs_prefetch_l2(a, jb + d * kRound, min(kRound, j1 - (jb + d * kRound) + kCsIpt) & ~(kCsIpt - 1u));
-        }
-        for (uint32_t base = jb; base < j1; base += kRound) {
-            if constexpr (PF > 0) {
-                const uint32_t pb = base + PF * kRound;
-                if (threadIdx.x == 0 && pb < j1)
-                    cs_prefetch_l2(a, pb, min(kRound, j1 - pb + kCsIpt) & ~(kCsIpt - 1u));
-            }
-            const uint32_t j = base + threadIdx.x * kCsIpt;
-            if (j < j1) {
-                uint4 c0, c1, v0, v1;
-                ldg_v8_stream(a.col + j, c0, c1);
-                ldg_v8_stream(a.val + j, v0, v1);
-                const uint4 lr = __ldg(reinterpret_cast<const uint4*>(a.lrow + j));
-                const uint32_t cc[kCsIpt] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-                const uint32_t vv[kCsIpt] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
-                const uint32_t rr[kCsIpt] = {lr.x & 0xFFFFu, lr.x >> 16, lr.y & 0xFFFFu, lr.y >> 16,
-                                             lr.z & 0xFFFFu, lr.z >> 16, lr.w & 0xFFFFu, lr.w >> 16};
-                typename SR::x_t xv[kCsIpt];
-#pragma unroll
-                for (int u = 0; u < (int)kCsIpt; ++u) {
-                    const bool in = j + u >= j0 && j + u < j1;
-                    xv[u] = in ? ldg_any(a.x + cc[u]) : typename SR::x_t{};
-                }
-#pragma unroll
-                for (int u = 0; u < (int)kCsIpt; ++u) {
-                    if (j + u >= j0 && j + u < j1) {
-                        typename SR::w_t w;
-                        memcpy(&w, &vv[u], 4);
-                        SR::reduce_shared(&ys[rr[u]], SR::combine(w, xv[u]));
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < rows; i += BLOCK) epi.emit(r0 + i, ys[i]);
-        __syncthreads();
-    }
-    epi.template block_end<BLOCK>(reinterpret_cast<char*>(dsm + L::EPI_OFF));
-}
-
 // ----------------------------------------------------------- epilogues
 
 // Plain SpMV: y[row] = value.

@@ -80,7 +80,7 @@ def test_python_variant_table_matches_the_launcher():
     d = int(re.search(r"kDefaultVariant\s*=\s*(\d+)", src).group(1))
     table = re.search(r"kMergeVariants\[\]\s*=\s*\{(.*?)\};", src, re.S).group(1)
     kinds = [int(k) for k in re.findall(r"\{\s*(\d+)\s*,", table)]
-    names = {0: "warp", 1: "cta_tma", 2: "warp_tma", 3: "nnz", 4: "colsort", 5: "nnz2"}
+    names = {0: "warp", 1: "cta_tma", 2: "warp_tma", 3: "nnz", 5: "nnz2"}
     assert len(g1.MERGE_VARIANTS) == n == len(kinds)
     assert tuple(names[k] for k in kinds) == g1.MERGE_VARIANTS
     assert g1.DEFAULT_MERGE_VARIANT == d
