@@ -2,7 +2,7 @@
 """Benchmark of the GraphOne hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload pagerank|sssp|bfs] [--scale S]
+                    [--scale S] [--kernel-workload NAME]
 
 Default workload (the headline): PageRank on RMAT scale 22 (4,194,304
 vertices, 16*2^22 directed samples, a/b/c/d = .57/.19/.19/.05, self loops
@@ -446,8 +446,9 @@ def serving_metrics(dev, n_requests: int, rate: float, sweep=(0.25, 0.5, 0.9, 1.
             if ta > now:
                 time.sleep(ta - now)
             tickets.append(srv.submit(gids[gi], q, src, outs[i]))
-        for tk in tickets:
-            srv.wait(tk, 0)
+        lat_by = {}
+        for tk, (_, gi, q, _) in zip(tickets, reqs):
+            lat_by.setdefault((gi, q), []).append(srv.wait(tk, 0))
         st = srv.stats()
         served = {"p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
                   "mean_ms": round(st["mean_ms"], 3), "queries_per_s": round(st["queries_per_s"], 1),
@@ -465,6 +466,12 @@ def serving_metrics(dev, n_requests: int, rate: float, sweep=(0.25, 0.5, 0.9, 1.
         plain = {"p50_ms": round(_pct(lat, 50), 3), "p99_ms": round(_pct(lat, 99), 3),
                  "mean_ms": round(float(np.mean(lat)), 3),
                  "queries_per_s": round(len(reqs) / (end - reqs[0][0]), 1)}
+        kinds = {g1.QUERY_SSSP: "sssp", g1.QUERY_BFS: "bfs", g1.QUERY_PPR: "ppr"}
+        groups = sorted(lat_by.items(), key=lambda kv: -max(kv[1]))[:4]
+        served["slowest_groups"] = [
+            {"graph": f"{SERVING_GRAPHS[gi][0]}{SERVING_GRAPHS[gi][1]}", "query": kinds[q],
+             "count": len(ls), "p50_ms": round(_pct(ls, 50), 2), "max_ms": round(max(ls), 2)}
+            for (gi, q), ls in groups]
         return {"offered_rate_per_s": round(r, 2), "requests": len(reqs), "served": served,
                 "plain_per_request": plain,
                 "served_over_plain_qps": round(served["queries_per_s"] / max(plain["queries_per_s"], 1e-9), 2),
@@ -795,6 +802,51 @@ def run_reference(args):
     }), flush=True)
 
 
+KERNEL_WORKLOADS = ("slot_sssp", "slot_bfs", "slot_ppr", "nearfar", "advance_grid", "advance_lb",
+                    "blas_rmat20")
+
+
+def run_kernel_workload(name: str):
+    """One small run of the workload that exercises one kernel family, twice
+    (a warm-up launch, then the launches an ncu capture skips to), for
+    per-kernel profiles; prints one line and no JSON:
+      slot_sssp / slot_bfs / slot_ppr  batched SSSP, BFS, PPR (20 iterations) of
+                                       256 sources on RMAT-18 (relabelled)
+      nearfar / advance_grid           SSSP from the corner of a 1024^2 grid on
+                                       the near-far / device-driven advance engine
+      advance_lb                       SSSP on RMAT-20 on the advance engine
+                                       (edge-balanced push steps), 4 sources
+      blas_rmat20                      SSSP on RMAT-20 on the BLAS engine, 4 sources
+    """
+    import torch
+    import graphone_b200 as g1
+    from graphone_b200 import gen
+    dev = "cuda"
+    if name.startswith("slot_"):
+        g = gen.rmat(18, 16, True, (1, 64), device=dev)
+        G = g1.Graph.from_gen(g, relabel=True)
+        srcs = gen.pick_sources(g, 256)
+        for _ in range(2):
+            if name == "slot_sssp":
+                G.sssp_batch(srcs)
+            elif name == "slot_bfs":
+                G.bfs_batch(srcs)
+            else:
+                G.ppr_batch(srcs, 0.85, 20)
+    elif name in ("nearfar", "advance_grid"):
+        g = gen.grid2d(1024, 1024, (1, 100), device=dev)
+        G = g1.Graph.from_gen(g)
+        for _ in range(2):
+            G.sssp(0, g1.ENGINE_NEARFAR if name == "nearfar" else g1.ENGINE_ADVANCE)
+    else:
+        g = gen.rmat(20, 16, True, (1, 64), device=dev)
+        G = g1.Graph.from_gen(g)
+        for s in gen.pick_sources(g, 4):
+            G.sssp(int(s), g1.ENGINE_ADVANCE if name == "advance_lb" else g1.ENGINE_BLAS)
+    torch.cuda.synchronize()
+    print("kernel workload", name, "done", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -817,7 +869,12 @@ def main():
     ap.add_argument("--sched", default="auto",
                     help="auto (the library's default merge variant) | tune (time every "
                          "variant and keep the fastest) | mergeN (variant N) | vector")
+    ap.add_argument("--kernel-workload", choices=KERNEL_WORKLOADS, default=None,
+                    help="run one small workload for a per-kernel profile and exit")
     args = ap.parse_args()
+    if args.kernel_workload:
+        run_kernel_workload(args.kernel_workload)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -35,7 +35,7 @@ PR_REFERENCE, PR_DANGLING = 0, 1
 MERGE_VARIANTS = ("warp", "warp", "warp", "cta_tma", "cta_tma", "warp",
                   "warp_tma", "warp_tma", "warp_tma", "warp_tma", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz",
                   "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz", "nnz",
-                  "nnz2", "nnz2", "nnz2", "nnz2")
+                  "nnz2", "nnz2", "nnz2", "nnz2", "nnz2", "nnz2", "nnz2", "nnz2")
 DEFAULT_MERGE_VARIANT = 17
 GRAPH_SYMMETRIC, GRAPH_INPUT_TRANSPOSE, GRAPH_BUILD_OTHER, GRAPH_NO_VALIDATE = 1, 2, 4, 8
 GRAPH_RELABEL = 16

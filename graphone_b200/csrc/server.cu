@@ -14,10 +14,11 @@
 //      launched and an event recorded behind it.
 // Executors never wait for one another, so work on different graphs and
 // kinds overlaps on the device, and a query joins a running batch at the
-// next step boundary instead of waiting for the batch to drain.  SSSP on
-// graphs of small uniform degree (grids) is the exception: there one query
-// at a time runs on the near-far engine (nearfar.cu), which beats batched
-// Bellman-Ford on such graphs by orders of magnitude.
+// next step boundary instead of waiting for the batch to drain.  SSSP and
+// BFS on graphs of small uniform degree (grids) are the exception: there one
+// query at a time runs on the near-far engine (nearfar.cu), which beats
+// batched Bellman-Ford on such graphs by orders of magnitude, and batched BFS
+// by its thousands of levels (a step each).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -70,9 +71,10 @@ struct Exec {
     std::vector<Request*> slot_req;  // query of each slot
     std::vector<Request*> retiring;  // results enqueued before ev
     DevBuf staging;                  // pageable outputs
-    // SSSP on graphs of small uniform degree: one query at a time on the
-    // near-far engine instead of slots (batched Bellman-Ford relaxes such
-    // graphs' vertices many times over)
+    // SSSP and BFS on graphs of small uniform degree: one query at a time on
+    // the near-far engine instead of slots (batched Bellman-Ford relaxes such
+    // graphs' vertices many times over; batched BFS steps through thousands
+    // of levels)
     bool nearfar = false;
     uint32_t nf_delta = 1;
     DevBuf nf_store;
@@ -319,7 +321,7 @@ bool service_nearfar(g1_server* S, Exec& E, bool stopping) {
     E.nf_req = r;
     const g1_graph* g = E.g;
     const uint32_t* perm = g->relabeled ? g->perm.as<uint32_t>() : nullptr;
-    bool ok = nearfar_launch(g, r->src, false, E.nf_delta, E.nf, E.s, perm) == G1_OK;
+    bool ok = nearfar_launch(g, r->src, E.kind == kSlotBfs, E.nf_delta, E.nf, E.s, perm) == G1_OK;
     // distances in caller order into the query's output
     const size_t row = (size_t)g->n * 4;
     void* dst = r->out_dev;
@@ -534,9 +536,9 @@ g1_status init_exec(g1_graph* g, int kind, Exec& E) {
     if (kind == kSlotSssp && g->vtype != G1_U32) return G1_OK;
     std::lock_guard<std::mutex> lk(g->mu);
     G1_TRY(slot_graph(g, kind, E.s, &E.sg));
-    if (kind == kSlotSssp && nearfar_suits(g)) {
+    if ((kind == kSlotSssp || kind == kSlotBfs) && nearfar_suits(g)) {
         E.nearfar = true;
-        G1_TRY(nearfar_delta(g, false, E.s, &E.nf_delta));
+        G1_TRY(nearfar_delta(g, kind == kSlotBfs, E.s, &E.nf_delta));
     }
     E.usable = true;
     return G1_OK;

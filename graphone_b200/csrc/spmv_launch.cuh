@@ -25,7 +25,8 @@ constexpr int kVectorBlock = 256;
 //           = next tile's col and val / col only staged in shared memory by
 //           bulk copies, stages / 32 = L2 prefetch distance in rounds;
 //   kind 5: nnz-split warp tiles of 32 * ipt nonzeros (spmv_nnz2_kernel, the
-//           nnz plan for that tile size).
+//           nnz plan for that tile size); stages bit 0 = contiguous tile
+//           ranges per block.
 // `warps` per block (kind 0/2/3), `hot` x entries cached in shared memory,
 // `minb` resident blocks per SM the register budget is sized for.
 struct MergeVariant {
@@ -48,8 +49,10 @@ constexpr MergeVariant kMergeVariants[] = {
     {3, 8, 8, 32, 32768, 1},  {3, 8, 8, 32, 16384, 1},  {3, 8, 16, 32, 32768, 1},
     {3, 8, 16, 32, 24576, 1}, {3, 8, 32, 32, 32768, 1}, {3, 8, 64, 32, 32768, 1},
     {3, 8, 128, 32, 32768, 1}, {3, 8, 66, 24, 32768, 1}, {5, 8, 0, 32, 32768, 1},
-    {5, 16, 0, 32, 32768, 1}, {5, 24, 0, 32, 32768, 1}, {5, 16, 0, 32, 16384, 1}};
-constexpr int kNumMergeVariants = 36;
+    {5, 16, 0, 32, 32768, 1}, {5, 24, 0, 32, 32768, 1}, {5, 16, 0, 32, 16384, 1},
+    {5, 8, 1, 32, 32768, 1},  {5, 8, 0, 32, 24576, 1},  {5, 8, 0, 32, 40960, 1},
+    {5, 8, 1, 32, 24576, 1}};
+constexpr int kNumMergeVariants = 40;
 constexpr int kDefaultVariant = 17;
 
 template <class K>
@@ -144,12 +147,12 @@ struct NnzKernel {
     }
 };
 
-template <class SR, class Epi, int WARPS, int HOT, int IPT>
+template <class SR, class Epi, int WARPS, int HOT, int IPT, bool CONTIG = false>
 struct Nnz2Kernel {
     using L = Nnz2Layout<SR, WARPS, HOT, IPT>;
     static int occupancy() {
         static int occ = [] {
-            auto k = spmv_nnz2_kernel<SR, Epi, WARPS, HOT, IPT>;
+            auto k = spmv_nnz2_kernel<SR, Epi, WARPS, HOT, IPT, CONTIG>;
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
             return blocks_per_sm(k, WARPS * 32, L::BYTES);
         }();
@@ -265,16 +268,16 @@ NnzArgs<SR> nnz_args(const g1_graph* g, int t, const NnzPlan& p, const typename 
     return a;
 }
 
-template <class SR, class Epi, int WARPS, int HOT, int IPT>
+template <class SR, class Epi, int WARPS, int HOT, int IPT, bool CONTIG = false>
 g1_status launch_nnz2(g1_graph* g, int t, const typename SR::x_t* x, const Epi& main_epi,
                       const Epi& fix_epi, cudaStream_t s) {
     NnzPlan* p = nullptr;
     G1_TRY(ensure_nnz_plan(g, t, &p, 32u * IPT));
-    using K = Nnz2Kernel<SR, Epi, WARPS, HOT, IPT>;
+    using K = Nnz2Kernel<SR, Epi, WARPS, HOT, IPT, CONTIG>;
     const NnzArgs<SR> a = nnz_args<SR>(g, t, *p, x);
     if (((uintptr_t)a.col | (uintptr_t)a.val) & 31u)
         return fail(G1_ERR_UNSUPPORTED, "nnz SpMV: col/val not 32-byte aligned");
-    auto mk = spmv_nnz2_kernel<SR, Epi, WARPS, HOT, IPT>;
+    auto mk = spmv_nnz2_kernel<SR, Epi, WARPS, HOT, IPT, CONTIG>;
     auto fk = spmv_nnz_fixup_kernel<SR, Epi, kMergeBlock>;
     if (profiling()) {
         prof_mark(s, true);
@@ -332,7 +335,11 @@ g1_status merge_grids(g1_graph* g, int t, uint32_t* main_grid, uint32_t* fix_gri
             case 32: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 8>::grid(g, q->n_tiles); break;
             case 33: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 16>::grid(g, q->n_tiles); break;
             case 34: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 24>::grid(g, q->n_tiles); break;
-            default: *main_grid = Nnz2Kernel<SR, Epi, 32, 16384, 16>::grid(g, q->n_tiles); break;
+            case 35: *main_grid = Nnz2Kernel<SR, Epi, 32, 16384, 16>::grid(g, q->n_tiles); break;
+            case 36: *main_grid = Nnz2Kernel<SR, Epi, 32, 32768, 8, true>::grid(g, q->n_tiles); break;
+            case 37: *main_grid = Nnz2Kernel<SR, Epi, 32, 24576, 8>::grid(g, q->n_tiles); break;
+            case 38: *main_grid = Nnz2Kernel<SR, Epi, 32, 40960, 8>::grid(g, q->n_tiles); break;
+            default: *main_grid = Nnz2Kernel<SR, Epi, 32, 24576, 8, true>::grid(g, q->n_tiles); break;
         }
         *fix_grid = nnz_fix_grid<SR, Epi>(g, *q);
         return G1_OK;
@@ -449,7 +456,11 @@ g1_status launch_merge(g1_graph* g, int t, const typename SR::x_t* x, const Epi&
             case 32: return launch_nnz2<SR, Epi, 32, 32768, 8>(g, t, x, main_epi, fix_epi, s);
             case 33: return launch_nnz2<SR, Epi, 32, 32768, 16>(g, t, x, main_epi, fix_epi, s);
             case 34: return launch_nnz2<SR, Epi, 32, 32768, 24>(g, t, x, main_epi, fix_epi, s);
-            default: return launch_nnz2<SR, Epi, 32, 16384, 16>(g, t, x, main_epi, fix_epi, s);
+            case 35: return launch_nnz2<SR, Epi, 32, 16384, 16>(g, t, x, main_epi, fix_epi, s);
+            case 36: return launch_nnz2<SR, Epi, 32, 32768, 8, true>(g, t, x, main_epi, fix_epi, s);
+            case 37: return launch_nnz2<SR, Epi, 32, 24576, 8>(g, t, x, main_epi, fix_epi, s);
+            case 38: return launch_nnz2<SR, Epi, 32, 40960, 8>(g, t, x, main_epi, fix_epi, s);
+            default: return launch_nnz2<SR, Epi, 32, 24576, 8, true>(g, t, x, main_epi, fix_epi, s);
         }
     }
     if (kMergeVariants[v].kind == 3) {

@@ -1610,7 +1610,11 @@ __device__ __forceinline__ void nnz2_finish(const NnzArgs<SR>& a, const Nnz2Read
     __syncwarp();
 }
 
-template <class SR, class Epi, int WARPS, int HOT, int IPT>
+// CONTIG: block b folds the contiguous tile range [b * T, (b + 1) * T),
+// T = ceil(n_tiles / blocks), its warps taking consecutive tiles, so that an
+// SM streams one contiguous stretch of col/val and writes one stretch of
+// rows; otherwise warp w of the grid takes tiles w, w + warps, ...
+template <class SR, class Epi, int WARPS, int HOT, int IPT, bool CONTIG = false>
 __global__ void __launch_bounds__(WARPS * 32, 1)
 spmv_nnz2_kernel(NnzArgs<SR> a, Epi epi) {
     using X = typename SR::x_t;
@@ -1629,9 +1633,19 @@ spmv_nnz2_kernel(NnzArgs<SR> a, Epi epi) {
         fill_x_cache<WARPS * 32>(xc, a.x, hot);
         __syncthreads();
     }
-    const uint32_t total_warps = gridDim.x * WARPS;
     const uint32_t n_tiles = a.plan.n_tiles;
-    for (uint32_t tile = blockIdx.x * WARPS + w; tile < n_tiles; tile += total_warps) {
+    uint32_t first, end, step;
+    if constexpr (CONTIG) {
+        const uint32_t per = (uint32_t)ceil_div(n_tiles, gridDim.x);
+        first = blockIdx.x * per + w;
+        end = min(n_tiles, (blockIdx.x + 1) * per);
+        step = WARPS;
+    } else {
+        first = blockIdx.x * WARPS + w;
+        end = n_tiles;
+        step = gridDim.x * WARPS;
+    }
+    for (uint32_t tile = first; tile < end; tile += step) {
         const Nnz2Ready<SR, Epi, IPT> r = nnz2_fetch<SR, Epi, HOT, IPT>(a, tile, xc, hot, epi);
         if (tile + 1 < n_tiles) nnz2_finish<SR, Epi, IPT, true>(a, r, tile, sy, epi);
         else nnz2_finish<SR, Epi, IPT, false>(a, r, tile, sy, epi);

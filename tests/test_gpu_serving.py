@@ -237,10 +237,11 @@ def test_concurrent_submitters(cuda):
         assert np.array_equal(outs[i], G.sssp(int(srcs[i])))
 
 
+@pytest.mark.parametrize("kind", [g1.QUERY_SSSP, g1.QUERY_BFS])
 @pytest.mark.parametrize("relabel", [False, True])
-def test_served_grid_sssp_runs_on_the_nearfar_engine(cuda, relabel):
-    """SSSP on a grid goes to the near-far engine one query at a time; the
-    results equal every other engine's, in caller vertex order."""
+def test_served_grid_sssp_runs_on_the_nearfar_engine(cuda, relabel, kind):
+    """SSSP and BFS on a grid go to the near-far engine one query at a time;
+    the results equal every other engine's, in caller vertex order."""
     g = gen.grid2d(48, 37, (1, 100))
     G = g1.Graph.from_gen(g, relabel=relabel)
     rp, ci, v = g.np("n")
@@ -249,13 +250,17 @@ def test_served_grid_sssp_runs_on_the_nearfar_engine(cuda, relabel):
     dev = torch.empty((len(srcs), g.n), dtype=torch.int32, device="cuda")
     with g1.Server() as srv:
         gid = srv.add_graph(G)
-        ts = [srv.submit(gid, g1.QUERY_SSSP, s, host[i]) for i, s in enumerate(srcs)]
-        ts += [srv.submit(gid, g1.QUERY_SSSP, s, dev[i]) for i, s in enumerate(srcs)]
+        ts = [srv.submit(gid, kind, s, host[i]) for i, s in enumerate(srcs)]
+        ts += [srv.submit(gid, kind, s, dev[i]) for i, s in enumerate(srcs)]
         for t in ts:
             srv.wait(t, 60000)
     d = dev.cpu().numpy().view(np.uint32)
     for i, s in enumerate(srcs):
-        ref = O.dijkstra_u32(rp, ci, v, s)
+        if kind == g1.QUERY_SSSP:
+            ref = O.dijkstra_u32(rp, ci, v, s)
+            assert np.array_equal(G.sssp(s, g1.ENGINE_NEARFAR), ref)
+        else:
+            ref = O.bfs(rp, ci, s)
+            assert np.array_equal(G.bfs(s, g1.ENGINE_NEARFAR), ref)
         assert np.array_equal(host[i], ref)
         assert np.array_equal(d[i], ref)
-        assert np.array_equal(G.sssp(s, g1.ENGINE_NEARFAR), ref)
