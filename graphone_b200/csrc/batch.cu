@@ -236,8 +236,3 @@ extern "C" g1_status g1_ppr_batch(g1_graph* g, const uint32_t* srcs, uint32_t k,
                                   uint32_t iters, float* rank_out, void* stream) {
     return entry(g, kSlotPpr, srcs, k, rank_out, nullptr, alpha, iters, kMaxSlots, stream);
 }
-
-extern "C" g1_status g1_ppr(g1_graph* g, uint32_t src, float alpha, uint32_t iters, float* rank_out,
-                            void* stream) {
-    return entry(g, kSlotPpr, &src, 1, rank_out, nullptr, alpha, iters, 32, stream);
-}

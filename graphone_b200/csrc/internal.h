@@ -231,6 +231,29 @@ g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out);
 // The nnz-split plan for tiles of `tile` nonzeros (a multiple of 32; 256 is
 // the default schedule's).
 g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out, uint32_t tile = 256);
+// Per-vertex out-degrees (edge count, n words in the graph's workspace),
+// derived once per graph; the caller holds g->mu.
+g1_status out_degrees(g1_graph* g, uint32_t** deg, cudaStream_t s);
+// Single-source personalized PageRank on the SpMV schedules (pagerank.cu).
+// A run's state lives in caller-owned device memory (`words` 4-byte words,
+// 256-byte aligned), so runs on different streams share no scratch.
+// ppr_prepare derives the graph's out-degrees and nnz plan (the caller holds
+// g->mu); ppr_enqueue then reads only the graph's fixed arrays and enqueues
+// the run on `s`: src is a caller id when perm (the graph's relabelling) is
+// given; *rank_out points into the store (internal vertex order).
+struct PprPlan {
+    const uint32_t* deg = nullptr;
+    const NnzPlan* plan = nullptr;  // null: the CSR-vector schedule
+    size_t words = 0;
+};
+size_t ppr_state_words(uint32_t n, const NnzPlan* plan);
+g1_status ppr_prepare(g1_graph* g, cudaStream_t s, PprPlan* out);
+g1_status ppr_enqueue(g1_graph* g, const PprPlan& pl, uint32_t* store, uint32_t src, float alpha,
+                      uint32_t iters, const uint32_t* perm, cudaStream_t s, const float** rank_out);
+// g1_ppr with the graph's workspace as the store (caller vertex src, ranks
+// in caller order into rank_out, host or device); the caller holds g->mu.
+g1_status ppr_locked(g1_graph* g, uint32_t src, float alpha, uint32_t iters, float* rank_out,
+                     cudaStream_t s);
 // Near-far SSSP (unit = BFS) from internal vertex src in one persistent
 // launch; *dist_out points to the graph's workspace distances.
 g1_status nearfar_traverse(g1_graph* g, uint32_t src, bool unit, uint32_t** dist_out, uint32_t* rounds,

@@ -276,6 +276,183 @@ static g1_status pr_iterate(g1_graph* g, const PrBuffers& b, const uint32_t* gri
     return launch_merge<PlusTimesF32>(g, t, b.x[cur], e, f, s);
 }
 
+// ------------------------------------------------ personalized PageRank
+//
+// Single-source PPR (the pagerank_blas iteration restarted at src, as the
+// batched slot engine runs it) on the same SpMV schedules: x[u] = rank[u] *
+// alpha / outdeg(u) is built by the previous iteration's epilogue, the SpMV
+// sums x over each row's in-edges with every edge weight taken as 1 (the
+// edge values are not read: 4 bytes per nonzero instead of 8), and the
+// epilogue adds the teleport (1 - alpha) + alpha * sum(rank[dangling]) at
+// src, writes x' and accumulates the next dangling sum (fixed point, as
+// PageRank's).  Every vertex other than src without in-edges has rank 0 from
+// the first iteration on, so before the last iteration the nnz fixup emits
+// no empty row: only src, when its own row is empty, is emitted by the
+// fixup's first thread.
+struct PprEpilogue {
+    static constexpr bool kRowsIndependent = true;
+    float* rank_next;
+    float* x_next;
+    const float* iw;
+    const uint32_t* src_p;  // internal id of the source
+    const unsigned long long* dang_in;
+    unsigned long long* dang_out;
+    unsigned long long* dang_clear;  // null in the fixup
+    double alpha;
+    int write_rank;
+    // nnz fixup before the last iteration: an empty list (no empty row
+    // emitted) and the in-edge row pointers, to emit src if its row is empty
+    const uint32_t* empty_list = nullptr;
+    uint32_t n_empty_list = 0;
+    const uint32_t* src_rows = nullptr;
+
+    uint32_t src;
+    float tele;
+    unsigned long long dang_local;
+
+    __device__ __forceinline__ void begin() {
+        dang_local = 0ull;
+        if (dang_clear && blockIdx.x == 0 && threadIdx.x == 0) *dang_clear = 0ull;
+        src = *src_p;
+        tele = (float)((1.0 - alpha) + alpha * ((double)(*dang_in) / kDangScale));
+        if (src_rows && blockIdx.x == 0 && threadIdx.x == 0 && src_rows[src] == src_rows[src + 1])
+            emit_prepared(src, 0.0f, iw[src]);
+    }
+    __device__ __forceinline__ void emit(uint32_t v, const float& y) {
+        emit_prepared(v, y, prepare(v));
+    }
+    __device__ __forceinline__ float prepare(uint32_t v) const { return __ldg(iw + v); }
+    __device__ __forceinline__ void emit_prepared(uint32_t v, const float& y, float w) {
+        const float r = v == src ? y + tele : y;
+        if (write_rank) rank_next[v] = r;
+        if (w != 0.0f) x_next[v] = r * w;
+        else dang_local += dang_fixed(r);
+    }
+    template <int BLOCK>
+    __device__ __forceinline__ void block_end(char* smem) {
+        dang_block_add<BLOCK>(dang_local, dang_out, smem);
+    }
+};
+
+// iw[v] = alpha / outdeg(v), 0 without out-edges (the slot engine's
+// transition weights, bit for bit).
+__global__ void ppr_iw_kernel(const uint32_t* deg, uint32_t n, double alpha, float* iw) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        iw[v] = deg[v] ? (float)(alpha / (double)deg[v]) : 0.0f;
+}
+
+// rank0 = e_src, x0 = rank0 * iw, the dangling sum of rank0 (fixed point:
+// 1.0 is 2^56); x0 and x1 are zero elsewhere (cleared by the caller).
+__global__ void ppr_init_kernel(const uint32_t* perm, uint32_t src, const float* iw, uint32_t* src_out,
+                                float* rank0, float* x0, unsigned long long* dang) {
+    const uint32_t v = perm ? perm[src] : src;
+    *src_out = v;
+    rank0[v] = 1.0f;
+    x0[v] = iw[v];
+    dang[0] = iw[v] == 0.0f ? (1ull << 56) : 0ull;
+    dang[1] = 0ull;
+    dang[2] = 0ull;
+}
+
+namespace {
+
+constexpr size_t kPprAlign = 64;  // words (256 bytes)
+size_t ppr_round(size_t w) { return (w + kPprAlign - 1) / kPprAlign * kPprAlign; }
+
+struct PprLayout {
+    unsigned long long* dang;
+    uint32_t* src;
+    float *iw, *rank[2], *x[2], *carry, *tail;
+};
+
+PprLayout ppr_layout(uint32_t n, const NnzPlan* plan, uint32_t* store) {
+    PprLayout L;
+    size_t w = 0;
+    auto take = [&](size_t words) {
+        uint32_t* p = store + w;
+        w += ppr_round(words);
+        return p;
+    };
+    L.dang = reinterpret_cast<unsigned long long*>(take(8));
+    L.src = take(1);
+    L.iw = reinterpret_cast<float*>(take(n));
+    for (int i = 0; i < 2; ++i) L.rank[i] = reinterpret_cast<float*>(take(n));
+    for (int i = 0; i < 2; ++i) L.x[i] = reinterpret_cast<float*>(take(n));
+    const size_t nt = plan ? (size_t)plan->n_tiles + 1 : 1;
+    L.carry = reinterpret_cast<float*>(take(nt));
+    L.tail = reinterpret_cast<float*>(take(nt));
+    return L;
+}
+
+}  // namespace
+
+size_t ppr_state_words(uint32_t n, const NnzPlan* plan) {
+    const size_t nt = plan ? (size_t)plan->n_tiles + 1 : 1;
+    return ppr_round(8) + ppr_round(1) + 5 * ppr_round(n) + 2 * ppr_round(nt);
+}
+
+g1_status ppr_prepare(g1_graph* g, cudaStream_t s, PprPlan* out) {
+    if (!g->o[1].present)
+        return fail(G1_ERR_UNSUPPORTED, "personalized PageRank needs the in-edge CSR (G1_GRAPH_BUILD_OTHER)");
+    uint32_t* deg = nullptr;
+    G1_TRY(out_degrees(g, &deg, s));
+    out->deg = deg;
+    out->plan = nullptr;
+    if (resolve_schedule(g, 1, G1_SCHED_AUTO) != G1_SCHED_VECTOR) {
+        NnzPlan* p = nullptr;
+        G1_TRY(ensure_nnz_plan(g, 1, &p));
+        out->plan = p;
+    }
+    out->words = ppr_state_words(g->n, out->plan);
+    return G1_OK;
+}
+
+g1_status ppr_enqueue(g1_graph* g, const PprPlan& pl, uint32_t* store, uint32_t src, float alpha,
+                      uint32_t iters, const uint32_t* perm, cudaStream_t s, const float** rank_out) {
+    const uint32_t n = g->n;
+    const int t = 1;
+    const PprLayout L = ppr_layout(n, pl.plan, store);
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
+    ppr_iw_kernel<<<grid, 256, 0, s>>>(pl.deg, n, (double)alpha, L.iw);
+    G1_CUDA(cudaMemsetAsync(L.x[0], 0, (size_t)n * 4, s));
+    G1_CUDA(cudaMemsetAsync(L.x[1], 0, (size_t)n * 4, s));
+    if (iters == 0) G1_CUDA(cudaMemsetAsync(L.rank[0], 0, (size_t)n * 4, s));
+    ppr_init_kernel<<<1, 1, 0, s>>>(perm, src, L.iw, L.src, L.rank[0], L.x[0], L.dang);
+    count_launches(2);
+    G1_CUDA(cudaGetLastError());
+    for (uint32_t it = 0; it < iters; ++it) {
+        const bool last = it + 1 == iters;
+        const int cur = it & 1, nxt = cur ^ 1;
+        PprEpilogue e;
+        e.rank_next = L.rank[nxt];
+        e.x_next = L.x[nxt];
+        e.iw = L.iw;
+        e.src_p = L.src;
+        e.dang_in = &L.dang[it % 3];
+        e.dang_out = &L.dang[(it + 1) % 3];
+        e.dang_clear = &L.dang[(it + 2) % 3];
+        e.alpha = (double)alpha;
+        e.write_rank = last ? 1 : 0;
+        if (!pl.plan) {
+            G1_TRY((launch_vector<PlusPatternF32>(g, t, L.x[cur], e, s)));
+            continue;
+        }
+        PprEpilogue f = e;
+        f.dang_clear = nullptr;
+        if (!last) {
+            f.empty_list = L.src;  // never read: the list is empty
+            f.n_empty_list = 0;
+            f.src_rows = g->o[t].rp;
+        }
+        G1_TRY((launch_nnz<PlusPatternF32, PprEpilogue, 32, 1, 32768>(g, t, *pl.plan, L.x[cur], e, f, s,
+                                                                      L.carry, L.tail)));
+    }
+    *rank_out = L.rank[iters & 1];
+    return G1_OK;
+}
+
 }  // namespace g1
 
 using namespace g1;
@@ -299,4 +476,32 @@ extern "C" g1_status g1_pagerank(g1_graph* g, float alpha, int iters, g1_pr_mode
         G1_TRY(pr_iterate(g, b, grids, alpha, mode, it, iters, G1_SCHED_AUTO, s));
     G1_TRY(copy_out_vertices(g, rank_out, b.rank[iters & 1], s));
     return check_device_error(g, s);
+}
+
+namespace g1 {
+
+g1_status ppr_locked(g1_graph* g, uint32_t src, float alpha, uint32_t iters, float* rank_out,
+                     cudaStream_t s) {
+    if (src >= g->n) return fail(G1_ERR_INVALID, "source vertex out of range");
+    PprPlan pl;
+    G1_TRY(ppr_prepare(g, s, &pl));
+    uint32_t* store = nullptr;
+    G1_TRY(g->ws.get("ppr_store", pl.words, &store));
+    const float* rank = nullptr;
+    const uint32_t* perm = g->relabeled ? g->perm.as<uint32_t>() : nullptr;
+    G1_TRY(ppr_enqueue(g, pl, store, src, alpha, iters, perm, s, &rank));
+    G1_TRY(copy_out_vertices(g, rank_out, rank, s));
+    return check_device_error(g, s);
+}
+
+}  // namespace g1
+
+extern "C" g1_status g1_ppr(g1_graph* g, uint32_t src, float alpha, uint32_t iters, float* rank_out,
+                            void* stream) {
+    if (!g || !rank_out) return fail(G1_ERR_INVALID, "g1_ppr: bad argument");
+    if (!(alpha > 0.0f && alpha < 1.0f))
+        return fail(G1_ERR_INVALID, "personalized PageRank: damping must be in (0, 1)");
+    DeviceGuard dg(g->device);
+    std::lock_guard<std::mutex> lk(g->mu);
+    return ppr_locked(g, src, alpha, iters, rank_out, as_stream(stream));
 }

@@ -14,11 +14,22 @@
 //      launched and an event recorded behind it.
 // Executors never wait for one another, so work on different graphs and
 // kinds overlaps on the device, and a query joins a running batch at the
-// next step boundary instead of waiting for the batch to drain.  SSSP and
-// BFS on graphs of small uniform degree (grids) are the exception: there one
-// query at a time runs on the near-far engine (nearfar.cu), which beats
-// batched Bellman-Ford on such graphs by orders of magnitude, and batched BFS
-// by its thousands of levels (a step each).
+// next step boundary instead of waiting for the batch to drain.
+//
+// Batches pay only when many queries share a step: a step of one 32-slot
+// word costs about what a full word's does, and up to a few dozen queries
+// the single-source engines finish them sooner one by one.  So the server
+// also has a solo lane: one worker thread that runs queries one at a time,
+// oldest first across executors, on the single-source engines (the calls a
+// plain per-request user makes: traverse.cu's AUTO engine, which picks the
+// near-far engine on grids, and pagerank.cu's SpMV PPR), on its own stream.
+//   - SSSP and BFS on graphs of small uniform degree (grids) always take
+//     the lane: batched Bellman-Ford relaxes such graphs' vertices many
+//     times over, and batched BFS steps through thousands of levels;
+//   - the other executors are hybrid: with their slots empty and fewer than
+//     a word of queries waiting (or a queue that one-by-one runs clear
+//     within solo_queue_ms) their queries take the lane; beyond that they
+//     are batched on the slot engine, concurrently with the lane.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -30,6 +41,8 @@
 #include <thread>
 #include <unordered_map>
 #include <vector>
+
+#include <pthread.h>
 
 #include "internal.h"
 #include "slots.cuh"
@@ -71,17 +84,32 @@ struct Exec {
     std::vector<Request*> slot_req;  // query of each slot
     std::vector<Request*> retiring;  // results enqueued before ev
     DevBuf staging;                  // pageable outputs
-    // SSSP and BFS on graphs of small uniform degree: one query at a time on
-    // the near-far engine instead of slots (batched Bellman-Ford relaxes such
-    // graphs' vertices many times over; batched BFS steps through thousands
-    // of levels)
-    bool nearfar = false;
-    uint32_t nf_delta = 1;
-    DevBuf nf_store;
-    NfBuffers nf{};
-    PinnedBuf nf_host;
-    Request* nf_req = nullptr;
+    // Where the executor's queries run (init_exec):
+    //  - lane_only: SSSP and BFS on graphs of small uniform degree (grids)
+    //    always run one at a time on the server's solo lane, where the AUTO
+    //    engine picks the near-far engine (batched Bellman-Ford relaxes such
+    //    graphs' vertices many times over; batched BFS steps through
+    //    thousands of levels);
+    //  - hybrid: while its slots are empty and the queue is short
+    //    (lane_mode), the executor's queries go to the solo lane too (SSSP /
+    //    BFS: traverse.cu's AUTO engine; PPR: pagerank.cu's SpMV schedules,
+    //    4 bytes per edge and iteration where a slot step reads a 128-byte
+    //    rank row per edge); beyond that they are batched on the slot engine;
+    //  - neither: always batched (solo_queue_ms < 0, or SSSP / BFS without
+    //    the out-edge CSR the AUTO engine pushes over).
+    bool lane_only = false;
+    bool hybrid = false;
+    std::atomic<bool> on_lane{false};  // one of its queries runs on the lane
+    std::atomic<double> solo_ms{0.0};  // moving average of its lane query time
 };
+
+// A hybrid executor batches on its slot engine once at least kSlotMinQueue
+// queries (one 32-slot word) wait and running them one by one would take
+// longer than the server's solo_queue_ms (default kSoloQueueMs).  Below a
+// word of queries a slot step costs about as much as a full word's, which
+// single-source runs beat.
+constexpr double kSoloQueueMs = 20.0;
+constexpr size_t kSlotMinQueue = 32;
 
 }  // namespace
 }  // namespace g1
@@ -94,7 +122,8 @@ struct g1_server {
     uint64_t reserve = 0, limit = 0;
     float alpha = 0.85f;
     uint32_t ppr_iters = 20;
-    uint32_t idle_ms = 1000;
+    uint32_t idle_ms = 0;  // 0: engine state is kept until memory is needed
+    double solo_queue_ms = kSoloQueueMs;  // negative: never solo
     std::vector<std::unique_ptr<Exec>> execs;  // graph * 3 + kind
     std::mutex mu;                             // everything below
     std::condition_variable cv_in, cv_done;
@@ -112,6 +141,16 @@ struct g1_server {
     std::atomic<uint32_t> engines{0};
     std::mutex graphs_mu;  // add_graph vs the loop's view of execs
     std::atomic<size_t> n_execs{0};
+    // The solo lane: one worker thread running queries one at a time on the
+    // single-source engines, oldest first across executors (the order and
+    // engines of plain per-request calls).
+    std::thread lane;
+    std::mutex lane_mu;  // lane_req, lane_exec, lane_stop
+    std::condition_variable lane_cv;
+    Request* lane_req = nullptr;
+    Exec* lane_exec = nullptr;
+    bool lane_stop = false;
+    std::atomic<bool> lane_busy{false};
 };
 
 namespace g1 {
@@ -144,20 +183,19 @@ void complete_one(g1_server* S, Request* r, g1_status st) {
     complete(S, v, st);
 }
 
-bool holds_memory(const Exec& E) { return E.eng.ready() || E.nf_store.p != nullptr; }
+bool holds_memory(const Exec& E) { return E.eng.ready(); }
 
 void release_engine(g1_server* S, Exec& E) {
     if (!holds_memory(E)) return;
-    S->dev_bytes -= E.eng.device_bytes() + E.nf_store.bytes;
+    S->dev_bytes -= E.eng.device_bytes();
     S->engines -= 1;
     E.eng.release();
-    E.nf_store.release();
     E.staging.release();
 }
 
 bool idle(const Exec& E) {
     return holds_memory(E) && E.eng.occupied() == 0 && !E.inflight && E.pending.empty() &&
-           E.retiring.empty() && !E.nf_req;
+           E.retiring.empty() && !E.on_lane.load();
 }
 
 // Frees the state of one idle engine other than `self`.
@@ -273,88 +311,97 @@ g1_status retire(g1_server* S, Exec& E, const std::vector<uint32_t>& fin) {
     return G1_OK;
 }
 
-// Near-far executor: one query in flight.
-bool service_nearfar(g1_server* S, Exec& E, bool stopping) {
-    bool progress = false;
-    if (E.inflight) {
-        const cudaError_t q = cudaEventQuery(E.ev);
-        if (q == cudaErrorNotReady) return false;
-        progress = true;
-        E.inflight = false;
-        g1_status st = G1_OK;
-        if (q != cudaSuccess) {
-            cudaGetLastError();
-            st = G1_ERR_DEVICE;
-        } else {
-            st = nearfar_result(E.nf_host.as<uint32_t>(), nullptr);
+// The solo lane's thread: runs the query handed to it on the single-source
+// engines (the calls of g1_sssp / g1_bfs with G1_ENGINE_AUTO and of g1_ppr),
+// on its own stream, then completes it.
+void lane_worker(g1_server* S) {
+    pthread_setname_np(pthread_self(), "g1-lane");
+    cudaSetDevice(S->device);
+    cudaStream_t ls = nullptr;
+    const bool have_stream = cudaStreamCreateWithFlags(&ls, cudaStreamNonBlocking) == cudaSuccess;
+    if (!have_stream) cudaGetLastError();
+    for (;;) {
+        Request* r = nullptr;
+        Exec* E = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(S->lane_mu);
+            S->lane_cv.wait(lk, [&] { return S->lane_req != nullptr || S->lane_stop; });
+            if (!S->lane_req) break;
+            r = S->lane_req;
+            E = S->lane_exec;
         }
-        complete_one(S, E.nf_req, st);
-        E.nf_req = nullptr;
-        if (st == G1_ERR_DEVICE) release_engine(S, E);
-    }
-    if (stopping || E.pending.empty()) return progress;
-    const size_t need = nearfar_words(E.g->n) * 4;
-    if (!E.nf_store.p) {
-        size_t free_b = device_free_bytes();
-        bool fits = need + S->reserve <= free_b && (!S->limit || S->dev_bytes + need <= S->limit);
-        while (!fits && release_one_idle(S, &E)) {
-            free_b = device_free_bytes();
-            fits = need + S->reserve <= free_b && (!S->limit || S->dev_bytes + need <= S->limit);
+        g1_status st = G1_ERR_DEVICE;
+        const auto t0 = Clock::now();
+        if (have_stream) {
+            std::lock_guard<std::mutex> lk(E->g->mu);
+            if (E->kind == kSlotPpr)
+                st = ppr_locked(E->g, r->src, S->alpha, S->ppr_iters, static_cast<float*>(r->out), ls);
+            else
+                st = traverse_locked(E->g, r->src, G1_ENGINE_AUTO, E->kind == kSlotBfs,
+                                     static_cast<uint32_t*>(r->out), nullptr, ls);
         }
-        if (!fits || E.nf_store.ensure(need) != G1_OK || E.nf_host.ensure(nearfar_ctl_bytes() + 64) != G1_OK) {
-            cudaGetLastError();
-            E.nf_store.release();
-            if (!others_hold_memory(S, &E)) {
-                std::vector<Request*> rs(E.pending.begin(), E.pending.end());
-                E.pending.clear();
-                complete(S, rs, G1_ERR_OOM);
-                return true;
-            }
-            return progress;  // wait for memory
+        const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+        const double prev = E->solo_ms.load();
+        E->solo_ms.store(prev == 0.0 ? ms : 0.75 * prev + 0.25 * ms);
+        complete_one(S, r, st);
+        {
+            std::lock_guard<std::mutex> lk(S->lane_mu);
+            S->lane_req = nullptr;
+            S->lane_exec = nullptr;
         }
-        nearfar_layout(E.g->n, E.nf_store.as<uint32_t>(), &E.nf);
-        S->dev_bytes += E.nf_store.bytes;
-        S->engines += 1;
+        E->on_lane.store(false);
+        S->lane_busy.store(false);
     }
-    Request* r = E.pending.front();
-    E.pending.pop_front();
-    E.nf_req = r;
-    const g1_graph* g = E.g;
-    const uint32_t* perm = g->relabeled ? g->perm.as<uint32_t>() : nullptr;
-    bool ok = nearfar_launch(g, r->src, E.kind == kSlotBfs, E.nf_delta, E.nf, E.s, perm) == G1_OK;
-    // distances in caller order into the query's output
-    const size_t row = (size_t)g->n * 4;
-    void* dst = r->out_dev;
-    if (ok && !dst) ok = E.staging.ensure(row + 16) == G1_OK;
-    if (ok) {
-        uint32_t* d = static_cast<uint32_t*>(dst ? dst : E.staging.p);
-        if (perm)
-            ok = to_caller_order(const_cast<g1_graph*>(g), d, E.nf.dist, E.s) == G1_OK;
-        else
-            ok = cudaMemcpyAsync(d, E.nf.dist, row, cudaMemcpyDeviceToDevice, E.s) == cudaSuccess;
-        if (ok && !dst) ok = cudaMemcpyAsync(r->out, E.staging.p, row, cudaMemcpyDeviceToHost, E.s) == cudaSuccess;
+    if (have_stream) cudaStreamDestroy(ls);
+}
+
+// Whether the executor's waiting queries go to the solo lane: always for
+// lane_only executors; for hybrid ones while their slots are empty, the
+// last step's results are completed and the queue is short.
+bool lane_mode(const g1_server* S, const Exec& E) {
+    if (E.lane_only) return true;
+    if (!E.hybrid || S->solo_queue_ms < 0.0) return false;
+    if (E.eng.occupied() > 0 || E.inflight || !E.retiring.empty()) return false;
+    const double solo = E.solo_ms.load();
+    return !(E.pending.size() >= kSlotMinQueue && solo > 0.0 &&
+             (double)E.pending.size() * solo > S->solo_queue_ms);
+}
+
+// Hands the oldest waiting query of the executors in lane mode to the lane
+// when it is free.
+bool dispatch_lane(g1_server* S, bool stopping) {
+    if (stopping || S->lane_busy.load()) return false;
+    Exec* best = nullptr;
+    const size_t ne = S->n_execs.load();
+    for (size_t i = 0; i < ne; ++i) {
+        Exec& E = *S->execs[i];
+        if (E.pending.empty() || !lane_mode(S, E)) continue;
+        if (!best || E.pending.front()->t_sub < best->pending.front()->t_sub) best = &E;
     }
-    if (ok) ok = cudaMemcpyAsync(E.nf_host.p, E.nf.ctl, nearfar_ctl_bytes(), cudaMemcpyDeviceToHost, E.s) == cudaSuccess;
-    if (ok) ok = cudaEventRecord(E.ev, E.s) == cudaSuccess;
-    if (!ok) {
-        cudaGetLastError();
-        complete_one(S, r, G1_ERR_DEVICE);
-        E.nf_req = nullptr;
-        return true;
+    if (!best) return false;
+    Request* r = best->pending.front();
+    best->pending.pop_front();
+    best->on_lane.store(true);
+    S->lane_busy.store(true);
+    {
+        std::lock_guard<std::mutex> lk(S->lane_mu);
+        S->lane_req = r;
+        S->lane_exec = best;
     }
+    if (!S->lane.joinable()) S->lane = std::thread(lane_worker, S);
+    S->lane_cv.notify_one();
     {
         std::lock_guard<std::mutex> lk(S->mu);
         ++S->steps;
         S->max_occ = std::max(S->max_occ, 1u);
     }
-    E.inflight = true;
-    E.last_busy = Clock::now();
+    best->last_busy = Clock::now();
     return true;
 }
 
 // One turn of one executor; true if anything happened.
 bool service(g1_server* S, Exec& E, bool stopping, std::vector<uint32_t>& fin) {
-    if (E.nearfar) return service_nearfar(S, E, stopping);
+    if (E.lane_only) return false;  // the lane runs its queries
     bool progress = false;
     if (E.inflight) {
         const cudaError_t q = cudaEventQuery(E.ev);
@@ -385,6 +432,7 @@ bool service(g1_server* S, Exec& E, bool stopping, std::vector<uint32_t>& fin) {
                 }
         }
     }
+    if (lane_mode(S, E)) return progress;  // its queries wait for the lane
     // admission
     if (!stopping && !E.pending.empty()) {
         if (!E.eng.ready() && !allocate(S, E) && !others_hold_memory(S, &E)) {
@@ -440,10 +488,11 @@ bool service(g1_server* S, Exec& E, bool stopping, std::vector<uint32_t>& fin) {
 }
 
 bool busy(const Exec& E) {
-    return E.inflight || E.eng.occupied() > 0 || !E.pending.empty() || E.nf_req != nullptr;
+    return E.inflight || E.eng.occupied() > 0 || !E.pending.empty() || E.on_lane.load();
 }
 
 void loop(g1_server* S) {
+    pthread_setname_np(pthread_self(), "g1-serve");
     cudaSetDevice(S->device);
     std::vector<Request*> fresh;
     std::vector<uint32_t> fin;
@@ -472,12 +521,13 @@ void loop(g1_server* S) {
         }
         bool progress = false;
         for (size_t i = 0; i < ne; ++i) progress |= service(S, *S->execs[i], stopping, fin);
+        progress |= dispatch_lane(S, stopping);
         const auto now = Clock::now();
-        bool still = false;
+        bool still = S->lane_busy.load();
         for (size_t i = 0; i < ne; ++i) {
             Exec& E = *S->execs[i];
             still |= busy(E) || !E.retiring.empty();
-            if (idle(E) &&
+            if (S->idle_ms && idle(E) &&
                 std::chrono::duration<double, std::milli>(now - E.last_busy).count() > S->idle_ms)
                 release_engine(S, E);
         }
@@ -514,6 +564,7 @@ extern "C" g1_status g1_server_create(int device, const g1_server_config* cfg, g
         }
         if (cfg->ppr_iters) S->ppr_iters = cfg->ppr_iters;
         if (cfg->idle_release_ms) S->idle_ms = cfg->idle_release_ms;
+        if (cfg->solo_queue_ms) S->solo_queue_ms = cfg->solo_queue_ms;
     }
     // executors for up to 4096 graphs; the vector never reallocates
     S->execs.reserve(3 * 4096);
@@ -537,9 +588,11 @@ g1_status init_exec(g1_graph* g, int kind, Exec& E) {
     std::lock_guard<std::mutex> lk(g->mu);
     G1_TRY(slot_graph(g, kind, E.s, &E.sg));
     if ((kind == kSlotSssp || kind == kSlotBfs) && nearfar_suits(g)) {
-        E.nearfar = true;
-        G1_TRY(nearfar_delta(g, kind == kSlotBfs, E.s, &E.nf_delta));
+        E.lane_only = true;
+        uint32_t delta = 0;  // derived once per graph, ahead of the first query
+        G1_TRY(nearfar_delta(g, kind == kSlotBfs, E.s, &delta));
     }
+    E.hybrid = !E.lane_only && (kind == kSlotPpr || g->o[0].present);
     E.usable = true;
     return G1_OK;
 }
@@ -704,6 +757,13 @@ extern "C" g1_status g1_server_destroy(g1_server* S) {
     }
     S->cv_in.notify_all();
     if (S->th.joinable()) S->th.join();
+    // the loop ended only after the lane's last query completed
+    {
+        std::lock_guard<std::mutex> lk(S->lane_mu);
+        S->lane_stop = true;
+    }
+    S->lane_cv.notify_all();
+    if (S->lane.joinable()) S->lane.join();
     {
         DeviceGuard dg(S->device);
         for (auto& e : S->execs) {

@@ -130,6 +130,24 @@ g1_status read_u32(const uint32_t* dev, uint32_t* out, cudaStream_t s) {
 
 }  // namespace
 
+g1_status out_degrees(g1_graph* g, uint32_t** deg, cudaStream_t s) {
+    const uint32_t n = g->n;
+    G1_TRY(g->ws.get("slot_outdeg", (size_t)n + 1, deg));
+    if (!g->outdeg_ready) {
+        if (g->o[0].present) {
+            out_degree_from_csr_kernel<<<grid_for(g, n), 256, 0, s>>>(g->o[0].rp, n, *deg);
+        } else {
+            G1_CUDA(cudaMemsetAsync(*deg, 0, (size_t)n * 4, s));
+            out_degree_from_transpose_kernel<<<grid_for(g, g->m), 256, 0, s>>>(g->o[1].col, g->m, *deg);
+        }
+        count_launches(1);
+        G1_CUDA(cudaGetLastError());
+        G1_CUDA(cudaStreamSynchronize(s));
+        g->outdeg_ready = true;
+    }
+    return G1_OK;
+}
+
 g1_status slot_graph(g1_graph* g, int kind, cudaStream_t s, SlotGraph* out) {
     if (!g->o[1].present)
         return fail(G1_ERR_UNSUPPORTED, "multi-source traversal needs the in-edge CSR (G1_GRAPH_BUILD_OTHER)");
@@ -206,19 +224,7 @@ g1_status slot_graph(g1_graph* g, int kind, cudaStream_t s, SlotGraph* out) {
         G1_TRY(ws.get("hub_v", (size_t)g->n_hubs + 1, &hub_v));
         G1_TRY(ws.get("hub_hp", (size_t)g->n_hubs + 1, &hub_hp));
         G1_TRY(ws.get("piece_hp", (size_t)g->n_pieces + 1, &piece_hp));
-        G1_TRY(ws.get("slot_outdeg", (size_t)n + 1, &deg));
-        if (!g->outdeg_ready) {
-            if (g->o[0].present) {
-                out_degree_from_csr_kernel<<<grid, 256, 0, s>>>(g->o[0].rp, n, deg);
-            } else {
-                G1_CUDA(cudaMemsetAsync(deg, 0, (size_t)n * 4, s));
-                out_degree_from_transpose_kernel<<<grid_for(g, g->m), 256, 0, s>>>(o.col, g->m, deg);
-            }
-            count_launches(1);
-            G1_CUDA(cudaGetLastError());
-            G1_CUDA(cudaStreamSynchronize(s));
-            g->outdeg_ready = true;
-        }
+        G1_TRY(out_degrees(g, &deg, s));
         sg.hub_v = hub_v;
         sg.hub_hp = hub_hp;
         sg.piece_hp = piece_hp;

@@ -296,9 +296,14 @@ g1_status launch_nnz2(g1_graph* g, int t, const typename SR::x_t* x, const Epi& 
 template <class SR, class Epi, int WARPS, int MINB, int HOT, bool HINTS = false, bool PIPE = false,
           bool PFL1 = false, int BULK = 0, int PFL2 = 0>
 g1_status launch_nnz(g1_graph* g, int t, const NnzPlan& p, const typename SR::x_t* x,
-                     const Epi& main_epi, const Epi& fix_epi, cudaStream_t s) {
+                     const Epi& main_epi, const Epi& fix_epi, cudaStream_t s,
+                     typename SR::value_t* carry = nullptr, typename SR::value_t* tail = nullptr) {
     using K = NnzKernel<SR, Epi, WARPS, MINB, HOT, HINTS, PIPE, PFL1, BULK, PFL2>;
-    const NnzArgs<SR> a = nnz_args<SR>(g, t, p, x);
+    NnzArgs<SR> a = nnz_args<SR>(g, t, p, x);
+    // a caller running concurrently with other SpMVs of the graph brings its
+    // own per-tile partials (n_tiles each)
+    if (carry) a.carry = carry;
+    if (tail) a.tail = tail;
     // the tile kernel reads each lane's col/val with 32-byte loads
     if (((uintptr_t)a.col | (uintptr_t)a.val) & 31u)
         return fail(G1_ERR_UNSUPPORTED, "nnz SpMV: col/val not 32-byte aligned");

@@ -4,6 +4,7 @@
 // functor into a semiring for the SpMV schedules.
 
 #include <cfloat>
+#include <type_traits>
 #include "g1/common.cuh"
 
 namespace g1 {
@@ -42,6 +43,7 @@ struct MinPlusF32 {
 // BFS: min-plus with every edge weight taken as 1 (the edge values are not
 // read).
 struct BfsU32 {
+    static constexpr bool kReadsWeight = false;
     using value_t = uint32_t;
     using x_t = uint32_t;
     using w_t = uint32_t;
@@ -67,6 +69,31 @@ struct PlusTimesF32 {
         return a + b;
     }
 };
+
+// plus over fp32 with every edge weight taken as 1: y[v] = sum of x over
+// v's in-neighbours (the transition of personalized PageRank, whose weights
+// 1/out-degree are folded into x).  The edge values, of any 4-byte type, are
+// not read.
+struct PlusPatternF32 {
+    static constexpr bool kReadsWeight = false;
+    using value_t = float;
+    using x_t = float;
+    using w_t = uint32_t;
+    __host__ __device__ static __forceinline__ float identity() { return 0.0f; }
+    __device__ static __forceinline__ float combine(const uint32_t&, const float& x) { return x; }
+    __device__ static __forceinline__ float reduce(const float& a, const float& b) {
+        return a + b;
+    }
+};
+
+// Whether a semiring's combine uses the edge value (kReadsWeight = false
+// lets the schedules skip loading the values; semirings without the member,
+// GraphOne's functors among them, read them).
+template <class SR, class = void>
+struct reads_weight : std::true_type {};
+template <class SR>
+struct reads_weight<SR, std::void_t<decltype(SR::kReadsWeight)>>
+    : std::integral_constant<bool, SR::kReadsWeight> {};
 
 // GraphOne user functor -> semiring, exactly as the reference's SpmvFunctor
 // adapter (engine/blas_gc.h:113-128): initialize = default_result,

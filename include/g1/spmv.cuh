@@ -41,6 +41,7 @@
 #include <utility>
 
 #include "g1/common.cuh"
+#include "g1/semiring.cuh"
 
 namespace g1 {
 
@@ -1113,17 +1114,20 @@ __device__ __forceinline__ NnzIn nnz_load(const NnzArgs<SR>& a, uint32_t tile, u
     const uint32_t j0 = tile * kNnzTile;
     const uint32_t jl = j0 + lane * kNnzIpt;
     NnzIn in;
+    in.v0 = in.v1 = make_uint4(0u, 0u, 0u, 0u);
     if constexpr (HINTS) {
         in.c0 = ldg_v4_policy(a.col + jl, pol_stream);
         in.c1 = ldg_v4_policy(a.col + jl + 4, pol_stream);
-        in.v0 = ldg_v4_policy(a.val + jl, pol_stream);
-        in.v1 = ldg_v4_policy(a.val + jl + 4, pol_stream);
+        if constexpr (reads_weight<SR>::value) {
+            in.v0 = ldg_v4_policy(a.val + jl, pol_stream);
+            in.v1 = ldg_v4_policy(a.val + jl + 4, pol_stream);
+        }
     } else {
         // a lane's 8 columns and values are 32 aligned bytes each (col and
         // val are 32-byte aligned; the host checks); read once, so they do
         // not displace the x lines the gathers reuse from L1
         ldg_v8_stream(a.col + jl, in.c0, in.c1);
-        ldg_v8_stream(a.val + jl, in.v0, in.v1);
+        if constexpr (reads_weight<SR>::value) ldg_v8_stream(a.val + jl, in.v0, in.v1);
     }
     in.sw = __ldg(a.plan.sbits + (j0 >> 5) + (lane >> 2));
     in.endw = __ldg(a.plan.sbits + ((j0 + kNnzTile) >> 5));
@@ -1268,9 +1272,10 @@ __device__ __forceinline__ void nnz_issue(const NnzArgs<SR>& a, uint32_t tile, u
                                           uint64_t* bar) {
     constexpr uint32_t kBytes = kNnzTile * 4;
     const size_t j0 = (size_t)tile * kNnzTile;
-    mbar_arrive_expect_tx(bar, (COL_ONLY ? 1 : 2) * kBytes);
+    constexpr bool kVal = !COL_ONLY && reads_weight<SR>::value;
+    mbar_arrive_expect_tx(bar, (kVal ? 2 : 1) * kBytes);
     bulk_g2s(st, a.col + j0, kBytes, bar);
-    if constexpr (!COL_ONLY) bulk_g2s(st + kBytes, a.val + j0, kBytes, bar);
+    if constexpr (kVal) bulk_g2s(st + kBytes, a.val + j0, kBytes, bar);
 }
 
 // Lanes 0-3 of a warp: L2 prefetch of tile `tile`'s col and val (1 KB each,
@@ -1281,7 +1286,7 @@ __device__ __forceinline__ void nnz_prefetch_l2(const NnzArgs<SR>& a, uint32_t t
     const uint32_t lane = lane_id();
     const size_t j0 = (size_t)tile * kNnzTile;
     if (lane == 0) prefetch_l2_bulk(a.col + j0, kNnzTile * 4);
-    else if (lane == 1) prefetch_l2_bulk(a.val + j0, kNnzTile * 4);
+    else if (lane == 1 && reads_weight<SR>::value) prefetch_l2_bulk(a.val + j0, kNnzTile * 4);
     else if (lane == 2) prefetch_l2(a.plan.sbits + (j0 >> 5));
     else if (lane == 3) prefetch_l2(a.plan.tile_seg + tile);
 }
@@ -1342,7 +1347,8 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
             in.sw = __ldg(a.plan.sbits + (j0 >> 5) + (lane >> 2));
             in.endw = __ldg(a.plan.sbits + ((j0 + kNnzTile) >> 5));
             in.seg0 = __ldg(a.plan.tile_seg + tile);
-            if constexpr (BULK == 2) {
+            in.v0 = in.v1 = make_uint4(0u, 0u, 0u, 0u);
+            if constexpr (BULK == 2 && reads_weight<SR>::value) {
                 in.v0 = __ldg(reinterpret_cast<const uint4*>(a.val + j0) + 2 * lane);
                 in.v1 = __ldg(reinterpret_cast<const uint4*>(a.val + j0) + 2 * lane + 1);
             }
@@ -1359,7 +1365,7 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
             }
             in.c0 = sc[0];
             in.c1 = sc[1];
-            if constexpr (BULK == 1) {
+            if constexpr (BULK == 1 && reads_weight<SR>::value) {
                 in.v0 = sv[0];
                 in.v1 = sv[1];
             }
@@ -1401,7 +1407,7 @@ spmv_nnz_kernel(NnzArgs<SR> a, Epi epi) {
                 // the next tile's 8 col and 8 val lines into L1 while this one runs
                 const uint32_t nt = tile + total_warps;
                 const uint32_t lane = lane_id();
-                if (nt < n_tiles && lane < 16) {
+                if (nt < n_tiles && lane < (reads_weight<SR>::value ? 16u : 8u)) {
                     const uint32_t jn = nt * kNnzTile + (lane & 7u) * 32u;
                     prefetch_l1(lane < 8 ? (const void*)(a.col + jn) : (const void*)(a.val + jn));
                 }
@@ -1506,9 +1512,9 @@ __device__ __forceinline__ Nnz2Ready<SR, Epi, IPT> nnz2_fetch(const NnzArgs<SR>&
     uint32_t cc[IPT];
 #pragma unroll
     for (int c = 0; c < IPT / 8; ++c) {
-        uint4 c0, c1, v0, v1;
+        uint4 c0, c1, v0 = make_uint4(0u, 0u, 0u, 0u), v1 = v0;
         ldg_v8_stream(a.col + jl + 8 * c, c0, c1);
-        ldg_v8_stream(a.val + jl + 8 * c, v0, v1);
+        if constexpr (reads_weight<SR>::value) ldg_v8_stream(a.val + jl + 8 * c, v0, v1);
         const uint32_t ci[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
         const uint32_t vi[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
 #pragma unroll

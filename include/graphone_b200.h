@@ -279,9 +279,13 @@ g1_status g1_sssp_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, uint32_t*
  * the indicator of src and `iters` times
  *     rank'[v] = sum_{u->v} rank[u] * alpha / outdeg(u)
  *                + [v == src] * ((1 - alpha) + alpha * sum_{outdeg(u)=0} rank[u]).
- * Transition weights are 1/out-degree (edge values are not used).  fp32,
- * bit-identical whether run alone, batched or served.  rank_out: n f32, host
- * or device.  Needs the in-edge CSR. */
+ * Transition weights are 1/out-degree (edge values are not used).  fp32.
+ * Runs on the SpMV schedules (one pass over the in-edge CSR per iteration,
+ * 4 bytes per edge); g1_ppr_batch runs the slot engine, whose per-slot
+ * results are the same bits wherever a query sits in a batch.  Both agree
+ * with an FP64 evaluation within 1e-6 relative L1; they are not bit-identical
+ * to each other (different summation orders).  rank_out: n f32, host or
+ * device.  Needs the in-edge CSR. */
 g1_status g1_ppr(g1_graph* g, uint32_t src, float alpha, uint32_t iters, float* rank_out,
                  void* stream);
 /* k personalized PageRanks, rank_out: k*n f32 source-major. */
@@ -291,17 +295,23 @@ g1_status g1_ppr_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, float alph
 /* --------------------------------------------------------- serving loop */
 /* A request loop (one host thread, one CUDA stream per graph and query
  * kind) over resident graphs.  Queries on the same graph and of the same
- * kind share a multi-source engine of up to max_batch slots (SSSP on graphs
- * of small uniform degree -- grids -- runs one query at a time on the
- * near-far engine instead); a query is
+ * kind share a multi-source engine of up to max_batch slots: a query is
  * admitted into a free slot between two iterations of the engine and its
  * result is written as soon as its own traversal completes, while the rest
- * of the batch keeps running (continuous batching).  Engines of different
- * graphs / kinds run concurrently on their own streams.  An engine's state
- * is allocated when its first query arrives, sized by the free device
- * memory (slots halve until it fits, down to 32; otherwise queries wait
- * for memory to be released), and released after idle_release_ms without
- * queries.  No GraphOne counterpart. */
+ * of the batch keeps running (continuous batching).  Batching pays only for
+ * dozens of queries at once, so while an executor's slots are empty and
+ * fewer than 32 queries wait (or the waiting ones would finish within
+ * solo_queue_ms one by one), its queries take the server's solo lane: one
+ * worker thread running queries one at a time, oldest first across graphs
+ * and kinds, on the single-source engines (the results of g1_sssp / g1_bfs
+ * with G1_ENGINE_AUTO and of g1_ppr).  SSSP and BFS on graphs of small
+ * uniform degree -- grids -- always take the lane (the near-far engine).  Executors of different graphs / kinds run
+ * concurrently on their own streams.  An engine's state is allocated when
+ * its first batch arrives, sized by the free device memory (slots halve
+ * until it fits, down to 32; otherwise queries wait for memory to be
+ * released), and kept until another engine needs the memory (or, with
+ * idle_release_ms set, released after that long without queries).  No
+ * GraphOne counterpart. */
 typedef struct g1_server g1_server;
 typedef enum { G1_QUERY_BFS = 0, G1_QUERY_SSSP = 1, G1_QUERY_PPR = 2 } g1_query_kind;
 typedef struct {
@@ -310,7 +320,13 @@ typedef struct {
     uint64_t memory_limit;    /* cap on engine state bytes; 0 = none */
     float ppr_alpha;          /* PPR damping; 0 = 0.85 */
     uint32_t ppr_iters;       /* PPR iterations; 0 = 20 */
-    uint32_t idle_release_ms; /* release idle engine state after this; 0 = 1000 */
+    uint32_t idle_release_ms; /* release idle engine state after this; 0 = keep it
+                                 until another engine needs the memory */
+    int32_t solo_queue_ms;    /* queries run one at a time on the single-source engines
+                                 while fewer than 32 wait or the waiting ones would
+                                 finish within this many ms that way (estimated),
+                                 batched beyond; 0 = 20; negative = always batched
+                                 (grid SSSP / BFS stay on the near-far engine) */
 } g1_server_config;
 typedef struct {
     uint64_t submitted, completed, failed;

@@ -3,8 +3,10 @@ loop (g1_ppr*, g1_server_*) against the oracle and against themselves:
 every query's result is the same alone, in a batch and in the served mix.
 
 Tolerances: BFS levels and SSSP distances bit-exact (u32); PPR within 1e-6
-relative L1 of the FP64 oracle, and bit-identical between the alone /
-batched / served runs (the per-slot arithmetic is fixed)."""
+relative L1 of the FP64 oracle on every path.  PPR results of one engine
+are bit-identical wherever the query runs: a slot engine query alone, in a
+batch or served on a small graph; g1_ppr (the SpMV schedules) alone or
+served solo on a graph of 2^22 edges or more."""
 import threading
 import time
 
@@ -28,14 +30,56 @@ def ppr_oracle(g, src, alpha=0.85, iters=20):
     return O.ppr_f64(trp, tci, np.ones(len(tci), np.float32), src, alpha, iters)
 
 
+@pytest.mark.parametrize("sched", [g1.SCHED_MERGE, g1.SCHED_VECTOR])
 @pytest.mark.parametrize("name", sorted(GRAPHS))
-def test_ppr_matches_fp64_oracle(cuda, name):
+def test_ppr_matches_fp64_oracle(cuda, name, sched):
     g = GRAPHS[name]
     G = g1.Graph.from_gen(g)
+    G.set_schedule(sched, g1.DEFAULT_MERGE_VARIANT)
     for src in sorted({0, g.n // 2, g.n - 1}):
         r = G.ppr(src, 0.85, 20)
         ref = ppr_oracle(g, src)
         assert O.rel_l1(r, ref) < PPR_TOL, (name, src)
+
+
+def small_directed():
+    """0->1->2->0 (a cycle), 3->0 (3 has no in-edges), 2->4 (4 has no
+    out-edges), 5 isolated, plus 6 with both a self loop and an edge to 4."""
+    src = torch.tensor([0, 1, 2, 3, 2, 6, 6])
+    dst = torch.tensor([1, 2, 0, 0, 4, 6, 4])
+    return gen.from_edges(src, dst, 7, False, (1, 9), name="small_directed")
+
+
+@pytest.mark.parametrize("sched", [g1.SCHED_MERGE, g1.SCHED_VECTOR])
+def test_ppr_sources_without_in_or_out_edges(cuda, sched):
+    """The source's own row empty (the nnz fixup emits it by itself before
+    the last iteration), a dangling source (its mass teleports back to it),
+    an isolated source (rank 1 at the source forever) and a self loop."""
+    g = small_directed()
+    G = g1.Graph.from_gen(g)
+    G.set_schedule(sched, g1.DEFAULT_MERGE_VARIANT)
+    for src in range(g.n):
+        for iters in (1, 2, 3, 20):
+            r = G.ppr(src, 0.85, iters)
+            ref = O.ppr_f64(*g.np("t")[:2], np.ones(g.m, np.float32), src, 0.85, iters)
+            assert O.rel_l1(r, ref) < PPR_TOL, (src, iters)
+    r = G.ppr(5, 0.85, 20)
+    assert r[5] == 1.0 and np.count_nonzero(r) == 1
+
+
+def test_ppr_directed_rmat_sources_with_empty_rows(cuda):
+    g = GRAPHS["rmat11_dir"]
+    G = g1.Graph.from_gen(g, relabel=True)
+    rp, _, _ = g.np("n")
+    trp, _, _ = g.np("t")
+    indeg, outdeg = np.diff(trp), np.diff(rp)
+    picks = [int(np.flatnonzero((indeg == 0) & (outdeg > 0))[0]),
+             int(np.flatnonzero((indeg > 0) & (outdeg == 0))[0]),
+             int(np.flatnonzero((indeg == 0) & (outdeg == 0))[0]),
+             int(np.argmax(indeg))]
+    for src in picks:
+        assert O.rel_l1(G.ppr(src, 0.85, 20), ppr_oracle(g, src)) < PPR_TOL, src
+        assert O.rel_l1(G.ppr(src, 0.5, 7), ppr_oracle(g, src, 0.5, 7)) < PPR_TOL, src
 
 
 def test_ppr_zero_iterations_is_the_indicator(cuda):
@@ -49,15 +93,16 @@ def test_ppr_zero_iterations_is_the_indicator(cuda):
 
 @pytest.mark.parametrize("name", ["rmat11_dir", "star20k", "grid32", "path3000"])
 @pytest.mark.parametrize("k", [1, 37, 300])
-def test_ppr_batch_bit_identical_to_single(cuda, name, k):
+def test_ppr_batch_bit_identical_wherever_a_query_sits(cuda, name, k):
     g = GRAPHS[name]
     G = g1.Graph.from_gen(g)
     rng = np.random.default_rng(k)
     srcs = rng.integers(0, g.n, size=k).astype(np.uint32)
     batch = G.ppr_batch(srcs, 0.85, 20)
     for i in sorted({0, k // 2, k - 1}):
-        one = G.ppr(int(srcs[i]), 0.85, 20)
+        one = G.ppr_batch(srcs[i:i + 1], 0.85, 20)[0]
         assert np.array_equal(batch[i], one), (name, k, i)
+        assert O.rel_l1(batch[i], G.ppr(int(srcs[i]), 0.85, 20)) < PPR_TOL
     assert O.rel_l1(batch[k - 1], ppr_oracle(g, int(srcs[k - 1]))) < PPR_TOL
 
 
@@ -102,11 +147,23 @@ def request_mix(graphs, count, seed):
 
 
 def alone(G, kind, src):
+    """The query run by itself on each engine the server may give it: the
+    single-source engine first, then a slot engine (PPR only; distances and
+    levels are the same on every engine)."""
     if kind == g1.QUERY_SSSP:
-        return G.sssp(src).view(np.uint32)
+        return [G.sssp(src).view(np.uint32)]
     if kind == g1.QUERY_BFS:
-        return G.bfs(src).view(np.uint32)
-    return G.ppr(src, 0.85, 20)
+        return [G.bfs(src).view(np.uint32)]
+    return [G.ppr(src, 0.85, 20), G.ppr_batch(np.array([src], np.uint32), 0.85, 20)[0]]
+
+
+def same_as_alone(res, G, kind, src, batched_only=False):
+    """Bit-identical to the query run alone on one of its engines (on the
+    slot engine when the server batches every query)."""
+    cands = alone(G, kind, src)
+    if batched_only:
+        cands = cands[-1:]
+    return any(np.array_equal(res.view(np.uint32), c.view(np.uint32)) for c in cands)
 
 
 def check_against_oracle(g, kind, src, res):
@@ -123,12 +180,15 @@ def host_out(g, kind):
     return np.empty(g.n, np.float32 if kind == g1.QUERY_PPR else np.uint32)
 
 
-@pytest.mark.parametrize("max_batch", [32, 256])
-def test_served_mix_equals_each_query_alone(cuda, max_batch):
+@pytest.mark.parametrize("max_batch,solo_queue_ms", [(32, -1), (256, -1), (256, 0), (64, 1000)])
+def test_served_mix_equals_each_query_alone(cuda, max_batch, solo_queue_ms):
+    """solo_queue_ms -1: SSSP / BFS always batched on the slot engines; 0:
+    the default hybrid (one at a time on the single-source engines while the
+    queue is short); 1000: mostly one at a time."""
     graphs = serving_graphs()
     Gs = [g1.Graph.from_gen(g) for g in graphs]
-    reqs = request_mix(graphs, 400, seed=max_batch)
-    with g1.Server(max_batch=max_batch) as srv:
+    reqs = request_mix(graphs, 400, seed=max_batch + solo_queue_ms)
+    with g1.Server(max_batch=max_batch, solo_queue_ms=solo_queue_ms) as srv:
         gids = [srv.add_graph(G) for G in Gs]
         outs = [host_out(graphs[gi], kind) for gi, kind, _ in reqs]
         # arrivals in waves, so later queries join batches already running
@@ -141,14 +201,36 @@ def test_served_mix_equals_each_query_alone(cuda, max_batch):
         st = srv.stats()
     assert st["completed"] == len(reqs) and st["failed"] == 0
     assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
-    assert st["max_occupancy"] > 1  # queries did share engine steps
+    if solo_queue_ms < 0:
+        assert st["max_occupancy"] > 1  # queries did share engine steps
     assert all(x > 0 for x in lat)
     for i, (gi, kind, src) in enumerate(reqs):
-        ref = alone(Gs[gi], kind, src)
-        assert np.array_equal(outs[i].view(np.uint32), ref.view(np.uint32)), (i, gi, kind, src)
+        assert same_as_alone(outs[i], Gs[gi], kind, src, solo_queue_ms < 0), (i, gi, kind, src)
     for i in range(0, len(reqs), 37):
         gi, kind, src = reqs[i]
         check_against_oracle(graphs[gi], kind, src, outs[i])
+
+
+def test_served_queries_run_solo_while_few_wait(cuda):
+    """A handful of PPR and SSSP queries on one graph are served one at a
+    time on the single-source engines: the same bits as g1_ppr / g1_sssp."""
+    g = gen.rmat(18, 16, True, (1, 100), device="cuda")
+    G = g1.Graph.from_gen(g, relabel=True)
+    srcs = [int(s) for s in gen.pick_sources(g, 6)]
+    with g1.Server() as srv:
+        gid = srv.add_graph(G)
+        pp = [np.empty(g.n, np.float32) for _ in srcs]
+        ss = [np.empty(g.n, np.uint32) for _ in srcs]
+        ts = []
+        for i, s in enumerate(srcs):
+            ts.append(srv.submit(gid, g1.QUERY_PPR, s, pp[i]))
+            ts.append(srv.submit(gid, g1.QUERY_SSSP, s, ss[i]))
+        for t in ts:
+            srv.wait(t, 120000)
+    for i, s in enumerate(srcs):
+        assert np.array_equal(pp[i], G.ppr(s, 0.85, 20)), i
+        assert np.array_equal(ss[i], G.sssp(s)), i
+    assert O.rel_l1(pp[0], ppr_oracle(g, srcs[0])) < PPR_TOL
 
 
 def test_served_device_and_pinned_outputs(cuda):
@@ -179,7 +261,7 @@ def test_admission_by_memory_limit(cuda):
     n_max = max(g.n for g in graphs)
     limit = 4 * n_max * 64 * 4  # room for engines of about 32-64 slots
     reqs = request_mix(graphs, 200, seed=7)
-    with g1.Server(max_batch=256, memory_limit=limit, idle_release_ms=1) as srv:
+    with g1.Server(max_batch=256, memory_limit=limit, idle_release_ms=1, solo_queue_ms=-1) as srv:
         gids = [srv.add_graph(G) for G in Gs]
         outs = [host_out(graphs[gi], kind) for gi, kind, _ in reqs]
         ts = [srv.submit(gids[gi], kind, src, outs[i]) for i, (gi, kind, src) in enumerate(reqs)]
@@ -189,7 +271,7 @@ def test_admission_by_memory_limit(cuda):
     assert st["completed"] == len(reqs)
     assert st["max_occupancy"] <= 64
     for i, (gi, kind, src) in enumerate(reqs):
-        assert np.array_equal(outs[i].view(np.uint32), alone(Gs[gi], kind, src).view(np.uint32))
+        assert same_as_alone(outs[i], Gs[gi], kind, src, batched_only=True), (i, gi, kind, src)
 
 
 def test_server_rejects_bad_requests(cuda):
