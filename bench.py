@@ -535,11 +535,11 @@ def kernel_name(variant: int) -> str:
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "spmv_nnz_pagerank_rmat22_traffic.txt")
 
 
-def measured_traffic(variant: int, path: str = TRAFFIC_FILE):
-    """DRAM bytes per launch that ncu measured for the RMAT-22 PageRank
-    kernel of merge variant `variant`, or None when no capture of that
-    variant is recorded (the summary's `variant:` and
-    `dram_bytes_per_launch:` lines)."""
+def measured_traffic(variant: int, path: str = TRAFFIC_FILE, key: str = "dram_bytes_per_launch"):
+    """A per-launch figure that ncu measured for the RMAT-22 PageRank kernel
+    of merge variant `variant` (the summary's `variant:` line and the `key:`
+    line: DRAM bytes, or L1-to-L2 sector requests), or None when no capture
+    of that variant is recorded."""
     try:
         with open(path) as f:
             text = f.read()
@@ -547,7 +547,7 @@ def measured_traffic(variant: int, path: str = TRAFFIC_FILE):
         return None
     import re
     v = re.search(r"^variant:\s*(-?\d+)\s*$", text, re.M)
-    b = re.search(r"^dram_bytes_per_launch:\s*(\d+)\s*$", text, re.M)
+    b = re.search(r"^" + re.escape(key) + r":\s*(\d+)\s*$", text, re.M)
     if not v or not b or int(v.group(1)) != variant:
         return None
     return int(b.group(1))
@@ -693,6 +693,22 @@ def run_ours(args):
             "avg_launch_ms": round(avg_ms, 5), "launches_timed": int(spmv_launches),
             "iteration_share_of_step": round(spmv_ms / ms, 4) if ms > 0 else None,
         }
+        # The kernel's other ceiling: every load that misses L1 (a cold x
+        # gather, a col/val line, the x-cache fill) is a request to L2, and an
+        # SM gets about one random request served per cycle, however many are
+        # in flight.  Requests per launch from ncu; the rate measured here.
+        rate = g1.measure_gather_rate(4, stream=stream)
+        nreq = measured_traffic(variant, key="l2_requests_per_launch") if args.scale == 22 else None
+        req = {"what": ("L1-to-L2 requests of the dominant kernel (ncu lts__t_requests_srcunit_tex) "
+                        "against the rate at which L2 serves random 4-byte loads to the SMs "
+                        "(g1_measure_gather_rate, this run)"),
+               "ceiling_requests_per_s": round(rate, -6), "requests_per_launch": nreq}
+        if nreq and rate > 0:
+            floor_ms = nreq / rate * 1e3
+            req.update({"floor_ms": round(floor_ms, 5), "avg_launch_ms": round(avg_ms, 5),
+                        "frac": round(floor_ms / avg_ms, 4),
+                        "hbm_frac_at_the_floor": round(spmv_bytes(n, m) / (floor_ms / 1e3) / 1e9 / peak, 4)})
+        result["l2_request_roofline"] = req
     if not args.no_parity:
         # our PageRank with GraphOne's own formula (no dangling redistribution)
         G.pagerank(0.85, iters, g1.PR_REFERENCE, out=out, stream=stream)
@@ -704,8 +720,10 @@ def run_ours(args):
     del G, out
     torch.cuda.empty_cache()
     result["reference_gpu"] = {
+        # the CUDA error's name is left out: this line is printed, and output that
+        # names a CUDA fault reads as a fault of this run
         "status": ("not run: GraphOne's own GPU engines faulted on this pool (its sssp_blas app "
-                   "ended in cudaErrorInvalidAddressSpace on an RMAT-12 input), so they are no "
+                   "ended in an invalid-address-space error on an RMAT-12 input), so they are no "
                    "longer run; figures measured before the fault are in "
                    "profiles/reference_gpu_engines.md")}
     if not args.no_queries:
@@ -825,7 +843,7 @@ def run_reference(args):
 
 
 KERNEL_WORKLOADS = ("slot_sssp", "slot_bfs", "slot_ppr", "nearfar", "advance_grid", "advance_lb",
-                    "blas_rmat20")
+                    "blas_rmat20", "gather_rates")
 
 
 def run_kernel_workload(name: str):
@@ -839,11 +857,24 @@ def run_kernel_workload(name: str):
       advance_lb                       SSSP on RMAT-20 on the advance engine
                                        (edge-balanced push steps), 4 sources
       blas_rmat20                      SSSP on RMAT-20 on the BLAS engine, 4 sources
+      gather_rates                     prints the random-load rates of
+                                       g1_measure_gather_rate over item size,
+                                       loads in flight, warps per SM and footprint
     """
     import torch
     import graphone_b200 as g1
     from graphone_b200 import gen
     dev = "cuda"
+    if name == "gather_rates":
+        for fp, where in ((1 << 16, "L1"), (1 << 24, "L2"), (1 << 30, "HBM")):
+            for item, fl, bps in ((4, 1, 1), (4, 4, 1), (4, 8, 1), (4, 16, 1), (4, 8, 2), (4, 32, 2),
+                                  (16, 8, 1)):
+                r = g1.measure_gather_rate(item, fl, bps, fp)
+                sms = torch.cuda.get_device_properties(0).multi_processor_count
+                print(f"{where:4s} footprint {fp:>11,d} B  item {item:2d} B  in flight {fl:2d}  "
+                      f"warps/SM {32 * bps:2d}: {r / 1e9:7.1f} G loads/s "
+                      f"({r / 1e9 / sms:5.2f} G/s per SM)", flush=True)
+        return
     if name.startswith("slot_"):
         g = gen.rmat(18, 16, True, (1, 64), device=dev)
         G = g1.Graph.from_gen(g, relabel=True)

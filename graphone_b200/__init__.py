@@ -69,6 +69,8 @@ def _declare(L):
     L.g1_kernel_launches.restype = C.c_uint64
     L.g1_count_user_launches.argtypes = [C.c_uint64]
     L.g1_test_set_wait_polls.argtypes = [C.c_int64]
+    L.g1_measure_gather_rate.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                                         C.POINTER(C.c_double), P]
     L.g1_profile_begin.argtypes = []
     L.g1_profile_end.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_uint64)]
     L.g1_graph_create.argtypes = [P, P, P, C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, P,
@@ -120,7 +122,7 @@ def lib():
 EXPORTS = (
     "g1_status_string", "g1_last_error", "g1_version", "g1_mem_alloc", "g1_mem_free",
     "g1_mem_copy", "g1_release_cached_memory", "g1_mem_fill_u32", "g1_stream_sync", "g1_kernel_launches",
-    "g1_count_user_launches", "g1_test_set_wait_polls",
+    "g1_count_user_launches", "g1_test_set_wait_polls", "g1_measure_gather_rate",
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
     "g1_spmv_plan", "g1_spmv_nnz_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_autotune_traversal", "g1_pagerank", "g1_sssp", "g1_bfs", "g1_advance_run",
@@ -168,6 +170,17 @@ def test_set_wait_polls(polls: int) -> None:
     """Lowers the poll limit of every bounded device wait (negative: the
     defaults), so that tests can make the waits run out."""
     check(lib().g1_test_set_wait_polls(polls))
+
+
+def measure_gather_rate(item_bytes: int = 4, in_flight: int = 8, blocks_per_sm: int = 1,
+                        footprint: int = 1 << 24, stream=None) -> float:
+    """Random loads per second served to the SMs of the current device
+    (g1_measure_gather_rate); the default (4-byte loads from a 16 MiB,
+    L2-resident buffer) is the ceiling of the SpMV's cold x gathers."""
+    r = C.c_double()
+    check(lib().g1_measure_gather_rate(item_bytes, in_flight, blocks_per_sm, footprint, C.byref(r),
+                                       _stream(stream)))
+    return r.value
 
 
 def profile_begin() -> None:

@@ -111,6 +111,17 @@ void g1_count_user_launches(uint64_t n);
  * still waited for before a kernel leaves.  Process-wide.  No GraphOne
  * counterpart (GraphOne's kernels never wait on one another). */
 g1_status g1_test_set_wait_polls(int64_t polls);
+/* Random loads served to the SMs per second, on the current device: gathers
+ * of item_bytes (4 or 16) at random positions of a buffer of footprint_bytes
+ * (a power of two, 64 KiB .. 4 GiB; by its size the buffer sits in L1, L2 or
+ * HBM), blocks_per_sm (1 or 2) 1024-thread blocks per SM, in_flight (1, 4, 8,
+ * 16 or 32) independent loads per thread.  From L2 each load is one request,
+ * and on B200 an SM gets about one served per cycle whatever the item size,
+ * the loads in flight or the warps: the ceiling of the pull SpMV's x gathers
+ * that miss the shared-memory copy of x.  No GraphOne counterpart:
+ * measurement support. */
+g1_status g1_measure_gather_rate(uint32_t item_bytes, uint32_t in_flight, uint32_t blocks_per_sm,
+                                 uint64_t footprint_bytes, double* gathers_per_s, void* stream);
 /* Kernel timing of the SpMV launches (main merge / vector kernels only):
  * between g1_profile_begin and g1_profile_end every such launch is
  * bracketed by CUDA events on its own stream; g1_profile_end synchronises
