@@ -506,8 +506,11 @@ def serving_metrics(dev, n_requests: int, rate: float, sweep=(0.25, 0.5, 0.9, 1.
         gb = [k for k, _ in SERVING_GRAPHS].index("rmat") + 2
         rng = np.random.default_rng(seed + 99)
         burst_reqs = [(0.0, gb, g1.QUERY_SSSP, int(cands[gb][rng.integers(0, len(cands[gb]))]))
-                      for _ in range(256)]
-        burst = run_point(srv, gids, burst_reqs, float("inf"))
+                      for _ in range(512)]
+        # the first burst allocates the executor's slot engine and captures
+        # its steps; the second is timed
+        run_point(srv, gids, burst_reqs[256:], float("inf"))
+        burst = run_point(srv, gids, burst_reqs[:256], float("inf"))
         burst["workload"] = ("256 SSSP queries on " + f"{SERVING_GRAPHS[gb][0]}{SERVING_GRAPHS[gb][1]}"
                              + " submitted at once")
         del burst["offered_rate_per_s"]

@@ -69,6 +69,7 @@ def _declare(L):
     L.g1_kernel_launches.restype = C.c_uint64
     L.g1_count_user_launches.argtypes = [C.c_uint64]
     L.g1_test_set_wait_polls.argtypes = [C.c_int64]
+    L.g1_set_traversal_thresholds.argtypes = [P, C.c_uint32, C.c_uint32]
     L.g1_measure_gather_rate.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                                          C.POINTER(C.c_double), P]
     L.g1_profile_begin.argtypes = []
@@ -125,7 +126,7 @@ EXPORTS = (
     "g1_count_user_launches", "g1_test_set_wait_polls", "g1_measure_gather_rate",
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
-    "g1_spmv_plan", "g1_spmv_nnz_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_autotune_traversal", "g1_pagerank", "g1_sssp", "g1_bfs", "g1_advance_run",
+    "g1_spmv_plan", "g1_spmv_nnz_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_autotune_traversal", "g1_set_traversal_thresholds", "g1_pagerank", "g1_sssp", "g1_bfs", "g1_advance_run",
     "g1_bfs_batch", "g1_sssp_batch", "g1_ppr", "g1_ppr_batch",
     "g1_server_create", "g1_server_add_graph", "g1_server_submit", "g1_server_poll",
     "g1_server_wait", "g1_server_stats", "g1_server_destroy",
@@ -280,6 +281,11 @@ class Graph:
         a, b, v = C.c_float(), C.c_float(), C.c_int()
         check(lib().g1_autotune(self._h, C.byref(a), C.byref(b), C.byref(v), _stream(stream)))
         return a.value, b.value, v.value
+
+    def set_traversal_thresholds(self, push_div=0, slot_div=0):
+        """Sets the push/pull divisors by hand (0 keeps one): see
+        g1_set_traversal_thresholds."""
+        check(lib().g1_set_traversal_thresholds(self._h, push_div, slot_div))
 
     def autotune_traversal(self, n_sources=16, stream=None):
         """(push_div, slot_div): the push/pull thresholds g1_autotune_traversal

@@ -222,6 +222,17 @@ extern "C" g1_status g1_autotune_traversal(g1_graph* g, uint32_t n_sources, uint
     return G1_OK;
 }
 
+extern "C" g1_status g1_set_traversal_thresholds(g1_graph* g, uint32_t push_div, uint32_t slot_div) {
+    if (!g) return fail(G1_ERR_INVALID, "g1_set_traversal_thresholds: null graph");
+    std::lock_guard<std::mutex> lk(g->mu);
+    if (push_div) g->push_div = push_div;
+    if (slot_div && slot_div != g->slot_div) {
+        g->slot_div = slot_div;
+        for (auto& e : g->slot_cache) e.reset();  // their captured steps hold the threshold
+    }
+    return G1_OK;
+}
+
 extern "C" g1_status g1_bfs_batch(g1_graph* g, const uint32_t* srcs, uint32_t k,
                                   uint32_t* levels_out, uint32_t* iters_out, void* stream) {
     return entry(g, kSlotBfs, srcs, k, levels_out, iters_out, 0.85f, 0, kMaxSlots, stream);

@@ -122,6 +122,7 @@ struct AdvGraphs {
     static constexpr int kModes = 4;  // {advance, BLAS pull} x {SSSP, BFS}
     cudaGraphExec_t exec[kModes][kSizes] = {};
     const void* key[kModes] = {};
+    unsigned long long param[kModes] = {};  // a launch argument the graphs hold (the sparse-pull limit)
     cudaStream_t capture = nullptr;
     AdvGraphs() = default;
     AdvGraphs(const AdvGraphs&) = delete;
@@ -133,6 +134,7 @@ struct AdvGraphs {
                 x = nullptr;
             }
         key[mode] = nullptr;
+        param[mode] = 0;
     }
     ~AdvGraphs() {
         for (int m = 0; m < kModes; ++m) reset(m);

@@ -314,15 +314,21 @@ __global__ void ag_init_kernel(uint32_t n, uint32_t src, const uint32_t* rp, AgS
 }
 
 // Last block of a step (every block calls this once, thread 0): zeroes c_in
-// (it is the next step's c_out) and advances the iteration count when the
-// step had a frontier.
-__device__ __forceinline__ void ag_last_block_rotate(AgCounter* c_in, uint32_t* ctl, uint32_t nF) {
+// (it is the next step's c_out) and `also` when given, and advances the
+// iteration count when the step had a frontier.
+__device__ __forceinline__ void ag_last_block_rotate(AgCounter* c_in, uint32_t* ctl, uint32_t nF,
+                                                     AgCounter* also = nullptr) {
     __threadfence();
     if (atomicAdd(&ctl[1], 1u) == gridDim.x - 1) {
         // every block has read c_in and published its appends
         if (nF) ctl[0] += 1u;
         c_in->n = 0u;
         c_in->deg = 0ull;
+        if (also) {
+            also->n = 0u;
+            also->pad = 0u;
+            also->deg = 0ull;
+        }
         ctl[1] = 0u;
         __threadfence();
     }
@@ -463,19 +469,167 @@ static g1_status advance_graph_traverse(g1_graph* g, uint32_t src, uint32_t* out
 // Per iteration the results are those of the reference loop, iteration
 // count included.
 
-// Store: the advance engine's (ag_layout), then x[n].
-inline size_t bg_words(uint32_t n) { return ag_words(n) + (size_t)n; }
+// Store: the advance engine's (ag_layout), then x[n], the sparse step's
+// listed rows cand[n], its counter (8 words: rows in n, heavy frontier
+// vertices in pad), row values res[n] and heavy frontier vertices heavy[n].
+inline size_t bg_words(uint32_t n) { return ag_words(n) + 4 * (size_t)n + 8; }
 
-__global__ void bg_x_init_kernel(uint32_t* x, uint32_t n) {
+struct BgSparse {
+    uint32_t* cand;
+    AgCounter* c_cand;
+    uint32_t* res;
+    uint32_t* heavy;
+};
+
+inline BgSparse bg_sparse_layout(uint32_t* store, uint32_t n) {
+    BgSparse b;
+    uint32_t* p = store + ag_words(n) + n;  // after x
+    b.cand = p;
+    b.c_cand = reinterpret_cast<AgCounter*>(p + n);  // 8-byte aligned: the store is, and 6n + 16 words precede
+    b.res = p + n + 8;
+    b.heavy = p + 2 * (size_t)n + 8;
+    return b;
+}
+
+// Frontier vertices with more out-edges than this are left to the whole grid
+// (bg_spmspv_heavy_kernel) instead of one warp.
+constexpr uint32_t kSparseHeavy = 2048;
+
+__global__ void bg_x_init_kernel(uint32_t* x, uint32_t n, BgSparse sp) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) x[v] = kU32Max;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+        x[v] = kU32Max;
+        sp.res[v] = kU32Max;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sp.c_cand->n = 0u;
+        sp.c_cand->pad = 0u;
+        sp.c_cand->deg = 0ull;
+    }
+}
+
+// Sparse step.  A row's min-plus value is the reduce of combine(w, x[u])
+// over its in-edges, and x is MAX (the identity of every combine) except on
+// the frontier, so only the frontier's out-edges contribute.  While they sum
+// below `limit` the step computes exactly those contributions -- each out-edge
+// (u -> v, w) of each frontier vertex u folds combine(w, x[u]) into res[v]
+// with atomicMin (min is order-free: the same value as the full pull's
+// row fold) -- and applies the rows it reached, as the full pull's epilogue
+// does.  Results and iteration counts are the full pull's; the work is the
+// frontier's out-edges instead of all m.
+constexpr uint32_t kSparseStepMinEdges = 1u << 20;
+
+__device__ __forceinline__ bool bg_sparse_step(const AgCounter* c_in, unsigned long long limit) {
+    return c_in->n != 0u && c_in->deg < limit;
+}
+
+// Folds out-edge k of a frontier vertex (value xu) into res[v]; a row is
+// listed by the edge that first lowers its value from MAX.
+template <class SR>
+__device__ __forceinline__ void bg_spmspv_edge(uint32_t k, uint32_t xu, const uint32_t* out_col,
+                                               const uint32_t* out_val, const BgSparse& sp, AgBlockQueue& bq) {
+    const uint32_t v = out_col[k];
+    const uint32_t c = SR::combine(reads_weight<SR>::value ? out_val[k] : 0u, xu);
+    if (c == kU32Max || c >= sp.res[v]) return;  // cheap pre-check; atomicMin decides
+    if (atomicMin(&sp.res[v], c) != kU32Max) return;  // listed already
+    const uint32_t p = atomicAdd(&bq.cnt, 1u);
+    if (p < (uint32_t)kAgQueue) bq.q[p] = v;
+    else sp.cand[atomicAdd(&sp.c_cand->n, 1u)] = v;  // queue full: straight out
+}
+
+// Publishes a block's listed rows (all threads of the block).
+__device__ __forceinline__ void bg_list_flush(AgBlockQueue& bq, const BgSparse& sp) {
+    __syncthreads();
+    const uint32_t cnt = min(bq.cnt, (uint32_t)kAgQueue);
+    if (threadIdx.x == 0) bq.base = cnt ? atomicAdd(&sp.c_cand->n, cnt) : 0u;
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < cnt; q += kAgBlock) sp.cand[bq.base + q] = bq.q[q];
+}
+
+// Sparse step, part 1: one warp per frontier vertex, lanes over its out-edges;
+// vertices of more than kSparseHeavy out-edges are listed for part 2.
+template <class SR>
+__global__ void __launch_bounds__(kAgBlock)
+bg_spmspv_kernel(const uint32_t* F_in, const AgCounter* c_in, unsigned long long limit, uint32_t n,
+                 const uint32_t* out_rp, const uint32_t* out_col, const uint32_t* out_val, const uint32_t* x,
+                 BgSparse sp, uint32_t* err) {
+    __shared__ AgBlockQueue bq;
+    if (!bg_sparse_step(c_in, limit)) return;  // the same for every block
+    const uint32_t nF = c_in->n;
+    if (threadIdx.x == 0) bq.cnt = 0u;
+    __syncthreads();
+    const uint32_t lane = lane_id();
+    const uint64_t warps = (uint64_t)gridDim.x * (kAgBlock / 32);
+    for (uint64_t i = ((uint64_t)blockIdx.x * kAgBlock + threadIdx.x) >> 5; i < nF; i += warps) {
+        const uint32_t u = F_in[i];
+        if (!frontier_vertex_ok(u, n, err)) continue;
+        const uint32_t b = out_rp[u], e = out_rp[u + 1];
+        if (e - b > kSparseHeavy) {
+            if (lane == 0) sp.heavy[atomicAdd(&sp.c_cand->pad, 1u)] = u;
+            continue;
+        }
+        const uint32_t xu = x[u];
+        for (uint32_t k = b + lane; k < e; k += 32) bg_spmspv_edge<SR>(k, xu, out_col, out_val, sp, bq);
+    }
+    bg_list_flush(bq, sp);
+}
+
+// Sparse step, part 2: the heavy frontier vertices' out-edges, spread over
+// the whole grid one vertex after another.
+template <class SR>
+__global__ void __launch_bounds__(kAgBlock)
+bg_spmspv_heavy_kernel(const AgCounter* c_in, unsigned long long limit, const uint32_t* out_rp,
+                       const uint32_t* out_col, const uint32_t* out_val, const uint32_t* x, BgSparse sp) {
+    __shared__ AgBlockQueue bq;
+    if (!bg_sparse_step(c_in, limit)) return;
+    const uint32_t nh = sp.c_cand->pad;
+    if (nh == 0) return;  // the same for every block
+    if (threadIdx.x == 0) bq.cnt = 0u;
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * kAgBlock;
+    for (uint32_t h = 0; h < nh; ++h) {
+        const uint32_t u = sp.heavy[h];
+        const uint32_t xu = x[u];
+        const uint32_t b = out_rp[u], e = out_rp[u + 1];
+        for (uint64_t k = b + (uint64_t)blockIdx.x * kAgBlock + threadIdx.x; k < e; k += stride)
+            bg_spmspv_edge<SR>((uint32_t)k, xu, out_col, out_val, sp, bq);
+    }
+    bg_list_flush(bq, sp);
+}
+
+// Sparse step, part 3: one thread per listed row applies its value as the
+// full pull's epilogue does (BgApplyEpilogue) and resets it to MAX.
+__global__ void __launch_bounds__(kAgBlock)
+bg_spmspv_apply_kernel(const AgCounter* c_in, unsigned long long limit, BgSparse sp, uint32_t* dist,
+                       uint32_t* F_out, AgCounter* c_out, const uint32_t* out_rp) {
+    __shared__ AgBlockQueue bq;
+    if (!bg_sparse_step(c_in, limit)) return;
+    const uint32_t nc = sp.c_cand->n;
+    if (threadIdx.x == 0) bq.cnt = 0u;
+    __syncthreads();
+    unsigned long long my_deg = 0ull;
+    const uint64_t stride = (uint64_t)gridDim.x * kAgBlock;
+    for (uint64_t i = (uint64_t)blockIdx.x * kAgBlock + threadIdx.x; i < nc; i += stride) {
+        const uint32_t v = sp.cand[i];
+        const uint32_t r = sp.res[v];
+        sp.res[v] = kU32Max;
+        if (r < dist[v]) {
+            dist[v] = r;
+            my_deg += out_rp[v + 1] - out_rp[v];
+            const uint32_t p = atomicAdd(&bq.cnt, 1u);
+            if (p < (uint32_t)kAgQueue) bq.q[p] = v;
+            else F_out[atomicAdd(&c_out->n, 1u)] = v;
+        }
+    }
+    ag_flush(bq, my_deg, F_out, c_out);
 }
 
 // x[f] = dist[f] (reset: MAX) over the frontier of c_in; with reset, the
-// last block also rotates the counters (ag_last_block_rotate).
+// last block also rotates the counters (ag_last_block_rotate) and zeroes
+// the sparse step's row count.
 __global__ void __launch_bounds__(kAgBlock)
 bg_frontier_x_kernel(const uint32_t* F_in, AgCounter* c_in, uint32_t* ctl, const uint32_t* dist,
-                     uint32_t* x, int reset) {
+                     uint32_t* x, int reset, AgCounter* c_cand) {
     const uint32_t nF = c_in->n;
     if (nF == 0) return;
     const uint64_t stride = (uint64_t)gridDim.x * kAgBlock;
@@ -483,7 +637,7 @@ bg_frontier_x_kernel(const uint32_t* F_in, AgCounter* c_in, uint32_t* ctl, const
         const uint32_t f = F_in[i];
         x[f] = reset ? kU32Max : dist[f];
     }
-    if (reset && threadIdx.x == 0) ag_last_block_rotate(c_in, ctl, nF);
+    if (reset && threadIdx.x == 0) ag_last_block_rotate(c_in, ctl, nF, c_cand);
 }
 
 // apply_each of the sssp_blas functor under the engine's guard, for the
@@ -496,7 +650,10 @@ struct BgApplyEpilogue {
     AgCounter* c_out;
     const AgCounter* c_in;
     const uint32_t* out_rp;  // out-edge offsets (for the degree sum)
-    __device__ __forceinline__ bool active() const { return c_in->n != 0u; }
+    unsigned long long sparse_limit;  // the sparse step runs instead below it
+    __device__ __forceinline__ bool active() const {
+        return c_in->n != 0u && !bg_sparse_step(c_in, sparse_limit);
+    }
     __device__ __forceinline__ void begin() {}
     __device__ __forceinline__ void emit(uint32_t v, const uint32_t& res) {
         if (res != kU32Max && res < dist[v]) {
@@ -521,18 +678,28 @@ static g1_status bg_prepare_spmv(g1_graph* g, int t) {
 }
 
 template <bool UNIT>
-static g1_status bg_enqueue_pairs(g1_graph* g, const AgState& a, uint32_t* x, const uint32_t* out_rp,
-                                  uint32_t pairs, uint32_t grid, cudaStream_t s) {
+static g1_status bg_enqueue_pairs(g1_graph* g, const AgState& a, uint32_t* x, const BgSparse& sp,
+                                  unsigned long long limit, const uint32_t* out_rp, uint32_t pairs,
+                                  uint32_t grid, cudaStream_t s) {
+    using SR = typename std::conditional<UNIT, BfsU32, MinPlusU32>::type;
     const int pull_t = 1;
     for (uint32_t p = 0; p < pairs; ++p)
         for (int h = 0; h < 2; ++h) {
-            bg_frontier_x_kernel<<<grid, kAgBlock, 0, s>>>(a.F[h], a.c[h], a.ctl, a.dist, x, 0);
-            BgApplyEpilogue e{a.dist, a.F[h ^ 1], a.c[h ^ 1], a.c[h], out_rp};
-            if (UNIT)
-                G1_TRY((run_spmv<BfsU32>(g, pull_t, G1_SCHED_AUTO, x, e, s)));
-            else
-                G1_TRY((run_spmv<MinPlusU32>(g, pull_t, G1_SCHED_AUTO, x, e, s)));
-            bg_frontier_x_kernel<<<grid, kAgBlock, 0, s>>>(a.F[h], a.c[h], a.ctl, a.dist, x, 1);
+            bg_frontier_x_kernel<<<grid, kAgBlock, 0, s>>>(a.F[h], a.c[h], a.ctl, a.dist, x, 0, sp.c_cand);
+            if (limit) {
+                const Orientation& o = g->o[0];
+                bg_spmspv_kernel<SR><<<grid, kAgBlock, 0, s>>>(a.F[h], a.c[h], limit, g->n, o.rp, o.col,
+                                                               static_cast<const uint32_t*>(o.val), x, sp,
+                                                               g->err_word);
+                bg_spmspv_heavy_kernel<SR><<<grid, kAgBlock, 0, s>>>(a.c[h], limit, o.rp, o.col,
+                                                                     static_cast<const uint32_t*>(o.val), x, sp);
+                bg_spmspv_apply_kernel<<<grid, kAgBlock, 0, s>>>(a.c[h], limit, sp, a.dist, a.F[h ^ 1], a.c[h ^ 1],
+                                                                 out_rp);
+                count_launches(3);
+            }
+            BgApplyEpilogue e{a.dist, a.F[h ^ 1], a.c[h ^ 1], a.c[h], out_rp, limit};
+            G1_TRY((run_spmv<SR>(g, pull_t, G1_SCHED_AUTO, x, e, s)));
+            bg_frontier_x_kernel<<<grid, kAgBlock, 0, s>>>(a.F[h], a.c[h], a.ctl, a.dist, x, 1, sp.c_cand);
             count_launches(2);
         }
     return G1_OK;
@@ -553,17 +720,27 @@ static g1_status blas_graph_traverse(g1_graph* g, uint32_t src, uint32_t* out, u
     G1_TRY(g->ws.get("bg_store", bg_words(n), &store));
     const AgState a = ag_layout(store, n);
     uint32_t* x = store + ag_words(n);
+    const BgSparse sp = bg_sparse_layout(store, n);
+    // sparse steps while the frontier's out-edges sum below m / push_div (the
+    // AUTO engine's push/pull switch); they need the out-edge CSR, and below
+    // kSparseStepMinEdges a full pull costs a few microseconds, no more than
+    // the sparse step's own two launches
+    const unsigned long long limit =
+        g->o[0].present && g->m >= kSparseStepMinEdges
+            ? (unsigned long long)g->m / std::max<uint32_t>(1, g->push_div)
+            : 0ull;
     G1_TRY(g->ws.pinned.ensure(64));
     uint32_t* host = g->ws.pinned.as<uint32_t>();
     if (!g->adv_graphs) g->adv_graphs.reset(new AdvGraphs());
     AdvGraphs& ag = *g->adv_graphs;
-    if (ag.key[mode] != store) ag.reset(mode);  // captured on another store
+    // captured on another store, or with another sparse-pull limit
+    if (ag.key[mode] != store || ag.param[mode] != limit) ag.reset(mode);
     if (!ag.capture) G1_CUDA(cudaStreamCreateWithFlags(&ag.capture, cudaStreamNonBlocking));
     const uint32_t grid = (uint32_t)std::max<uint64_t>(
         1, std::min<uint64_t>(ceil_div(n, kAgBlock), (uint64_t)g->sm_count * 4));
     const uint32_t gi = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div(n, 256), grid));
     ag_init_kernel<<<gi, 256, 0, s>>>(n, src, out_rp, a);
-    bg_x_init_kernel<<<gi, 256, 0, s>>>(x, n);
+    bg_x_init_kernel<<<gi, 256, 0, s>>>(x, n, sp);
     count_launches(2);
     G1_CUDA(cudaGetLastError());
     int i = 1;
@@ -573,7 +750,7 @@ static g1_status blas_graph_traverse(g1_graph* g, uint32_t src, uint32_t* out, u
             cudaGraph_t graph = nullptr;
             CaptureScope cs;
             G1_CUDA(cudaStreamBeginCapture(ag.capture, cudaStreamCaptureModeThreadLocal));
-            const g1_status st = bg_enqueue_pairs<UNIT>(g, a, x, out_rp, 1u << i, grid, ag.capture);
+            const g1_status st = bg_enqueue_pairs<UNIT>(g, a, x, sp, limit, out_rp, 1u << i, grid, ag.capture);
             const cudaError_t e = cudaStreamEndCapture(ag.capture, &graph);
             if (st != G1_OK) {
                 if (graph) cudaGraphDestroy(graph);
@@ -587,6 +764,7 @@ static g1_status blas_graph_traverse(g1_graph* g, uint32_t src, uint32_t* out, u
                 return fail_cuda(ei, "cudaGraphInstantiate(BLAS steps)");
             }
             ag.key[mode] = store;
+            ag.param[mode] = limit;
         }
         G1_CUDA(cudaGraphLaunch(gx, s));
         G1_CUDA(cudaMemcpyAsync(host, a.ctl, 16, cudaMemcpyDeviceToHost, s));

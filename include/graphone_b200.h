@@ -240,6 +240,13 @@ g1_status g1_autotune(g1_graph* g, float* merge_ms, float* vector_ms, int* merge
  * direction switch: AdvanceGC always pushes, BlasGcEngine always pulls). */
 g1_status g1_autotune_traversal(g1_graph* g, uint32_t n_sources, uint32_t* push_div,
                                 uint32_t* slot_div, void* stream);
+/* Sets those divisors by hand (0 keeps one).  push_div also sets where the
+ * G1_ENGINE_BLAS loop (on graphs of 2^20 edges or more with the out-edge
+ * CSR) computes a step from the frontier's out-edges alone instead of
+ * pulling every row: while the frontier's out-degree sum is below
+ * m / push_div.  Results and iteration counts never depend on them.  No
+ * GraphOne counterpart. */
+g1_status g1_set_traversal_thresholds(g1_graph* g, uint32_t push_div, uint32_t slot_div);
 
 /* ------------------------------------------------------------- algorithms */
 /* PageRank for a fixed iteration count (Run<PRFunctor> over

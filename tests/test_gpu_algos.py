@@ -26,14 +26,31 @@ def test_sssp_bit_exact(cuda, name, engine):
         assert np.array_equal(d, O.dijkstra_u32(rp, ci, v, s)), (name, s, engine)
 
 
-@pytest.mark.parametrize("name", ["rmat10_sym", "grid32", "path3000"])
-def test_sssp_blas_iterations_match_reference_engine(cuda, name):
-    g = GRAPHS[name]
+SPARSE_STEP_GRAPHS = {  # 2^20 edges or more: the BLAS engine's sparse steps apply
+    "rmat16_sym": lambda: gen.rmat(16, 16, True, (1, 64)),
+    "rmat17_dir": lambda: gen.rmat(17, 16, False, (1, 64)),
+}
+
+
+@pytest.mark.parametrize("push_div", [1, 16, 1 << 30])
+@pytest.mark.parametrize("name", ["rmat10_sym", "grid32", "path3000", "rmat16_sym", "rmat17_dir"])
+def test_sssp_blas_iterations_match_reference_engine(cuda, name, push_div):
+    """The BLAS engine's distances and iteration count are the reference
+    loop's whether its steps pull every row (push_div 2^30: never sparse) or
+    are computed from the frontier's out-edges (push_div 1: nearly always,
+    on the graphs of 2^20 edges or more)."""
+    g = GRAPHS[name] if name in GRAPHS else SPARSE_STEP_GRAPHS[name]()
+    if name in SPARSE_STEP_GRAPHS:
+        assert g.m >= 1 << 20
     G = g1.Graph.from_gen(g)
+    G.set_traversal_thresholds(push_div=push_div)
     trp, tci, tv = g.np("t")
-    d, it = G.sssp(0, g1.ENGINE_BLAS, return_iters=True)
-    d_o, it_o = O.sssp_blas_u32(trp, tci, tv, 0)
-    assert np.array_equal(d, d_o) and it == it_o
+    rp, ci, _ = g.np("n")
+    for s in sorted({0, g.n // 3, g.n - 1}):
+        d, it = G.sssp(s, g1.ENGINE_BLAS, return_iters=True)
+        d_o, it_o = O.sssp_blas_u32(trp, tci, tv, s)
+        assert np.array_equal(d, d_o) and it == it_o, (name, s)
+        assert np.array_equal(G.bfs(s, g1.ENGINE_BLAS), O.bfs(rp, ci, s)), (name, s)
 
 
 @pytest.mark.parametrize("engine", ENGINES)
