@@ -518,6 +518,7 @@ __global__ void bg_x_init_kernel(uint32_t* x, uint32_t n, BgSparse sp) {
 // does.  Results and iteration counts are the full pull's; the work is the
 // frontier's out-edges instead of all m.
 constexpr uint32_t kSparseStepMinEdges = 1u << 20;
+constexpr uint32_t kAutoDeviceEdges = 1u << 24;
 
 __device__ __forceinline__ bool bg_sparse_step(const AgCounter* c_in, unsigned long long limit) {
     return c_in->n != 0u && c_in->deg < limit;
@@ -815,7 +816,14 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
     if (!UNIT && g->vtype != G1_U32) return fail(G1_ERR_INVALID, "SSSP needs u32 edge weights");
     if (engine == G1_ENGINE_ADVANCE && advance_graph_suits(g))
         return advance_graph_traverse<UNIT>(g, src, out, iters_out, s);
-    if (engine == G1_ENGINE_BLAS) return blas_graph_traverse<UNIT>(g, src, out, iters_out, s);
+    // AUTO below kAutoDeviceEdges: the device-driven BLAS engine, whose sparse
+    // steps (from 2^20 edges) are the same push/pull switch with no host round
+    // trip per iteration, is the faster one there (SSSP p50, relabelled RMAT:
+    // 0.24 against 0.37 ms at scale 14, 0.57 against 0.66 ms at 18); above it
+    // the host-driven loop's edge-balanced push wins by a few percent (RMAT-20
+    // and -22).  Distances are the same on every engine.
+    if (engine == G1_ENGINE_BLAS || (engine == G1_ENGINE_AUTO && g->m < kAutoDeviceEdges))
+        return blas_graph_traverse<UNIT>(g, src, out, iters_out, s);
     Workspace& ws = g->ws;
     TrState st;
     G1_TRY(ws.get("tr_dist", n, &st.dist));

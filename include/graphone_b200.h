@@ -52,10 +52,13 @@ typedef enum {
 } g1_schedule;
 
 typedef enum {
-    G1_ENGINE_BLAS = 0,    /* pull SpMV per iteration (BlasGcEngine, sparse frontier) */
+    G1_ENGINE_BLAS = 0,    /* pull SpMV per iteration (BlasGcEngine, sparse frontier);
+                              from 2^20 edges, steps whose frontier is small are computed
+                              from the frontier's out-edges (same results) */
     G1_ENGINE_ADVANCE = 1, /* push advance/filter (AdvanceGC) */
-    G1_ENGINE_AUTO = 2,    /* near-far on graphs of small uniform degree, else push while
-                              the frontier is small and pull when it is large */
+    G1_ENGINE_AUTO = 2,    /* near-far on graphs of small uniform degree; else push while
+                              the frontier is small and pull when it is large (below 2^24
+                              edges: the BLAS engine with its sparse steps) */
     G1_ENGINE_NEARFAR = 3  /* distance-ordered near/far queues in one persistent launch
                               (no GraphOne counterpart; for high-diameter graphs) */
 } g1_engine;
