@@ -246,13 +246,15 @@ def query_metrics(dev, stream, parity, budget_queries: int = 256):
       (directed CSR edges of reachable vertices / median time), for the BLAS
       (min-plus SpMV), advance/filter and push/pull engines.
     * RMAT-20 (same shape) k=256 sources: plain engine queries/s over 64 of
-      the sources vs one batched k=256 pass.
+      the sources vs one batched k=256 pass; personalized PageRank (20
+      iterations) single-source over 16 sources vs one batched k=256 pass.
     * 4096^2 grid (uint32 weights [1,100]) SSSP and BFS from the corner on the
       near-far and advance engines (GTEPS = directed CSR edges / time).
 
     Parity (into `parity`): RMAT-14 SSSP from vertex 0 on every engine vs the
     oracle's Dijkstra; all 256 batched BFS/SSSP results vs 256 plain runs,
-    and 8 of each vs the oracle's BFS / Dijkstra; the grid's SSSP and BFS
+    and 8 of each vs the oracle's BFS / Dijkstra; two PPR sources, single and
+    batched, vs the oracle's FP64 PPR (relative L1); the grid's SSSP and BFS
     from the corner on both engines vs the oracle.
 
     """
@@ -336,6 +338,29 @@ def query_metrics(dev, stream, parity, budget_queries: int = 256):
                      "plain_p99_ms": round(_pct(lat, 99), 4),
                      "batched_queries_per_s": round(qb, 1), "batched_ms_per_256": round(tb, 3),
                      "batched_over_plain": round(qb / qp, 2)}
+    # personalized PageRank (20 iterations): single-source on the SpMV
+    # schedules, batched on the slot engine; both against the FP64 oracle
+    trp20, tci20, _ = g.np("t")
+    ones20 = np.ones(len(tci20), np.float32)
+    onef = torch.empty(g.n, dtype=torch.float32, device=dev)
+    blkf = torch.empty((256, g.n), dtype=torch.float32, device=dev)
+    G.ppr(int(srcs[0]), 0.85, 20, out=onef, stream=stream)
+    lat = [_event_ms(lambda s=s: G.ppr(int(s), 0.85, 20, out=onef, stream=stream), stream)
+           for s in srcs[:16]]
+    G.ppr_batch(srcs, 0.85, 20, out=blkf, stream=stream)
+    tb = _event_ms(lambda: G.ppr_batch(srcs, 0.85, 20, out=blkf, stream=stream), stream)
+    for i in (0, 255):
+        G.ppr(int(srcs[i]), 0.85, 20, out=onef, stream=stream)
+        torch.cuda.synchronize()
+        for tag, got in (("single", onef.cpu().numpy().copy()), ("batched", blkf[i].cpu().numpy().copy())):
+            parity.expect(f"ppr_rmat20_{tag}#{i}_rel_l1_vs_fp64", O.ppr_f64,
+                          (trp20, tci20, ones20, int(srcs[i]), 0.85, 20),
+                          lambda ref, got=got: float(O.rel_l1(got, ref)))
+    qs = 1e3 / statistics.mean(lat)
+    res["ppr"] = {"single_p50_ms": round(_pct(lat, 50), 4), "single_queries_per_s": round(qs, 1),
+                  "batched_ms_per_256": round(tb, 3), "batched_queries_per_s": round(256e3 / tb, 1),
+                  "batched_over_single": round(256e3 / tb / qs, 2)}
+    del blkf
     out["batch_rmat20_k256"] = res
     G.close()
     del g, G, one, blk
