@@ -116,6 +116,71 @@ inline unsigned grid_for(uint32_t n) {
     return std::max(1u, std::min<uint32_t>(want, (uint32_t)detail::sm_count() * 8));
 }
 
+// Sparse steps of the sparse-frontier engine (BlasGcEngine<SPARSE_BASED>).
+// Whether every edge's gather_combine with default_info gives default_result
+// and default_result folds into itself: then a row without an in-neighbour on
+// the frontier (x is default_info off the frontier) folds to default_result,
+// which apply never sees.  *bad is set when not.
+template <class F, class SR>
+__global__ void sparse_check_kernel(const typename SR::w_t* val, uint32_t m, uint32_t* bad) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += stride)
+        if (SR::combine(val[k], F::default_info()) != F::default_result()) atomicOr(bad, 1u);
+    if (blockIdx.x == 0 && threadIdx.x == 0 &&
+        SR::reduce(F::default_result(), F::default_result()) != F::default_result())
+        atomicOr(bad, 1u);
+}
+
+// The frontier's out-neighbours (the rows it reaches), each listed once
+// (its bit set first), and the sum of their in-degrees: cnt[0] rows,
+// cnt[2..3] the sum (64-bit).  One warp per frontier vertex.
+template <class V>
+__global__ void sparse_expand_kernel(const V* in, uint32_t n_in, const uint32_t* out_rp, const uint32_t* out_col,
+                                     const uint32_t* in_rp, uint32_t* bits, uint32_t* cand, uint32_t* cnt) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / 32;
+    unsigned long long* insum = reinterpret_cast<unsigned long long*>(cnt + 2);
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n_in; i += warps) {
+        const uint32_t u = (uint32_t)in[i];
+        for (uint32_t k = out_rp[u] + lane; k < out_rp[u + 1]; k += 32) {
+            const uint32_t v = out_col[k];
+            const uint32_t bit = 1u << (v & 31u);
+            if (atomicOr(&bits[v >> 5], bit) & bit) continue;  // listed already
+            cand[atomicAdd(&cnt[0], 1u)] = v;
+            atomicAdd(insum, (unsigned long long)(in_rp[v + 1] - in_rp[v]));
+        }
+    }
+}
+
+// The listed rows, one warp each: the row's fold over all its in-edges (the
+// functor's gather_combine / gather_reduce, as the full pull folds it), then
+// apply as SparseEpi does; the row's bit is cleared.
+template <class F, class SR, class D, class V>
+__global__ void sparse_rows_kernel(const uint32_t* cand, uint32_t nc, const uint32_t* in_rp, const uint32_t* in_col,
+                                   const typename SR::w_t* in_val, const typename SR::x_t* x, D ds, V* out,
+                                   uint32_t* count, uint32_t* bits) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / 32;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nc; i += warps) {
+        const uint32_t v = cand[i];
+        typename SR::value_t acc = SR::identity();
+        for (uint32_t k = in_rp[v] + lane; k < in_rp[v + 1]; k += 32)
+            acc = SR::reduce(acc, SR::combine(in_val[k], x[in_col[k]]));
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc = SR::reduce(acc, g1::shfl_down_any(0xffffffffu, acc, off));
+        if (lane == 0) {
+            atomicAnd(&bits[v >> 5], ~(1u << (v & 31u)));
+            if (acc != F::default_result() && F::apply_each(V(v), acc, ds)) g1::append(out, count, v);
+        }
+    }
+}
+
+// Clears the bits of the listed rows (when the step pulls every row after all).
+__global__ void sparse_clear_kernel(const uint32_t* cand, uint32_t nc, uint32_t* bits) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nc; i += gridDim.x * blockDim.x)
+        atomicAnd(&bits[cand[i] >> 5], ~(1u << (cand[i] & 31u)));
+}
+
 }  // namespace blas_detail
 
 template <typename functor_t, typename comp_t, typename frontier_t>
@@ -298,6 +363,7 @@ class BlasGcEngine<functor_t, comp_t, frontier_t,
 public:
     BlasGcEngine(comp_t& comp, frontier_t& frontier) : B(comp, frontier) {
         this->fill_x(0, functor_t::default_info());
+        init_sparse(comp);
     }
 
     void Forward() override {
@@ -312,8 +378,9 @@ public:
                 <<<blas_detail::grid_for(n_in), 256, 0, this->stream_>>>(f.input().data(), n_in, ds, x);
         f.reserve_output(this->n_);
         this->counters_.clear(this->stream_);
-        this->spmv(x, blas_detail::SparseEpi<functor_t, D, V>{ds, f.output().data(),
-                                                              this->counters_.dev});
+        if (!sparse_step(f, n_in, x, ds))
+            this->spmv(x, blas_detail::SparseEpi<functor_t, D, V>{ds, f.output().data(),
+                                                                  this->counters_.dev});
         if (n_in)
             blas_detail::set_list_kernel<<<blas_detail::grid_for(n_in), 256, 0, this->stream_>>>(
                 f.input().data(), n_in, functor_t::default_info(), x);
@@ -321,6 +388,78 @@ public:
         this->counters_.read(this->stream_);
         f.reset_output(this->counters_.count());
     }
+
+private:
+    // Sparse steps.  GraphOne pulls every row each iteration
+    // (engine/blas_gc.h:199-245).  When a row without an in-neighbour on the
+    // frontier folds to default_result (checked once on the device over the
+    // graph's edge values, sparse_check_kernel), only the rows the frontier
+    // reaches can be applied, so a step with a small frontier lists the
+    // frontier's out-neighbours and folds just those rows, each over all its
+    // in-edges as the full pull does: the same rows applied with the same
+    // values.  Used on graphs of 2^20 edges or more (a full pull of a smaller
+    // one costs a few microseconds) with both orientations, while the listed
+    // rows hold fewer than m / 16 in-edges.
+    static constexpr uint32_t kSparseMinEdges = 1u << 20;
+    static constexpr uint32_t kSparseDiv = 16;
+
+    void init_sparse(comp_t& comp) {
+        const uint32_t m = this->args_.plan.nnz;
+        if (this->side_ != 1 || m < kSparseMinEdges) return;
+        const uint32_t* orp = nullptr;
+        const uint32_t* oci = nullptr;
+        const void* oval = nullptr;
+        if (g1_graph_arrays(comp.graph.handle(), 0, &orp, &oci, &oval) != G1_OK || !orp) return;
+        uint32_t* bad = this->counters_.dev + 15;
+        detail::check_cuda(cudaMemsetAsync(bad, 0, 4, this->stream_), "sparse check");
+        blas_detail::sparse_check_kernel<functor_t, typename B::SR>
+            <<<blas_detail::grid_for(m), 256, 0, this->stream_>>>(this->args_.val, m, bad);
+        g1_count_user_launches(1);
+        this->counters_.read_set(this->stream_, 1);
+        if (this->counters_.host[7] != 0u) return;
+        out_rp_ = orp;
+        out_col_ = oci;
+        bits_ = DenseVec<arch_t::cuda, uint32_t>((this->n_ + 31) / 32 + 1);
+        cand_ = DenseVec<arch_t::cuda, uint32_t>(std::max<typename B::vertex_t>(this->n_, 1));
+        blas_detail::fill_kernel<<<blas_detail::grid_for((this->n_ + 31) / 32 + 1), 256, 0, this->stream_>>>(
+            bits_.data(), (uint32_t)((this->n_ + 31) / 32 + 1), 0u);
+        g1_count_user_launches(1);
+    }
+
+    template <class D>
+    bool sparse_step(frontier_t& f, uint32_t n_in, const typename B::info_t* x, const D& ds) {
+        using V = typename B::vertex_t;
+        if (!out_rp_ || n_in == 0 || n_in > this->n_ / 32) return false;
+        const uint32_t m = this->args_.plan.nnz;
+        uint32_t* cnt = this->counters_.dev + 8;
+        detail::check_cuda(cudaMemsetAsync(cnt, 0, 16, this->stream_), "sparse counters");
+        blas_detail::sparse_expand_kernel<V><<<blas_detail::grid_for(n_in * 32), 256, 0, this->stream_>>>(
+            f.input().data(), n_in, out_rp_, out_col_, this->args_.plan.row_ptr, bits_.data(), cand_.data(), cnt);
+        g1_count_user_launches(1);
+        this->counters_.read_set(this->stream_, 1);
+        const uint32_t nc = this->counters_.host[0];
+        const unsigned long long insum =
+            (unsigned long long)this->counters_.host[2] | ((unsigned long long)this->counters_.host[3] << 32);
+        if (insum >= m / kSparseDiv) {
+            blas_detail::sparse_clear_kernel<<<blas_detail::grid_for(nc), 256, 0, this->stream_>>>(
+                cand_.data(), nc, bits_.data());
+            g1_count_user_launches(1);
+            return false;
+        }
+        if (nc) {
+            blas_detail::sparse_rows_kernel<functor_t, typename B::SR, D, V>
+                <<<blas_detail::grid_for(nc * 32), 256, 0, this->stream_>>>(
+                    cand_.data(), nc, this->args_.plan.row_ptr, this->args_.col, this->args_.val, x, ds,
+                    f.output().data(), this->counters_.dev, bits_.data());
+            g1_count_user_launches(1);
+        }
+        return true;
+    }
+
+    const uint32_t* out_rp_ = nullptr;
+    const uint32_t* out_col_ = nullptr;
+    DenseVec<arch_t::cuda, uint32_t> bits_;
+    DenseVec<arch_t::cuda, uint32_t> cand_;
 };
 
 // Dense frontier: counts only (GraphOne: engine/blas_gc.h:250-351).

@@ -33,6 +33,9 @@ def sssp_expected(g, src, n_out):
 GRAPHS = {
     "rmat11": lambda: gen.rmat(11, 8, True, (1, 64)),
     "grid48": lambda: gen.grid2d(48, 48, (1, 100)),
+    # 2^20 edges or more: sssp_blas's engine takes its sparse steps (small
+    # frontiers fold only the rows they reach)
+    "rmat17": lambda: gen.rmat(17, 8, True, (1, 64)),
 }
 
 
