@@ -246,8 +246,11 @@ def query_metrics(dev, stream, parity, budget_queries: int = 256):
       (directed CSR edges of reachable vertices / median time), for the BLAS
       (min-plus SpMV), advance/filter and push/pull engines.
     * RMAT-20 (same shape) k=256 sources: plain engine queries/s over 64 of
-      the sources vs one batched k=256 pass; personalized PageRank (20
-      iterations) single-source over 16 sources vs one batched k=256 pass.
+      the sources vs one batched k=256 pass, with the batch's iterations,
+      GTEPS (edges of the reached vertices over all sources / time) and the
+      k-source SpMM-equivalent bytes 4(N+1) + 8M + 2*4*N*k + 2*N*k/8 per
+      iteration as GB/s; personalized PageRank (20 iterations) single-source
+      over 16 sources vs one batched k=256 pass.
     * 4096^2 grid (uint32 weights [1,100]) SSSP and BFS from the corner on the
       near-far and advance engines (GTEPS = directed CSR edges / time).
 
@@ -308,6 +311,7 @@ def query_metrics(dev, stream, parity, budget_queries: int = 256):
     res["autotuned"] = {"push_while_frontier_out_edges_below": f"m/{push_div}",
                         "sparse_slot_iterations_while_changed_out_edges_below": f"(m+n)/{slot_div}"}
     n_oracle = 8
+    deg20 = torch.from_numpy(np.diff(rp20.astype(np.int64)).astype(np.float32)).to(dev)
     for kind in ("bfs", "sssp"):
         single = G.bfs if kind == "bfs" else G.sssp
         batch = G.bfs_batch if kind == "bfs" else G.sssp_batch
@@ -315,7 +319,7 @@ def query_metrics(dev, stream, parity, budget_queries: int = 256):
         nq = 64
         lat = [_event_ms(lambda s=s: single(int(s), out=one, stream=stream), stream)
                for s in srcs[:nq]]
-        batch(srcs, out=blk, stream=stream)
+        _, b_iters = batch(srcs, out=blk, stream=stream, return_iters=True)
         tb = _event_ms(lambda: batch(srcs, out=blk, stream=stream), stream)
         # every batched result against its plain single-source run
         same = 0
@@ -334,10 +338,22 @@ def query_metrics(dev, stream, parity, budget_queries: int = 256):
                           lambda ref, got=got: bool(np.array_equal(got, ref)))
         qp = 1e3 / statistics.mean(lat)
         qb = 256 * 1e3 / tb
+        # edges of the reached vertices, summed over the 256 sources (GTEPS),
+        # and the batched k-source SpMM's bytes per iteration:
+        # 4(N+1) + 8M + 2*4*N*k (X and Y blocks) + 2*N*k/8 (bitmaps)
+        reach = sum(float(((blk[c:c + 32] != -1).to(torch.float32) @ deg20).sum().item())
+                    for c in range(0, 256, 32))
+        nk = g.n * 256
+        spmm_bytes = 4 * (g.n + 1) + 8 * g.m + 8 * nk + nk // 4
         res[kind] = {"plain_queries_per_s": round(qp, 1), "plain_p50_ms": round(_pct(lat, 50), 4),
                      "plain_p99_ms": round(_pct(lat, 99), 4),
                      "batched_queries_per_s": round(qb, 1), "batched_ms_per_256": round(tb, 3),
-                     "batched_over_plain": round(qb / qp, 2)}
+                     "batched_over_plain": round(qb / qp, 2),
+                     "batched_iterations": int(b_iters),
+                     "batched_gteps": round(reach / (tb / 1e3) / 1e9, 2),
+                     "spmm_bytes_per_iteration": spmm_bytes,
+                     "spmm_equivalent_gbs": round(spmm_bytes * b_iters / (tb / 1e3) / 1e9, 1),
+                     "gather_bytes_bound_per_iteration": 4 * 256 * g.m}
     # personalized PageRank (20 iterations): single-source on the SpMV
     # schedules, batched on the slot engine; both against the FP64 oracle
     trp20, tci20, _ = g.np("t")
