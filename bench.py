@@ -822,6 +822,10 @@ def cpu_baseline(trp, tci, tv, n, m, args, budget_s=20.0):
         dt = time.perf_counter() - t0
         sample = (f"{k} PageRank iterations (SpMV_cpu_navie + restated apply/construct) "
                   f"on the full graph, {threads} threads")
+        # the same code on one thread, one iteration
+        t0 = time.perf_counter()
+        R.ref_pagerank_f32(n, p(trp), p(tci), p(tv), p(outw), C.c_float(0.85), 1, 1, p(rank), 1)
+        single = spmv_bytes(n, m) / (time.perf_counter() - t0) / 1e9
     else:
         kind = "port"
         threads = 1
@@ -832,8 +836,11 @@ def cpu_baseline(trp, tci, tv, n, m, args, budget_s=20.0):
         k = 1
         sample = "1 SpMV of the C oracle (single thread) on the full graph"
     gbs = spmv_bytes(n, m) * k / dt / 1e9
-    return {"value": round(gbs, 2), "unit": "GB/s", "cores": threads, "kind": kind,
-            "sample": sample, "seconds": round(dt, 2)}
+    out = {"value": round(gbs, 2), "unit": "GB/s", "cores": threads, "kind": kind,
+           "sample": sample, "seconds": round(dt, 2)}
+    if R is not None:
+        out["single_thread_value"] = round(single, 2)
+    return out
 
 
 def run_reference(args):

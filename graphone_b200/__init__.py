@@ -364,7 +364,7 @@ class ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_uint32), ("reserve_bytes", C.c_uint64),
                 ("memory_limit", C.c_uint64), ("ppr_alpha", C.c_float),
                 ("ppr_iters", C.c_uint32), ("idle_release_ms", C.c_uint32),
-                ("solo_queue_ms", C.c_int32)]
+                ("solo_queue_ms", C.c_int32), ("solo_lanes", C.c_uint32)]
 
 
 class ServerStats(C.Structure):
@@ -385,9 +385,9 @@ class Server:
     """
 
     def __init__(self, device=0, max_batch=0, reserve_bytes=0, memory_limit=0,
-                 ppr_alpha=0.0, ppr_iters=0, idle_release_ms=0, solo_queue_ms=0):
+                 ppr_alpha=0.0, ppr_iters=0, idle_release_ms=0, solo_queue_ms=0, solo_lanes=0):
         cfg = ServerConfig(max_batch, reserve_bytes, memory_limit, ppr_alpha, ppr_iters,
-                           idle_release_ms, solo_queue_ms)
+                           idle_release_ms, solo_queue_ms, solo_lanes)
         h = C.c_void_p()
         check(lib().g1_server_create(device, C.byref(cfg), C.byref(h)))
         self._h = h.value

@@ -19,17 +19,18 @@
 // Batches pay only when many queries share a step: a step of one 32-slot
 // word costs about what a full word's does, and up to a few dozen queries
 // the single-source engines finish them sooner one by one.  So the server
-// also has a solo lane: one worker thread that runs queries one at a time,
-// oldest first across executors, on the single-source engines (the calls a
-// plain per-request user makes: traverse.cu's AUTO engine, which picks the
-// near-far engine on grids, and pagerank.cu's SpMV PPR), on its own stream.
-//   - SSSP and BFS on graphs of small uniform degree (grids) always take
-//     the lane: batched Bellman-Ford relaxes such graphs' vertices many
-//     times over, and batched BFS steps through thousands of levels;
+// also has solo lanes: worker threads that each run one query at a time,
+// oldest first across executors and never two of one graph at once, on the
+// single-source engines (the calls a plain per-request user makes:
+// traverse.cu's AUTO engine, which picks the near-far engine on grids, and
+// pagerank.cu's SpMV PPR), each on its own stream.
+//   - SSSP and BFS on graphs of small uniform degree (grids) always take a
+//     lane: batched Bellman-Ford relaxes such graphs' vertices many times
+//     over, and batched BFS steps through thousands of levels;
 //   - the other executors are hybrid: with their slots empty and fewer than
 //     a word of queries waiting (or a queue that one-by-one runs clear
-//     within solo_queue_ms) their queries take the lane; beyond that they
-//     are batched on the slot engine, concurrently with the lane.
+//     within solo_queue_ms) their queries take the lanes; beyond that they
+//     are batched on the slot engine, concurrently with the lanes.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -86,7 +87,7 @@ struct Exec {
     DevBuf staging;                  // pageable outputs
     // Where the executor's queries run (init_exec):
     //  - lane_only: SSSP and BFS on graphs of small uniform degree (grids)
-    //    always run one at a time on the server's solo lane, where the AUTO
+    //    always run one at a time on the server's solo lanes, where the AUTO
     //    engine picks the near-far engine (batched Bellman-Ford relaxes such
     //    graphs' vertices many times over; batched BFS steps through
     //    thousands of levels);
@@ -99,7 +100,7 @@ struct Exec {
     //    the out-edge CSR the AUTO engine pushes over).
     bool lane_only = false;
     bool hybrid = false;
-    std::atomic<bool> on_lane{false};  // one of its queries runs on the lane
+    std::atomic<bool> on_lane{false};  // one of its queries runs on a lane
     std::atomic<double> solo_ms{0.0};  // moving average of its lane query time
 };
 
@@ -110,6 +111,22 @@ struct Exec {
 // single-source runs beat.
 constexpr double kSoloQueueMs = 20.0;
 constexpr size_t kSlotMinQueue = 32;
+// One lane by default: with two, the concurrent queries slowed each other
+// (p99 of the bench's mixed stream 1-10% above one lane's at every load; the
+// near-far kernel, a cooperative launch over every SM, waits for the other
+// lane's kernels to drain).
+constexpr uint32_t kDefaultLanes = 1;
+
+struct Lane {
+    std::thread th;
+    std::mutex mu;  // req, exec, stop
+    std::condition_variable cv;
+    Request* req = nullptr;
+    Exec* exec = nullptr;
+    bool stop = false;
+    std::atomic<bool> busy{false};
+    std::atomic<const g1_graph*> graph{nullptr};  // the graph of its query, while busy
+};
 
 }  // namespace
 }  // namespace g1
@@ -141,16 +158,10 @@ struct g1_server {
     std::atomic<uint32_t> engines{0};
     std::mutex graphs_mu;  // add_graph vs the loop's view of execs
     std::atomic<size_t> n_execs{0};
-    // The solo lane: one worker thread running queries one at a time on the
-    // single-source engines, oldest first across executors (the order and
-    // engines of plain per-request calls).
-    std::thread lane;
-    std::mutex lane_mu;  // lane_req, lane_exec, lane_stop
-    std::condition_variable lane_cv;
-    Request* lane_req = nullptr;
-    Exec* lane_exec = nullptr;
-    bool lane_stop = false;
-    std::atomic<bool> lane_busy{false};
+    // The solo lanes: worker threads each running one query at a time on
+    // the single-source engines, oldest first across executors (the order
+    // and engines of plain per-request calls), never two of one graph.
+    std::vector<std::unique_ptr<g1::Lane>> lanes;
 };
 
 namespace g1 {
@@ -311,10 +322,10 @@ g1_status retire(g1_server* S, Exec& E, const std::vector<uint32_t>& fin) {
     return G1_OK;
 }
 
-// The solo lane's thread: runs the query handed to it on the single-source
+// A solo lane's thread: runs the query handed to it on the single-source
 // engines (the calls of g1_sssp / g1_bfs with G1_ENGINE_AUTO and of g1_ppr),
 // on its own stream, then completes it.
-void lane_worker(g1_server* S) {
+void lane_worker(g1_server* S, Lane* L) {
     pthread_setname_np(pthread_self(), "g1-lane");
     cudaSetDevice(S->device);
     cudaStream_t ls = nullptr;
@@ -324,11 +335,11 @@ void lane_worker(g1_server* S) {
         Request* r = nullptr;
         Exec* E = nullptr;
         {
-            std::unique_lock<std::mutex> lk(S->lane_mu);
-            S->lane_cv.wait(lk, [&] { return S->lane_req != nullptr || S->lane_stop; });
-            if (!S->lane_req) break;
-            r = S->lane_req;
-            E = S->lane_exec;
+            std::unique_lock<std::mutex> lk(L->mu);
+            L->cv.wait(lk, [&] { return L->req != nullptr || L->stop; });
+            if (!L->req) break;
+            r = L->req;
+            E = L->exec;
         }
         g1_status st = G1_ERR_DEVICE;
         const auto t0 = Clock::now();
@@ -345,14 +356,21 @@ void lane_worker(g1_server* S) {
         E->solo_ms.store(prev == 0.0 ? ms : 0.75 * prev + 0.25 * ms);
         complete_one(S, r, st);
         {
-            std::lock_guard<std::mutex> lk(S->lane_mu);
-            S->lane_req = nullptr;
-            S->lane_exec = nullptr;
+            std::lock_guard<std::mutex> lk(L->mu);
+            L->req = nullptr;
+            L->exec = nullptr;
         }
         E->on_lane.store(false);
-        S->lane_busy.store(false);
+        L->graph.store(nullptr);
+        L->busy.store(false);
     }
     if (have_stream) cudaStreamDestroy(ls);
+}
+
+bool lanes_busy(const g1_server* S) {
+    for (const auto& L : S->lanes)
+        if (L->busy.load()) return true;
+    return false;
 }
 
 // Whether the executor's waiting queries go to the solo lane: always for
@@ -367,36 +385,47 @@ bool lane_mode(const g1_server* S, const Exec& E) {
              (double)E.pending.size() * solo > S->solo_queue_ms);
 }
 
-// Hands the oldest waiting query of the executors in lane mode to the lane
-// when it is free.
-bool dispatch_lane(g1_server* S, bool stopping) {
-    if (stopping || S->lane_busy.load()) return false;
-    Exec* best = nullptr;
-    const size_t ne = S->n_execs.load();
-    for (size_t i = 0; i < ne; ++i) {
-        Exec& E = *S->execs[i];
-        if (E.pending.empty() || !lane_mode(S, E)) continue;
-        if (!best || E.pending.front()->t_sub < best->pending.front()->t_sub) best = &E;
+// Hands each free lane the oldest waiting query of the executors in lane
+// mode whose graph no other lane is working on (the calls of one graph
+// would only wait for each other's lock).
+bool dispatch_lanes(g1_server* S, bool stopping) {
+    if (stopping) return false;
+    bool any = false;
+    for (auto& Lp : S->lanes) {
+        Lane* L = Lp.get();
+        if (L->busy.load()) continue;
+        Exec* best = nullptr;
+        const size_t ne = S->n_execs.load();
+        for (size_t i = 0; i < ne; ++i) {
+            Exec& E = *S->execs[i];
+            if (E.pending.empty() || !lane_mode(S, E)) continue;
+            bool graph_busy = false;
+            for (const auto& O : S->lanes) graph_busy |= O->busy.load() && O->graph.load() == E.g;
+            if (graph_busy) continue;
+            if (!best || E.pending.front()->t_sub < best->pending.front()->t_sub) best = &E;
+        }
+        if (!best) break;  // no other lane would find one either
+        Request* r = best->pending.front();
+        best->pending.pop_front();
+        best->on_lane.store(true);
+        L->graph.store(best->g);
+        L->busy.store(true);
+        {
+            std::lock_guard<std::mutex> lk(L->mu);
+            L->req = r;
+            L->exec = best;
+        }
+        if (!L->th.joinable()) L->th = std::thread(lane_worker, S, L);
+        L->cv.notify_one();
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            ++S->steps;
+            S->max_occ = std::max(S->max_occ, 1u);
+        }
+        best->last_busy = Clock::now();
+        any = true;
     }
-    if (!best) return false;
-    Request* r = best->pending.front();
-    best->pending.pop_front();
-    best->on_lane.store(true);
-    S->lane_busy.store(true);
-    {
-        std::lock_guard<std::mutex> lk(S->lane_mu);
-        S->lane_req = r;
-        S->lane_exec = best;
-    }
-    if (!S->lane.joinable()) S->lane = std::thread(lane_worker, S);
-    S->lane_cv.notify_one();
-    {
-        std::lock_guard<std::mutex> lk(S->mu);
-        ++S->steps;
-        S->max_occ = std::max(S->max_occ, 1u);
-    }
-    best->last_busy = Clock::now();
-    return true;
+    return any;
 }
 
 // One turn of one executor; true if anything happened.
@@ -521,9 +550,9 @@ void loop(g1_server* S) {
         }
         bool progress = false;
         for (size_t i = 0; i < ne; ++i) progress |= service(S, *S->execs[i], stopping, fin);
-        progress |= dispatch_lane(S, stopping);
+        progress |= dispatch_lanes(S, stopping);
         const auto now = Clock::now();
-        bool still = S->lane_busy.load();
+        bool still = lanes_busy(S);
         for (size_t i = 0; i < ne; ++i) {
             Exec& E = *S->execs[i];
             still |= busy(E) || !E.retiring.empty();
@@ -565,9 +594,12 @@ extern "C" g1_status g1_server_create(int device, const g1_server_config* cfg, g
         if (cfg->ppr_iters) S->ppr_iters = cfg->ppr_iters;
         if (cfg->idle_release_ms) S->idle_ms = cfg->idle_release_ms;
         if (cfg->solo_queue_ms) S->solo_queue_ms = cfg->solo_queue_ms;
+        if (cfg->solo_lanes > 16) return fail(G1_ERR_INVALID, "solo_lanes above 16");
     }
     // executors for up to 4096 graphs; the vector never reallocates
     S->execs.reserve(3 * 4096);
+    const uint32_t nl = cfg && cfg->solo_lanes ? cfg->solo_lanes : kDefaultLanes;
+    for (uint32_t i = 0; i < nl; ++i) S->lanes.emplace_back(new Lane());
     S->th = std::thread(loop, S.get());
     *out = S.release();
     return G1_OK;
@@ -757,13 +789,15 @@ extern "C" g1_status g1_server_destroy(g1_server* S) {
     }
     S->cv_in.notify_all();
     if (S->th.joinable()) S->th.join();
-    // the loop ended only after the lane's last query completed
-    {
-        std::lock_guard<std::mutex> lk(S->lane_mu);
-        S->lane_stop = true;
+    // the loop ended only after the lanes' last queries completed
+    for (auto& L : S->lanes) {
+        {
+            std::lock_guard<std::mutex> lk(L->mu);
+            L->stop = true;
+        }
+        L->cv.notify_all();
+        if (L->th.joinable()) L->th.join();
     }
-    S->lane_cv.notify_all();
-    if (S->lane.joinable()) S->lane.join();
     {
         DeviceGuard dg(S->device);
         for (auto& e : S->execs) {

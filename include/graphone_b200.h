@@ -322,11 +322,12 @@ g1_status g1_ppr_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, float alph
  * of the batch keeps running (continuous batching).  Batching pays only for
  * dozens of queries at once, so while an executor's slots are empty and
  * fewer than 32 queries wait (or the waiting ones would finish within
- * solo_queue_ms one by one), its queries take the server's solo lane: one
- * worker thread running queries one at a time, oldest first across graphs
- * and kinds, on the single-source engines (the results of g1_sssp / g1_bfs
- * with G1_ENGINE_AUTO and of g1_ppr).  SSSP and BFS on graphs of small
- * uniform degree -- grids -- always take the lane (the near-far engine).  Executors of different graphs / kinds run
+ * solo_queue_ms one by one), its queries take the server's solo lanes:
+ * worker threads (solo_lanes) each running one query at a time, oldest
+ * first across graphs and kinds, never two of one graph at once, on the
+ * single-source engines (the results of g1_sssp / g1_bfs with
+ * G1_ENGINE_AUTO and of g1_ppr).  SSSP and BFS on graphs of small uniform
+ * degree -- grids -- always take a lane (the near-far engine).  Executors of different graphs / kinds run
  * concurrently on their own streams.  An engine's state is allocated when
  * its first batch arrives, sized by the free device memory (slots halve
  * until it fits, down to 32; otherwise queries wait for memory to be
@@ -348,6 +349,8 @@ typedef struct {
                                  finish within this many ms that way (estimated),
                                  batched beyond; 0 = 20; negative = always batched
                                  (grid SSSP / BFS stay on the near-far engine) */
+    uint32_t solo_lanes;      /* worker threads running such queries, one each, never two
+                                 of one graph at a time; 0 = 1, at most 16 */
 } g1_server_config;
 typedef struct {
     uint64_t submitted, completed, failed;
