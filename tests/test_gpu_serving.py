@@ -180,15 +180,16 @@ def host_out(g, kind):
     return np.empty(g.n, np.float32 if kind == g1.QUERY_PPR else np.uint32)
 
 
-@pytest.mark.parametrize("max_batch,solo_queue_ms", [(32, -1), (256, -1), (256, 0), (64, 1000)])
-def test_served_mix_equals_each_query_alone(cuda, max_batch, solo_queue_ms):
+@pytest.mark.parametrize("max_batch,solo_queue_ms,lanes",
+                         [(32, -1, 0), (256, -1, 0), (256, 0, 0), (64, 1000, 0), (256, 1000, 3)])
+def test_served_mix_equals_each_query_alone(cuda, max_batch, solo_queue_ms, lanes):
     """solo_queue_ms -1: SSSP / BFS always batched on the slot engines; 0:
     the default hybrid (one at a time on the single-source engines while the
-    queue is short); 1000: mostly one at a time."""
+    queue is short); 1000: mostly one at a time, on one lane or three."""
     graphs = serving_graphs()
     Gs = [g1.Graph.from_gen(g) for g in graphs]
-    reqs = request_mix(graphs, 400, seed=max_batch + solo_queue_ms)
-    with g1.Server(max_batch=max_batch, solo_queue_ms=solo_queue_ms) as srv:
+    reqs = request_mix(graphs, 400, seed=max_batch + solo_queue_ms + lanes)
+    with g1.Server(max_batch=max_batch, solo_queue_ms=solo_queue_ms, solo_lanes=lanes) as srv:
         gids = [srv.add_graph(G) for G in Gs]
         outs = [host_out(graphs[gi], kind) for gi, kind, _ in reqs]
         # arrivals in waves, so later queries join batches already running
