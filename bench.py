@@ -770,9 +770,10 @@ def run_ours(args):
                    "ended in an invalid-address-space error on an RMAT-12 input), so they are no "
                    "longer run; figures measured before the fault are in "
                    "profiles/reference_gpu_engines.md")}
-    if not args.no_queries:
+    # query and serving measurements are single-GPU: rank 0 runs them
+    if not args.no_queries and rank == 0:
         result["queries"] = query_metrics(dev, stream, parity)
-    if args.serve_requests > 0:
+    if args.serve_requests > 0 and rank == 0:
         result["serving"] = serving_metrics(dev, args.serve_requests, args.serve_rate)
     if not args.no_parity:
         p = parity.finish()
