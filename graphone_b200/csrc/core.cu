@@ -51,10 +51,14 @@ uint32_t wait_polls(uint32_t dflt) {
     return p < 0 ? dflt : (uint32_t)p;
 }
 
-void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
-
 namespace {
 thread_local int t_capturing = 0;
+}
+
+// Kernels enqueued while this thread captures a CUDA graph are counted when
+// the graph is launched, by the caller.
+void count_launches(uint64_t n) {
+    if (t_capturing == 0) g_launches.fetch_add(n, std::memory_order_relaxed);
 }
 CaptureScope::CaptureScope() { ++t_capturing; }
 CaptureScope::~CaptureScope() { --t_capturing; }

@@ -1017,8 +1017,13 @@ g1_status SlotEngine::step_graph(int i, uint32_t phase, cudaGraphExec_t* out) {
         if (!capture_) G1_CUDA(cudaStreamCreateWithFlags(&capture_, cudaStreamNonBlocking));
         cudaGraph_t graph = nullptr;
         G1_CUDA(cudaStreamBeginCapture(capture_, cudaStreamCaptureModeThreadLocal));
-        const g1_status st = enqueue_iterations(1u << i, phase, capture_);
-        const cudaError_t e = cudaStreamEndCapture(capture_, &graph);
+        g1_status st;
+        cudaError_t e;
+        {
+            CaptureScope cs;  // counted per launch in step()
+            st = enqueue_iterations(1u << i, phase, capture_);
+            e = cudaStreamEndCapture(capture_, &graph);
+        }
         if (st != G1_OK) {
             if (graph) cudaGraphDestroy(graph);
             return st;

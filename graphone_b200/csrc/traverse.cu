@@ -744,6 +744,10 @@ static g1_status blas_graph_traverse(g1_graph* g, uint32_t src, uint32_t* out, u
     bg_x_init_kernel<<<gi, 256, 0, s>>>(x, n, sp);
     count_launches(2);
     G1_CUDA(cudaGetLastError());
+    // kernels per pair of steps (counted per graph launch): x set and
+    // reset, the SpMV's one or two, the sparse step's three
+    const uint64_t per_pair =
+        2ull * (2 + (resolve_schedule(g, pull_t, G1_SCHED_AUTO) == G1_SCHED_VECTOR ? 1 : 2) + (limit ? 3 : 0));
     int i = 1;
     for (;;) {
         cudaGraphExec_t& gx = ag.exec[mode][i];
@@ -768,6 +772,7 @@ static g1_status blas_graph_traverse(g1_graph* g, uint32_t src, uint32_t* out, u
             ag.param[mode] = limit;
         }
         G1_CUDA(cudaGraphLaunch(gx, s));
+        count_launches(per_pair << i);
         G1_CUDA(cudaMemcpyAsync(host, a.ctl, 16, cudaMemcpyDeviceToHost, s));
         G1_CUDA(cudaMemcpyAsync(host + 4, a.c[0], 4, cudaMemcpyDeviceToHost, s));
         G1_CUDA(cudaStreamSynchronize(s));
