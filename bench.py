@@ -895,7 +895,7 @@ def run_reference(args):
 
 
 KERNEL_WORKLOADS = ("slot_sssp", "slot_bfs", "slot_ppr", "nearfar", "advance_grid", "advance_lb",
-                    "blas_rmat20", "gather_rates")
+                    "blas_rmat20", "gather_rates", "ppr_rmat22", "blas_sparse_rmat22")
 
 
 def run_kernel_workload(name: str):
@@ -912,6 +912,12 @@ def run_kernel_workload(name: str):
       gather_rates                     prints the random-load rates of
                                        g1_measure_gather_rate over item size,
                                        loads in flight, warps per SM and footprint
+      ppr_rmat22                       single-source PPR (20 iterations, the nnz
+                                       SpMV with the PPR epilogue) on RMAT-22
+                                       directed, relabelled, 2 sources
+      blas_sparse_rmat22               SSSP on RMAT-22 symmetric (relabelled) on
+                                       the BLAS engine, whose small-frontier
+                                       steps are sparse steps, 2 sources
     """
     import torch
     import graphone_b200 as g1
@@ -926,6 +932,22 @@ def run_kernel_workload(name: str):
                 print(f"{where:4s} footprint {fp:>11,d} B  item {item:2d} B  in flight {fl:2d}  "
                       f"warps/SM {32 * bps:2d}: {r / 1e9:7.1f} G loads/s "
                       f"({r / 1e9 / sms:5.2f} G/s per SM)", flush=True)
+        return
+    if name == "ppr_rmat22":
+        g = gen.rmat(22, 16, False, float_values=True, device=dev)
+        G = g1.Graph.from_gen(g, relabel=True)
+        for s in gen.pick_sources(g, 2):
+            G.ppr(int(s), 0.85, 20)
+        torch.cuda.synchronize()
+        print("kernel workload", name, "done", flush=True)
+        return
+    if name == "blas_sparse_rmat22":
+        g = gen.rmat(22, 16, True, (1, 64), device=dev)
+        G = g1.Graph.from_gen(g, relabel=True)
+        for s in gen.pick_sources(g, 2):
+            G.sssp(int(s), g1.ENGINE_BLAS)
+        torch.cuda.synchronize()
+        print("kernel workload", name, "done", flush=True)
         return
     if name.startswith("slot_"):
         g = gen.rmat(18, 16, True, (1, 64), device=dev)
