@@ -982,7 +982,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--iters", type=int, default=30)
-    ap.add_argument("--ref-iters", type=int, default=1)
+    ap.add_argument("--ref-iters", type=int, default=30,
+                    help="PageRank iterations per reference step (30: the same step as ours)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-relabel", action="store_true")
     ap.add_argument("--no-parity", action="store_true",
