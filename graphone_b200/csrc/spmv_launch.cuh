@@ -78,8 +78,10 @@ inline g1_schedule resolve_schedule(const g1_graph* g, int t, g1_schedule sched)
     const Orientation& o = g->o[t];
     if (o.tuned_sched) return (g1_schedule)o.tuned_sched;
     const double mean = g->n ? (double)g->m / g->n : 0.0;
-    // Uniform small degrees: one short row per lane group, no merge bookkeeping.
-    return (o.max_deg <= 64 && mean <= 16.0 && o.max_deg <= 8 * std::max(1.0, mean))
+    // Uniform small degrees on a small graph: one short row per lane group, no
+    // merge bookkeeping.  From 2^22 nonzeros the nnz tiles win even there (a
+    // 4096^2 grid: 170 against 337 us per SpMV; a 1024^2 grid: a tie).
+    return (o.max_deg <= 64 && mean <= 16.0 && o.max_deg <= 8 * std::max(1.0, mean) && g->m < (1u << 22))
                ? G1_SCHED_VECTOR
                : G1_SCHED_MERGE;
 }
