@@ -247,6 +247,12 @@ struct PprPlan {
     const uint32_t* deg = nullptr;
     const NnzPlan* plan = nullptr;  // null: the CSR-vector schedule
     size_t words = 0;
+    // sparse steps (0: none): the out-edge CSR and the limit on the in-edges
+    // of the rows a step reaches
+    const uint32_t* out_rp = nullptr;
+    const uint32_t* out_col = nullptr;
+    unsigned long long sparse_limit = 0;
+    uint32_t sparse_steps = 0;  // the steps that may be sparse (the first ones)
 };
 size_t ppr_state_words(uint32_t n, const NnzPlan* plan);
 g1_status ppr_prepare(g1_graph* g, cudaStream_t s, PprPlan* out);

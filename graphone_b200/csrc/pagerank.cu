@@ -305,11 +305,15 @@ struct PprEpilogue {
     const uint32_t* empty_list = nullptr;
     uint32_t n_empty_list = 0;
     const uint32_t* src_rows = nullptr;
+    // sparse steps: the word that says this iteration is one (its kernels
+    // then return at once), or null
+    const uint32_t* sparse_now = nullptr;
 
     uint32_t src;
     float tele;
     unsigned long long dang_local;
 
+    __device__ __forceinline__ bool active() const { return !sparse_now || *sparse_now == 0u; }
     __device__ __forceinline__ void begin() {
         dang_local = 0ull;
         if (dang_clear && blockIdx.x == 0 && threadIdx.x == 0) *dang_clear = 0ull;
@@ -355,6 +359,191 @@ __global__ void ppr_init_kernel(const uint32_t* perm, uint32_t src, const float*
     dang[2] = 0ull;
 }
 
+// Sparse steps of single-source PPR.  x is zero off the vertices its last
+// step reached (x0 off src), and a row's value sums x over its in-edges, so
+// a step only has to compute the rows the nonzeros of x reach (their
+// out-neighbours, and src for the teleport): every other row is 0 (its rank
+// and x stay 0).  A step lists those rows and folds each over all its
+// in-edges while
+//   - their in-edges sum below a limit and none has more than kPprRowCap
+//     (a row is one warp's loop), and
+//   - the vertices it expands have out-edges summing below the limit and
+//     none more than kPprRowCap (checked before any is expanded, from the
+//     sums the previous step took of its rows);
+// once a step is not sparse every later one is a full SpMV (a sticky flag).
+// The lists rotate through three buffers: F the nonzeros of x (this step's
+// input), C the rows being listed (the next F), Z the nonzeros x' still
+// holds from two steps ago (zeroed first; a full SpMV overwrites them all
+// anyway).  No host round trip: each kernel reads the decision from the
+// control words.
+constexpr uint32_t kPprRowCap = 1024;
+
+struct PprSparse {
+    // [0] dense from now on, [1] this step is sparse, [2..3] in-edge sum of
+    // C (u64), [4..6] list counts, [7] block ticket, [8] the max in-degree
+    // in C; [12 + 4p .. 15 + 4p] for p = step parity: the out-edge sum (u64)
+    // and max out-degree of the rows listed in the step of that parity
+    uint32_t* ctl;
+    uint32_t* bits;  // a bit per vertex: listed in this step
+    uint32_t* list[3];
+    const uint32_t* out_rp;
+    const uint32_t* out_col;
+    const uint32_t* in_rp;
+    unsigned long long limit;
+};
+
+__device__ __forceinline__ uint32_t warp_max_u32(uint32_t v) { return __reduce_max_sync(0xffffffffu, v); }
+
+// Checks the step can be sparse, zeroes x' on Z, then lists C: the
+// out-neighbours of F's vertices and src, each once, with their in- and
+// out-edge sums and maxima; the last block decides.
+__global__ void __launch_bounds__(256)
+ppr_sparse_expand_kernel(PprSparse sp, uint32_t it, const uint32_t* src_p, uint32_t n, float* x_next) {
+    __shared__ unsigned long long part[8];
+    __shared__ uint32_t smax[2];
+    if (sp.ctl[0]) return;  // dense from now on: the same for every block
+    const uint32_t fi = it % 3;
+    const uint32_t src = *src_p;
+    unsigned long long fout;
+    uint32_t fmax;
+    if (it == 0) {
+        fout = fmax = sp.out_rp[src + 1] - sp.out_rp[src];
+    } else {
+        const uint32_t* p = sp.ctl + 12 + 4 * (it & 1u);
+        fout = (unsigned long long)p[0] | ((unsigned long long)p[1] << 32);
+        fmax = p[2];
+    }
+    if (fout >= sp.limit || fmax > kPprRowCap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            sp.ctl[1] = 0u;
+            sp.ctl[0] = 1u;
+        }
+        return;
+    }
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t threads = (uint64_t)gridDim.x * blockDim.x;
+    {
+        const uint32_t zi = (fi + 2) % 3;
+        const uint32_t nz = sp.ctl[4 + zi];
+        for (uint64_t i = tid; i < nz; i += threads) x_next[sp.list[zi][i]] = 0.0f;
+    }
+    if (threadIdx.x < 2) smax[threadIdx.x] = 0u;
+    __syncthreads();
+    const uint32_t* F = sp.list[fi];
+    uint32_t* C = sp.list[(fi + 1) % 3];
+    const uint32_t nf = sp.ctl[4 + fi];
+    uint32_t* nc = &sp.ctl[4 + (fi + 1) % 3];
+    unsigned long long in_sum = 0ull, out_sum = 0ull;
+    uint32_t in_max = 0u, out_max = 0u;
+    auto list = [&](uint32_t v) {
+        const uint32_t bit = 1u << (v & 31u);
+        if (atomicOr(&sp.bits[v >> 5], bit) & bit) return;
+        C[atomicAdd(nc, 1u)] = v;
+        const uint32_t di = sp.in_rp[v + 1] - sp.in_rp[v];
+        const uint32_t dout = sp.out_rp[v + 1] - sp.out_rp[v];
+        in_sum += di;
+        out_sum += dout;
+        in_max = max(in_max, di);
+        out_max = max(out_max, dout);
+    };
+    if (tid == 0) list(src);
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint64_t i = tid >> 5; i < nf; i += threads >> 5) {
+        const uint32_t u = F[i];
+        if (u >= n) continue;
+        for (uint32_t k = sp.out_rp[u] + lane; k < sp.out_rp[u + 1]; k += 32) list(sp.out_col[k]);
+    }
+    in_max = warp_max_u32(in_max);
+    out_max = warp_max_u32(out_max);
+    if (lane == 0) {
+        if (in_max) atomicMax(&smax[0], in_max);
+        if (out_max) atomicMax(&smax[1], out_max);
+    }
+    const unsigned long long bin = block_sum<unsigned long long, 256>(in_sum, part);
+    const unsigned long long bout = block_sum<unsigned long long, 256>(out_sum, part);
+    if (threadIdx.x == 0) {
+        unsigned long long* g_in = reinterpret_cast<unsigned long long*>(sp.ctl + 2);
+        uint32_t* nxt = sp.ctl + 12 + 4 * ((it + 1) & 1u);
+        if (bin) atomicAdd(g_in, bin);
+        if (bout) atomicAdd(reinterpret_cast<unsigned long long*>(nxt), bout);
+        if (smax[0]) atomicMax(&sp.ctl[8], smax[0]);
+        if (smax[1]) atomicMax(&nxt[2], smax[1]);
+        __threadfence();
+        if (atomicAdd(&sp.ctl[7], 1u) == gridDim.x - 1) {
+            // every block has listed its rows and added its sums; atomic
+            // reads, as this block's L1 may hold the line from its reads of
+            // ctl above
+            const bool sparse = atomicAdd(g_in, 0ull) < sp.limit && atomicMax(&sp.ctl[8], 0u) <= kPprRowCap;
+            sp.ctl[1] = sparse ? 1u : 0u;
+            if (!sparse) sp.ctl[0] = 1u;
+            sp.ctl[7] = 0u;
+            __threadfence();
+        }
+    }
+}
+
+// The listed rows, one warp each: the sum of x over all the row's in-edges
+// (each lane in edge order, four loads in flight, then a shuffle tree: a
+// fixed order), then the epilogue's arithmetic (teleport at src, x', rank
+// in the last step, the dangling sum); clears the rows' bits and, for the
+// next step, Z's count (its C), the in-edge sum and maximum and the
+// out-edge sums this step read.
+__global__ void __launch_bounds__(256)
+ppr_sparse_rows_kernel(PprSparse sp, uint32_t it, const uint32_t* in_col, const float* x, const float* iw,
+                       const uint32_t* src_p, const unsigned long long* dang_in, unsigned long long* dang_out,
+                       unsigned long long* dang_clear, double alpha, float* x_next, float* rank_next, int write_rank) {
+    __shared__ alignas(16) char smem[64 * 8];
+    if (!sp.ctl[1]) return;
+    const uint32_t fi = it % 3;
+    const uint32_t ci = (fi + 1) % 3;
+    const uint32_t nc = sp.ctl[4 + ci];
+    const uint32_t* C = sp.list[ci];
+    const uint32_t src = *src_p;
+    const float tele = (float)((1.0 - alpha) + alpha * ((double)(*dang_in) / kDangScale));
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    unsigned long long dl = 0ull;
+    for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nc; i += warps) {
+        const uint32_t v = C[i];
+        const uint32_t end = sp.in_rp[v + 1];
+        float acc = 0.0f;
+        for (uint32_t k = sp.in_rp[v] + lane; k < end; k += 128) {
+            float a[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t kk = k + 32u * j;
+                a[j] = kk < end ? x[in_col[kk]] : 0.0f;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc += a[j];
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == 0) {
+            atomicAnd(&sp.bits[v >> 5], ~(1u << (v & 31u)));
+            const float r = v == src ? acc + tele : acc;
+            if (write_rank) rank_next[v] = r;
+            const float w = iw[v];
+            if (w != 0.0f) x_next[v] = r * w;
+            else dl += dang_fixed(r);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 8) {
+        uint32_t* cur = sp.ctl + 12 + 4 * (it & 1u);
+        switch (threadIdx.x) {
+            case 0: *dang_clear = 0ull; break;
+            case 1: sp.ctl[4 + (fi + 2) % 3] = 0u; break;  // Z becomes the next step's C
+            case 2: sp.ctl[2] = 0u; break;
+            case 3: sp.ctl[3] = 0u; break;
+            case 4: sp.ctl[8] = 0u; break;
+            case 5: cur[0] = 0u; break;  // the next step accumulates here
+            case 6: cur[1] = 0u; break;
+            case 7: cur[2] = 0u; break;
+        }
+    }
+    dang_block_add<256>(dl, dang_out, smem);
+}
+
 namespace {
 
 constexpr size_t kPprAlign = 64;  // words (256 bytes)
@@ -364,6 +553,7 @@ struct PprLayout {
     unsigned long long* dang;
     uint32_t* src;
     float *iw, *rank[2], *x[2], *carry, *tail;
+    uint32_t *ctl, *bits, *list[3];  // sparse steps
 };
 
 PprLayout ppr_layout(uint32_t n, const NnzPlan* plan, uint32_t* store) {
@@ -382,6 +572,9 @@ PprLayout ppr_layout(uint32_t n, const NnzPlan* plan, uint32_t* store) {
     const size_t nt = plan ? (size_t)plan->n_tiles + 1 : 1;
     L.carry = reinterpret_cast<float*>(take(nt));
     L.tail = reinterpret_cast<float*>(take(nt));
+    L.ctl = take(32);
+    L.bits = take((size_t)n / 32 + 1);
+    for (int i = 0; i < 3; ++i) L.list[i] = take(n);
     return L;
 }
 
@@ -389,7 +582,8 @@ PprLayout ppr_layout(uint32_t n, const NnzPlan* plan, uint32_t* store) {
 
 size_t ppr_state_words(uint32_t n, const NnzPlan* plan) {
     const size_t nt = plan ? (size_t)plan->n_tiles + 1 : 1;
-    return ppr_round(8) + ppr_round(1) + 5 * ppr_round(n) + 2 * ppr_round(nt);
+    return ppr_round(8) + ppr_round(1) + 5 * ppr_round(n) + 2 * ppr_round(nt) + ppr_round(32) +
+           ppr_round((size_t)n / 32 + 1) + 3 * ppr_round(n);
 }
 
 g1_status ppr_prepare(g1_graph* g, cudaStream_t s, PprPlan* out) {
@@ -405,6 +599,20 @@ g1_status ppr_prepare(g1_graph* g, cudaStream_t s, PprPlan* out) {
         out->plan = p;
     }
     out->words = ppr_state_words(g->n, out->plan);
+    // sparse steps need the out-edges (the in-edge CSR itself when symmetric),
+    // on graphs of 2^20 edges or more (below, a full SpMV costs a few
+    // microseconds); the limit on the listed rows' in-edges is m / push_div,
+    // the BLAS traversal loop's threshold
+    out->out_rp = g->o[0].present ? g->o[0].rp : (g->symmetric ? g->o[1].rp : nullptr);
+    out->out_col = g->o[0].present ? g->o[0].col : (g->symmetric ? g->o[1].col : nullptr);
+    out->sparse_limit = out->out_rp && g->m >= (1u << 20)
+                            ? (unsigned long long)g->m / std::max<uint32_t>(1, g->push_div)
+                            : 0ull;
+    // with rows or out-lists longer than kPprRowCap (hubs), a query reaches
+    // one within a step or two and runs dense from there: its sparse
+    // kernels are launched for the first three steps only
+    const uint32_t out_max = g->o[0].present ? g->o[0].max_deg : g->o[1].max_deg;
+    out->sparse_steps = std::max(g->o[1].max_deg, out_max) > kPprRowCap ? 3u : UINT32_MAX;
     return G1_OK;
 }
 
@@ -422,9 +630,38 @@ g1_status ppr_enqueue(g1_graph* g, const PprPlan& pl, uint32_t* store, uint32_t 
     ppr_init_kernel<<<1, 1, 0, s>>>(perm, src, L.iw, L.src, L.rank[0], L.x[0], L.dang);
     count_launches(2);
     G1_CUDA(cudaGetLastError());
+    PprSparse sp{};
+    const bool sparse = pl.sparse_limit != 0;
+    if (sparse) {
+        sp.ctl = L.ctl;
+        sp.bits = L.bits;
+        for (int i = 0; i < 3; ++i) sp.list[i] = L.list[i];
+        sp.out_rp = pl.out_rp;
+        sp.out_col = pl.out_col;
+        sp.in_rp = g->o[t].rp;
+        sp.limit = pl.sparse_limit;
+        // F0 = {src} (ctl[4] = 1), the other counts, sums, flags and bits zero
+        G1_CUDA(cudaMemsetAsync(L.ctl, 0, 32 * 4, s));
+        G1_CUDA(cudaMemsetAsync(L.bits, 0, ((size_t)n / 32 + 1) * 4, s));
+        G1_CUDA(cudaMemcpyAsync(L.list[0], L.src, 4, cudaMemcpyDeviceToDevice, s));
+        G1_TRY(g1_mem_fill_u32(L.ctl + 4, 1u, 1, s));
+    }
+    const uint32_t sgrid = (uint32_t)g->sm_count * 2;
     for (uint32_t it = 0; it < iters; ++it) {
         const bool last = it + 1 == iters;
         const int cur = it & 1, nxt = cur ^ 1;
+        const bool sparse_it = sparse && it < pl.sparse_steps;
+        if (sparse_it) {
+            // a sparse last step writes only its rows' ranks
+            if (last) G1_CUDA(cudaMemsetAsync(L.rank[nxt], 0, (size_t)n * 4, s));
+            ppr_sparse_expand_kernel<<<sgrid, 256, 0, s>>>(sp, it, L.src, n, L.x[nxt]);
+            ppr_sparse_rows_kernel<<<sgrid, 256, 0, s>>>(sp, it, g->o[t].col, L.x[cur], L.iw, L.src,
+                                                         &L.dang[it % 3], &L.dang[(it + 1) % 3],
+                                                         &L.dang[(it + 2) % 3], (double)alpha, L.x[nxt],
+                                                         L.rank[nxt], last ? 1 : 0);
+            count_launches(2);
+            G1_CUDA(cudaGetLastError());
+        }
         PprEpilogue e;
         e.rank_next = L.rank[nxt];
         e.x_next = L.x[nxt];
@@ -435,6 +672,7 @@ g1_status ppr_enqueue(g1_graph* g, const PprPlan& pl, uint32_t* store, uint32_t 
         e.dang_clear = &L.dang[(it + 2) % 3];
         e.alpha = (double)alpha;
         e.write_rank = last ? 1 : 0;
+        e.sparse_now = sparse_it ? L.ctl + 1 : nullptr;
         if (!pl.plan) {
             G1_TRY((launch_vector<PlusPatternF32>(g, t, L.x[cur], e, s)));
             continue;

@@ -247,7 +247,10 @@ g1_status g1_autotune_traversal(g1_graph* g, uint32_t n_sources, uint32_t* push_
  * G1_ENGINE_BLAS loop (on graphs of 2^20 edges or more with the out-edge
  * CSR) computes a step from the frontier's out-edges alone instead of
  * pulling every row: while the frontier's out-degree sum is below
- * m / push_div.  Results and iteration counts never depend on them.  No
+ * m / push_div; and where g1_ppr's sparse steps end (same graphs: while
+ * the rows a step reaches have fewer than m / push_div in-edges).  BFS and
+ * SSSP results and iteration counts never depend on them; PPR ranks only
+ * in rounding (a listed row sums its in-edges in another order).  No
  * GraphOne counterpart. */
 g1_status g1_set_traversal_thresholds(g1_graph* g, uint32_t push_div, uint32_t slot_div);
 
@@ -302,7 +305,11 @@ g1_status g1_sssp_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, uint32_t*
  *                + [v == src] * ((1 - alpha) + alpha * sum_{outdeg(u)=0} rank[u]).
  * Transition weights are 1/out-degree (edge values are not used).  fp32.
  * Runs on the SpMV schedules (one pass over the in-edge CSR per iteration,
- * 4 bytes per edge); g1_ppr_batch runs the slot engine, whose per-slot
+ * 4 bytes per edge), except while rank is still confined near src: on
+ * graphs of 2^20 edges or more with the out-edge CSR (or symmetric), a step
+ * whose reachable rows have fewer than m / push_div in-edges computes only
+ * those rows (every step of a short query on a grid; the first few on
+ * RMAT).  g1_ppr_batch runs the slot engine, whose per-slot
  * results are the same bits wherever a query sits in a batch.  Both agree
  * with an FP64 evaluation within 1e-6 relative L1; they are not bit-identical
  * to each other (different summation orders).  rank_out: n f32, host or

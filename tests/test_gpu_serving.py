@@ -82,6 +82,46 @@ def test_ppr_directed_rmat_sources_with_empty_rows(cuda):
         assert O.rel_l1(G.ppr(src, 0.5, 7), ppr_oracle(g, src, 0.5, 7)) < PPR_TOL, src
 
 
+SPARSE_GRAPHS = {
+    "grid1024": lambda: gen.grid2d(1024, 1024, (1, 100)),
+    "rmat16_sym": lambda: gen.rmat(16, 16, True, (1, 64)),
+    "rmat17_dir": lambda: gen.rmat(17, 16, False, (1, 64)),
+    # uniform random (no hubs): sparse until the reach covers m / 16 edges
+    "uniform17": lambda: gen.from_edges(*gen.rmat_samples(17, 8, 0.25, 0.25, 0.25), 1 << 17, True,
+                                        (1, 64), name="uniform17"),
+}
+
+
+@pytest.mark.parametrize("sched", [g1.SCHED_MERGE, g1.SCHED_VECTOR])
+@pytest.mark.parametrize("name", sorted(SPARSE_GRAPHS))
+def test_ppr_sparse_steps_match_oracle(cuda, name, sched):
+    """Graphs of 2^20 edges or more, where g1_ppr's first steps compute only
+    the rows the source's neighbourhood reaches: every step of 20 on the
+    grid, a few on the uniform graph before the full SpMV takes over, at
+    most the first three on RMAT (whose hubs end them at once).
+    Sources of every kind: a hub, a leaf, no out-edges, no in-edges,
+    isolated; the last step sparse (1-3 iterations) or dense."""
+    g = SPARSE_GRAPHS[name]()
+    assert g.m >= 1 << 20
+    G = g1.Graph.from_gen(g, relabel=name != "grid1024")
+    G.set_schedule(sched, g1.DEFAULT_MERGE_VARIANT)
+    rp, _, _ = g.np("n")
+    trp, _, _ = g.np("t")
+    indeg, outdeg = np.diff(trp), np.diff(rp)
+    picks = {0, g.n // 2 + 17, g.n - 1, int(np.argmax(indeg))}
+    for mask in ((outdeg == 1), (outdeg == 0) & (indeg > 0), (indeg == 0) & (outdeg > 0),
+                 (indeg == 0) & (outdeg == 0)):
+        hit = np.flatnonzero(mask)
+        if len(hit):
+            picks.add(int(hit[len(hit) // 2]))
+    for src in sorted(picks):
+        for iters in (1, 2, 3, 20):
+            r = G.ppr(src, 0.85, iters)
+            assert O.rel_l1(r, ppr_oracle(g, src, 0.85, iters)) < PPR_TOL, (src, iters)
+        # the same bits again (the store's lists and flags reset per query)
+        assert np.array_equal(G.ppr(src, 0.85, 20), r), src
+
+
 def test_ppr_zero_iterations_is_the_indicator(cuda):
     g = GRAPHS["rmat10_sym"]
     G = g1.Graph.from_gen(g)
