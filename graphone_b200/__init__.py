@@ -26,6 +26,7 @@ SR_MINPLUS_U32, SR_MINPLUS_F32, SR_PLUSTIMES_F32, SR_BFS_U32 = 0, 1, 2, 3
 SCHED_AUTO, SCHED_MERGE, SCHED_VECTOR = 0, 1, 2
 ENGINE_BLAS, ENGINE_ADVANCE, ENGINE_AUTO, ENGINE_NEARFAR = 0, 1, 2, 3
 PR_REFERENCE, PR_DANGLING = 0, 1
+HOT_COLUMNS_AUTO, HOT_COLUMNS_OFF, HOT_COLUMNS_ON = 0, 1, 2
 # Kernel family of each merge-schedule variant, indexed like kMergeVariants
 # in csrc/spmv_launch.cuh: "warp" = spmv_wmerge_kernel (warp tiles, plain
 # loads), "cta_tma" = spmv_merge_kernel (CTA tiles staged by bulk copies),
@@ -70,6 +71,7 @@ def _declare(L):
     L.g1_count_user_launches.argtypes = [C.c_uint64]
     L.g1_test_set_wait_polls.argtypes = [C.c_int64]
     L.g1_set_traversal_thresholds.argtypes = [P, C.c_uint32, C.c_uint32]
+    L.g1_graph_set_hot_columns.argtypes = [P, C.c_int]
     L.g1_measure_gather_rate.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                                          C.POINTER(C.c_double), P]
     L.g1_profile_begin.argtypes = []
@@ -126,7 +128,7 @@ EXPORTS = (
     "g1_count_user_launches", "g1_test_set_wait_polls", "g1_measure_gather_rate",
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
-    "g1_spmv_plan", "g1_spmv_nnz_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_autotune_traversal", "g1_set_traversal_thresholds", "g1_pagerank", "g1_sssp", "g1_bfs", "g1_advance_run",
+    "g1_spmv_plan", "g1_spmv_nnz_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_autotune_traversal", "g1_set_traversal_thresholds", "g1_graph_set_hot_columns", "g1_pagerank", "g1_sssp", "g1_bfs", "g1_advance_run",
     "g1_bfs_batch", "g1_sssp_batch", "g1_ppr", "g1_ppr_batch",
     "g1_server_create", "g1_server_add_graph", "g1_server_submit", "g1_server_poll",
     "g1_server_wait", "g1_server_stats", "g1_server_destroy",
@@ -286,6 +288,10 @@ class Graph:
         """Sets the push/pull divisors by hand (0 keeps one): see
         g1_set_traversal_thresholds."""
         check(lib().g1_set_traversal_thresholds(self._h, push_div, slot_div))
+
+    def set_hot_columns(self, mode: int = HOT_COLUMNS_AUTO):
+        """PageRank's column layout on this graph: see g1_graph_set_hot_columns."""
+        check(lib().g1_graph_set_hot_columns(self._h, mode))
 
     def autotune_traversal(self, n_sources=16, stream=None):
         """(push_div, slot_div): the push/pull thresholds g1_autotune_traversal

@@ -377,15 +377,19 @@ uint32_t grid_for(uint64_t n, int block, int sm_count, int per_sm = 8) {
 // Allocates an orientation's arrays.  The padding past row_ptr[n] and past
 // the last nonzero is zero-filled: bulk copies and warp tiles read whole
 // aligned ranges without bounds checks (a padding column 0 is a valid index).
-g1_status alloc_orientation(Orientation& o, uint32_t n, uint32_t m) {
+// Arrays of n + 1 row offsets and m columns and values, each followed by a
+// zeroed pad (the tile kernels' 32-byte loads may run past the last
+// nonzero); the caller writes [0, n + 1) and [0, m) on stream s.
+g1_status alloc_orientation(Orientation& o, uint32_t n, uint32_t m, cudaStream_t s) {
     const size_t rp_bytes = ((size_t)n + 1 + 64) * 4;
     const size_t nz_bytes = ((size_t)m + kWarpTilePad + 64) * 4;
     G1_TRY(o.b_rp.ensure(rp_bytes));
     G1_TRY(o.b_col.ensure(nz_bytes));
     G1_TRY(o.b_val.ensure(nz_bytes));
-    G1_CUDA(cudaMemset(o.b_rp.p, 0, o.b_rp.bytes));
-    G1_CUDA(cudaMemset(o.b_col.p, 0, o.b_col.bytes));
-    G1_CUDA(cudaMemset(o.b_val.p, 0, o.b_val.bytes));
+    const size_t rp_used = ((size_t)n + 1) * 4, nz_used = (size_t)m * 4;
+    G1_CUDA(cudaMemsetAsync(static_cast<char*>(o.b_rp.p) + rp_used, 0, o.b_rp.bytes - rp_used, s));
+    G1_CUDA(cudaMemsetAsync(static_cast<char*>(o.b_col.p) + nz_used, 0, o.b_col.bytes - nz_used, s));
+    G1_CUDA(cudaMemsetAsync(static_cast<char*>(o.b_val.p) + nz_used, 0, o.b_val.bytes - nz_used, s));
     o.rp = o.b_rp.as<uint32_t>();
     o.col = o.b_col.as<uint32_t>();
     o.val = o.b_val.p;
@@ -407,7 +411,7 @@ g1_status upload(void* dst, const void* src, size_t bytes, cudaStream_t s) {
 g1_status rebuild_csr(g1_graph* g, const Orientation& src, Orientation& dst, bool swap,
                       const uint32_t* map, cudaStream_t s) {
     const uint32_t n = g->n, m = g->m;
-    G1_TRY(alloc_orientation(dst, n, m));
+    G1_TRY(alloc_orientation(dst, n, m, s));
     G1_CUDA(cudaMemsetAsync(dst.rp, 0, ((size_t)n + 1) * 4, s));
     if (m == 0) return G1_OK;
     DevBuf keys, keys2, idx, idx2, counts, temp;
@@ -516,11 +520,17 @@ g1_status relabel_by_degree(g1_graph* g, cudaStream_t s) {
 
 }  // namespace
 
+// The orientation whose plans serve t: symmetric graphs share one CSR and
+// its plans; the hot-column copy (2) has the in-edge CSR's rows.
+static Orientation& plan_owner(g1_graph* g, int t) {
+    const int u = t == 2 ? 1 : t;
+    return (u == 1 && g->symmetric && g->o[0].present) ? g->o[0] : g->o[u];
+}
+
 g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out) {
     Orientation& o = g->o[t];
     if (!o.present) return fail(G1_ERR_UNSUPPORTED, "orientation not built");
-    // symmetric graphs share one CSR: share its plans too
-    Orientation& owner = (t == 1 && g->symmetric && g->o[0].present) ? g->o[0] : o;
+    Orientation& owner = plan_owner(g, t);
     auto it = owner.plans.find(items);
     if (it != owner.plans.end()) {
         *out = it->second.get();
@@ -650,7 +660,7 @@ g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out, uint32_t tile) {
     Orientation& o = g->o[t];
     if (!o.present) return fail(G1_ERR_UNSUPPORTED, "orientation not built");
     if (tile == 0 || tile % 32 != 0) return fail(G1_ERR_INVALID, "nnz plan: tile not a multiple of 32");
-    Orientation& owner = (t == 1 && g->symmetric && g->o[0].present) ? g->o[0] : o;
+    Orientation& owner = plan_owner(g, t);
     auto& slot = owner.nnz_plans[tile];
     if (slot) {
         *out = slot.get();
@@ -915,7 +925,7 @@ g1_status g1_graph_create(const uint32_t* row_ptr, const uint32_t* col, const vo
     g->symmetric = (flags & G1_GRAPH_SYMMETRIC) != 0;
     const int side = (flags & G1_GRAPH_INPUT_TRANSPOSE) ? 1 : 0;
     Orientation& o = g->o[side];
-    G1_TRY(alloc_orientation(o, n, m));
+    G1_TRY(alloc_orientation(o, n, m, s));
     G1_TRY(upload(o.rp, row_ptr, ((size_t)n + 1) * 4, s));
     G1_TRY(upload(o.col, col, (size_t)m * 4, s));
     G1_TRY(upload(o.val, val, (size_t)m * 4, s));
@@ -993,7 +1003,7 @@ g1_status g1_graph_arrays(const g1_graph* g, int transpose, const uint32_t** row
 size_t g1_graph_device_bytes(const g1_graph* g) {
     if (!g) return 0;
     size_t s = g->ws.bytes();
-    for (int t = 0; t < 2; ++t) {
+    for (int t = 0; t < 3; ++t) {
         const Orientation& o = g->o[t];
         s += o.b_rp.bytes + o.b_col.bytes + o.b_val.bytes;
         for (auto& kv : o.plans)

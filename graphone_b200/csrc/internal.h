@@ -169,7 +169,10 @@ struct g1_graph {
     uint32_t m = 0;
     g1_dtype vtype = G1_U32;
     bool symmetric = false;
-    g1::Orientation o[2];  // 0 = out-edges (normal), 1 = in-edges (transpose)
+    // 0 = out-edges (normal), 1 = in-edges (transpose), 2 = PageRank's
+    // hot-column copy of 1 on graphs kept in the caller's order (its own
+    // column array; rows, values and plans are 1's)
+    g1::Orientation o[3];
     g1::Workspace ws;
     std::mutex mu;
     int sm_count = 148;
@@ -204,6 +207,8 @@ struct g1_graph {
     // vertex id to the internal id, iperm the reverse.
     bool relabeled = false;
     g1::DevBuf perm, iperm;
+    // PageRank's hot-column layout (orientation 2): a g1_hot_columns mode
+    int hot_mode = 0;
     // Device error word written by kernels (bounded waits that ran out).
     g1::DevBuf err_buf;
     uint32_t* err_word = nullptr;

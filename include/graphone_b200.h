@@ -254,6 +254,25 @@ g1_status g1_autotune_traversal(g1_graph* g, uint32_t n_sources, uint32_t* push_
  * GraphOne counterpart. */
 g1_status g1_set_traversal_thresholds(g1_graph* g, uint32_t push_div, uint32_t slot_div);
 
+/* PageRank's column layout on this graph.  The pull SpMV gathers x[u] once
+ * per out-edge of u and its tile kernel keeps a prefix of x in shared
+ * memory, so it runs fastest when the vertices with the most out-edges come
+ * first.  G1_GRAPH_RELABEL gets that by rebuilding both CSRs in degree order
+ * (about 11 ms on a 65 M-edge graph).  On a graph kept in the caller's order,
+ * g1_pagerank instead renames only the in-edge CSR's columns (vertices by
+ * decreasing out-degree), into a copy of the column array (4 bytes per edge
+ * more on the device, built on the first call, about 0.5 ms on 65 M edges)
+ * and keeps x in that order.  Each row's nonzeros keep their order: the ranks
+ * are the same bits either way.  AUTO (the default): on graphs of 2^22 edges
+ * or more that are not relabelled and not on the CSR-vector schedule; OFF:
+ * never; ON: always.  No GraphOne counterpart. */
+typedef enum {
+    G1_HOT_COLUMNS_AUTO = 0,
+    G1_HOT_COLUMNS_OFF = 1,
+    G1_HOT_COLUMNS_ON = 2
+} g1_hot_columns;
+g1_status g1_graph_set_hot_columns(g1_graph* g, g1_hot_columns mode);
+
 /* ------------------------------------------------------------- algorithms */
 /* PageRank for a fixed iteration count (Run<PRFunctor> over
  * AllActiveFrontier with BlasGcEngine<ALL_ACTIVE>, engine/blas_gc.h:353-434,

@@ -215,6 +215,32 @@ def test_pagerank_rmat20_within_1e6_of_fp64(cuda, relabel):
     assert err < 1e-6, err  # tolerance: relative L1 vs the FP64 oracle
 
 
+@pytest.mark.parametrize("relabel", [False, True])
+def test_pagerank_hot_columns_same_bits(cuda, relabel):
+    """The hot-column layout renames the in-edge CSR's columns by decreasing
+    out-degree and keeps x in that order; rows keep their nonzeros' order, so
+    on every schedule the ranks are the same bits as on the plain layout."""
+    g = gen.rmat(16, 16, False, float_values=True)
+    trp, tci, tv = g.np("t")
+    plain = g1.Graph.from_csr(trp, tci, tv, input_transpose=True, build_other=False, relabel=relabel)
+    hot = g1.Graph.from_csr(trp, tci, tv, input_transpose=True, build_other=False, relabel=relabel)
+    plain.set_hot_columns(g1.HOT_COLUMNS_OFF)
+    hot.set_hot_columns(g1.HOT_COLUMNS_ON)
+    bytes_plain = plain.device_bytes()
+    ref = O.pagerank_f64(trp, tci, tv, 0.85, 30, 1)
+    cases = [(g1.SCHED_VECTOR, 0)] + [(g1.SCHED_MERGE, v) for v in range(len(g1.MERGE_VARIANTS))]
+    for sched, var in cases:
+        for G in (plain, hot):
+            G.set_schedule(sched, var, transpose=1)
+        for iters in (1, 30):
+            a = plain.pagerank(0.85, iters, g1.PR_DANGLING)
+            b = hot.pagerank(0.85, iters, g1.PR_DANGLING)
+            assert np.array_equal(a, b), (sched, var, iters)
+        assert O.rel_l1(b, ref) < 1e-6, (sched, var)  # tolerance: relative L1 vs FP64
+    # the copy of the column array (4 bytes per edge) and the hot ids
+    assert hot.device_bytes() >= bytes_plain + 4 * g.m
+
+
 @pytest.mark.parametrize("name", ["rmat10_sym", "rmat11_dir", "star20k", "grid32"])
 def test_autotune_traversal_keeps_results_exact(cuda, name):
     """g1_autotune_traversal picks the push/pull divisors among its
