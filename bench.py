@@ -895,7 +895,8 @@ def run_reference(args):
 
 
 KERNEL_WORKLOADS = ("slot_sssp", "slot_bfs", "slot_ppr", "nearfar", "advance_grid", "advance_lb",
-                    "blas_rmat20", "gather_rates", "ppr_rmat22", "blas_sparse_rmat22")
+                    "blas_rmat20", "gather_rates", "ppr_rmat22", "blas_sparse_rmat22",
+                    "pagerank_e2e_rmat22")
 
 
 def run_kernel_workload(name: str):
@@ -918,6 +919,11 @@ def run_kernel_workload(name: str):
       blas_sparse_rmat22               SSSP on RMAT-22 symmetric (relabelled) on
                                        the BLAS engine, whose small-frontier
                                        steps are sparse steps, 2 sources
+      pagerank_e2e_rmat22              the end-to-end step at 2 iterations: a new
+                                       graph from the pinned host in-edge CSR of
+                                       RMAT-22 (caller order), PageRank (setup:
+                                       out-weights, hot-column layout, plan), ranks
+                                       to host, graph closed; two steps
     """
     import torch
     import graphone_b200 as g1
@@ -938,6 +944,23 @@ def run_kernel_workload(name: str):
         G = g1.Graph.from_gen(g, relabel=True)
         for s in gen.pick_sources(g, 2):
             G.ppr(int(s), 0.85, 20)
+        torch.cuda.synchronize()
+        print("kernel workload", name, "done", flush=True)
+        return
+    if name == "pagerank_e2e_rmat22":
+        g = make_pagerank_graph(22, dev)
+        trp, tci, tv = g.np("t")
+        h_rp = torch.from_numpy(trp.view(np.int32)).pin_memory()
+        h_ci = torch.from_numpy(tci.view(np.int32)).pin_memory()
+        h_v = torch.from_numpy(tv).pin_memory()
+        h_out = torch.empty(g.n, dtype=torch.float32).pin_memory()
+        del g
+        torch.cuda.empty_cache()
+        for _ in range(2):
+            G = g1.Graph.from_csr(h_rp, h_ci, h_v, input_transpose=True, build_other=False,
+                                  validate=False)
+            G.pagerank(0.85, 2, g1.PR_DANGLING, out=h_out.numpy())
+            G.close()
         torch.cuda.synchronize()
         print("kernel workload", name, "done", flush=True)
         return

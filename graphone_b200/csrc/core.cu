@@ -514,6 +514,8 @@ g1_status relabel_by_degree(g1_graph* g, cudaStream_t s) {
         other.plans.clear();
     }
     g->relabeled = true;
+    g->outw_ready = false;  // per-vertex data derived before are in the old ids
+    g->outdeg_ready = false;
     G1_CUDA(cudaStreamSynchronize(s));
     return G1_OK;
 }
@@ -901,6 +903,10 @@ g1_status g1_stream_sync(void* stream) {
     return G1_OK;
 }
 
+// Edges from which graph creation sums a directed in-edge CSR's out-weights
+// during its upload.
+constexpr uint32_t kEagerOutwMinEdges = 1u << 22;
+
 g1_status g1_graph_create(const uint32_t* row_ptr, const uint32_t* col, const void* val,
                           g1_dtype vtype, uint32_t n, uint32_t m, uint32_t flags, void* stream,
                           g1_graph** out) {
@@ -927,8 +933,17 @@ g1_status g1_graph_create(const uint32_t* row_ptr, const uint32_t* col, const vo
     Orientation& o = g->o[side];
     G1_TRY(alloc_orientation(o, n, m, s));
     G1_TRY(upload(o.rp, row_ptr, ((size_t)n + 1) * 4, s));
-    G1_TRY(upload(o.col, col, (size_t)m * 4, s));
-    G1_TRY(upload(o.val, val, (size_t)m * 4, s));
+    // A large directed in-edge CSR with f32 values (a PageRank input) from
+    // host memory, kept as it is (no out-edge CSR built, not relabelled):
+    // its out-weights are summed while the copy is in flight.
+    if (side == 1 && !g->symmetric && vtype == G1_F32 && m >= kEagerOutwMinEdges &&
+        !(flags & (G1_GRAPH_BUILD_OTHER | G1_GRAPH_RELABEL)) && !is_device_ptr(col) &&
+        !is_device_ptr(val)) {
+        G1_TRY(upload_transpose_with_outw(g.get(), col, val, s));
+    } else {
+        G1_TRY(upload(o.col, col, (size_t)m * 4, s));
+        G1_TRY(upload(o.val, val, (size_t)m * 4, s));
+    }
 
     DevBuf chk;
     G1_TRY(chk.ensure(16));

@@ -238,6 +238,10 @@ g1_status ensure_plan(g1_graph* g, int t, uint32_t items, MergePlan** out);
 // The nnz-split plan for tiles of `tile` nonzeros (a multiple of 32; 256 is
 // the default schedule's).
 g1_status ensure_nnz_plan(g1_graph* g, int t, NnzPlan** out, uint32_t tile = 256);
+// Graph creation of a large in-edge CSR with f32 values from host memory:
+// uploads its columns and values on s while a second stream sums the
+// arrived chunks' out-weights for PageRank (pagerank.cu).
+g1_status upload_transpose_with_outw(g1_graph* g, const uint32_t* col, const void* val, cudaStream_t s);
 // Per-vertex out-degrees (edge count, n words in the graph's workspace),
 // derived once per graph; the caller holds g->mu.
 g1_status out_degrees(g1_graph* g, uint32_t** deg, cudaStream_t s);

@@ -133,7 +133,7 @@ pr_outw_from_transpose_kernel(const uint32_t* tcol, const float* tval, uint32_t 
     __syncthreads();
     auto add = [&](uint32_t u, float w) {
         if (u < PRIV) atomicAdd(&bins[u], w);
-        else atomicAdd(&outw[u], w);
+        else if (u < n) atomicAdd(&outw[u], w);  // ids are validated after an eager upload
     };
     const uint64_t stride = (uint64_t)gridDim.x * BLOCK;
     const uint64_t m4 = m / 4;
@@ -150,6 +150,64 @@ pr_outw_from_transpose_kernel(const uint32_t* tcol, const float* tval, uint32_t 
     __syncthreads();
     for (int i = threadIdx.x; i < PRIV && i < (int)n; i += BLOCK)
         if (bins[i] != 0.0f) atomicAdd(&outw[i], bins[i]);
+}
+
+constexpr int kEagerOutwChunks = 8;
+
+// Uploads the in-edge CSR's columns and f32 values from host memory in
+// chunks on s; a second stream sums each chunk's out-weights as soon as it
+// has arrived (workspace "pr_outw", what PageRank's first call would
+// otherwise compute after the whole copy), so only the last chunk's
+// histogram is left when the copy ends.  s waits for the histograms.
+g1_status upload_transpose_with_outw(g1_graph* g, const uint32_t* col, const void* val, cudaStream_t s) {
+    Orientation& o = g->o[1];
+    const uint32_t n = g->n, m = g->m;
+    float* outw = nullptr;
+    G1_TRY(g->ws.get("pr_outw", n, &outw));
+    G1_CUDA(cudaMemsetAsync(outw, 0, (size_t)n * 4, s));
+    // chunk starts at multiples of 1024 edges: 16-byte aligned for the
+    // kernel's vector loads
+    const size_t chunk = (ceil_div((size_t)m, (size_t)kEagerOutwChunks) + 1023) & ~size_t(1023);
+    cudaStream_t h = nullptr;
+    G1_CUDA(cudaStreamCreateWithFlags(&h, cudaStreamNonBlocking));
+    cudaEvent_t ev[kEagerOutwChunks + 1] = {};
+    g1_status st = G1_OK;
+    auto check = [&](cudaError_t e, const char* what) {
+        if (st == G1_OK && e != cudaSuccess) st = fail_cuda(e, what);
+        return st == G1_OK;
+    };
+    int used = 0;
+    for (int c = 0; c < kEagerOutwChunks && st == G1_OK; ++c) {
+        const size_t lo = (size_t)c * chunk;
+        if (lo >= m) break;
+        const size_t cnt = std::min(chunk, (size_t)m - lo);
+        if (!check(cudaMemcpyAsync(o.col + lo, col + lo, cnt * 4, cudaMemcpyHostToDevice, s), "upload col"))
+            break;
+        if (!check(cudaMemcpyAsync(static_cast<char*>(o.val) + lo * 4, static_cast<const char*>(val) + lo * 4,
+                                   cnt * 4, cudaMemcpyHostToDevice, s),
+                   "upload val"))
+            break;
+        if (!check(cudaEventCreateWithFlags(&ev[c], cudaEventDisableTiming), "event")) break;
+        used = c + 1;
+        if (!check(cudaEventRecord(ev[c], s), "event record")) break;
+        if (!check(cudaStreamWaitEvent(h, ev[c], 0), "stream wait")) break;
+        pr_outw_from_transpose_kernel<8192, 1024><<<(uint32_t)g->sm_count * 2, 1024, 0, h>>>(
+            o.col + lo, static_cast<const float*>(o.val) + lo, (uint32_t)cnt, n, outw);
+        count_launches(1);
+        check(cudaGetLastError(), "pr_outw_from_transpose_kernel");
+    }
+    // s continues after the histograms, whatever happened above
+    cudaEvent_t& done = ev[kEagerOutwChunks];
+    if (check(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "event") &&
+        check(cudaEventRecord(done, h), "event record"))
+        check(cudaStreamWaitEvent(s, done, 0), "stream wait");
+    else
+        cudaStreamSynchronize(h);
+    for (int c = 0; c < used; ++c) cudaEventDestroy(ev[c]);
+    if (done) cudaEventDestroy(done);
+    cudaStreamDestroy(h);  // released once its work completes
+    if (st == G1_OK) g->outw_ready = true;
+    return st;
 }
 
 // iweights = alpha / out-weight (0 for a vertex without out-weight,
@@ -276,25 +334,32 @@ static g1_status pr_hot_layout(g1_graph* g, const float* outw, cudaStream_t s, i
     const uint32_t n = g->n, m = g->m;
     Orientation& h = g->o[2];
     uint32_t* hot = nullptr;
-    G1_TRY(g->ws.get("pr_hot", n, &hot));
     if (!h.present) {
         const uint32_t* deg = reinterpret_cast<const uint32_t*>(outw);
         DevBuf keys, ids, order, temp;
-        G1_TRY(keys.ensure((size_t)n * 4 + 16));
-        G1_TRY(ids.ensure((size_t)n * 4 + 16));
-        G1_TRY(order.ensure((size_t)n * 4 + 16));
-        // the same zeroed pad as the other column arrays
-        const size_t nz_used = (size_t)m * 4;
-        G1_TRY(h.b_col.ensure(((size_t)m + kWarpTilePad + 64) * 4));
-        G1_CUDA(cudaMemsetAsync(h.b_col.as<char>() + nz_used, 0, h.b_col.bytes - nz_used, s));
-        const uint32_t grid = (uint32_t)std::max<uint64_t>(
-            1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
-        pr_iota_kernel<<<grid, 256, 0, s>>>(ids.as<uint32_t>(), n);
         size_t tb = 0;
         G1_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, deg, keys.as<uint32_t>(),
                                                           ids.as<uint32_t>(), order.as<uint32_t>(),
                                                           (int)n, 0, 32, s));
-        G1_TRY(temp.ensure(tb + 16));
+        // all memory first: under AUTO a graph that does not fit its copy of
+        // the columns runs on the plain layout instead (same results)
+        g1_status st = g->ws.get("pr_hot", n, &hot);
+        if (st == G1_OK) st = keys.ensure((size_t)n * 4 + 16);
+        if (st == G1_OK) st = ids.ensure((size_t)n * 4 + 16);
+        if (st == G1_OK) st = order.ensure((size_t)n * 4 + 16);
+        if (st == G1_OK) st = temp.ensure(tb + 16);
+        // the same zeroed pad as the other column arrays
+        if (st == G1_OK) st = h.b_col.ensure(((size_t)m + kWarpTilePad + 64) * 4);
+        if (st != G1_OK) {
+            h.b_col.release();
+            if (st == G1_ERR_OOM && g->hot_mode == G1_HOT_COLUMNS_AUTO) return G1_OK;
+            return st;
+        }
+        const size_t nz_used = (size_t)m * 4;
+        G1_CUDA(cudaMemsetAsync(h.b_col.as<char>() + nz_used, 0, h.b_col.bytes - nz_used, s));
+        const uint32_t grid = (uint32_t)std::max<uint64_t>(
+            1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
+        pr_iota_kernel<<<grid, 256, 0, s>>>(ids.as<uint32_t>(), n);
         G1_CUDA(cub::DeviceRadixSort::SortPairsDescending(temp.p, tb, deg, keys.as<uint32_t>(),
                                                           ids.as<uint32_t>(), order.as<uint32_t>(),
                                                           (int)n, 0, 32, s));
@@ -309,6 +374,8 @@ static g1_status pr_hot_layout(g1_graph* g, const float* outw, cudaStream_t s, i
         h.val = in.val;
         h.max_deg = in.max_deg;
         h.present = true;
+    } else {
+        G1_TRY(g->ws.get("pr_hot", n, &hot));
     }
     h.tuned_sched = in.tuned_sched;
     h.tuned_variant = in.tuned_variant;
