@@ -912,7 +912,9 @@ def run_kernel_workload(name: str):
       blas_rmat20                      SSSP on RMAT-20 on the BLAS engine, 4 sources
       gather_rates                     prints the random-load rates of
                                        g1_measure_gather_rate over item size,
-                                       loads in flight, warps per SM and footprint
+                                       loads in flight, warps per SM and footprint,
+                                       and of g1_measure_smem_gather_rate (own
+                                       block / cluster-wide shared memory)
       ppr_rmat22                       single-source PPR (20 iterations, the nnz
                                        SpMV with the PPR epilogue) on RMAT-22
                                        directed, relabelled, 2 sources
@@ -938,6 +940,12 @@ def run_kernel_workload(name: str):
                 print(f"{where:4s} footprint {fp:>11,d} B  item {item:2d} B  in flight {fl:2d}  "
                       f"warps/SM {32 * bps:2d}: {r / 1e9:7.1f} G loads/s "
                       f"({r / 1e9 / sms:5.2f} G/s per SM)", flush=True)
+        for cl in (1, 2, 4, 8, 16):
+            for remote in (False, True):
+                r, blocks = g1.measure_smem_gather_rate(cl, remote)
+                print(f"smem cluster {cl:2d} {'cluster-wide' if remote else 'own block  '}: "
+                      f"{r / 1e9:7.1f} G loads/s over {blocks:3d} blocks "
+                      f"({r / 1e9 / blocks:5.2f} G/s per block)", flush=True)
         return
     if name == "ppr_rmat22":
         g = gen.rmat(22, 16, False, float_values=True, device=dev)

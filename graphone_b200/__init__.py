@@ -72,6 +72,8 @@ def _declare(L):
     L.g1_test_set_wait_polls.argtypes = [C.c_int64]
     L.g1_set_traversal_thresholds.argtypes = [P, C.c_uint32, C.c_uint32]
     L.g1_graph_set_hot_columns.argtypes = [P, C.c_int]
+    L.g1_measure_smem_gather_rate.argtypes = [C.c_uint32, C.c_int, C.POINTER(C.c_double),
+                                              C.POINTER(C.c_uint32), P]
     L.g1_measure_gather_rate.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                                          C.POINTER(C.c_double), P]
     L.g1_profile_begin.argtypes = []
@@ -126,6 +128,7 @@ EXPORTS = (
     "g1_status_string", "g1_last_error", "g1_version", "g1_mem_alloc", "g1_mem_free",
     "g1_mem_copy", "g1_release_cached_memory", "g1_mem_fill_u32", "g1_stream_sync", "g1_kernel_launches",
     "g1_count_user_launches", "g1_test_set_wait_polls", "g1_measure_gather_rate",
+    "g1_measure_smem_gather_rate",
     "g1_profile_begin", "g1_profile_end", "g1_graph_create",
     "g1_graph_destroy", "g1_graph_info", "g1_graph_arrays", "g1_graph_device_bytes",
     "g1_spmv_plan", "g1_spmv_nnz_plan", "g1_spmv", "g1_spmv_noalloc", "g1_graph_set_schedule", "g1_autotune", "g1_autotune_traversal", "g1_set_traversal_thresholds", "g1_graph_set_hot_columns", "g1_pagerank", "g1_sssp", "g1_bfs", "g1_advance_run",
@@ -173,6 +176,16 @@ def test_set_wait_polls(polls: int) -> None:
     """Lowers the poll limit of every bounded device wait (negative: the
     defaults), so that tests can make the waits run out."""
     check(lib().g1_test_set_wait_polls(polls))
+
+
+def measure_smem_gather_rate(cluster_size: int = 1, remote: bool = False, stream=None):
+    """(random 4-byte shared-memory loads per second, blocks that ran): from a
+    block's own shared memory, or from random blocks of its thread-block
+    cluster (remote); see g1_measure_smem_gather_rate."""
+    r, b = C.c_double(), C.c_uint32()
+    check(lib().g1_measure_smem_gather_rate(cluster_size, 1 if remote else 0, C.byref(r), C.byref(b),
+                                            _stream(stream)))
+    return r.value, b.value
 
 
 def measure_gather_rate(item_bytes: int = 4, in_flight: int = 8, blocks_per_sm: int = 1,

@@ -7,6 +7,8 @@
 // thread blocks and a chosen number of independent loads per thread.
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "g1/common.cuh"
 #include "internal.h"
 
@@ -86,10 +88,114 @@ g1_status probe_ilp(uint32_t in_flight, int sms, uint32_t bps, uint64_t fp, doub
     }
 }
 
+// Shared-memory gathers: each 1024-thread block (one per SM, 128 KB of
+// shared memory) fills its words, then every thread gathers `iters` x 8
+// words at hashed positions: from its own block's shared memory (REMOTE
+// false) or from a random block of its thread-block cluster (distributed
+// shared memory).  Cluster barriers before the gathers and before exit keep
+// every block's memory alive while others read it.
+constexpr uint32_t kSmemProbeWordsLog2 = 15;
+
+__device__ __forceinline__ uint32_t probe_mix(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
+template <bool REMOTE>
+__global__ void __launch_bounds__(1024, 1) smem_gather_probe_kernel(uint32_t iters, uint32_t* out) {
+    extern __shared__ uint32_t words[];
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    constexpr uint32_t kWords = 1u << kSmemProbeWordsLog2;
+    for (uint32_t i = threadIdx.x; i < kWords; i += blockDim.x) words[i] = probe_mix(i + blockIdx.x);
+    cl.sync();
+    const uint32_t c = cl.num_blocks();
+    uint32_t st = probe_mix(blockIdx.x * 1024u + threadIdx.x + 1u);
+    uint32_t acc = 0;
+    for (uint32_t it = 0; it < iters; ++it) {
+        uint32_t v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            st = probe_mix(st + (uint32_t)j + 0x9e3779b9u);
+            const uint32_t* base = REMOTE ? cl.map_shared_rank(words, (st >> 24) % c) : words;
+            v[j] = base[st & (kWords - 1)];
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc ^= v[j];
+    }
+    cl.sync();
+    out[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+
+template <bool REMOTE>
+g1_status smem_probe(uint32_t cluster, double* rate, uint32_t* blocks_out, cudaStream_t s) {
+    auto k = smem_gather_probe_kernel<REMOTE>;
+    const size_t smem = (size_t)4 << kSmemProbeWordsLog2;
+    G1_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (cluster > 8) G1_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cluster);
+    cfg.blockDim = dim3(1024);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    G1_CUDA(cudaOccupancyMaxActiveClusters(&clusters, k, &cfg));
+    if (clusters <= 0) return fail(G1_ERR_UNSUPPORTED, "g1_measure_smem_gather_rate: no cluster of that size fits");
+    const uint32_t grid = (uint32_t)clusters * cluster;  // every cluster resident at once
+    *blocks_out = grid;
+    cfg.gridDim = dim3(grid);
+    DevBuf out;
+    G1_TRY(out.ensure((size_t)grid * 1024 * 4));
+    const uint32_t iters = 256;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    G1_CUDA(cudaEventCreate(&e0));
+    G1_CUDA(cudaEventCreate(&e1));
+    const int reps = 4;
+    cudaError_t err = cudaLaunchKernelEx(&cfg, k, iters, out.as<uint32_t>());
+    if (err == cudaSuccess) err = cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && err == cudaSuccess; ++r) err = cudaLaunchKernelEx(&cfg, k, iters, out.as<uint32_t>());
+    if (err == cudaSuccess) err = cudaEventRecord(e1, s);
+    count_launches(reps + 1);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (err != cudaSuccess) return fail_cuda(err, "shared-memory gather probe");
+    const double total = (double)grid * 1024 * iters * 8 * reps;
+    *rate = ms > 0.0f ? total / ((double)ms * 1e-3) : 0.0;
+    return G1_OK;
+}
+
 }  // namespace
 }  // namespace g1
 
 using namespace g1;
+
+extern "C" g1_status g1_measure_smem_gather_rate(uint32_t cluster_size, int remote, double* gathers_per_s,
+                                                 uint32_t* blocks, void* stream) {
+    if (!gathers_per_s || (cluster_size != 1 && cluster_size != 2 && cluster_size != 4 && cluster_size != 8 &&
+                           cluster_size != 16))
+        return fail(G1_ERR_INVALID, "g1_measure_smem_gather_rate: cluster_size must be 1, 2, 4, 8 or 16");
+    *gathers_per_s = 0.0;
+    uint32_t b = 0;
+    cudaStream_t s = as_stream(stream);
+    const g1_status st = remote ? smem_probe<true>(cluster_size, gathers_per_s, &b, s)
+                                : smem_probe<false>(cluster_size, gathers_per_s, &b, s);
+    if (blocks) *blocks = b;
+    return st;
+}
 
 extern "C" g1_status g1_measure_gather_rate(uint32_t item_bytes, uint32_t in_flight, uint32_t blocks_per_sm,
                                             uint64_t footprint_bytes, double* gathers_per_s, void* stream) {

@@ -125,6 +125,17 @@ g1_status g1_test_set_wait_polls(int64_t polls);
  * measurement support. */
 g1_status g1_measure_gather_rate(uint32_t item_bytes, uint32_t in_flight, uint32_t blocks_per_sm,
                                  uint64_t footprint_bytes, double* gathers_per_s, void* stream);
+/* Random 4-byte loads served per second from shared memory, on the current
+ * device: one 1024-thread block per SM with 128 KB of shared memory, in
+ * thread-block clusters of cluster_size (1, 2, 4, 8 or 16) blocks, all
+ * resident at once; each thread gathers from its own block's shared memory
+ * (remote 0) or from a random block of its cluster (remote 1, distributed
+ * shared memory).  *blocks (may be NULL): the blocks that ran.  With the L2
+ * rate of g1_measure_gather_rate beside it, this shows whether a
+ * cluster-wide copy of the SpMV's x could serve the gathers that miss a
+ * block's own copy.  No GraphOne counterpart. */
+g1_status g1_measure_smem_gather_rate(uint32_t cluster_size, int remote, double* gathers_per_s,
+                                      uint32_t* blocks, void* stream);
 /* Kernel timing of the SpMV launches (main merge / vector kernels only):
  * between g1_profile_begin and g1_profile_end every such launch is
  * bracketed by CUDA events on its own stream; g1_profile_end synchronises

@@ -21,3 +21,21 @@ def test_gather_rates_are_ordered_by_memory_level(cuda):
 def test_gather_rate_rejects_bad_arguments(cuda, args):
     with pytest.raises(g1.G1Error):
         g1.measure_gather_rate(*args)
+
+
+def test_smem_gather_rates(cuda):
+    """g1_measure_smem_gather_rate: gathers from a block's own shared memory
+    outrun L2; distributed shared memory (another block of the cluster) is
+    measured for clusters of 2 and 16 blocks."""
+    own, blocks = g1.measure_smem_gather_rate(1, False)
+    l2 = g1.measure_gather_rate(4, 8, 1, 1 << 24)
+    assert own > l2 > 0 and blocks > 0
+    for cl in (2, 16):
+        r, b = g1.measure_smem_gather_rate(cl, True)
+        assert r > 0 and b > 0 and b % cl == 0
+
+
+@pytest.mark.parametrize("cluster", [0, 3, 32])
+def test_smem_gather_rate_rejects_bad_cluster_sizes(cuda, cluster):
+    with pytest.raises(g1.G1Error):
+        g1.measure_smem_gather_rate(cluster, True)
