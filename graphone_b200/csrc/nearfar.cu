@@ -32,13 +32,12 @@ namespace g1 {
 // per-step values rotate through three slots (step s reads slot s % 3,
 // fills slot (s+1) % 3 and resets slot (s+2) % 3).
 struct NfCtl {
+    unsigned long long bar;  // grid barrier: block arrivals so far (never reset)
     uint32_t qn[3];      // near-queue size
     uint32_t kind[3];    // 1: the step is a threshold move (after a minimum step)
     uint32_t thresh[3];  // T
     uint32_t minfar[3];  // smallest pending far distance
     uint32_t fn[2];      // far-pile sizes (double-buffered piles)
-    uint32_t bar_count;  // grid barrier
-    uint32_t bar_gen;
     uint32_t err;        // 1 = a barrier wait ran out
     uint32_t rounds;     // relax rounds
 };
@@ -63,24 +62,22 @@ constexpr uint32_t kNfSpinLimit = 1u << 23;
 
 __device__ __forceinline__ uint32_t ld_vol(const uint32_t* p) { return *(const volatile uint32_t*)p; }
 
-__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
-    uint32_t r;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(r) : "l"(p) : "memory");
-    return r;
+__device__ __forceinline__ void red_add_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
-__device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t v) {
-    uint32_t r;
-    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(r) : "l"(p), "r"(v) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long r;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(r) : "l"(p) : "memory");
     return r;
-}
-__device__ __forceinline__ void atom_add_release(uint32_t* p, uint32_t v) {
-    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Counting grid barrier: the block's writes are released by its thread 0's
-// arrival (after bar.sync), and the other blocks' writes acquired through
-// the generation word.  false if the wait ran out (the kernel then returns:
-// the host reports G1_ERR_TIMEOUT).
+// Counting grid barrier over a monotonic arrival count: barrier k (k = 1,
+// 2, ...) is passed once k * nblocks blocks have arrived.  The block's
+// writes are released by its thread 0's arrival (a fire-and-forget add,
+// after bar.sync) and the other blocks' writes acquired by the load that
+// sees the count; one word, no reset and no generation word, so a wait is
+// one polling round trip after the last arrival.  false if the wait ran
+// out (the kernel then returns: the host reports G1_ERR_TIMEOUT).
 // The control words a step reads, copied into shared memory by thread 0 of
 // each block after the barrier (one read per block instead of one per warp
 // of the same few words).
@@ -103,17 +100,13 @@ __device__ bool nf_barrier(NfCtl* c, uint32_t nblocks, uint32_t st_next, uint32_
                            uint32_t spin_limit) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        const uint32_t g0 = ld_acquire(&c->bar_gen);
-        if (atom_add_acq_rel(&c->bar_count, 1u) == nblocks - 1) {
-            c->bar_count = 0u;  // seen by the next arrivals through bar_gen
-            atom_add_release(&c->bar_gen, 1u);
-        } else {
-            uint32_t spins = 0;
-            while (ld_acquire(&c->bar_gen) == g0) {
-                if (++spins > spin_limit) {
-                    atomicOr(&c->err, 1u);
-                    break;
-                }
+        const unsigned long long target = (unsigned long long)st_next * nblocks;
+        red_add_release_u64(&c->bar, 1ull);
+        uint32_t spins = 0;
+        while (ld_acquire_u64(&c->bar) < target) {
+            if (++spins > spin_limit) {
+                atomicOr(&c->err, 1u);
+                break;
             }
         }
         nf_read_ctl(c, st_next, fp, sc);
