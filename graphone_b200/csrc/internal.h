@@ -272,9 +272,13 @@ g1_status ppr_enqueue(g1_graph* g, const PprPlan& pl, uint32_t* store, uint32_t 
 g1_status ppr_locked(g1_graph* g, uint32_t src, float alpha, uint32_t iters, float* rank_out,
                      cudaStream_t s);
 // Near-far SSSP (unit = BFS) from internal vertex src in one persistent
-// launch; *dist_out points to the graph's workspace distances.
+// launch; *dist_out points to the graph's workspace distances.  frontier:
+// no distance buckets (threshold infinite), so every round relaxes the
+// out-edges of all vertices the previous round improved -- the advance /
+// filter frontier algorithm, in one launch (for BFS the same rounds as the
+// near-far engine's levels).
 g1_status nearfar_traverse(g1_graph* g, uint32_t src, bool unit, uint32_t** dist_out, uint32_t* rounds,
-                           cudaStream_t s);
+                           cudaStream_t s, bool frontier = false);
 // The same in caller-owned buffers, enqueued only: buffers laid out in one
 // store of nearfar_words(n) words (256-byte aligned), the bucket width (mean weight based; the caller holds
 // g->mu the first time), the launch, and the outcome from a host copy of the

@@ -410,9 +410,9 @@ g1_status nearfar_result(const uint32_t* host_ctl, uint32_t* rounds) {
 uint32_t nearfar_ctl_bytes() { return (uint32_t)sizeof(NfCtl); }
 
 g1_status nearfar_traverse(g1_graph* g, uint32_t src, bool unit, uint32_t** dist_out, uint32_t* rounds,
-                           cudaStream_t s) {
-    uint32_t delta = 1;
-    G1_TRY(nearfar_delta(g, unit, s, &delta));
+                           cudaStream_t s, bool frontier) {
+    uint32_t delta = kU32Max;  // frontier: the first threshold is already infinite
+    if (!frontier) G1_TRY(nearfar_delta(g, unit, s, &delta));
     uint32_t* store = nullptr;
     G1_TRY(g->ws.get("nf_store", nearfar_words(g->n), &store));
     NfBuffers b;

@@ -805,11 +805,21 @@ static g1_status traverse(g1_graph* g, uint32_t src_caller, g1_engine engine, ui
     uint32_t src = src_caller;
     G1_TRY(internal_vertex(g, src_caller, &src, s));
     if (engine == G1_ENGINE_AUTO && nearfar_suits(g)) engine = G1_ENGINE_NEARFAR;
-    if (engine == G1_ENGINE_NEARFAR) {
+    // BFS on the advance engine on graphs of small uniform degree (grids,
+    // meshes): thousands of small frontiers, so one persistent launch whose
+    // rounds are the advance/filter steps (every vertex the last round
+    // reached pushes its out-edges; the newly reached ones, once each, form
+    // the next frontier), separated by a grid barrier instead of launches:
+    // 4096^2 grid 57-63 -> 35 ms.  Not for SSSP: without distance buckets,
+    // Bellman-Ford's correction waves make large frontiers, where the
+    // edge-balanced push of the captured steps below is faster (745 against
+    // 314 ms on that grid).
+    const bool frontier = UNIT && engine == G1_ENGINE_ADVANCE && nearfar_suits(g);
+    if (engine == G1_ENGINE_NEARFAR || frontier) {
         if (!UNIT && g->vtype != G1_U32) return fail(G1_ERR_INVALID, "SSSP needs u32 edge weights");
         uint32_t* dist = nullptr;
         uint32_t rounds = 0;
-        G1_TRY(nearfar_traverse(g, src, UNIT, &dist, &rounds, s));
+        G1_TRY(nearfar_traverse(g, src, UNIT, &dist, &rounds, s, frontier));
         if (iters_out) *iters_out = rounds;
         G1_TRY(copy_out_vertices(g, out, dist, s));
         return check_device_error(g, s);

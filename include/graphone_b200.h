@@ -55,7 +55,8 @@ typedef enum {
     G1_ENGINE_BLAS = 0,    /* pull SpMV per iteration (BlasGcEngine, sparse frontier);
                               from 2^20 edges, steps whose frontier is small are computed
                               from the frontier's out-edges (same results) */
-    G1_ENGINE_ADVANCE = 1, /* push advance/filter (AdvanceGC) */
+    G1_ENGINE_ADVANCE = 1, /* push advance/filter (AdvanceGC); BFS on graphs of small uniform
+                              degree runs its rounds in one persistent launch */
     G1_ENGINE_AUTO = 2,    /* near-far on graphs of small uniform degree; else push while
                               the frontier is small and pull when it is large (below 2^24
                               edges: the BLAS engine with its sparse steps) */
