@@ -896,7 +896,7 @@ def run_reference(args):
 
 KERNEL_WORKLOADS = ("slot_sssp", "slot_bfs", "slot_ppr", "nearfar", "advance_grid", "advance_lb",
                     "blas_rmat20", "gather_rates", "ppr_rmat22", "blas_sparse_rmat22",
-                    "pagerank_e2e_rmat22")
+                    "pagerank_e2e_rmat22", "ppr_grid1024")
 
 
 def run_kernel_workload(name: str):
@@ -921,6 +921,9 @@ def run_kernel_workload(name: str):
       blas_sparse_rmat22               SSSP on RMAT-22 symmetric (relabelled) on
                                        the BLAS engine, whose small-frontier
                                        steps are sparse steps, 2 sources
+      ppr_grid1024                     single-source PPR (20 iterations) from 2
+                                       sources of the 1024^2 grid: every step a
+                                       sparse step
       pagerank_e2e_rmat22              the end-to-end step at 2 iterations: a new
                                        graph from the pinned host in-edge CSR of
                                        RMAT-22 (caller order), PageRank (setup:
@@ -969,6 +972,14 @@ def run_kernel_workload(name: str):
                                   validate=False)
             G.pagerank(0.85, 2, g1.PR_DANGLING, out=h_out.numpy())
             G.close()
+        torch.cuda.synchronize()
+        print("kernel workload", name, "done", flush=True)
+        return
+    if name == "ppr_grid1024":
+        g = gen.grid2d(1024, 1024, (1, 100), device=dev)
+        G = g1.Graph.from_gen(g)
+        for s in gen.pick_sources(g, 2):
+            G.ppr(int(s), 0.85, 20)
         torch.cuda.synchronize()
         print("kernel workload", name, "done", flush=True)
         return
