@@ -284,7 +284,8 @@ g1_status nearfar_traverse(g1_graph* g, uint32_t src, bool unit, uint32_t** dist
 // g->mu the first time), the launch, and the outcome from a host copy of the
 // control block (nearfar_ctl_bytes() bytes at NfBuffers::ctl).
 struct NfBuffers {
-    uint32_t *dist, *stamp, *fstamp, *near[2], *far[2], *ctl;
+    unsigned long long* key;  // per vertex: distance << 32 | tag of its last improvement
+    uint32_t *dist, *near[2], *far[2], *ctl;
 };
 size_t nearfar_words(uint32_t n);  // 4-byte words of one store
 void nearfar_layout(uint32_t n, uint32_t* store, NfBuffers* b);

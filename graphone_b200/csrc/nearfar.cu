@@ -9,7 +9,7 @@
 //     near queue; a relax round pushes every near vertex's out-edges
 //     (atomicMin); improved vertices below T join the next near queue,
 //     the others the far pile (each vertex at most once per queue and per
-//     bucket, by stamps);
+//     bucket, by the tag kept beside its distance);
 //   * when the near queue runs dry, T moves to (smallest pending distance)
 //     + delta and the far pile is split into the new near queue and the
 //     rest; entries below the old T are stale and dropped.
@@ -42,15 +42,24 @@ struct NfCtl {
     uint32_t rounds;     // relax rounds
 };
 
+// Per vertex one 64-bit key: the tentative distance in the high half, in the
+// low half the tag of its last improvement, 2 * round + (1 if it went to the
+// far pile).  One atomicMin on the key both improves the distance and
+// returns whether the vertex was already queued this round (same round, near
+// tag) or is already on the current far pile (a tag from this bucket): no
+// second, dependent atomic on a separate stamp array.
+__device__ __forceinline__ unsigned long long nf_key(uint32_t d, uint32_t tag) {
+    return ((unsigned long long)d << 32) | tag;
+}
+
 struct NfArgs {
     const uint32_t* rp;
     const uint32_t* col;
     const uint32_t* val;
     uint32_t n;
     uint32_t delta;
-    uint32_t* dist;
-    uint32_t* stamp;   // near-queue generation a vertex was queued in
-    uint32_t* fstamp;  // bucket a vertex was put on the far pile in
+    unsigned long long* key;  // distance << 32 | tag
+    uint32_t* dist;           // the distances, written at the end
     uint32_t* near[2];
     uint32_t* far[2];
     NfCtl* ctl;
@@ -61,6 +70,9 @@ struct NfArgs {
 constexpr uint32_t kNfSpinLimit = 1u << 23;
 
 __device__ __forceinline__ uint32_t ld_vol(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+__device__ __forceinline__ uint32_t ld_dist(const unsigned long long* key) {
+    return (uint32_t)(*(const volatile unsigned long long*)key >> 32);
+}
 
 __device__ __forceinline__ void red_add_release_u64(unsigned long long* p, unsigned long long v) {
     asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
@@ -116,15 +128,12 @@ __device__ bool nf_barrier(NfCtl* c, uint32_t nblocks, uint32_t st_next, uint32_
 }
 
 // src is an internal vertex id, or a caller id mapped through perm.
-__global__ void nf_init_kernel(uint32_t n, uint32_t src, const uint32_t* perm, uint32_t t0, uint32_t* dist,
-                               uint32_t* stamp, uint32_t* fstamp, uint32_t* near0, NfCtl* ctl) {
+__global__ void nf_init_kernel(uint32_t n, uint32_t src, const uint32_t* perm, uint32_t t0,
+                               unsigned long long* key, uint32_t* near0, NfCtl* ctl) {
     if (perm) src = perm[src];
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
-        dist[v] = v == src ? 0u : kU32Max;
-        stamp[v] = 0u;
-        fstamp[v] = 0u;
-    }
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        key[v] = nf_key(v == src ? 0u : kU32Max, 0u);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         near0[0] = src;
         NfCtl c{};
@@ -149,8 +158,8 @@ __device__ __forceinline__ uint32_t agg_slot(uint32_t* ctr) {
 
 // TPV lanes per near-queue item (1..32, the power of two at or above the
 // graph's mean degree): a step's edges then run about one per thread, where
-// one lane per item would chain its items' edges (each an atomicMin, a stamp
-// and an append) one after another.  Lists of 32 or more edges are pushed by
+// one lane per item would chain its items' edges (each an atomicMin and an
+// append) one after another.  Lists of 32 or more edges are pushed by
 // the whole warp.
 template <bool UNIT, int TPV>
 __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
@@ -159,8 +168,8 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
     const uint32_t gs = gridDim.x * blockDim.x;
     NfCtl* c = a.ctl;
     uint32_t par = 0, fp = 0;
-    uint32_t gen = 1;     // near-queue generation (stamp)
-    uint32_t bucket = 1;  // far-pile bucket (fstamp)
+    uint32_t gen = 1;      // round number (every step counts one)
+    uint32_t bucket = 1;   // tags from here on belong to the current far pile's bucket
     __shared__ NfStepCtl sc;
     if (threadIdx.x == 0) nf_read_ctl(c, 0, 0, &sc);
     __syncthreads();
@@ -189,17 +198,24 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
             const uint32_t* in = a.near[par];
             uint32_t* outq = a.near[par ^ 1];
             uint32_t* farq = a.far[fp];
+            const uint32_t near_tag = 2u * gen;
             auto relax = [&](uint32_t du, uint32_t e) {
                 const uint32_t v = a.col[e];
                 const uint32_t nd = du + (UNIT ? 1u : a.val[e]);
                 // no plain pre-check: one dependent memory access fewer on the
                 // critical path of a step
-                if (nd >= atomicMin(a.dist + v, nd)) return;
-                if (nd < T) {
-                    // BFS: every improvement in a step sets the same level, so
-                    // only the first one succeeds -- no duplicate to stamp
-                    if (UNIT || atomicExch(a.stamp + v, gen) != gen) outq[agg_slot(&c->qn[nxt])] = v;
-                } else if (atomicExch(a.fstamp + v, bucket) != bucket) {
+                const bool is_near = nd < T;
+                const unsigned long long old = atomicMin(a.key + v, nf_key(nd, near_tag + (is_near ? 0u : 1u)));
+                if (nd >= (uint32_t)(old >> 32)) return;
+                const uint32_t tag = (uint32_t)old;
+                if (is_near) {
+                    // queued once per round (BFS: every improvement in a round
+                    // sets the same level, so only the first one succeeds); a
+                    // vertex that went to the far pile earlier in the round
+                    // still joins the near queue
+                    if (UNIT || tag != near_tag) outq[agg_slot(&c->qn[nxt])] = v;
+                } else if (tag < 2u * bucket) {
+                    // not on the current far pile yet
                     farq[agg_slot(&c->fn[fp])] = v;
                 }
             };
@@ -214,7 +230,7 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
                 uint32_t du = 0, b = 0, e1 = 0;
                 if (i < qn) {
                     const uint32_t u = in[i];
-                    du = ld_vol(a.dist + u);
+                    du = ld_dist(a.key + u);
                     b = a.rp[u];
                     e1 = a.rp[u + 1];
                 }
@@ -235,7 +251,7 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
             uint32_t mn = kU32Max;
             const uint32_t* fin = a.far[fp];
             for (uint32_t i = gt; i < fn; i += gs) {
-                const uint32_t d = ld_vol(a.dist + fin[i]);
+                const uint32_t d = ld_dist(a.key + fin[i]);
                 if (d >= T) mn = min(mn, d);
             }
 #pragma unroll
@@ -255,17 +271,22 @@ __global__ void __launch_bounds__(1024, 1) nf_kernel(NfArgs a) {
             }
             if (gt == 0) c->thresh[nxt] = tn;
             ++gen;
-            ++bucket;
+            // the new bucket's far pile starts here: a vertex carried over is
+            // tagged into it, so the next rounds do not add it again
+            bucket = gen;
             const uint32_t* fin = a.far[fp];
             uint32_t* fout = a.far[fp ^ 1];
             uint32_t* outq = a.near[par ^ 1];
+            // every vertex is on the pile at most once and no relaxation runs
+            // in this step: plain loads and stores of the keys
             for (uint32_t i = gt; i < fn; i += gs) {
                 const uint32_t v = fin[i];
-                const uint32_t d = ld_vol(a.dist + v);
+                const uint32_t d = ld_dist(a.key + v);
                 if (d < T) continue;
                 if (d < tn) {
-                    if (atomicExch(a.stamp + v, gen) != gen) outq[agg_slot(&c->qn[nxt])] = v;
-                } else if (atomicExch(a.fstamp + v, bucket) != bucket) {
+                    outq[agg_slot(&c->qn[nxt])] = v;
+                } else {
+                    a.key[v] = nf_key(d, 2u * bucket + 1u);
                     fout[agg_slot(&c->fn[fp ^ 1])] = v;
                 }
             }
@@ -325,16 +346,22 @@ g1_status nearfar_delta(g1_graph* g, bool unit, cudaStream_t s, uint32_t* out) {
     return G1_OK;
 }
 
+// The distances out of the keys.
+__global__ void nf_dist_kernel(const unsigned long long* key, uint32_t n, uint32_t* dist) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        dist[v] = (uint32_t)(key[v] >> 32);
+}
+
 size_t nearfar_words(uint32_t n) {
-    // dist, stamp, fstamp; two near queues and two far piles (each vertex at
-    // most once in each); the control block (16-byte aligned)
+    // keys (8 bytes each), distances; two near queues and two far piles
+    // (each vertex at most once in each); the control block (16-byte aligned)
     return 3 * (size_t)n + 4 * ((size_t)n + 1) + sizeof(NfCtl) / 4 + 8;
 }
 
 void nearfar_layout(uint32_t n, uint32_t* p, NfBuffers* b) {
-    b->dist = p;
-    b->stamp = p + n;
-    b->fstamp = p + 2 * (size_t)n;
+    b->key = reinterpret_cast<unsigned long long*>(p);  // the store is 256-byte aligned
+    b->dist = p + 2 * (size_t)n;
     uint32_t* q = p + 3 * (size_t)n;
     b->near[0] = q;
     b->near[1] = q + (n + 1);
@@ -356,9 +383,8 @@ g1_status nearfar_launch(const g1_graph* g, uint32_t src, bool unit, uint32_t de
     a.val = static_cast<const uint32_t*>(o.val);
     a.n = n;
     a.delta = delta;
+    a.key = b.key;
     a.dist = b.dist;
-    a.stamp = b.stamp;
-    a.fstamp = b.fstamp;
     a.near[0] = b.near[0];
     a.near[1] = b.near[1];
     a.far[0] = b.far[0];
@@ -369,8 +395,7 @@ g1_status nearfar_launch(const g1_graph* g, uint32_t src, bool unit, uint32_t de
         1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
     // BFS: a threshold above every level -- each step is one level and the
     // far pile stays empty
-    nf_init_kernel<<<gi, 256, 0, s>>>(n, src, perm, unit ? kU32Max : a.delta, a.dist, a.stamp, a.fstamp,
-                                      a.near[0], a.ctl);
+    nf_init_kernel<<<gi, 256, 0, s>>>(n, src, perm, unit ? kU32Max : a.delta, a.key, a.near[0], a.ctl);
     count_launches(1);
     G1_CUDA(cudaGetLastError());
     // every block of a cooperative launch is resident, so the grid barrier
@@ -395,7 +420,9 @@ g1_status nearfar_launch(const g1_graph* g, uint32_t src, bool unit, uint32_t de
     if (per_sm < 1) return fail(G1_ERR_UNSUPPORTED, "near-far engine: kernel does not fit an SM");
     void* params[] = {&a};
     G1_CUDA(cudaLaunchCooperativeKernel(fn, dim3((uint32_t)g->sm_count), dim3(1024), params, 0, s));
-    count_launches(1);
+    nf_dist_kernel<<<gi, 256, 0, s>>>(a.key, n, a.dist);
+    count_launches(2);
+    G1_CUDA(cudaGetLastError());
     return G1_OK;
 }
 
