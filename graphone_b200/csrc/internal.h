@@ -262,6 +262,10 @@ struct PprPlan {
     const uint32_t* out_col = nullptr;
     unsigned long long sparse_limit = 0;
     uint32_t sparse_steps = 0;  // the steps that may be sparse (the first ones)
+    // the in-edge CSR the SpMV runs on: 1, or its hot-column copy 2 with x
+    // stored by hot id (xperm: vertex -> hot id)
+    int t = 1;
+    const uint32_t* xperm = nullptr;
 };
 size_t ppr_state_words(uint32_t n, const NnzPlan* plan);
 g1_status ppr_prepare(g1_graph* g, cudaStream_t s, PprPlan* out);

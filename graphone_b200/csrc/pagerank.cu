@@ -317,34 +317,39 @@ __global__ void pr_hot_cols_kernel(const uint32_t* col, uint32_t m, const uint32
 }
 
 constexpr uint32_t kHotLayoutMinEdges = 1u << 22;
+constexpr uint32_t kHotLayoutMinMaxDegree = 64;
 
 // Builds orientation 2 and the hot ids (workspace "pr_hot") if the graph
-// qualifies, ordering by outw (non-negative floats: their bits sort as
-// unsigned integers); *t the orientation PageRank runs on.  Caller holds
-// g->mu.
-static g1_status pr_hot_layout(g1_graph* g, const float* outw, cudaStream_t s, int* t,
+// qualifies, ordering by `keys` (PageRank: the out-weights, non-negative
+// floats whose bits sort as unsigned integers; personalized PageRank: the
+// out-degrees); *t the orientation the SpMV runs on.  A layout built by one
+// serves the other (any order gives the same results).  Caller holds g->mu.
+static g1_status pr_hot_layout(g1_graph* g, const uint32_t* keys, cudaStream_t s, int* t,
                                const uint32_t** xperm) {
     *t = 1;
     *xperm = nullptr;
     const Orientation& in = g->o[1];
     if (g->hot_mode == G1_HOT_COLUMNS_OFF) return G1_OK;
+    // AUTO: large graphs in the caller's order with skewed degrees (where a
+    // few vertices take most gathers; on a grid every vertex is as hot)
     if (g->hot_mode == G1_HOT_COLUMNS_AUTO &&
-        (g->relabeled || g->m < kHotLayoutMinEdges || resolve_schedule(g, 1, G1_SCHED_AUTO) == G1_SCHED_VECTOR))
+        (g->relabeled || g->m < kHotLayoutMinEdges || in.max_deg <= kHotLayoutMinMaxDegree ||
+         resolve_schedule(g, 1, G1_SCHED_AUTO) == G1_SCHED_VECTOR))
         return G1_OK;
     const uint32_t n = g->n, m = g->m;
     Orientation& h = g->o[2];
     uint32_t* hot = nullptr;
     if (!h.present) {
-        const uint32_t* deg = reinterpret_cast<const uint32_t*>(outw);
-        DevBuf keys, ids, order, temp;
+        const uint32_t* deg = keys;
+        DevBuf sorted, ids, order, temp;
         size_t tb = 0;
-        G1_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, deg, keys.as<uint32_t>(),
+        G1_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, deg, sorted.as<uint32_t>(),
                                                           ids.as<uint32_t>(), order.as<uint32_t>(),
                                                           (int)n, 0, 32, s));
         // all memory first: under AUTO a graph that does not fit its copy of
         // the columns runs on the plain layout instead (same results)
         g1_status st = g->ws.get("pr_hot", n, &hot);
-        if (st == G1_OK) st = keys.ensure((size_t)n * 4 + 16);
+        if (st == G1_OK) st = sorted.ensure((size_t)n * 4 + 16);
         if (st == G1_OK) st = ids.ensure((size_t)n * 4 + 16);
         if (st == G1_OK) st = order.ensure((size_t)n * 4 + 16);
         if (st == G1_OK) st = temp.ensure(tb + 16);
@@ -360,7 +365,7 @@ static g1_status pr_hot_layout(g1_graph* g, const float* outw, cudaStream_t s, i
         const uint32_t grid = (uint32_t)std::max<uint64_t>(
             1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
         pr_iota_kernel<<<grid, 256, 0, s>>>(ids.as<uint32_t>(), n);
-        G1_CUDA(cub::DeviceRadixSort::SortPairsDescending(temp.p, tb, deg, keys.as<uint32_t>(),
+        G1_CUDA(cub::DeviceRadixSort::SortPairsDescending(temp.p, tb, deg, sorted.as<uint32_t>(),
                                                           ids.as<uint32_t>(), order.as<uint32_t>(),
                                                           (int)n, 0, 32, s));
         pr_hot_rank_kernel<<<grid, 256, 0, s>>>(order.as<uint32_t>(), n, hot);
@@ -416,7 +421,7 @@ static g1_status pr_setup(g1_graph* g, float alpha, PrBuffers& b, uint32_t* grid
         G1_CUDA(cudaGetLastError());
         g->outw_ready = true;
     }
-    G1_TRY(pr_hot_layout(g, outw, s, &b.t, &b.xperm));
+    G1_TRY(pr_hot_layout(g, reinterpret_cast<const uint32_t*>(outw), s, &b.t, &b.xperm));
     const int t = b.t;
     G1_TRY((merge_grids<PlusTimesF32, PrEpilogue>(g, t, &grids[0], &grids[1])));
     grids[2] = vector_grid<PlusTimesF32, PrEpilogue>(g);
@@ -500,6 +505,9 @@ struct PprEpilogue {
     // sparse steps: the word that says this iteration is one (its kernels
     // then return at once), or null
     const uint32_t* sparse_now = nullptr;
+    // hot-column layout: x is stored by hot id (row v's entry at xperm[v]);
+    // null: by vertex id
+    const uint32_t* xperm = nullptr;
 
     uint32_t src;
     float tele;
@@ -512,16 +520,22 @@ struct PprEpilogue {
         src = *src_p;
         tele = (float)((1.0 - alpha) + alpha * ((double)(*dang_in) / kDangScale));
         if (src_rows && blockIdx.x == 0 && threadIdx.x == 0 && src_rows[src] == src_rows[src + 1])
-            emit_prepared(src, 0.0f, iw[src]);
+            emit_prepared(src, 0.0f, prepare(src));
     }
+    struct Pre {
+        float w;
+        uint32_t xi;
+    };
     __device__ __forceinline__ void emit(uint32_t v, const float& y) {
         emit_prepared(v, y, prepare(v));
     }
-    __device__ __forceinline__ float prepare(uint32_t v) const { return __ldg(iw + v); }
-    __device__ __forceinline__ void emit_prepared(uint32_t v, const float& y, float w) {
+    __device__ __forceinline__ Pre prepare(uint32_t v) const {
+        return Pre{__ldg(iw + v), xperm ? __ldg(xperm + v) : v};
+    }
+    __device__ __forceinline__ void emit_prepared(uint32_t v, const float& y, const Pre& p) {
         const float r = v == src ? y + tele : y;
         if (write_rank) rank_next[v] = r;
-        if (w != 0.0f) x_next[v] = r * w;
+        if (p.w != 0.0f) x_next[p.xi] = r * p.w;
         else dang_local += dang_fixed(r);
     }
     template <int BLOCK>
@@ -541,11 +555,11 @@ __global__ void ppr_iw_kernel(const uint32_t* deg, uint32_t n, double alpha, flo
 // rank0 = e_src, x0 = rank0 * iw, the dangling sum of rank0 (fixed point:
 // 1.0 is 2^56); x0 and x1 are zero elsewhere (cleared by the caller).
 __global__ void ppr_init_kernel(const uint32_t* perm, uint32_t src, const float* iw, uint32_t* src_out,
-                                float* rank0, float* x0, unsigned long long* dang) {
+                                float* rank0, float* x0, unsigned long long* dang, const uint32_t* xperm) {
     const uint32_t v = perm ? perm[src] : src;
     *src_out = v;
     rank0[v] = 1.0f;
-    x0[v] = iw[v];
+    x0[xperm ? xperm[v] : v] = iw[v];
     dang[0] = iw[v] == 0.0f ? (1ull << 56) : 0ull;
     dang[1] = 0ull;
     dang[2] = 0ull;
@@ -581,6 +595,7 @@ struct PprSparse {
     const uint32_t* out_rp;
     const uint32_t* out_col;
     const uint32_t* in_rp;
+    const uint32_t* xperm;  // hot-column layout: row v's x entry at xperm[v]; null: at v
     unsigned long long limit;
 };
 
@@ -617,7 +632,10 @@ ppr_sparse_expand_kernel(PprSparse sp, uint32_t it, const uint32_t* src_p, uint3
     {
         const uint32_t zi = (fi + 2) % 3;
         const uint32_t nz = sp.ctl[4 + zi];
-        for (uint64_t i = tid; i < nz; i += threads) x_next[sp.list[zi][i]] = 0.0f;
+        for (uint64_t i = tid; i < nz; i += threads) {
+            const uint32_t v = sp.list[zi][i];
+            x_next[sp.xperm ? sp.xperm[v] : v] = 0.0f;
+        }
     }
     if (threadIdx.x < 2) smax[threadIdx.x] = 0u;
     __syncthreads();
@@ -716,7 +734,7 @@ ppr_sparse_rows_kernel(PprSparse sp, uint32_t it, const uint32_t* in_col, const 
             const float r = v == src ? acc + tele : acc;
             if (write_rank) rank_next[v] = r;
             const float w = iw[v];
-            if (w != 0.0f) x_next[v] = r * w;
+            if (w != 0.0f) x_next[sp.xperm ? sp.xperm[v] : v] = r * w;
             else dl += dang_fixed(r);
         }
     }
@@ -785,6 +803,9 @@ g1_status ppr_prepare(g1_graph* g, cudaStream_t s, PprPlan* out) {
     G1_TRY(out_degrees(g, &deg, s));
     out->deg = deg;
     out->plan = nullptr;
+    // the SpMV on the hot-column copy of the in-edge CSR where it applies
+    // (a graph kept in the caller's order), x by hot id
+    G1_TRY(pr_hot_layout(g, deg, s, &out->t, &out->xperm));
     if (resolve_schedule(g, 1, G1_SCHED_AUTO) != G1_SCHED_VECTOR) {
         NnzPlan* p = nullptr;
         G1_TRY(ensure_nnz_plan(g, 1, &p));
@@ -811,7 +832,7 @@ g1_status ppr_prepare(g1_graph* g, cudaStream_t s, PprPlan* out) {
 g1_status ppr_enqueue(g1_graph* g, const PprPlan& pl, uint32_t* store, uint32_t src, float alpha,
                       uint32_t iters, const uint32_t* perm, cudaStream_t s, const float** rank_out) {
     const uint32_t n = g->n;
-    const int t = 1;
+    const int t = pl.t;  // 1, or the hot-column copy 2 (same rows, plans and values)
     const PprLayout L = ppr_layout(n, pl.plan, store);
     const uint32_t grid = (uint32_t)std::max<uint64_t>(
         1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
@@ -819,7 +840,7 @@ g1_status ppr_enqueue(g1_graph* g, const PprPlan& pl, uint32_t* store, uint32_t 
     G1_CUDA(cudaMemsetAsync(L.x[0], 0, (size_t)n * 4, s));
     G1_CUDA(cudaMemsetAsync(L.x[1], 0, (size_t)n * 4, s));
     if (iters == 0) G1_CUDA(cudaMemsetAsync(L.rank[0], 0, (size_t)n * 4, s));
-    ppr_init_kernel<<<1, 1, 0, s>>>(perm, src, L.iw, L.src, L.rank[0], L.x[0], L.dang);
+    ppr_init_kernel<<<1, 1, 0, s>>>(perm, src, L.iw, L.src, L.rank[0], L.x[0], L.dang, pl.xperm);
     count_launches(2);
     G1_CUDA(cudaGetLastError());
     PprSparse sp{};
@@ -831,6 +852,7 @@ g1_status ppr_enqueue(g1_graph* g, const PprPlan& pl, uint32_t* store, uint32_t 
         sp.out_rp = pl.out_rp;
         sp.out_col = pl.out_col;
         sp.in_rp = g->o[t].rp;
+        sp.xperm = pl.xperm;
         sp.limit = pl.sparse_limit;
         // F0 = {src} (ctl[4] = 1), the other counts, sums, flags and bits zero
         G1_CUDA(cudaMemsetAsync(L.ctl, 0, 32 * 4, s));
@@ -865,6 +887,7 @@ g1_status ppr_enqueue(g1_graph* g, const PprPlan& pl, uint32_t* store, uint32_t 
         e.alpha = (double)alpha;
         e.write_rank = last ? 1 : 0;
         e.sparse_now = sparse_it ? L.ctl + 1 : nullptr;
+        e.xperm = pl.xperm;
         if (!pl.plan) {
             G1_TRY((launch_vector<PlusPatternF32>(g, t, L.x[cur], e, s)));
             continue;

@@ -275,9 +275,11 @@ g1_status g1_set_traversal_thresholds(g1_graph* g, uint32_t push_div, uint32_t s
  * decreasing out-degree), into a copy of the column array (4 bytes per edge
  * more on the device, built on the first call, about 0.5 ms on 65 M edges)
  * and keeps x in that order.  Each row's nonzeros keep their order: the ranks
- * are the same bits either way.  AUTO (the default): on graphs of 2^22 edges
- * or more that are not relabelled and not on the CSR-vector schedule; OFF:
- * never; ON: always.  No GraphOne counterpart. */
+ * are the same bits either way.  g1_ppr uses the same copy (built by it
+ * first, the order is by out-degree).  AUTO (the default): on graphs of 2^22
+ * edges or more that are not relabelled, have a row of more than 64 in-edges
+ * (skewed degrees) and are not on the CSR-vector schedule; OFF: never; ON:
+ * always.  No GraphOne counterpart. */
 typedef enum {
     G1_HOT_COLUMNS_AUTO = 0,
     G1_HOT_COLUMNS_OFF = 1,

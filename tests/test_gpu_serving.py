@@ -122,6 +122,38 @@ def test_ppr_sparse_steps_match_oracle(cuda, name, sched):
         assert np.array_equal(G.ppr(src, 0.85, 20), r), src
 
 
+@pytest.mark.parametrize("name", ["rmat16_sym", "rmat17_dir"])
+def test_ppr_hot_columns_same_bits(cuda, name):
+    """g1_ppr on the hot-column copy of the in-edge CSR (x stored by hot id,
+    the full SpMV and the sparse steps) gives the same bits as on the plain
+    layout, whichever of PageRank and PPR built the copy."""
+    g = SPARSE_GRAPHS[name]()
+    plain = g1.Graph.from_gen(g)
+    hot = g1.Graph.from_gen(g)
+    plain.set_hot_columns(g1.HOT_COLUMNS_OFF)
+    hot.set_hot_columns(g1.HOT_COLUMNS_ON)
+    srcs = [int(s) for s in gen.pick_sources(g, 4)]
+    for sched in (g1.SCHED_MERGE, g1.SCHED_VECTOR):
+        for G in (plain, hot):
+            G.set_schedule(sched, g1.DEFAULT_MERGE_VARIANT)
+        for src in srcs:
+            for iters in (1, 3, 20):
+                a = plain.ppr(src, 0.85, iters)
+                b = hot.ppr(src, 0.85, iters)
+                assert np.array_equal(a, b), (sched, src, iters)
+        assert O.rel_l1(b, ppr_oracle(g, srcs[-1])) < PPR_TOL
+    # a copy built by PageRank (out-weight order; the same edges with f32
+    # values, which PPR does not read) serves PPR as well
+    if not g.symmetric:
+        gf = gen.rmat(17, 16, False, (1, 64), float_values=True)
+        assert gf.m == g.m
+        pr = g1.Graph.from_gen(gf)
+        pr.set_hot_columns(g1.HOT_COLUMNS_ON)
+        pr.pagerank(0.85, 2, g1.PR_DANGLING)
+        plain.set_schedule(g1.SCHED_AUTO, g1.DEFAULT_MERGE_VARIANT)
+        assert np.array_equal(pr.ppr(srcs[0], 0.85, 20), plain.ppr(srcs[0], 0.85, 20))
+
+
 def test_ppr_zero_iterations_is_the_indicator(cuda):
     g = GRAPHS["rmat10_sym"]
     G = g1.Graph.from_gen(g)
