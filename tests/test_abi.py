@@ -84,3 +84,29 @@ def test_python_variant_table_matches_the_launcher():
     assert len(g1.MERGE_VARIANTS) == n == len(kinds)
     assert tuple(names[k] for k in kinds) == g1.MERGE_VARIANTS
     assert g1.DEFAULT_MERGE_VARIANT == d
+
+
+def test_size_and_argument_limits_are_refused_before_any_device_work():
+    """n + m at or above 2^32 - 1 (the u32 ids and offsets), an unknown
+    hot-column mode, and probe arguments out of range: each is refused with
+    G1_ERR_INVALID by the argument checks, before any CUDA call."""
+    import numpy as np
+    L = g1.lib()
+    rp = np.zeros(2, np.uint32)
+    ci = np.zeros(1, np.uint32)
+    val = np.zeros(1, np.uint32)
+    out = C.c_void_p()
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    st = L.g1_graph_create(p(rp), p(ci), p(val), 0, 0xFFFFFFFF - 5, 5, 0, None, C.byref(out))
+    assert st == 1 and out.value is None
+    assert b"2^32" in L.g1_last_error()
+    st = L.g1_graph_create(p(rp), p(ci), p(val), 7, 1, 1, 0, None, C.byref(out))
+    assert st == 1 and b"value type" in L.g1_last_error()
+    fake = C.c_void_p(16)  # never dereferenced: the mode check comes first
+    assert L.g1_graph_set_hot_columns(fake, 3) == 1
+    assert L.g1_graph_set_hot_columns(None, 0) == 1
+    r, b = C.c_double(), C.c_uint32()
+    for cl in (0, 3, 32):
+        assert L.g1_measure_smem_gather_rate(cl, 1, C.byref(r), C.byref(b), None) == 1
+    assert L.g1_measure_gather_rate(8, 8, 1, 1 << 24, C.byref(r), None) == 1
+    assert L.g1_measure_gather_rate(4, 8, 1, 1000, C.byref(r), None) == 1
