@@ -166,3 +166,49 @@ def test_loader_matches_graphone_loader_and_oracle(driver, tmp_path, case, flags
             assert g[:2] == r[:2]
             for a, b in zip(g[2:], r[2:]):
                 assert np.array_equal(a, b)
+
+
+def run_threads(driver, path, flags, threads):
+    env = dict(os.environ, G1_LOADER_THREADS=str(threads))
+    r = subprocess.run([driver, path, *("1" if f else "0" for f in flags)], capture_output=True, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return r.stdout
+
+
+@pytest.mark.parametrize("flags", [(True, False, False, False), (False, True, False, False),
+                                   (True, True, True, True)],
+                         ids=lambda f: "".join("dRsD"[i] if x else "-" for i, x in enumerate(f)))
+def test_parallel_read_of_a_large_file_equals_the_one_thread_read(driver, tmp_path, flags):
+    """A file of several MiB is parsed by several threads (parts cut at line
+    ends) and its duplicates merged by a parallel stable sort: the output,
+    warnings included, is the same bytes as with one thread, and matches the
+    restated reading rules.  Duplicates with different weights check that
+    the first one in file order keeps its weight either way."""
+    rng = np.random.default_rng(11)
+    body = random_adj(rng, 200_000, 400_000).split("\n")
+    # comments, blank lines, one-token lines (a warning each) and
+    # conflicting duplicates, spread over the file (and so over the parts)
+    extra = ["% comment", "", "   ", "12345", "7 8 1", "7 8 2", "8 7 3"]
+    for k, pos in enumerate(rng.integers(0, len(body), 400)):
+        body.insert(int(pos), extra[k % len(extra)])
+    text = "\n".join(body) + "\n"
+    path = str(tmp_path / "large.adj")
+    with open(path, "w") as f:
+        f.write(text)
+    assert len(text) > 6 << 20
+    one = run_threads(driver, path, flags, 1)
+    many = run_threads(driver, path, flags, 6)
+    assert one == many
+    assert one.count(b"[WARN]") >= 50
+    if not flags[3]:
+        # without the conflicting duplicates the restated rules apply too
+        clean = "\n".join(ln for ln in body if ln not in ("7 8 2", "8 7 3")) + "\n"
+        cpath = str(tmp_path / "clean.adj")
+        with open(cpath, "w") as f:
+            f.write(clean)
+        got = ours(driver, cpath, flags)
+        n, src, dst, w = parse(clean, *flags)
+        for t, (gn, gm, rp, ci, v) in enumerate(got):
+            assert (gn, gm) == (n, len(src))
+            erp, eci, ev = O.csr_build(n, src, dst, w, transpose=t == 1)
+            assert np.array_equal(rp, erp) and np.array_equal(ci, eci) and np.array_equal(v, ev)
