@@ -350,8 +350,12 @@ private:
     static void parse_edge_line(std::string& line, const LoadEdgeOpts& opts,
                                 std::vector<EdgeUnit<edata_t, index_t>>& out,
                                 std::vector<std::string>& warnings) {
-        line = utils::StrStrip(line);
-        if (line.empty() || utils::StrStartWith(line, opts.comment_prefix)) return;
+        // utils::StrStrip's trim (" \t\n\r"), in place in the reused buffer
+        const auto first = line.find_first_not_of(" \t\n\r");
+        if (first == std::string::npos) return;
+        line.erase(line.find_last_not_of(" \t\n\r") + 1);
+        line.erase(0, first);
+        if (utils::StrStartWith(line, opts.comment_prefix)) return;
         char* save = nullptr;
         char* tok = strtok_r(line.data(), opts.line_sep.c_str(), &save);
         if (!tok) return;
