@@ -418,7 +418,7 @@ SERVING_GRAPHS = (("rmat", 16), ("rmat", 18), ("rmat", 20), ("rmat", 22),
 
 
 def serving_metrics(dev, n_requests: int, rate: float, sweep=(0.25, 0.5, 0.9, 1.5),
-                    seed: int = 20261203):
+                    seed: int = 20261203, lane_stretch: float = 0.0):
     """Serving loop over 8 resident graphs (RMAT 16/18/20/22 symmetrised and
     4-neighbour grids 512^2 .. 4096^2, uint32 weights in [1, 100]).
 
@@ -530,7 +530,7 @@ def serving_metrics(dev, n_requests: int, rate: float, sweep=(0.25, 0.5, 0.9, 1.
                 "served_over_plain_p99": round(plain["p99_ms"] / max(served["p99_ms"], 1e-9), 2),
                 "spot_results_agree": same}
 
-    with g1.Server(max_batch=256) as srv:
+    with g1.Server(max_batch=256, lane_stretch=lane_stretch) as srv:
         gids = [srv.add_graph(G) for G in graphs]
         # one warm-up query per engine kind and graph (state allocation)
         for gi, G in enumerate(graphs):

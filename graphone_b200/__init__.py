@@ -383,7 +383,8 @@ class ServerConfig(C.Structure):
     _fields_ = [("max_batch", C.c_uint32), ("reserve_bytes", C.c_uint64),
                 ("memory_limit", C.c_uint64), ("ppr_alpha", C.c_float),
                 ("ppr_iters", C.c_uint32), ("idle_release_ms", C.c_uint32),
-                ("solo_queue_ms", C.c_int32), ("solo_lanes", C.c_uint32)]
+                ("solo_queue_ms", C.c_int32), ("solo_lanes", C.c_uint32),
+                ("lane_stretch", C.c_float)]
 
 
 class ServerStats(C.Structure):
@@ -404,13 +405,15 @@ class Server:
     """
 
     def __init__(self, device=0, max_batch=0, reserve_bytes=0, memory_limit=0,
-                 ppr_alpha=0.0, ppr_iters=0, idle_release_ms=0, solo_queue_ms=0, solo_lanes=0):
+                 ppr_alpha=0.0, ppr_iters=0, idle_release_ms=0, solo_queue_ms=0, solo_lanes=0,
+                 lane_stretch=0.0):
         cfg = ServerConfig(max_batch, reserve_bytes, memory_limit, ppr_alpha, ppr_iters,
-                           idle_release_ms, solo_queue_ms, solo_lanes)
+                           idle_release_ms, solo_queue_ms, solo_lanes, lane_stretch)
         h = C.c_void_p()
         check(lib().g1_server_create(device, C.byref(cfg), C.byref(h)))
         self._h = h.value
         self._graphs = []  # keep the Graph objects alive while registered
+        self._outs = {}    # each query's output buffer, alive until it is done
 
     def add_graph(self, graph) -> int:
         gid = C.c_uint32()
@@ -419,19 +422,28 @@ class Server:
         return gid.value
 
     def submit(self, graph_id, kind, src, out) -> int:
+        """Queues one query; `out` is kept alive until wait or poll reports
+        the query done (the library writes into it until then)."""
         t = C.c_uint64()
         check(lib().g1_server_submit(self._h, graph_id, kind, src, _ptr(out), C.byref(t)))
+        self._outs[t.value] = out
         return t.value
 
     def poll(self, ticket):
         """None while running, else the latency in ms (raises if the query failed)."""
         done, lat = C.c_int(), C.c_double()
-        check(lib().g1_server_poll(self._h, ticket, C.byref(done), C.byref(lat)))
+        st = lib().g1_server_poll(self._h, ticket, C.byref(done), C.byref(lat))
+        if done.value or st != 0:
+            self._outs.pop(ticket, None)
+        check(st)
         return lat.value if done.value else None
 
     def wait(self, ticket, timeout_ms=0) -> float:
         lat = C.c_double()
-        check(lib().g1_server_wait(self._h, ticket, timeout_ms, C.byref(lat)))
+        st = lib().g1_server_wait(self._h, ticket, timeout_ms, C.byref(lat))
+        if st != 4:  # anything but a timeout: the query is done and forgotten
+            self._outs.pop(ticket, None)
+        check(st)
         return lat.value
 
     def stats(self, reset=False) -> dict:
@@ -443,6 +455,7 @@ class Server:
         if getattr(self, "_h", None):
             check(lib().g1_server_destroy(self._h))
             self._h = None
+            self._outs = {}
 
     def __del__(self):
         try:

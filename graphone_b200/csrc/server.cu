@@ -20,7 +20,8 @@
 // word costs about what a full word's does, and up to a few dozen queries
 // the single-source engines finish them sooner one by one.  So the server
 // also has solo lanes: worker threads that each run one query at a time,
-// oldest first across executors and never two of one graph at once, on the
+// never two of one graph at once, the next one chosen by lane_stretch (see
+// dispatch_lanes: shortest expected first, with waiting time counted in), on the
 // single-source engines (the calls a plain per-request user makes:
 // traverse.cu's AUTO engine, which picks the near-far engine on grids, and
 // pagerank.cu's SpMV PPR), each on its own stream.
@@ -110,6 +111,7 @@ struct Exec {
 // word of queries a slot step costs about as much as a full word's, which
 // single-source runs beat.
 constexpr double kSoloQueueMs = 20.0;
+constexpr double kLaneStretch = 2.0;
 constexpr size_t kSlotMinQueue = 32;
 // One lane by default: with two, the concurrent queries slowed each other
 // (p99 of the bench's mixed stream 1-10% above one lane's at every load; the
@@ -141,6 +143,7 @@ struct g1_server {
     uint32_t ppr_iters = 20;
     uint32_t idle_ms = 0;  // 0: engine state is kept until memory is needed
     double solo_queue_ms = kSoloQueueMs;  // negative: never solo
+    double lane_stretch = kLaneStretch;   // <= 0: the lanes take the oldest query first
     std::vector<std::unique_ptr<Exec>> execs;  // graph * 3 + kind
     std::mutex mu;                             // everything below
     std::condition_variable cv_in, cv_done;
@@ -159,8 +162,8 @@ struct g1_server {
     std::mutex graphs_mu;  // add_graph vs the loop's view of execs
     std::atomic<size_t> n_execs{0};
     // The solo lanes: worker threads each running one query at a time on
-    // the single-source engines, oldest first across executors (the order
-    // and engines of plain per-request calls), never two of one graph.
+    // the single-source engines (the engines of plain per-request calls),
+    // never two of one graph.
     std::vector<std::unique_ptr<g1::Lane>> lanes;
 };
 
@@ -388,13 +391,22 @@ bool lane_mode(const g1_server* S, const Exec& E) {
 // Hands each free lane the oldest waiting query of the executors in lane
 // mode whose graph no other lane is working on (the calls of one graph
 // would only wait for each other's lock).
+// Which waiting query a free lane takes: the head of the executor with the
+// lowest score, expected_ms - waited_ms / lane_stretch (expected_ms: the
+// executor's moving average of its lane queries, 0 until one has run).
+// Short queries go first, so a burst of them does not queue behind a long
+// traversal, while a query's own wait keeps lowering its score: a query
+// expected to take T ms longer than the others waits at most about
+// lane_stretch * T before it is next.  lane_stretch <= 0: oldest first.
 bool dispatch_lanes(g1_server* S, bool stopping) {
     if (stopping) return false;
     bool any = false;
+    const auto now = Clock::now();
     for (auto& Lp : S->lanes) {
         Lane* L = Lp.get();
         if (L->busy.load()) continue;
         Exec* best = nullptr;
+        double best_score = 0.0;
         const size_t ne = S->n_execs.load();
         for (size_t i = 0; i < ne; ++i) {
             Exec& E = *S->execs[i];
@@ -402,7 +414,13 @@ bool dispatch_lanes(g1_server* S, bool stopping) {
             bool graph_busy = false;
             for (const auto& O : S->lanes) graph_busy |= O->busy.load() && O->graph.load() == E.g;
             if (graph_busy) continue;
-            if (!best || E.pending.front()->t_sub < best->pending.front()->t_sub) best = &E;
+            const double waited = std::chrono::duration<double, std::milli>(now - E.pending.front()->t_sub).count();
+            const double score =
+                S->lane_stretch > 0.0 ? E.solo_ms.load() - waited / S->lane_stretch : -waited;
+            if (!best || score < best_score) {
+                best = &E;
+                best_score = score;
+            }
         }
         if (!best) break;  // no other lane would find one either
         Request* r = best->pending.front();
@@ -595,6 +613,7 @@ extern "C" g1_status g1_server_create(int device, const g1_server_config* cfg, g
         if (cfg->idle_release_ms) S->idle_ms = cfg->idle_release_ms;
         if (cfg->solo_queue_ms) S->solo_queue_ms = cfg->solo_queue_ms;
         if (cfg->solo_lanes > 16) return fail(G1_ERR_INVALID, "solo_lanes above 16");
+        if (cfg->lane_stretch != 0.0f) S->lane_stretch = cfg->lane_stretch;
     }
     // executors for up to 4096 graphs; the vector never reallocates
     S->execs.reserve(3 * 4096);

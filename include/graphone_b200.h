@@ -363,8 +363,9 @@ g1_status g1_ppr_batch(g1_graph* g, const uint32_t* srcs, uint32_t k, float alph
  * dozens of queries at once, so while an executor's slots are empty and
  * fewer than 32 queries wait (or the waiting ones would finish within
  * solo_queue_ms one by one), its queries take the server's solo lanes:
- * worker threads (solo_lanes) each running one query at a time, oldest
- * first across graphs and kinds, never two of one graph at once, on the
+ * worker threads (solo_lanes) each running one query at a time, shortest
+ * expected first across graphs and kinds with waiting time counted in
+ * (lane_stretch), never two of one graph at once, on the
  * single-source engines (the results of g1_sssp / g1_bfs with
  * G1_ENGINE_AUTO and of g1_ppr).  SSSP and BFS on graphs of small uniform
  * degree -- grids -- always take a lane (the near-far engine).  Executors of different graphs / kinds run
@@ -391,6 +392,12 @@ typedef struct {
                                  (grid SSSP / BFS stay on the near-far engine) */
     uint32_t solo_lanes;      /* worker threads running such queries, one each, never two
                                  of one graph at a time; 0 = 1, at most 16 */
+    float lane_stretch;       /* which waiting query a free lane takes: the lowest
+                                 expected_ms - waited_ms / lane_stretch, expected_ms being
+                                 the moving average of that graph and kind's lane queries
+                                 (short ones first; a query expected T ms longer than the
+                                 others waits at most about lane_stretch * T); 0 = 2;
+                                 negative = oldest first */
 } g1_server_config;
 typedef struct {
     uint64_t submitted, completed, failed;

@@ -306,6 +306,39 @@ def test_served_queries_run_solo_while_few_wait(cuda):
     assert O.rel_l1(pp[0], ppr_oracle(g, srcs[0])) < PPR_TOL
 
 
+@pytest.mark.parametrize("stretch", [4.0, -1.0])
+def test_lane_takes_short_queries_first_unless_told_oldest_first(cuda, stretch):
+    """While a long grid traversal runs on the lane, a second long one (another
+    grid) and then twelve short ones (a small RMAT graph) arrive.  With
+    lane_stretch > 0 the lane takes the short ones first (their expected
+    time is far lower and none has waited long); with a negative stretch it
+    takes the oldest, the second grid.  Every result is the plain call's."""
+    grids = [g1.Graph.from_gen(gen.grid2d(700, 700, (1, 100), seed=s)) for s in (1, 2)]
+    g = gen.rmat(10, 16, True, (1, 100))
+    small = g1.Graph.from_gen(g)
+    srcs = [int(x) for x in gen.pick_sources(g, 12)]
+    with g1.Server(lane_stretch=stretch) as srv:
+        gids = [srv.add_graph(G) for G in grids + [small]]
+        # one query per executor first: the lane's time estimates
+        warm = [np.empty(G.n, np.uint32) for G in grids + [small]]
+        for gid, w in zip(gids, warm):
+            srv.wait(srv.submit(gid, g1.QUERY_SSSP, 0, w), 120000)
+        outs = [np.empty(grids[0].n, np.uint32), np.empty(grids[1].n, np.uint32)]
+        t_long = [srv.submit(gids[0], g1.QUERY_SSSP, 5, outs[0]),
+                  srv.submit(gids[1], g1.QUERY_SSSP, 7, outs[1])]
+        so = [np.empty(g.n, np.uint32) for _ in srcs]
+        t_short = [srv.submit(gids[2], g1.QUERY_SSSP, s, so[i]) for i, s in enumerate(srcs)]
+        lat_long = [srv.wait(t, 120000) for t in t_long]
+        lat_short = [srv.wait(t, 120000) for t in t_short]
+    for i, s in enumerate(srcs):
+        assert np.array_equal(so[i], small.sssp(s)), i
+    assert np.array_equal(outs[0], grids[0].sssp(5)) and np.array_equal(outs[1], grids[1].sssp(7))
+    if stretch > 0:
+        assert max(lat_short) < lat_long[1], (lat_short, lat_long)
+    else:
+        assert min(lat_short) > lat_long[1], (lat_short, lat_long)
+
+
 def test_served_device_and_pinned_outputs(cuda):
     g = gen.rmat(11, 16, True, (1, 100))
     G = g1.Graph.from_gen(g)
