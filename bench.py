@@ -768,8 +768,7 @@ def run_ours(args):
         # names a CUDA fault reads as a fault of this run
         "status": ("not run: GraphOne's own GPU engines faulted on this pool (its sssp_blas app "
                    "ended in an invalid-address-space error on an RMAT-12 input), so they are no "
-                   "longer run; figures measured before the fault are in "
-                   "profiles/reference_gpu_engines.md")}
+                   "longer run; the figures measured before the fault are kept with the profiles")}
     # query and serving measurements are single-GPU: rank 0 runs them
     if not args.no_queries and rank == 0:
         result["queries"] = query_metrics(dev, stream, parity)
