@@ -152,64 +152,6 @@ pr_outw_from_transpose_kernel(const uint32_t* tcol, const float* tval, uint32_t 
         if (bins[i] != 0.0f) atomicAdd(&outw[i], bins[i]);
 }
 
-constexpr int kEagerOutwChunks = 8;
-
-// Uploads the in-edge CSR's columns and f32 values from host memory in
-// chunks on s; a second stream sums each chunk's out-weights as soon as it
-// has arrived (workspace "pr_outw", what PageRank's first call would
-// otherwise compute after the whole copy), so only the last chunk's
-// histogram is left when the copy ends.  s waits for the histograms.
-g1_status upload_transpose_with_outw(g1_graph* g, const uint32_t* col, const void* val, cudaStream_t s) {
-    Orientation& o = g->o[1];
-    const uint32_t n = g->n, m = g->m;
-    float* outw = nullptr;
-    G1_TRY(g->ws.get("pr_outw", n, &outw));
-    G1_CUDA(cudaMemsetAsync(outw, 0, (size_t)n * 4, s));
-    // chunk starts at multiples of 1024 edges: 16-byte aligned for the
-    // kernel's vector loads
-    const size_t chunk = (ceil_div((size_t)m, (size_t)kEagerOutwChunks) + 1023) & ~size_t(1023);
-    cudaStream_t h = nullptr;
-    G1_CUDA(cudaStreamCreateWithFlags(&h, cudaStreamNonBlocking));
-    cudaEvent_t ev[kEagerOutwChunks + 1] = {};
-    g1_status st = G1_OK;
-    auto check = [&](cudaError_t e, const char* what) {
-        if (st == G1_OK && e != cudaSuccess) st = fail_cuda(e, what);
-        return st == G1_OK;
-    };
-    int used = 0;
-    for (int c = 0; c < kEagerOutwChunks && st == G1_OK; ++c) {
-        const size_t lo = (size_t)c * chunk;
-        if (lo >= m) break;
-        const size_t cnt = std::min(chunk, (size_t)m - lo);
-        if (!check(cudaMemcpyAsync(o.col + lo, col + lo, cnt * 4, cudaMemcpyHostToDevice, s), "upload col"))
-            break;
-        if (!check(cudaMemcpyAsync(static_cast<char*>(o.val) + lo * 4, static_cast<const char*>(val) + lo * 4,
-                                   cnt * 4, cudaMemcpyHostToDevice, s),
-                   "upload val"))
-            break;
-        if (!check(cudaEventCreateWithFlags(&ev[c], cudaEventDisableTiming), "event")) break;
-        used = c + 1;
-        if (!check(cudaEventRecord(ev[c], s), "event record")) break;
-        if (!check(cudaStreamWaitEvent(h, ev[c], 0), "stream wait")) break;
-        pr_outw_from_transpose_kernel<8192, 1024><<<(uint32_t)g->sm_count * 2, 1024, 0, h>>>(
-            o.col + lo, static_cast<const float*>(o.val) + lo, (uint32_t)cnt, n, outw);
-        count_launches(1);
-        check(cudaGetLastError(), "pr_outw_from_transpose_kernel");
-    }
-    // s continues after the histograms, whatever happened above
-    cudaEvent_t& done = ev[kEagerOutwChunks];
-    if (check(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "event") &&
-        check(cudaEventRecord(done, h), "event record"))
-        check(cudaStreamWaitEvent(s, done, 0), "stream wait");
-    else
-        cudaStreamSynchronize(h);
-    for (int c = 0; c < used; ++c) cudaEventDestroy(ev[c]);
-    if (done) cudaEventDestroy(done);
-    cudaStreamDestroy(h);  // released once its work completes
-    if (st == G1_OK) g->outw_ready = true;
-    return st;
-}
-
 // iweights = alpha / out-weight (0 for a vertex without out-weight,
 // apps/pagerank_blas.cu:41-53), the initial ranks 1/N, x0 = rank0 * iw,
 // x1 = 0 where there is no out-weight (never written after), and the
@@ -382,10 +324,162 @@ static g1_status pr_hot_layout(g1_graph* g, const uint32_t* keys, cudaStream_t s
     } else {
         G1_TRY(g->ws.get("pr_hot", n, &hot));
     }
+    h.max_deg = in.max_deg;
     h.tuned_sched = in.tuned_sched;
     h.tuned_variant = in.tuned_variant;
     *t = 2;
     *xperm = hot;
+    return G1_OK;
+}
+
+constexpr int kEagerOutwChunks = 8;
+// the chunks whose out-weights order the hot-column layout built during an upload
+constexpr int kEagerHotChunks = 6;
+
+__global__ void pr_max_row_kernel(const uint32_t* rp, uint32_t n, uint32_t* out) {
+    uint32_t mx = 0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride)
+        mx = max(mx, rp[v + 1] - rp[v]);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31u) == 0 && mx) atomicMax(out, mx);
+}
+
+// Uploads the in-edge CSR's columns and f32 values from host memory in
+// chunks on s; a second stream sums each chunk's out-weights as soon as it
+// has arrived (workspace "pr_outw", what PageRank's first call would
+// otherwise compute after the whole copy), so only the last chunk's
+// histogram is left when the copy ends.  Where PageRank would build its
+// hot-column layout (degrees skewed: a row of more than 64 in-edges), the
+// second stream also builds it: once the first kEagerHotChunks chunks are
+// summed it orders the vertices by those partial out-weights (any order
+// gives the same ranks), remaps the arrived chunks' columns while the rest
+// are copied, and each later chunk as it arrives.  s waits for all of it.
+g1_status upload_transpose_with_outw(g1_graph* g, const uint32_t* col, const void* val, cudaStream_t s) {
+    Orientation& o = g->o[1];
+    const uint32_t n = g->n, m = g->m;
+    float* outw = nullptr;
+    G1_TRY(g->ws.get("pr_outw", n, &outw));
+    G1_CUDA(cudaMemsetAsync(outw, 0, (size_t)n * 4, s));
+    // chunk starts at multiples of 1024 edges: 16-byte aligned for the
+    // kernels' vector loads
+    const size_t chunk = (ceil_div((size_t)m, (size_t)kEagerOutwChunks) + 1023) & ~size_t(1023);
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(ceil_div(n, 256), (uint64_t)g->sm_count * 8));
+    // the largest in-degree (the row offsets are on the device already),
+    // read back without holding up the chunks queued after it
+    const bool may_hot = g->hot_mode != G1_HOT_COLUMNS_OFF && m >= kHotLayoutMinEdges &&
+                         (size_t)(kEagerHotChunks + 1) * chunk <= m;
+    uint32_t* d_max = nullptr;
+    cudaEvent_t ev_max = nullptr;
+    if (may_hot) {
+        G1_TRY(g->ws.get("pr_up_max", 4, &d_max));
+        G1_TRY(g->ws.pinned.ensure(64));
+        G1_CUDA(cudaMemsetAsync(d_max, 0, 4, s));
+        pr_max_row_kernel<<<grid, 256, 0, s>>>(o.rp, n, d_max);
+        count_launches(1);
+        G1_CUDA(cudaGetLastError());
+        G1_CUDA(cudaMemcpyAsync(g->ws.pinned.p, d_max, 4, cudaMemcpyDeviceToHost, s));
+        G1_CUDA(cudaEventCreateWithFlags(&ev_max, cudaEventDisableTiming));
+        G1_CUDA(cudaEventRecord(ev_max, s));
+    }
+    cudaStream_t h = nullptr;
+    G1_CUDA(cudaStreamCreateWithFlags(&h, cudaStreamNonBlocking));
+    cudaEvent_t ev[kEagerOutwChunks + 1] = {};
+    g1_status st = G1_OK;
+    auto check = [&](cudaError_t e, const char* what) {
+        if (st == G1_OK && e != cudaSuccess) st = fail_cuda(e, what);
+        return st == G1_OK;
+    };
+    Orientation& hc = g->o[2];
+    uint32_t* hot = nullptr;
+    DevBuf sorted, ids, order, temp;  // released to the block cache (reused after a device sync)
+    bool build_hot = false;
+    auto remap = [&](size_t lo, size_t cnt) {
+        pr_hot_cols_kernel<<<(uint32_t)g->sm_count * 8, 256, 0, h>>>(o.col + lo, (uint32_t)cnt, hot,
+                                                                     hc.b_col.as<uint32_t>() + lo);
+        count_launches(1);
+        check(cudaGetLastError(), "pr_hot_cols_kernel");
+    };
+    int used = 0;
+    for (int c = 0; c < kEagerOutwChunks && st == G1_OK; ++c) {
+        const size_t lo = (size_t)c * chunk;
+        if (lo >= m) break;
+        const size_t cnt = std::min(chunk, (size_t)m - lo);
+        if (!check(cudaMemcpyAsync(o.col + lo, col + lo, cnt * 4, cudaMemcpyHostToDevice, s), "upload col"))
+            break;
+        if (!check(cudaMemcpyAsync(static_cast<char*>(o.val) + lo * 4, static_cast<const char*>(val) + lo * 4,
+                                   cnt * 4, cudaMemcpyHostToDevice, s),
+                   "upload val"))
+            break;
+        if (!check(cudaEventCreateWithFlags(&ev[c], cudaEventDisableTiming), "event")) break;
+        used = c + 1;
+        if (!check(cudaEventRecord(ev[c], s), "event record")) break;
+        if (!check(cudaStreamWaitEvent(h, ev[c], 0), "stream wait")) break;
+        pr_outw_from_transpose_kernel<8192, 1024><<<(uint32_t)g->sm_count * 2, 1024, 0, h>>>(
+            o.col + lo, static_cast<const float*>(o.val) + lo, (uint32_t)cnt, n, outw);
+        count_launches(1);
+        if (!check(cudaGetLastError(), "pr_outw_from_transpose_kernel")) break;
+        if (build_hot) remap(lo, cnt);
+        if (may_hot && c == kEagerHotChunks - 1) {
+            // the copies queued so far keep the copy engine busy meanwhile
+            if (!check(cudaEventSynchronize(ev_max), "event sync")) break;
+            const uint32_t max_in = *g->ws.pinned.as<uint32_t>();
+            if (max_in <= kHotLayoutMinMaxDegree && g->hot_mode == G1_HOT_COLUMNS_AUTO) continue;
+            size_t tb = 0;
+            if (!check(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, (const uint32_t*)nullptr,
+                                                                 (uint32_t*)nullptr, (const uint32_t*)nullptr,
+                                                                 (uint32_t*)nullptr, (int)n, 0, 32, h),
+                       "sort size"))
+                break;
+            // all memory first: a graph without room for the copy simply
+            // gets it (or not) at PageRank's first call
+            g1_status a = g->ws.get("pr_hot", n, &hot);
+            if (a == G1_OK) a = sorted.ensure((size_t)n * 4 + 16);
+            if (a == G1_OK) a = ids.ensure((size_t)n * 4 + 16);
+            if (a == G1_OK) a = order.ensure((size_t)n * 4 + 16);
+            if (a == G1_OK) a = temp.ensure(tb + 16);
+            if (a == G1_OK) a = hc.b_col.ensure(((size_t)m + kWarpTilePad + 64) * 4);
+            if (a != G1_OK) {
+                hc.b_col.release();
+                continue;
+            }
+            const size_t nz_used = (size_t)m * 4;
+            if (!check(cudaMemsetAsync(hc.b_col.as<char>() + nz_used, 0, hc.b_col.bytes - nz_used, h), "pad"))
+                break;
+            const uint32_t* keys = reinterpret_cast<const uint32_t*>(outw);
+            pr_iota_kernel<<<grid, 256, 0, h>>>(ids.as<uint32_t>(), n);
+            if (!check(cub::DeviceRadixSort::SortPairsDescending(temp.p, tb, keys, sorted.as<uint32_t>(),
+                                                                 ids.as<uint32_t>(), order.as<uint32_t>(),
+                                                                 (int)n, 0, 32, h),
+                       "sort"))
+                break;
+            pr_hot_rank_kernel<<<grid, 256, 0, h>>>(order.as<uint32_t>(), n, hot);
+            count_launches(2);
+            if (!check(cudaGetLastError(), "hot ids")) break;
+            build_hot = true;
+            remap(0, lo + cnt);  // the chunks that have arrived
+        }
+    }
+    // s continues after the histograms (and the remaps), whatever happened above
+    cudaEvent_t& done = ev[kEagerOutwChunks];
+    if (check(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "event") &&
+        check(cudaEventRecord(done, h), "event record"))
+        check(cudaStreamWaitEvent(s, done, 0), "stream wait");
+    else
+        cudaStreamSynchronize(h);
+    for (int c = 0; c < used; ++c) cudaEventDestroy(ev[c]);
+    if (done) cudaEventDestroy(done);
+    if (ev_max) cudaEventDestroy(ev_max);
+    cudaStreamDestroy(h);  // released once its work completes
+    if (st != G1_OK) return st;
+    g->outw_ready = true;
+    if (build_hot) {
+        hc.rp = o.rp;
+        hc.col = hc.b_col.as<uint32_t>();
+        hc.val = o.val;
+        hc.present = true;
+    }
     return G1_OK;
 }
 

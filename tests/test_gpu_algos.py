@@ -217,23 +217,28 @@ def test_pagerank_rmat20_within_1e6_of_fp64(cuda, relabel):
 
 def test_pagerank_outweights_summed_during_upload(cuda):
     """A directed in-edge CSR of 2^22 edges or more with f32 values, from
-    host memory, has its out-weights summed chunk by chunk while it is
-    copied.  Same ranks as a graph built from device arrays (summed on
-    PageRank's first call; the integer-valued weights sum exactly in any
-    order), within 1e-6 of FP64; a column out of range is still rejected
-    (the chunk histograms skip it)."""
+    host memory, has its out-weights summed and its hot-column copy built
+    chunk by chunk while it is copied.  Same ranks as a graph built from
+    device arrays (both made at PageRank's first call; the integer-valued
+    weights sum exactly in any order, and any column order gives the same
+    bits), within 1e-6 of FP64; a column out of range is still rejected (the
+    chunk histograms skip it)."""
     import torch
     g = gen.rmat(19, 16, False, float_values=True)
     assert g.m >= 1 << 22
     trp, tci, tv = g.np("t")
     ref = O.pagerank_f64(trp, tci, tv, 0.85, 30, 1)
-    runs = []
+    runs, created_bytes = [], []
     for host_input, validate in ((True, True), (True, False), (False, True)):
         args = (trp, tci, tv) if host_input else tuple(
             torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).cuda() for a in (trp, tci, tv))
         G = g1.Graph.from_csr(*args, input_transpose=True, build_other=False, validate=validate)
+        created_bytes.append(G.device_bytes())
         runs.append(G.pagerank(0.85, 30, g1.PR_DANGLING))
         G.close()
+    # from host memory the hot-column copy (4 bytes per edge) was built during
+    # the upload too; from device memory at PageRank's first call
+    assert created_bytes[0] >= created_bytes[2] + 4 * g.m
     assert np.array_equal(runs[0], runs[1]) and np.array_equal(runs[0], runs[2])
     assert O.rel_l1(runs[0], ref) < 1e-6  # tolerance: relative L1 vs the FP64 oracle
     bad = tci.copy()
