@@ -102,7 +102,8 @@ struct Exec {
     bool lane_only = false;
     bool hybrid = false;
     std::atomic<bool> on_lane{false};  // one of its queries runs on a lane
-    std::atomic<double> solo_ms{0.0};  // moving average of its lane query time
+    std::atomic<double> solo_ms{0.0};  // moving average of its lane query time (0: none yet)
+    std::atomic<uint32_t> solo_runs{0};  // lane queries run
 };
 
 // A hybrid executor batches on its slot engine once at least kSlotMinQueue
@@ -355,8 +356,12 @@ void lane_worker(g1_server* S, Lane* L) {
                                      static_cast<uint32_t*>(r->out), nullptr, ls);
         }
         const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
-        const double prev = E->solo_ms.load();
-        E->solo_ms.store(prev == 0.0 ? ms : 0.75 * prev + 0.25 * ms);
+        // the first lane query of an executor also pays one-time costs
+        // (engine state, plans, captured CUDA graphs): it sets no estimate
+        if (E->solo_runs.fetch_add(1) > 0) {
+            const double prev = E->solo_ms.load();
+            E->solo_ms.store(prev == 0.0 ? ms : 0.75 * prev + 0.25 * ms);
+        }
         complete_one(S, r, st);
         {
             std::lock_guard<std::mutex> lk(L->mu);

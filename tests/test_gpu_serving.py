@@ -319,13 +319,18 @@ def test_lane_takes_short_queries_first_unless_told_oldest_first(cuda, stretch):
     srcs = [int(x) for x in gen.pick_sources(g, 12)]
     with g1.Server(lane_stretch=stretch) as srv:
         gids = [srv.add_graph(G) for G in grids + [small]]
-        # one query per executor first: the lane's time estimates
+        # a few queries per executor first: the lane's time estimates (its
+        # first query, which pays one-time costs, sets none)
         warm = [np.empty(G.n, np.uint32) for G in grids + [small]]
-        for gid, w in zip(gids, warm):
-            srv.wait(srv.submit(gid, g1.QUERY_SSSP, 0, w), 120000)
+        for _ in range(3):
+            for gid, w in zip(gids, warm):
+                srv.wait(srv.submit(gid, g1.QUERY_SSSP, 0, w), 120000)
         outs = [np.empty(grids[0].n, np.uint32), np.empty(grids[1].n, np.uint32)]
-        t_long = [srv.submit(gids[0], g1.QUERY_SSSP, 5, outs[0]),
-                  srv.submit(gids[1], g1.QUERY_SSSP, 7, outs[1])]
+        t_long = [srv.submit(gids[0], g1.QUERY_SSSP, 5, outs[0])]
+        # the first long query takes the idle lane at once (it runs ~8 ms);
+        # the rest arrive while it runs
+        time.sleep(0.003)
+        t_long.append(srv.submit(gids[1], g1.QUERY_SSSP, 7, outs[1]))
         so = [np.empty(g.n, np.uint32) for _ in srcs]
         t_short = [srv.submit(gids[2], g1.QUERY_SSSP, s, so[i]) for i, s in enumerate(srcs)]
         lat_long = [srv.wait(t, 120000) for t in t_long]
